@@ -1,0 +1,149 @@
+"""ctypes mirror of the C ABI in include/sapb.h.
+
+The struct layouts here must match the header field for field; the
+``test_abi_layout`` test checks sizes against the compiled library.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+SAPB_ABI_VERSION = 1
+
+SAPB_OK = 0
+SAPB_ERR_INVALID_ARGUMENT = -100
+SAPB_ERR_UNSUPPORTED = -101
+SAPB_ERR_CUDA = -102
+SAPB_ERR_WORKSPACE_TOO_SMALL = -103
+
+SAPB_LS_ASCENT_DIRECTION = -1
+SAPB_LS_ALPHA_UNDERFLOW = -2
+SAPB_LS_BAD_BRACKET = -3
+SAPB_LS_BAD_GUESS = -4
+SAPB_LS_ROOT_ITERATION_CAP = -5
+
+SAPB_CONTACT_MODE_NONE = 0
+SAPB_CONTACT_MODE_STICTION = 1
+SAPB_CONTACT_MODE_SLIDING = 2
+SAPB_CONTACT_MODE_FRICTIONLESS = 3
+
+SAPB_LS_MONOTONE_DECAY = 0
+SAPB_LS_ARMIJO_DECAY = 1
+SAPB_LS_EXACT_ROOT = 2
+
+SAPB_FP64 = 0
+SAPB_FP32 = 1
+
+LINE_SEARCH_VARIANTS = {
+    "monotone_decay": SAPB_LS_MONOTONE_DECAY,
+    "armijo_decay": SAPB_LS_ARMIJO_DECAY,
+    "exact_root": SAPB_LS_EXACT_ROOT,
+}
+
+_p = C.c_void_p
+
+
+class SolveOptions(C.Structure):
+    _fields_ = [
+        ("contact_beta", C.c_double),
+        ("contact_sigma", C.c_double),
+        ("contact_tau_d", C.c_double),
+        ("diag_shift", C.c_double),
+        ("max_iterations", C.c_int32),
+        ("optimality_abs_tol", C.c_double),
+        ("optimality_rel_tol", C.c_double),
+        ("cost_abs_tol", C.c_double),
+        ("cost_rel_tol", C.c_double),
+        ("line_search_max_iterations", C.c_int32),
+        ("armijo_c", C.c_double),
+        ("rho", C.c_double),
+        ("line_search_relative_slop", C.c_double),
+        ("line_search_variant", C.c_int32),
+        ("linear_solve_precision", C.c_int32),
+        ("hessian_precision", C.c_int32),
+        ("cubic_init", C.c_int32),
+    ]
+
+
+class DofTerms(C.Structure):
+    _fields_ = [
+        ("has_pd", C.c_int32),
+        ("has_limits", C.c_int32),
+        ("dof_coord_index", _p),
+        ("dof_target_index", _p),
+        ("limit_supported", _p),
+        ("joint_target_mode", _p),
+        ("joint_target_ke", _p),
+        ("joint_target_kd", _p),
+        ("joint_effort_limit", _p),
+        ("joint_limit_lower", _p),
+        ("joint_limit_upper", _p),
+        ("joint_limit_ke", _p),
+        ("joint_limit_kd", _p),
+        ("joint_q", _p),
+        ("joint_target_pos", _p),
+        ("joint_target_vel", _p),
+        ("joint_act", _p),
+    ]
+
+
+class ContactProblem(C.Structure):
+    _fields_ = [
+        ("num_envs", C.c_int32),
+        ("dof_per_env", C.c_int32),
+        ("max_contacts", C.c_int32),
+        ("contact_count", _p),
+        ("dynamics_matrix", _p),
+        ("jacobian", _p),
+        ("phi0", _p),
+        ("w_eff", _p),
+        ("mu", _p),
+        ("stiffness", _p),
+        ("tau_d", _p),
+        ("body0", _p),
+        ("body1", _p),
+        ("body_dof_start", _p),
+        ("body_dof_count", _p),
+        ("v_star", _p),
+        ("v0", _p),
+        ("v_guess", _p),
+        ("v_guess_active", _p),
+        ("dt", _p),
+        ("dof", C.POINTER(DofTerms)),
+    ]
+
+
+class SolveOutputs(C.Structure):
+    _fields_ = [
+        ("v", _p),
+        ("contact_gamma", _p),
+        ("contact_mode", _p),
+        ("cost", _p),
+        ("newton_iterations", _p),
+        ("line_search_iterations", _p),
+        ("converged", _p),
+        ("status", _p),
+        ("grad_norm", _p),
+    ]
+
+
+# name -> (restype, argtypes) of every symbol include/sapb.h declares.
+EXPORTS = {
+    "sapb_solve_options_default": (None, [C.POINTER(SolveOptions), C.c_int32]),
+    "sapb_abi_version": (C.c_int32, []),
+    "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
+    "sapb_contact_solve": (
+        C.c_int32,
+        [C.POINTER(ContactProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p, C.c_size_t, _p],
+    ),
+    "sapb_last_error": (C.c_char_p, []),
+}
+
+
+def bind(lib: C.CDLL) -> C.CDLL:
+    """Attach restype/argtypes for every exported symbol; raises if one is missing."""
+    for name, (restype, argtypes) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    return lib

@@ -1,0 +1,114 @@
+// sapb_capi.cu -- the extern "C" entry points declared in include/sapb.h.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "sapb_internal.h"
+
+namespace sapb {
+
+static thread_local char g_last_error[512] = {0};
+
+void set_last_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+}
+
+}  // namespace sapb
+
+extern "C" {
+
+int32_t sapb_abi_version(void) { return SAPB_ABI_VERSION; }
+
+const char* sapb_last_error(void) { return sapb::g_last_error; }
+
+void sapb_solve_options_default(sapb_solve_options* o, int32_t variant) {
+  // SapContactSolve defaults: sim/contact_solve.py:3299-3316 and 6129-6182.
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->contact_beta = 1.0;
+  o->contact_sigma = 1.0e-3;
+  o->contact_tau_d = 0.1;
+  o->diag_shift = 0.0;
+  o->max_iterations = 100;
+  o->optimality_abs_tol = 1.0e-14;
+  o->optimality_rel_tol = 1.0e-6;
+  o->line_search_variant = variant;
+  o->cost_abs_tol = variant == SAPB_LS_MONOTONE_DECAY ? 0.0 : 1.0e-30;
+  o->cost_rel_tol = variant == SAPB_LS_MONOTONE_DECAY ? 5.0e-3 : 1.0e-15;
+  o->line_search_max_iterations = variant == SAPB_LS_EXACT_ROOT ? 100 : 40;
+  o->armijo_c = 1.0e-4;
+  o->rho = 0.8;
+  o->line_search_relative_slop = 1000.0 * 2.220446049250313e-16;
+  o->linear_solve_precision = SAPB_FP64;
+  o->hessian_precision = SAPB_FP64;
+  o->cubic_init = 1;
+}
+
+size_t sapb_contact_solve_workspace_size(int32_t num_envs, int32_t dof_per_env, int32_t max_contacts) {
+  (void)num_envs;
+  (void)dof_per_env;
+  (void)max_contacts;
+  return 256;  // the persistent kernel's work counter, padded
+}
+
+int32_t sapb_contact_solve(const sapb_contact_problem* p, const sapb_solve_options* o, const sapb_solve_outputs* out,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+  if (!p || !o || !out || !out->v) {
+    sapb::set_last_error("sapb_contact_solve: null problem, options or output velocity");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->num_envs < 0 || p->dof_per_env <= 0 || p->max_contacts < 0) {
+    sapb::set_last_error("sapb_contact_solve: bad sizes num_envs=%d dof_per_env=%d max_contacts=%d", p->num_envs,
+                         p->dof_per_env, p->max_contacts);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->dof_per_env > 64) {
+    sapb::set_last_error("sapb_contact_solve: dof_per_env=%d > 64 is not supported by the on-chip solve",
+                         p->dof_per_env);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if (!p->contact_count || !p->dynamics_matrix || !p->v_star || !p->v0 || !p->dt) {
+    sapb::set_last_error("sapb_contact_solve: missing required input array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->max_contacts > 0 && (!p->jacobian || !p->phi0 || !p->w_eff || !p->mu || !p->stiffness)) {
+    sapb::set_last_error("sapb_contact_solve: missing contact array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->dof && (p->dof->has_pd || p->dof->has_limits) && (!p->dof->dof_coord_index || !p->dof->joint_q)) {
+    sapb::set_last_error("sapb_contact_solve: PD/limit terms requested without dof maps");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->dof && p->dof->has_pd &&
+      (!p->dof->dof_target_index || !p->dof->joint_target_mode || !p->dof->joint_target_ke ||
+       !p->dof->joint_target_kd || !p->dof->joint_effort_limit)) {
+    sapb::set_last_error("sapb_contact_solve: PD terms requested without drive arrays");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->dof && p->dof->has_limits &&
+      (!p->dof->limit_supported || !p->dof->joint_limit_lower || !p->dof->joint_limit_upper ||
+       !p->dof->joint_limit_ke || !p->dof->joint_limit_kd)) {
+    sapb::set_last_error("sapb_contact_solve: limit terms requested without limit arrays");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (o->line_search_variant < SAPB_LS_MONOTONE_DECAY || o->line_search_variant > SAPB_LS_EXACT_ROOT) {
+    sapb::set_last_error("sapb_contact_solve: unknown line search variant %d", o->line_search_variant);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (o->line_search_variant == SAPB_LS_ARMIJO_DECAY && !(o->rho > 0.0 && o->rho < 1.0)) {
+    sapb::set_last_error("sapb_contact_solve: rho must lie in (0, 1), got %g", o->rho);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (!workspace || workspace_bytes < sapb_contact_solve_workspace_size(p->num_envs, p->dof_per_env, p->max_contacts)) {
+    sapb::set_last_error("sapb_contact_solve: workspace missing or smaller than sapb_contact_solve_workspace_size");
+    return SAPB_ERR_WORKSPACE_TOO_SMALL;
+  }
+  return sapb::contact_solve_launch(p, o, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

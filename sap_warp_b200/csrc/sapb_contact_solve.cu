@@ -1,0 +1,1033 @@
+// sapb_contact_solve.cu -- fused SAP stage-2 Newton solve, one CTA per world.
+//
+// Restates SapContactSolve.solve (sim/contact_solve.py:6129-6285) as ONE
+// persistent launch.  A CTA pulls a world index from a device counter, stages
+// the world's dynamics matrix A and contact Jacobian J in shared memory once,
+// and runs prepare (:4285-4429), the Newton loop (:5474-5655) and the chosen
+// line search (:2207-3175) entirely on chip.  Per Newton iteration it reads
+// nothing from HBM; per line-search trial it touches O(contacts + DOFs) data
+// because the contact velocity along the search line is vc + alpha * (J dv)
+// (vc is linear in v).  The reference issues ~35 launches per Newton
+// iteration and re-reads A and J on every trial.
+//
+// Precision: the gradient, costs, line search, velocity update and the
+// convergence test are FP64.  The Hessian H = A + J^T G J + diag and its LDL^T
+// factorization run in HT (double, or float for the mixed path).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+
+#include "sapb_device.cuh"
+#include "sapb_internal.h"
+
+namespace sapb {
+
+// Flag bits of the per-DOF flags array.
+constexpr int kFlagPd = 1, kFlagLo = 2, kFlagUp = 4, kFlagPart = 8;
+
+struct SolveParams {
+  sapb_contact_problem p;
+  sapb_dof_terms dof;  // copy of *p.dof (has_pd/has_limits 0 if none)
+  sapb_solve_options o;
+  sapb_solve_outputs out;
+  int32_t use_guess_flag_ptr_valid;
+  int32_t* queue;      // work counter (zeroed before launch)
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Shared-memory layout of one world.  Leading dimensions: ldJ multiple of 4
+// (16-byte aligned rows for the Hessian tiles), ldH odd (conflict-free column
+// reads in the triangular solves).
+struct Layout {
+  int n, C, ldJ, ldH, nb;
+  size_t off_A, off_J, off_Jh, off_GJ, off_H, off_vec, off_con, off_flags, total;
+  static constexpr int kVecs = 22;
+  static constexpr int kConPer = 28;
+};
+
+__host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
+  Layout L;
+  L.n = n;
+  L.C = C;
+  L.ldJ = (n + 3) / 4 * 4;
+  L.ldH = (n % 2 == 0) ? n + 1 : n;
+  L.nb = (n + 3) / 4;
+  size_t o = 0;
+  L.off_A = o;
+  o = align_up(o + sizeof(double) * (size_t)n * n, 16);
+  L.off_J = o;
+  o = align_up(o + sizeof(double) * (size_t)3 * C * L.ldJ, 16);
+  L.off_Jh = o;  // HT copy of J (aliases J when HT is double)
+  if (hsize == 4) o = align_up(o + sizeof(float) * (size_t)3 * C * L.ldJ, 16);
+  L.off_GJ = o;
+  o = align_up(o + (size_t)hsize * 3 * C * L.ldJ, 16);
+  L.off_H = o;
+  o = align_up(o + (size_t)hsize * n * L.ldH, 16);
+  L.off_vec = o;
+  o = align_up(o + sizeof(double) * (size_t)Layout::kVecs * L.ldJ, 16);
+  L.off_con = o;
+  o = align_up(o + sizeof(double) * (size_t)Layout::kConPer * (C > 0 ? C : 1), 16);
+  L.off_flags = o;
+  o = align_up(o + sizeof(int) * (size_t)L.ldJ, 16);
+  L.total = o;
+  return L;
+}
+
+// Vector slots inside off_vec (each ldJ doubles).
+enum Vec {
+  V_V = 0, V_VSTAR, V_DV, V_GRAD, V_DYN, V_ARES, V_IMP, V_DP, V_DSCALE, V_AINV,
+  V_PDA, V_PDGAIN, V_PDLIM, V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_TMP1
+};
+// Contact slots inside off_con (each C doubles).
+enum Con {
+  C_RT = 0, C_RN, C_RTINV, C_RNINV, C_VHAT, C_MU, C_MUHAT, C_FACTOR, C_VC, C_DVC = C_VC + 3, C_GAMMA = C_DVC + 3,
+  C_G = C_GAMMA + 3, C_COST = C_G + 9, C_END = C_COST + 2
+};
+static_assert(C_END <= Layout::kConPer, "contact slots");
+
+template <int NT, typename HT>
+struct World {
+  const Layout& L;
+  double* A;
+  double* J;
+  HT* Jh;
+  HT* GJ;
+  HT* H;
+  double* vec;
+  double* con;
+  int* flags;
+  double* red;
+  int n, count;
+  __device__ double* V(int k) const { return vec + (size_t)k * L.ldJ; }
+  __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
+  __device__ ContactConst cc(int c) const {
+    ContactConst x;
+    x.rt = Cn(C_RT)[c];
+    x.rn = Cn(C_RN)[c];
+    x.rt_inv = Cn(C_RTINV)[c];
+    x.rn_inv = Cn(C_RNINV)[c];
+    x.vhat_n = Cn(C_VHAT)[c];
+    x.mu = Cn(C_MU)[c];
+    x.mu_hat = Cn(C_MUHAT)[c];
+    x.factor = Cn(C_FACTOR)[c];
+    return x;
+  }
+};
+
+// rows r < 3*count of J times a vector x (length n, shared) -> out[c*3+k] at
+// slot base (C_VC or C_DVC).  One warp per row, lanes over columns.
+template <int NT, typename HT>
+__device__ void contact_rows_times(const World<NT, HT>& w, const double* x, int slot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rows = 3 * w.count;
+  for (int r = warp; r < rows; r += NT / 32) {
+    const double* row = w.J + (size_t)r * w.L.ldJ;
+    double s = 0.0;
+    for (int j = lane; j < w.n; j += 32) s += row[j] * x[j];
+    s = warp_sum<NT>(s);
+    if (lane == 0) {
+      const int c = r / 3, k = r - 3 * (r / 3);
+      w.Cn(slot + k)[c] = s;
+    }
+  }
+}
+
+// Objective at the current v (shared V_V): contact gamma/G/cost, A(v-v*), Av,
+// J^T gamma, PD and limit terms, gradient.  Returns {cost, |g|^2, |p|^2, |jc|^2}
+// (scaled, over participating DOFs) to every thread.  Restates
+// _solver_update_active sim/contact_solve.py:4080-4136.
+template <int NT, typename HT>
+__device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt, double out4[4]) {
+  const int tid = threadIdx.x;
+  contact_rows_times<NT, HT>(w, w.V(V_V), C_VC);
+  __syncthreads();
+  double csum = 0.0;
+  for (int c = tid; c < w.count; c += NT) {
+    const ContactConst cc = w.cc(c);
+    double g[3], cost, G[9];
+    project_contact(cc, w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cost, G);
+    w.Cn(C_GAMMA + 0)[c] = g[0];
+    w.Cn(C_GAMMA + 1)[c] = g[1];
+    w.Cn(C_GAMMA + 2)[c] = g[2];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) w.Cn(C_G + k)[c] = G[k];
+    csum += cost;
+  }
+  __syncthreads();
+  double model_cost = 0.0, g2 = 0.0, p2 = 0.0, j2 = 0.0;
+  const double* v = w.V(V_V);
+  const double* vs = w.V(V_VSTAR);
+  for (int i = tid; i < w.n; i += NT) {
+    double a_res = 0.0, a_v = 0.0;
+    for (int j = 0; j < w.n; ++j) {
+      const double aij = w.A[(size_t)j * w.n + i];  // symmetric: column i
+      a_res += aij * (v[j] - vs[j]);
+      a_v += aij * v[j];
+    }
+    double imp = 0.0;
+    const int rows = 3 * w.count;
+    for (int r = 0; r < rows; ++r) {
+      const int c = r / 3, k = r - 3 * c;
+      imp += w.J[(size_t)r * w.L.ldJ + i] * w.Cn(C_GAMMA + k)[c];
+    }
+    const double vi = v[i];
+    double mc = 0.5 * (vi - vs[i]) * a_res;
+    const int fl = w.flags[i];
+    double pdg = 0.0, hd = 0.0;
+    if (P.dof.has_pd && (fl & kFlagPd)) {
+      const double gain = w.V(V_PDGAIN)[i], lim = w.V(V_PDLIM)[i];
+      const double y = w.V(V_PDA)[i] - gain * vi;
+      pdg = dt * clamp_limit(y, lim);
+      hd += dt * gain * clamp_limit_derivative(y, lim);
+      if (gain > 0.0) mc += (dt / gain) * clamp_limit_antiderivative(y, lim);
+    }
+    double lg = 0.0;
+    if (P.dof.has_limits) {
+      double lc = 0.0;
+      if (fl & kFlagLo) {
+        const double g = w.V(V_LORINV)[i] * (w.V(V_LOVHAT)[i] - vi);
+        if (g > 0.0) {
+          lg += g;
+          hd += w.V(V_LORINV)[i];
+          lc += 0.5 * w.V(V_LOR)[i] * g * g;
+        }
+      }
+      if (fl & kFlagUp) {
+        const double g = w.V(V_UPRINV)[i] * (w.V(V_UPVHAT)[i] + vi);
+        if (g > 0.0) {
+          lg -= g;
+          hd += w.V(V_UPRINV)[i];
+          lc += 0.5 * w.V(V_UPR)[i] * g * g;
+        }
+      }
+      mc += lc;
+    }
+    imp += pdg + lg;
+    const double grad = a_res - imp;
+    w.V(V_ARES)[i] = a_res;
+    w.V(V_DYN)[i] = a_v;
+    w.V(V_IMP)[i] = imp;
+    w.V(V_GRAD)[i] = grad;
+    w.V(V_HDIAG)[i] = hd;
+    model_cost += mc;
+    if (fl & kFlagPart) {
+      const double s = w.V(V_DSCALE)[i];
+      const double gs = s * grad, ps = s * a_v, js = s * imp;
+      g2 += gs * gs;
+      p2 += ps * ps;
+      j2 += js * js;
+    }
+  }
+  double r[4] = {csum + model_cost, g2, p2, j2};
+  block_sum<NT, 4>(r, w.red);
+  out4[0] = r[0];
+  out4[1] = r[1];
+  out4[2] = r[2];
+  out4[3] = r[3];
+}
+
+// H = A + J^T G J + diag(PD + limit + shift), lower triangle, in HT.
+// GJ rows are formed first; the product uses 4x4 register tiles with the
+// contact rows split into KS slices that add into H in turn (deterministic).
+template <int NT, typename HT>
+__device__ void assemble_hessian(const World<NT, HT>& w, double diag_shift) {
+  const int tid = threadIdx.x;
+  const int n = w.n, ldJ = w.L.ldJ, ldH = w.L.ldH, rows = 3 * w.count;
+  // GJ = G_c J_c per contact (rows 3c..3c+2), zero in padded columns.
+  for (int e = tid; e < rows * ldJ; e += NT) {
+    const int r = e / ldJ, j = e - r * ldJ;
+    const int c = r / 3, k = r - 3 * c;
+    HT val = HT(0);
+    if (j < n) {
+      const double* Jc = w.J + (size_t)(3 * c) * ldJ;
+      const double g0 = w.Cn(C_G + 3 * k + 0)[c], g1 = w.Cn(C_G + 3 * k + 1)[c], g2 = w.Cn(C_G + 3 * k + 2)[c];
+      val = HT(g0 * Jc[j] + g1 * Jc[ldJ + j] + g2 * Jc[2 * ldJ + j]);
+    }
+    w.GJ[(size_t)r * ldJ + j] = val;
+  }
+  // H lower = A lower (+ diagonal terms)
+  for (int e = tid; e < n * n; e += NT) {
+    const int i = e / n, j = e - i * n;
+    if (j <= i) {
+      double a = w.A[(size_t)i * n + j];
+      if (i == j) a += w.V(V_HDIAG)[i] + diag_shift;
+      w.H[(size_t)i * ldH + j] = HT(a);
+    }
+  }
+  __syncthreads();
+  const int nb = w.L.nb;
+  const int tiles = nb * (nb + 1) / 2;
+  int ks = NT / (tiles > 0 ? tiles : 1);
+  if (ks < 1) ks = 1;
+  if (ks > 8) ks = 8;
+  const int items = tiles * ks;
+  const int per = (rows + ks - 1) / ks;
+  for (int slice = 0; slice < ks; ++slice) {
+    for (int it = tid; it < items; it += NT) {
+      const int t = it / ks, s = it - t * ks;
+      if (s != slice) continue;
+      // tile t -> (bi, bj) with bj <= bi
+      int bi = 0;
+      while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+      const int bj = t - bi * (bi + 1) / 2;
+      const int r0 = s * per, r1 = min(rows, r0 + per);
+      HT acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = HT(0);
+      for (int r = r0; r < r1; ++r) {
+        const HT* jr = w.Jh + (size_t)r * ldJ + 4 * bi;
+        const HT* gr = w.GJ + (size_t)r * ldJ + 4 * bj;
+        HT x[4], y[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          x[a] = jr[a];
+          y[a] = gr[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = 4 * bi + a;
+        if (i >= n) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int j = 4 * bj + b;
+          if (j > i || j >= n) continue;
+          w.H[(size_t)i * ldH + j] += acc[a][b];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// In-place LDL^T of the lower triangle of H (unit L stored below the
+// diagonal unscaled as H_ik, D on the diagonal) followed by the solve
+// H dv = -grad.  Mathematically the Cholesky solve of the reference's
+// BlockCholeskySolverBatched (sim/blocked_cholesky.py:414-604).  Returns
+// false (every thread) if a pivot is not positive/finite: dv is then NaN so
+// the line search reports an ascent direction like the reference's NaN factor.
+template <int NT, typename HT>
+__device__ bool factor_and_solve(const World<NT, HT>& w) {
+  const int tid = threadIdx.x;
+  const int n = w.n, ldH = w.L.ldH;
+  HT* H = w.H;
+  bool ok = true;
+  for (int k = 0; k < n; ++k) {
+    const HT d = H[(size_t)k * ldH + k];
+    if (!(d > HT(0)) || !isfinite(double(d))) ok = false;
+    const HT rinv = HT(1) / d;
+    // trailing update of rows i > k, columns k < j <= i
+    const int m = n - k - 1;
+    const int cnt = m * (m + 1) / 2;
+    for (int e = tid; e < cnt; e += NT) {
+      // e -> (ii, jj) lower-triangular within the trailing block
+      int ii = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+      while ((ii + 1) * (ii + 2) / 2 <= e) ++ii;
+      while (ii * (ii + 1) / 2 > e) --ii;
+      const int jj = e - ii * (ii + 1) / 2;
+      const int i = k + 1 + ii, j = k + 1 + jj;
+      H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + k] * rinv) * H[(size_t)j * ldH + k];
+    }
+    __syncthreads();
+  }
+  // Solve with one warp: forward z = D^-1 (L^-1 b), backward x = L^-T z.
+  double* dv = w.V(V_DV);
+  if (tid < 32) {
+    const int lane = tid;
+    double b0 = 0.0, b1 = 0.0;  // rows lane, lane + 32
+    if (lane < n) b0 = -w.V(V_GRAD)[lane];
+    if (lane + 32 < n) b1 = -w.V(V_GRAD)[lane + 32];
+    HT hb0 = HT(b0), hb1 = HT(b1);
+    for (int k = 0; k < n; ++k) {
+      const HT bk = __shfl_sync(0xffffffffu, k < 32 ? hb0 : hb1, k & 31);
+      const HT zk = bk / H[(size_t)k * ldH + k];
+      if (lane == (k & 31)) {
+        if (k < 32) hb0 = zk;
+        else hb1 = zk;
+      }
+      if (lane > k && lane < n) hb0 -= H[(size_t)lane * ldH + k] * zk;
+      if (lane + 32 > k && lane + 32 < n) hb1 -= H[(size_t)(lane + 32) * ldH + k] * zk;
+    }
+    // now hb = z; backward: x_i = z_i - (sum_{k>i} H_ki x_k) / d_i
+    HT s0 = HT(0), s1 = HT(0);
+    for (int i = n - 1; i >= 0; --i) {
+      HT xi_local = HT(0);
+      if (lane == (i & 31)) {
+        const HT zi = i < 32 ? hb0 : hb1;
+        const HT si = i < 32 ? s0 : s1;
+        xi_local = zi - si / H[(size_t)i * ldH + i];
+        if (i < 32) hb0 = xi_local;
+        else hb1 = xi_local;
+      }
+      const HT xi = __shfl_sync(0xffffffffu, xi_local, i & 31);
+      if (lane < i) s0 += H[(size_t)i * ldH + lane] * xi;
+      if (lane + 32 < i) s1 += H[(size_t)i * ldH + lane + 32] * xi;
+    }
+    const double nanv = __longlong_as_double(0x7ff8000000000000ULL);
+    if (lane < n) dv[lane] = ok ? double(hb0) : nanv;
+    if (lane + 32 < n) dv[lane + 32] = ok ? double(hb1) : nanv;
+  }
+  __syncthreads();
+  return ok;
+}
+
+// Regularizer terms along the line at step alpha (contact, PD and limit
+// costs), the impulse projection onto dv, and (want2) the curvature.
+// Restates _replace_trial_cost_with_sap_line_search_cost :2379-2420, the line
+// derivative :2304-2321 and the second derivative :2324-2375, using
+// vc(alpha) = vc + alpha * dvc.
+template <int NT, typename HT>
+__device__ void line_terms(const World<NT, HT>& w, const SolveParams& P, double dt, double alpha, bool want2,
+                           double out3[3]) {
+  const int tid = threadIdx.x;
+  double reg = 0.0, proj = 0.0, curv = 0.0;
+  for (int c = tid; c < w.count; c += NT) {
+    const ContactConst cc = w.cc(c);
+    const double dx = w.Cn(C_DVC + 0)[c], dy = w.Cn(C_DVC + 1)[c], dz = w.Cn(C_DVC + 2)[c];
+    double g[3], cost, G[9];
+    project_contact(cc, w.Cn(C_VC + 0)[c] + alpha * dx, w.Cn(C_VC + 1)[c] + alpha * dy,
+                    w.Cn(C_VC + 2)[c] + alpha * dz, g, &cost, want2 ? G : nullptr);
+    reg += cost;
+    proj += g[0] * dx + g[1] * dy + g[2] * dz;
+    if (want2) {
+      curv += dx * (G[0] * dx + G[1] * dy + G[2] * dz) + dy * (G[3] * dx + G[4] * dy + G[5] * dz) +
+              dz * (G[6] * dx + G[7] * dy + G[8] * dz);
+    }
+  }
+  if (P.dof.has_pd || P.dof.has_limits) {
+    for (int i = tid; i < w.n; i += NT) {
+      const double vi = w.V(V_V)[i] + alpha * w.V(V_DV)[i];
+      const double dvi = w.V(V_DV)[i];
+      const int fl = w.flags[i];
+      double hd = 0.0;
+      if (P.dof.has_pd && (fl & kFlagPd)) {
+        const double gain = w.V(V_PDGAIN)[i], lim = w.V(V_PDLIM)[i];
+        const double y = w.V(V_PDA)[i] - gain * vi;
+        proj += dvi * dt * clamp_limit(y, lim);
+        hd += dt * gain * clamp_limit_derivative(y, lim);
+        if (gain > 0.0) reg += (dt / gain) * clamp_limit_antiderivative(y, lim);
+      }
+      if (P.dof.has_limits) {
+        if (fl & kFlagLo) {
+          const double g = w.V(V_LORINV)[i] * (w.V(V_LOVHAT)[i] - vi);
+          if (g > 0.0) {
+            proj += dvi * g;
+            hd += w.V(V_LORINV)[i];
+            reg += 0.5 * w.V(V_LOR)[i] * g * g;
+          }
+        }
+        if (fl & kFlagUp) {
+          const double g = w.V(V_UPRINV)[i] * (w.V(V_UPVHAT)[i] + vi);
+          if (g > 0.0) {
+            proj -= dvi * g;
+            hd += w.V(V_UPRINV)[i];
+            reg += 0.5 * w.V(V_UPR)[i] * g * g;
+          }
+        }
+      }
+      curv += hd * dvi * dvi;
+    }
+  }
+  double r[3] = {reg, proj, curv};
+  block_sum<NT, 3>(r, w.red);
+  out3[0] = r[0];
+  out3[1] = r[1];
+  out3[2] = r[2];
+}
+
+struct LsResult {
+  int accepted, status, iterations;
+  double alpha, accepted_cost;
+};
+
+// Line coefficients (sim/contact_solve.py:2234-2263, 1657-1692):
+// dp = A dv, dvc = J dv and {dell0, dell_a0, d2ell_a, mom0}.
+template <int NT, typename HT>
+__device__ void line_coefficients(const World<NT, HT>& w, double c4[4]) {
+  const int tid = threadIdx.x;
+  contact_rows_times<NT, HT>(w, w.V(V_DV), C_DVC);
+  double d0 = 0.0, da0 = 0.0, d2 = 0.0, m0 = 0.0;
+  const double* v = w.V(V_V);
+  const double* vs = w.V(V_VSTAR);
+  const double* dv = w.V(V_DV);
+  for (int i = tid; i < w.n; i += NT) {
+    double acc = 0.0;
+    for (int j = 0; j < w.n; ++j) acc += w.A[(size_t)j * w.n + i] * dv[j];
+    w.V(V_DP)[i] = acc;
+    const double ri = v[i] - vs[i];
+    d0 += w.V(V_GRAD)[i] * dv[i];
+    da0 += acc * ri;
+    d2 += dv[i] * acc;
+    m0 += 0.5 * ri * w.V(V_ARES)[i];
+  }
+  double r[4] = {d0, da0, d2, m0};
+  block_sum<NT, 4>(r, w.red);  // its barriers also publish dvc / dp
+  c4[0] = r[0];
+  c4[1] = r[1];
+  c4[2] = r[2];
+  c4[3] = r[3];
+}
+
+__device__ __forceinline__ bool armijo_ok(double alpha, double ell, double ell0, double dell0, double c) {
+  return ell < ell0 + c * alpha * dell0;  // sim/sap_helpers.py:2600-2608
+}
+
+// armijo_decay backtracking (sim/contact_solve.py:2670-2904, driver :5108-5305).
+template <int NT, typename HT>
+__device__ LsResult ls_armijo(const World<NT, HT>& w, const SolveParams& P, double dt, double cost) {
+  const sapb_solve_options& o = P.o;
+  LsResult r{0, 0, 0, 0.0, cost};
+  double c4[4];
+  line_coefficients<NT, HT>(w, c4);
+  const double dell0 = c4[0], dell_a0 = c4[1], d2ell_a = c4[2], mom0 = c4[3];
+  const double amax = 1.0 / o.rho;
+  const double slop_rel = o.line_search_relative_slop;
+  double alpha = amax, alpha_prev = amax, ell_prev = cost;
+  double ell_slop = (slop_rel / 10.0) * fmax(1.0, fabs(cost));
+  r.alpha = alpha;
+  if (o.line_search_max_iterations <= 0) return r;
+  if (dell0 >= 0.0 || !isfinite(dell0)) {
+    r.status = SAPB_LS_ASCENT_DIRECTION;
+    return r;
+  }
+  double t3[3];
+  line_terms<NT, HT>(w, P, dt, alpha, false, t3);
+  double ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + t3[0];
+  const double deriv = dell_a0 + alpha * d2ell_a - t3[1];
+  {
+    const double scale = fmax(1.0, 0.5 * (fabs(ell) + fabs(cost)));
+    const double slop = (slop_rel / 10.0) * scale;
+    ell_slop = slop;
+    if (deriv < 0.0 || deriv < slop) {
+      r.accepted = 1;
+      r.accepted_cost = ell;
+      return r;
+    }
+    alpha_prev = alpha;
+    ell_prev = ell;
+  }
+  if (o.line_search_max_iterations <= 1) return r;
+  for (int iteration = 1;; ++iteration) {
+    alpha = alpha * o.rho;
+    line_terms<NT, HT>(w, P, dt, alpha, false, t3);
+    ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + t3[0];
+    const double a = alpha, a_prev = alpha_prev, e_prev = ell_prev;
+    const double denom = a - a_prev;
+    double dell_approx = 0.0;
+    if (fabs(denom) > 0.0) dell_approx = (ell - e_prev) / denom;
+    int accept = 0, accept_prev = 0;
+    if (fabs(dell_approx) < ell_slop) {
+      accept = 1;
+    } else if (ell > e_prev && armijo_ok(a, ell, cost, dell0, o.armijo_c)) {
+      accept = 1;
+      if (armijo_ok(a_prev, e_prev, cost, dell0, o.armijo_c)) accept_prev = 1;
+    }
+    if (accept) {
+      r.accepted = 1;
+      r.iterations = iteration;
+      r.alpha = accept_prev ? a_prev : a;
+      r.accepted_cost = accept_prev ? e_prev : ell;
+      return r;
+    }
+    if (iteration >= o.line_search_max_iterations - 1) {
+      r.alpha = alpha;
+      if (armijo_ok(alpha, ell, cost, dell0, o.armijo_c)) {
+        r.accepted = 1;
+        r.iterations = o.line_search_max_iterations;
+        r.accepted_cost = ell;
+      } else {
+        r.status = SAPB_LS_ALPHA_UNDERFLOW;
+      }
+      return r;
+    }
+    alpha_prev = a;
+    ell_prev = ell;
+  }
+}
+
+// monotone_decay (fused kernel sim/contact_solve.py:2483-2667).
+template <int NT, typename HT>
+__device__ LsResult ls_monotone(const World<NT, HT>& w, const SolveParams& P, double dt, double cost) {
+  const sapb_solve_options& o = P.o;
+  LsResult r{0, 0, 0, 1.0, cost};
+  double c4[4];
+  line_coefficients<NT, HT>(w, c4);
+  const double base_linear = c4[1], base_quadratic = c4[2], base0 = c4[3];
+  double alpha = 1.0, trial = cost;
+  for (int it = 0; it < o.line_search_max_iterations; ++it) {
+    double t3[3];
+    line_terms<NT, HT>(w, P, dt, alpha, false, t3);
+    trial = base0 + alpha * base_linear + 0.5 * alpha * alpha * base_quadratic + t3[0];
+    r.iterations += 1;
+    const double tol = 1.0e-14 + 1.0e-12 * fabs(cost);
+    if (trial <= cost + tol) {
+      r.accepted = 1;
+      break;
+    }
+    alpha = alpha * 0.5;
+    if (alpha < 1.0e-8) {
+      r.status = SAPB_LS_ALPHA_UNDERFLOW;
+      break;
+    }
+  }
+  r.alpha = alpha;
+  r.accepted_cost = r.accepted ? trial : cost;
+  return r;
+}
+
+// exact_root (sim/contact_solve.py:2914-3140, driver :5700-5861).
+template <int NT, typename HT>
+__device__ LsResult ls_exact(const World<NT, HT>& w, const SolveParams& P, double dt, double cost) {
+  const sapb_solve_options& o = P.o;
+  LsResult r{0, 0, 0, kExactAlphaMax, cost};
+  const int max_it = o.line_search_max_iterations;
+  if (max_it <= 0) return r;
+  double c4[4];
+  line_coefficients<NT, HT>(w, c4);
+  const double dell0 = c4[0], dell_a0 = c4[1], d2ell_a = c4[2], mom0 = c4[3];
+  const double amax = kExactAlphaMax;
+  if (dell0 >= 0.0 || !isfinite(dell0)) {
+    r.status = SAPB_LS_ASCENT_DIRECTION;
+    return r;
+  }
+  double t3[3];
+  line_terms<NT, HT>(w, P, dt, amax, true, t3);
+  const double ell = mom0 + amax * dell_a0 + 0.5 * amax * amax * d2ell_a + t3[0];
+  const double deriv = dell_a0 + amax * d2ell_a - t3[1];
+  const double deriv2 = d2ell_a + t3[2];
+  bool active = false;
+  double scale = 0, x_lo = 0, x_hi = 0, f_hi = 0, root = 0, mdx = 0, mdx_prev = 0, xtol = 0;
+  if (deriv <= 0.0) {
+    r.accepted = 1;
+    r.alpha = amax;
+  } else if (-dell0 < o.cost_abs_tol + o.cost_rel_tol * ell) {
+    r.accepted = 1;
+    r.alpha = 1.0;
+  } else {
+    scale = -dell0;
+    const double f_upper = deriv / scale;
+    if (!isfinite(f_upper) || f_upper <= 0.0) {
+      r.status = SAPB_LS_BAD_BRACKET;
+    } else {
+      double guess = -dell0 / deriv2;
+      if (o.cubic_init) {
+        const double h = amax, c0 = cost, d0 = dell0, c1 = ell, d1 = deriv;
+        const double theta = d0 + d1 - 3.0 * (c1 - c0) / h;
+        const double disc = theta * theta - d0 * d1;
+        if (isfinite(disc) && disc >= 0.0) {
+          const double g = sqrt(disc);
+          const double denom = d1 - d0 + 2.0 * g;
+          if (denom != 0.0) {
+            const double cg = h - h * (d1 + g - theta) / denom;
+            if (isfinite(cg) && cg > 0.0 && cg <= h) guess = cg;
+          }
+        }
+      }
+      if (guess > amax) guess = amax;
+      if (!isfinite(guess) || guess < 0.0 || guess > amax || kExactFTol * guess <= 0.0) {
+        r.status = SAPB_LS_BAD_GUESS;
+      } else {
+        x_lo = 0.0;
+        x_hi = amax;
+        f_hi = f_upper;
+        root = guess;
+        mdx = -amax;
+        mdx_prev = -amax;
+        xtol = kExactFTol * guess;
+        r.alpha = guess;
+        active = true;
+      }
+    }
+  }
+  for (int iteration = 1; active; ++iteration) {
+    line_terms<NT, HT>(w, P, dt, r.alpha, true, t3);
+    const double d = dell_a0 + r.alpha * d2ell_a - t3[1];
+    const double d2 = d2ell_a + t3[2];
+    const double f = d / scale, df = d2 / scale;
+    const double f_upper = f_hi;
+    if ((f < 0.0 && f_upper >= 0.0) || (f >= 0.0 && f_upper < 0.0)) {
+      x_lo = root;
+    } else {
+      x_hi = root;
+      f_hi = f;
+    }
+    if (fabs(f) < kExactFTol) {
+      r.accepted = 1;
+      r.iterations = iteration;
+      r.alpha = root;
+      break;
+    }
+    if (iteration >= max_it) {
+      r.status = SAPB_LS_ROOT_ITERATION_CAP;
+      break;
+    }
+    const bool slow = 2.0 * fabs(f) > fabs(mdx_prev * df);
+    mdx_prev = mdx;
+    const double bis_mdx = 0.5 * (x_lo - x_hi);
+    const double bis_root = x_lo - bis_mdx;
+    double n_mdx = 0.0, n_root = root;
+    if (fabs(df) > 0.0) {
+      n_mdx = f / df;
+      n_root = root - n_mdx;
+    }
+    bool use_bisect = slow;
+    if (n_root < x_lo || n_root > x_hi) use_bisect = true;
+    if (!isfinite(n_root) || !isfinite(n_mdx)) use_bisect = true;
+    const double next_root = use_bisect ? bis_root : n_root;
+    const double next_mdx = use_bisect ? bis_mdx : n_mdx;
+    if (fabs(next_mdx) < xtol) {
+      r.accepted = 1;
+      r.iterations = iteration;
+      r.alpha = next_root;
+      break;
+    }
+    root = next_root;
+    mdx = next_mdx;
+    r.alpha = next_root;
+  }
+  if (r.accepted) {
+    line_terms<NT, HT>(w, P, dt, r.alpha, false, t3);
+    r.accepted_cost = mom0 + r.alpha * dell_a0 + 0.5 * r.alpha * r.alpha * d2ell_a + t3[0];
+  }
+  return r;
+}
+
+template <int NT, typename HT>
+__global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double red[8 * (NT / 32)];
+  __shared__ int s_world;
+  const int tid = threadIdx.x;
+  const int n = P.p.dof_per_env, C = P.p.max_contacts;
+  const Layout L = make_layout(n, C, (int)sizeof(HT));
+  const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
+
+  for (;;) {
+    if (tid == 0) s_world = atomicAdd(P.queue, 1);
+    __syncthreads();
+    const int e = s_world;
+    if (e >= P.p.num_envs) break;
+
+    World<NT, HT> w{L,
+                    reinterpret_cast<double*>(smem + L.off_A),
+                    reinterpret_cast<double*>(smem + L.off_J),
+                    reinterpret_cast<HT*>(smem + (sizeof(HT) == 4 ? L.off_Jh : L.off_J)),
+                    reinterpret_cast<HT*>(smem + L.off_GJ),
+                    reinterpret_cast<HT*>(smem + L.off_H),
+                    reinterpret_cast<double*>(smem + L.off_vec),
+                    reinterpret_cast<double*>(smem + L.off_con),
+                    reinterpret_cast<int*>(smem + L.off_flags),
+                    red,
+                    n,
+                    0};
+    int count = P.p.contact_count[e];
+    if (count > C) count = C;
+    if (count < 0) count = 0;
+    w.count = count;
+    const double dt = P.p.dt[e];
+    const size_t base = (size_t)e * n;
+
+    // ---- stage A, J, per-contact constants and vectors ----------------------
+    {
+      const double* Ag = P.p.dynamics_matrix + (size_t)e * n * n;
+      for (int k = tid; k < n * n; k += NT) w.A[k] = Ag[k];
+      const int rows = 3 * count;
+      const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n;
+      for (int k = tid; k < rows * L.ldJ; k += NT) {
+        const int r = k / L.ldJ, j = k - r * L.ldJ;
+        const double val = j < n ? Jg[(size_t)r * n + j] : 0.0;
+        w.J[k] = val;
+        if (sizeof(HT) == 4) w.Jh[k] = HT(val);
+      }
+      for (int c = tid; c < count; c += NT) {
+        const size_t ci = (size_t)e * C + c;
+        const double tau = P.p.tau_d ? P.p.tau_d[ci] : P.o.contact_tau_d;
+        const ContactConst cc = make_contact_const(P.p.phi0[ci], P.p.w_eff[ci], P.p.mu[ci], P.p.stiffness[ci], tau,
+                                                   P.o.contact_beta, P.o.contact_sigma, dt);
+        w.Cn(C_RT)[c] = cc.rt;
+        w.Cn(C_RN)[c] = cc.rn;
+        w.Cn(C_RTINV)[c] = cc.rt_inv;
+        w.Cn(C_RNINV)[c] = cc.rn_inv;
+        w.Cn(C_VHAT)[c] = cc.vhat_n;
+        w.Cn(C_MU)[c] = cc.mu;
+        w.Cn(C_MUHAT)[c] = cc.mu_hat;
+        w.Cn(C_FACTOR)[c] = cc.factor;
+      }
+      for (int i = tid; i < L.ldJ; i += NT) {
+        if (i < n) {
+          w.V(V_VSTAR)[i] = P.p.v_star[base + i];
+          double v = P.p.v0[base + i];
+          if (P.p.v_guess) {
+            if (use_guess) v = P.p.v_guess[base + i];
+            P.p.v_guess[base + i] = v;
+          }
+          w.V(V_V)[i] = v;
+          double d = Ag[(size_t)i * n + i];
+          if (d < 1.0e-12 || !isfinite(d)) d = 1.0e-12;
+          w.V(V_AINV)[i] = 1.0 / d;
+          w.V(V_DSCALE)[i] = 1.0 / sqrt(d);
+        } else {
+          for (int k = 0; k < Layout::kVecs; ++k) w.V(k)[i] = 0.0;
+        }
+      }
+    }
+    // ---- PD and limit terms (sim/contact_solve.py:490-683) ------------------
+    for (int i = tid; i < n; i += NT) {
+      int fl = 0;
+      const size_t dof = base + i;
+      const sapb_dof_terms& D = P.dof;
+      if (D.has_pd) {
+        const int coord = D.dof_coord_index[dof];
+        int target = D.dof_target_index[dof];
+        if (target < 0) target = (int)dof;
+        if (D.joint_target_mode[target] != 0) {
+          const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
+          if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {
+            double kpe, kde;
+            effective_pd_gains(kp, kd, dt, w.V(V_AINV)[i], &kpe, &kde);
+            const double gain = dt * kpe + kde;
+            if (gain > 0.0) {
+              double q0 = 0.0, qd = 0.0;
+              if (coord >= 0) {
+                q0 = D.joint_q[coord];
+                qd = D.joint_target_pos ? (double)D.joint_target_pos[target] : 0.0;
+              }
+              const double vd = D.joint_target_vel ? (double)D.joint_target_vel[target] : 0.0;
+              const double u0 = D.joint_act ? (double)D.joint_act[target] : 0.0;
+              fl |= kFlagPd;
+              w.V(V_PDA)[i] = kpe * (qd - q0) + kde * vd + u0;
+              w.V(V_PDGAIN)[i] = gain;
+              w.V(V_PDLIM)[i] = (double)D.joint_effort_limit[target];
+            }
+          }
+        }
+      }
+      w.V(V_LOR)[i] = 1.0;
+      w.V(V_UPR)[i] = 1.0;
+      if (D.has_limits) {
+        const int coord = D.dof_coord_index[dof];
+        const double ke = coord >= 0 ? D.joint_limit_ke[dof] : 0.0;
+        if (coord >= 0 && D.limit_supported[dof] != 0 && ke > 0.0) {
+          const double q0 = D.joint_q[coord];
+          const double lower = D.joint_limit_lower[dof], upper = D.joint_limit_upper[dof];
+          const double speed = fmax(fabs(P.p.v0[base + i]), fabs(w.V(V_VSTAR)[i]));
+          const double window = kLimitWindow * dt * speed;
+          const double kd = D.joint_limit_kd[dof];
+          const double tau_d = kd > 0.0 ? kd / ke : 0.0;
+          const double bf = kLimitBeta * kLimitBeta / (4.0 * kPi * kPi);
+          const double r_nr = bf * fmax(w.V(V_AINV)[i], 1.0e-12);
+          const double r_soft = 1.0 / (dt * ke * (dt + tau_d));
+          const double rr = fmax(r_nr, r_soft);
+          if (isfinite(lower) && q0 - lower <= window) {
+            fl |= kFlagLo;
+            w.V(V_LOVHAT)[i] = -(q0 - lower) / (dt + tau_d);
+            w.V(V_LOR)[i] = rr;
+            w.V(V_LORINV)[i] = 1.0 / rr;
+          }
+          if (isfinite(upper) && upper - q0 <= window) {
+            fl |= kFlagUp;
+            w.V(V_UPVHAT)[i] = -(upper - q0) / (dt + tau_d);
+            w.V(V_UPR)[i] = rr;
+            w.V(V_UPRINV)[i] = 1.0 / rr;
+          }
+        }
+      }
+      w.flags[i] = fl;
+    }
+    __syncthreads();
+    // ---- participating DOFs (sim/contact_solve.py:423-488) ------------------
+    int any_model_term = 0;
+    for (int i = tid; i < n; i += NT) {
+      int part = (w.flags[i] & (kFlagPd | kFlagLo | kFlagUp)) ? 1 : 0;
+      any_model_term |= part;
+      for (int c = 0; c < count && !part; ++c) {
+        const size_t ci = (size_t)e * C + c;
+        const int b0 = P.p.body0 ? P.p.body0[ci] : -1;
+        const int b1 = P.p.body1 ? P.p.body1[ci] : -1;
+        if (P.p.body_dof_start) {
+          if (b0 >= 0) {
+            const int s = P.p.body_dof_start[b0], m = P.p.body_dof_count[b0];
+            if (s >= 0 && m > 0 && i >= s && i < s + m) part = 1;
+          }
+          if (b1 >= 0) {
+            const int s = P.p.body_dof_start[b1], m = P.p.body_dof_count[b1];
+            if (s >= 0 && m > 0 && i >= s && i < s + m) part = 1;
+          }
+        }
+        const double* Jc = w.J + (size_t)(3 * c) * L.ldJ;
+        if (Jc[i] != 0.0 || Jc[L.ldJ + i] != 0.0 || Jc[2 * L.ldJ + i] != 0.0) part = 1;
+      }
+      if (part) w.flags[i] |= kFlagPart;
+    }
+    const int model_terms = __syncthreads_or(any_model_term);
+    const bool unconstrained = (count == 0) && !model_terms;
+
+    int newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
+    double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
+    bool evaluated = false;
+    if (unconstrained) {
+      converged = 1;
+      for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
+      __syncthreads();
+    } else {
+      for (int i = tid; i < n; i += NT)
+        if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
+      __syncthreads();
+      const double cost_min_alpha = P.o.line_search_variant == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
+      int it = 0;
+      bool active = true;
+      for (;;) {
+        double e4[4];
+        evaluate<NT, HT>(w, P, dt, e4);
+        evaluated = true;
+        cost = e4[0];
+        // convergence test (sim/contact_solve.py:2043-2087)
+        const double gn = sqrt(fmax(e4[1], 0.0)), pn = sqrt(fmax(e4[2], 0.0)), jn = sqrt(fmax(e4[3], 0.0));
+        grad_norm = gn;
+        const double opt_tol = P.o.optimality_abs_tol + P.o.optimality_rel_tol * fmax(pn, jn);
+        const bool opt = gn <= opt_tol;
+        bool cost_ok = false;
+        if (it > 0 && alpha > cost_min_alpha) {
+          const double sc = 0.5 * (fabs(cost) + fabs(previous_cost));
+          const double tol = P.o.cost_abs_tol + P.o.cost_rel_tol * sc;
+          if (fabs(cost - previous_cost) < tol) cost_ok = true;
+        }
+        newton_iterations = it;
+        if (opt || cost_ok) {
+          converged = 1;
+          active = false;
+        } else if (it >= P.o.max_iterations) {
+          active = false;
+        } else {
+          converged = 0;
+        }
+        if (!active) break;
+        // Newton direction
+        assemble_hessian<NT, HT>(w, P.o.diag_shift);
+        factor_and_solve<NT, HT>(w);
+        LsResult r;
+        if (P.o.line_search_variant == SAPB_LS_ARMIJO_DECAY)
+          r = ls_armijo<NT, HT>(w, P, dt, cost);
+        else if (P.o.line_search_variant == SAPB_LS_EXACT_ROOT)
+          r = ls_exact<NT, HT>(w, P, dt, cost);
+        else
+          r = ls_monotone<NT, HT>(w, P, dt, cost);
+        alpha = r.alpha;
+        status = r.status;
+        const bool mono = P.o.line_search_variant == SAPB_LS_MONOTONE_DECAY;
+        if (r.accepted || mono) ls_total += r.iterations;
+        if (r.accepted) {
+          previous_cost = cost;
+          for (int i = tid; i < n; i += NT) w.V(V_V)[i] += r.alpha * w.V(V_DV)[i];
+        } else if (mono) {
+          previous_cost = cost;
+        }
+        __syncthreads();
+        ++it;
+      }
+    }
+    // ---- outputs ------------------------------------------------------------
+    for (int i = tid; i < n; i += NT) P.out.v[base + i] = w.V(V_V)[i];
+    for (int c = tid; c < C; c += NT) {
+      const size_t ci = (size_t)e * C + c;
+      const bool live = evaluated && c < count;
+      if (P.out.contact_gamma) {
+        P.out.contact_gamma[ci * 3 + 0] = live ? w.Cn(C_GAMMA + 0)[c] : 0.0;
+        P.out.contact_gamma[ci * 3 + 1] = live ? w.Cn(C_GAMMA + 1)[c] : 0.0;
+        P.out.contact_gamma[ci * 3 + 2] = live ? w.Cn(C_GAMMA + 2)[c] : 0.0;
+      }
+      if (P.out.contact_mode) {
+        int mode = SAPB_CONTACT_MODE_NONE;
+        if (live) {
+          double g[3], cst;
+          mode = project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cst, nullptr);
+        }
+        P.out.contact_mode[ci] = mode;
+      }
+    }
+    if (tid == 0) {
+      if (P.out.cost) P.out.cost[e] = evaluated ? cost : 0.0;
+      if (P.out.newton_iterations) P.out.newton_iterations[e] = newton_iterations;
+      if (P.out.line_search_iterations) P.out.line_search_iterations[e] = ls_total;
+      if (P.out.converged) P.out.converged[e] = converged;
+      if (P.out.status) P.out.status[e] = status;
+      if (P.out.grad_norm) P.out.grad_norm[e] = grad_norm;
+    }
+    __syncthreads();
+  }
+}
+
+template <int NT, typename HT>
+static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
+  const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT));
+  auto kern = contact_solve_kernel<NT, HT>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  if (err != cudaSuccess) return err;
+  int dev = 0;
+  err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  int sms = 0;
+  err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, L.total);
+  if (err != cudaSuccess) return err;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  int blocks = sms * per_sm;
+  if (blocks > P.p.num_envs) blocks = P.p.num_envs;
+  if (blocks < 1) blocks = 1;
+  if (blocks_out) *blocks_out = blocks;
+  err = cudaMemsetAsync(P.queue, 0, sizeof(int32_t), stream);
+  if (err != cudaSuccess) return err;
+  kern<<<blocks, NT, L.total, stream>>>(P);
+  return cudaGetLastError();
+}
+
+size_t contact_solve_smem_bytes(int n, int C, int hessian_precision) {
+  return make_layout(n, C, hessian_precision == SAPB_FP32 ? 4 : 8).total;
+}
+
+int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_options* o, const sapb_solve_outputs* out,
+                             void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+  SolveParams P;
+  memset(&P, 0, sizeof(P));
+  P.p = *p;
+  if (p->dof) P.dof = *p->dof;
+  P.o = *o;
+  P.out = *out;
+  P.use_guess_flag_ptr_valid = (p->v_guess && p->v_guess_active) ? 1 : 0;
+  P.queue = reinterpret_cast<int32_t*>(workspace);
+  if (p->num_envs == 0) return SAPB_OK;
+  // The FP32 Hessian path also needs an FP32 linear solve: LDL^T in the
+  // Hessian type.  An FP64 Hessian with an FP32 factorization is not a
+  // separate kernel: the factor runs in FP64 then.
+  const bool fp32 = o->hessian_precision == SAPB_FP32 || o->linear_solve_precision == SAPB_FP32;
+  const size_t smem = contact_solve_smem_bytes(p->dof_per_env, p->max_contacts, fp32 ? SAPB_FP32 : SAPB_FP64);
+  if (smem > kMaxSmemPerBlock) {
+    set_last_error("contact solve: world too large for the on-chip path (shared memory %zu > %zu bytes)", smem,
+                   (size_t)kMaxSmemPerBlock);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  cudaError_t err;
+  if (fp32)
+    err = launch_solve<128, float>(P, stream, nullptr);
+  else
+    err = launch_solve<128, double>(P, stream, nullptr);
+  if (err != cudaSuccess) {
+    set_last_error("contact solve launch: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  (void)workspace_bytes;
+  return SAPB_OK;
+}
+
+}  // namespace sapb

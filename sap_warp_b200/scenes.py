@@ -1,0 +1,289 @@
+"""Seeded synthetic SAP problems with the shapes of the reference's workloads.
+
+No public dataset or scene file is involved: the reference ships no benchmark
+data, so every input here is generated from a seed.  The generators build a
+real kinematic tree (free base + revolute chain), its mass matrix
+A = M(q) + diag(armature) by the composite-rigid-body sum sum_b J_b^T I_b J_b,
+and contact rows J_c = R_WC^T J_point(p) at random points of random bodies,
+so A is SPD and J has the sparsity and scale of an articulated robot.
+
+Conventions follow the reference: spatial velocities are [omega; v] at the
+body origin, angular first (sim/sap_helpers.py:771-785); the free joint's six
+DOFs come first in SAP order; contact rows are (t1, t2, n) with the normal
+pointing from body0 (the ground, -1) to body1 (sim/contact_jacobian.py:404-562).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+def _skew(v: np.ndarray) -> np.ndarray:
+    """[v]x for a (..., 3) array -> (..., 3, 3)."""
+    z = np.zeros(v.shape[:-1], dtype=v.dtype)
+    return np.stack(
+        [
+            np.stack([z, -v[..., 2], v[..., 1]], -1),
+            np.stack([v[..., 2], z, -v[..., 0]], -1),
+            np.stack([-v[..., 1], v[..., 0], z], -1),
+        ],
+        -2,
+    )
+
+
+def _axis_angle(axis: np.ndarray, angle: np.ndarray) -> np.ndarray:
+    """Rotation matrices (..., 3, 3) for unit axes (3,) or (...,3) and angles (...)."""
+    axis = np.broadcast_to(axis, angle.shape + (3,))
+    K = _skew(axis)
+    s = np.sin(angle)[..., None, None]
+    c = np.cos(angle)[..., None, None]
+    eye = np.eye(3)
+    return eye + s * K + (1.0 - c) * (K @ K)
+
+
+def _random_rotations(rng: np.random.Generator, n: int) -> np.ndarray:
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    x, y, z, w = q.T
+    return np.stack(
+        [
+            np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+            np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+            np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+        ],
+        -2,
+    )
+
+
+@dataclass
+class ChainModel:
+    """A floating-base serial chain: body 0 is the base, body k>0 hangs from k-1
+    by a revolute joint about `axis[k]` (parent frame) at offset `offset[k]`."""
+
+    masses: np.ndarray  # (B,)
+    inertia: np.ndarray  # (B, 3, 3) body-frame inertia about the COM
+    com: np.ndarray  # (B, 3) COM in the body frame
+    axis: np.ndarray  # (B, 3) joint axis in the parent frame (row 0 unused)
+    offset: np.ndarray  # (B, 3) joint origin in the parent frame (row 0 unused)
+    armature: float
+
+    @property
+    def bodies(self) -> int:
+        return int(self.masses.shape[0])
+
+    @property
+    def dofs(self) -> int:
+        return 6 + self.bodies - 1
+
+
+def make_chain(rng: np.random.Generator, bodies: int, mass_range=(0.5, 2.0), link=0.12) -> ChainModel:
+    masses = rng.uniform(*mass_range, size=bodies)
+    masses[0] *= 4.0  # heavier torso/base
+    # diagonal-dominant SPD inertia: R diag(d) R^T + delta I
+    R = _random_rotations(rng, bodies)
+    d = rng.uniform(0.5, 2.0, size=(bodies, 3)) * masses[:, None] * link * link / 6.0
+    inertia = np.einsum("bij,bj,bkj->bik", R, d, R) + 1e-4 * np.eye(3)[None]
+    com = rng.uniform(-0.5, 0.5, size=(bodies, 3)) * link * 0.5
+    axis = rng.normal(size=(bodies, 3))
+    axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+    off = rng.normal(size=(bodies, 3))
+    off /= np.linalg.norm(off, axis=1, keepdims=True)
+    off *= link
+    return ChainModel(masses, inertia, com, axis, off, armature=0.01)
+
+
+def chain_kinematics(model: ChainModel, q_base_R: np.ndarray, q_base_p: np.ndarray, q_joint: np.ndarray):
+    """World rotations (E,B,3,3), origins (E,B,3) and the body Jacobians
+    (E,B,6,n) mapping SAP-order generalized velocities to [omega; v_origin]."""
+    E = q_joint.shape[0]
+    B = model.bodies
+    n = model.dofs
+    Rw = np.zeros((E, B, 3, 3))
+    ow = np.zeros((E, B, 3))
+    Rw[:, 0] = q_base_R
+    ow[:, 0] = q_base_p
+    axes_w = np.zeros((E, B, 3))
+    for k in range(1, B):
+        Rp = Rw[:, k - 1]
+        ow[:, k] = ow[:, k - 1] + np.einsum("eij,j->ei", Rp, model.offset[k])
+        axes_w[:, k] = np.einsum("eij,j->ei", Rp, model.axis[k])
+        Rw[:, k] = Rp @ _axis_angle(model.axis[k], q_joint[:, k - 1])
+    Jb = np.zeros((E, B, 6, n))
+    eye = np.eye(3)
+    for k in range(B):
+        # base angular DOFs 0..2 and linear DOFs 3..5 (world frame, base origin)
+        Jb[:, k, 0:3, 0:3] = eye
+        Jb[:, k, 3:6, 0:3] = -_skew(ow[:, k] - ow[:, 0])  # e x r = -[r]x e
+        Jb[:, k, 3:6, 3:6] = eye
+        for j in range(1, k + 1):
+            a = axes_w[:, j]
+            Jb[:, k, 0:3, 5 + j] = a
+            Jb[:, k, 3:6, 5 + j] = np.cross(a, ow[:, k] - ow[:, j])
+    return Rw, ow, Jb
+
+
+def chain_mass_matrix(model: ChainModel, Rw: np.ndarray, ow: np.ndarray, Jb: np.ndarray) -> np.ndarray:
+    """A = sum_b J_b^T I_b J_b + diag(armature on revolute DOFs), spatial
+    inertia about the body origin in the world frame, angular first."""
+    E, B = Rw.shape[:2]
+    n = model.dofs
+    A = np.zeros((E, n, n))
+    for k in range(B):
+        m = model.masses[k]
+        c = np.einsum("eij,j->ei", Rw[:, k], model.com[k])  # COM offset, world
+        Ic = Rw[:, k] @ model.inertia[k] @ np.swapaxes(Rw[:, k], -1, -2)
+        cx = _skew(c)
+        I6 = np.zeros((E, 6, 6))
+        I6[:, 0:3, 0:3] = Ic + m * np.swapaxes(cx, -1, -2) @ cx
+        I6[:, 0:3, 3:6] = m * cx
+        I6[:, 3:6, 0:3] = m * np.swapaxes(cx, -1, -2)
+        I6[:, 3:6, 3:6] = m * np.eye(3)
+        A += np.swapaxes(Jb[:, k], -1, -2) @ I6 @ Jb[:, k]
+    A[:, 6:, 6:] += model.armature * np.eye(n - 6)
+    return 0.5 * (A + np.swapaxes(A, -1, -2))
+
+
+def contact_frames(normals: np.ndarray) -> np.ndarray:
+    """Rows (t1, t2, n) of an orthonormal frame with third axis = normal."""
+    n = normals / np.linalg.norm(normals, axis=-1, keepdims=True)
+    helper = np.where(np.abs(n[..., 0:1]) < 0.9, np.array([1.0, 0.0, 0.0]), np.array([0.0, 1.0, 0.0]))
+    t1 = np.cross(helper, n)
+    t1 /= np.linalg.norm(t1, axis=-1, keepdims=True)
+    t2 = np.cross(n, t1)
+    return np.stack([t1, t2, n], axis=-2)
+
+
+@dataclass
+class ContactProblemArrays:
+    """Host arrays of one sapb_contact_problem (FP64 unless noted)."""
+
+    num_envs: int
+    dof_per_env: int
+    max_contacts: int
+    bodies_per_env: int
+    contact_count: np.ndarray  # int32 (E,)
+    dynamics_matrix: np.ndarray  # (E, n, n)
+    jacobian: np.ndarray  # (E, C, 3, n)
+    phi0: np.ndarray  # (E, C)
+    w_eff: np.ndarray
+    mu: np.ndarray
+    stiffness: np.ndarray
+    tau_d: np.ndarray
+    body0: np.ndarray  # int32 (E, C)
+    body1: np.ndarray
+    body_dof_start: np.ndarray  # int32 (E*B,)
+    body_dof_count: np.ndarray
+    v_star: np.ndarray  # (E*n,)
+    v0: np.ndarray
+    dt: np.ndarray  # (E,)
+
+    def subset(self, worlds: np.ndarray) -> "ContactProblemArrays":
+        """The same problem restricted to a list of worlds (bodies renumbered)."""
+        worlds = np.asarray(worlds, dtype=np.int64)
+        E, n, B = len(worlds), self.dof_per_env, self.bodies_per_env
+        remap = lambda b: np.where(b >= 0, (b % B) + np.arange(E)[:, None] * B, -1).astype(np.int32)
+        body_idx = (worlds[:, None] * B + np.arange(B)[None]).reshape(-1)
+        dof_idx = (worlds[:, None] * n + np.arange(n)[None]).reshape(-1)
+        return ContactProblemArrays(
+            E, n, self.max_contacts, B,
+            self.contact_count[worlds].copy(), self.dynamics_matrix[worlds].copy(), self.jacobian[worlds].copy(),
+            self.phi0[worlds].copy(), self.w_eff[worlds].copy(), self.mu[worlds].copy(),
+            self.stiffness[worlds].copy(), self.tau_d[worlds].copy(),
+            remap(self.body0[worlds]), remap(self.body1[worlds]),
+            self.body_dof_start[body_idx].copy(), self.body_dof_count[body_idx].copy(),
+            self.v_star[dof_idx].copy(), self.v0[dof_idx].copy(), self.dt[worlds].copy(),
+        )
+
+
+def diag_delassus_weight(jac: np.ndarray, A: np.ndarray) -> np.ndarray:
+    """w = max(||J diag(A)^-1 J^T||_F / 3, 1e-12) per contact
+    (sim/contact_jacobian.py:153-251, the diag_delassus mode)."""
+    dinv = 1.0 / np.clip(np.einsum("eii->ei", A), 1e-12, None)  # (E, n)
+    W = np.einsum("ecrj,ej,eckj->ecrk", jac, dinv, jac)
+    return np.maximum(np.linalg.norm(W, axis=(-2, -1)) / 3.0, 1e-12)
+
+
+def humanoid_contact_problem(
+    num_worlds: int,
+    seed: int = 2,
+    *,
+    revolute: int = 29,
+    contacts: tuple[int, int] = (8, 32),
+    max_contacts: int = 32,
+    dt: float = 2.0e-3,
+    phi0_range=(-2.0e-3, 0.0),
+    mu_range=(0.3, 1.0),
+    v_star_std: float = 0.5,
+    stiffness: float = 1.0e5,
+    tau_d: float = 0.01,
+    mass_range=(0.5, 2.0),
+) -> ContactProblemArrays:
+    """Batched floating-base serial-chain 'humanoid' worlds (6 + `revolute`
+    DOFs, one tree per world) with a random pose q, A = M(q) + armature,
+    C ~ U{contacts} foot/hand-style point contacts against the ground and
+    v* ~ N(0, v_star_std)."""
+    rng = np.random.default_rng(seed)
+    model = make_chain(rng, revolute + 1, mass_range=mass_range)
+    E, B, n, C = num_worlds, model.bodies, model.dofs, max_contacts
+    base_R = _random_rotations(rng, E)
+    base_p = np.stack([rng.uniform(-1, 1, E), rng.uniform(-1, 1, E), rng.uniform(0.8, 1.2, E)], -1)
+    qj = rng.uniform(-1.0, 1.0, size=(E, B - 1))
+    Rw, ow, Jb = chain_kinematics(model, base_R, base_p, qj)
+    A = chain_mass_matrix(model, Rw, ow, Jb)
+
+    count = rng.integers(contacts[0], contacts[1] + 1, size=E).astype(np.int32)
+    count = np.minimum(count, C)
+    # contacts favour the distal half of the chain (feet / hands)
+    bodies = rng.integers(B // 2, B, size=(E, C))
+    r_local = rng.normal(size=(E, C, 3))
+    r_local *= (rng.uniform(0.0, 0.05, size=(E, C)) / np.linalg.norm(r_local, axis=-1))[..., None]
+    Rb = np.take_along_axis(Rw, bodies[..., None, None], axis=1)  # (E,C,3,3)
+    r_world = np.einsum("ecij,ecj->eci", Rb, r_local)
+    normals = np.array([0.0, 0.0, 1.0]) + rng.normal(scale=0.1, size=(E, C, 3))
+    frame = contact_frames(normals)  # (E,C,3,3) rows t1,t2,n
+    Jsel = np.take_along_axis(Jb, bodies[..., None, None], axis=1)  # (E,C,6,n)
+    J_point = Jsel[:, :, 3:6, :] - np.einsum("ecij,ecjk->ecik", _skew(r_world), Jsel[:, :, 0:3, :])
+    jac = np.einsum("ecrj,ecjk->ecrk", frame, J_point)
+    live = np.arange(C)[None, :] < count[:, None]
+    jac *= live[..., None, None]
+
+    phi0 = rng.uniform(*phi0_range, size=(E, C)) * live
+    mu = rng.uniform(*mu_range, size=(E, C)) * live
+    w_eff = diag_delassus_weight(jac, A) * live
+    k = np.full((E, C), stiffness) * live
+    tau = np.full((E, C), tau_d) * live
+    body1 = np.where(live, bodies + np.arange(E)[:, None] * B, -1).astype(np.int32)
+    body0 = np.full((E, C), -1, dtype=np.int32)
+    v_star = rng.normal(scale=v_star_std, size=(E, n))
+    v0 = v_star + rng.normal(scale=0.01, size=(E, n))
+    return ContactProblemArrays(
+        num_envs=E,
+        dof_per_env=n,
+        max_contacts=C,
+        bodies_per_env=B,
+        contact_count=count,
+        dynamics_matrix=A,
+        jacobian=jac,
+        phi0=phi0,
+        w_eff=w_eff,
+        mu=mu,
+        stiffness=k,
+        tau_d=tau,
+        body0=body0,
+        body1=body1,
+        body_dof_start=np.zeros(E * B, dtype=np.int32),
+        body_dof_count=np.full(E * B, n, dtype=np.int32),
+        v_star=v_star.reshape(-1),
+        v0=v0.reshape(-1),
+        dt=np.full(E, dt),
+    )
+
+
+def quadruped_contact_problem(num_worlds: int, seed: int = 1, **kw) -> ContactProblemArrays:
+    """18-DOF floating-base stand-in (6 + 12 revolute) with <= 16 contacts."""
+    kw.setdefault("contacts", (4, 16))
+    kw.setdefault("max_contacts", 16)
+    kw.setdefault("mu_range", (0.5, 1.0))
+    return humanoid_contact_problem(num_worlds, seed, revolute=12, **kw)

@@ -1,0 +1,68 @@
+"""The C-ABI library loads without a GPU, exports every symbol include/sapb.h
+declares, and the ctypes mirror matches the header's struct layouts."""
+
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from sap_warp_b200 import _abi
+from sap_warp_b200.build import LIB_PATH, build_library
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADERS = sorted((ROOT / "include").glob("*.h"))
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(sapb_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build_library()
+    return _abi.bind(ctypes.CDLL(str(LIB_PATH)))
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert "sapb_contact_solve" in names
+    for name in names:
+        assert hasattr(lib, name), name
+    assert names <= set(_abi.EXPORTS), names - set(_abi.EXPORTS)
+
+
+def test_no_compute_entry_points_without_gpu(lib):
+    assert lib.sapb_abi_version() == _abi.SAPB_ABI_VERSION
+    o = _abi.SolveOptions()
+    lib.sapb_solve_options_default(ctypes.byref(o), _abi.SAPB_LS_EXACT_ROOT)
+    assert o.line_search_max_iterations == 100 and o.cost_rel_tol == 1e-15 and o.rho == 0.8
+    lib.sapb_solve_options_default(ctypes.byref(o), _abi.SAPB_LS_MONOTONE_DECAY)
+    assert o.cost_rel_tol == 5e-3 and o.cost_abs_tol == 0.0
+    assert lib.sapb_contact_solve_workspace_size(4096, 35, 32) >= 4
+    # argument errors are reported before any CUDA call
+    assert lib.sapb_contact_solve(None, None, None, None, 0, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert b"null" in lib.sapb_last_error()
+
+
+def test_struct_layout_matches_header(tmp_path):
+    src = tmp_path / "sizes.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "sapb.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(sapb_solve_options),"
+        " sizeof(sapb_dof_terms), sizeof(sapb_contact_problem), sizeof(sapb_solve_outputs),"
+        " offsetof(sapb_contact_problem, dof), offsetof(sapb_solve_options, cubic_init)); return 0;}\n"
+    )
+    exe = tmp_path / "sizes"
+    cc = "/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc"
+    subprocess.run([cc, "-I", str(ROOT / "include"), "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [ctypes.sizeof(_abi.SolveOptions), ctypes.sizeof(_abi.DofTerms), ctypes.sizeof(_abi.ContactProblem),
+            ctypes.sizeof(_abi.SolveOutputs), _abi.ContactProblem.dof.offset, _abi.SolveOptions.cubic_init.offset]
+    assert got == want
