@@ -91,6 +91,7 @@ typedef struct sapb_solve_options {
 typedef struct sapb_dof_terms {
   int32_t has_pd;                 /* _detect_model_pd_terms, :3760-3770 */
   int32_t has_limits;             /* _detect_model_limit_terms, :3772-3785 */
+  int32_t joint_coord_count;      /* length of joint_q; coordinates beyond it are ignored */
   const int32_t* dof_coord_index; /* [E*n] coordinate of each DOF or -1 */
   const int32_t* dof_target_index;/* [E*n] */
   const int32_t* limit_supported; /* [E*n] */
@@ -115,6 +116,7 @@ typedef struct sapb_contact_problem {
   int32_t num_envs;
   int32_t dof_per_env;
   int32_t max_contacts;           /* C: per-world slot capacity */
+  int32_t num_bodies;             /* length of body_dof_start / body_dof_count */
   const int32_t* contact_count;   /* [E] contacts per world (clamped to C) */
   const double* dynamics_matrix;  /* [E,n,n] */
   const double* jacobian;         /* [E,C,3,n] */
@@ -140,7 +142,7 @@ typedef struct sapb_contact_problem {
 typedef struct sapb_solve_outputs {
   double* v;                      /* [E*n] solved velocity (v_flat) */
   double* contact_gamma;          /* [E,C,3] impulses at the solution */
-  int32_t* contact_mode;          /* [E,C] projection mode at the last Hessian */
+  int32_t* contact_mode;          /* [E,C] projection mode at the returned velocity */
   double* cost;                   /* [E] */
   int32_t* newton_iterations;     /* [E] */
   int32_t* line_search_iterations;/* [E] accumulated accepted trials */

@@ -115,6 +115,7 @@ def solve(prob, line_search_variant: str = "monotone_decay", threads: int = 0, v
 
     P = _abi.ContactProblem()
     P.num_envs, P.dof_per_env, P.max_contacts = E, n, C
+    P.num_bodies = int(np.asarray(prob.body_dof_start).size)
     P.contact_count = ptr("count", prob.contact_count, np.int32)
     P.dynamics_matrix = ptr("A", prob.dynamics_matrix, np.float64)
     P.jacobian = ptr("J", prob.jacobian, np.float64)
@@ -142,6 +143,8 @@ def solve(prob, line_search_variant: str = "monotone_decay", threads: int = 0, v
         D = _abi.DofTerms()
         D.has_pd = int(dof_terms.get("has_pd", 0))
         D.has_limits = int(dof_terms.get("has_limits", 0))
+        jq = dof_terms.get("joint_q")
+        D.joint_coord_count = int(np.asarray(jq).size) if jq is not None else 0
         types = {
             "dof_coord_index": np.int32, "dof_target_index": np.int32, "limit_supported": np.int32,
             "joint_target_mode": np.int32, "joint_target_ke": np.float32, "joint_target_kd": np.float32,

@@ -927,9 +927,10 @@ static void solve_world(const sapb_contact_problem* P, const sapb_solve_options*
     w.pd_active[i] = 0;
     if (!w.has_pd) continue;
     const size_t dof = base + i;
-    const int32_t coord = D->dof_coord_index[dof];
+    int32_t coord = D->dof_coord_index[dof];
+    if (coord >= D->joint_coord_count) coord = -1;
     int32_t target = D->dof_target_index[dof];
-    if (target < 0) target = (int32_t)dof;
+    if (target < 0 || target >= P->num_envs * n) target = (int32_t)dof;
     if (D->joint_target_mode[target] == 0) continue;
     const double kp = (double)D->joint_target_ke[target];
     const double kd = (double)D->joint_target_kd[target];
@@ -959,7 +960,8 @@ static void solve_world(const sapb_contact_problem* P, const sapb_solve_options*
     w.up_r[i] = 1.0;
     if (!w.has_lim) continue;
     const size_t dof = base + i;
-    const int32_t coord = D->dof_coord_index[dof];
+    int32_t coord = D->dof_coord_index[dof];
+    if (coord >= D->joint_coord_count) coord = -1;
     if (coord < 0 || D->limit_supported[dof] == 0) continue;
     const double ke = D->joint_limit_ke[dof];
     if (ke <= 0.0) continue;
@@ -1000,7 +1002,7 @@ static void solve_world(const sapb_contact_problem* P, const sapb_solve_options*
                                P->body1 ? P->body1[(size_t)e * C + c] : -1};
     for (int b = 0; b < 2; ++b) {
       const int32_t body = bodies[b];
-      if (body < 0 || !P->body_dof_start) continue;
+      if (body < 0 || body >= P->num_bodies || !P->body_dof_start) continue;
       const int32_t s = P->body_dof_start[body], m = P->body_dof_count[body];
       if (s >= 0 && m > 0)
         for (int32_t i = s; i < s + m && i < n; ++i)

@@ -69,6 +69,7 @@ class DofTerms(C.Structure):
     _fields_ = [
         ("has_pd", C.c_int32),
         ("has_limits", C.c_int32),
+        ("joint_coord_count", C.c_int32),
         ("dof_coord_index", _p),
         ("dof_target_index", _p),
         ("limit_supported", _p),
@@ -92,6 +93,7 @@ class ContactProblem(C.Structure):
         ("num_envs", C.c_int32),
         ("dof_per_env", C.c_int32),
         ("max_contacts", C.c_int32),
+        ("num_bodies", C.c_int32),
         ("contact_count", _p),
         ("dynamics_matrix", _p),
         ("jacobian", _p),

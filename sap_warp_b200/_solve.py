@@ -107,6 +107,8 @@ class DofTermArrays:
         self.struct = _abi.DofTerms()
         self.struct.has_pd = self.has_pd
         self.struct.has_limits = self.has_limits
+        jq = arrays.get("joint_q")
+        self.struct.joint_coord_count = int(jq.numel()) if jq is not None else 0
         types = {
             "dof_coord_index": I32, "dof_target_index": I32, "limit_supported": I32, "joint_target_mode": I32,
             "joint_target_ke": F32, "joint_target_kd": F32, "joint_effort_limit": F32,
@@ -146,6 +148,7 @@ def contact_solve(
     E, n, C = buffers.num_envs, buffers.dof_per_env, buffers.max_contacts
     P = _abi.ContactProblem()
     P.num_envs, P.dof_per_env, P.max_contacts = E, n, C
+    P.num_bodies = int(body_dof_start.numel()) if body_dof_start is not None else 0
     P.contact_count = _ptr(contact_count, I32, E, "contact_count")
     P.dynamics_matrix = _ptr(dynamics_matrix, F64, E * n * n, "dynamics_matrix")
     P.jacobian = _ptr(jacobian, F64, E * C * 3 * n, "jacobian")

@@ -786,9 +786,10 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
       const size_t dof = base + i;
       const sapb_dof_terms& D = P.dof;
       if (D.has_pd) {
-        const int coord = D.dof_coord_index[dof];
+        int coord = D.dof_coord_index[dof];
+        if (coord >= D.joint_coord_count) coord = -1;
         int target = D.dof_target_index[dof];
-        if (target < 0) target = (int)dof;
+        if (target < 0 || target >= P.p.num_envs * n) target = (int)dof;
         if (D.joint_target_mode[target] != 0) {
           const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
           if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {
@@ -814,7 +815,8 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
       w.V(V_LOR)[i] = 1.0;
       w.V(V_UPR)[i] = 1.0;
       if (D.has_limits) {
-        const int coord = D.dof_coord_index[dof];
+        int coord = D.dof_coord_index[dof];
+        if (coord >= D.joint_coord_count) coord = -1;
         const double ke = coord >= 0 ? D.joint_limit_ke[dof] : 0.0;
         if (coord >= 0 && D.limit_supported[dof] != 0 && ke > 0.0) {
           const double q0 = D.joint_q[coord];
@@ -854,11 +856,11 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
         const int b0 = P.p.body0 ? P.p.body0[ci] : -1;
         const int b1 = P.p.body1 ? P.p.body1[ci] : -1;
         if (P.p.body_dof_start) {
-          if (b0 >= 0) {
+          if (b0 >= 0 && b0 < P.p.num_bodies) {
             const int s = P.p.body_dof_start[b0], m = P.p.body_dof_count[b0];
             if (s >= 0 && m > 0 && i >= s && i < s + m) part = 1;
           }
-          if (b1 >= 0) {
+          if (b1 >= 0 && b1 < P.p.num_bodies) {
             const int s = P.p.body_dof_start[b1], m = P.p.body_dof_count[b1];
             if (s >= 0 && m > 0 && i >= s && i < s + m) part = 1;
           }
