@@ -43,16 +43,19 @@ __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a -
 // reads in the triangular solves).
 struct Layout {
   int n, C, ldJ, ldH, nb;
-  size_t off_A, off_J, off_Jh, off_GJ, off_H, off_vec, off_con, off_flags, total;
+  size_t off_A, off_J, off_Jh, off_GJ, off_H, off_vec, off_con, off_flags, off_tri, total;
   static constexpr int kVecs = 22;
   static constexpr int kConPer = 28;
+  static constexpr int kMaxWarps = 8;  // partial-sum scratch (aliases GJ)
 };
 
 __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
   Layout L;
   L.n = n;
   L.C = C;
-  L.ldJ = (n + 3) / 4 * 4;
+  // ldJ: room for the 4-wide Hessian tiles, odd so that thread-per-row
+  // reads of J (stride ldJ doubles) are free of bank conflicts.
+  L.ldJ = (n + 3) / 4 * 4 + 1;
   L.ldH = (n % 2 == 0) ? n + 1 : n;
   L.nb = (n + 3) / 4;
   size_t o = 0;
@@ -62,8 +65,12 @@ __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
   o = align_up(o + sizeof(double) * (size_t)3 * C * L.ldJ, 16);
   L.off_Jh = o;  // HT copy of J (aliases J when HT is double)
   if (hsize == 4) o = align_up(o + sizeof(float) * (size_t)3 * C * L.ldJ, 16);
-  L.off_GJ = o;
-  o = align_up(o + (size_t)hsize * 3 * C * L.ldJ, 16);
+  L.off_GJ = o;  // also the partial-sum scratch of the DOF products
+  {
+    const size_t gj = (size_t)hsize * 3 * C * L.ldJ;
+    const size_t part = sizeof(double) * 3 * Layout::kMaxWarps * 64;
+    o = align_up(o + (gj > part ? gj : part), 16);
+  }
   L.off_H = o;
   o = align_up(o + (size_t)hsize * n * L.ldH, 16);
   L.off_vec = o;
@@ -72,6 +79,8 @@ __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
   o = align_up(o + sizeof(double) * (size_t)Layout::kConPer * (C > 0 ? C : 1), 16);
   L.off_flags = o;
   o = align_up(o + sizeof(int) * (size_t)L.ldJ, 16);
+  L.off_tri = o;  // (i << 8 | j) of the strict lower triangle, columns descending
+  o = align_up(o + sizeof(uint16_t) * (size_t)(n * (n - 1) / 2 + 1), 16);
   L.total = o;
   return L;
 }
@@ -90,7 +99,7 @@ static_assert(C_END <= Layout::kConPer, "contact slots");
 
 template <int NT, typename HT>
 struct World {
-  const Layout& L;
+  Layout L;
   double* A;
   double* J;
   HT* Jh;
@@ -99,8 +108,12 @@ struct World {
   double* vec;
   double* con;
   int* flags;
+  const uint16_t* tri;
   double* red;
   int n, count;
+  __device__ double* part(int which, int warp) const {
+    return reinterpret_cast<double*>(GJ) + ((size_t)which * Layout::kMaxWarps + warp) * 64;
+  }
   __device__ double* V(int k) const { return vec + (size_t)k * L.ldJ; }
   __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
   __device__ ContactConst cc(int c) const {
@@ -121,18 +134,64 @@ struct World {
 // slot base (C_VC or C_DVC).  One warp per row, lanes over columns.
 template <int NT, typename HT>
 __device__ void contact_rows_times(const World<NT, HT>& w, const double* x, int slot) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rows = 3 * w.count;
-  for (int r = warp; r < rows; r += NT / 32) {
+  for (int r = threadIdx.x; r < rows; r += NT) {
     const double* row = w.J + (size_t)r * w.L.ldJ;
-    double s = 0.0;
-    for (int j = lane; j < w.n; j += 32) s += row[j] * x[j];
-    s = warp_sum<NT>(s);
-    if (lane == 0) {
-      const int c = r / 3, k = r - 3 * (r / 3);
-      w.Cn(slot + k)[c] = s;
+    double s0 = 0.0, s1 = 0.0;
+    int j = 0;
+    for (; j + 1 < w.n; j += 2) {
+      s0 += row[j] * x[j];
+      s1 += row[j + 1] * x[j + 1];
     }
+    if (j < w.n) s0 += row[j] * x[j];
+    const int c = r / 3, k = r - 3 * c;
+    w.Cn(slot + k)[c] = s0 + s1;
   }
+}
+
+// Partial sums of the per-DOF products over a warp's share of the columns of
+// A and rows of J: part(0)[i] += sum_j A[j][i] x[j], part(1)[i] +=
+// sum_j A[j][i] y[j], part(2)[i] += sum_r J[r][i] g[r] (g = gamma slots).
+// Lanes own DOFs i = lane and lane + 32; A and J are read down columns, so
+// the lanes of a warp touch consecutive addresses.
+template <int NT, typename HT>
+__device__ void dof_partials(const World<NT, HT>& w, const double* x, const double* y, bool with_gamma) {
+  constexpr int NW = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = w.n;
+  const int jchunk = (n + NW - 1) / NW;
+  const int j0 = warp * jchunk, j1 = min(n, j0 + jchunk);
+  const int cchunk = (w.count + NW - 1) / NW;
+  const int c0 = warp * cchunk, c1 = min(w.count, c0 + cchunk);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int i = lane + 32 * h;
+    if (i >= n) continue;
+    double a = 0.0, b = 0.0, g = 0.0;
+    for (int j = j0; j < j1; ++j) {
+      const double aij = w.A[(size_t)j * n + i];
+      a += aij * x[j];
+      if (y) b += aij * y[j];
+    }
+    if (with_gamma) {
+      for (int c = c0; c < c1; ++c) {
+        const double* Jc = w.J + (size_t)(3 * c) * w.L.ldJ + i;
+        g += Jc[0] * w.Cn(C_GAMMA + 0)[c] + Jc[w.L.ldJ] * w.Cn(C_GAMMA + 1)[c] + Jc[2 * w.L.ldJ] * w.Cn(C_GAMMA + 2)[c];
+      }
+    }
+    w.part(0, warp)[i] = a;
+    w.part(1, warp)[i] = b;
+    w.part(2, warp)[i] = g;
+  }
+}
+
+template <int NT, typename HT>
+__device__ __forceinline__ double sum_partials(const World<NT, HT>& w, int which, int i) {
+  constexpr int NW = NT / 32;
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) s += w.part(which, k)[i];
+  return s;
 }
 
 // Objective at the current v (shared V_V): contact gamma/G/cost, A(v-v*), Av,
@@ -156,23 +215,17 @@ __device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt
     for (int k = 0; k < 9; ++k) w.Cn(C_G + k)[c] = G[k];
     csum += cost;
   }
+  for (int i = tid; i < w.n; i += NT) w.V(V_TMP0)[i] = w.V(V_V)[i] - w.V(V_VSTAR)[i];
+  __syncthreads();
+  dof_partials<NT, HT>(w, w.V(V_TMP0), w.V(V_V), true);
   __syncthreads();
   double model_cost = 0.0, g2 = 0.0, p2 = 0.0, j2 = 0.0;
   const double* v = w.V(V_V);
   const double* vs = w.V(V_VSTAR);
   for (int i = tid; i < w.n; i += NT) {
-    double a_res = 0.0, a_v = 0.0;
-    for (int j = 0; j < w.n; ++j) {
-      const double aij = w.A[(size_t)j * w.n + i];  // symmetric: column i
-      a_res += aij * (v[j] - vs[j]);
-      a_v += aij * v[j];
-    }
-    double imp = 0.0;
-    const int rows = 3 * w.count;
-    for (int r = 0; r < rows; ++r) {
-      const int c = r / 3, k = r - 3 * c;
-      imp += w.J[(size_t)r * w.L.ldJ + i] * w.Cn(C_GAMMA + k)[c];
-    }
+    const double a_res = sum_partials<NT, HT>(w, 0, i);
+    const double a_v = sum_partials<NT, HT>(w, 1, i);
+    double imp = sum_partials<NT, HT>(w, 2, i);
     const double vi = v[i];
     double mc = 0.5 * (vi - vs[i]) * a_res;
     const int fl = w.flags[i];
@@ -237,16 +290,13 @@ __device__ void assemble_hessian(const World<NT, HT>& w, double diag_shift) {
   const int tid = threadIdx.x;
   const int n = w.n, ldJ = w.L.ldJ, ldH = w.L.ldH, rows = 3 * w.count;
   // GJ = G_c J_c per contact (rows 3c..3c+2), zero in padded columns.
-  for (int e = tid; e < rows * ldJ; e += NT) {
-    const int r = e / ldJ, j = e - r * ldJ;
+  const int ncol = 4 * w.L.nb;
+  for (int r = tid; r < rows; r += NT) {
     const int c = r / 3, k = r - 3 * c;
-    HT val = HT(0);
-    if (j < n) {
-      const double* Jc = w.J + (size_t)(3 * c) * ldJ;
-      const double g0 = w.Cn(C_G + 3 * k + 0)[c], g1 = w.Cn(C_G + 3 * k + 1)[c], g2 = w.Cn(C_G + 3 * k + 2)[c];
-      val = HT(g0 * Jc[j] + g1 * Jc[ldJ + j] + g2 * Jc[2 * ldJ + j]);
-    }
-    w.GJ[(size_t)r * ldJ + j] = val;
+    const double* Jc = w.J + (size_t)(3 * c) * ldJ;
+    const double g0 = w.Cn(C_G + 3 * k + 0)[c], g1 = w.Cn(C_G + 3 * k + 1)[c], g2 = w.Cn(C_G + 3 * k + 2)[c];
+    HT* out = w.GJ + (size_t)r * ldJ;
+    for (int j = 0; j < ncol; ++j) out[j] = HT(g0 * Jc[j] + g1 * Jc[ldJ + j] + g2 * Jc[2 * ldJ + j]);
   }
   // H lower = A lower (+ diagonal terms)
   for (int e = tid; e < n * n; e += NT) {
@@ -321,23 +371,22 @@ __device__ bool factor_and_solve(const World<NT, HT>& w) {
   const int n = w.n, ldH = w.L.ldH;
   HT* H = w.H;
   bool ok = true;
-  for (int k = 0; k < n; ++k) {
-    const HT d = H[(size_t)k * ldH + k];
-    if (!(d > HT(0)) || !isfinite(double(d))) ok = false;
-    const HT rinv = HT(1) / d;
-    // trailing update of rows i > k, columns k < j <= i
-    const int m = n - k - 1;
-    const int cnt = m * (m + 1) / 2;
-    for (int e = tid; e < cnt; e += NT) {
-      // e -> (ii, jj) lower-triangular within the trailing block
-      int ii = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
-      while ((ii + 1) * (ii + 2) / 2 <= e) ++ii;
-      while (ii * (ii + 1) / 2 > e) --ii;
-      const int jj = e - ii * (ii + 1) / 2;
-      const int i = k + 1 + ii, j = k + 1 + jj;
-      H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + k] * rinv) * H[(size_t)j * ldH + k];
+  if (tid < 32) {
+    // One warp, no block barriers: at step k the (n-k-1)(n-k)/2 trailing
+    // entries are the first ones of the column-descending triangle list.
+    for (int k = 0; k < n; ++k) {
+      const HT d = H[(size_t)k * ldH + k];
+      if (!(d > HT(0)) || !isfinite(double(d))) ok = false;
+      const HT rinv = HT(1) / d;
+      const int m = n - k - 1;
+      const int cnt = m * (m + 1) / 2;
+      for (int e = tid; e < cnt; e += 32) {
+        const int ij = w.tri[e];
+        const int i = ij >> 8, j = ij & 255;
+        H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + k] * rinv) * H[(size_t)j * ldH + k];
+      }
+      __syncwarp();
     }
-    __syncthreads();
   }
   // Solve with one warp: forward z = D^-1 (L^-1 b), backward x = L^-T z.
   double* dv = w.V(V_DV);
@@ -377,7 +426,7 @@ __device__ bool factor_and_solve(const World<NT, HT>& w) {
     if (lane + 32 < n) dv[lane + 32] = ok ? double(hb1) : nanv;
   }
   __syncthreads();
-  return ok;
+  return true;
 }
 
 // Regularizer terms along the line at step alpha (contact, PD and limit
@@ -455,13 +504,14 @@ template <int NT, typename HT>
 __device__ void line_coefficients(const World<NT, HT>& w, double c4[4]) {
   const int tid = threadIdx.x;
   contact_rows_times<NT, HT>(w, w.V(V_DV), C_DVC);
+  dof_partials<NT, HT>(w, w.V(V_DV), nullptr, false);
+  __syncthreads();
   double d0 = 0.0, da0 = 0.0, d2 = 0.0, m0 = 0.0;
   const double* v = w.V(V_V);
   const double* vs = w.V(V_VSTAR);
   const double* dv = w.V(V_DV);
   for (int i = tid; i < w.n; i += NT) {
-    double acc = 0.0;
-    for (int j = 0; j < w.n; ++j) acc += w.A[(size_t)j * w.n + i] * dv[j];
+    const double acc = sum_partials<NT, HT>(w, 0, i);
     w.V(V_DP)[i] = acc;
     const double ri = v[i] - vs[i];
     d0 += w.V(V_GRAD)[i] * dv[i];
@@ -710,6 +760,13 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
   const int n = P.p.dof_per_env, C = P.p.max_contacts;
   const Layout L = make_layout(n, C, (int)sizeof(HT));
   const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
+  {
+    uint16_t* tri = reinterpret_cast<uint16_t*>(smem + L.off_tri);
+    for (int j = n - 1 - tid; j >= 1; j -= NT) {
+      const int off = (n - 1 - j) * (n - j) / 2;
+      for (int i = j; i < n; ++i) tri[off + (i - j)] = (uint16_t)((i << 8) | j);
+    }
+  }
 
   for (;;) {
     if (tid == 0) s_world = atomicAdd(P.queue, 1);
@@ -726,6 +783,7 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
                     reinterpret_cast<double*>(smem + L.off_vec),
                     reinterpret_cast<double*>(smem + L.off_con),
                     reinterpret_cast<int*>(smem + L.off_flags),
+                    reinterpret_cast<const uint16_t*>(smem + L.off_tri),
                     red,
                     n,
                     0};
@@ -742,11 +800,13 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
       for (int k = tid; k < n * n; k += NT) w.A[k] = Ag[k];
       const int rows = 3 * count;
       const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n;
-      for (int k = tid; k < rows * L.ldJ; k += NT) {
-        const int r = k / L.ldJ, j = k - r * L.ldJ;
-        const double val = j < n ? Jg[(size_t)r * n + j] : 0.0;
-        w.J[k] = val;
-        if (sizeof(HT) == 4) w.Jh[k] = HT(val);
+      const int lane = tid & 31, warp = tid >> 5;
+      for (int r = warp; r < rows; r += NT / 32) {
+        for (int j = lane; j < L.ldJ; j += 32) {
+          const double val = j < n ? Jg[(size_t)r * n + j] : 0.0;
+          w.J[(size_t)r * L.ldJ + j] = val;
+          if (sizeof(HT) == 4) w.Jh[(size_t)r * L.ldJ + j] = HT(val);
+        }
       }
       for (int c = tid; c < count; c += NT) {
         const size_t ci = (size_t)e * C + c;
