@@ -67,8 +67,8 @@ int32_t sapb_contact_solve(const sapb_contact_problem* p, const sapb_solve_optio
                          p->dof_per_env, p->max_contacts);
     return SAPB_ERR_INVALID_ARGUMENT;
   }
-  if (p->dof_per_env > 64) {
-    sapb::set_last_error("sapb_contact_solve: dof_per_env=%d > 64 is not supported by the on-chip solve",
+  if (p->dof_per_env > 60) {
+    sapb::set_last_error("sapb_contact_solve: dof_per_env=%d > 60 is not supported by the on-chip solve",
                          p->dof_per_env);
     return SAPB_ERR_UNSUPPORTED;
   }

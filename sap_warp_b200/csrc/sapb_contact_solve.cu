@@ -2,13 +2,14 @@
 //
 // Restates SapContactSolve.solve (sim/contact_solve.py:6129-6285) as ONE
 // persistent launch.  A CTA pulls a world index from a device counter, stages
-// the world's dynamics matrix A and contact Jacobian J in shared memory once,
-// and runs prepare (:4285-4429), the Newton loop (:5474-5655) and the chosen
-// line search (:2207-3175) entirely on chip.  Per Newton iteration it reads
-// nothing from HBM; per line-search trial it touches O(contacts + DOFs) data
-// because the contact velocity along the search line is vc + alpha * (J dv)
-// (vc is linear in v).  The reference issues ~35 launches per Newton
-// iteration and re-reads A and J on every trial.
+// the world's contact Jacobian J in shared memory once, and runs prepare
+// (:4285-4429), the Newton loop (:5474-5655) and the chosen line search
+// (:2207-3175) on chip.  The dynamics matrix A is read through L1 (it is the
+// only per-world array re-read from outside shared memory; 3-4 passes per
+// Newton iteration hit L1/L2).  Per line-search trial the kernel touches
+// O(contacts + DOFs) data because the contact velocity along the search line
+// is vc + alpha * (J dv) (vc is linear in v); the reference issues ~35
+// launches per Newton iteration and re-reads A and J on every trial.
 //
 // Precision: the gradient, costs, line search, velocity update and the
 // convergence test are FP64.  The Hessian H = A + J^T G J + diag and its LDL^T
@@ -38,48 +39,48 @@ struct SolveParams {
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// Shared-memory layout of one world.  Leading dimensions: ldJ multiple of 4
-// (16-byte aligned rows for the Hessian tiles), ldH odd (conflict-free column
-// reads in the triangular solves).
+// Contacts per G J chunk of the Hessian assembly.
+constexpr int kChunk = 16;
+
+// Shared-memory layout of one world.  ldJ: room for the 4-wide Hessian tiles
+// and odd, so thread-per-row reads of J are free of bank conflicts.  ldH odd
+// for conflict-free column reads in the factorization.
 struct Layout {
   int n, C, ldJ, ldH, nb;
-  size_t off_A, off_J, off_Jh, off_GJ, off_H, off_vec, off_con, off_flags, off_tri, total;
-  static constexpr int kVecs = 22;
-  static constexpr int kConPer = 28;
-  static constexpr int kMaxWarps = 8;  // partial-sum scratch (aliases GJ)
+  size_t off_J, off_scr, off_H, off_G, off_vec, off_con, off_flags, off_tri, total;
+  static constexpr int kVecs = 19;
+  static constexpr int kConPer = 17;
+  static constexpr int kMaxWarps = 4;  // partial-sum scratch (blocks of <= 128 threads)
 };
 
 __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
   Layout L;
   L.n = n;
   L.C = C;
-  // ldJ: room for the 4-wide Hessian tiles, odd so that thread-per-row
-  // reads of J (stride ldJ doubles) are free of bank conflicts.
   L.ldJ = (n + 3) / 4 * 4 + 1;
   L.ldH = (n % 2 == 0) ? n + 1 : n;
   L.nb = (n + 3) / 4;
   size_t o = 0;
-  L.off_A = o;
-  o = align_up(o + sizeof(double) * (size_t)n * n, 16);
   L.off_J = o;
   o = align_up(o + sizeof(double) * (size_t)3 * C * L.ldJ, 16);
-  L.off_Jh = o;  // HT copy of J (aliases J when HT is double)
-  if (hsize == 4) o = align_up(o + sizeof(float) * (size_t)3 * C * L.ldJ, 16);
-  L.off_GJ = o;  // also the partial-sum scratch of the DOF products
+  L.off_scr = o;  // one chunk of G J rows, or the partial sums of the DOF products
   {
-    const size_t gj = (size_t)hsize * 3 * C * L.ldJ;
+    const int ch = C < kChunk ? C : kChunk;
+    const size_t gj = (size_t)hsize * 3 * ch * L.ldJ;
     const size_t part = sizeof(double) * 3 * Layout::kMaxWarps * 64;
     o = align_up(o + (gj > part ? gj : part), 16);
   }
   L.off_H = o;
   o = align_up(o + (size_t)hsize * n * L.ldH, 16);
+  L.off_G = o;
+  o = align_up(o + sizeof(double) * 9 * (size_t)(C > 0 ? C : 1), 16);
   L.off_vec = o;
   o = align_up(o + sizeof(double) * (size_t)Layout::kVecs * L.ldJ, 16);
   L.off_con = o;
   o = align_up(o + sizeof(double) * (size_t)Layout::kConPer * (C > 0 ? C : 1), 16);
   L.off_flags = o;
   o = align_up(o + sizeof(int) * (size_t)L.ldJ, 16);
-  L.off_tri = o;  // (i << 8 | j) of the strict lower triangle, columns descending
+  L.off_tri = o;  // (i << 8 | j) of the lower triangle below row 0, columns descending
   o = align_up(o + sizeof(uint16_t) * (size_t)(n * (n - 1) / 2 + 1), 16);
   L.total = o;
   return L;
@@ -87,35 +88,36 @@ __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
 
 // Vector slots inside off_vec (each ldJ doubles).
 enum Vec {
-  V_V = 0, V_VSTAR, V_DV, V_GRAD, V_DYN, V_ARES, V_IMP, V_DP, V_DSCALE, V_AINV,
-  V_PDA, V_PDGAIN, V_PDLIM, V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_TMP1
+  V_V = 0, V_VSTAR, V_DV, V_GRAD, V_ARES, V_DP, V_DSCALE, V_AINV, V_PDA, V_PDGAIN, V_PDLIM,
+  V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_END
 };
+static_assert(V_END <= Layout::kVecs, "vector slots");
 // Contact slots inside off_con (each C doubles).
 enum Con {
   C_RT = 0, C_RN, C_RTINV, C_RNINV, C_VHAT, C_MU, C_MUHAT, C_FACTOR, C_VC, C_DVC = C_VC + 3, C_GAMMA = C_DVC + 3,
-  C_G = C_GAMMA + 3, C_COST = C_G + 9, C_END = C_COST + 2
+  C_END = C_GAMMA + 3
 };
 static_assert(C_END <= Layout::kConPer, "contact slots");
 
 template <int NT, typename HT>
 struct World {
   Layout L;
-  double* A;
+  const double* A;  // global, this world's [n][n]
   double* J;
-  HT* Jh;
-  HT* GJ;
+  HT* GJ;           // chunk rows, aliased with the partial sums
   HT* H;
+  double* G;        // [C][9]
   double* vec;
   double* con;
   int* flags;
   const uint16_t* tri;
   double* red;
   int n, count;
+  __device__ double* V(int k) const { return vec + (size_t)k * L.ldJ; }
+  __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
   __device__ double* part(int which, int warp) const {
     return reinterpret_cast<double*>(GJ) + ((size_t)which * Layout::kMaxWarps + warp) * 64;
   }
-  __device__ double* V(int k) const { return vec + (size_t)k * L.ldJ; }
-  __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
   __device__ ContactConst cc(int c) const {
     ContactConst x;
     x.rt = Cn(C_RT)[c];
@@ -130,8 +132,8 @@ struct World {
   }
 };
 
-// rows r < 3*count of J times a vector x (length n, shared) -> out[c*3+k] at
-// slot base (C_VC or C_DVC).  One warp per row, lanes over columns.
+// vc-type products: rows r < 3*count of J times x (length n, shared) into the
+// contact slots `slot..slot+2`.  One thread per row.
 template <int NT, typename HT>
 __device__ void contact_rows_times(const World<NT, HT>& w, const double* x, int slot) {
   const int rows = 3 * w.count;
@@ -150,10 +152,9 @@ __device__ void contact_rows_times(const World<NT, HT>& w, const double* x, int 
 }
 
 // Partial sums of the per-DOF products over a warp's share of the columns of
-// A and rows of J: part(0)[i] += sum_j A[j][i] x[j], part(1)[i] +=
-// sum_j A[j][i] y[j], part(2)[i] += sum_r J[r][i] g[r] (g = gamma slots).
-// Lanes own DOFs i = lane and lane + 32; A and J are read down columns, so
-// the lanes of a warp touch consecutive addresses.
+// A and of the contacts: part(0)[i] = sum_j A[j][i] x[j], part(1)[i] =
+// sum_j A[j][i] y[j], part(2)[i] = sum_c J_c[:, i] . gamma_c.  Lanes own DOFs
+// i = lane and lane + 32, so a warp reads consecutive addresses.
 template <int NT, typename HT>
 __device__ void dof_partials(const World<NT, HT>& w, const double* x, const double* y, bool with_gamma) {
   constexpr int NW = NT / 32;
@@ -169,14 +170,15 @@ __device__ void dof_partials(const World<NT, HT>& w, const double* x, const doub
     if (i >= n) continue;
     double a = 0.0, b = 0.0, g = 0.0;
     for (int j = j0; j < j1; ++j) {
-      const double aij = w.A[(size_t)j * n + i];
+      const double aij = __ldg(w.A + (size_t)j * n + i);
       a += aij * x[j];
       if (y) b += aij * y[j];
     }
     if (with_gamma) {
+      const int ld = w.L.ldJ;
       for (int c = c0; c < c1; ++c) {
-        const double* Jc = w.J + (size_t)(3 * c) * w.L.ldJ + i;
-        g += Jc[0] * w.Cn(C_GAMMA + 0)[c] + Jc[w.L.ldJ] * w.Cn(C_GAMMA + 1)[c] + Jc[2 * w.L.ldJ] * w.Cn(C_GAMMA + 2)[c];
+        const double* Jc = w.J + (size_t)(3 * c) * ld + i;
+        g += Jc[0] * w.Cn(C_GAMMA + 0)[c] + Jc[ld] * w.Cn(C_GAMMA + 1)[c] + Jc[2 * ld] * w.Cn(C_GAMMA + 2)[c];
       }
     }
     w.part(0, warp)[i] = a;
@@ -194,7 +196,7 @@ __device__ __forceinline__ double sum_partials(const World<NT, HT>& w, int which
   return s;
 }
 
-// Objective at the current v (shared V_V): contact gamma/G/cost, A(v-v*), Av,
+// Objective at the current v (shared V_V): contact gamma and cost, A(v-v*),
 // J^T gamma, PD and limit terms, gradient.  Returns {cost, |g|^2, |p|^2, |jc|^2}
 // (scaled, over participating DOFs) to every thread.  Restates
 // _solver_update_active sim/contact_solve.py:4080-4136.
@@ -202,20 +204,17 @@ template <int NT, typename HT>
 __device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt, double out4[4]) {
   const int tid = threadIdx.x;
   contact_rows_times<NT, HT>(w, w.V(V_V), C_VC);
+  for (int i = tid; i < w.n; i += NT) w.V(V_TMP0)[i] = w.V(V_V)[i] - w.V(V_VSTAR)[i];
   __syncthreads();
   double csum = 0.0;
   for (int c = tid; c < w.count; c += NT) {
-    const ContactConst cc = w.cc(c);
-    double g[3], cost, G[9];
-    project_contact(cc, w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cost, G);
+    double g[3], cost;
+    project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cost, nullptr);
     w.Cn(C_GAMMA + 0)[c] = g[0];
     w.Cn(C_GAMMA + 1)[c] = g[1];
     w.Cn(C_GAMMA + 2)[c] = g[2];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) w.Cn(C_G + k)[c] = G[k];
     csum += cost;
   }
-  for (int i = tid; i < w.n; i += NT) w.V(V_TMP0)[i] = w.V(V_V)[i] - w.V(V_VSTAR)[i];
   __syncthreads();
   dof_partials<NT, HT>(w, w.V(V_TMP0), w.V(V_V), true);
   __syncthreads();
@@ -261,8 +260,6 @@ __device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt
     imp += pdg + lg;
     const double grad = a_res - imp;
     w.V(V_ARES)[i] = a_res;
-    w.V(V_DYN)[i] = a_v;
-    w.V(V_IMP)[i] = imp;
     w.V(V_GRAD)[i] = grad;
     w.V(V_HDIAG)[i] = hd;
     model_cost += mc;
@@ -283,59 +280,73 @@ __device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt
 }
 
 // H = A + J^T G J + diag(PD + limit + shift), lower triangle, in HT.
-// GJ rows are formed first; the product uses 4x4 register tiles with the
-// contact rows split into KS slices that add into H in turn (deterministic).
+// G (at the stored vc) and G J are formed chunk by chunk; each thread owns one
+// 4x4 tile of H and one of KS slices of a chunk's rows, accumulates in
+// registers across chunks, and the slices add into H in turn (deterministic).
 template <int NT, typename HT>
 __device__ void assemble_hessian(const World<NT, HT>& w, double diag_shift) {
   const int tid = threadIdx.x;
-  const int n = w.n, ldJ = w.L.ldJ, ldH = w.L.ldH, rows = 3 * w.count;
-  // GJ = G_c J_c per contact (rows 3c..3c+2), zero in padded columns.
-  const int ncol = 4 * w.L.nb;
-  for (int r = tid; r < rows; r += NT) {
-    const int c = r / 3, k = r - 3 * c;
-    const double* Jc = w.J + (size_t)(3 * c) * ldJ;
-    const double g0 = w.Cn(C_G + 3 * k + 0)[c], g1 = w.Cn(C_G + 3 * k + 1)[c], g2 = w.Cn(C_G + 3 * k + 2)[c];
-    HT* out = w.GJ + (size_t)r * ldJ;
-    for (int j = 0; j < ncol; ++j) out[j] = HT(g0 * Jc[j] + g1 * Jc[ldJ + j] + g2 * Jc[2 * ldJ + j]);
+  const int lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = NT / 32;
+  const int n = w.n, ldJ = w.L.ldJ, ldH = w.L.ldH, nb = w.L.nb;
+  const int ncol = 4 * nb;
+  // G at the current contact velocities (sim/contact_solve.py:1071-1217).
+  for (int c = tid; c < w.count; c += NT) {
+    double g[3], cost, G[9];
+    project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cost, G);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) w.G[9 * c + k] = G[k];
   }
-  // H lower = A lower (+ diagonal terms)
-  for (int e = tid; e < n * n; e += NT) {
-    const int i = e / n, j = e - i * n;
-    if (j <= i) {
-      double a = w.A[(size_t)i * n + j];
+  // H lower = A lower + diagonal terms
+  for (int i = warp; i < n; i += NW) {
+    for (int j = lane; j <= i; j += 32) {
+      double a = __ldg(w.A + (size_t)i * n + j);
       if (i == j) a += w.V(V_HDIAG)[i] + diag_shift;
       w.H[(size_t)i * ldH + j] = HT(a);
     }
   }
-  __syncthreads();
-  const int nb = w.L.nb;
   const int tiles = nb * (nb + 1) / 2;
   int ks = NT / (tiles > 0 ? tiles : 1);
   if (ks < 1) ks = 1;
-  if (ks > 8) ks = 8;
+  if (ks > 4) ks = 4;
   const int items = tiles * ks;
-  const int per = (rows + ks - 1) / ks;
-  for (int slice = 0; slice < ks; ++slice) {
-    for (int it = tid; it < items; it += NT) {
-      const int t = it / ks, s = it - t * ks;
-      if (s != slice) continue;
-      // tile t -> (bi, bj) with bj <= bi
-      int bi = 0;
-      while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
-      const int bj = t - bi * (bi + 1) / 2;
-      const int r0 = s * per, r1 = min(rows, r0 + per);
-      HT acc[4][4];
+  // This thread's item (a thread holds at most one: items <= NT is checked
+  // on the host; n <= 64 gives tiles <= 136, ks >= 1).
+  const bool has_item = tid < items;
+  int bi = 0, bj = 0, slice = 0;
+  if (has_item) {
+    const int t = tid / ks;
+    slice = tid - t * ks;
+    while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+    bj = t - bi * (bi + 1) / 2;
+  }
+  HT acc[4][4];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = HT(0);
+    for (int b = 0; b < 4; ++b) acc[a][b] = HT(0);
+  for (int cb = 0; cb < w.count; cb += kChunk) {
+    const int cn = min(kChunk, w.count - cb);
+    __syncthreads();  // G ready / previous chunk consumed
+    for (int rr = tid; rr < 3 * cn; rr += NT) {
+      const int c = cb + rr / 3, k = rr - 3 * (rr / 3);
+      const double* Jc = w.J + (size_t)(3 * c) * ldJ;
+      const double g0 = w.G[9 * c + 3 * k + 0], g1 = w.G[9 * c + 3 * k + 1], g2 = w.G[9 * c + 3 * k + 2];
+      HT* out = w.GJ + (size_t)rr * ldJ;
+      for (int j = 0; j < ncol; ++j) out[j] = HT(g0 * Jc[j] + g1 * Jc[ldJ + j] + g2 * Jc[2 * ldJ + j]);
+    }
+    __syncthreads();
+    if (has_item) {
+      const int rows = 3 * cn;
+      const int per = (rows + ks - 1) / ks;
+      const int r0 = slice * per, r1 = min(rows, r0 + per);
       for (int r = r0; r < r1; ++r) {
-        const HT* jr = w.Jh + (size_t)r * ldJ + 4 * bi;
+        const double* jr = w.J + (size_t)(3 * cb + r) * ldJ + 4 * bi;
         const HT* gr = w.GJ + (size_t)r * ldJ + 4 * bj;
         HT x[4], y[4];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          x[a] = jr[a];
+          x[a] = HT(jr[a]);
           y[a] = gr[a];
         }
 #pragma unroll
@@ -343,6 +354,11 @@ __device__ void assemble_hessian(const World<NT, HT>& w, double diag_shift) {
 #pragma unroll
           for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
       }
+    }
+  }
+  __syncthreads();  // H init visible
+  for (int s = 0; s < ks; ++s) {
+    if (has_item && slice == s) {
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         const int i = 4 * bi + a;
@@ -360,20 +376,21 @@ __device__ void assemble_hessian(const World<NT, HT>& w, double diag_shift) {
 }
 
 // In-place LDL^T of the lower triangle of H (unit L stored below the
-// diagonal unscaled as H_ik, D on the diagonal) followed by the solve
+// diagonal unscaled as H_ik, D on the diagonal) by one warp, then the solve
 // H dv = -grad.  Mathematically the Cholesky solve of the reference's
-// BlockCholeskySolverBatched (sim/blocked_cholesky.py:414-604).  Returns
-// false (every thread) if a pivot is not positive/finite: dv is then NaN so
-// the line search reports an ascent direction like the reference's NaN factor.
+// BlockCholeskySolverBatched (sim/blocked_cholesky.py:414-604).  A pivot that
+// is not positive/finite makes dv NaN, so the line search reports an ascent
+// direction as the reference's NaN factor does.
 template <int NT, typename HT>
-__device__ bool factor_and_solve(const World<NT, HT>& w) {
+__device__ void factor_and_solve(const World<NT, HT>& w) {
   const int tid = threadIdx.x;
   const int n = w.n, ldH = w.L.ldH;
   HT* H = w.H;
-  bool ok = true;
+  double* dv = w.V(V_DV);
   if (tid < 32) {
-    // One warp, no block barriers: at step k the (n-k-1)(n-k)/2 trailing
-    // entries are the first ones of the column-descending triangle list.
+    bool ok = true;
+    // At step k the (n-k-1)(n-k)/2 trailing entries are the first ones of the
+    // column-descending triangle list.
     for (int k = 0; k < n; ++k) {
       const HT d = H[(size_t)k * ldH + k];
       if (!(d > HT(0)) || !isfinite(double(d))) ok = false;
@@ -387,15 +404,11 @@ __device__ bool factor_and_solve(const World<NT, HT>& w) {
       }
       __syncwarp();
     }
-  }
-  // Solve with one warp: forward z = D^-1 (L^-1 b), backward x = L^-T z.
-  double* dv = w.V(V_DV);
-  if (tid < 32) {
+    // Forward z = D^-1 (L^-1 b), backward x = L^-T z; lanes own rows lane, lane+32.
     const int lane = tid;
-    double b0 = 0.0, b1 = 0.0;  // rows lane, lane + 32
-    if (lane < n) b0 = -w.V(V_GRAD)[lane];
-    if (lane + 32 < n) b1 = -w.V(V_GRAD)[lane + 32];
-    HT hb0 = HT(b0), hb1 = HT(b1);
+    HT hb0 = HT(0), hb1 = HT(0);
+    if (lane < n) hb0 = HT(-w.V(V_GRAD)[lane]);
+    if (lane + 32 < n) hb1 = HT(-w.V(V_GRAD)[lane + 32]);
     for (int k = 0; k < n; ++k) {
       const HT bk = __shfl_sync(0xffffffffu, k < 32 ? hb0 : hb1, k & 31);
       const HT zk = bk / H[(size_t)k * ldH + k];
@@ -406,7 +419,6 @@ __device__ bool factor_and_solve(const World<NT, HT>& w) {
       if (lane > k && lane < n) hb0 -= H[(size_t)lane * ldH + k] * zk;
       if (lane + 32 > k && lane + 32 < n) hb1 -= H[(size_t)(lane + 32) * ldH + k] * zk;
     }
-    // now hb = z; backward: x_i = z_i - (sum_{k>i} H_ki x_k) / d_i
     HT s0 = HT(0), s1 = HT(0);
     for (int i = n - 1; i >= 0; --i) {
       HT xi_local = HT(0);
@@ -426,7 +438,6 @@ __device__ bool factor_and_solve(const World<NT, HT>& w) {
     if (lane + 32 < n) dv[lane + 32] = ok ? double(hb1) : nanv;
   }
   __syncthreads();
-  return true;
 }
 
 // Regularizer terms along the line at step alpha (contact, PD and limit
@@ -751,8 +762,9 @@ __device__ LsResult ls_exact(const World<NT, HT>& w, const SolveParams& P, doubl
   return r;
 }
 
-template <int NT, typename HT>
-__global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) {
+template <int NT, typename HT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolveParams P) {
+  static_assert(NT / 32 <= Layout::kMaxWarps, "partial-sum scratch sized for kMaxWarps warps");
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[8 * (NT / 32)];
   __shared__ int s_world;
@@ -775,11 +787,11 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
     if (e >= P.p.num_envs) break;
 
     World<NT, HT> w{L,
-                    reinterpret_cast<double*>(smem + L.off_A),
+                    P.p.dynamics_matrix + (size_t)e * n * n,
                     reinterpret_cast<double*>(smem + L.off_J),
-                    reinterpret_cast<HT*>(smem + (sizeof(HT) == 4 ? L.off_Jh : L.off_J)),
-                    reinterpret_cast<HT*>(smem + L.off_GJ),
+                    reinterpret_cast<HT*>(smem + L.off_scr),
                     reinterpret_cast<HT*>(smem + L.off_H),
+                    reinterpret_cast<double*>(smem + L.off_G),
                     reinterpret_cast<double*>(smem + L.off_vec),
                     reinterpret_cast<double*>(smem + L.off_con),
                     reinterpret_cast<int*>(smem + L.off_flags),
@@ -794,19 +806,13 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
     const double dt = P.p.dt[e];
     const size_t base = (size_t)e * n;
 
-    // ---- stage A, J, per-contact constants and vectors ----------------------
+    // ---- stage J, per-contact constants and vectors -------------------------
     {
-      const double* Ag = P.p.dynamics_matrix + (size_t)e * n * n;
-      for (int k = tid; k < n * n; k += NT) w.A[k] = Ag[k];
       const int rows = 3 * count;
       const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n;
       const int lane = tid & 31, warp = tid >> 5;
       for (int r = warp; r < rows; r += NT / 32) {
-        for (int j = lane; j < L.ldJ; j += 32) {
-          const double val = j < n ? Jg[(size_t)r * n + j] : 0.0;
-          w.J[(size_t)r * L.ldJ + j] = val;
-          if (sizeof(HT) == 4) w.Jh[(size_t)r * L.ldJ + j] = HT(val);
-        }
+        for (int j = lane; j < L.ldJ; j += 32) w.J[(size_t)r * L.ldJ + j] = j < n ? __ldg(Jg + (size_t)r * n + j) : 0.0;
       }
       for (int c = tid; c < count; c += NT) {
         const size_t ci = (size_t)e * C + c;
@@ -831,7 +837,7 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
             P.p.v_guess[base + i] = v;
           }
           w.V(V_V)[i] = v;
-          double d = Ag[(size_t)i * n + i];
+          double d = __ldg(w.A + (size_t)i * n + i);
           if (d < 1.0e-12 || !isfinite(d)) d = 1.0e-12;
           w.V(V_AINV)[i] = 1.0 / d;
           w.V(V_DSCALE)[i] = 1.0 / sqrt(d);
@@ -1028,10 +1034,10 @@ __global__ void __launch_bounds__(NT) contact_solve_kernel(const SolveParams P) 
   }
 }
 
-template <int NT, typename HT>
+template <int NT, typename HT, int MINB>
 static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
   const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT));
-  auto kern = contact_solve_kernel<NT, HT>;
+  auto kern = contact_solve_kernel<NT, HT, MINB>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (err != cudaSuccess) return err;
   int dev = 0;
@@ -1081,9 +1087,9 @@ int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_opt
   }
   cudaError_t err;
   if (fp32)
-    err = launch_solve<128, float>(P, stream, nullptr);
+    err = launch_solve<128, float, 4>(P, stream, nullptr);
   else
-    err = launch_solve<128, double>(P, stream, nullptr);
+    err = launch_solve<128, double, 3>(P, stream, nullptr);
   if (err != cudaSuccess) {
     set_last_error("contact solve launch: %s", cudaGetErrorString(err));
     return SAPB_ERR_CUDA;
