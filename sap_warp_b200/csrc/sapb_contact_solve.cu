@@ -99,7 +99,7 @@ enum Con {
 };
 static_assert(C_END <= Layout::kConPer, "contact slots");
 
-template <int NT, typename HT>
+template <int NT, typename HT, int NS>
 struct World {
   Layout L;
   const double* A;  // global, this world's [n][n]
@@ -113,7 +113,12 @@ struct World {
   const uint16_t* tri;
   double* red;
   int n, count;
-  __device__ double* V(int k) const { return vec + (size_t)k * L.ldJ; }
+  // DOF count and leading dimensions: compile-time constants when NS > 0.
+  __device__ __forceinline__ int dofs() const { return NS > 0 ? NS : n; }
+  __device__ __forceinline__ int ldJ() const { return NS > 0 ? (NS + 3) / 4 * 4 + 1 : L.ldJ; }
+  __device__ __forceinline__ int ldH() const { return NS > 0 ? ((NS % 2 == 0) ? NS + 1 : NS) : L.ldH; }
+  __device__ __forceinline__ int nb() const { return NS > 0 ? (NS + 3) / 4 : L.nb; }
+  __device__ double* V(int k) const { return vec + (size_t)k * ldJ(); }
   __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
   __device__ double* part(int which, int warp) const {
     return reinterpret_cast<double*>(GJ) + ((size_t)which * Layout::kMaxWarps + warp) * 64;
@@ -134,18 +139,18 @@ struct World {
 
 // vc-type products: rows r < 3*count of J times x (length n, shared) into the
 // contact slots `slot..slot+2`.  One thread per row.
-template <int NT, typename HT>
-__device__ void contact_rows_times(const World<NT, HT>& w, const double* x, int slot) {
+template <int NT, typename HT, int NS>
+__device__ void contact_rows_times(const World<NT, HT, NS>& w, const double* x, int slot) {
   const int rows = 3 * w.count;
   for (int r = threadIdx.x; r < rows; r += NT) {
-    const double* row = w.J + (size_t)r * w.L.ldJ;
+    const double* row = w.J + (size_t)r * w.ldJ();
     double s0 = 0.0, s1 = 0.0;
     int j = 0;
-    for (; j + 1 < w.n; j += 2) {
+    for (; j + 1 < w.dofs(); j += 2) {
       s0 += row[j] * x[j];
       s1 += row[j + 1] * x[j + 1];
     }
-    if (j < w.n) s0 += row[j] * x[j];
+    if (j < w.dofs()) s0 += row[j] * x[j];
     const int c = r / 3, k = r - 3 * c;
     w.Cn(slot + k)[c] = s0 + s1;
   }
@@ -155,11 +160,11 @@ __device__ void contact_rows_times(const World<NT, HT>& w, const double* x, int 
 // A and of the contacts: part(0)[i] = sum_j A[j][i] x[j], part(1)[i] =
 // sum_j A[j][i] y[j], part(2)[i] = sum_c J_c[:, i] . gamma_c.  Lanes own DOFs
 // i = lane and lane + 32, so a warp reads consecutive addresses.
-template <int NT, typename HT>
-__device__ void dof_partials(const World<NT, HT>& w, const double* x, const double* y, bool with_gamma) {
+template <int NT, typename HT, int NS>
+__device__ void dof_partials(const World<NT, HT, NS>& w, const double* x, const double* y, bool with_gamma) {
   constexpr int NW = NT / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int n = w.n;
+  const int n = w.dofs();
   const int jchunk = (n + NW - 1) / NW;
   const int j0 = warp * jchunk, j1 = min(n, j0 + jchunk);
   const int cchunk = (w.count + NW - 1) / NW;
@@ -175,7 +180,7 @@ __device__ void dof_partials(const World<NT, HT>& w, const double* x, const doub
       if (y) b += aij * y[j];
     }
     if (with_gamma) {
-      const int ld = w.L.ldJ;
+      const int ld = w.ldJ();
       for (int c = c0; c < c1; ++c) {
         const double* Jc = w.J + (size_t)(3 * c) * ld + i;
         g += Jc[0] * w.Cn(C_GAMMA + 0)[c] + Jc[ld] * w.Cn(C_GAMMA + 1)[c] + Jc[2 * ld] * w.Cn(C_GAMMA + 2)[c];
@@ -187,8 +192,8 @@ __device__ void dof_partials(const World<NT, HT>& w, const double* x, const doub
   }
 }
 
-template <int NT, typename HT>
-__device__ __forceinline__ double sum_partials(const World<NT, HT>& w, int which, int i) {
+template <int NT, typename HT, int NS>
+__device__ __forceinline__ double sum_partials(const World<NT, HT, NS>& w, int which, int i) {
   constexpr int NW = NT / 32;
   double s = 0.0;
 #pragma unroll
@@ -200,11 +205,11 @@ __device__ __forceinline__ double sum_partials(const World<NT, HT>& w, int which
 // J^T gamma, PD and limit terms, gradient.  Returns {cost, |g|^2, |p|^2, |jc|^2}
 // (scaled, over participating DOFs) to every thread.  Restates
 // _solver_update_active sim/contact_solve.py:4080-4136.
-template <int NT, typename HT>
-__device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt, double out4[4]) {
+template <int NT, typename HT, int NS>
+__device__ void evaluate(const World<NT, HT, NS>& w, const SolveParams& P, double dt, double out4[4]) {
   const int tid = threadIdx.x;
-  contact_rows_times<NT, HT>(w, w.V(V_V), C_VC);
-  for (int i = tid; i < w.n; i += NT) w.V(V_TMP0)[i] = w.V(V_V)[i] - w.V(V_VSTAR)[i];
+  contact_rows_times<NT, HT, NS>(w, w.V(V_V), C_VC);
+  for (int i = tid; i < w.dofs(); i += NT) w.V(V_TMP0)[i] = w.V(V_V)[i] - w.V(V_VSTAR)[i];
   __syncthreads();
   double csum = 0.0;
   for (int c = tid; c < w.count; c += NT) {
@@ -216,15 +221,15 @@ __device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt
     csum += cost;
   }
   __syncthreads();
-  dof_partials<NT, HT>(w, w.V(V_TMP0), w.V(V_V), true);
+  dof_partials<NT, HT, NS>(w, w.V(V_TMP0), w.V(V_V), true);
   __syncthreads();
   double model_cost = 0.0, g2 = 0.0, p2 = 0.0, j2 = 0.0;
   const double* v = w.V(V_V);
   const double* vs = w.V(V_VSTAR);
-  for (int i = tid; i < w.n; i += NT) {
-    const double a_res = sum_partials<NT, HT>(w, 0, i);
-    const double a_v = sum_partials<NT, HT>(w, 1, i);
-    double imp = sum_partials<NT, HT>(w, 2, i);
+  for (int i = tid; i < w.dofs(); i += NT) {
+    const double a_res = sum_partials<NT, HT, NS>(w, 0, i);
+    const double a_v = sum_partials<NT, HT, NS>(w, 1, i);
+    double imp = sum_partials<NT, HT, NS>(w, 2, i);
     const double vi = v[i];
     double mc = 0.5 * (vi - vs[i]) * a_res;
     const int fl = w.flags[i];
@@ -283,12 +288,12 @@ __device__ void evaluate(const World<NT, HT>& w, const SolveParams& P, double dt
 // G (at the stored vc) and G J are formed chunk by chunk; each thread owns one
 // 4x4 tile of H and one of KS slices of a chunk's rows, accumulates in
 // registers across chunks, and the slices add into H in turn (deterministic).
-template <int NT, typename HT>
-__device__ void assemble_hessian(const World<NT, HT>& w, double diag_shift) {
+template <int NT, typename HT, int NS>
+__device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   constexpr int NW = NT / 32;
-  const int n = w.n, ldJ = w.L.ldJ, ldH = w.L.ldH, nb = w.L.nb;
+  const int n = w.dofs(), ldJ = w.ldJ(), ldH = w.ldH(), nb = w.nb();
   const int ncol = 4 * nb;
   // G at the current contact velocities (sim/contact_solve.py:1071-1217).
   for (int c = tid; c < w.count; c += NT) {
@@ -381,28 +386,58 @@ __device__ void assemble_hessian(const World<NT, HT>& w, double diag_shift) {
 // BlockCholeskySolverBatched (sim/blocked_cholesky.py:414-604).  A pivot that
 // is not positive/finite makes dv NaN, so the line search reports an ascent
 // direction as the reference's NaN factor does.
-template <int NT, typename HT>
-__device__ void factor_and_solve(const World<NT, HT>& w) {
+template <int NT, typename HT, int NS>
+__device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   const int tid = threadIdx.x;
-  const int n = w.n, ldH = w.L.ldH;
+  const int n = w.dofs(), ldH = w.ldH();
   HT* H = w.H;
+  HT* dinv = reinterpret_cast<HT*>(w.V(V_TMP0));  // 1/d_k, written one step ahead
   double* dv = w.V(V_DV);
+  // Right-looking LDL^T, all warps, one barrier per column.  At step k the
+  // (n-k-1)(n-k)/2 trailing entries are the first ones of the column-
+  // descending triangle list; thread 0 updates the next pivot first and
+  // stores its reciprocal, so no division sits on the other threads' path.
+  if (tid == 0) dinv[0] = HT(1) / H[0];
+  __syncthreads();
+  for (int k = 0; k < n - 1; ++k) {
+    const HT rinv = dinv[k];
+    const int m = n - k - 1;
+    const int cnt = m * (m + 1) / 2;
+    const size_t kk1 = (size_t)(k + 1) * ldH + (k + 1);
+    if (tid == 0) {
+      const HT l = H[(size_t)(k + 1) * ldH + k];
+      const HT d1 = H[kk1] - (l * rinv) * l;
+      H[kk1] = d1;
+      dinv[k + 1] = HT(1) / d1;
+    }
+    const int skip = cnt - m;  // list position of (k+1, k+1): first entry of column k+1
+    for (int e0 = tid; e0 < cnt; e0 += 4 * NT) {
+      int ii[4], jj[4];
+      HT hik[4], hjk[4], hij[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * NT;
+        ii[u] = -1;
+        if (e < cnt && e != skip) {
+          const int ij = w.tri[e];
+          ii[u] = ij >> 8;
+          jj[u] = ij & 255;
+          hik[u] = H[(size_t)ii[u] * ldH + k];
+          hjk[u] = H[(size_t)jj[u] * ldH + k];
+          hij[u] = H[(size_t)ii[u] * ldH + jj[u]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (ii[u] >= 0) H[(size_t)ii[u] * ldH + jj[u]] = hij[u] - (hik[u] * rinv) * hjk[u];
+    }
+    __syncthreads();
+  }
   if (tid < 32) {
     bool ok = true;
-    // At step k the (n-k-1)(n-k)/2 trailing entries are the first ones of the
-    // column-descending triangle list.
     for (int k = 0; k < n; ++k) {
       const HT d = H[(size_t)k * ldH + k];
       if (!(d > HT(0)) || !isfinite(double(d))) ok = false;
-      const HT rinv = HT(1) / d;
-      const int m = n - k - 1;
-      const int cnt = m * (m + 1) / 2;
-      for (int e = tid; e < cnt; e += 32) {
-        const int ij = w.tri[e];
-        const int i = ij >> 8, j = ij & 255;
-        H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + k] * rinv) * H[(size_t)j * ldH + k];
-      }
-      __syncwarp();
     }
     // Forward z = D^-1 (L^-1 b), backward x = L^-T z; lanes own rows lane, lane+32.
     const int lane = tid;
@@ -411,7 +446,7 @@ __device__ void factor_and_solve(const World<NT, HT>& w) {
     if (lane + 32 < n) hb1 = HT(-w.V(V_GRAD)[lane + 32]);
     for (int k = 0; k < n; ++k) {
       const HT bk = __shfl_sync(0xffffffffu, k < 32 ? hb0 : hb1, k & 31);
-      const HT zk = bk / H[(size_t)k * ldH + k];
+      const HT zk = bk * dinv[k];
       if (lane == (k & 31)) {
         if (k < 32) hb0 = zk;
         else hb1 = zk;
@@ -425,7 +460,7 @@ __device__ void factor_and_solve(const World<NT, HT>& w) {
       if (lane == (i & 31)) {
         const HT zi = i < 32 ? hb0 : hb1;
         const HT si = i < 32 ? s0 : s1;
-        xi_local = zi - si / H[(size_t)i * ldH + i];
+        xi_local = zi - si * dinv[i];
         if (i < 32) hb0 = xi_local;
         else hb1 = xi_local;
       }
@@ -445,8 +480,8 @@ __device__ void factor_and_solve(const World<NT, HT>& w) {
 // Restates _replace_trial_cost_with_sap_line_search_cost :2379-2420, the line
 // derivative :2304-2321 and the second derivative :2324-2375, using
 // vc(alpha) = vc + alpha * dvc.
-template <int NT, typename HT>
-__device__ void line_terms(const World<NT, HT>& w, const SolveParams& P, double dt, double alpha, bool want2,
+template <int NT, typename HT, int NS>
+__device__ void line_terms(const World<NT, HT, NS>& w, const SolveParams& P, double dt, double alpha, bool want2,
                            double out3[3]) {
   const int tid = threadIdx.x;
   double reg = 0.0, proj = 0.0, curv = 0.0;
@@ -464,7 +499,7 @@ __device__ void line_terms(const World<NT, HT>& w, const SolveParams& P, double 
     }
   }
   if (P.dof.has_pd || P.dof.has_limits) {
-    for (int i = tid; i < w.n; i += NT) {
+    for (int i = tid; i < w.dofs(); i += NT) {
       const double vi = w.V(V_V)[i] + alpha * w.V(V_DV)[i];
       const double dvi = w.V(V_DV)[i];
       const int fl = w.flags[i];
@@ -511,18 +546,18 @@ struct LsResult {
 
 // Line coefficients (sim/contact_solve.py:2234-2263, 1657-1692):
 // dp = A dv, dvc = J dv and {dell0, dell_a0, d2ell_a, mom0}.
-template <int NT, typename HT>
-__device__ void line_coefficients(const World<NT, HT>& w, double c4[4]) {
+template <int NT, typename HT, int NS>
+__device__ void line_coefficients(const World<NT, HT, NS>& w, double c4[4]) {
   const int tid = threadIdx.x;
-  contact_rows_times<NT, HT>(w, w.V(V_DV), C_DVC);
-  dof_partials<NT, HT>(w, w.V(V_DV), nullptr, false);
+  contact_rows_times<NT, HT, NS>(w, w.V(V_DV), C_DVC);
+  dof_partials<NT, HT, NS>(w, w.V(V_DV), nullptr, false);
   __syncthreads();
   double d0 = 0.0, da0 = 0.0, d2 = 0.0, m0 = 0.0;
   const double* v = w.V(V_V);
   const double* vs = w.V(V_VSTAR);
   const double* dv = w.V(V_DV);
-  for (int i = tid; i < w.n; i += NT) {
-    const double acc = sum_partials<NT, HT>(w, 0, i);
+  for (int i = tid; i < w.dofs(); i += NT) {
+    const double acc = sum_partials<NT, HT, NS>(w, 0, i);
     w.V(V_DP)[i] = acc;
     const double ri = v[i] - vs[i];
     d0 += w.V(V_GRAD)[i] * dv[i];
@@ -543,12 +578,12 @@ __device__ __forceinline__ bool armijo_ok(double alpha, double ell, double ell0,
 }
 
 // armijo_decay backtracking (sim/contact_solve.py:2670-2904, driver :5108-5305).
-template <int NT, typename HT>
-__device__ LsResult ls_armijo(const World<NT, HT>& w, const SolveParams& P, double dt, double cost) {
+template <int NT, typename HT, int NS>
+__device__ LsResult ls_armijo(const World<NT, HT, NS>& w, const SolveParams& P, double dt, double cost) {
   const sapb_solve_options& o = P.o;
   LsResult r{0, 0, 0, 0.0, cost};
   double c4[4];
-  line_coefficients<NT, HT>(w, c4);
+  line_coefficients<NT, HT, NS>(w, c4);
   const double dell0 = c4[0], dell_a0 = c4[1], d2ell_a = c4[2], mom0 = c4[3];
   const double amax = 1.0 / o.rho;
   const double slop_rel = o.line_search_relative_slop;
@@ -561,7 +596,7 @@ __device__ LsResult ls_armijo(const World<NT, HT>& w, const SolveParams& P, doub
     return r;
   }
   double t3[3];
-  line_terms<NT, HT>(w, P, dt, alpha, false, t3);
+  line_terms<NT, HT, NS>(w, P, dt, alpha, false, t3);
   double ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + t3[0];
   const double deriv = dell_a0 + alpha * d2ell_a - t3[1];
   {
@@ -579,7 +614,7 @@ __device__ LsResult ls_armijo(const World<NT, HT>& w, const SolveParams& P, doub
   if (o.line_search_max_iterations <= 1) return r;
   for (int iteration = 1;; ++iteration) {
     alpha = alpha * o.rho;
-    line_terms<NT, HT>(w, P, dt, alpha, false, t3);
+    line_terms<NT, HT, NS>(w, P, dt, alpha, false, t3);
     ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + t3[0];
     const double a = alpha, a_prev = alpha_prev, e_prev = ell_prev;
     const double denom = a - a_prev;
@@ -616,17 +651,17 @@ __device__ LsResult ls_armijo(const World<NT, HT>& w, const SolveParams& P, doub
 }
 
 // monotone_decay (fused kernel sim/contact_solve.py:2483-2667).
-template <int NT, typename HT>
-__device__ LsResult ls_monotone(const World<NT, HT>& w, const SolveParams& P, double dt, double cost) {
+template <int NT, typename HT, int NS>
+__device__ LsResult ls_monotone(const World<NT, HT, NS>& w, const SolveParams& P, double dt, double cost) {
   const sapb_solve_options& o = P.o;
   LsResult r{0, 0, 0, 1.0, cost};
   double c4[4];
-  line_coefficients<NT, HT>(w, c4);
+  line_coefficients<NT, HT, NS>(w, c4);
   const double base_linear = c4[1], base_quadratic = c4[2], base0 = c4[3];
   double alpha = 1.0, trial = cost;
   for (int it = 0; it < o.line_search_max_iterations; ++it) {
     double t3[3];
-    line_terms<NT, HT>(w, P, dt, alpha, false, t3);
+    line_terms<NT, HT, NS>(w, P, dt, alpha, false, t3);
     trial = base0 + alpha * base_linear + 0.5 * alpha * alpha * base_quadratic + t3[0];
     r.iterations += 1;
     const double tol = 1.0e-14 + 1.0e-12 * fabs(cost);
@@ -646,14 +681,14 @@ __device__ LsResult ls_monotone(const World<NT, HT>& w, const SolveParams& P, do
 }
 
 // exact_root (sim/contact_solve.py:2914-3140, driver :5700-5861).
-template <int NT, typename HT>
-__device__ LsResult ls_exact(const World<NT, HT>& w, const SolveParams& P, double dt, double cost) {
+template <int NT, typename HT, int NS>
+__device__ LsResult ls_exact(const World<NT, HT, NS>& w, const SolveParams& P, double dt, double cost) {
   const sapb_solve_options& o = P.o;
   LsResult r{0, 0, 0, kExactAlphaMax, cost};
   const int max_it = o.line_search_max_iterations;
   if (max_it <= 0) return r;
   double c4[4];
-  line_coefficients<NT, HT>(w, c4);
+  line_coefficients<NT, HT, NS>(w, c4);
   const double dell0 = c4[0], dell_a0 = c4[1], d2ell_a = c4[2], mom0 = c4[3];
   const double amax = kExactAlphaMax;
   if (dell0 >= 0.0 || !isfinite(dell0)) {
@@ -661,7 +696,7 @@ __device__ LsResult ls_exact(const World<NT, HT>& w, const SolveParams& P, doubl
     return r;
   }
   double t3[3];
-  line_terms<NT, HT>(w, P, dt, amax, true, t3);
+  line_terms<NT, HT, NS>(w, P, dt, amax, true, t3);
   const double ell = mom0 + amax * dell_a0 + 0.5 * amax * amax * d2ell_a + t3[0];
   const double deriv = dell_a0 + amax * d2ell_a - t3[1];
   const double deriv2 = d2ell_a + t3[2];
@@ -710,7 +745,7 @@ __device__ LsResult ls_exact(const World<NT, HT>& w, const SolveParams& P, doubl
     }
   }
   for (int iteration = 1; active; ++iteration) {
-    line_terms<NT, HT>(w, P, dt, r.alpha, true, t3);
+    line_terms<NT, HT, NS>(w, P, dt, r.alpha, true, t3);
     const double d = dell_a0 + r.alpha * d2ell_a - t3[1];
     const double d2 = d2ell_a + t3[2];
     const double f = d / scale, df = d2 / scale;
@@ -756,20 +791,20 @@ __device__ LsResult ls_exact(const World<NT, HT>& w, const SolveParams& P, doubl
     r.alpha = next_root;
   }
   if (r.accepted) {
-    line_terms<NT, HT>(w, P, dt, r.alpha, false, t3);
+    line_terms<NT, HT, NS>(w, P, dt, r.alpha, false, t3);
     r.accepted_cost = mom0 + r.alpha * dell_a0 + 0.5 * r.alpha * r.alpha * d2ell_a + t3[0];
   }
   return r;
 }
 
-template <int NT, typename HT, int MINB>
+template <int NT, typename HT, int MINB, int NS>
 __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolveParams P) {
   static_assert(NT / 32 <= Layout::kMaxWarps, "partial-sum scratch sized for kMaxWarps warps");
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[8 * (NT / 32)];
-  __shared__ int s_world;
+  __shared__ int s_next;
   const int tid = threadIdx.x;
-  const int n = P.p.dof_per_env, C = P.p.max_contacts;
+  const int n = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
   const Layout L = make_layout(n, C, (int)sizeof(HT));
   const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
   {
@@ -780,13 +815,33 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
     }
   }
 
+  if (tid == 0) s_next = atomicAdd(P.queue, 1);
   for (;;) {
-    if (tid == 0) s_world = atomicAdd(P.queue, 1);
+    // Take the prefetched index, claim the next world and warm L2 with its A
+    // and J (prefetch.global.L2 is a hint and has no alignment rule).
     __syncthreads();
-    const int e = s_world;
+    const int e = s_next;
     if (e >= P.p.num_envs) break;
+    __syncthreads();
+    if (tid == 0) s_next = atomicAdd(P.queue, 1);
+    __syncthreads();
+    {
+      const int nx = s_next;
+      if (nx < P.p.num_envs) {
+        const char* a0 = reinterpret_cast<const char*>(P.p.dynamics_matrix + (size_t)nx * n * n);
+        const size_t abytes = sizeof(double) * (size_t)n * n;
+        int cnt = P.p.contact_count[nx];
+        cnt = cnt < 0 ? 0 : (cnt > C ? C : cnt);
+        const char* j0 = reinterpret_cast<const char*>(P.p.jacobian + (size_t)nx * C * 3 * n);
+        const size_t jbytes = sizeof(double) * (size_t)cnt * 3 * n;
+        for (size_t off = (size_t)tid * 128; off < abytes; off += (size_t)NT * 128)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a0 + off));
+        for (size_t off = (size_t)tid * 128; off < jbytes; off += (size_t)NT * 128)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(j0 + off));
+      }
+    }
 
-    World<NT, HT> w{L,
+    World<NT, HT, NS> w{L,
                     P.p.dynamics_matrix + (size_t)e * n * n,
                     reinterpret_cast<double*>(smem + L.off_J),
                     reinterpret_cast<HT*>(smem + L.off_scr),
@@ -810,9 +865,29 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
     {
       const int rows = 3 * count;
       const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n;
-      const int lane = tid & 31, warp = tid >> 5;
-      for (int r = warp; r < rows; r += NT / 32) {
-        for (int j = lane; j < L.ldJ; j += 32) w.J[(size_t)r * L.ldJ + j] = j < n ? __ldg(Jg + (size_t)r * n + j) : 0.0;
+      const int ldj = w.ldJ();
+      // Flat copy of the contiguous rows*n block, 4 loads in flight per thread.
+      const int total = rows * n;
+      for (int k0 = tid; k0 < total; k0 += 4 * NT) {
+        double val[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + u * NT;
+          val[u] = k < total ? __ldg(Jg + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + u * NT;
+          if (k < total) {
+            const int r = k / n, j = k - r * n;
+            w.J[(size_t)r * ldj + j] = val[u];
+          }
+        }
+      }
+      // zero padding columns n..ldj-1
+      for (int k = tid; k < rows * (ldj - n); k += NT) {
+        const int r = k / (ldj - n), j = n + (k - r * (ldj - n));
+        w.J[(size_t)r * ldj + j] = 0.0;
       }
       for (int c = tid; c < count; c += NT) {
         const size_t ci = (size_t)e * C + c;
@@ -955,7 +1030,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       bool active = true;
       for (;;) {
         double e4[4];
-        evaluate<NT, HT>(w, P, dt, e4);
+        evaluate<NT, HT, NS>(w, P, dt, e4);
         evaluated = true;
         cost = e4[0];
         // convergence test (sim/contact_solve.py:2043-2087)
@@ -980,15 +1055,15 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         }
         if (!active) break;
         // Newton direction
-        assemble_hessian<NT, HT>(w, P.o.diag_shift);
-        factor_and_solve<NT, HT>(w);
+        assemble_hessian<NT, HT, NS>(w, P.o.diag_shift);
+        factor_and_solve<NT, HT, NS>(w);
         LsResult r;
         if (P.o.line_search_variant == SAPB_LS_ARMIJO_DECAY)
-          r = ls_armijo<NT, HT>(w, P, dt, cost);
+          r = ls_armijo<NT, HT, NS>(w, P, dt, cost);
         else if (P.o.line_search_variant == SAPB_LS_EXACT_ROOT)
-          r = ls_exact<NT, HT>(w, P, dt, cost);
+          r = ls_exact<NT, HT, NS>(w, P, dt, cost);
         else
-          r = ls_monotone<NT, HT>(w, P, dt, cost);
+          r = ls_monotone<NT, HT, NS>(w, P, dt, cost);
         alpha = r.alpha;
         status = r.status;
         const bool mono = P.o.line_search_variant == SAPB_LS_MONOTONE_DECAY;
@@ -1034,10 +1109,10 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   }
 }
 
-template <int NT, typename HT, int MINB>
+template <int NT, typename HT, int MINB, int NS>
 static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
   const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT));
-  auto kern = contact_solve_kernel<NT, HT, MINB>;
+  auto kern = contact_solve_kernel<NT, HT, MINB, NS>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (err != cudaSuccess) return err;
   int dev = 0;
@@ -1075,9 +1150,9 @@ int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_opt
   P.use_guess_flag_ptr_valid = (p->v_guess && p->v_guess_active) ? 1 : 0;
   P.queue = reinterpret_cast<int32_t*>(workspace);
   if (p->num_envs == 0) return SAPB_OK;
-  // The FP32 Hessian path also needs an FP32 linear solve: LDL^T in the
-  // Hessian type.  An FP64 Hessian with an FP32 factorization is not a
-  // separate kernel: the factor runs in FP64 then.
+  // If either the Hessian or the linear-solve precision is FP32, both the
+  // J^T G J assembly and the LDL^T factorization run in FP32; the gradient,
+  // costs, line search and convergence test stay FP64 in every variant.
   const bool fp32 = o->hessian_precision == SAPB_FP32 || o->linear_solve_precision == SAPB_FP32;
   const size_t smem = contact_solve_smem_bytes(p->dof_per_env, p->max_contacts, fp32 ? SAPB_FP32 : SAPB_FP64);
   if (smem > kMaxSmemPerBlock) {
@@ -1086,10 +1161,23 @@ int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_opt
     return SAPB_ERR_UNSUPPORTED;
   }
   cudaError_t err;
-  if (fp32)
-    err = launch_solve<128, float, 4>(P, stream, nullptr);
-  else
-    err = launch_solve<128, double, 3>(P, stream, nullptr);
+  // Kernels specialised on the DOF count of the common trees (humanoid 35,
+  // quadruped 18, arm + box 13, single free body 6); a generic one otherwise.
+  switch (p->dof_per_env) {
+#define SAPB_DISPATCH_N(NV)                                                              \
+  case NV:                                                                               \
+    err = fp32 ? launch_solve<128, float, 4, NV>(P, stream, nullptr)                     \
+               : launch_solve<128, double, 3, NV>(P, stream, nullptr);                   \
+    break;
+    SAPB_DISPATCH_N(35)
+    SAPB_DISPATCH_N(18)
+    SAPB_DISPATCH_N(13)
+    SAPB_DISPATCH_N(6)
+#undef SAPB_DISPATCH_N
+    default:
+      err = fp32 ? launch_solve<128, float, 4, 0>(P, stream, nullptr)
+                 : launch_solve<128, double, 3, 0>(P, stream, nullptr);
+  }
   if (err != cudaSuccess) {
     set_last_error("contact solve launch: %s", cudaGetErrorString(err));
     return SAPB_ERR_CUDA;
