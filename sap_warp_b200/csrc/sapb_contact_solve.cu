@@ -397,7 +397,7 @@ __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   // (n-k-1)(n-k)/2 trailing entries are the first ones of the column-
   // descending triangle list; thread 0 updates the next pivot first and
   // stores its reciprocal, so no division sits on the other threads' path.
-  if (tid == 0) dinv[0] = HT(1) / H[0];
+  if (tid == 0) dinv[0] = fast_recip(H[0]);
   __syncthreads();
   for (int k = 0; k < n - 1; ++k) {
     const HT rinv = dinv[k];
@@ -408,7 +408,7 @@ __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
       const HT l = H[(size_t)(k + 1) * ldH + k];
       const HT d1 = H[kk1] - (l * rinv) * l;
       H[kk1] = d1;
-      dinv[k + 1] = HT(1) / d1;
+      dinv[k + 1] = fast_recip(d1);
     }
     const int skip = cnt - m;  // list position of (k+1, k+1): first entry of column k+1
     for (int e0 = tid; e0 < cnt; e0 += 4 * NT) {

@@ -61,11 +61,8 @@ __device__ __forceinline__ int project_contact(const ContactConst& cc, double vc
   const double y2 = cc.rn_inv * (cc.vhat_n - vcz);
   const double m = cc.mu;
   const double yr = sqrt(y0 * y0 + y1 * y1 + kSoftNormTol * kSoftNormTol);
-  double tx = 0.0, ty = 0.0;
-  if (yr > 0.0) {
-    tx = y0 / yr;
-    ty = y1 / yr;
-  }
+  const double inv_yr = 1.0 / yr;  // yr >= 1e-7 > 0
+  const double tx = y0 * inv_yr, ty = y1 * inv_yr;
   double g0 = 0.0, g1 = 0.0, g2 = 0.0;
   int mode = SAPB_CONTACT_MODE_NONE;
   if (G) {
@@ -98,8 +95,7 @@ __device__ __forceinline__ int project_contact(const ContactConst& cc, double vc
       g2 = gn;
       if (G) {
         const double p00 = tx * tx, p01 = tx * ty, p11 = ty * ty;
-        double gn_over_yr = 0.0;
-        if (yr > 0.0) gn_over_yr = gn / yr;
+        const double gn_over_yr = gn * inv_yr;
         const double d00 = m * (gn_over_yr * (1.0 - p00) + mu_hat * factor * p00);
         const double d01 = m * (gn_over_yr * (-p01) + mu_hat * factor * p01);
         const double d11 = m * (gn_over_yr * (1.0 - p11) + mu_hat * factor * p11);
@@ -168,6 +164,22 @@ __device__ __forceinline__ void effective_pd_gains(double kp, double kd, double 
     *kd_eff = 0.0;
   }
 }
+
+// Reciprocal for pivots on a serial critical path.  Newton-Raphson iteration
+// for 1/d (x <- x + x (1 - d x), each step squaring the relative error) from
+// the FP32 reciprocal as seed: two steps take the ~2^-23 seed error to below
+// 2^-52, i.e. within an ulp or two of the correctly rounded quotient.  Values
+// outside the FP32 range (or not finite) use the IEEE division.
+__device__ __forceinline__ double fast_recip(double d) {
+  const double ad = fabs(d);
+  if (!(ad > 1.0e-30 && ad < 1.0e30)) return 1.0 / d;
+  double x = (double)__frcp_rn((float)d);
+  double e = fma(-d, x, 1.0);
+  x = fma(x, e, x);
+  e = fma(-d, x, 1.0);
+  return fma(x, e, x);
+}
+__device__ __forceinline__ float fast_recip(float d) { return __frcp_rn(d); }
 
 template <int NT>
 __device__ __forceinline__ double warp_sum(double v) {
