@@ -393,43 +393,61 @@ __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   HT* H = w.H;
   HT* dinv = reinterpret_cast<HT*>(w.V(V_TMP0));  // 1/d_k, written one step ahead
   double* dv = w.V(V_DV);
-  // Right-looking LDL^T, all warps, one barrier per column.  At step k the
-  // (n-k-1)(n-k)/2 trailing entries are the first ones of the column-
-  // descending triangle list; thread 0 updates the next pivot first and
-  // stores its reciprocal, so no division sits on the other threads' path.
-  if (tid == 0) dinv[0] = fast_recip(H[0]);
-  __syncthreads();
-  for (int k = 0; k < n - 1; ++k) {
-    const HT rinv = dinv[k];
-    const int m = n - k - 1;
-    const int cnt = m * (m + 1) / 2;
-    const size_t kk1 = (size_t)(k + 1) * ldH + (k + 1);
-    if (tid == 0) {
-      const HT l = H[(size_t)(k + 1) * ldH + k];
-      const HT d1 = H[kk1] - (l * rinv) * l;
-      H[kk1] = d1;
-      dinv[k + 1] = fast_recip(d1);
+  // Blocked right-looking LDL^T, 8-column blocks, three barriers per block.
+  // Storage: below the diagonal H[i][k] = L_ik d_k (L unit lower), D on the
+  // diagonal, dinv[k] = 1/d_k -- the layout the triangular solves read.
+  constexpr int B = 8;
+  const int lane = tid & 31;
+  for (int K = 0; K < n; K += B) {
+    const int bs = min(B, n - K);
+    // (1) diagonal block, unblocked, by warp 0
+    if (tid < 32) {
+      for (int s = 0; s < bs; ++s) {
+        const int ks = K + s;
+        const HT rinv = fast_recip(H[(size_t)ks * ldH + ks]);
+        if (lane == 0) dinv[ks] = rinv;
+        const int m = bs - s - 1;  // trailing entries (a, c), s < c <= a < bs
+        for (int q = lane; q < m * (m + 1) / 2; q += 32) {
+          int a = 0;
+          while ((a + 1) * (a + 2) / 2 <= q) ++a;
+          const int c = q - a * (a + 1) / 2;
+          const int i = ks + 1 + a, j = ks + 1 + c;
+          H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + ks] * rinv) * H[(size_t)j * ldH + ks];
+        }
+        __syncwarp();
+      }
     }
-    const int skip = cnt - m;  // list position of (k+1, k+1): first entry of column k+1
-    for (int e0 = tid; e0 < cnt; e0 += 4 * NT) {
-      int ii[4], jj[4];
-      HT hik[4], hjk[4], hij[4];
+    __syncthreads();
+    const int rest = n - K - bs;
+    if (rest <= 0) break;
+    // (2) panel rows: P L_K^T = H_panel (forward substitution over the block columns)
+    for (int t = tid; t < rest; t += NT) {
+      const int i = K + bs + t;
+      HT p[B];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * NT;
-        ii[u] = -1;
-        if (e < cnt && e != skip) {
-          const int ij = w.tri[e];
-          ii[u] = ij >> 8;
-          jj[u] = ij & 255;
-          hik[u] = H[(size_t)ii[u] * ldH + k];
-          hjk[u] = H[(size_t)jj[u] * ldH + k];
-          hij[u] = H[(size_t)ii[u] * ldH + jj[u]];
+      for (int c = 0; c < B; ++c) {
+        if (c < bs) {
+          HT h = H[(size_t)i * ldH + K + c];
+#pragma unroll
+          for (int m2 = 0; m2 < B; ++m2)
+            if (m2 < c) h -= p[m2] * (H[(size_t)(K + c) * ldH + K + m2] * dinv[K + m2]);
+          p[c] = h;
+          H[(size_t)i * ldH + K + c] = h;
         }
       }
+    }
+    __syncthreads();
+    // (3) trailing update of entries (i, j), j >= K + bs: the first
+    // rest*(rest+1)/2 entries of the column-descending triangle list.
+    const int cnt = rest * (rest + 1) / 2;
+    for (int e = tid; e < cnt; e += NT) {
+      const int ij = w.tri[e];
+      const int i = ij >> 8, j = ij & 255;
+      HT acc = H[(size_t)i * ldH + j];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (ii[u] >= 0) H[(size_t)ii[u] * ldH + jj[u]] = hij[u] - (hik[u] * rinv) * hjk[u];
+      for (int c = 0; c < B; ++c)
+        if (c < bs) acc -= H[(size_t)i * ldH + K + c] * dinv[K + c] * H[(size_t)j * ldH + K + c];
+      H[(size_t)i * ldH + j] = acc;
     }
     __syncthreads();
   }
