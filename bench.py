@@ -26,7 +26,6 @@ import json
 import os
 import subprocess
 import sys
-import threading
 import time
 
 import numpy as np
@@ -42,7 +41,7 @@ SEED = 2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--worlds", type=int, default=WORLDS)
@@ -61,56 +60,80 @@ def algorithmic_bytes(prob) -> int:
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling around the timed region.
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    Samples stream to a file every 50 ms from before the warm-up until the
+    timed region has ended; samples stamped inside the region are used (the
+    nearest ones if the region is shorter than the sampling period)."""
+
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
+        import tempfile
+
         self.index = index
         self.proc = None
-        self.lines: list[str] = []
+        self.path = tempfile.mktemp(prefix="sapb_clocks_", suffix=".csv")
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+                 "-lms", "50", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        deadline = time.time() + 5.0  # wait for the first sample
+        while time.time() < deadline:
+            if os.path.exists(self.path) and os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def mark_begin(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(0.12)  # let a sample land after the region
 
     def stop(self) -> dict:
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        rows = []
+        try:
+            lines = open(self.path).read().splitlines()
+            os.unlink(self.path)
+        except OSError:
+            lines = []
+        from datetime import datetime
+
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 7:
+            if len(parts) < 8:
                 continue
             try:
-                sm.append(float(parts[0]))
-                smax.append(float(parts[1]))
+                ts = datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[1]), float(parts[2]), parts[4:8]))
             except ValueError:
                 continue
-            for name, val in zip(names, parts[3:7]):
-                if val.lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        inside = [r for r in rows if self.t0 is not None and self.t0 <= r[0] <= self.t1]
+        if not inside and self.t0 is not None:
+            mid = 0.5 * (self.t0 + self.t1)
+            inside = sorted(rows, key=lambda r: abs(r[0] - mid))[:2]
+        reasons = sorted({n for r in inside for n, v in zip(self.NAMES, r[3]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[1] for r in inside])), "sm_max_mhz": max(r[2] for r in inside),
+                "reasons": reasons, "samples": len(inside)}
 
 
 def oracle_time(prob, steps: int, threads: int, min_seconds: float = 0.0):
@@ -141,7 +164,7 @@ def run_reference(args, rank: int, world_size: int):
     cores = os.cpu_count() or 1
     for _ in range(max(0, args.warmup)):
         oracle_time(prob.subset(np.arange(min(256, prob.num_envs))), 1, cores)
-    sec, k = oracle_time(prob, args.steps, cores, min_seconds=120.0)
+    sec, k = oracle_time(prob, args.steps, cores, min_seconds=60.0)
     value = prob.num_envs / sec
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "world-steps/s", "n_gpus": args.gpus,
@@ -199,16 +222,20 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         return float(tt.item())
 
-    def timed(opts, steps, warmup):
+    def timed(opts, steps, warmup, sampler=None):
         for _ in range(warmup):
             contact_solve(**t, buffers=buf, options=opts)
         barrier()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.mark_begin()
         ev0.record(stream)
         for _ in range(steps):
             contact_solve(**t, buffers=buf, options=opts)
         ev1.record(stream)
         barrier()
+        if sampler:
+            sampler.mark_end()
         return max_over_ranks(ev0.elapsed_time(ev1) / steps)
 
     # plain FP64 solve
@@ -219,7 +246,7 @@ def main():
     # fast path (the headline)
     sampler = ClockSampler(local_rank)
     sampler.start()
-    ms_fast = timed(opt_fast, args.steps, args.warmup)
+    ms_fast = timed(opt_fast, args.steps, args.warmup, sampler)
     clocks = sampler.stop()
     it_fast = float(buf.newton_iterations.double().mean())
     conv_fast = bool(buf.converged.all())
