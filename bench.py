@@ -33,6 +33,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one solve
+# launch on this workload, measured once with ncu.
+NCU_TRAFFIC_BYTES = 117.821440e6 + 5.310464e6
+
 METRIC = "world-steps/s, 4096 humanoids: learned+FP32 vs plain FP64, same B200, same tol"
 WORLDS = 4096
 SEED = 2
@@ -303,7 +307,8 @@ def main():
         "e2e": {"value": total_worlds / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None,
+                     "frac": achieved / hbm_peak,
+                     "traffic": NCU_TRAFFIC_BYTES if args.worlds == WORLDS else None,
                      "note": "kernel is FP64/FP32-pipe bound, not HBM bound; achieved = algorithmic bytes / "
                              "kernel time (of measured peak)"},
         "gpu_launches": args.steps,
