@@ -172,6 +172,21 @@ int32_t sapb_contact_solve(const sapb_contact_problem* problem, const sapb_solve
                            const sapb_solve_outputs* out, void* workspace, size_t workspace_bytes,
                            void* stream);
 
+/* The same solve as sapb_contact_solve for callers that cannot allocate device
+ * memory (for example a plugin whose host runtime owns every device
+ * allocation, or a binding with no device allocator): no workspace argument,
+ * and no cudaMalloc / cudaFree or allocating library call.  No counterpart in
+ * the reference.  Its scratch is a fixed 4 KiB array compiled into the
+ * library, held by every GPU that loads the library until exit; problems
+ * whose sapb_contact_solve_workspace_size exceeds it are rejected with
+ * SAPB_ERR_WORKSPACE_TOO_SMALL.  The first call on a device looks up the
+ * array's device address (once per device, with that device current); make
+ * that first call before any stream capture.  All calls share the array and
+ * the solve clears what must start at zero, so calls that overlap on the GPU
+ * (concurrent streams) race: serialize them. */
+int32_t sapb_contact_solve_noalloc(const sapb_contact_problem* problem, const sapb_solve_options* opts,
+                                   const sapb_solve_outputs* out, void* stream);
+
 /* Last CUDA error string seen by the library on this thread ("" if none). */
 const char* sapb_last_error(void);
 

@@ -138,6 +138,9 @@ EXPORTS = {
         C.c_int32,
         [C.POINTER(ContactProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p, C.c_size_t, _p],
     ),
+    "sapb_contact_solve_noalloc": (
+        C.c_int32, [C.POINTER(ContactProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p]
+    ),
     "sapb_last_error": (C.c_char_p, []),
 }
 
