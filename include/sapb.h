@@ -50,6 +50,15 @@ extern "C" {
 #define SAPB_CONTACT_MODE_SLIDING 2
 #define SAPB_CONTACT_MODE_FRICTIONLESS 3
 
+/* joint types (sim/sap_runtime.py:21-27) */
+#define SAPB_JOINT_PRISMATIC 0
+#define SAPB_JOINT_REVOLUTE 1
+#define SAPB_JOINT_BALL 2
+#define SAPB_JOINT_FIXED 3
+#define SAPB_JOINT_FREE 4
+#define SAPB_JOINT_DISTANCE 5
+#define SAPB_JOINT_D6 6
+
 /* line-search variants (sim/contact_solve.py:69-81) */
 #define SAPB_LS_MONOTONE_DECAY 0
 #define SAPB_LS_ARMIJO_DECAY 1
@@ -150,6 +159,123 @@ typedef struct sapb_solve_outputs {
   int32_t* status;                /* [E] last line-search status (0 or SAPB_LS_*) */
   double* grad_norm;              /* [E] ||D^-1/2 grad|| over participating DOFs */
 } sapb_solve_outputs;
+
+/* ---- free motion + contact Jacobian ---------------------------------------
+ * Model of W replicated worlds with equal contiguous per-world blocks of
+ * joints, bodies, DOFs and coordinates (the layout the reference requires,
+ * sim/contact_solve.py:3327-3335).  Arrays are global (all worlds), indices
+ * global, as in SapModel (sim/sap_runtime.py:47-174).  Joints are ordered
+ * parents before children within each articulation. */
+typedef struct sapb_model_desc {
+  int32_t num_worlds;
+  int32_t joints_per_world;
+  int32_t bodies_per_world;
+  int32_t dofs_per_world;
+  int32_t coords_per_world;
+  int32_t articulations_per_world;
+  int32_t num_shapes;
+  const int32_t* joint_type;        /* [J] SAP_JOINT_* of sim/sap_runtime.py:21-27 */
+  const int32_t* joint_parent;      /* [J] parent body or -1 */
+  const int32_t* joint_child;       /* [J] child body */
+  const int32_t* joint_ancestor;    /* [J] parent joint or -1 */
+  const int32_t* joint_q_start;     /* [J+1] */
+  const int32_t* joint_qd_start;    /* [J+1] */
+  const int32_t* joint_dof_dim;     /* [J][2] linear, angular axis counts */
+  const int32_t* articulation_start;/* [A+1] */
+  const double* joint_axis;         /* [dofs][3] */
+  const double* joint_X_p;          /* [J][7] p, q(xyzw): joint frame F in the parent */
+  const double* joint_X_c;          /* [J][7] joint frame M in the child */
+  const double* joint_armature;     /* [dofs] */
+  const double* body_mass;          /* [B] */
+  const double* body_inertia;       /* [B][3][3] about the COM, body axes */
+  const double* body_com;           /* [B][3] body frame */
+  const double* gravity;            /* [W][3] */
+  const int32_t* shape_body;        /* [S] (-1: static) */
+  const double* shape_material_mu;  /* [S] or NULL -> fallback */
+  const double* shape_material_ke;  /* [S] or NULL -> fallback */
+  const double* shape_material_tau; /* [S] or NULL -> fallback */
+} sapb_model_desc;
+
+/* Start-of-step state, control and the flat contact buffer of collision
+ * (SapState / SapControl / SapContacts, sim/sap_runtime.py:177-264), SAP DOF
+ * order, FP64 mirrors of the contact arrays. */
+typedef struct sapb_step_inputs {
+  const double* joint_q;            /* [coords] */
+  const double* joint_qd;           /* [dofs] */
+  const double* joint_f;            /* [dofs] or NULL */
+  const double* body_f;             /* [B][6] negated applied wrench at the body origin, or NULL */
+  const double* dt;                 /* [W] */
+  int32_t contact_capacity;         /* length of the flat contact arrays */
+  const int32_t* contact_count;     /* [1] live contacts */
+  const int32_t* contact_shape0;    /* [N] */
+  const int32_t* contact_shape1;    /* [N] */
+  const double* contact_point0;     /* [N][3] in the body frame of shape0's body (world if static) */
+  const double* contact_point1;     /* [N][3] */
+  const double* contact_normal;     /* [N][3] world, from shape0 to shape1 */
+  const double* contact_margin0;    /* [N] */
+  const double* contact_margin1;    /* [N] */
+} sapb_step_inputs;
+
+#define SAPB_WEIGHT_BODY_INERTIA 0
+#define SAPB_WEIGHT_DIAG_DELASSUS 1
+#define SAPB_POINT_WITNESS 0
+#define SAPB_POINT_MIDPOINT 1
+
+typedef struct sapb_prepare_options {
+  int32_t max_contacts;             /* per-world slots (max_rigid_contact) */
+  int32_t contact_weight_mode;      /* SAPB_WEIGHT_* (sim/contact_jacobian.py:153-401) */
+  int32_t contact_point_mode;       /* SAPB_POINT_* */
+  double fallback_mu;
+  double fallback_stiffness;
+  double fallback_tau_d;
+} sapb_prepare_options;
+
+/* Outputs: SapFreeMotionResult (sim/free_motion.py:63-68) and the
+ * SapContactJacobianResult arrays the contact solve reads
+ * (sim/contact_jacobian.py:51-84).  Any pointer but v_star,
+ * dynamics_matrix, jacobian and the contact arrays may be NULL. */
+typedef struct sapb_prepare_outputs {
+  double* v_star;                   /* [dofs] */
+  double* vdot;                     /* [dofs] */
+  double* dynamics_matrix;          /* [W][n][n]  A = M + diag(armature) */
+  double* jacobian;                 /* [W][C][3][n] */
+  int32_t* contact_count;           /* [W] contacts in each world (before clamping to C) */
+  double* phi0;                     /* [W][C] */
+  double* w_eff;                    /* [W][C] */
+  double* mu;                       /* [W][C] */
+  double* stiffness;                /* [W][C] */
+  double* tau_d;                    /* [W][C] */
+  int32_t* body0;                   /* [W][C] global bodies */
+  int32_t* body1;                   /* [W][C] */
+  double* point;                    /* [W][C][3] stiffness-weighted contact point, or NULL */
+  double* frame;                    /* [W][C][9] rows t1, t2, n, or NULL */
+  int32_t* truncated_count;         /* [1] contacts beyond max_contacts, or NULL */
+  double* body_q;                   /* [B][7] start-of-step body poses, or NULL */
+} sapb_prepare_outputs;
+
+/* Device workspace bytes of sapb_free_motion_contacts. */
+size_t sapb_prepare_workspace_size(const sapb_model_desc* model, int32_t max_contacts);
+
+/* Free motion and contact Jacobian of every world: FK, bias forces, RNEA,
+ * the mass matrix and v* (SapFreeMotion.compute, sim/free_motion.py:2180-2208
+ * with _compute_sap_core :2094-2178), then the per-world contact slots, frames,
+ * phi0, combined materials, Jacobian rows and weights
+ * (SapContactJacobian.compute, sim/contact_jacobian.py:1649-1985).  Slots are
+ * taken in arrival order like the reference's atomic scatter (:470). */
+int32_t sapb_free_motion_contacts(const sapb_model_desc* model, const sapb_step_inputs* in,
+                                  const sapb_prepare_options* opts, const sapb_prepare_outputs* out,
+                                  void* workspace, size_t workspace_bytes, void* stream);
+
+#define SAPB_INTEGRATE_SAP_EULER 0
+#define SAPB_INTEGRATE_MIDPOINT 1
+
+/* Position integration q_{n+1} from SAP-order velocities (FP64 state),
+ * replaces _integrate_generalized_positions_{sap_euler,midpoint}_f64
+ * (sim/solver_sap.py:288-733, driven by :1267-1386).  v_prev is the
+ * start-of-step velocity (midpoint only). */
+int32_t sapb_integrate_positions(const sapb_model_desc* model, const double* joint_q_in, const double* v_prev,
+                                 const double* v_new, const double* dt, int32_t mode, double* joint_q_out,
+                                 void* stream);
 
 /* Fill the reference defaults of SapContactSolve for a line-search variant.
  * Replaces the Python defaults of solve(), sim/contact_solve.py:6129-6182. */

@@ -129,6 +129,96 @@ class SolveOutputs(C.Structure):
     ]
 
 
+SAPB_JOINT_PRISMATIC, SAPB_JOINT_REVOLUTE, SAPB_JOINT_BALL, SAPB_JOINT_FIXED = 0, 1, 2, 3
+SAPB_JOINT_FREE, SAPB_JOINT_DISTANCE, SAPB_JOINT_D6 = 4, 5, 6
+SAPB_WEIGHT_BODY_INERTIA, SAPB_WEIGHT_DIAG_DELASSUS = 0, 1
+SAPB_POINT_WITNESS, SAPB_POINT_MIDPOINT = 0, 1
+SAPB_INTEGRATE_SAP_EULER, SAPB_INTEGRATE_MIDPOINT = 0, 1
+
+
+class ModelDesc(C.Structure):
+    _fields_ = [
+        ("num_worlds", C.c_int32),
+        ("joints_per_world", C.c_int32),
+        ("bodies_per_world", C.c_int32),
+        ("dofs_per_world", C.c_int32),
+        ("coords_per_world", C.c_int32),
+        ("articulations_per_world", C.c_int32),
+        ("num_shapes", C.c_int32),
+        ("joint_type", _p),
+        ("joint_parent", _p),
+        ("joint_child", _p),
+        ("joint_ancestor", _p),
+        ("joint_q_start", _p),
+        ("joint_qd_start", _p),
+        ("joint_dof_dim", _p),
+        ("articulation_start", _p),
+        ("joint_axis", _p),
+        ("joint_X_p", _p),
+        ("joint_X_c", _p),
+        ("joint_armature", _p),
+        ("body_mass", _p),
+        ("body_inertia", _p),
+        ("body_com", _p),
+        ("gravity", _p),
+        ("shape_body", _p),
+        ("shape_material_mu", _p),
+        ("shape_material_ke", _p),
+        ("shape_material_tau", _p),
+    ]
+
+
+class StepInputs(C.Structure):
+    _fields_ = [
+        ("joint_q", _p),
+        ("joint_qd", _p),
+        ("joint_f", _p),
+        ("body_f", _p),
+        ("dt", _p),
+        ("contact_capacity", C.c_int32),
+        ("contact_count", _p),
+        ("contact_shape0", _p),
+        ("contact_shape1", _p),
+        ("contact_point0", _p),
+        ("contact_point1", _p),
+        ("contact_normal", _p),
+        ("contact_margin0", _p),
+        ("contact_margin1", _p),
+    ]
+
+
+class PrepareOptions(C.Structure):
+    _fields_ = [
+        ("max_contacts", C.c_int32),
+        ("contact_weight_mode", C.c_int32),
+        ("contact_point_mode", C.c_int32),
+        ("fallback_mu", C.c_double),
+        ("fallback_stiffness", C.c_double),
+        ("fallback_tau_d", C.c_double),
+    ]
+
+
+class PrepareOutputs(C.Structure):
+    _fields_ = [
+        ("v_star", _p),
+        ("vdot", _p),
+        ("dynamics_matrix", _p),
+        ("jacobian", _p),
+        ("contact_count", _p),
+        ("phi0", _p),
+        ("w_eff", _p),
+        ("mu", _p),
+        ("stiffness", _p),
+        ("tau_d", _p),
+        ("body0", _p),
+        ("body1", _p),
+        ("point", _p),
+        ("frame", _p),
+        ("truncated_count", _p),
+        ("body_q", _p),
+    ]
+
+
 # name -> (restype, argtypes) of every symbol include/sapb.h declares.
 EXPORTS = {
     "sapb_solve_options_default": (None, [C.POINTER(SolveOptions), C.c_int32]),
@@ -142,6 +232,15 @@ EXPORTS = {
         C.c_int32, [C.POINTER(ContactProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p]
     ),
     "sapb_last_error": (C.c_char_p, []),
+    "sapb_prepare_workspace_size": (C.c_size_t, [C.POINTER(ModelDesc), C.c_int32]),
+    "sapb_free_motion_contacts": (
+        C.c_int32,
+        [C.POINTER(ModelDesc), C.POINTER(StepInputs), C.POINTER(PrepareOptions), C.POINTER(PrepareOutputs), _p,
+         C.c_size_t, _p],
+    ),
+    "sapb_integrate_positions": (
+        C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, C.c_int32, _p, _p]
+    ),
 }
 
 

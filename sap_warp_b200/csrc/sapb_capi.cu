@@ -111,4 +111,73 @@ int32_t sapb_contact_solve(const sapb_contact_problem* p, const sapb_solve_optio
   return sapb::contact_solve_launch(p, o, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
+size_t sapb_prepare_workspace_size(const sapb_model_desc* m, int32_t max_contacts) {
+  if (!m || max_contacts < 0) return 0;
+  return sizeof(int32_t) * ((size_t)m->num_worlds * (size_t)(max_contacts + 1) + 1) + 256;
+}
+
+static int32_t check_model(const sapb_model_desc* m, const char* where) {
+  if (!m || m->num_worlds < 0 || m->joints_per_world <= 0 || m->bodies_per_world <= 0 || m->dofs_per_world <= 0 ||
+      m->articulations_per_world <= 0) {
+    sapb::set_last_error("%s: bad model sizes", where);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (!m->joint_type || !m->joint_parent || !m->joint_child || !m->joint_ancestor || !m->joint_q_start ||
+      !m->joint_qd_start || !m->joint_dof_dim || !m->articulation_start || !m->joint_axis || !m->joint_X_p ||
+      !m->joint_X_c || !m->joint_armature || !m->body_mass || !m->body_inertia || !m->body_com || !m->gravity) {
+    sapb::set_last_error("%s: missing model array", where);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return SAPB_OK;
+}
+
+int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inputs* in,
+                                  const sapb_prepare_options* o, const sapb_prepare_outputs* out,
+                                  void* workspace, size_t workspace_bytes, void* stream) {
+  const int32_t st = check_model(m, "sapb_free_motion_contacts");
+  if (st != SAPB_OK) return st;
+  if (!in || !o || !out || !in->joint_q || !in->joint_qd || !in->dt || !out->v_star || !out->dynamics_matrix) {
+    sapb::set_last_error("sapb_free_motion_contacts: missing input or output array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (o->max_contacts < 0 || in->contact_capacity < 0) {
+    sapb::set_last_error("sapb_free_motion_contacts: negative contact sizes");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (in->contact_capacity > 0 &&
+      (!in->contact_count || !in->contact_shape0 || !in->contact_shape1 || !in->contact_point0 ||
+       !in->contact_point1 || !in->contact_normal || !m->shape_body)) {
+    sapb::set_last_error("sapb_free_motion_contacts: missing contact array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (o->max_contacts > 0 && (!out->jacobian || !out->phi0 || !out->w_eff || !out->mu || !out->stiffness ||
+                              !out->tau_d || !out->body0 || !out->body1)) {
+    sapb::set_last_error("sapb_free_motion_contacts: missing contact output array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  const size_t smem = sapb::prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, o->max_contacts);
+  if (smem > sapb::kMaxSmemPerBlock) {
+    sapb::set_last_error("sapb_free_motion_contacts: world too large for one block (%zu bytes of shared memory)",
+                         smem);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if (!workspace || workspace_bytes < sapb_prepare_workspace_size(m, o->max_contacts)) {
+    sapb::set_last_error("sapb_free_motion_contacts: workspace missing or too small");
+    return SAPB_ERR_WORKSPACE_TOO_SMALL;
+  }
+  return sapb::prepare_launch(m, in, o, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int32_t sapb_integrate_positions(const sapb_model_desc* m, const double* q_in, const double* v_prev,
+                                 const double* v_new, const double* dt, int32_t mode, double* q_out, void* stream) {
+  const int32_t st = check_model(m, "sapb_integrate_positions");
+  if (st != SAPB_OK) return st;
+  if (!q_in || !v_new || !dt || !q_out || (mode == SAPB_INTEGRATE_MIDPOINT && !v_prev) ||
+      (mode != SAPB_INTEGRATE_MIDPOINT && mode != SAPB_INTEGRATE_SAP_EULER)) {
+    sapb::set_last_error("sapb_integrate_positions: bad arguments");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::integrate_launch(m, q_in, v_prev, v_new, dt, mode, q_out, static_cast<cudaStream_t>(stream));
+}
+
 }  // extern "C"

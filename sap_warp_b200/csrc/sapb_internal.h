@@ -20,4 +20,11 @@ size_t contact_solve_smem_bytes(int n, int C, int hessian_precision);
 int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_options* o, const sapb_solve_outputs* out,
                              void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
+size_t prepare_smem_bytes(int B, int n, int C);
+int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, const sapb_prepare_options* o,
+                       const sapb_prepare_outputs* out, void* workspace, size_t workspace_bytes,
+                       cudaStream_t stream);
+int32_t integrate_launch(const sapb_model_desc* m, const double* q_in, const double* v_prev, const double* v_new,
+                         const double* dt, int mode, double* q_out, cudaStream_t stream);
+
 }  // namespace sapb

@@ -1,0 +1,293 @@
+"""Seeded synthetic models of the reference's workload shapes, as SapModel
+(torch) and as plain numpy dictionaries, plus a ground-contact generator
+that writes the flat SapContacts buffer the way the reference's collision
+writer does (witness points in the body frames of their shapes, normal from
+shape0 to shape1; sim/collision/pipeline.py:52-118).
+
+No scene file or dataset is involved: the reference's robot assets are
+fetched over the network and its benchmark data is synthetic, so every model
+here is generated from a seed.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .runtime import (
+    SAP_JOINT_FREE,
+    SAP_JOINT_PRISMATIC,
+    SAP_JOINT_REVOLUTE,
+    SapContacts,
+    SapModel,
+)
+
+_IDENT7 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0])
+
+
+def _random_unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _random_quat(rng, n):
+    q = rng.normal(size=(n, 4))
+    return q / np.linalg.norm(q, axis=1, keepdims=True)
+
+
+def _spd_inertia(rng, m, link):
+    from .scenes import _random_rotations
+
+    R = _random_rotations(rng, 1)[0]
+    d = rng.uniform(0.5, 2.0, size=3) * m * link * link / 6.0
+    return R @ np.diag(d) @ R.T + 1e-4 * np.eye(3)
+
+
+def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: bool = False) -> dict:
+    """One world's topology and inertia (numpy).  kind: 'humanoid' (free base
+    + 29-revolute serial chain, 35 DOF), 'quadruped' (free base + 4 legs x 3
+    revolute, 18 DOF), 'box' (one free box, 6 DOF), 'arm_box' (7-revolute
+    fixed-base arm + free box, 13 DOF), 'slider' (free base + prismatic +
+    revolute chain)."""
+    joints = []  # (type, parent_body, axis or None, X_p, X_c)
+    link = 0.12
+    if kind == "humanoid":
+        joints.append((SAP_JOINT_FREE, -1, None))
+        for b in range(1, 30):
+            joints.append((SAP_JOINT_REVOLUTE, b - 1, None))
+    elif kind == "quadruped":
+        joints.append((SAP_JOINT_FREE, -1, None))
+        for leg in range(4):
+            for k in range(3):
+                parent = 0 if k == 0 else len(joints) - 1
+                joints.append((SAP_JOINT_REVOLUTE, parent, None))
+    elif kind == "box":
+        joints.append((SAP_JOINT_FREE, -1, None))
+    elif kind == "arm_box":
+        for k in range(7):
+            joints.append((SAP_JOINT_REVOLUTE, k - 1, None))
+        joints.append((SAP_JOINT_FREE, -1, None))
+    elif kind == "slider":
+        joints.append((SAP_JOINT_FREE, -1, None))
+        joints.append((SAP_JOINT_PRISMATIC, 0, None))
+        for b in range(2, 6):
+            joints.append((SAP_JOINT_REVOLUTE, b - 1, None))
+    else:
+        raise ValueError(kind)
+    B = len(joints)
+    jtype = np.array([j[0] for j in joints], np.int32)
+    parent = np.array([j[1] for j in joints], np.int32)
+    axis_per_joint = _random_unit(rng, B)
+    X_p = np.tile(_IDENT7, (B, 1))
+    X_c = np.tile(_IDENT7, (B, 1))
+    for k in range(B):
+        if parent[k] >= 0:
+            X_p[k, :3] = _random_unit(rng, 1)[0] * link
+            if random_child_frames:
+                X_p[k, 3:] = _random_quat(rng, 1)[0]
+        elif jtype[k] != SAP_JOINT_FREE:
+            X_p[k, :3] = [0.0, 0.0, 0.5]
+        if random_child_frames:
+            X_c[k, :3] = _random_unit(rng, 1)[0] * 0.03
+            X_c[k, 3:] = _random_quat(rng, 1)[0]
+    mass = rng.uniform(0.5, 2.0, size=B)
+    if kind in ("humanoid", "quadruped", "slider"):
+        mass[0] *= 4.0
+    inertia = np.stack([_spd_inertia(rng, mass[b], link) for b in range(B)])
+    com = rng.uniform(-0.5, 0.5, size=(B, 3)) * link * 0.5
+    dofdim = np.zeros((B, 2), np.int32)
+    ncoord = np.zeros(B, np.int32)
+    for k in range(B):
+        if jtype[k] == SAP_JOINT_FREE:
+            dofdim[k] = (3, 3)
+            ncoord[k] = 7
+        elif jtype[k] == SAP_JOINT_REVOLUTE:
+            dofdim[k] = (0, 1)
+            ncoord[k] = 1
+        elif jtype[k] == SAP_JOINT_PRISMATIC:
+            dofdim[k] = (1, 0)
+            ncoord[k] = 1
+    ndof = dofdim.sum(1)
+    qd_start = np.concatenate([[0], np.cumsum(ndof)]).astype(np.int32)
+    q_start = np.concatenate([[0], np.cumsum(ncoord)]).astype(np.int32)
+    n = int(qd_start[-1])
+    axis = np.zeros((n, 3))
+    for k in range(B):
+        if jtype[k] in (SAP_JOINT_REVOLUTE, SAP_JOINT_PRISMATIC):
+            axis[qd_start[k]] = axis_per_joint[k]
+    # joint ancestor: the joint whose child is this joint's parent body
+    child = np.arange(B, dtype=np.int32)
+    ancestor = np.array([parent[k] if parent[k] >= 0 else -1 for k in range(B)], np.int32)
+    # articulations: roots start new ones (joints ordered parent before child)
+    art_start = [k for k in range(B) if parent[k] < 0] + [B]
+    armature = np.where(np.repeat(jtype == SAP_JOINT_FREE, ndof), 0.0, 0.01)
+    return dict(kind=kind, joint_type=jtype, joint_parent=parent, joint_child=child, joint_ancestor=ancestor,
+                joint_q_start=q_start, joint_qd_start=qd_start, joint_dof_dim=dofdim, joint_axis=axis,
+                joint_X_p=X_p, joint_X_c=X_c, body_mass=mass, body_inertia=inertia, body_com=com,
+                joint_armature=armature, articulation_start=np.array(art_start, np.int32),
+                bodies_per_world=B, joints_per_world=B, dofs_per_world=n, coords_per_world=int(q_start[-1]))
+
+
+def random_joint_q(tpl: dict, rng: np.random.Generator, worlds: int, spread: float = 0.05) -> np.ndarray:
+    """Coordinates per world: free bases at height ~1 m with random yaw/tilt,
+    revolute/prismatic coordinates ~ N(0, spread) around a random rest pose."""
+    Q = tpl["coords_per_world"]
+    q = np.zeros((worlds, Q))
+    rest = rng.uniform(-1.0, 1.0, size=Q)
+    for k, jt in enumerate(tpl["joint_type"]):
+        qs = tpl["joint_q_start"][k]
+        if jt == SAP_JOINT_FREE:
+            q[:, qs:qs + 3] = np.stack([rng.uniform(-1, 1, worlds), rng.uniform(-1, 1, worlds),
+                                        rng.uniform(0.8, 1.2, worlds)], -1)
+            q[:, qs + 3:qs + 7] = _random_quat(rng, worlds)
+        else:
+            q[:, qs] = rest[qs] + rng.normal(scale=spread, size=worlds)
+    return q
+
+
+def replicate(tpl: dict, worlds: int, rng: np.random.Generator, *, gravity=(0.0, 0.0, -9.81),
+              mu_range=(0.3, 1.0), stiffness=1.0e5, tau_d=0.005) -> dict:
+    """Global (all-worlds) numpy arrays in the reference's layout: equal
+    contiguous per-world blocks of joints, bodies, coordinates and DOFs.  Each
+    body owns one shape; shape index S-1 is a static ground (body -1)."""
+    B, Jw, n, Q = tpl["bodies_per_world"], tpl["joints_per_world"], tpl["dofs_per_world"], tpl["coords_per_world"]
+    E = worlds
+    g = {}
+    off = lambda a, step: (a[None, :] + step * np.arange(E)[:, None]).reshape(-1)
+    g["joint_type"] = np.tile(tpl["joint_type"], E)
+    g["joint_parent"] = np.where(np.tile(tpl["joint_parent"], E) >= 0, off(tpl["joint_parent"], B), -1).astype(np.int32)
+    g["joint_child"] = off(tpl["joint_child"], B).astype(np.int32)
+    g["joint_ancestor"] = np.where(np.tile(tpl["joint_ancestor"], E) >= 0, off(tpl["joint_ancestor"], Jw),
+                                   -1).astype(np.int32)
+    g["joint_articulation"] = np.zeros(E * Jw, np.int32)
+    qs = np.concatenate([off(tpl["joint_q_start"][:-1], Q), [E * Q]]).astype(np.int32)
+    ds = np.concatenate([off(tpl["joint_qd_start"][:-1], n), [E * n]]).astype(np.int32)
+    g["joint_q_start"], g["joint_qd_start"] = qs, ds
+    g["joint_dof_dim"] = np.tile(tpl["joint_dof_dim"], (E, 1))
+    g["joint_axis"] = np.tile(tpl["joint_axis"], (E, 1))
+    g["joint_X_p"] = np.tile(tpl["joint_X_p"], (E, 1))
+    g["joint_X_c"] = np.tile(tpl["joint_X_c"], (E, 1))
+    g["joint_armature"] = np.tile(tpl["joint_armature"], E)
+    arts = tpl["articulation_start"]
+    A_w = len(arts) - 1
+    starts = (arts[:-1][None, :] + Jw * np.arange(E)[:, None]).reshape(-1)
+    g["articulation_start"] = np.concatenate([starts, [E * Jw]]).astype(np.int32)
+    for a in range(E * A_w):
+        g["joint_articulation"][g["articulation_start"][a]:g["articulation_start"][a + 1]] = a
+    g["body_mass"] = np.tile(tpl["body_mass"], E)
+    g["body_inertia"] = np.tile(tpl["body_inertia"], (E, 1, 1))
+    g["body_com"] = np.tile(tpl["body_com"], (E, 1))
+    g["body_world"] = np.repeat(np.arange(E, dtype=np.int32), B)
+    g["gravity"] = np.tile(np.asarray(gravity, np.float64), (E, 1))
+    S = E * B + 1
+    g["shape_body"] = np.concatenate([np.arange(E * B), [-1]]).astype(np.int32)
+    g["shape_material_mu"] = np.concatenate([rng.uniform(*mu_range, E * B), [1.0]])
+    g["shape_material_ke"] = np.full(S, 2.0 * stiffness)  # series combination halves it
+    g["shape_material_tau"] = np.full(S, tau_d)
+    g["counts"] = dict(joints=E * Jw, dofs=E * n, coords=E * Q, bodies=E * B, articulations=E * A_w, worlds=E,
+                       shapes=S)
+    return g
+
+
+def to_model(tpl: dict, g: dict, joint_q: np.ndarray, device) -> SapModel:
+    """SapModel (torch) from the numpy arrays of `replicate`."""
+    c = g["counts"]
+    t64 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=device)
+    t32 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=device)
+    ti = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int32, device=device)
+    D = c["dofs"]
+    return SapModel(
+        device=device, joint_count=c["joints"], joint_dof_count=D, joint_coord_count=c["coords"],
+        body_count=c["bodies"], articulation_count=c["articulations"], world_count=c["worlds"],
+        shape_count=c["shapes"], requires_grad=False,
+        joint_type=ti(g["joint_type"]), joint_articulation=ti(g["joint_articulation"]),
+        joint_parent=ti(g["joint_parent"]), joint_child=ti(g["joint_child"]),
+        joint_q_start=ti(g["joint_q_start"]), joint_qd_start=ti(g["joint_qd_start"]),
+        joint_dof_dim=ti(g["joint_dof_dim"]), joint_axis=t64(g["joint_axis"]), joint_X_p=t64(g["joint_X_p"]),
+        joint_X_c=t64(g["joint_X_c"]), joint_ancestor=ti(g["joint_ancestor"]),
+        articulation_start=ti(g["articulation_start"]), joint_q=t64(joint_q.reshape(-1)),
+        joint_qd=torch.zeros(D, dtype=torch.float64, device=device),
+        body_q=torch.zeros(c["bodies"], 7, dtype=torch.float64, device=device),
+        body_qd=torch.zeros(c["bodies"], 6, dtype=torch.float64, device=device),
+        body_mass=t64(g["body_mass"]), body_inertia=t64(g["body_inertia"]), body_com=t64(g["body_com"]),
+        body_flags=torch.ones(c["bodies"], dtype=torch.int32, device=device), body_world=ti(g["body_world"]),
+        gravity=t64(g["gravity"]), joint_armature=t64(g["joint_armature"]), shape_body=ti(g["shape_body"]),
+        shape_material_mu=t64(g["shape_material_mu"]), shape_material_ke=t64(g["shape_material_ke"]),
+        shape_material_tau=t64(g["shape_material_tau"]),
+        joint_target_mode=torch.zeros(D, dtype=torch.int32, device=device),
+        joint_target_ke=torch.zeros(D, dtype=torch.float32, device=device),
+        joint_target_kd=torch.zeros(D, dtype=torch.float32, device=device),
+        joint_target_pos=torch.zeros(D, dtype=torch.float32, device=device),
+        joint_target_vel=torch.zeros(D, dtype=torch.float32, device=device),
+        joint_f=torch.zeros(D, dtype=torch.float64, device=device),
+        joint_act=torch.zeros(D, dtype=torch.float32, device=device),
+        joint_effort_limit=torch.zeros(D, dtype=torch.float32, device=device),
+        joint_limit_lower=torch.full((D,), -np.inf, dtype=torch.float64, device=device),
+        joint_limit_upper=torch.full((D,), np.inf, dtype=torch.float64, device=device),
+        joint_limit_ke=torch.zeros(D, dtype=torch.float64, device=device),
+        joint_limit_kd=torch.zeros(D, dtype=torch.float64, device=device),
+    )
+
+
+def _qrot(q, v):
+    qv = q[..., :3]
+    t = 2.0 * np.cross(qv, v)
+    return v + q[..., 3:4] * t + np.cross(qv, t)
+
+
+def ground_contacts(rng: np.random.Generator, body_pos: np.ndarray, body_quat: np.ndarray, per_world, *,
+                    bodies_from: int = 0, phi0_range=(-2e-3, 0.0), tilt: float = 0.1, shuffle: bool = True,
+                    capacity: int | None = None) -> dict:
+    """Flat contact buffer of body-vs-ground contacts.  body_pos (E,B,3),
+    body_quat (E,B,4) are the body poses of the step's start state;
+    per_world: int or (E,) counts.  shape0 = ground (static), shape1 = the
+    body's shape, point1 in the body frame, point0 in world (its shape is
+    static), normal ~ +z from ground to body, (x1 - x0).n = phi0."""
+    E, B = body_pos.shape[:2]
+    counts = np.broadcast_to(np.asarray(per_world), (E,)).astype(np.int64)
+    N = int(counts.sum())
+    world = np.repeat(np.arange(E), counts)
+    body = rng.integers(bodies_from, B, size=N)
+    r_local = rng.normal(size=(N, 3))
+    r_local *= (rng.uniform(0.0, 0.05, size=N) / np.linalg.norm(r_local, axis=1))[:, None]
+    q = body_quat[world, body]
+    q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    x1 = body_pos[world, body] + _qrot(q, r_local)
+    nrm = np.array([0.0, 0.0, 1.0]) + rng.normal(scale=tilt, size=(N, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    phi0 = rng.uniform(*phi0_range, size=N)
+    x0 = x1 - phi0[:, None] * nrm
+    order = rng.permutation(N) if shuffle else np.arange(N)
+    cap = max(capacity or N, N)
+    def pad(a, fill=0):
+        out = np.full((cap,) + a.shape[1:], fill, dtype=a.dtype)
+        out[:N] = a[order]
+        return out
+    ground_shape = E * B
+    return dict(
+        count=np.array([N], np.int32),
+        shape0=pad(np.full(N, ground_shape, np.int32), -1),
+        shape1=pad((world * B + body).astype(np.int32), -1),
+        point0=pad(x0.astype(np.float32)), point1=pad(r_local.astype(np.float32)),
+        normal=pad(nrm.astype(np.float32)),
+        margin0=pad(np.zeros(N, np.float32)), margin1=pad(np.zeros(N, np.float32)),
+        point0d=pad(x0), point1d=pad(r_local), normald=pad(nrm),
+        margin0d=pad(np.zeros(N)), margin1d=pad(np.zeros(N)),
+    )
+
+
+def contacts_to_torch(c: dict, device, *, with_f64: bool = True) -> SapContacts:
+    t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=device)
+    kw = dict(
+        rigid_contact_count=t(c["count"], torch.int32), rigid_contact_shape0=t(c["shape0"], torch.int32),
+        rigid_contact_shape1=t(c["shape1"], torch.int32), rigid_contact_point0=t(c["point0"], torch.float32),
+        rigid_contact_point1=t(c["point1"], torch.float32), rigid_contact_normal=t(c["normal"], torch.float32),
+        rigid_contact_margin0=t(c["margin0"], torch.float32), rigid_contact_margin1=t(c["margin1"], torch.float32),
+    )
+    if with_f64:
+        kw.update(rigid_contact_point0d=t(c["point0d"], torch.float64),
+                  rigid_contact_point1d=t(c["point1d"], torch.float64),
+                  rigid_contact_normald=t(c["normald"], torch.float64),
+                  rigid_contact_margin0d=t(c["margin0d"], torch.float64),
+                  rigid_contact_margin1d=t(c["margin1d"], torch.float64))
+    return SapContacts(**kw)

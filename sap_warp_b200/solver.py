@@ -1,0 +1,741 @@
+"""Drop-in SAP step API: SolverSAP and its components, mirroring
+sim/solver_sap.py, sim/free_motion.py, sim/contact_jacobian.py and
+sim/contact_solve.py of the reference (constructor keywords, presets,
+result dataclasses, errors), running on the native library only.
+
+Every buffer is allocated in the constructors; `step` / `compute` / `solve`
+only launch kernels on the current torch stream (no host synchronisation,
+no allocation), so a whole step can be captured in a CUDA graph.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import warnings
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._lib import check, load
+from ._solve import F32, F64, I32, normalize_sap_line_search_mode
+from .runtime import (
+    SAP_JOINT_D6,
+    SAP_JOINT_DISTANCE,
+    SAP_JOINT_FREE,
+    SAP_JOINT_PRISMATIC,
+    SAP_JOINT_REVOLUTE,
+    SAP_JOINT_TARGET_NONE,
+    SapContacts,
+    SapControl,
+    SapModel,
+    SapState,
+    sap_contacts_from_newton,
+)
+
+SAP_CONTACT_PRESET_VARIANTS = ("approx32", "approx64", "drake")
+
+# sim/solver_sap.py:75-106
+_CONTACT_PRESET_KWARGS = {
+    "approx32": dict(use_f64_boundary_pose=False, free_motion_solve_precision="fp32", contact_solve_precision="fp64",
+                     contact_linear_solve_precision="fp32", sap_contact_weight_precision="fp32",
+                     contact_weight_mode="body_inertia", contact_point_mode="witness_point",
+                     position_integration="midpoint"),
+    "approx64": dict(use_f64_boundary_pose=True, free_motion_solve_precision="fp64", contact_solve_precision="fp64",
+                     contact_linear_solve_precision="fp64", sap_contact_weight_precision="fp64",
+                     contact_weight_mode="body_inertia", contact_point_mode="witness_point",
+                     position_integration="midpoint"),
+    "drake": dict(use_f64_boundary_pose=True, free_motion_solve_precision="fp64", contact_solve_precision="fp64",
+                  contact_linear_solve_precision="fp64", sap_contact_weight_precision="fp64",
+                  contact_weight_mode="diag_delassus", contact_point_mode="contact_midpoint",
+                  position_integration="sap_euler"),
+}
+
+
+def _normalize_precision_knob(value: str, *, option_name: str) -> str:
+    """sim/solver_sap.py:62-70"""
+    p = str(value).strip().lower()
+    p = {"f32": "fp32", "f64": "fp64"}.get(p, p)
+    if p not in ("fp32", "fp64"):
+        raise ValueError(f"{option_name} must be 'fp32'/'f32' or 'fp64'/'f64', got {value!r}.")
+    return p
+
+
+def _normalize_contact_preset_variant(value: str | None) -> str:
+    """sim/solver_sap.py:109-120"""
+    if value is None:
+        return "approx32"
+    v = str(value).strip().lower().replace("-", "_")
+    v = {"approx_32": "approx32", "approx_64": "approx64"}.get(v, v)
+    if v not in _CONTACT_PRESET_KWARGS:
+        raise ValueError(f"contact_preset_variant must be one of {', '.join(SAP_CONTACT_PRESET_VARIANTS)}, "
+                         f"got {value!r}.")
+    return v
+
+
+def _ptr(t: torch.Tensor | None) -> int:
+    return 0 if t is None else t.data_ptr()
+
+
+def _f64(t: torch.Tensor) -> torch.Tensor:
+    return t if t.dtype == F64 and t.is_contiguous() else t.to(F64).contiguous()
+
+
+class _ModelView:
+    """Per-world sizes, host maps and the sapb_model_desc of a SapModel."""
+
+    def __init__(self, model: SapModel):
+        if not isinstance(model, SapModel):
+            raise TypeError("SolverSAP requires SapModel; convert frontend data before constructing the solver.")
+        W = max(int(model.world_count), 1)
+        J, B, D, Q = int(model.joint_count), int(model.body_count), int(model.joint_dof_count), int(
+            model.joint_coord_count)
+        if J <= 0 or D <= 0:
+            raise ValueError("SolverSAP requires a model with articulated joint DOFs.")
+        if J % W or B % W or D % W or Q % W or int(model.articulation_count) % W:
+            raise ValueError("SolverSAP requires contiguous equal-sized per-world joint/body/dof/coord blocks "
+                             f"(worlds={W}, joints={J}, bodies={B}, dofs={D}, coords={Q}).")
+        self.model = model
+        self.W, self.Jw, self.Bw, self.n, self.Qw = W, J // W, B // W, D // W, Q // W
+        self.Aw = int(model.articulation_count) // W
+        jt = model.joint_type.cpu().numpy()
+        if np.any(jt == SAP_JOINT_D6):
+            raise NotImplementedError("D6 joints are not supported by the native free motion.")
+        parent_joint = model.joint_ancestor.cpu().numpy()
+        if np.any(parent_joint >= np.arange(J)):
+            raise ValueError("joints must be ordered parents before children")
+        self.device = model.joint_type.device
+        d = _abi.ModelDesc()
+        d.num_worlds, d.joints_per_world, d.bodies_per_world = W, self.Jw, self.Bw
+        d.dofs_per_world, d.coords_per_world, d.articulations_per_world = self.n, self.Qw, self.Aw
+        d.num_shapes = int(model.shape_body.numel()) if model.shape_body is not None else 0
+        self._keep = {}
+
+        def k(name, t, dtype):
+            t = t.to(dtype).contiguous()
+            self._keep[name] = t
+            return t.data_ptr()
+
+        for name in ("joint_type", "joint_parent", "joint_child", "joint_ancestor", "joint_q_start",
+                     "joint_qd_start", "articulation_start"):
+            setattr(d, name, k(name, getattr(model, name), I32))
+        d.joint_dof_dim = k("joint_dof_dim", model.joint_dof_dim.reshape(-1), I32)
+        for name in ("joint_axis", "joint_X_p", "joint_X_c", "joint_armature", "body_mass", "body_inertia",
+                     "body_com", "gravity"):
+            setattr(d, name, k(name, getattr(model, name).reshape(-1), F64))
+        if d.num_shapes:
+            d.shape_body = k("shape_body", model.shape_body, I32)
+            for name in ("shape_material_mu", "shape_material_ke", "shape_material_tau"):
+                t = getattr(model, name)
+                setattr(d, name, k(name, t, F64) if t is not None else 0)
+        self.desc = d
+        self._build_dof_maps(jt)
+
+    def _build_dof_maps(self, jt):
+        """sim/contact_solve.py:3681-3758: DOF -> coordinate, drive target and
+        limit support; body -> articulation DOF range (world-local)."""
+        m = self.model
+        D = int(m.joint_dof_count)
+        qs = m.joint_q_start.cpu().numpy()
+        ds = m.joint_qd_start.cpu().numpy()
+        dim = m.joint_dof_dim.cpu().numpy().reshape(-1, 2)
+        coord = np.full(D, -1, np.int32)
+        target = np.arange(D, dtype=np.int32)
+        limit_ok = np.zeros(D, np.int32)
+        for j, t in enumerate(jt):
+            d0 = int(ds[j])
+            if t in (SAP_JOINT_FREE, SAP_JOINT_DISTANCE):
+                for a in range(3):
+                    target[d0 + a] = d0 + a + 3
+                    target[d0 + a + 3] = d0 + a
+            if t not in (SAP_JOINT_PRISMATIC, SAP_JOINT_REVOLUTE, SAP_JOINT_D6):
+                continue
+            cnt = int(dim[j].sum())
+            for a in range(cnt):
+                coord[d0 + a] = int(qs[j]) + a
+                if cnt == 1:
+                    limit_ok[d0 + a] = 1
+        child = m.joint_child.cpu().numpy()
+        art = m.articulation_start.cpu().numpy()
+        B = int(m.body_count)
+        bstart = np.full(B, -1, np.int32)
+        bcount = np.zeros(B, np.int32)
+        for a in range(len(art) - 1):
+            js = range(int(art[a]), int(art[a + 1]))
+            counts = [int(dim[j].sum()) for j in js]
+            starts = [int(ds[j]) for j, c in zip(js, counts) if c > 0]
+            tot = sum(counts)
+            if not starts or tot <= 0:
+                continue
+            s0 = min(starts)
+            for j in js:
+                b = int(child[j])
+                if 0 <= b < B:
+                    env = b // self.Bw
+                    bstart[b] = s0 - env * self.n
+                    bcount[b] = tot
+        dev = self.device
+        self.dof_coord_index = torch.as_tensor(coord, device=dev)
+        self.dof_target_index = torch.as_tensor(target, device=dev)
+        self.limit_supported = torch.as_tensor(limit_ok, device=dev)
+        self.body_dof_start = torch.as_tensor(bstart, device=dev)
+        self.body_dof_count = torch.as_tensor(bcount, device=dev)
+        mode = m.joint_target_mode.cpu().numpy()
+        ke = m.joint_target_ke.cpu().numpy()
+        kd = m.joint_target_kd.cpu().numpy()
+        self.has_pd = bool(np.any((mode != SAP_JOINT_TARGET_NONE) & ((ke > 0) | (kd > 0))))
+        lo = m.joint_limit_lower.cpu().numpy()
+        hi = m.joint_limit_upper.cpu().numpy()
+        lke = m.joint_limit_ke.cpu().numpy()
+        self.has_limits = bool(np.any((limit_ok != 0) & (lke > 0) & (np.isfinite(lo) | np.isfinite(hi))))
+
+
+@dataclass(frozen=True)
+class SapFreeMotionResult:
+    """sim/free_motion.py:63-68"""
+
+    v_star: torch.Tensor
+    vdot: torch.Tensor
+    dynamics_matrix: torch.Tensor | None
+
+
+@dataclass(frozen=True)
+class SapContactJacobianResult:
+    """Views into buffers owned by SapContactJacobian (sim/contact_jacobian.py:51-84)."""
+
+    contact_count: int
+    truncated_contact_count: int
+    contact_env_count: torch.Tensor
+    contact_env_phi0: torch.Tensor
+    contact_env_jacobian: torch.Tensor
+    contact_env_w_eff: torch.Tensor
+    contact_env_mu: torch.Tensor
+    contact_env_stiffness: torch.Tensor
+    contact_env_R_WC: torch.Tensor
+    contact_env_point: torch.Tensor
+    contact_env_witness0: torch.Tensor | None
+    contact_env_witness1: torch.Tensor | None
+    contact_env_body0: torch.Tensor
+    contact_env_body1: torch.Tensor
+    body_jacobian_local: torch.Tensor | None
+    dynamics_matrix_env: torch.Tensor
+    contact_env_tau_d: torch.Tensor | None = None
+
+
+@dataclass(frozen=True)
+class SapContactSolveResult:
+    """Views into buffers owned by SapContactSolve (sim/contact_solve.py:188-232)."""
+
+    v_env: torch.Tensor
+    v_flat: torch.Tensor
+    cost: torch.Tensor
+    contact_gamma: torch.Tensor
+    contact_mode: torch.Tensor
+    newton_iterations_env: torch.Tensor
+    line_search_iterations_env: torch.Tensor
+    converged_env: torch.Tensor
+    line_search_status_env: torch.Tensor
+    grad_norm_env: torch.Tensor
+    iterations: int
+    line_search_iterations: int
+    converged: bool
+
+
+class SapContactJacobian:
+    """Free motion + contact Jacobian of every world in two launches
+    (SapContactJacobian, sim/contact_jacobian.py:1242-1985, which owns the
+    SapFreeMotion of sim/free_motion.py)."""
+
+    def __init__(self, model: SapModel, *, max_rigid_contact: int = 128, fallback_mu: float | None = None,
+                 fallback_stiffness: float = 1.0e10, fallback_tau_d: float = 0.1,
+                 contact_weight_mode: str = "diag_delassus", contact_point_mode: str = "contact_midpoint",
+                 capture_local_snapshots: bool = False, use_f64_boundary_pose: bool = True,
+                 free_motion_solve_precision: str = "fp64", sap_contact_weight_precision: str = "fp64",
+                 _view: _ModelView | None = None):
+        self.view = _view or _ModelView(model)
+        v = self.view
+        self.model = model
+        self.max_rigid_contact = max(int(max_rigid_contact), 1)
+        wm = str(contact_weight_mode).strip().lower()
+        if wm not in ("body_inertia", "diag_delassus"):
+            raise ValueError(f"contact_weight_mode must be 'body_inertia' or 'diag_delassus', got {contact_weight_mode!r}")
+        pm = str(contact_point_mode).strip().lower()
+        if pm not in ("witness_point", "contact_midpoint"):
+            raise ValueError(f"contact_point_mode must be 'witness_point' or 'contact_midpoint', got {contact_point_mode!r}")
+        self.contact_weight_mode, self.contact_point_mode = wm, pm
+        if fallback_mu is None:  # _infer_contact_mu_fallback (sim/sap_helpers.py:40-45)
+            mu = model.shape_material_mu.cpu().numpy() if model.shape_material_mu is not None else np.zeros(0)
+            pos = mu[mu > 0.0]
+            fallback_mu = float(pos.min()) if pos.size else 0.1
+        self.opts = _abi.PrepareOptions()
+        self.opts.max_contacts = self.max_rigid_contact
+        self.opts.contact_weight_mode = (_abi.SAPB_WEIGHT_DIAG_DELASSUS if wm == "diag_delassus"
+                                         else _abi.SAPB_WEIGHT_BODY_INERTIA)
+        self.opts.contact_point_mode = _abi.SAPB_POINT_MIDPOINT if pm == "contact_midpoint" else _abi.SAPB_POINT_WITNESS
+        self.opts.fallback_mu = float(fallback_mu)
+        self.opts.fallback_stiffness = float(fallback_stiffness)
+        self.opts.fallback_tau_d = float(fallback_tau_d)
+        W, n, C, dev = v.W, v.n, self.max_rigid_contact, v.device
+        z = lambda *s, dt=F64: torch.zeros(*s, dtype=dt, device=dev)
+        self.v_star = z(W * n)
+        self.vdot = z(W * n)
+        self.dynamics_matrix_env = z(W, n, n)
+        self.contact_env_jacobian = z(W, C, 3, n)
+        self.contact_env_count = z(W, dt=I32)
+        self.contact_env_phi0 = z(W, C)
+        self.contact_env_w_eff = z(W, C)
+        self.contact_env_mu = z(W, C)
+        self.contact_env_stiffness = z(W, C)
+        self.contact_env_tau_d = z(W, C)
+        self.contact_env_body0 = torch.full((W, C), -1, dtype=I32, device=dev)
+        self.contact_env_body1 = torch.full((W, C), -1, dtype=I32, device=dev)
+        self.contact_env_point = z(W, C, 3)
+        self.contact_env_R_WC = z(W, C, 3, 3)
+        self.truncated = z(1, dt=I32)
+        self.body_q_sap = z(v.W * v.Bw, 7)
+        self.dt_world = z(W)
+        ws = int(load().sapb_prepare_workspace_size(ctypes.byref(v.desc), C))
+        self.workspace = torch.zeros(max(ws, 16), dtype=torch.uint8, device=dev)
+        self._contact_f64 = None
+        o = _abi.PrepareOutputs()
+        o.v_star, o.vdot, o.dynamics_matrix = _ptr(self.v_star), _ptr(self.vdot), _ptr(self.dynamics_matrix_env)
+        o.jacobian, o.contact_count = _ptr(self.contact_env_jacobian), _ptr(self.contact_env_count)
+        o.phi0, o.w_eff, o.mu = _ptr(self.contact_env_phi0), _ptr(self.contact_env_w_eff), _ptr(self.contact_env_mu)
+        o.stiffness, o.tau_d = _ptr(self.contact_env_stiffness), _ptr(self.contact_env_tau_d)
+        o.body0, o.body1 = _ptr(self.contact_env_body0), _ptr(self.contact_env_body1)
+        o.point, o.frame = _ptr(self.contact_env_point), _ptr(self.contact_env_R_WC)
+        o.truncated_count, o.body_q = _ptr(self.truncated), _ptr(self.body_q_sap)
+        self.outputs = o
+
+    def set_dt(self, dt) -> None:
+        """Per-world time step (scalar or [W] tensor), sim/solver_sap.py:975-992."""
+        if isinstance(dt, torch.Tensor):
+            if dt.numel() != self.view.W:
+                raise ValueError(f"per-world dt length {dt.numel()} != num_envs {self.view.W}")
+            self.dt_world.copy_(dt.reshape(-1))
+        else:
+            self.dt_world.fill_(float(dt))
+
+    def _contact_arrays(self, contacts: SapContacts):
+        if contacts is None or contacts.rigid_contact_count is None:
+            return None
+        if contacts.has_f64_rigid_contacts:
+            return (contacts.rigid_contact_point0d, contacts.rigid_contact_point1d, contacts.rigid_contact_normald,
+                    contacts.rigid_contact_margin0d, contacts.rigid_contact_margin1d)
+        N = int(contacts.rigid_contact_shape0.numel())
+        if self._contact_f64 is None or self._contact_f64[0].shape[0] != N:
+            dev = self.view.device
+            self._contact_f64 = [torch.zeros(N, 3, dtype=F64, device=dev), torch.zeros(N, 3, dtype=F64, device=dev),
+                                 torch.zeros(N, 3, dtype=F64, device=dev), torch.zeros(N, dtype=F64, device=dev),
+                                 torch.zeros(N, dtype=F64, device=dev)]
+        srcs = (contacts.rigid_contact_point0, contacts.rigid_contact_point1, contacts.rigid_contact_normal,
+                contacts.rigid_contact_margin0, contacts.rigid_contact_margin1)
+        for dst, src in zip(self._contact_f64, srcs):
+            if src is None:
+                dst.zero_()
+            else:
+                dst.copy_(src.reshape(dst.shape))
+        return tuple(self._contact_f64)
+
+    def compute(self, state: SapState, contacts: SapContacts, *, control: SapControl | None = None, dt=None):
+        """Free motion and contact rows for `state` and the flat `contacts`."""
+        if not isinstance(state, SapState):
+            raise TypeError("SapContactJacobian.compute requires SapState.")
+        if getattr(state, "joint_qd_order", "sap") != "sap" or (control is not None and
+                                                                getattr(control, "joint_f_order", "sap") != "sap"):
+            raise NotImplementedError("public-order boundary conversion is not supported; pass SAP-order arrays.")
+        if dt is not None:
+            self.set_dt(dt)
+        self._q = _f64(state.joint_q)
+        self._qd = _f64(state.joint_qd)
+        jf = _f64(control.joint_f) if control is not None and control.joint_f is not None else None
+        bf = _f64(state.body_f.reshape(-1, 6)) if state.body_f is not None else None
+        inp = _abi.StepInputs()
+        inp.joint_q, inp.joint_qd, inp.joint_f, inp.body_f = _ptr(self._q), _ptr(self._qd), _ptr(jf), _ptr(bf)
+        inp.dt = _ptr(self.dt_world)
+        arrays = self._contact_arrays(contacts)
+        if arrays is not None:
+            inp.contact_capacity = int(contacts.rigid_contact_shape0.numel())
+            inp.contact_count = _ptr(contacts.rigid_contact_count)
+            inp.contact_shape0 = _ptr(contacts.rigid_contact_shape0)
+            inp.contact_shape1 = _ptr(contacts.rigid_contact_shape1)
+            inp.contact_point0, inp.contact_point1, inp.contact_normal = (_ptr(a) for a in arrays[:3])
+            inp.contact_margin0, inp.contact_margin1 = _ptr(arrays[3]), _ptr(arrays[4])
+        self._inputs = inp
+        status = load().sapb_free_motion_contacts(ctypes.byref(self.view.desc), ctypes.byref(inp),
+                                                  ctypes.byref(self.opts), ctypes.byref(self.outputs),
+                                                  self.workspace.data_ptr(), self.workspace.numel(),
+                                                  ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream))
+        check(status, "sapb_free_motion_contacts")
+        return self.result()
+
+    def result(self) -> SapContactJacobianResult:
+        return SapContactJacobianResult(
+            contact_count=-1, truncated_contact_count=-1,  # device counters; read without a host sync
+            contact_env_count=self.contact_env_count, contact_env_phi0=self.contact_env_phi0,
+            contact_env_jacobian=self.contact_env_jacobian, contact_env_w_eff=self.contact_env_w_eff,
+            contact_env_mu=self.contact_env_mu, contact_env_stiffness=self.contact_env_stiffness,
+            contact_env_R_WC=self.contact_env_R_WC, contact_env_point=self.contact_env_point,
+            contact_env_witness0=None, contact_env_witness1=None, contact_env_body0=self.contact_env_body0,
+            contact_env_body1=self.contact_env_body1, body_jacobian_local=None,
+            dynamics_matrix_env=self.dynamics_matrix_env, contact_env_tau_d=self.contact_env_tau_d)
+
+    @property
+    def free_motion_result(self) -> SapFreeMotionResult:
+        return SapFreeMotionResult(v_star=self.v_star, vdot=self.vdot, dynamics_matrix=None)
+
+
+class SapFreeMotion:
+    """SapFreeMotion.compute (sim/free_motion.py:2180-2208): v* and vdot in
+    SAP order.  Runs the same fused launch as SapContactJacobian with no
+    contacts."""
+
+    def __init__(self, model: SapModel, **kwargs):
+        self._cj = SapContactJacobian(model, max_rigid_contact=1, **kwargs)
+
+    def compute(self, state: SapState, control: SapControl | None, dt, *, assemble_dynamics_matrix: bool = False):
+        if control is None or not isinstance(control, SapControl):
+            raise TypeError("SapFreeMotion.compute requires SapControl; convert before entering SAP components.")
+        self._cj.compute(state, SapContacts(), control=control, dt=dt)
+        r = self._cj.free_motion_result
+        if assemble_dynamics_matrix:
+            W, n = self._cj.view.W, self._cj.view.n
+            A = torch.zeros(W * n, W * n, dtype=F64, device=self._cj.view.device)
+            for e in range(W):
+                A[e * n:(e + 1) * n, e * n:(e + 1) * n] = self._cj.dynamics_matrix_env[e]
+            return SapFreeMotionResult(r.v_star, r.vdot, A)
+        return r
+
+
+class SapContactSolve:
+    """Stage-2 Newton solve (sim/contact_solve.py:3291-6341) in one launch."""
+
+    def __init__(self, model: SapModel, *, max_rigid_contact: int = 128, contact_beta: float = 1.0,
+                 contact_sigma: float = 1.0e-3, contact_tau_d: float = 0.1, block_size: int | None = None,
+                 diag_shift: float = 0.0, contact_assembly_tile_size: int = 256, solve_precision: str = "fp64",
+                 linear_solve_precision: str = "fp64", hessian_precision: str | None = None,
+                 _view: _ModelView | None = None):
+        self.view = _view or _ModelView(model)
+        v = self.view
+        if v.n > 60:
+            raise NotImplementedError(f"the on-chip solve supports up to 60 DOFs per world, got {v.n}")
+        self.model = model
+        self.max_rigid_contact = max(int(max_rigid_contact), 1)
+        self.contact_beta, self.contact_sigma = float(contact_beta), float(contact_sigma)
+        self.contact_tau_d, self.diag_shift = float(contact_tau_d), float(diag_shift)
+        self.solve_precision = _normalize_precision_knob(solve_precision, option_name="solve_precision")
+        if self.solve_precision != "fp64":
+            raise NotImplementedError("the contact objective is always evaluated in fp64")
+        self.linear_solve_precision = _normalize_precision_knob(linear_solve_precision,
+                                                                option_name="linear_solve_precision")
+        self.hessian_precision = _normalize_precision_knob(hessian_precision or self.linear_solve_precision,
+                                                           option_name="hessian_precision")
+        W, n, C, dev = v.W, v.n, self.max_rigid_contact, v.device
+        z = lambda *s, dt=F64: torch.zeros(*s, dtype=dt, device=dev)
+        self.v_flat = z(W * n)
+        self.v_env = self.v_flat.view(W, n)
+        self.contact_gamma = z(W, C, 3)
+        self.contact_mode = z(W, C, dt=I32)
+        self.cost = z(W)
+        self.newton_iterations_env = z(W, dt=I32)
+        self.ls_iterations_total = z(W, dt=I32)
+        self.converged_env = z(W, dt=I32)
+        self.ls_status = z(W, dt=I32)
+        self.grad_norm = z(W)
+        self.dt_world = z(W)
+        ws = int(load().sapb_contact_solve_workspace_size(W, n, C))
+        self.workspace = torch.zeros(max(ws, 16), dtype=torch.uint8, device=dev)
+        self.zero_f32 = z(W * n, dt=F32)
+        out = _abi.SolveOutputs()
+        out.v, out.contact_gamma, out.contact_mode = _ptr(self.v_flat), _ptr(self.contact_gamma), _ptr(self.contact_mode)
+        out.cost, out.newton_iterations = _ptr(self.cost), _ptr(self.newton_iterations_env)
+        out.line_search_iterations, out.converged = _ptr(self.ls_iterations_total), _ptr(self.converged_env)
+        out.status, out.grad_norm = _ptr(self.ls_status), _ptr(self.grad_norm)
+        self.outputs = out
+        self.dof = None
+        if v.has_pd or v.has_limits:
+            m = model
+            self.dof = _abi.DofTerms()
+            self.dof.has_pd, self.dof.has_limits = int(v.has_pd), int(v.has_limits)
+            self.dof.joint_coord_count = int(m.joint_coord_count)
+            self._dof_keep = dict(
+                dof_coord_index=v.dof_coord_index, dof_target_index=v.dof_target_index,
+                limit_supported=v.limit_supported, joint_target_mode=m.joint_target_mode.to(I32).contiguous(),
+                joint_target_ke=m.joint_target_ke.to(F32).contiguous(),
+                joint_target_kd=m.joint_target_kd.to(F32).contiguous(),
+                joint_effort_limit=m.joint_effort_limit.to(F32).contiguous(),
+                joint_limit_lower=_f64(m.joint_limit_lower), joint_limit_upper=_f64(m.joint_limit_upper),
+                joint_limit_ke=_f64(m.joint_limit_ke), joint_limit_kd=_f64(m.joint_limit_kd))
+            for k, t in self._dof_keep.items():
+                setattr(self.dof, k, t.data_ptr())
+
+    def options(self, line_search_variant, **kw) -> _abi.SolveOptions:
+        from ._solve import make_options
+
+        return make_options(line_search_variant, contact_beta=self.contact_beta, contact_sigma=self.contact_sigma,
+                            contact_tau_d=self.contact_tau_d, diag_shift=self.diag_shift,
+                            linear_solve_precision=self.linear_solve_precision,
+                            hessian_precision=self.hessian_precision, **kw)
+
+    def solve(self, contact_result: SapContactJacobianResult, state: SapState, control: SapControl | None, dt,
+              v_star: torch.Tensor, *, v0: torch.Tensor | None = None, v_guess: torch.Tensor | None = None,
+              v_guess_active: torch.Tensor | None = None, max_iterations: int = 100,
+              optimality_abs_tol: float = 1.0e-14, optimality_rel_tol: float = 1.0e-6,
+              cost_abs_tol: float | None = None, cost_rel_tol: float | None = None,
+              line_search_max_iterations: int = 40, armijo_c: float = 1.0e-4, rho: float = 0.8,
+              line_search_relative_slop: float | None = None, line_search_variant: str = "monotone_decay",
+              collect_iteration_stats: bool = True, check_line_search_errors: bool = True,
+              graph_conditional: bool = True, static_loop: bool = False) -> SapContactSolveResult:
+        """sim/contact_solve.py:6129-6285"""
+        variant = normalize_sap_line_search_mode(line_search_variant)
+        if not bool(graph_conditional):
+            raise ValueError("SapContactSolve only supports graph_conditional=True; "
+                             "the Python Newton-loop fallback has been removed.")
+        if variant == "armijo_decay" and not (0.0 < float(rho) < 1.0):
+            raise ValueError(f"rho must lie in (0, 1), got {rho!r}.")
+        if variant == "exact_root" and int(line_search_max_iterations) == 40:
+            line_search_max_iterations = 100
+        if cost_abs_tol is None:
+            cost_abs_tol = 0.0 if variant == "monotone_decay" else 1.0e-30
+        if cost_rel_tol is None:
+            cost_rel_tol = 5.0e-3 if variant == "monotone_decay" else 1.0e-15
+        if line_search_relative_slop is None:
+            line_search_relative_slop = 1000.0 * np.finfo(np.float64).eps
+        if isinstance(dt, torch.Tensor):
+            self.dt_world.copy_(dt.reshape(-1))
+        else:
+            self.dt_world.fill_(float(dt))
+        if v0 is None:
+            v0 = v_guess if v_guess is not None else v_star
+        opts = self.options(variant, max_iterations=int(max_iterations), optimality_abs_tol=float(optimality_abs_tol),
+                            optimality_rel_tol=float(optimality_rel_tol), cost_abs_tol=float(cost_abs_tol),
+                            cost_rel_tol=float(cost_rel_tol),
+                            line_search_max_iterations=int(line_search_max_iterations), armijo_c=float(armijo_c),
+                            rho=float(rho), line_search_relative_slop=float(line_search_relative_slop))
+        v = self.view
+        W, n, C = v.W, v.n, self.max_rigid_contact
+        P = _abi.ContactProblem()
+        P.num_envs, P.dof_per_env, P.max_contacts = W, n, int(contact_result.contact_env_jacobian.shape[1])
+        P.num_bodies = int(v.body_dof_start.numel())
+        r = contact_result
+        P.contact_count, P.dynamics_matrix = _ptr(r.contact_env_count), _ptr(r.dynamics_matrix_env)
+        P.jacobian, P.phi0, P.w_eff = _ptr(r.contact_env_jacobian), _ptr(r.contact_env_phi0), _ptr(r.contact_env_w_eff)
+        P.mu, P.stiffness, P.tau_d = _ptr(r.contact_env_mu), _ptr(r.contact_env_stiffness), _ptr(r.contact_env_tau_d)
+        P.body0, P.body1 = _ptr(r.contact_env_body0), _ptr(r.contact_env_body1)
+        P.body_dof_start, P.body_dof_count = _ptr(v.body_dof_start), _ptr(v.body_dof_count)
+        self._vs, self._v0 = _f64(v_star), _f64(v0)
+        P.v_star, P.v0, P.dt = _ptr(self._vs), _ptr(self._v0), _ptr(self.dt_world)
+        if v_guess is not None:
+            if v_guess.dtype != F64 or not v_guess.is_contiguous():
+                raise TypeError("v_guess must be a contiguous float64 tensor (it is written back)")
+            P.v_guess = _ptr(v_guess)
+            P.v_guess_active = _ptr(v_guess_active)
+        if self.dof is not None:
+            self._jq = _f64(state.joint_q)
+            self.dof.joint_q = _ptr(self._jq)
+            for name, t in (("joint_target_pos", getattr(control, "joint_target_pos", None)),
+                            ("joint_target_vel", getattr(control, "joint_target_vel", None)),
+                            ("joint_act", getattr(control, "joint_act", None))):
+                tt = t.to(F32).contiguous() if t is not None else None
+                self._dof_keep["_" + name] = tt
+                setattr(self.dof, name, _ptr(tt))
+            P.dof = ctypes.pointer(self.dof)
+        status = load().sapb_contact_solve(ctypes.byref(P), ctypes.byref(opts), ctypes.byref(self.outputs),
+                                           self.workspace.data_ptr(), self.workspace.numel(),
+                                           ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream))
+        check(status, "sapb_contact_solve")
+        return self.result()
+
+    def result(self) -> SapContactSolveResult:
+        return SapContactSolveResult(
+            v_env=self.v_env, v_flat=self.v_flat, cost=self.cost, contact_gamma=self.contact_gamma,
+            contact_mode=self.contact_mode, newton_iterations_env=self.newton_iterations_env,
+            line_search_iterations_env=self.ls_iterations_total, converged_env=self.converged_env,
+            line_search_status_env=self.ls_status, grad_norm_env=self.grad_norm,
+            iterations=-1, line_search_iterations=-1, converged=True)
+
+
+class SolverSAP:
+    """SAP timestepper (sim/solver_sap.py:736-1512): free motion and contact
+    Jacobian, the stage-2 solve and position integration, three native
+    launches per step (plus small memsets)."""
+
+    def __init__(self, model: SapModel, *, max_rigid_contact: int = 128, fallback_mu: float | None = None,
+                 fallback_stiffness: float = 1.0e10, contact_beta: float = 1.0, contact_sigma: float = 1.0e-3,
+                 contact_tau_d: float | None = None, block_size: int | None = None, diag_shift: float = 0.0,
+                 max_iterations: int = 100, optimality_abs_tol: float = 1.0e-14, optimality_rel_tol: float = 1.0e-6,
+                 cost_abs_tol: float | None = None, cost_rel_tol: float | None = None,
+                 line_search_max_iterations: int = 40, armijo_c: float = 1.0e-4, rho: float = 0.8,
+                 line_search_relative_slop: float | None = None, line_search_variant: str = "armijo_decay",
+                 contact_preset_variant: str | None = None, contact_weight_mode: str | None = None,
+                 contact_point_mode: str | None = None, capture_contact_jacobian_snapshots: bool = False,
+                 use_f64_boundary_pose: bool | None = None, free_motion_solve_precision: str | None = None,
+                 contact_solve_precision: str | None = None, contact_linear_solve_precision: str | None = None,
+                 sap_contact_weight_precision: str | None = None, collect_iteration_stats: bool = False,
+                 check_line_search_errors: bool = False, graph_conditional: bool = True,
+                 static_substep: bool = False, static_substep_iterations: int = 8,
+                 static_substep_line_search_iterations: int = 6, position_integration: str | None = None,
+                 hessian_precision: str | None = None):
+        view = _ModelView(model)
+        preset = dict(_CONTACT_PRESET_KWARGS[_normalize_contact_preset_variant(contact_preset_variant)])
+        self.contact_preset_variant = _normalize_contact_preset_variant(contact_preset_variant)
+        pick = lambda v, k: preset[k] if v is None else v
+        contact_weight_mode = pick(contact_weight_mode, "contact_weight_mode")
+        contact_point_mode = pick(contact_point_mode, "contact_point_mode")
+        position_integration = pick(position_integration, "position_integration")
+        self.contact_linear_solve_precision = _normalize_precision_knob(
+            pick(contact_linear_solve_precision, "contact_linear_solve_precision"),
+            option_name="contact_linear_solve_precision")
+        self.contact_solve_precision = _normalize_precision_knob(pick(contact_solve_precision,
+                                                                      "contact_solve_precision"),
+                                                                 option_name="contact_solve_precision")
+        self.free_motion_solve_precision = _normalize_precision_knob(
+            pick(free_motion_solve_precision, "free_motion_solve_precision"),
+            option_name="free_motion_solve_precision")
+        self.sap_contact_weight_precision = _normalize_precision_knob(
+            pick(sap_contact_weight_precision, "sap_contact_weight_precision"),
+            option_name="sap_contact_weight_precision")
+        self.use_f64_boundary_pose = bool(pick(use_f64_boundary_pose, "use_f64_boundary_pose"))
+        self.model = model
+        self.max_rigid_contact = int(max_rigid_contact)
+        self.max_iterations = int(max_iterations)
+        self.optimality_abs_tol, self.optimality_rel_tol = float(optimality_abs_tol), float(optimality_rel_tol)
+        self.armijo_c, self.rho = float(armijo_c), float(rho)
+        self.line_search_relative_slop = line_search_relative_slop
+        self.line_search_variant = normalize_sap_line_search_mode(line_search_variant)
+        if self.line_search_variant == "armijo_decay" and not (0.0 < float(rho) < 1.0):
+            raise ValueError(f"rho must lie in (0, 1), got {rho!r}.")
+        if cost_abs_tol is None:
+            cost_abs_tol = 0.0 if self.line_search_variant == "monotone_decay" else 1.0e-30
+        if cost_rel_tol is None:
+            cost_rel_tol = 5.0e-3 if self.line_search_variant == "monotone_decay" else 1.0e-15
+        self.cost_abs_tol, self.cost_rel_tol = float(cost_abs_tol), float(cost_rel_tol)
+        self.line_search_max_iterations = int(line_search_max_iterations)
+        if self.line_search_variant == "exact_root" and self.line_search_max_iterations == 40:
+            self.line_search_max_iterations = 100
+        if not bool(graph_conditional):
+            raise ValueError("SolverSAP only supports graph_conditional=True; "
+                             "the Python contact-solve loop has been removed.")
+        self.static_substep = bool(static_substep)
+        self.static_substep_iterations = int(static_substep_iterations)
+        self.static_substep_line_search_iterations = int(static_substep_line_search_iterations)
+        self.position_integration = str(position_integration).strip().lower().replace("-", "_")
+        if self.position_integration not in ("sap_euler", "midpoint"):
+            raise ValueError(f"position_integration must be 'sap_euler' or 'midpoint', got {position_integration!r}.")
+        self.collect_iteration_stats = bool(collect_iteration_stats)
+        self.check_line_search_errors = bool(check_line_search_errors)
+        tau = model.shape_material_tau.cpu().numpy() if model.shape_material_tau is not None else np.zeros(0)
+        explicit = tau[np.isfinite(tau) & (tau >= 0.0)]
+        shape_tau = (float(explicit[0]) if explicit.size else 0.0) if contact_tau_d is None else float(contact_tau_d)
+        if contact_tau_d is None and shape_tau == 0.0:
+            warnings.warn("No contact dissipation authored on the model and no contact_tau_d given: tau_d falls "
+                          "back to 0.0.", stacklevel=2)
+        self.contact_jacobian = SapContactJacobian(
+            model, max_rigid_contact=self.max_rigid_contact, fallback_mu=fallback_mu,
+            fallback_stiffness=fallback_stiffness, fallback_tau_d=shape_tau, contact_weight_mode=contact_weight_mode,
+            contact_point_mode=contact_point_mode, _view=view)
+        # the solve-side fallback is per pair: tau(shape0) + tau(shape1) (sim/solver_sap.py:945-955)
+        self.contact_solve = SapContactSolve(
+            model, max_rigid_contact=self.max_rigid_contact, contact_beta=contact_beta, contact_sigma=contact_sigma,
+            contact_tau_d=2.0 * shape_tau, block_size=block_size, diag_shift=diag_shift,
+            solve_precision=self.contact_solve_precision, linear_solve_precision=self.contact_linear_solve_precision,
+            hessian_precision=hessian_precision, _view=view)
+        self.view = view
+        self.num_envs, self.dof_count, self.dof_per_env = view.W, int(model.joint_dof_count), view.n
+        dev = view.device
+        self._v_guess_active = torch.zeros(1, dtype=I32, device=dev)
+        self._q_out_tmp = torch.zeros(int(model.joint_coord_count), dtype=F64, device=dev)
+        self.reset_runtime_state()
+
+    @property
+    def device(self):
+        return self.view.device
+
+    def get_max_contact_count(self) -> int:
+        return int(self.max_rigid_contact) * max(int(self.num_envs), 1)
+
+    def close(self) -> None:
+        pass
+
+    def notify_model_changed(self, flags: int) -> None:
+        return
+
+    def reset_runtime_state(self, state: SapState | None = None) -> None:
+        """sim/solver_sap.py:1004-1017"""
+        self.sim_time = 0.0
+        self.frame_id = 0
+        self.last_contact_count = 0
+        self.last_truncated_contact_count = 0
+        self.last_solve_iterations = 0
+        self.last_line_search_iterations = 0
+        self.last_converged = True
+        self._v_guess_active.zero_()
+        self.last_contacts = None
+        self.last_contact_jacobian_result = None
+        self.last_contact_solve_result = None
+
+    def step(self, state_in: SapState, state_out: SapState, control: SapControl | None, contacts, dt) -> SapState:
+        """sim/solver_sap.py:1388-1494"""
+        if getattr(state_in, "requires_grad", False):
+            raise NotImplementedError("SolverSAP does not support grad states.")
+        if not isinstance(state_in, SapState):
+            raise TypeError("SolverSAP.step requires SapState input.")
+        if not isinstance(state_out, SapState):
+            raise TypeError("SolverSAP.step requires SapState output.")
+        if control is not None and not isinstance(control, SapControl):
+            raise TypeError("SolverSAP.step requires SapControl.")
+        if contacts is None:
+            contacts = SapContacts()
+        if not isinstance(contacts, SapContacts):
+            contacts = sap_contacts_from_newton(contacts)
+        for s, name in ((state_in, "state_in"), (state_out, "state_out")):
+            if getattr(s, "joint_qd_order", "sap") not in ("sap", "public"):
+                raise ValueError(f"Unsupported SapState joint_qd_order={s.joint_qd_order!r}.")
+        self.contact_jacobian.set_dt(dt)
+        self.last_contacts = contacts
+        cr = self.contact_jacobian.compute(state_in, contacts, control=control)
+        if self.static_substep:
+            iters, ls_iters = self.static_substep_iterations, self.static_substep_line_search_iterations
+        else:
+            iters, ls_iters = self.max_iterations, self.line_search_max_iterations
+        v0 = self.contact_jacobian._qd
+        sr = self.contact_solve.solve(
+            cr, state_in, control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
+            v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, max_iterations=iters,
+            optimality_abs_tol=self.optimality_abs_tol, optimality_rel_tol=self.optimality_rel_tol,
+            cost_abs_tol=self.cost_abs_tol, cost_rel_tol=self.cost_rel_tol, line_search_max_iterations=ls_iters,
+            armijo_c=self.armijo_c, rho=self.rho, line_search_relative_slop=self.line_search_relative_slop,
+            line_search_variant=self.line_search_variant)
+        # position integration (sim/solver_sap.py:1267-1386)
+        mode = _abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint" else _abi.SAPB_INTEGRATE_SAP_EULER
+        q_in = self.contact_jacobian._q
+        q_out = state_out.joint_q if (state_out.joint_q.dtype == F64 and state_out.joint_q.is_contiguous()
+                                      and state_out.joint_q.data_ptr() != q_in.data_ptr()) else self._q_out_tmp
+        q_out.copy_(q_in)  # fixed joints keep their coordinates
+        status = load().sapb_integrate_positions(
+            ctypes.byref(self.view.desc), _ptr(q_in), _ptr(v0), _ptr(sr.v_flat), _ptr(self.contact_jacobian.dt_world),
+            mode, _ptr(q_out), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream))
+        check(status, "sapb_integrate_positions")
+        if q_out is not state_out.joint_q:
+            state_out.joint_q.copy_(q_out)
+        state_out.joint_qd.copy_(sr.v_flat)
+        if state_out.body_f is not None and state_in.body_f is not None and state_out.body_f is not state_in.body_f:
+            state_out.body_f.copy_(state_in.body_f)
+        self._v_guess_active.fill_(1)  # warm start from this step's solution (sim/solver_sap.py:1441-1451)
+        self.last_contact_jacobian_result = cr
+        self.last_contact_solve_result = sr
+        self.last_solve_iterations = -1
+        self.last_line_search_iterations = -1
+        self.last_converged = True
+        if not isinstance(dt, torch.Tensor):
+            self.sim_time += float(dt)
+        self.frame_id += 1
+        return state_out
+
+    def update_contacts(self, contacts: SapContacts) -> None:
+        raise NotImplementedError("SolverSAP does not expose contact-force writeback yet.")
+
+
+__all__ = ["SolverSAP", "SapFreeMotion", "SapContactJacobian", "SapContactSolve", "SapFreeMotionResult",
+           "SapContactJacobianResult", "SapContactSolveResult", "SAP_CONTACT_PRESET_VARIANTS"]

@@ -55,14 +55,18 @@ def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "sizes.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "sapb.h"\n'
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(sapb_solve_options),"
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(sapb_solve_options),"
         " sizeof(sapb_dof_terms), sizeof(sapb_contact_problem), sizeof(sapb_solve_outputs),"
-        " offsetof(sapb_contact_problem, dof), offsetof(sapb_solve_options, cubic_init)); return 0;}\n"
+        " offsetof(sapb_contact_problem, dof), offsetof(sapb_solve_options, cubic_init),"
+        " sizeof(sapb_model_desc), sizeof(sapb_step_inputs), sizeof(sapb_prepare_options),"
+        " sizeof(sapb_prepare_outputs)); return 0;}\n"
     )
     exe = tmp_path / "sizes"
     cc = "/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc"
     subprocess.run([cc, "-I", str(ROOT / "include"), "-o", str(exe), str(src)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(_abi.SolveOptions), ctypes.sizeof(_abi.DofTerms), ctypes.sizeof(_abi.ContactProblem),
-            ctypes.sizeof(_abi.SolveOutputs), _abi.ContactProblem.dof.offset, _abi.SolveOptions.cubic_init.offset]
+            ctypes.sizeof(_abi.SolveOutputs), _abi.ContactProblem.dof.offset, _abi.SolveOptions.cubic_init.offset,
+            ctypes.sizeof(_abi.ModelDesc), ctypes.sizeof(_abi.StepInputs), ctypes.sizeof(_abi.PrepareOptions),
+            ctypes.sizeof(_abi.PrepareOutputs)]
     assert got == want
