@@ -294,7 +294,14 @@ def contact_jacobian(m: Model, fm: dict, contacts: dict, max_contacts: int, *, p
     their rows (sim/contact_jacobian.py:404-562) and weights (:153-251).
     Returns per-world arrays; slot order = order of the flat buffer."""
     E, B, n, C = fm["pos"].shape[0], m.bodies_per_world, m.dofs_per_world, max_contacts
-    cnt = int(contacts["count"])
+    cnt = int(np.asarray(contacts["count"]).reshape(-1)[0])
+    # the FP64 mirrors when the buffer carries them (sim/sap_runtime.py:241-264)
+    f64 = all(k in contacts for k in ("point0d", "point1d", "normald", "margin0d", "margin1d"))
+    P0 = contacts["point0d"] if f64 else contacts["point0"]
+    P1 = contacts["point1d"] if f64 else contacts["point1"]
+    NR = contacts["normald"] if f64 else contacts["normal"]
+    M0 = contacts["margin0d"] if f64 else contacts["margin0"]
+    M1 = contacts["margin1d"] if f64 else contacts["margin1"]
     sh0, sh1 = contacts["shape0"][:cnt], contacts["shape1"][:cnt]
     b0 = np.where(sh0 >= 0, m.shape_body_global[np.maximum(sh0, 0)], -1)
     b1 = np.where(sh1 >= 0, m.shape_body_global[np.maximum(sh1, 0)], -1)
@@ -316,8 +323,8 @@ def contact_jacobian(m: Model, fm: dict, contacts: dict, max_contacts: int, *, p
         if slot >= C:
             out["truncated"] += 1
             continue
-        x0 = contacts["point0"][t].astype(np.float64)
-        x1 = contacts["point1"][t].astype(np.float64)
+        x0 = np.asarray(P0[t], np.float64)
+        x1 = np.asarray(P1[t], np.float64)
         p0 = p1 = np.zeros(3)
         lb0 = b0[t] - e * B if b0[t] >= 0 else -1
         lb1 = b1[t] - e * B if b1[t] >= 0 else -1
@@ -327,7 +334,7 @@ def contact_jacobian(m: Model, fm: dict, contacts: dict, max_contacts: int, *, p
         if lb1 >= 0:
             p1 = fm["pos"][e, lb1]
             x1 = p1 + qrotate(qnormalize(fm["quat"][e, lb1]), x1)
-        nrm = contacts["normal"][t].astype(np.float64)
+        nrm = np.asarray(NR[t], np.float64)
         nn = np.linalg.norm(nrm)
         nrm = nrm / nn if nn > 0 else nrm
         F = contact_frame_rows(nrm)
@@ -357,7 +364,7 @@ def contact_jacobian(m: Model, fm: dict, contacts: dict, max_contacts: int, *, p
             rel += Jw[3:] - skew(xj1 - p1) @ Jw[:3]
         J = F @ rel
         out["jac"][e, slot] = J
-        out["phi0"][e, slot] = (x1 - x0) @ nrm - contacts["margin0"][t] - contacts["margin1"][t]
+        out["phi0"][e, slot] = (x1 - x0) @ nrm - float(M0[t]) - float(M1[t])
         out["mu"][e, slot] = combine_mu(mu0, mu1)
         out["k"][e, slot] = combine_k(k0, k1)
         out["tau"][e, slot] = t0 + t1
