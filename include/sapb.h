@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 1
+#define SAPB_ABI_VERSION 2
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -36,6 +36,7 @@ extern "C" {
 #define SAPB_ERR_UNSUPPORTED (-101)
 #define SAPB_ERR_CUDA (-102)
 #define SAPB_ERR_WORKSPACE_TOO_SMALL (-103)
+#define SAPB_ERR_TIMEOUT (-104)          /* a bounded device-side wait gave up */
 /* per-world line-search status, the reference's device codes
  * (sim/contact_solve.py:2703-2705, 2873, 2904, 2989, 3026, 3099) */
 #define SAPB_LS_ASCENT_DIRECTION (-1)
@@ -144,6 +145,11 @@ typedef struct sapb_contact_problem {
   const int32_t* v_guess_active;  /* [1] nonzero: start from v_guess; NULL: never */
   const double* dt;               /* [E] per-world time step */
   const sapb_dof_terms* dof;      /* NULL: no PD / limit terms */
+  /* Learned warm start (no counterpart in the reference): starting impulses
+   * [E,C,3] or NULL.  When set, the solve forms v_L = v* + A^-1 J^T gamma0 on
+   * the participating DOFs and starts Newton from v_L only if
+   * cost(v_L) < cost(plain start), the plain start being v_guess or v0. */
+  const double* gamma0;
 } sapb_contact_problem;
 
 /* Outputs: the SapContactSolveResult fields a caller reads
@@ -158,6 +164,7 @@ typedef struct sapb_solve_outputs {
   int32_t* converged;             /* [E] 1 if optimality or cost test met */
   int32_t* status;                /* [E] last line-search status (0 or SAPB_LS_*) */
   double* grad_norm;              /* [E] ||D^-1/2 grad|| over participating DOFs */
+  int32_t* warm_start_accepted;   /* [E] 1 if the gamma0 start was taken (NULL: not written) */
 } sapb_solve_outputs;
 
 /* ---- free motion + contact Jacobian ---------------------------------------
@@ -315,6 +322,80 @@ int32_t sapb_contact_solve_noalloc(const sapb_contact_problem* problem, const sa
 
 /* Last CUDA error string seen by the library on this thread ("" if none). */
 const char* sapb_last_error(void);
+
+/* ---- learned warm start -----------------------------------------------------
+ * A per-contact MLP 12 -> 128 -> 128 -> 128 -> 3 (GELU, tanh form), BF16
+ * weights and activations, FP32 accumulation, run and trained on the tensor
+ * cores (tcgen05) by the kernels below.  No counterpart in the reference,
+ * whose only warm start is the previous step's velocity
+ * (sim/solver_sap.py:1441-1451).
+ *
+ * Inputs of a contact slot (raw, before normalisation): phi0; J_c v* in the
+ * contact frame (t1, t2, n); the world-up component of the contact normal;
+ * mu; log10(stiffness); tau_d; dt; w_eff * gamma_prev (t1, t2, n).  The
+ * output y maps to u = y * output_scale + output_shift (velocity units) and
+ * gamma0 = u / w_eff, projected onto the friction cone. */
+#define SAPB_MLP_INPUTS 12
+#define SAPB_MLP_INPUTS_PADDED 16
+#define SAPB_MLP_HIDDEN 128
+#define SAPB_MLP_OUTPUTS 3
+/* FP32 master parameters W1[128][12] b1[128] W2[128][128] b2 W3[128][128] b3
+ * W4[3][128] b4[3]; the forward reads BF16 operand images (packed) and FP32
+ * biases made from them by sapb_mlp_pack / sapb_mlp_adam. */
+#define SAPB_MLP_PARAM_COUNT 35075
+#define SAPB_MLP_PACKED_COUNT 35200
+#define SAPB_MLP_BIAS_COUNT 387
+
+typedef struct sapb_warmstart_norm {
+  float feature_mean[SAPB_MLP_INPUTS];
+  float feature_inv_std[SAPB_MLP_INPUTS];
+  float output_scale[SAPB_MLP_OUTPUTS];
+  float output_shift[SAPB_MLP_OUTPUTS];
+} sapb_warmstart_norm;
+
+/* Saved forward state of one training batch of `rows` rows. */
+typedef struct sapb_mlp_train_buffers {
+  uint16_t* act;  /* BF16 [act_elems] hidden activations (tile images) */
+  float* pre;     /* FP32 [pre_elems] pre-activations */
+  float* dy;      /* FP32 [rows,3] dL/dy of the mean squared error */
+  float* loss;    /* FP32 [1] sum of squared errors, accumulated */
+} sapb_mlp_train_buffers;
+
+typedef struct sapb_adam_options {
+  float lr, beta1, beta2, eps, weight_decay;  /* decoupled weight decay */
+} sapb_adam_options;
+
+int32_t sapb_mlp_param_count(void);
+int32_t sapb_mlp_packed_count(void);
+int32_t sapb_mlp_bias_count(void);
+int32_t sapb_mlp_train_buffer_sizes(int32_t rows, int64_t* act_elems, int64_t* pre_elems);
+/* params [PARAM_COUNT] -> packed [PACKED_COUNT] (BF16 bits), bias [BIAS_COUNT]. */
+int32_t sapb_mlp_pack(const float* params, uint16_t* packed, float* bias, void* stream);
+/* y[rows,3] = MLP(x), x [rows,16] BF16 (16-byte aligned, columns 12..15 zero). */
+int32_t sapb_mlp_forward(const uint16_t* packed, const float* bias, const uint16_t* x, int32_t rows, float* y,
+                         void* stream);
+/* Training forward: saves buf->act / buf->pre, writes buf->dy and adds the
+ * squared error to buf->loss; y optional. */
+int32_t sapb_mlp_forward_train(const uint16_t* packed, const float* bias, const uint16_t* x, const float* target,
+                               int32_t rows, const sapb_mlp_train_buffers* buf, float* y, void* stream);
+/* Adds dL/dparams (master layout) of the batch to grad. */
+int32_t sapb_mlp_backward(const uint16_t* packed, const uint16_t* x, int32_t rows, const sapb_mlp_train_buffers* buf,
+                          float* grad, void* stream);
+/* One Adam step (step >= 1) on params with moments m, v; refreshes packed/bias. */
+int32_t sapb_mlp_adam(float* params, const float* grad, float* m, float* v, const sapb_adam_options* opt,
+                      int32_t step, uint16_t* packed, float* bias, void* stream);
+/* Reads and clears the MLP kernels' timeout flag (synchronises `stream`):
+ * SAPB_OK or SAPB_ERR_TIMEOUT. */
+int32_t sapb_mlp_error(void* stream);
+/* Per-slot network inputs of a stage-2 problem: normalised BF16 rows
+ * features [E*C,16] and/or raw FP32 rows raw [E*C,12]; dead slots are zero.
+ * normal_up [E,C] (NULL: 1), gamma_prev [E,C,3] (NULL: 0). */
+int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const double* normal_up,
+                                const double* gamma_prev, const sapb_warmstart_norm* norm, double tau_fallback,
+                                uint16_t* features, float* raw, void* stream);
+/* gamma0 [E,C,3] from the network output mlp_out [E*C,3]. */
+int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float* mlp_out,
+                                const sapb_warmstart_norm* norm, double* gamma0, void* stream);
 
 #ifdef __cplusplus
 }

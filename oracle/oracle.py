@@ -100,8 +100,9 @@ def _c(a, dtype):
 
 
 def solve(prob, line_search_variant: str = "monotone_decay", threads: int = 0, v_guess=None,
-          v_guess_active: bool = False, dof_terms: dict | None = None, **overrides) -> dict:
-    """Run the oracle on a scenes.ContactProblemArrays (host)."""
+          v_guess_active: bool = False, dof_terms: dict | None = None, gamma0=None, **overrides) -> dict:
+    """Run the oracle on a scenes.ContactProblemArrays (host).  gamma0
+    (E, C, 3): learned starting impulses (accepted on the cost test)."""
     lib = load()
     E, n, C = prob.num_envs, prob.dof_per_env, prob.max_contacts
     keep = {}
@@ -131,6 +132,7 @@ def solve(prob, line_search_variant: str = "monotone_decay", threads: int = 0, v
     P.v_star = ptr("vs", prob.v_star, np.float64)
     P.v0 = ptr("v0", prob.v0, np.float64)
     P.dt = ptr("dt", prob.dt, np.float64)
+    P.gamma0 = ptr("gamma0", gamma0, np.float64)
     guess = None
     if v_guess is not None:
         guess = _c(v_guess, np.float64).copy()
@@ -160,6 +162,7 @@ def solve(prob, line_search_variant: str = "monotone_decay", threads: int = 0, v
         v=np.zeros(E * n), contact_gamma=np.zeros((E, max(C, 1), 3)), contact_mode=np.zeros((E, max(C, 1)), np.int32),
         cost=np.zeros(E), newton_iterations=np.zeros(E, np.int32), line_search_iterations=np.zeros(E, np.int32),
         converged=np.zeros(E, np.int32), status=np.zeros(E, np.int32), grad_norm=np.zeros(E),
+        warm_start_accepted=np.zeros(E, np.int32),
     )
     O = _abi.SolveOutputs()
     for k, a in out.items():

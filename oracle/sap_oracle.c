@@ -1019,6 +1019,7 @@ static void solve_world(const sapb_contact_problem* P, const sapb_solve_options*
   /* Initialization and unconstrained worlds (:340-394). */
   int32_t newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
   double alpha = 1.0, previous_cost = 0.0, grad_norm = 0.0;
+  int32_t ws_accepted = 0;
   int unconstrained = count == 0;
   for (int32_t i = 0; i < n; ++i)
     if (w.pd_active[i] || w.lo_act[i] || w.up_act[i]) unconstrained = 0;
@@ -1029,6 +1030,45 @@ static void solve_world(const sapb_contact_problem* P, const sapb_solve_options*
   } else {
     for (int32_t i = 0; i < n; ++i)
       if (!w.part[i]) w.v[i] = w.v_star[i];
+    /* Learned warm start (no counterpart in the reference): the candidate
+     * v_L = v* + A^-1 J^T gamma0 on the participating DOFs replaces the plain
+     * start only if its cost is lower. */
+    if (P->gamma0 && count > 0) {
+      const double cost_plain = evaluate(&w, w.v, w.vc, w.gamma, w.ccost, w.impulse, w.grad, w.dyn, w.pd_gamma,
+                                         w.pd_hdiag, w.lim_grad, w.lim_hdiag, NULL);
+      double* L = (double*)malloc(sizeof(double) * nd * nd);
+      double* x = (double*)malloc(sizeof(double) * nd);
+      double* vsave = (double*)malloc(sizeof(double) * nd);
+      const double* g0 = P->gamma0 + (size_t)e * C * 3;
+      memcpy(L, w.A, sizeof(double) * nd * nd);
+      memcpy(vsave, w.v, sizeof(double) * nd);
+      for (int32_t i = 0; i < n; ++i) {
+        double acc = 0.0;
+        for (int32_t c = 0; c < count; ++c)
+          for (int32_t r = 0; r < 3; ++r) acc += w.J[((size_t)c * 3 + r) * n + i] * g0[3 * c + r];
+        x[i] = acc;
+      }
+      if (sapo_cholesky(L, n) == 0) {
+        for (int32_t i = 0; i < n; ++i) {
+          double t = x[i];
+          for (int32_t k = 0; k < i; ++k) t -= L[i * n + k] * x[k];
+          x[i] = t / L[i * n + i];
+        }
+        for (int32_t i = n - 1; i >= 0; --i) {
+          double t = x[i];
+          for (int32_t k = i + 1; k < n; ++k) t -= L[k * n + i] * x[k];
+          x[i] = t / L[i * n + i];
+        }
+        for (int32_t i = 0; i < n; ++i) w.v[i] = w.part[i] ? w.v_star[i] + x[i] : w.v_star[i];
+        const double cost_l = evaluate(&w, w.v, w.vc, w.gamma, w.ccost, w.impulse, w.grad, w.dyn, w.pd_gamma,
+                                       w.pd_hdiag, w.lim_grad, w.lim_hdiag, NULL);
+        if (cost_l < cost_plain) ws_accepted = 1;
+        else memcpy(w.v, vsave, sizeof(double) * nd);
+      }
+      free(L);
+      free(x);
+      free(vsave);
+    }
     /* Newton loop (:5559-5655 with the body :5474-5557). */
     int32_t it = 0;
     w.cost = evaluate(&w, w.v, w.vc, w.gamma, w.ccost, w.impulse, w.grad, w.dyn, w.pd_gamma, w.pd_hdiag,
@@ -1097,6 +1137,7 @@ static void solve_world(const sapb_contact_problem* P, const sapb_solve_options*
   if (out->converged) out->converged[e] = converged;
   if (out->status) out->status[e] = status;
   if (out->grad_norm) out->grad_norm[e] = grad_norm;
+  if (out->warm_start_accepted) out->warm_start_accepted[e] = ws_accepted;
   free(pool);
   free(ipool);
 }

@@ -8,13 +8,14 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 1
+SAPB_ABI_VERSION = 2
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
 SAPB_ERR_UNSUPPORTED = -101
 SAPB_ERR_CUDA = -102
 SAPB_ERR_WORKSPACE_TOO_SMALL = -103
+SAPB_ERR_TIMEOUT = -104
 
 SAPB_LS_ASCENT_DIRECTION = -1
 SAPB_LS_ALPHA_UNDERFLOW = -2
@@ -112,6 +113,7 @@ class ContactProblem(C.Structure):
         ("v_guess_active", _p),
         ("dt", _p),
         ("dof", C.POINTER(DofTerms)),
+        ("gamma0", _p),
     ]
 
 
@@ -126,6 +128,7 @@ class SolveOutputs(C.Structure):
         ("converged", _p),
         ("status", _p),
         ("grad_norm", _p),
+        ("warm_start_accepted", _p),
     ]
 
 
@@ -219,6 +222,33 @@ class PrepareOutputs(C.Structure):
     ]
 
 
+SAPB_MLP_INPUTS = 12
+SAPB_MLP_INPUTS_PADDED = 16
+SAPB_MLP_HIDDEN = 128
+SAPB_MLP_OUTPUTS = 3
+SAPB_MLP_PARAM_COUNT = 35075
+SAPB_MLP_PACKED_COUNT = 35200
+SAPB_MLP_BIAS_COUNT = 387
+
+
+class WarmstartNorm(C.Structure):
+    _fields_ = [
+        ("feature_mean", C.c_float * SAPB_MLP_INPUTS),
+        ("feature_inv_std", C.c_float * SAPB_MLP_INPUTS),
+        ("output_scale", C.c_float * SAPB_MLP_OUTPUTS),
+        ("output_shift", C.c_float * SAPB_MLP_OUTPUTS),
+    ]
+
+
+class MlpTrainBuffers(C.Structure):
+    _fields_ = [("act", _p), ("pre", _p), ("dy", _p), ("loss", _p)]
+
+
+class AdamOptions(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("weight_decay", C.c_float)]
+
+
 # name -> (restype, argtypes) of every symbol include/sapb.h declares.
 EXPORTS = {
     "sapb_solve_options_default": (None, [C.POINTER(SolveOptions), C.c_int32]),
@@ -241,6 +271,20 @@ EXPORTS = {
     "sapb_integrate_positions": (
         C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, C.c_int32, _p, _p]
     ),
+    "sapb_mlp_param_count": (C.c_int32, []),
+    "sapb_mlp_packed_count": (C.c_int32, []),
+    "sapb_mlp_bias_count": (C.c_int32, []),
+    "sapb_mlp_train_buffer_sizes": (C.c_int32, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "sapb_mlp_pack": (C.c_int32, [_p, _p, _p, _p]),
+    "sapb_mlp_forward": (C.c_int32, [_p, _p, _p, C.c_int32, _p, _p]),
+    "sapb_mlp_forward_train": (C.c_int32, [_p, _p, _p, _p, C.c_int32, C.POINTER(MlpTrainBuffers), _p, _p]),
+    "sapb_mlp_backward": (C.c_int32, [_p, _p, C.c_int32, C.POINTER(MlpTrainBuffers), _p, _p]),
+    "sapb_mlp_adam": (C.c_int32, [_p, _p, _p, _p, C.POINTER(AdamOptions), C.c_int32, _p, _p, _p]),
+    "sapb_mlp_error": (C.c_int32, [_p]),
+    "sapb_warmstart_features": (
+        C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), C.c_double, _p, _p, _p]
+    ),
+    "sapb_warmstart_impulses": (C.c_int32, [C.POINTER(ContactProblem), _p, C.POINTER(WarmstartNorm), _p, _p]),
 }
 
 

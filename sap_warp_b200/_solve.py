@@ -80,6 +80,7 @@ class ContactSolveBuffers:
     converged: torch.Tensor = field(init=False)
     status: torch.Tensor = field(init=False)
     grad_norm: torch.Tensor = field(init=False)
+    warm_start_accepted: torch.Tensor = field(init=False)
     workspace: torch.Tensor = field(init=False)
 
     def __post_init__(self):
@@ -93,6 +94,7 @@ class ContactSolveBuffers:
         self.converged = torch.zeros(E, dtype=I32, device=dev)
         self.status = torch.zeros(E, dtype=I32, device=dev)
         self.grad_norm = torch.zeros(E, dtype=F64, device=dev)
+        self.warm_start_accepted = torch.zeros(E, dtype=I32, device=dev)
         ws = int(load().sapb_contact_solve_workspace_size(E, n, C))
         self.workspace = torch.zeros(max(ws, 16), dtype=torch.uint8, device=dev)
 
@@ -119,8 +121,11 @@ class DofTermArrays:
             setattr(self.struct, name, _ptr(arrays.get(name), dtype, name=name))
 
 
-def contact_solve(
+def build_problem(
     *,
+    num_envs: int,
+    dof_per_env: int,
+    max_contacts: int,
     contact_count: torch.Tensor,
     dynamics_matrix: torch.Tensor,
     jacobian: torch.Tensor,
@@ -132,8 +137,6 @@ def contact_solve(
     v_star: torch.Tensor,
     v0: torch.Tensor,
     dt: torch.Tensor,
-    buffers: ContactSolveBuffers,
-    options: _abi.SolveOptions,
     body0: torch.Tensor | None = None,
     body1: torch.Tensor | None = None,
     body_dof_start: torch.Tensor | None = None,
@@ -141,11 +144,10 @@ def contact_solve(
     v_guess: torch.Tensor | None = None,
     v_guess_active: torch.Tensor | None = None,
     dof_terms: DofTermArrays | None = None,
-    stream: torch.cuda.Stream | None = None,
-) -> ContactSolveBuffers:
-    """Launch the fused solve; results land in `buffers` (no host sync)."""
-    lib = load()
-    E, n, C = buffers.num_envs, buffers.dof_per_env, buffers.max_contacts
+    gamma0: torch.Tensor | None = None,
+) -> _abi.ContactProblem:
+    """sapb_contact_problem over device tensors (shapes and dtypes checked)."""
+    E, n, C = num_envs, dof_per_env, max_contacts
     P = _abi.ContactProblem()
     P.num_envs, P.dof_per_env, P.max_contacts = E, n, C
     P.num_bodies = int(body_dof_start.numel()) if body_dof_start is not None else 0
@@ -166,10 +168,29 @@ def contact_solve(
     P.v_guess = _ptr(v_guess, F64, E * n, "v_guess")
     P.v_guess_active = _ptr(v_guess_active, I32, 1, "v_guess_active")
     P.dt = _ptr(dt, F64, E, "dt")
+    P.gamma0 = _ptr(gamma0, F64, E * C * 3, "gamma0")
     if dof_terms is not None:
         P.dof = ctypes.pointer(dof_terms.struct)
-    out = _abi.SolveOutputs()
+    return P
+
+
+def contact_solve(
+    *,
+    buffers: ContactSolveBuffers,
+    options: _abi.SolveOptions,
+    stream: torch.cuda.Stream | None = None,
+    **arrays,
+) -> ContactSolveBuffers:
+    """Launch the fused solve; results land in `buffers` (no host sync).
+
+    `arrays` are the keyword tensors of `build_problem` (contact_count,
+    dynamics_matrix, jacobian, phi0, w_eff, mu, stiffness, tau_d, v_star, v0,
+    dt and the optional body maps, v_guess, v_guess_active, dof_terms and the
+    learned starting impulses gamma0)."""
+    lib = load()
     b = buffers
+    P = build_problem(num_envs=b.num_envs, dof_per_env=b.dof_per_env, max_contacts=b.max_contacts, **arrays)
+    out = _abi.SolveOutputs()
     out.v = b.v.data_ptr()
     out.contact_gamma = b.contact_gamma.data_ptr()
     out.contact_mode = b.contact_mode.data_ptr()
@@ -179,6 +200,7 @@ def contact_solve(
     out.converged = b.converged.data_ptr()
     out.status = b.status.data_ptr()
     out.grad_norm = b.grad_norm.data_ptr()
+    out.warm_start_accepted = b.warm_start_accepted.data_ptr()
     s = stream if stream is not None else torch.cuda.current_stream(b.device)
     status = lib.sapb_contact_solve(
         ctypes.byref(P), ctypes.byref(options), ctypes.byref(out), b.workspace.data_ptr(), b.workspace.numel(),

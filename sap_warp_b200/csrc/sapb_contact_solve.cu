@@ -48,7 +48,7 @@ constexpr int kChunk = 16;
 struct Layout {
   int n, C, ldJ, ldH, nb;
   size_t off_J, off_scr, off_H, off_G, off_vec, off_con, off_flags, off_tri, total;
-  static constexpr int kVecs = 19;
+  static constexpr int kVecs = 20;
   static constexpr int kConPer = 17;
   static constexpr int kMaxWarps = 4;  // partial-sum scratch (blocks of <= 128 threads)
 };
@@ -89,7 +89,7 @@ __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
 // Vector slots inside off_vec (each ldJ doubles).
 enum Vec {
   V_V = 0, V_VSTAR, V_DV, V_GRAD, V_ARES, V_DP, V_DSCALE, V_AINV, V_PDA, V_PDGAIN, V_PDLIM,
-  V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_END
+  V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_SAVE, V_END
 };
 static_assert(V_END <= Layout::kVecs, "vector slots");
 // Contact slots inside off_con (each C doubles).
@@ -1034,6 +1034,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
 
     int newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
     double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
+    int ws_accepted = 0;
     bool evaluated = false;
     if (unconstrained) {
       converged = 1;
@@ -1043,12 +1044,59 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       for (int i = tid; i < n; i += NT)
         if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
+      // Learned warm start (no counterpart in the reference): the candidate
+      // v_L = v* + A^-1 J^T gamma0 on the participating DOFs, A factored in
+      // this kernel's factor precision, replaces the plain start only if its
+      // cost is lower.  An accepted candidate's evaluation seeds iteration 0.
+      bool have_e4 = false;
+      double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
+      if (P.p.gamma0 && count > 0) {
+        double e4p[4];
+        evaluate<NT, HT, NS>(w, P, dt, e4p);
+        const double* g0 = P.p.gamma0 + (size_t)e * C * 3;
+        const int ldj = w.ldJ(), ldh = w.ldH();
+        for (int i = tid; i < n; i += NT) {
+          w.V(V_SAVE)[i] = w.V(V_V)[i];
+          double acc = 0.0;
+          for (int c = 0; c < count; ++c) {
+            const double* Jc = w.J + (size_t)(3 * c) * ldj;
+            acc += Jc[i] * __ldg(g0 + 3 * c) + Jc[ldj + i] * __ldg(g0 + 3 * c + 1) +
+                   Jc[2 * ldj + i] * __ldg(g0 + 3 * c + 2);
+          }
+          w.V(V_GRAD)[i] = -acc;  // factor_and_solve solves H dv = -grad
+        }
+        {
+          const int lane = tid & 31, warp = tid >> 5;
+          for (int i = warp; i < n; i += NT / 32)
+            for (int j = lane; j <= i; j += 32) w.H[(size_t)i * ldh + j] = HT(__ldg(w.A + (size_t)i * n + j));
+        }
+        __syncthreads();
+        factor_and_solve<NT, HT, NS>(w);
+        for (int i = tid; i < n; i += NT)
+          w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? w.V(V_VSTAR)[i] + w.V(V_DV)[i] : w.V(V_VSTAR)[i];
+        __syncthreads();
+        double e4l[4];
+        evaluate<NT, HT, NS>(w, P, dt, e4l);
+        if (e4l[0] < e4p[0]) {
+          ws_accepted = 1;
+          have_e4 = true;
+          for (int k = 0; k < 4; ++k) e4_seed[k] = e4l[k];
+        } else {
+          for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_SAVE)[i];
+          __syncthreads();
+        }
+      }
       const double cost_min_alpha = P.o.line_search_variant == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
       int it = 0;
       bool active = true;
       for (;;) {
         double e4[4];
-        evaluate<NT, HT, NS>(w, P, dt, e4);
+        if (have_e4) {
+          for (int k = 0; k < 4; ++k) e4[k] = e4_seed[k];
+          have_e4 = false;
+        } else {
+          evaluate<NT, HT, NS>(w, P, dt, e4);
+        }
         evaluated = true;
         cost = e4[0];
         // convergence test (sim/contact_solve.py:2043-2087)
@@ -1122,6 +1170,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       if (P.out.converged) P.out.converged[e] = converged;
       if (P.out.status) P.out.status[e] = status;
       if (P.out.grad_norm) P.out.grad_norm[e] = grad_norm;
+      if (P.out.warm_start_accepted) P.out.warm_start_accepted[e] = ws_accepted;
     }
     __syncthreads();
   }

@@ -178,6 +178,7 @@ class ContactProblemArrays:
     v_star: np.ndarray  # (E*n,)
     v0: np.ndarray
     dt: np.ndarray  # (E,)
+    normal_up: np.ndarray | None = None  # (E, C) world-up component of the contact normal
 
     def subset(self, worlds: np.ndarray) -> "ContactProblemArrays":
         """The same problem restricted to a list of worlds (bodies renumbered)."""
@@ -194,6 +195,7 @@ class ContactProblemArrays:
             remap(self.body0[worlds]), remap(self.body1[worlds]),
             self.body_dof_start[body_idx].copy(), self.body_dof_count[body_idx].copy(),
             self.v_star[dof_idx].copy(), self.v0[dof_idx].copy(), self.dt[worlds].copy(),
+            None if self.normal_up is None else self.normal_up[worlds].copy(),
         )
 
 
@@ -278,6 +280,7 @@ def humanoid_contact_problem(
         v_star=v_star.reshape(-1),
         v0=v0.reshape(-1),
         dt=np.full(E, dt),
+        normal_up=frame[:, :, 2, 2] * live,
     )
 
 

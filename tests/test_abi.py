@@ -49,6 +49,14 @@ def test_no_compute_entry_points_without_gpu(lib):
     # argument errors are reported before any CUDA call
     assert lib.sapb_contact_solve(None, None, None, None, 0, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
     assert b"null" in lib.sapb_last_error()
+    assert lib.sapb_mlp_param_count() == _abi.SAPB_MLP_PARAM_COUNT
+    assert lib.sapb_mlp_packed_count() == _abi.SAPB_MLP_PACKED_COUNT
+    assert lib.sapb_mlp_bias_count() == _abi.SAPB_MLP_BIAS_COUNT
+    a, p = ctypes.c_int64(), ctypes.c_int64()
+    assert lib.sapb_mlp_train_buffer_sizes(300, ctypes.byref(a), ctypes.byref(p)) == _abi.SAPB_OK
+    assert a.value == p.value == 3 * 3 * 128 * 128
+    assert lib.sapb_mlp_forward(None, None, None, 4, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert lib.sapb_warmstart_features(None, None, None, None, 0.0, None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
 
 
 def test_struct_layout_matches_header(tmp_path):
@@ -59,7 +67,9 @@ def test_struct_layout_matches_header(tmp_path):
         " sizeof(sapb_dof_terms), sizeof(sapb_contact_problem), sizeof(sapb_solve_outputs),"
         " offsetof(sapb_contact_problem, dof), offsetof(sapb_solve_options, cubic_init),"
         " sizeof(sapb_model_desc), sizeof(sapb_step_inputs), sizeof(sapb_prepare_options),"
-        " sizeof(sapb_prepare_outputs)); return 0;}\n"
+        " sizeof(sapb_prepare_outputs)); printf(\"%zu %zu %zu %zu\\n\", sizeof(sapb_warmstart_norm),"
+        " sizeof(sapb_mlp_train_buffers), sizeof(sapb_adam_options), offsetof(sapb_contact_problem, gamma0));"
+        " return 0;}\n"
     )
     exe = tmp_path / "sizes"
     cc = "/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc"
@@ -68,5 +78,6 @@ def test_struct_layout_matches_header(tmp_path):
     want = [ctypes.sizeof(_abi.SolveOptions), ctypes.sizeof(_abi.DofTerms), ctypes.sizeof(_abi.ContactProblem),
             ctypes.sizeof(_abi.SolveOutputs), _abi.ContactProblem.dof.offset, _abi.SolveOptions.cubic_init.offset,
             ctypes.sizeof(_abi.ModelDesc), ctypes.sizeof(_abi.StepInputs), ctypes.sizeof(_abi.PrepareOptions),
-            ctypes.sizeof(_abi.PrepareOutputs)]
+            ctypes.sizeof(_abi.PrepareOutputs), ctypes.sizeof(_abi.WarmstartNorm),
+            ctypes.sizeof(_abi.MlpTrainBuffers), ctypes.sizeof(_abi.AdamOptions), _abi.ContactProblem.gamma0.offset]
     assert got == want

@@ -1,0 +1,160 @@
+"""The tcgen05 MLP kernels (forward, training forward, backward, Adam, packing)
+against the numpy network oracle, which mirrors their BF16 rounding points,
+and the backward also against float64 autograd of the unrounded network.
+
+Tolerances: the kernels accumulate in FP32 and evaluate tanh with the
+hardware approximation, so a hidden activation can land one BF16 ulp
+(2^-8 relative) away from the oracle's; outputs and gradients are compared
+in relative max / norm terms well above that."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp as om
+from sap_warp_b200 import _abi
+from sap_warp_b200.warmstart import TrainBuffers, WarmStartMLP
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16_rows(x: np.ndarray, device) -> torch.Tensor:
+    pad = np.zeros((x.shape[0], om.IN_PAD), np.float32)
+    pad[:, :om.IN] = x
+    return torch.from_numpy(om.bf16_bits(pad).view(np.int16)).to(device).contiguous()
+
+
+def core_index(rows: int, cols: int) -> np.ndarray:
+    r, k = np.meshgrid(np.arange(rows), np.arange(cols), indexing="ij")
+    return ((k >> 3) * (rows >> 3) + (r >> 3)) * 64 + (r & 7) * 8 + (k & 7)
+
+
+def params_with_output(seed: int, scale: float = 10.0) -> np.ndarray:
+    p = om.init_params(seed)
+    p[om.offsets()["W4"][0]:] *= scale
+    return p
+
+
+def rel_norm(a, b) -> float:
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-30))
+
+
+def test_packed_images(cuda_device):
+    params = params_with_output(7)
+    mlp = WarmStartMLP(cuda_device, params=params)
+    torch.cuda.synchronize()
+    got = mlp.packed.cpu().numpy().view(np.uint16)
+    p = om.unpack(params)
+    want = np.zeros(_abi.SAPB_MLP_PACKED_COUNT, np.uint16)
+    w1 = np.zeros((128, 16), np.float32)
+    w1[:, :12] = p["W1"]
+    want[0:2048][core_index(128, 16).reshape(-1)] = om.bf16_bits(w1).reshape(-1)
+    want[2048:18432][core_index(128, 128).reshape(-1)] = om.bf16_bits(p["W2"]).reshape(-1)
+    want[18432:34816][core_index(128, 128).reshape(-1)] = om.bf16_bits(p["W3"]).reshape(-1)
+    want[34816:] = om.bf16_bits(p["W4"]).reshape(-1)
+    np.testing.assert_array_equal(got, want)
+    np.testing.assert_array_equal(mlp.bias.cpu().numpy(), np.concatenate([p["b1"], p["b2"], p["b3"], p["b4"]]))
+
+
+@pytest.mark.parametrize("rows", [1, 128, 1000, 20000])
+def test_forward_matches_oracle(cuda_device, rows):
+    rng = np.random.default_rng(rows)
+    params = params_with_output(5)
+    x = om.bf16(rng.normal(size=(rows, om.IN)).astype(np.float32))
+    mlp = WarmStartMLP(cuda_device, params=params)
+    y = mlp.forward(bf16_rows(x, cuda_device)).cpu().numpy()
+    mlp.check_error()
+    ref = om.forward(params, x)["y"]
+    assert np.abs(y - ref).max() <= 1e-2 * np.abs(ref).max() + 1e-4, np.abs(y - ref).max()
+
+
+def test_forward_train_saves_state(cuda_device):
+    rows = 300
+    rng = np.random.default_rng(11)
+    params = params_with_output(6)
+    x = om.bf16(rng.normal(size=(rows, om.IN)).astype(np.float32))
+    t = rng.normal(size=(rows, 3)).astype(np.float32)
+    mlp = WarmStartMLP(cuda_device, params=params)
+    buf = TrainBuffers(rows, cuda_device)
+    y = torch.zeros(rows, 3, dtype=torch.float32, device=cuda_device)
+    mlp.forward_train(bf16_rows(x, cuda_device), torch.from_numpy(t).to(cuda_device), buf, y)
+    mlp.check_error()
+    ref = om.forward(params, x)
+    yg = y.cpu().numpy()
+    assert np.abs(yg - ref["y"]).max() <= 1e-2 * np.abs(ref["y"]).max() + 1e-4
+    tiles = (rows + 127) // 128
+    pre = buf.pre.cpu().numpy().reshape(tiles, 3, 128, 128)
+    act = buf.act.cpu().numpy().view(np.uint16).reshape(tiles, 3, -1)
+    idx = core_index(128, 128)
+    for layer in range(3):
+        z = np.concatenate([pre[i, layer].T for i in range(tiles)])[:rows]
+        h = np.concatenate([om.from_bf16_bits(act[i, layer][idx]) for i in range(tiles)])[:rows]
+        zr, hr = ref[f"z{layer + 1}"], ref[f"h{layer + 1}"]
+        assert np.abs(z - zr).max() <= 1e-2 * np.abs(zr).max(), layer
+        assert np.abs(h - hr).max() <= 1e-2 * np.abs(hr).max() + 1e-3, layer
+    dy = buf.dy.cpu().numpy()
+    np.testing.assert_allclose(dy, (yg - t) * (2.0 / (3.0 * rows)), rtol=1e-5, atol=1e-9)
+    np.testing.assert_allclose(buf.loss.item(), ((yg - t) ** 2).sum(), rtol=1e-4)
+
+
+@pytest.mark.parametrize("rows", [200, 4096])
+def test_backward_matches_oracle_and_autograd(cuda_device, rows):
+    rng = np.random.default_rng(rows + 1)
+    params = params_with_output(8)
+    x = om.bf16(rng.normal(size=(rows, om.IN)).astype(np.float32))
+    t = rng.normal(size=(rows, 3)).astype(np.float32)
+    mlp = WarmStartMLP(cuda_device, params=params)
+    buf = TrainBuffers(rows, cuda_device)
+    xd = bf16_rows(x, cuda_device)
+    mlp.grad.zero_()
+    mlp.forward_train(xd, torch.from_numpy(t).to(cuda_device), buf)
+    mlp.backward(xd, buf)
+    mlp.check_error()
+    g = om.unpack(mlp.grad.cpu().numpy())
+    _, gm, _ = om.backward(params, x, t, mirror=True)
+    _, gx, _ = om.backward(params, x, t, mirror=False)
+    gm, gx = om.unpack(gm), om.unpack(gx)
+    for k in gm:
+        assert rel_norm(g[k], gm[k]) < 2e-2, (k, rel_norm(g[k], gm[k]))
+        assert rel_norm(g[k], gx[k]) < 6e-2, (k, rel_norm(g[k], gx[k]))
+
+
+def test_adam_matches_oracle(cuda_device):
+    rng = np.random.default_rng(3)
+    params = om.init_params(9)
+    mlp = WarmStartMLP(cuda_device, params=params)
+    grad = rng.normal(size=om.PARAM_COUNT).astype(np.float32)
+    p, m, v = params.copy(), np.zeros_like(params), np.zeros_like(params)
+    for step in range(1, 4):
+        mlp.grad.copy_(torch.from_numpy(grad * step))
+        mlp.adam(1e-3, weight_decay=1e-4)
+        p, m, v = om.adam(p, grad * step, m, v, step, 1e-3, weight_decay=1e-4)
+    np.testing.assert_allclose(mlp.params.cpu().numpy(), p, rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(mlp.m.cpu().numpy(), m, rtol=1e-5, atol=1e-9)
+    np.testing.assert_allclose(mlp.v.cpu().numpy(), v, rtol=1e-5, atol=1e-12)
+    packed = mlp.packed.clone()
+    mlp.pack()
+    torch.testing.assert_close(mlp.packed, packed, rtol=0, atol=0)
+
+
+def test_training_fits_a_teacher(cuda_device):
+    """Adam on the kernels' gradients fits a random teacher network."""
+    rng = np.random.default_rng(4)
+    teacher = params_with_output(21, scale=5.0)
+    x = om.bf16(rng.normal(size=(32768, om.IN)).astype(np.float32))
+    t = om.forward(teacher, x, mirror=False)["y"].astype(np.float32)
+    t = (t - t.mean(0)) / t.std(0)
+    mlp = WarmStartMLP(cuda_device, seed=1)
+    xd, td = bf16_rows(x, cuda_device), torch.from_numpy(t).to(cuda_device)
+    batch = 4096
+    buf = TrainBuffers(batch, cuda_device)
+    gen = torch.Generator(device=cuda_device)
+    gen.manual_seed(0)
+    losses = []
+    for k in range(600):
+        idx = torch.randint(0, x.shape[0], (batch,), generator=gen, device=cuda_device)
+        loss = mlp.train_step(xd[idx].contiguous(), td[idx].contiguous(), buf, 3e-3 if k < 400 else 5e-4)
+        if k % 50 == 0 or k == 599:
+            losses.append(loss.item() / (3 * batch))
+    mlp.check_error()
+    assert losses[-1] < 0.1 * losses[0], losses
