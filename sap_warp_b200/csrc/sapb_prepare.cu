@@ -2,8 +2,9 @@
 //
 // Two launches per step:
 //   scatter_contacts_kernel: each flat contact claims a slot in its world
-//     (atomic, arrival order, like _scatter_sap_contacts_to_env_direct,
-//     sim/contact_jacobian.py:404-562);
+//     (atomic, like _scatter_sap_contacts_to_env_direct,
+//     sim/contact_jacobian.py:404-562); the world's CTA then re-ranks its
+//     slots by flat contact index, so slot order is deterministic;
 //   prepare_world_kernel: one CTA per world runs forward kinematics with
 //     velocities and bias accelerations, body dynamics, the reverse force
 //     pass, body Jacobians, A = sum_b J_b^T I_b J_b + armature, the free-motion
@@ -438,6 +439,21 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   const int total = P.env_count[e];
   const int cc = total < C ? total : C;
   if (tid == 0 && P.out.contact_count) P.out.contact_count[e] = total;
+  // Canonical slot order: the slots the scatter claimed in arrival order are
+  // re-ranked by flat contact index (distinct), so an untruncated world's
+  // slots follow the flat buffer's order on every step.
+  {
+    int* tmp = conint;  // 2*C ints, free until the rows below use them
+    for (int c = tid; c < cc; c += kPrepNT) tmp[c] = P.env_src[(size_t)e * C + c];
+    __syncthreads();
+    for (int c = tid; c < cc; c += kPrepNT) {
+      const int v = tmp[c];
+      int rank = 0;
+      for (int j = 0; j < cc; ++j) rank += tmp[j] < v ? 1 : 0;
+      P.env_src[(size_t)e * C + rank] = v;
+    }
+    __syncthreads();
+  }
   for (int c = tid; c < cc; c += kPrepNT) {
     const int src = P.env_src[(size_t)e * C + c];
     const int sh0 = P.in.contact_shape0[src], sh1 = P.in.contact_shape1[src];

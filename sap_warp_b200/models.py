@@ -291,3 +291,36 @@ def contacts_to_torch(c: dict, device, *, with_f64: bool = True) -> SapContacts:
                   rigid_contact_margin0d=t(c["margin0d"], torch.float64),
                   rigid_contact_margin1d=t(c["margin1d"], torch.float64))
     return SapContacts(**kw)
+
+
+def rollout_scene(kind: str, worlds: int, seed: int, device, *, contacts=(8, 32), qd_std: float = 0.5,
+                  phi0_range=(-2.0e-3, 0.0), mu_range=(0.3, 1.0), stiffness: float = 1.0e5, tau_d: float = 0.01,
+                  tilt: float = 0.1, dt: float = 2.0e-3):
+    """A batch of `worlds` copies of `kind` with random poses, joint
+    velocities ~ N(0, qd_std) and C ~ U{contacts} body-vs-ground point
+    contacts per world on the distal half of the bodies, phi0 ~ U[phi0_range]
+    at the start, pair stiffness `stiffness`, pair dissipation time `tau_d`.
+    Body poses come from one free-motion pass on the device.  Returns
+    (model, state, control, contacts (SapContacts), host contact dict)."""
+    from .runtime import SapContacts, SapControl, SapState
+    from .solver import SapContactJacobian
+
+    rng = np.random.default_rng(seed)
+    tpl = world_template(kind, rng)
+    g = replicate(tpl, worlds, rng, mu_range=mu_range, stiffness=stiffness, tau_d=0.5 * tau_d)
+    q = random_joint_q(tpl, rng, worlds)
+    n, B = tpl["dofs_per_world"], tpl["bodies_per_world"]
+    model = to_model(tpl, g, q, device)
+    qd = rng.normal(scale=qd_std, size=(worlds, n))
+    state = SapState(joint_q=torch.as_tensor(q.reshape(-1), dtype=torch.float64, device=device),
+                     joint_qd=torch.as_tensor(qd.reshape(-1), dtype=torch.float64, device=device),
+                     body_q=model.body_q.clone(),
+                     body_f=torch.zeros(model.body_count, 6, dtype=torch.float64, device=device))
+    control = SapControl(joint_f=torch.zeros(model.joint_dof_count, dtype=torch.float64, device=device))
+    cj = SapContactJacobian(model, max_rigid_contact=1, fallback_tau_d=0.0)
+    cj.compute(state, SapContacts(), control=control, dt=dt)
+    bq = cj.body_q_sap.reshape(worlds, B, 7).cpu().numpy()
+    counts = rng.integers(contacts[0], contacts[1] + 1, size=worlds)
+    con = ground_contacts(rng, bq[..., :3], bq[..., 3:], counts, bodies_from=B // 2, phi0_range=phi0_range,
+                          tilt=tilt, capacity=int(counts.sum()))
+    return model, state, control, contacts_to_torch(con, device), con

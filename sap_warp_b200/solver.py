@@ -11,6 +11,7 @@ no allocation), so a whole step can be captured in a CUDA graph.
 from __future__ import annotations
 
 import ctypes
+import os
 import warnings
 from dataclasses import dataclass
 
@@ -443,6 +444,7 @@ class SapContactSolve:
         self.converged_env = z(W, dt=I32)
         self.ls_status = z(W, dt=I32)
         self.grad_norm = z(W)
+        self.warm_start_accepted_env = z(W, dt=I32)
         self.dt_world = z(W)
         ws = int(load().sapb_contact_solve_workspace_size(W, n, C))
         self.workspace = torch.zeros(max(ws, 16), dtype=torch.uint8, device=dev)
@@ -452,6 +454,7 @@ class SapContactSolve:
         out.cost, out.newton_iterations = _ptr(self.cost), _ptr(self.newton_iterations_env)
         out.line_search_iterations, out.converged = _ptr(self.ls_iterations_total), _ptr(self.converged_env)
         out.status, out.grad_norm = _ptr(self.ls_status), _ptr(self.grad_norm)
+        out.warm_start_accepted = _ptr(self.warm_start_accepted_env)
         self.outputs = out
         self.dof = None
         if v.has_pd or v.has_limits:
@@ -486,8 +489,11 @@ class SapContactSolve:
               line_search_max_iterations: int = 40, armijo_c: float = 1.0e-4, rho: float = 0.8,
               line_search_relative_slop: float | None = None, line_search_variant: str = "monotone_decay",
               collect_iteration_stats: bool = True, check_line_search_errors: bool = True,
-              graph_conditional: bool = True, static_loop: bool = False) -> SapContactSolveResult:
-        """sim/contact_solve.py:6129-6285"""
+              graph_conditional: bool = True, static_loop: bool = False,
+              gamma0: torch.Tensor | None = None) -> SapContactSolveResult:
+        """sim/contact_solve.py:6129-6285.  gamma0 (W, C, 3) FP64: learned
+        starting impulses (no counterpart in the reference), tried against the
+        plain start on the cost."""
         variant = normalize_sap_line_search_mode(line_search_variant)
         if not bool(graph_conditional):
             raise ValueError("SapContactSolve only supports graph_conditional=True; "
@@ -531,6 +537,10 @@ class SapContactSolve:
                 raise TypeError("v_guess must be a contiguous float64 tensor (it is written back)")
             P.v_guess = _ptr(v_guess)
             P.v_guess_active = _ptr(v_guess_active)
+        if gamma0 is not None:
+            if gamma0.dtype != F64 or not gamma0.is_contiguous() or gamma0.numel() < W * P.max_contacts * 3:
+                raise TypeError("gamma0 must be a contiguous float64 (W, C, 3) tensor")
+            P.gamma0 = _ptr(gamma0)
         if self.dof is not None:
             self._jq = _f64(state.joint_q)
             self.dof.joint_q = _ptr(self._jq)
@@ -576,7 +586,20 @@ class SolverSAP:
                  check_line_search_errors: bool = False, graph_conditional: bool = True,
                  static_substep: bool = False, static_substep_iterations: int = 8,
                  static_substep_line_search_iterations: int = 6, position_integration: str | None = None,
-                 hessian_precision: str | None = None):
+                 hessian_precision: str | None = None, warm_start: str = "previous_velocity",
+                 learned_warm_start=None):
+        """Keyword arguments of the reference's SolverSAP (sim/solver_sap.py:
+        749-791) plus: hessian_precision ("fp64" / "fp32": J^T G J assembly and
+        factorization precision; the gradient, cost, line search and
+        convergence test stay FP64); warm_start, one of
+          "previous_velocity"  the reference's: start from the last solution;
+          "previous_impulses"  also try v* + A^-1 J^T gamma_prev;
+          "learned"            also try v* + A^-1 J^T gamma0, gamma0 from the
+                               per-contact network (learned_warm_start: a
+                               LearnedWarmStart, a weights path, or None for
+                               the packaged weights);
+        a candidate start replaces the previous-velocity start only if its
+        cost is lower, and Newton always runs to the same tolerance."""
         view = _ModelView(model)
         preset = dict(_CONTACT_PRESET_KWARGS[_normalize_contact_preset_variant(contact_preset_variant)])
         self.contact_preset_variant = _normalize_contact_preset_variant(contact_preset_variant)
@@ -646,6 +669,21 @@ class SolverSAP:
         dev = view.device
         self._v_guess_active = torch.zeros(1, dtype=I32, device=dev)
         self._q_out_tmp = torch.zeros(int(model.joint_coord_count), dtype=F64, device=dev)
+        self.warm_start = str(warm_start).strip().lower().replace("-", "_")
+        if self.warm_start not in ("previous_velocity", "previous_impulses", "learned"):
+            raise ValueError("warm_start must be 'previous_velocity', 'previous_impulses' or 'learned', "
+                             f"got {warm_start!r}.")
+        self.learned_warm_start = None
+        if self.warm_start == "learned":
+            from .warmstart import DEFAULT_WEIGHTS, LearnedWarmStart
+
+            lw = learned_warm_start
+            if lw is None or isinstance(lw, (str, os.PathLike)):
+                lw = LearnedWarmStart.load(DEFAULT_WEIGHTS if lw is None else str(lw), dev)
+            self.learned_warm_start = lw
+        C = self.max_rigid_contact
+        self._gamma_prev = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
+        self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
         self.reset_runtime_state()
 
     @property
@@ -671,6 +709,8 @@ class SolverSAP:
         self.last_line_search_iterations = 0
         self.last_converged = True
         self._v_guess_active.zero_()
+        if hasattr(self, "_gamma_prev"):
+            self._gamma_prev.zero_()
         self.last_contacts = None
         self.last_contact_jacobian_result = None
         self.last_contact_solve_result = None
@@ -700,9 +740,22 @@ class SolverSAP:
         else:
             iters, ls_iters = self.max_iterations, self.line_search_max_iterations
         v0 = self.contact_jacobian._qd
+        gamma0 = None
+        if self.warm_start == "previous_impulses":
+            gamma0 = self._gamma_prev
+        elif self.warm_start == "learned":
+            self._normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
+            gamma0 = self.learned_warm_start.predict(
+                num_envs=self.view.W, dof_per_env=self.view.n, max_contacts=self.max_rigid_contact,
+                normal_up=self._normal_up, gamma_prev=self._gamma_prev, contact_count=cr.contact_env_count,
+                dynamics_matrix=cr.dynamics_matrix_env, jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0,
+                w_eff=cr.contact_env_w_eff, mu=cr.contact_env_mu, stiffness=cr.contact_env_stiffness,
+                tau_d=cr.contact_env_tau_d, v_star=self.contact_jacobian.v_star, v0=self.contact_jacobian.v_star,
+                dt=self.contact_jacobian.dt_world)
         sr = self.contact_solve.solve(
             cr, state_in, control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
-            v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, max_iterations=iters,
+            v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, gamma0=gamma0,
+            max_iterations=iters,
             optimality_abs_tol=self.optimality_abs_tol, optimality_rel_tol=self.optimality_rel_tol,
             cost_abs_tol=self.cost_abs_tol, cost_rel_tol=self.cost_rel_tol, line_search_max_iterations=ls_iters,
             armijo_c=self.armijo_c, rho=self.rho, line_search_relative_slop=self.line_search_relative_slop,
@@ -723,6 +776,8 @@ class SolverSAP:
         if state_out.body_f is not None and state_in.body_f is not None and state_out.body_f is not state_in.body_f:
             state_out.body_f.copy_(state_in.body_f)
         self._v_guess_active.fill_(1)  # warm start from this step's solution (sim/solver_sap.py:1441-1451)
+        if self.warm_start != "previous_velocity":
+            self._gamma_prev.copy_(sr.contact_gamma)
         self.last_contact_jacobian_result = cr
         self.last_contact_solve_result = sr
         self.last_solve_iterations = -1
