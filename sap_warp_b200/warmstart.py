@@ -294,6 +294,47 @@ def solver_dataset(problems, device, line_search_variant: str = "armijo_decay"):
     return torch.cat(raws), torch.cat(us)
 
 
+def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every: int = 1,
+                    hessian_precision: str = "fp64"):
+    """(raw inputs (N, 12), targets u = w_eff * gamma (N, 3)) of the live
+    contacts along SolverSAP trajectories (reference warm start, FP64): at
+    step k the inputs carry gamma_prev = the impulses of step k-1 in the same
+    slot (slot order is canonical, so a persistent contact keeps its slot),
+    the targets are step k's converged impulses.  Every `every`-th step."""
+    from . import models
+    from .runtime import SapState
+    from .solver import SolverSAP
+
+    raws, us = [], []
+    for seed in seeds:
+        model, state, control, con, _ = models.rollout_scene(kind, worlds, seed, device)
+        solver = SolverSAP(model, max_rigid_contact=32, hessian_precision=hessian_precision)
+        other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(),
+                         body_q=state.body_q.clone(), body_f=state.body_f.clone())
+        W, n, C = solver.view.W, solver.view.n, solver.max_rigid_contact
+        gamma_prev = torch.zeros(W, C, 3, dtype=F64, device=device)
+        normal_up = torch.zeros(W, C, dtype=F64, device=device)
+        for k in range(steps):
+            solver.step(state, other, control, con, 2.0e-3)
+            if k % every == 0:
+                cr = solver.last_contact_jacobian_result
+                normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
+                arrays = dict(contact_count=cr.contact_env_count, dynamics_matrix=cr.dynamics_matrix_env,
+                              jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff,
+                              mu=cr.contact_env_mu, stiffness=cr.contact_env_stiffness, tau_d=cr.contact_env_tau_d,
+                              v_star=solver.contact_jacobian.v_star, v0=solver.contact_jacobian.v_star,
+                              dt=solver.contact_jacobian.dt_world)
+                raw = raw_features(arrays, W, n, C, normal_up=normal_up, gamma_prev=gamma_prev)
+                cnt = cr.contact_env_count.clamp(max=C)
+                live = (torch.arange(C, device=device)[None, :] < cnt[:, None]).reshape(-1)
+                u = (cr.contact_env_w_eff[..., None] * solver.contact_solve.contact_gamma).reshape(-1, 3)
+                raws.append(raw[live])
+                us.append(u[live].to(F32))
+            gamma_prev.copy_(solver.contact_solve.contact_gamma)
+            state, other = other, state
+    return torch.cat(raws), torch.cat(us)
+
+
 def train(mlp: WarmStartMLP, raw: torch.Tensor, u: torch.Tensor, norm: FeatureNorm, steps: int = 4000,
           batch: int = 8192, lr: float = 2e-3, lr_final: float = 5e-5, seed: int = 0, log_every: int = 200):
     """Adam on the standardised targets with a cosine learning-rate decay;
@@ -337,14 +378,20 @@ def _main():
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--humanoid-seeds", type=int, default=25)
-    ap.add_argument("--quadruped-seeds", type=int, default=10)
+    ap.add_argument("--humanoid-seeds", type=int, default=4)
+    ap.add_argument("--quadruped-seeds", type=int, default=2)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--rollout-steps", type=int, default=80)
+    ap.add_argument("--rollout-every", type=int, default=2)
     a = ap.parse_args()
     dev = torch.device("cuda", 0)
     t0 = time.time()
-    raw, u = solver_dataset(default_training_problems(range(100, 100 + a.humanoid_seeds),
-                                                      range(200, 200 + a.quadruped_seeds)), dev)
+    parts = [rollout_dataset("humanoid", 4096, range(100, 100 + a.humanoid_seeds), a.rollout_steps, dev,
+                             every=a.rollout_every),
+             rollout_dataset("quadruped", 4096, range(200, 200 + a.quadruped_seeds), a.rollout_steps, dev,
+                             every=a.rollout_every)]
+    raw = torch.cat([p[0] for p in parts])
+    u = torch.cat([p[1] for p in parts])
     t1 = time.time()
     norm = FeatureNorm.from_data(raw.cpu().numpy(), u.cpu().numpy())
     mlp = WarmStartMLP(dev, seed=a.seed)
