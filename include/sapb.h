@@ -268,7 +268,10 @@ size_t sapb_prepare_workspace_size(const sapb_model_desc* model, int32_t max_con
  * with _compute_sap_core :2094-2178), then the per-world contact slots, frames,
  * phi0, combined materials, Jacobian rows and weights
  * (SapContactJacobian.compute, sim/contact_jacobian.py:1649-1985).  Slots are
- * taken in arrival order like the reference's atomic scatter (:470). */
+ * claimed atomically like the reference's scatter (:470), then ordered by
+ * flat contact index within each world, so an untruncated world's slot order
+ * is the flat buffer's.  At most 64 bodies and 128 DOFs per world
+ * (SAPB_ERR_UNSUPPORTED otherwise). */
 int32_t sapb_free_motion_contacts(const sapb_model_desc* model, const sapb_step_inputs* in,
                                   const sapb_prepare_options* opts, const sapb_prepare_outputs* out,
                                   void* workspace, size_t workspace_bytes, void* stream);
@@ -333,8 +336,9 @@ const char* sapb_last_error(void);
  * Inputs of a contact slot (raw, before normalisation): phi0; J_c v* in the
  * contact frame (t1, t2, n); the world-up component of the contact normal;
  * mu; log10(stiffness); tau_d; dt; w_eff * gamma_prev (t1, t2, n).  The
- * output y maps to u = y * output_scale + output_shift (velocity units) and
- * gamma0 = u / w_eff, projected onto the friction cone. */
+ * output y maps to a correction u = y * output_scale + output_shift
+ * (velocity units) of the previous impulses: gamma0 = gamma_prev + u / w_eff
+ * (gamma_prev = 0 when not given), projected onto the friction cone. */
 #define SAPB_MLP_INPUTS 12
 #define SAPB_MLP_INPUTS_PADDED 16
 #define SAPB_MLP_HIDDEN 128
@@ -393,9 +397,11 @@ int32_t sapb_mlp_error(void* stream);
 int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const double* normal_up,
                                 const double* gamma_prev, const sapb_warmstart_norm* norm, double tau_fallback,
                                 uint16_t* features, float* raw, void* stream);
-/* gamma0 [E,C,3] from the network output mlp_out [E*C,3]. */
+/* gamma0 [E,C,3] from the network output mlp_out [E*C,3] and the previous
+ * step's impulses gamma_prev [E,C,3] (NULL: 0). */
 int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float* mlp_out,
-                                const sapb_warmstart_norm* norm, double* gamma0, void* stream);
+                                const double* gamma_prev, const sapb_warmstart_norm* norm, double* gamma0,
+                                void* stream);
 
 #ifdef __cplusplus
 }

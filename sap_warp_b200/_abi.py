@@ -284,7 +284,7 @@ EXPORTS = {
     "sapb_warmstart_features": (
         C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), C.c_double, _p, _p, _p]
     ),
-    "sapb_warmstart_impulses": (C.c_int32, [C.POINTER(ContactProblem), _p, C.POINTER(WarmstartNorm), _p, _p]),
+    "sapb_warmstart_impulses": (C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), _p, _p]),
 }
 
 

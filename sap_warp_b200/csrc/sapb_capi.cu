@@ -155,6 +155,11 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inpu
     sapb::set_last_error("sapb_free_motion_contacts: missing contact output array");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
+  if (m->bodies_per_world > 64 || m->dofs_per_world > 128) {
+    sapb::set_last_error("sapb_free_motion_contacts: at most 64 bodies and 128 DOFs per world (got %d, %d)",
+                         m->bodies_per_world, m->dofs_per_world);
+    return SAPB_ERR_UNSUPPORTED;
+  }
   const size_t smem = sapb::prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, o->max_contacts);
   if (smem > sapb::kMaxSmemPerBlock) {
     sapb::set_last_error("sapb_free_motion_contacts: world too large for one block (%zu bytes of shared memory)",

@@ -18,8 +18,9 @@
 //              BF16 operand images the forward reads.
 //
 // plus the two domain kernels around it: per-contact features from the
-// stage-2 problem, and the map from the network output to starting impulses
-// gamma0 projected onto the friction cone (the solve maps gamma0 to
+// stage-2 problem, and the map from the network output (a correction to the
+// previous step's impulses, when given) to starting impulses gamma0
+// projected onto the friction cone (the solve maps gamma0 to
 // v0 = v* + A^-1 J^T gamma0).  The reference warm-starts from the previous
 // step's velocity only (sim/solver_sap.py:1441-1451); this network has no
 // counterpart there.
@@ -635,6 +636,7 @@ __global__ void features_kernel(const FeatParams P) {
 struct ImpulseParams {
   sapb_contact_problem p;
   const float* y;
+  const double* gamma_prev;  // residual base (NULL: 0)
   sapb_warmstart_norm norm;
   double* gamma0;
 };
@@ -650,8 +652,10 @@ __global__ void impulses_kernel(const ImpulseParams P) {
     if (c < count) {
       const double w = fmax(P.p.w_eff[s], 1.0e-12);
 #pragma unroll
-      for (int j = 0; j < 3; ++j)
+      for (int j = 0; j < 3; ++j) {
         g[j] = ((double)P.y[3 * s + j] * P.norm.output_scale[j] + P.norm.output_shift[j]) / w;
+        if (P.gamma_prev) g[j] += P.gamma_prev[3 * s + j];
+      }
       // onto the friction cone: gamma_n >= 0, |gamma_t| <= mu gamma_n
       g[2] = fmax(g[2], 0.0);
       const double tm = sqrt(g[0] * g[0] + g[1] * g[1]);
@@ -860,7 +864,8 @@ int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const doubl
 }
 
 int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float* mlp_out,
-                                const sapb_warmstart_norm* norm, double* gamma0, void* stream) {
+                                const double* gamma_prev, const sapb_warmstart_norm* norm, double* gamma0,
+                                void* stream) {
   if (!problem || !mlp_out || !norm || !gamma0 || problem->num_envs < 0 || problem->max_contacts < 0) {
     set_last_error("sapb_warmstart_impulses: invalid argument");
     return SAPB_ERR_INVALID_ARGUMENT;
@@ -874,6 +879,7 @@ int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float
   ImpulseParams P;
   P.p = *problem;
   P.y = mlp_out;
+  P.gamma_prev = gamma_prev;
   P.norm = *norm;
   P.gamma0 = gamma0;
   long blocks = (slots + 255) / 256;

@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstring>
 
+#include "sapb_device.cuh"
 #include "sapb_internal.h"
 #include "sapb_spatial.cuh"
 
@@ -35,29 +36,42 @@ struct PrepParams {
 
 __host__ __device__ inline size_t prep_align(size_t x) { return (x + 15) / 16 * 16; }
 
+// Shared-memory layout of one world (doubles unless noted).  Spatial
+// quantities are Plucker vectors about the world origin in world axes
+// ([angular; linear]), so velocities, forces and inertias of different bodies
+// add without shifts.
 struct PrepLayout {
-  size_t body, S, Jb, H, K, con, conint, bj, total;
+  size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, dbody, total;
 };
 
 __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C) {
   PrepLayout L;
+  const size_t Cc = (size_t)(C > 0 ? C : 1);
   size_t o = 0;
-  L.body = o;  // pos3 quat4 V6 Ab6 fb6 ft6 I6[36] = 67 per body
-  o = prep_align(o + sizeof(double) * 67 * (size_t)B);
-  L.S = o;  // S[n][6], tau[n], vdot[n]
-  o = prep_align(o + sizeof(double) * 8 * (size_t)n);
-  L.Jb = o;
-  o = prep_align(o + sizeof(double) * 6 * (size_t)B * n);
-  L.H = o;
-  o = prep_align(o + sizeof(double) * (size_t)n * n);
-  L.K = o;
-  o = prep_align(o + sizeof(double) * 6 * (size_t)n);
-  L.con = o;  // per contact: xj0 3, xj1 3, p0 3, p1 3, F 9 = 21
-  o = prep_align(o + sizeof(double) * 21 * (size_t)(C > 0 ? C : 1));
-  L.conint = o;  // lb0, lb1
-  o = prep_align(o + sizeof(int) * 2 * (size_t)(C > 0 ? C : 1));
-  L.bj = o;  // body -> global joint
-  o = prep_align(o + sizeof(int) * (size_t)B);
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = prep_align(o + bytes);
+    return at;
+  };
+  L.pose = take(sizeof(double) * 8 * B);    // p 3, q 4 (pointer-jumping buffer A)
+  L.pose2 = take(sizeof(double) * 8 * B);   // buffer B
+  L.fm = take(sizeof(double) * 8 * B);      // X_FM of the body's joint
+  L.vj = take(sizeof(double) * 6 * B);      // joint velocity S q_dot
+  L.cb = take(sizeof(double) * 6 * B);      // joint bias acceleration
+  L.vb = take(sizeof(double) * 6 * B);      // body velocity
+  L.fb = take(sizeof(double) * 6 * B);      // body force
+  L.ib = take(sizeof(double) * 10 * B);     // inertia: m, h = m c, I_O (xx yy zz xy xz yz)
+  L.fs = take(sizeof(double) * 16 * B);     // subtree force 6 + composite inertia 10
+  L.S = take(sizeof(double) * 6 * n);       // motion subspace columns
+  L.F = take(sizeof(double) * 6 * n);       // composite inertia times S
+  L.vec = take(sizeof(double) * 4 * n);     // tau, vdot, diag(A), 1/d
+  L.H = take(sizeof(double) * (size_t)n * n);
+  L.con = take(sizeof(double) * 21 * Cc);   // per contact: x0 3, x1 3, -, -, frame 9
+  L.conint = take(sizeof(int) * 2 * Cc);    // local bodies lb0, lb1
+  L.anc = take(sizeof(uint64_t) * 2 * B);   // ancestor-or-self masks (two buffers)
+  L.jmp = take(sizeof(int) * 2 * B);        // pointer-jumping parents (two buffers)
+  L.bj = take(sizeof(int) * B);             // joint (global index) of each body, -1
+  L.dbody = take(sizeof(int) * n);          // body of each DOF
   L.total = o;
   return L;
 }
@@ -143,282 +157,384 @@ __device__ inline double shape_tau(const PrepParams& P, int sh) {
   return v;
 }
 
+// Spatial helpers about the world origin.
+__device__ __forceinline__ Sv crm(Sv a, Sv b) {  // motion x motion
+  return Sv{cross(a.w, b.w), cross(a.w, b.v) + cross(a.v, b.w)};
+}
+__device__ __forceinline__ Sv crf(Sv a, Sv f) {  // motion x* force
+  return Sv{cross(a.w, f.w) + cross(a.v, f.v), cross(a.w, f.v)};
+}
+// Inertia (m, h = m c, I_O symmetric xx yy zz xy xz yz) times a motion vector.
+__device__ __forceinline__ Sv inertia_times(const double* I, Sv m) {
+  const V3 h = v3(I[1], I[2], I[3]);
+  const V3 w = m.w;
+  const V3 Iw = v3(I[4] * w.x + I[7] * w.y + I[8] * w.z, I[7] * w.x + I[5] * w.y + I[9] * w.z,
+                   I[8] * w.x + I[9] * w.y + I[6] * w.z);
+  return Sv{Iw + cross(h, m.v), I[0] * m.v - cross(h, w)};
+}
+__device__ __forceinline__ Xf pose_load(const double* p) {
+  return Xf{v3(p[0], p[1], p[2]), Q4{p[3], p[4], p[5], p[6]}};
+}
+__device__ __forceinline__ void pose_store(double* p, Xf x) {
+  p[0] = x.p.x;
+  p[1] = x.p.y;
+  p[2] = x.p.z;
+  p[3] = x.q.x;
+  p[4] = x.q.y;
+  p[5] = x.q.z;
+  p[6] = x.q.w;
+}
+
+// One CTA per world.  The tree recursions of the reference's free motion
+// (sim/free_motion.py:412-1249, 1804-2178) become: poses by pointer jumping
+// over the parent links (log depth rounds), per-joint motion subspaces and
+// joint velocities in parallel, body velocities / bias accelerations as sums
+// over ancestor masks, subtree forces and composite inertias as sums over
+// descendants, A by the composite-rigid-body pairs H_ij = S_j . (I^c S_i),
+// then a one-barrier-per-column LDL^T and warp-parallel triangular solves.
+// The contact rows are J_c = R_WC (v_O + w x x_c) of the ancestor DOFs' S
+// columns (sim/contact_jacobian.py:404-562).
 __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31;
   const int e = blockIdx.x;
   const int B = P.m.bodies_per_world, n = P.m.dofs_per_world, C = P.o.max_contacts;
-  const int Jw = P.m.joints_per_world, Aw = P.m.articulations_per_world;
+  const int Jw = P.m.joints_per_world;
   const PrepLayout L = prep_layout(B, n, C);
-  double* body = reinterpret_cast<double*>(smem + L.body);
+  double* poseA = reinterpret_cast<double*>(smem + L.pose);
+  double* poseB = reinterpret_cast<double*>(smem + L.pose2);
+  double* fm = reinterpret_cast<double*>(smem + L.fm);
+  double* vj = reinterpret_cast<double*>(smem + L.vj);
+  double* cbias = reinterpret_cast<double*>(smem + L.cb);
+  double* vb = reinterpret_cast<double*>(smem + L.vb);
+  double* fb = reinterpret_cast<double*>(smem + L.fb);
+  double* ib = reinterpret_cast<double*>(smem + L.ib);
+  double* fs = reinterpret_cast<double*>(smem + L.fs);
   double* S = reinterpret_cast<double*>(smem + L.S);
-  double* tau = S + 6 * n;
+  double* Fi = reinterpret_cast<double*>(smem + L.F);
+  double* tau = reinterpret_cast<double*>(smem + L.vec);
   double* vdot = tau + n;
-  double* Jb = reinterpret_cast<double*>(smem + L.Jb);
+  double* adiag = tau + 2 * n;
+  double* dinv = tau + 3 * n;
   double* H = reinterpret_cast<double*>(smem + L.H);
-  double* K = reinterpret_cast<double*>(smem + L.K);
   double* con = reinterpret_cast<double*>(smem + L.con);
   int* conint = reinterpret_cast<int*>(smem + L.conint);
+  uint64_t* ancA = reinterpret_cast<uint64_t*>(smem + L.anc);
+  uint64_t* ancB = ancA + B;
+  int* jmpA = reinterpret_cast<int*>(smem + L.jmp);
+  int* jmpB = jmpA + B;
   int* bj = reinterpret_cast<int*>(smem + L.bj);
-  auto POS = [&](int b) { return body + 67 * b; };
-  auto QUAT = [&](int b) { return body + 67 * b + 3; };
-  auto VEL = [&](int b) { return body + 67 * b + 7; };
-  auto ACC = [&](int b) { return body + 67 * b + 13; };
-  auto FB = [&](int b) { return body + 67 * b + 19; };
-  auto FT = [&](int b) { return body + 67 * b + 25; };
-  auto I6 = [&](int b) { return body + 67 * b + 31; };
+  int* dbody = reinterpret_cast<int*>(smem + L.dbody);
   const int j0 = e * Jw, b0g = e * B, d0 = e * n;
+  const double* q = P.in.joint_q;
+  const double* qd = P.in.joint_qd;
 
+  // ---- topology of this world --------------------------------------------
+  for (int b = tid; b < B; b += kPrepNT) bj[b] = -1;
+  for (int i = tid; i < n; i += kPrepNT) dbody[i] = -1;
   for (int k = tid; k < 6 * n; k += kPrepNT) S[k] = 0.0;
-  for (int k = tid; k < 6 * B * n; k += kPrepNT) Jb[k] = 0.0;
+  __syncthreads();
   for (int jl = tid; jl < Jw; jl += kPrepNT) {
-    const int cb = P.m.joint_child[j0 + jl] - b0g;
-    if (cb >= 0 && cb < B) bj[cb] = j0 + jl;
+    const int j = j0 + jl;
+    const int cb = P.m.joint_child[j] - b0g;
+    if (cb < 0 || cb >= B) continue;
+    bj[cb] = j;
+    const int dl = P.m.joint_qd_start[j] - d0;
+    const int dim = P.m.joint_dof_dim[2 * j] + P.m.joint_dof_dim[2 * j + 1];
+    for (int k = 0; k < dim; ++k)
+      if (dl + k >= 0 && dl + k < n) dbody[dl + k] = cb;
   }
   __syncthreads();
 
-  // ---- forward kinematics, velocities, bias accelerations -----------------
-  // One thread per articulation; joints in index order (parents first).
-  // sim/free_motion.py:412-530 with sim/sap_helpers.py:1164-1433.
-  for (int a = tid; a < Aw; a += kPrepNT) {
-    const int ja = P.m.articulation_start[e * Aw + a], jb = P.m.articulation_start[e * Aw + a + 1];
-    for (int j = ja; j < jb; ++j) {
+  // ---- local transforms X_{parent body, body} = X_p X_FM(q) X_c^-1 ---------
+  // (sim/sap_helpers.py:1164-1243)
+  for (int b = tid; b < B; b += kPrepNT) {
+    const int j = bj[b];
+    Xf T{v3(0, 0, 0), qident()}, X_FM{v3(0, 0, 0), qident()};
+    int parent = -1;
+    if (j >= 0) {
       const int jt = P.m.joint_type[j];
-      const int pb = P.m.joint_parent[j] >= 0 ? P.m.joint_parent[j] - b0g : -1;
-      const int cb = P.m.joint_child[j] - b0g;
-      const int qs = P.m.joint_q_start[j], ds = P.m.joint_qd_start[j], dl = ds - d0;
-      const double* q = P.in.joint_q;
-      const double* qd = P.in.joint_qd;
-      const Xf Xp = xf_load(P.m.joint_X_p + 7 * (size_t)j);
-      const Xf Xc = xf_load(P.m.joint_X_c + 7 * (size_t)j);
-      Xf X_WF = Xp;
-      if (pb >= 0) X_WF = xf_compose(Xf{load3(POS(pb)), Q4{QUAT(pb)[0], QUAT(pb)[1], QUAT(pb)[2], QUAT(pb)[3]}}, Xp);
-      Xf X_FM{v3(0, 0, 0), qident()};
-      Sv V_FM = sv_zero();
+      const int qs = P.m.joint_q_start[j], ds = P.m.joint_qd_start[j];
       if (jt == SAPB_JOINT_PRISMATIC) {
-        const V3 ax = load3(P.m.joint_axis + 3 * (size_t)ds);
-        X_FM.p = q[qs] * ax;
-        V_FM = sv(v3(0, 0, 0), qd[ds] * ax);
+        X_FM.p = q[qs] * load3(P.m.joint_axis + 3 * (size_t)ds);
       } else if (jt == SAPB_JOINT_REVOLUTE) {
-        const V3 ax = load3(P.m.joint_axis + 3 * (size_t)ds);
-        X_FM.q = qaxis_angle(ax, q[qs]);
-        V_FM = sv(qd[ds] * ax, v3(0, 0, 0));
+        X_FM.q = qaxis_angle(load3(P.m.joint_axis + 3 * (size_t)ds), q[qs]);
       } else if (jt == SAPB_JOINT_BALL) {
         X_FM.q = Q4{q[qs], q[qs + 1], q[qs + 2], q[qs + 3]};
-        V_FM = sv(v3(qd[ds], qd[ds + 1], qd[ds + 2]), v3(0, 0, 0));
       } else if (jt == SAPB_JOINT_FREE || jt == SAPB_JOINT_DISTANCE) {
         X_FM.p = v3(q[qs], q[qs + 1], q[qs + 2]);
         X_FM.q = Q4{q[qs + 3], q[qs + 4], q[qs + 5], q[qs + 6]};
-        V_FM = sv(v3(qd[ds], qd[ds + 1], qd[ds + 2]), v3(qd[ds + 3], qd[ds + 4], qd[ds + 5]));
       }
-      const Xf X_WM = xf_compose(X_WF, X_FM);
-      const Xf X_MB = xf_inverse(Xc);
-      const Xf X_WB = xf_compose(X_WM, X_MB);
-      const V3 p_MoBo_F = qrot(qnormalize(X_FM.q), X_MB.p);
-      const Q4 R_WF = qnormalize(X_WF.q);
-      // motion subspace columns
-      if (jt == SAPB_JOINT_PRISMATIC) {
-        sv_store(S + 6 * dl, mobilizer_velocity_to_body(R_WF, p_MoBo_F,
-                                                        sv(v3(0, 0, 0), load3(P.m.joint_axis + 3 * (size_t)ds))));
-      } else if (jt == SAPB_JOINT_REVOLUTE) {
-        const V3 ax = load3(P.m.joint_axis + 3 * (size_t)ds);
-        sv_store(S + 6 * dl, sv(qrot(R_WF, ax), qrot(R_WF, cross(ax, p_MoBo_F))));
-      } else if (jt == SAPB_JOINT_BALL || jt == SAPB_JOINT_FREE || jt == SAPB_JOINT_DISTANCE) {
-        const int cnt = jt == SAPB_JOINT_BALL ? 3 : 6;
-        for (int k = 0; k < cnt; ++k) {
-          double u[6] = {0, 0, 0, 0, 0, 0};
-          u[k] = 1.0;
-          sv_store(S + 6 * (dl + k), mobilizer_velocity_to_body(R_WF, p_MoBo_F, sv_load(u)));
-        }
-      }
-      const Sv V_PB = mobilizer_velocity_to_body(R_WF, p_MoBo_F, V_FM);
-      const Sv A_PB = mobilizer_accel_bias_to_body(R_WF, p_MoBo_F, V_FM.w);
-      store3(POS(cb), X_WB.p);
-      QUAT(cb)[0] = X_WB.q.x;
-      QUAT(cb)[1] = X_WB.q.y;
-      QUAT(cb)[2] = X_WB.q.z;
-      QUAT(cb)[3] = X_WB.q.w;
-      if (pb >= 0) {
-        const Sv Vp = sv_load(VEL(pb)), Ap = sv_load(ACC(pb));
-        const V3 p_PB = X_WB.p - load3(POS(pb));
-        sv_store(VEL(cb), compose_velocity(Vp, p_PB, V_PB));
-        sv_store(ACC(cb), compose_acceleration(Ap, Vp, p_PB, V_PB, A_PB));
-      } else {
-        sv_store(VEL(cb), V_PB);
-        sv_store(ACC(cb), A_PB);
-      }
+      T = xf_compose(xf_compose(xf_load(P.m.joint_X_p + 7 * (size_t)j), X_FM),
+                     xf_inverse(xf_load(P.m.joint_X_c + 7 * (size_t)j)));
+      parent = P.m.joint_parent[j] >= 0 ? P.m.joint_parent[j] - b0g : -1;
+      if (parent >= B) parent = -1;
     }
+    pose_store(poseA + 8 * b, T);
+    pose_store(fm + 8 * b, X_FM);
+    jmpA[b] = parent;
+    ancA[b] = 1ull << b;
   }
   __syncthreads();
+  // ---- world poses and ancestor masks by pointer jumping ------------------
+  double* cur = poseA;
+  double* nxt = poseB;
+  int* jc = jmpA;
+  int* jn = jmpB;
+  uint64_t* ac = ancA;
+  uint64_t* an = ancB;
+  for (int round = 0; round < 8; ++round) {
+    int active = 0;
+    for (int b = tid; b < B; b += kPrepNT) {
+      const int J = jc[b];
+      if (J >= 0) {
+        pose_store(nxt + 8 * b, xf_compose(pose_load(cur + 8 * J), pose_load(cur + 8 * b)));
+        jn[b] = jc[J];
+        an[b] = ac[b] | ac[J];
+        active = 1;
+      } else {
+        for (int k = 0; k < 7; ++k) nxt[8 * b + k] = cur[8 * b + k];
+        jn[b] = -1;
+        an[b] = ac[b];
+      }
+    }
+    double* t = cur;
+    cur = nxt;
+    nxt = t;
+    int* tj = jc;
+    jc = jn;
+    jn = tj;
+    uint64_t* ta = ac;
+    ac = an;
+    an = ta;
+    if (!__syncthreads_or(active)) break;
+  }
+  const double* pose = cur;
+  const uint64_t* anc = ac;
 
-  // ---- body dynamics (sim/free_motion.py:680-719, sim/sap_helpers.py:1027-1105)
+  // ---- motion subspaces, joint velocities, body inertias ------------------
+  // S in world-origin coordinates of the reference's mobilizer columns
+  // (sim/sap_helpers.py:1289-1433): revolute [w; p_F x w], prismatic [0; a],
+  // ball [w_k; p_F x w_k], free [w_k; p_M x w_k] and [0; a_k], all axes
+  // rotated by R_WF.
+  const V3 grav = load3(P.m.gravity + 3 * (size_t)e);
   for (int b = tid; b < B; b += kPrepNT) {
-    const Q4 q = qnormalize(Q4{QUAT(b)[0], QUAT(b)[1], QUAT(b)[2], QUAT(b)[3]});
+    const int j = bj[b];
+    Sv vJ = sv_zero(), c = sv_zero();
+    if (j >= 0) {
+      const int jt = P.m.joint_type[j];
+      const int ds = P.m.joint_qd_start[j], dl = ds - d0;
+      const int parent = P.m.joint_parent[j] >= 0 ? P.m.joint_parent[j] - b0g : -1;
+      const Xf X_Wl = (parent >= 0 && parent < B) ? pose_load(pose + 8 * parent) : Xf{v3(0, 0, 0), qident()};
+      const Xf X_WF = xf_compose(X_Wl, xf_load(P.m.joint_X_p + 7 * (size_t)j));
+      const Xf X_WM = xf_compose(X_WF, pose_load(fm + 8 * b));
+      const Q4 R = qnormalize(X_WF.q);
+      auto put = [&](int k, Sv s) {
+        sv_store(S + 6 * (dl + k), s);
+        vJ = vJ + qd[ds + k] * s;
+      };
+      if (jt == SAPB_JOINT_PRISMATIC) {
+        put(0, sv(v3(0, 0, 0), qrot(R, load3(P.m.joint_axis + 3 * (size_t)ds))));
+      } else if (jt == SAPB_JOINT_REVOLUTE) {
+        const V3 w = qrot(R, load3(P.m.joint_axis + 3 * (size_t)ds));
+        put(0, sv(w, cross(X_WF.p, w)));
+      } else if (jt == SAPB_JOINT_BALL) {
+        for (int k = 0; k < 3; ++k) {
+          const V3 w = qrot(R, v3(k == 0, k == 1, k == 2));
+          put(k, sv(w, cross(X_WF.p, w)));
+        }
+      } else if (jt == SAPB_JOINT_FREE || jt == SAPB_JOINT_DISTANCE) {
+        for (int k = 0; k < 3; ++k) {
+          const V3 w = qrot(R, v3(k == 0, k == 1, k == 2));
+          put(k, sv(w, cross(X_WM.p, w)));
+          put(k + 3, sv(v3(0, 0, 0), w));
+        }
+        // the DOFs' own motion: d/dt of p_M x w_k along the relative
+        // translation gives [0; v_rel x w_rel]
+        const V3 w_rel = qrot(R, v3(qd[ds], qd[ds + 1], qd[ds + 2]));
+        const V3 v_rel = qrot(R, v3(qd[ds + 3], qd[ds + 4], qd[ds + 5]));
+        c = sv(v3(0, 0, 0), cross(v_rel, w_rel));
+      }
+    }
+    sv_store(vj + 6 * b, vJ);
+    sv_store(cbias + 6 * b, c);
+    // inertia about the world origin (sim/sap_helpers.py:1027-1062)
+    const Xf X = pose_load(pose + 8 * b);
+    const Q4 qb = qnormalize(X.q);
     const double m = P.m.body_mass[b0g + b];
     const double* Ic = P.m.body_inertia + 9 * (size_t)(b0g + b);
-    const V3 c = qrot(q, load3(P.m.body_com + 3 * (size_t)(b0g + b)));
-    // R Ic R^T with R's columns the rotated axes
-    V3 col[3] = {qrot(q, v3(1, 0, 0)), qrot(q, v3(0, 1, 0)), qrot(q, v3(0, 0, 1))};
-    double R[3][3], IW[3][3];
-    for (int r = 0; r < 3; ++r) {
-      R[r][0] = r == 0 ? col[0].x : (r == 1 ? col[0].y : col[0].z);
-      R[r][1] = r == 0 ? col[1].x : (r == 1 ? col[1].y : col[1].z);
-      R[r][2] = r == 0 ? col[2].x : (r == 1 ? col[2].y : col[2].z);
-    }
+    const V3 cw = X.p + qrot(qb, load3(P.m.body_com + 3 * (size_t)(b0g + b)));
+    const V3 col[3] = {qrot(qb, v3(1, 0, 0)), qrot(qb, v3(0, 1, 0)), qrot(qb, v3(0, 0, 1))};
+    const double Rm[3][3] = {{col[0].x, col[1].x, col[2].x}, {col[0].y, col[1].y, col[2].y},
+                             {col[0].z, col[1].z, col[2].z}};
+    double IW[3][3];
     for (int r = 0; r < 3; ++r)
-      for (int s = 0; s < 3; ++s) {
+      for (int t = 0; t < 3; ++t) {
         double acc = 0.0;
         for (int u = 0; u < 3; ++u)
-          for (int v = 0; v < 3; ++v) acc += R[r][u] * Ic[3 * u + v] * R[s][v];
-        IW[r][s] = acc;
+          for (int v = 0; v < 3; ++v) acc += Rm[r][u] * Ic[3 * u + v] * Rm[t][v];
+        IW[r][t] = acc;
       }
-    const double cc[3] = {c.x, c.y, c.z};
-    const double cdc = dot(c, c);
-    double* I = I6(b);
-    for (int r = 0; r < 3; ++r)
-      for (int s = 0; s < 3; ++s) {
-        I[6 * r + s] = IW[r][s] + m * ((r == s ? cdc : 0.0) - cc[r] * cc[s]);
-        I[6 * (r + 3) + (s + 3)] = r == s ? m : 0.0;
-      }
-    // m [c]x in the upper right, -m [c]x lower left
-    const double cx[3][3] = {{0.0, -c.z, c.y}, {c.z, 0.0, -c.x}, {-c.y, c.x, 0.0}};
-    for (int r = 0; r < 3; ++r)
-      for (int s = 0; s < 3; ++s) {
-        I[6 * r + (s + 3)] = m * cx[r][s];
-        I[6 * (r + 3) + s] = -m * cx[r][s];
-      }
-    const Sv a = sv_load(ACC(b)), V = sv_load(VEL(b));
-    double av[6], Ia[6];
-    sv_store(av, a);
-    for (int r = 0; r < 6; ++r) {
-      double acc = 0.0;
-      for (int s = 0; s < 6; ++s) acc += I[6 * r + s] * av[s];
-      Ia[r] = acc;
-    }
-    const V3 w = V.w;
-    const V3 Iw = v3(I[0] * w.x + I[1] * w.y + I[2] * w.z, I[6] * w.x + I[7] * w.y + I[8] * w.z,
-                     I[12] * w.x + I[13] * w.y + I[14] * w.z);
-    const V3 bias_t = cross(w, Iw);
-    const V3 bias_f = m * cross(w, cross(w, c));
-    const int world_g = e;
-    const V3 g = load3(P.m.gravity + 3 * (size_t)world_g);
-    const V3 fg = m * g;
-    const V3 tg = cross(c, fg);
-    double* fb = FB(b);
-    fb[0] = Ia[0] + bias_t.x - tg.x;
-    fb[1] = Ia[1] + bias_t.y - tg.y;
-    fb[2] = Ia[2] + bias_t.z - tg.z;
-    fb[3] = Ia[3] + bias_f.x - fg.x;
-    fb[4] = Ia[4] + bias_f.y - fg.y;
-    fb[5] = Ia[5] + bias_f.z - fg.z;
-    for (int k = 0; k < 6; ++k) FT(b)[k] = 0.0;
+    const double cc = dot(cw, cw);
+    double* I = ib + 10 * b;
+    I[0] = m;
+    I[1] = m * cw.x;
+    I[2] = m * cw.y;
+    I[3] = m * cw.z;
+    I[4] = IW[0][0] + m * (cc - cw.x * cw.x);
+    I[5] = IW[1][1] + m * (cc - cw.y * cw.y);
+    I[6] = IW[2][2] + m * (cc - cw.z * cw.z);
+    I[7] = IW[0][1] - m * cw.x * cw.y;
+    I[8] = IW[0][2] - m * cw.x * cw.z;
+    I[9] = IW[1][2] - m * cw.y * cw.z;
   }
   __syncthreads();
-
-  // ---- reverse pass (sim/free_motion.py:154-220, sim/sap_helpers.py:2090-2118)
-  for (int a = tid; a < Aw; a += kPrepNT) {
-    const int ja = P.m.articulation_start[e * Aw + a], jb = P.m.articulation_start[e * Aw + a + 1];
-    for (int j = jb - 1; j >= ja; --j) {
-      const int pb = P.m.joint_parent[j] >= 0 ? P.m.joint_parent[j] - b0g : -1;
-      const int cb = P.m.joint_child[j] - b0g;
-      const int ds = P.m.joint_qd_start[j], dl = ds - d0;
-      const int dim = P.m.joint_dof_dim[2 * j] + P.m.joint_dof_dim[2 * j + 1];
-      Sv f = sv_load(FB(cb)) + sv_load(FT(cb));
-      if (P.in.body_f) f = f + sv_load(P.in.body_f + 6 * (size_t)(b0g + cb));
-      for (int k = 0; k < dim; ++k) {
-        const double jf = P.in.joint_f ? P.in.joint_f[ds + k] : 0.0;
-        tau[dl + k] = -sdot(sv_load(S + 6 * (dl + k)), f) + jf;
-      }
-      if (pb >= 0) {
-        const Sv sf = shift_force(f, load3(POS(pb)) - load3(POS(cb)));
-        double* ft = FT(pb);
-        ft[0] += sf.w.x;
-        ft[1] += sf.w.y;
-        ft[2] += sf.w.z;
-        ft[3] += sf.v.x;
-        ft[4] += sf.v.y;
-        ft[5] += sf.v.z;
-      }
-    }
-  }
-  // ---- body Jacobians in world-local DOF numbering (sim/free_motion.py:722-765)
+  // ---- body velocities: sums of the ancestors' joint velocities -------------
   for (int b = tid; b < B; b += kPrepNT) {
-    int jj = bj[b];
-    const V3 pb = load3(POS(b));
-    while (jj >= 0) {
-      const int colb = P.m.joint_child[jj] - b0g;
-      const int dl = P.m.joint_qd_start[jj] - d0;
-      const int dim = P.m.joint_dof_dim[2 * jj] + P.m.joint_dof_dim[2 * jj + 1];
-      const V3 p = pb - load3(POS(colb));
-      for (int k = 0; k < dim; ++k) {
-        const Sv s = shift_velocity(sv_load(S + 6 * (dl + k)), p);
-        double out[6];
-        sv_store(out, s);
-        for (int r = 0; r < 6; ++r) Jb[((size_t)b * 6 + r) * n + dl + k] = out[r];
-      }
-      jj = P.m.joint_ancestor[jj];
+    Sv v = sv_zero();
+    uint64_t mk = anc[b];
+    while (mk) {
+      const int d = __ffsll((long long)mk) - 1;
+      mk &= mk - 1;
+      v = v + sv_load(vj + 6 * d);
     }
+    sv_store(vb + 6 * b, v);
   }
-  for (int k = tid; k < n * n; k += kPrepNT) H[k] = 0.0;
   __syncthreads();
-
-  // ---- A = sum_b J_b^T I_b J_b + armature (sim/free_motion.py:814-1179) ------
-  for (int b = 0; b < B; ++b) {
-    const double* I = I6(b);
-    const double* Jbb = Jb + (size_t)b * 6 * n;
-    for (int k = tid; k < 6 * n; k += kPrepNT) {
-      const int r = k / n, col = k - r * n;
-      double acc = 0.0;
-      for (int s = 0; s < 6; ++s) acc += I[6 * r + s] * Jbb[(size_t)s * n + col];
-      K[k] = acc;
-    }
-    __syncthreads();
-    for (int k = tid; k < n * n; k += kPrepNT) {
-      const int i = k / n, j = k - i * n;
-      if (j > i) continue;
-      double acc = 0.0;
-      for (int r = 0; r < 6; ++r) acc += Jbb[(size_t)r * n + i] * K[(size_t)r * n + j];
-      H[k] += acc;
-    }
-    __syncthreads();
+  // joint bias accelerations c_b = v_parent x vJ_b (+ the free-joint term)
+  for (int b = tid; b < B; b += kPrepNT) {
+    const int j = bj[b];
+    if (j < 0) continue;
+    const int parent = P.m.joint_parent[j] >= 0 ? P.m.joint_parent[j] - b0g : -1;
+    if (parent < 0 || parent >= B) continue;
+    sv_store(cbias + 6 * b, sv_load(cbias + 6 * b) + crm(sv_load(vb + 6 * parent), sv_load(vj + 6 * b)));
   }
+  __syncthreads();
+  // ---- body forces f = I a + v x* I v - f_gravity + body_f -------------------
+  // (sim/sap_helpers.py:1065-1105; gravity as the base acceleration -g)
+  for (int b = tid; b < B; b += kPrepNT) {
+    Sv a = sv(v3(0, 0, 0), -grav);
+    uint64_t mk = anc[b];
+    while (mk) {
+      const int d = __ffsll((long long)mk) - 1;
+      mk &= mk - 1;
+      a = a + sv_load(cbias + 6 * d);
+    }
+    const double* I = ib + 10 * b;
+    const Sv v = sv_load(vb + 6 * b);
+    Sv f = inertia_times(I, a) + crf(v, inertia_times(I, v));
+    if (P.in.body_f) {
+      const Sv bf = sv_load(P.in.body_f + 6 * (size_t)(b0g + b));  // at the body origin
+      const V3 pb = v3(pose[8 * b], pose[8 * b + 1], pose[8 * b + 2]);
+      f = f + Sv{bf.w + cross(pb, bf.v), bf.v};
+    }
+    sv_store(fb + 6 * b, f);
+  }
+  __syncthreads();
+  // ---- subtree forces and composite inertias --------------------------------
+  for (int k = tid; k < 16 * B; k += kPrepNT) {
+    const int b = k >> 4, comp = k & 15;
+    double acc = 0.0;
+    for (int d = 0; d < B; ++d)
+      if ((anc[d] >> b) & 1ull) acc += comp < 6 ? fb[6 * d + comp] : ib[10 * d + comp - 6];
+    fs[16 * b + comp] = acc;
+  }
+  __syncthreads();
+  // ---- tau = joint_f - S^T f_subtree, F_i = I^c S_i (sim/sap_helpers.py:2090-2118)
+  for (int i = tid; i < n; i += kPrepNT) {
+    const int b = dbody[i];
+    Sv F = sv_zero();
+    double t = P.in.joint_f ? P.in.joint_f[d0 + i] : 0.0;
+    if (b >= 0) {
+      const Sv s = sv_load(S + 6 * i);
+      F = inertia_times(fs + 16 * b + 6, s);
+      t -= sdot(s, sv_load(fs + 16 * b));
+    }
+    sv_store(Fi + 6 * i, F);
+    tau[i] = t;
+  }
+  __syncthreads();
+  // ---- A = composite-rigid-body pairs + armature ------------------------------
   double* Ag = P.out.dynamics_matrix + (size_t)e * n * n;
   for (int k = tid; k < n * n; k += kPrepNT) {
     const int i = k / n, j = k - i * n;
-    double v = i >= j ? H[(size_t)i * n + j] : H[(size_t)j * n + i];
-    if (i == j) v += P.m.joint_armature[d0 + i];
-    Ag[k] = v;
+    if (j > i) continue;
+    const int bi = dbody[i], bjj = dbody[j];
+    double v = 0.0;
+    if (bi >= 0 && bjj >= 0) {
+      if ((anc[bi] >> bjj) & 1ull) v = sdot(sv_load(S + 6 * j), sv_load(Fi + 6 * i));
+      else if ((anc[bjj] >> bi) & 1ull) v = sdot(sv_load(S + 6 * i), sv_load(Fi + 6 * j));
+    }
+    if (i == j) {
+      v += P.m.joint_armature[d0 + i];
+      adiag[i] = v;
+    }
+    H[(size_t)i * n + j] = v;
+    Ag[(size_t)i * n + j] = v;
+    Ag[(size_t)j * n + i] = v;
   }
   __syncthreads();
-  for (int i = tid; i < n; i += kPrepNT) H[(size_t)i * n + i] += P.m.joint_armature[d0 + i];
-  __syncthreads();
 
-  // ---- free-motion solve A vdot = tau (LDL^T, lower triangle) ---------------
+  // ---- free-motion solve A vdot = tau: LDL^T (H_ik = L_ik d_k below the diagonal)
   for (int k = 0; k < n; ++k) {
-    const double rinv = 1.0 / H[(size_t)k * n + k];
+    const double rinv = fast_recip(H[(size_t)k * n + k]);
     const int m = n - k - 1;
-    const int cnt = m * (m + 1) / 2;
-    for (int q = tid; q < cnt; q += kPrepNT) {
-      int ii = (int)((sqrtf(8.0f * (float)q + 1.0f) - 1.0f) * 0.5f);
-      while ((ii + 1) * (ii + 2) / 2 <= q) ++ii;
-      while (ii * (ii + 1) / 2 > q) --ii;
-      const int jj = q - ii * (ii + 1) / 2;
-      const int i = k + 1 + ii, j = k + 1 + jj;
-      H[(size_t)i * n + j] -= (H[(size_t)i * n + k] * rinv) * H[(size_t)j * n + k];
+    for (int idx = tid; idx < m * m; idx += kPrepNT) {
+      const int a = idx / m, c = idx - a * m;
+      if (c > a) continue;
+      const int i = k + 1 + a, j = k + 1 + c;
+      H[(size_t)i * n + j] -= H[(size_t)i * n + k] * rinv * H[(size_t)j * n + k];
     }
     __syncthreads();
   }
-  if (tid == 0) {
-    for (int i = 0; i < n; ++i) {
-      double s = tau[i];
-      for (int k = 0; k < i; ++k) s -= (H[(size_t)i * n + k] / H[(size_t)k * n + k]) * vdot[k];
-      vdot[i] = s;
+  for (int k = tid; k < n; k += kPrepNT) dinv[k] = fast_recip(H[(size_t)k * n + k]);
+  __syncthreads();
+  if (tid < 32) {
+    // lanes own rows lane + 32 r (n <= 128): forward z = D^-1 L^-1 tau, then x = L^-T z
+    double hb[4], sacc[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = lane + 32 * r;
+      hb[r] = i < n ? tau[i] : 0.0;
+      sacc[r] = 0.0;
     }
-    for (int i = 0; i < n; ++i) vdot[i] /= H[(size_t)i * n + i];
+    for (int k = 0; k < n; ++k) {
+      const int kr = k >> 5;
+      double bk = 0.0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (r == kr) bk = hb[r];
+      bk = __shfl_sync(0xffffffffu, bk, k & 31);
+      const double zk = bk * dinv[k];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = lane + 32 * r;
+        if (i == k) hb[r] = zk;
+        else if (i > k && i < n) hb[r] -= H[(size_t)i * n + k] * zk;
+      }
+    }
     for (int i = n - 1; i >= 0; --i) {
-      double s = vdot[i];
-      for (int k = i + 1; k < n; ++k) s -= (H[(size_t)k * n + i] / H[(size_t)i * n + i]) * vdot[k];
-      vdot[i] = s;
+      const int ir = i >> 5;
+      double xi = 0.0;
+      if (lane == (i & 31)) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (r == ir) {
+            xi = hb[r] - sacc[r] * dinv[i];
+            hb[r] = xi;
+          }
+      }
+      xi = __shfl_sync(0xffffffffu, xi, i & 31);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int l = lane + 32 * r;
+        if (l < i) sacc[r] += H[(size_t)i * n + l] * xi;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = lane + 32 * r;
+      if (i < n) vdot[i] = hb[r];
     }
   }
   __syncthreads();
@@ -428,10 +544,9 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     if (P.out.vdot) P.out.vdot[d0 + i] = vd;
   }
   if (P.out.body_q) {
-    for (int b = tid; b < B; b += kPrepNT) {
-      double* o = P.out.body_q + 7 * (size_t)(b0g + b);
-      for (int k = 0; k < 3; ++k) o[k] = POS(b)[k];
-      for (int k = 0; k < 4; ++k) o[3 + k] = QUAT(b)[k];
+    for (int k = tid; k < 7 * B; k += kPrepNT) {
+      const int b = k / 7, c = k - 7 * b;
+      P.out.body_q[7 * (size_t)(b0g + b) + c] = pose[8 * b + c];
     }
   }
 
@@ -454,6 +569,8 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     }
     __syncthreads();
   }
+  auto POSE_P = [&](int b) { return v3(pose[8 * b], pose[8 * b + 1], pose[8 * b + 2]); };
+  auto POSE_Q = [&](int b) { return qnormalize(Q4{pose[8 * b + 3], pose[8 * b + 4], pose[8 * b + 5], pose[8 * b + 6]}); };
   for (int c = tid; c < cc; c += kPrepNT) {
     const int src = P.env_src[(size_t)e * C + c];
     const int sh0 = P.in.contact_shape0[src], sh1 = P.in.contact_shape1[src];
@@ -463,15 +580,8 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     const int lb0 = gb0 >= 0 ? gb0 - b0g : -1, lb1 = gb1 >= 0 ? gb1 - b0g : -1;
     V3 x0 = load3(P.in.contact_point0 + 3 * (size_t)src);
     V3 x1 = load3(P.in.contact_point1 + 3 * (size_t)src);
-    V3 p0 = v3(0, 0, 0), p1 = v3(0, 0, 0);
-    if (lb0 >= 0) {
-      p0 = load3(POS(lb0));
-      x0 = p0 + qrot(qnormalize(Q4{QUAT(lb0)[0], QUAT(lb0)[1], QUAT(lb0)[2], QUAT(lb0)[3]}), x0);
-    }
-    if (lb1 >= 0) {
-      p1 = load3(POS(lb1));
-      x1 = p1 + qrot(qnormalize(Q4{QUAT(lb1)[0], QUAT(lb1)[1], QUAT(lb1)[2], QUAT(lb1)[3]}), x1);
-    }
+    if (lb0 >= 0) x0 = POSE_P(lb0) + qrot(POSE_Q(lb0), x0);
+    if (lb1 >= 0) x1 = POSE_P(lb1) + qrot(POSE_Q(lb1), x1);
     V3 nrm = load3(P.in.contact_normal + 3 * (size_t)src);
     const double nn = sqrt(dot(nrm, nrm));
     if (nn > 0.0) nrm = (1.0 / nn) * nrm;
@@ -507,11 +617,9 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     const bool mid = P.o.contact_point_mode == SAPB_POINT_MIDPOINT;
     store3(cs + 0, mid ? pC : x0);
     store3(cs + 3, mid ? pC : x1);
-    store3(cs + 6, p0);
-    store3(cs + 9, p1);
     for (int k = 0; k < 9; ++k) cs[12 + k] = F[k];
-    conint[2 * c] = lb0;
-    conint[2 * c + 1] = lb1;
+    conint[2 * c] = (lb0 >= 0 && lb0 < B) ? lb0 : -1;
+    conint[2 * c + 1] = (lb1 >= 0 && lb1 < B) ? lb1 : -1;
   }
   __syncthreads();
   double* Jout = P.out.jacobian + (size_t)e * C * 3 * n;
@@ -519,16 +627,12 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     const int c = k / n, col = k - c * n;
     const double* cs = con + 21 * (size_t)c;
     V3 rel = v3(0, 0, 0);
-    const int lb0 = conint[2 * c], lb1 = conint[2 * c + 1];
-    if (lb1 >= 0) {
-      const double* J = Jb + (size_t)lb1 * 6 * n + col;
-      const V3 w = v3(J[0], J[n], J[2 * n]), v = v3(J[3 * n], J[4 * n], J[5 * n]);
-      rel = rel + (v + cross(w, load3(cs + 3) - load3(cs + 9)));
-    }
-    if (lb0 >= 0) {
-      const double* J = Jb + (size_t)lb0 * 6 * n + col;
-      const V3 w = v3(J[0], J[n], J[2 * n]), v = v3(J[3 * n], J[4 * n], J[5 * n]);
-      rel = rel - (v + cross(w, load3(cs + 0) - load3(cs + 6)));
+    const int bcol = dbody[col];
+    if (bcol >= 0) {
+      const Sv s = sv_load(S + 6 * col);
+      const int lb0 = conint[2 * c], lb1 = conint[2 * c + 1];
+      if (lb1 >= 0 && ((anc[lb1] >> bcol) & 1ull)) rel = rel + (s.v + cross(s.w, load3(cs + 3)));
+      if (lb0 >= 0 && ((anc[lb0] >> bcol) & 1ull)) rel = rel - (s.v + cross(s.w, load3(cs + 0)));
     }
     for (int r = 0; r < 3; ++r) Jout[((size_t)c * 3 + r) * n + col] = dot(load3(cs + 12 + 3 * r), rel);
   }
@@ -541,7 +645,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
       double w00 = 0, w01 = 0, w02 = 0, w11 = 0, w12 = 0, w22 = 0;
       const double* Jc = Jout + (size_t)c * 3 * n;
       for (int j = 0; j < n; ++j) {
-        double aii = Ag[(size_t)j * n + j];
+        double aii = adiag[j];
         if (aii < 1.0e-12) aii = 1.0e-12;
         const double inv = 1.0 / aii;
         const double a0 = Jc[j], a1 = Jc[n + j], a2 = Jc[2 * n + j];
@@ -564,15 +668,15 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
         if (lb < 0) continue;
         const double mass = P.m.body_mass[b0g + lb];
         if (mass <= 1.0e-12) continue;
-        const Q4 q = qnormalize(Q4{QUAT(lb)[0], QUAT(lb)[1], QUAT(lb)[2], QUAT(lb)[3]});
-        const V3 pb = load3(POS(lb));
-        const V3 xw = pb + qrot(q, load3((side == 0 ? P.in.contact_point0 : P.in.contact_point1) + 3 * (size_t)src));
-        const V3 com = pb + qrot(q, load3(P.m.body_com + 3 * (size_t)(b0g + lb)));
+        const Q4 qq = POSE_Q(lb);
+        const V3 pb = POSE_P(lb);
+        const V3 xw = pb + qrot(qq, load3((side == 0 ? P.in.contact_point0 : P.in.contact_point1) + 3 * (size_t)src));
+        const V3 com = pb + qrot(qq, load3(P.m.body_com + 3 * (size_t)(b0g + lb)));
         const V3 r = xw - com;
         const double* Ic = P.m.body_inertia + 9 * (size_t)(b0g + lb);
         const double ix = fmax(Ic[0], 1.0e-12), iy = fmax(Ic[4], 1.0e-12), iz = fmax(Ic[8], 1.0e-12);
         for (int d = 0; d < 3; ++d) {
-          const V3 cb = qrot(qconj(q), cross(r, load3(cs + 12 + 3 * d)));
+          const V3 cb = qrot(qconj(qq), cross(r, load3(cs + 12 + 3 * d)));
           wsum += 1.0 / mass + cb.x * cb.x / ix + cb.y * cb.y / iy + cb.z * cb.z / iz;
         }
       }

@@ -16,9 +16,11 @@ composes with (the plain start it competes against is v_guess when active).
 Network inputs of a contact slot (raw): phi0; J_c v* in the contact frame
 (t1, t2, n); the world-up component of the contact normal (1 when unknown);
 mu; log10(stiffness); tau_d; dt; w_eff * gamma_prev (t1, t2, n; 0 when no
-previous impulses are given).  The target is u = w_eff * gamma* (velocity
-units) of the converged FP64 solve; features and targets are standardised
-with the statistics of the training set, which travel with the weights.
+previous impulses are given).  The network predicts the correction
+w_eff * (gamma* - gamma_prev) (velocity units) to the previous impulses, so a
+zero output reproduces the previous-impulse start; gamma* is the converged
+FP64 solve's.  Inputs and targets are standardised with the statistics of the
+training set, which travel with the weights.
 """
 
 from __future__ import annotations
@@ -242,7 +244,7 @@ class LearnedWarmStart:
         check(lib.sapb_warmstart_features(ctypes.byref(P), nu, gp, ctypes.byref(self.norm_struct), self.tau_fallback,
                                           b["x"].data_ptr(), None, s), "sapb_warmstart_features")
         self.mlp.forward(b["x"], b["y"])
-        check(lib.sapb_warmstart_impulses(ctypes.byref(P), b["y"].data_ptr(), ctypes.byref(self.norm_struct),
+        check(lib.sapb_warmstart_impulses(ctypes.byref(P), b["y"].data_ptr(), gp, ctypes.byref(self.norm_struct),
                                           b["gamma0"].data_ptr(), s), "sapb_warmstart_impulses")
         return b["gamma0"]
 
@@ -335,12 +337,18 @@ def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every:
     return torch.cat(raws), torch.cat(us)
 
 
+def residual_targets(raw: torch.Tensor, u: torch.Tensor) -> torch.Tensor:
+    """w_eff * (gamma* - gamma_prev): the targets u minus the w-scaled
+    previous impulses carried in raw input columns 9..11."""
+    return (u - raw[:, 9:12]).contiguous()
+
+
 def train(mlp: WarmStartMLP, raw: torch.Tensor, u: torch.Tensor, norm: FeatureNorm, steps: int = 4000,
           batch: int = 8192, lr: float = 2e-3, lr_final: float = 5e-5, seed: int = 0, log_every: int = 200):
     """Adam on the standardised targets with a cosine learning-rate decay;
     returns [(step, mean squared error of the batch)]."""
     x_all = norm.encode(raw)
-    t_all = norm.targets(u)
+    t_all = norm.targets(residual_targets(raw, u))
     N = x_all.shape[0]
     gen = torch.Generator(device=mlp.device)
     gen.manual_seed(seed)
@@ -393,7 +401,7 @@ def _main():
     raw = torch.cat([p[0] for p in parts])
     u = torch.cat([p[1] for p in parts])
     t1 = time.time()
-    norm = FeatureNorm.from_data(raw.cpu().numpy(), u.cpu().numpy())
+    norm = FeatureNorm.from_data(raw.cpu().numpy(), residual_targets(raw, u).cpu().numpy())
     mlp = WarmStartMLP(dev, seed=a.seed)
     log = train(mlp, raw, u, norm, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed)
     torch.cuda.synchronize()

@@ -9,8 +9,8 @@ import torch
 
 from sap_warp_b200 import scenes
 from sap_warp_b200._solve import ContactSolveBuffers, contact_solve, make_options, problem_to_device
-from sap_warp_b200.warmstart import (FeatureNorm, LearnedWarmStart, WarmStartMLP, raw_features, solver_dataset,
-                                     train)
+from sap_warp_b200.warmstart import (FeatureNorm, LearnedWarmStart, WarmStartMLP, raw_features, residual_targets,
+                                     solver_dataset, train)
 
 pytestmark = pytest.mark.gpu
 
@@ -74,10 +74,12 @@ def test_impulses_are_scaled_and_projected(cuda_device):
     norm.out_shift = np.array([0.1, -0.2, 0.3], np.float32)
     ws = LearnedWarmStart(WarmStartMLP(cuda_device, seed=2), norm)
     t = problem_to_device(prob, cuda_device)
-    g0 = ws.predict(num_envs=E, dof_per_env=n, max_contacts=C, **t).cpu().numpy()
+    gp = np.random.default_rng(1).normal(scale=0.01, size=(E, C, 3))
+    g0 = ws.predict(num_envs=E, dof_per_env=n, max_contacts=C, gamma_prev=torch.as_tensor(gp).to(cuda_device),
+                    **t).cpu().numpy()
     y = ws.buffers(E, C)["y"].cpu().numpy().astype(np.float64).reshape(E, C, 3)
     u = y * norm.out_scale.astype(np.float64) + norm.out_shift.astype(np.float64)
-    g = u / np.maximum(prob.w_eff, 1e-12)[..., None]
+    g = gp + u / np.maximum(prob.w_eff, 1e-12)[..., None]
     g[..., 2] = np.maximum(g[..., 2], 0.0)
     tm = np.linalg.norm(g[..., :2], axis=-1)
     lim = prob.mu * g[..., 2]
@@ -129,7 +131,7 @@ def test_learned_start_reduces_newton_iterations(cuda_device, oracle):
     the learned start must be as accurate as the plain ones."""
     train_probs = [scenes.humanoid_contact_problem(2048, seed=s) for s in (300, 301, 302)]
     raw, u = solver_dataset(train_probs, cuda_device)
-    norm = FeatureNorm.from_data(raw.cpu().numpy(), u.cpu().numpy())
+    norm = FeatureNorm.from_data(raw.cpu().numpy(), residual_targets(raw, u).cpu().numpy())
     mlp = WarmStartMLP(cuda_device, seed=0)
     log = train(mlp, raw, u, norm, steps=1500, batch=8192, lr=2e-3, log_every=500)
     assert log[-1][1] < 0.5 * log[0][1], log
