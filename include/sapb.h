@@ -145,11 +145,13 @@ typedef struct sapb_contact_problem {
   const int32_t* v_guess_active;  /* [1] nonzero: start from v_guess; NULL: never */
   const double* dt;               /* [E] per-world time step */
   const sapb_dof_terms* dof;      /* NULL: no PD / limit terms */
-  /* Learned warm start (no counterpart in the reference): starting impulses
-   * [E,C,3] or NULL.  When set, the solve forms v_L = v* + A^-1 J^T gamma0 on
-   * the participating DOFs and starts Newton from v_L only if
-   * cost(v_L) < cost(plain start), the plain start being v_guess or v0. */
+  /* Candidate starts (no counterpart in the reference): gamma0_count sets of
+   * starting impulses [K][E,C,3] back to back, or NULL.  For each set the
+   * solve forms v_c = v* + A^-1 J^T gamma_c on the participating DOFs and
+   * starts Newton from the lowest-cost start among the plain one (v_guess or
+   * v0) and the candidates.  gamma0_count <= 1 means one set. */
   const double* gamma0;
+  int32_t gamma0_count;
 } sapb_contact_problem;
 
 /* Outputs: the SapContactSolveResult fields a caller reads
@@ -164,7 +166,7 @@ typedef struct sapb_solve_outputs {
   int32_t* converged;             /* [E] 1 if optimality or cost test met */
   int32_t* status;                /* [E] last line-search status (0 or SAPB_LS_*) */
   double* grad_norm;              /* [E] ||D^-1/2 grad|| over participating DOFs */
-  int32_t* warm_start_accepted;   /* [E] 1 if the gamma0 start was taken (NULL: not written) */
+  int32_t* warm_start_accepted;   /* [E] chosen start: 0 plain, k = candidate set k (NULL: not written) */
 } sapb_solve_outputs;
 
 /* ---- free motion + contact Jacobian ---------------------------------------
@@ -337,8 +339,9 @@ const char* sapb_last_error(void);
  * contact frame (t1, t2, n); the world-up component of the contact normal;
  * mu; log10(stiffness); tau_d; dt; w_eff * gamma_prev (t1, t2, n).  The
  * output y maps to a correction u = y * output_scale + output_shift
- * (velocity units) of the previous impulses: gamma0 = gamma_prev + u / w_eff
- * (gamma_prev = 0 when not given), projected onto the friction cone. */
+ * (velocity units) of SAP's unprojected impulse y0 = gamma_prev + u / w_eff
+ * (gamma_prev = 0 when not given); gamma0 is the regularized projection of
+ * y0 (the impulse SAP assigns to the contact velocity vhat - R y0). */
 #define SAPB_MLP_INPUTS 12
 #define SAPB_MLP_INPUTS_PADDED 16
 #define SAPB_MLP_HIDDEN 128
@@ -398,10 +401,11 @@ int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const doubl
                                 const double* gamma_prev, const sapb_warmstart_norm* norm, double tau_fallback,
                                 uint16_t* features, float* raw, void* stream);
 /* gamma0 [E,C,3] from the network output mlp_out [E*C,3] and the previous
- * step's impulses gamma_prev [E,C,3] (NULL: 0). */
+ * step's impulses gamma_prev [E,C,3] (NULL: 0); opts supplies the
+ * regularization (contact_beta, contact_sigma, contact_tau_d fallback). */
 int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float* mlp_out,
-                                const double* gamma_prev, const sapb_warmstart_norm* norm, double* gamma0,
-                                void* stream);
+                                const double* gamma_prev, const sapb_warmstart_norm* norm,
+                                const sapb_solve_options* opts, double* gamma0, void* stream);
 
 #ifdef __cplusplus
 }

@@ -102,7 +102,8 @@ def _c(a, dtype):
 def solve(prob, line_search_variant: str = "monotone_decay", threads: int = 0, v_guess=None,
           v_guess_active: bool = False, dof_terms: dict | None = None, gamma0=None, **overrides) -> dict:
     """Run the oracle on a scenes.ContactProblemArrays (host).  gamma0
-    (E, C, 3): learned starting impulses (accepted on the cost test)."""
+    (E, C, 3) or (K, E, C, 3): candidate starting impulse sets (the
+    lowest-cost start among the plain one and the candidates is taken)."""
     lib = load()
     E, n, C = prob.num_envs, prob.dof_per_env, prob.max_contacts
     keep = {}
@@ -133,6 +134,8 @@ def solve(prob, line_search_variant: str = "monotone_decay", threads: int = 0, v
     P.v0 = ptr("v0", prob.v0, np.float64)
     P.dt = ptr("dt", prob.dt, np.float64)
     P.gamma0 = ptr("gamma0", gamma0, np.float64)
+    if gamma0 is not None:
+        P.gamma0_count = int(np.asarray(gamma0).size // (3 * max(E * C, 1)))
     guess = None
     if v_guess is not None:
         guess = _c(v_guess, np.float64).copy()

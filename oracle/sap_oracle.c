@@ -1030,44 +1030,51 @@ static void solve_world(const sapb_contact_problem* P, const sapb_solve_options*
   } else {
     for (int32_t i = 0; i < n; ++i)
       if (!w.part[i]) w.v[i] = w.v_star[i];
-    /* Learned warm start (no counterpart in the reference): the candidate
-     * v_L = v* + A^-1 J^T gamma0 on the participating DOFs replaces the plain
-     * start only if its cost is lower. */
+    /* Candidate starts (no counterpart in the reference): for each impulse
+     * set, v_c = v* + A^-1 J^T gamma_c on the participating DOFs; the start
+     * with the lowest cost among the plain one and the candidates is taken. */
     if (P->gamma0 && count > 0) {
-      const double cost_plain = evaluate(&w, w.v, w.vc, w.gamma, w.ccost, w.impulse, w.grad, w.dyn, w.pd_gamma,
-                                         w.pd_hdiag, w.lim_grad, w.lim_hdiag, NULL);
+      const int32_t K = P->gamma0_count > 1 ? P->gamma0_count : 1;
+      double best_cost = evaluate(&w, w.v, w.vc, w.gamma, w.ccost, w.impulse, w.grad, w.dyn, w.pd_gamma,
+                                  w.pd_hdiag, w.lim_grad, w.lim_hdiag, NULL);
       double* L = (double*)malloc(sizeof(double) * nd * nd);
       double* x = (double*)malloc(sizeof(double) * nd);
-      double* vsave = (double*)malloc(sizeof(double) * nd);
-      const double* g0 = P->gamma0 + (size_t)e * C * 3;
+      double* vbest = (double*)malloc(sizeof(double) * nd);
       memcpy(L, w.A, sizeof(double) * nd * nd);
-      memcpy(vsave, w.v, sizeof(double) * nd);
-      for (int32_t i = 0; i < n; ++i) {
-        double acc = 0.0;
-        for (int32_t c = 0; c < count; ++c)
-          for (int32_t r = 0; r < 3; ++r) acc += w.J[((size_t)c * 3 + r) * n + i] * g0[3 * c + r];
-        x[i] = acc;
-      }
+      memcpy(vbest, w.v, sizeof(double) * nd);
       if (sapo_cholesky(L, n) == 0) {
-        for (int32_t i = 0; i < n; ++i) {
-          double t = x[i];
-          for (int32_t k = 0; k < i; ++k) t -= L[i * n + k] * x[k];
-          x[i] = t / L[i * n + i];
+        for (int32_t k = 0; k < K; ++k) {
+          const double* g0 = P->gamma0 + ((size_t)k * P->num_envs + e) * C * 3;
+          for (int32_t i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int32_t c = 0; c < count; ++c)
+              for (int32_t r = 0; r < 3; ++r) acc += w.J[((size_t)c * 3 + r) * n + i] * g0[3 * c + r];
+            x[i] = acc;
+          }
+          for (int32_t i = 0; i < n; ++i) {
+            double t = x[i];
+            for (int32_t q = 0; q < i; ++q) t -= L[i * n + q] * x[q];
+            x[i] = t / L[i * n + i];
+          }
+          for (int32_t i = n - 1; i >= 0; --i) {
+            double t = x[i];
+            for (int32_t q = i + 1; q < n; ++q) t -= L[q * n + i] * x[q];
+            x[i] = t / L[i * n + i];
+          }
+          for (int32_t i = 0; i < n; ++i) w.v[i] = w.part[i] ? w.v_star[i] + x[i] : w.v_star[i];
+          const double cost_c = evaluate(&w, w.v, w.vc, w.gamma, w.ccost, w.impulse, w.grad, w.dyn, w.pd_gamma,
+                                         w.pd_hdiag, w.lim_grad, w.lim_hdiag, NULL);
+          if (cost_c < best_cost) {
+            best_cost = cost_c;
+            ws_accepted = k + 1;
+            memcpy(vbest, w.v, sizeof(double) * nd);
+          }
         }
-        for (int32_t i = n - 1; i >= 0; --i) {
-          double t = x[i];
-          for (int32_t k = i + 1; k < n; ++k) t -= L[k * n + i] * x[k];
-          x[i] = t / L[i * n + i];
-        }
-        for (int32_t i = 0; i < n; ++i) w.v[i] = w.part[i] ? w.v_star[i] + x[i] : w.v_star[i];
-        const double cost_l = evaluate(&w, w.v, w.vc, w.gamma, w.ccost, w.impulse, w.grad, w.dyn, w.pd_gamma,
-                                       w.pd_hdiag, w.lim_grad, w.lim_hdiag, NULL);
-        if (cost_l < cost_plain) ws_accepted = 1;
-        else memcpy(w.v, vsave, sizeof(double) * nd);
       }
+      memcpy(w.v, vbest, sizeof(double) * nd);
       free(L);
       free(x);
-      free(vsave);
+      free(vbest);
     }
     /* Newton loop (:5559-5655 with the body :5474-5557). */
     int32_t it = 0;

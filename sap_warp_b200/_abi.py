@@ -114,6 +114,7 @@ class ContactProblem(C.Structure):
         ("dt", _p),
         ("dof", C.POINTER(DofTerms)),
         ("gamma0", _p),
+        ("gamma0_count", C.c_int32),
     ]
 
 
@@ -284,7 +285,9 @@ EXPORTS = {
     "sapb_warmstart_features": (
         C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), C.c_double, _p, _p, _p]
     ),
-    "sapb_warmstart_impulses": (C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), _p, _p]),
+    "sapb_warmstart_impulses": (
+        C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), C.POINTER(SolveOptions), _p, _p]
+    ),
 }
 
 

@@ -169,6 +169,8 @@ def build_problem(
     P.v_guess_active = _ptr(v_guess_active, I32, 1, "v_guess_active")
     P.dt = _ptr(dt, F64, E, "dt")
     P.gamma0 = _ptr(gamma0, F64, E * C * 3, "gamma0")
+    if gamma0 is not None:
+        P.gamma0_count = int(gamma0.numel() // (3 * max(E * C, 1)))
     if dof_terms is not None:
         P.dof = ctypes.pointer(dof_terms.struct)
     return P
@@ -186,7 +188,7 @@ def contact_solve(
     `arrays` are the keyword tensors of `build_problem` (contact_count,
     dynamics_matrix, jacobian, phi0, w_eff, mu, stiffness, tau_d, v_star, v0,
     dt and the optional body maps, v_guess, v_guess_active, dof_terms and the
-    learned starting impulses gamma0)."""
+    candidate starting impulses gamma0, (E, C, 3) or (K, E, C, 3))."""
     lib = load()
     b = buffers
     P = build_problem(num_envs=b.num_envs, dof_per_env=b.dof_per_env, max_contacts=b.max_contacts, **arrays)

@@ -48,7 +48,7 @@ constexpr int kChunk = 16;
 struct Layout {
   int n, C, ldJ, ldH, nb;
   size_t off_J, off_scr, off_H, off_G, off_vec, off_con, off_flags, off_tri, total;
-  static constexpr int kVecs = 20;
+  static constexpr int kVecs = 22;
   static constexpr int kConPer = 17;
   static constexpr int kMaxWarps = 4;  // partial-sum scratch (blocks of <= 128 threads)
 };
@@ -89,7 +89,7 @@ __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
 // Vector slots inside off_vec (each ldJ doubles).
 enum Vec {
   V_V = 0, V_VSTAR, V_DV, V_GRAD, V_ARES, V_DP, V_DSCALE, V_AINV, V_PDA, V_PDGAIN, V_PDLIM,
-  V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_SAVE, V_END
+  V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_SAVE, V_BEST, V_DINV, V_END
 };
 static_assert(V_END <= Layout::kVecs, "vector slots");
 // Contact slots inside off_con (each C doubles).
@@ -387,11 +387,14 @@ __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) 
 // is not positive/finite makes dv NaN, so the line search reports an ascent
 // direction as the reference's NaN factor does.
 template <int NT, typename HT, int NS>
+__device__ void solve_factored(const World<NT, HT, NS>& w);
+
+template <int NT, typename HT, int NS>
 __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   const int tid = threadIdx.x;
   const int n = w.dofs(), ldH = w.ldH();
   HT* H = w.H;
-  HT* dinv = reinterpret_cast<HT*>(w.V(V_TMP0));  // 1/d_k, written one step ahead
+  HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));  // 1/d_k, written one step ahead
   double* dv = w.V(V_DV);
   // Blocked right-looking LDL^T, 8-column blocks, three barriers per block.
   // Storage: below the diagonal H[i][k] = L_ik d_k (L unit lower), D on the
@@ -451,6 +454,19 @@ __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
     }
     __syncthreads();
   }
+  solve_factored<NT, HT, NS>(w);
+}
+
+// dv = -H^-1 grad with the LDL^T that factor_and_solve left in H and V_DINV
+// (one warp; lanes own rows lane, lane + 32).  A pivot that is not
+// positive / finite makes dv NaN.
+template <int NT, typename HT, int NS>
+__device__ void solve_factored(const World<NT, HT, NS>& w) {
+  const int tid = threadIdx.x;
+  const int n = w.dofs(), ldH = w.ldH();
+  const HT* H = w.H;
+  const HT* dinv = reinterpret_cast<const HT*>(w.V(V_DINV));
+  double* dv = w.V(V_DV);
   if (tid < 32) {
     bool ok = true;
     for (int k = 0; k < n; ++k) {
@@ -1044,47 +1060,64 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       for (int i = tid; i < n; i += NT)
         if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
-      // Learned warm start (no counterpart in the reference): the candidate
-      // v_L = v* + A^-1 J^T gamma0 on the participating DOFs, A factored in
-      // this kernel's factor precision, replaces the plain start only if its
-      // cost is lower.  An accepted candidate's evaluation seeds iteration 0.
+      // Candidate starts (no counterpart in the reference): for each of the
+      // gamma0_count impulse sets, v_c = v* + A^-1 J^T gamma_c on the
+      // participating DOFs with A factored once in this kernel's factor
+      // precision; the start with the lowest cost among the plain start and
+      // the candidates is taken.  Its evaluation seeds iteration 0 when it
+      // was the last one evaluated.
       bool have_e4 = false;
       double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
       if (P.p.gamma0 && count > 0) {
+        const int K = P.p.gamma0_count > 1 ? P.p.gamma0_count : 1;
         double e4p[4];
         evaluate<NT, HT, NS>(w, P, dt, e4p);
-        const double* g0 = P.p.gamma0 + (size_t)e * C * 3;
+        double best_cost = e4p[0];
         const int ldj = w.ldJ(), ldh = w.ldH();
-        for (int i = tid; i < n; i += NT) {
-          w.V(V_SAVE)[i] = w.V(V_V)[i];
-          double acc = 0.0;
-          for (int c = 0; c < count; ++c) {
-            const double* Jc = w.J + (size_t)(3 * c) * ldj;
-            acc += Jc[i] * __ldg(g0 + 3 * c) + Jc[ldj + i] * __ldg(g0 + 3 * c + 1) +
-                   Jc[2 * ldj + i] * __ldg(g0 + 3 * c + 2);
-          }
-          w.V(V_GRAD)[i] = -acc;  // factor_and_solve solves H dv = -grad
-        }
+        for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
         {
           const int lane = tid & 31, warp = tid >> 5;
           for (int i = warp; i < n; i += NT / 32)
             for (int j = lane; j <= i; j += 32) w.H[(size_t)i * ldh + j] = HT(__ldg(w.A + (size_t)i * n + j));
         }
+        for (int i = tid; i < n; i += NT) w.V(V_GRAD)[i] = 0.0;
         __syncthreads();
-        factor_and_solve<NT, HT, NS>(w);
-        for (int i = tid; i < n; i += NT)
-          w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? w.V(V_VSTAR)[i] + w.V(V_DV)[i] : w.V(V_VSTAR)[i];
-        __syncthreads();
-        double e4l[4];
-        evaluate<NT, HT, NS>(w, P, dt, e4l);
-        if (e4l[0] < e4p[0]) {
-          ws_accepted = 1;
-          have_e4 = true;
-          for (int k = 0; k < 4; ++k) e4_seed[k] = e4l[k];
-        } else {
-          for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_SAVE)[i];
+        factor_and_solve<NT, HT, NS>(w);  // the factor of A (the solve of a zero rhs is unused)
+        bool last_is_best = false;
+        for (int k = 0; k < K; ++k) {
+          const double* g0 = P.p.gamma0 + ((size_t)k * P.p.num_envs + e) * C * 3;
+          for (int i = tid; i < n; i += NT) {
+            double acc = 0.0;
+            for (int c = 0; c < count; ++c) {
+              const double* Jc = w.J + (size_t)(3 * c) * ldj;
+              acc += Jc[i] * __ldg(g0 + 3 * c) + Jc[ldj + i] * __ldg(g0 + 3 * c + 1) +
+                     Jc[2 * ldj + i] * __ldg(g0 + 3 * c + 2);
+            }
+            w.V(V_GRAD)[i] = -acc;  // solve_factored solves H dv = -grad
+          }
           __syncthreads();
+          solve_factored<NT, HT, NS>(w);
+          for (int i = tid; i < n; i += NT)
+            w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? w.V(V_VSTAR)[i] + w.V(V_DV)[i] : w.V(V_VSTAR)[i];
+          __syncthreads();
+          double e4c[4];
+          evaluate<NT, HT, NS>(w, P, dt, e4c);
+          last_is_best = false;
+          if (e4c[0] < best_cost) {
+            best_cost = e4c[0];
+            ws_accepted = k + 1;
+            last_is_best = true;
+            for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
+            for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
+          }
         }
+        if (last_is_best) {
+          have_e4 = true;
+        } else {
+          const int src = ws_accepted > 0 ? V_BEST : V_SAVE;
+          for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(src)[i];
+        }
+        __syncthreads();
       }
       const double cost_min_alpha = P.o.line_search_variant == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
       int it = 0;

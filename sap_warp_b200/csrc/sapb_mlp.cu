@@ -18,10 +18,10 @@
 //              BF16 operand images the forward reads.
 //
 // plus the two domain kernels around it: per-contact features from the
-// stage-2 problem, and the map from the network output (a correction to the
-// previous step's impulses, when given) to starting impulses gamma0
-// projected onto the friction cone (the solve maps gamma0 to
-// v0 = v* + A^-1 J^T gamma0).  The reference warm-starts from the previous
+// stage-2 problem, and the map from the network output (a correction, in
+// SAP's unprojected impulse variable, to the previous step's impulses) to
+// starting impulses gamma0 through SAP's regularized cone projection (the
+// solve maps gamma0 to v0 = v* + A^-1 J^T gamma0).  The reference warm-starts from the previous
 // step's velocity only (sim/solver_sap.py:1441-1451); this network has no
 // counterpart there.
 #include <cuda_bf16.h>
@@ -30,6 +30,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "sapb_device.cuh"
 #include "sapb_internal.h"
 #include "sapb_umma.cuh"
 
@@ -638,9 +639,15 @@ struct ImpulseParams {
   const float* y;
   const double* gamma_prev;  // residual base (NULL: 0)
   sapb_warmstart_norm norm;
+  double beta, sigma, tau_fallback;
   double* gamma0;
 };
 
+// The network predicts a correction u (velocity units) of the unprojected
+// impulse y = -R^-1 (vc - vhat) of SAP's regularized projection; gamma0 is
+// the projection of y0 = gamma_prev + u / w_eff, i.e. the impulse SAP assigns
+// to the contact velocity vc = vhat - R y0 (sim/contact_solve.py:743-921).
+// Separated contacts have y_n well below zero and project to exactly zero.
 __global__ void impulses_kernel(const ImpulseParams P) {
   const int C = P.p.max_contacts;
   const long slots = (long)P.p.num_envs * C;
@@ -651,20 +658,17 @@ __global__ void impulses_kernel(const ImpulseParams P) {
     double g[3] = {0.0, 0.0, 0.0};
     if (c < count) {
       const double w = fmax(P.p.w_eff[s], 1.0e-12);
+      double y[3];
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        g[j] = ((double)P.y[3 * s + j] * P.norm.output_scale[j] + P.norm.output_shift[j]) / w;
-        if (P.gamma_prev) g[j] += P.gamma_prev[3 * s + j];
+        y[j] = ((double)P.y[3 * s + j] * P.norm.output_scale[j] + P.norm.output_shift[j]) / w;
+        if (P.gamma_prev) y[j] += P.gamma_prev[3 * s + j];
       }
-      // onto the friction cone: gamma_n >= 0, |gamma_t| <= mu gamma_n
-      g[2] = fmax(g[2], 0.0);
-      const double tm = sqrt(g[0] * g[0] + g[1] * g[1]);
-      const double lim = fmax(P.p.mu[s], 0.0) * g[2];
-      if (tm > lim) {
-        const double sc = tm > 0.0 ? lim / tm : 0.0;
-        g[0] *= sc;
-        g[1] *= sc;
-      }
+      const double tau = P.p.tau_d ? P.p.tau_d[s] : P.tau_fallback;
+      const ContactConst cc = make_contact_const(P.p.phi0[s], P.p.w_eff[s], P.p.mu[s], P.p.stiffness[s], tau, P.beta,
+                                                 P.sigma, P.p.dt[e]);
+      double cost;
+      project_contact(cc, -cc.rt * y[0], -cc.rt * y[1], cc.vhat_n - cc.rn * y[2], g, &cost, nullptr);
     }
     P.gamma0[3 * s + 0] = g[0];
     P.gamma0[3 * s + 1] = g[1];
@@ -864,15 +868,16 @@ int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const doubl
 }
 
 int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float* mlp_out,
-                                const double* gamma_prev, const sapb_warmstart_norm* norm, double* gamma0,
-                                void* stream) {
-  if (!problem || !mlp_out || !norm || !gamma0 || problem->num_envs < 0 || problem->max_contacts < 0) {
+                                const double* gamma_prev, const sapb_warmstart_norm* norm,
+                                const sapb_solve_options* opts, double* gamma0, void* stream) {
+  if (!problem || !mlp_out || !norm || !opts || !gamma0 || problem->num_envs < 0 || problem->max_contacts < 0) {
     set_last_error("sapb_warmstart_impulses: invalid argument");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   const long slots = (long)problem->num_envs * problem->max_contacts;
   if (slots == 0) return SAPB_OK;
-  if (!problem->contact_count || !problem->w_eff || !problem->mu) {
+  if (!problem->contact_count || !problem->w_eff || !problem->mu || !problem->phi0 || !problem->stiffness ||
+      !problem->dt) {
     set_last_error("sapb_warmstart_impulses: missing problem array");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
@@ -881,6 +886,9 @@ int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float
   P.y = mlp_out;
   P.gamma_prev = gamma_prev;
   P.norm = *norm;
+  P.beta = opts->contact_beta;
+  P.sigma = opts->contact_sigma;
+  P.tau_fallback = opts->contact_tau_d;
   P.gamma0 = gamma0;
   long blocks = (slots + 255) / 256;
   if (blocks > 8L * sm_count()) blocks = 8L * sm_count();

@@ -538,9 +538,11 @@ class SapContactSolve:
             P.v_guess = _ptr(v_guess)
             P.v_guess_active = _ptr(v_guess_active)
         if gamma0 is not None:
-            if gamma0.dtype != F64 or not gamma0.is_contiguous() or gamma0.numel() < W * P.max_contacts * 3:
-                raise TypeError("gamma0 must be a contiguous float64 (W, C, 3) tensor")
+            per_set = W * P.max_contacts * 3
+            if gamma0.dtype != F64 or not gamma0.is_contiguous() or gamma0.numel() < per_set:
+                raise TypeError("gamma0 must be a contiguous float64 (W, C, 3) or (K, W, C, 3) tensor")
             P.gamma0 = _ptr(gamma0)
+            P.gamma0_count = int(gamma0.numel() // per_set)
         if self.dof is not None:
             self._jq = _f64(state.joint_q)
             self.dof.joint_q = _ptr(self._jq)
@@ -594,12 +596,13 @@ class SolverSAP:
         convergence test stay FP64); warm_start, one of
           "previous_velocity"  the reference's: start from the last solution;
           "previous_impulses"  also try v* + A^-1 J^T gamma_prev;
-          "learned"            also try v* + A^-1 J^T gamma0, gamma0 from the
+          "learned"            also try v* + A^-1 J^T gamma_prev and
+                               v* + A^-1 J^T gamma0, gamma0 from the
                                per-contact network (learned_warm_start: a
                                LearnedWarmStart, a weights path, or None for
                                the packaged weights);
-        a candidate start replaces the previous-velocity start only if its
-        cost is lower, and Newton always runs to the same tolerance."""
+        the lowest-cost start among the previous-velocity one and the
+        candidates is taken, and Newton always runs to the same tolerance."""
         view = _ModelView(model)
         preset = dict(_CONTACT_PRESET_KWARGS[_normalize_contact_preset_variant(contact_preset_variant)])
         self.contact_preset_variant = _normalize_contact_preset_variant(contact_preset_variant)
@@ -682,8 +685,12 @@ class SolverSAP:
                 lw = LearnedWarmStart.load(DEFAULT_WEIGHTS if lw is None else str(lw), dev)
             self.learned_warm_start = lw
         C = self.max_rigid_contact
-        self._gamma_prev = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
+        # candidate impulse sets: [0] the previous step's impulses, [1] the network's
+        self._gamma_cand = torch.zeros(2, view.W, max(C, 1), 3, dtype=F64, device=dev)
+        self._gamma_prev = self._gamma_cand[0]
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
+        if self.learned_warm_start is not None:
+            self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
         self.reset_runtime_state()
 
     @property
@@ -709,8 +716,8 @@ class SolverSAP:
         self.last_line_search_iterations = 0
         self.last_converged = True
         self._v_guess_active.zero_()
-        if hasattr(self, "_gamma_prev"):
-            self._gamma_prev.zero_()
+        if hasattr(self, "_gamma_cand"):
+            self._gamma_cand.zero_()
         self.last_contacts = None
         self.last_contact_jacobian_result = None
         self.last_contact_solve_result = None
@@ -742,16 +749,18 @@ class SolverSAP:
         v0 = self.contact_jacobian._qd
         gamma0 = None
         if self.warm_start == "previous_impulses":
-            gamma0 = self._gamma_prev
+            gamma0 = self._gamma_cand[0]
         elif self.warm_start == "learned":
             self._normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
-            gamma0 = self.learned_warm_start.predict(
+            self.learned_warm_start.predict(
                 num_envs=self.view.W, dof_per_env=self.view.n, max_contacts=self.max_rigid_contact,
-                normal_up=self._normal_up, gamma_prev=self._gamma_prev, contact_count=cr.contact_env_count,
-                dynamics_matrix=cr.dynamics_matrix_env, jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0,
-                w_eff=cr.contact_env_w_eff, mu=cr.contact_env_mu, stiffness=cr.contact_env_stiffness,
-                tau_d=cr.contact_env_tau_d, v_star=self.contact_jacobian.v_star, v0=self.contact_jacobian.v_star,
+                normal_up=self._normal_up, gamma_prev=self._gamma_prev, out=self._gamma_cand[1],
+                contact_count=cr.contact_env_count, dynamics_matrix=cr.dynamics_matrix_env,
+                jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff,
+                mu=cr.contact_env_mu, stiffness=cr.contact_env_stiffness, tau_d=cr.contact_env_tau_d,
+                v_star=self.contact_jacobian.v_star, v0=self.contact_jacobian.v_star,
                 dt=self.contact_jacobian.dt_world)
+            gamma0 = self._gamma_cand
         sr = self.contact_solve.solve(
             cr, state_in, control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
             v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, gamma0=gamma0,

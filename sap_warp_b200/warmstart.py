@@ -16,11 +16,13 @@ composes with (the plain start it competes against is v_guess when active).
 Network inputs of a contact slot (raw): phi0; J_c v* in the contact frame
 (t1, t2, n); the world-up component of the contact normal (1 when unknown);
 mu; log10(stiffness); tau_d; dt; w_eff * gamma_prev (t1, t2, n; 0 when no
-previous impulses are given).  The network predicts the correction
-w_eff * (gamma* - gamma_prev) (velocity units) to the previous impulses, so a
-zero output reproduces the previous-impulse start; gamma* is the converged
-FP64 solve's.  Inputs and targets are standardised with the statistics of the
-training set, which travel with the weights.
+previous impulses are given).  The network predicts a correction
+w_eff * (y* - gamma_prev) (velocity units), y* being SAP's unprojected impulse
+-R^-1 (vc - vhat) at the converged FP64 solution; the impulse map projects
+gamma_prev + correction / w_eff with the solve's regularized cone projection,
+so separated contacts (y_n << 0) start at exactly zero impulse.  Inputs and
+targets are standardised with the statistics of the training set, which
+travel with the weights.
 """
 
 from __future__ import annotations
@@ -207,14 +209,23 @@ class WarmStartMLP:
 
 
 class LearnedWarmStart:
-    """Trained network + standardisation: gamma0 for a stage-2 problem."""
+    """Trained network + standardisation: gamma0 for a stage-2 problem.
+    contact_beta / contact_sigma / tau_fallback are the solve's
+    regularization, used to project the predicted unprojected impulses."""
 
-    def __init__(self, mlp: WarmStartMLP, norm: FeatureNorm, tau_fallback: float = 0.0):
+    def __init__(self, mlp: WarmStartMLP, norm: FeatureNorm, tau_fallback: float = 0.0, contact_beta: float = 1.0,
+                 contact_sigma: float = 1.0e-3):
         self.mlp = mlp
         self.norm = norm
         self.norm_struct = norm.struct()
         self.tau_fallback = float(tau_fallback)
+        self.set_regularization(contact_beta, contact_sigma, tau_fallback)
         self._bufs: dict = {}
+
+    def set_regularization(self, contact_beta: float, contact_sigma: float, tau_fallback: float) -> None:
+        self.tau_fallback = float(tau_fallback)
+        self.solve_options = make_options("armijo_decay", contact_beta=float(contact_beta),
+                                          contact_sigma=float(contact_sigma), contact_tau_d=float(tau_fallback))
 
     @property
     def device(self):
@@ -231,12 +242,13 @@ class LearnedWarmStart:
         return self._bufs[key]
 
     def predict(self, *, num_envs: int, dof_per_env: int, max_contacts: int, normal_up: torch.Tensor | None = None,
-                gamma_prev: torch.Tensor | None = None, **arrays) -> torch.Tensor:
-        """gamma0 (E, C, 3) FP64 on the device: features -> MLP -> impulses,
-        three launches on the current stream, no host sync, no allocation
-        after the first call for a shape."""
+                gamma_prev: torch.Tensor | None = None, out: torch.Tensor | None = None, **arrays) -> torch.Tensor:
+        """gamma0 (E, C, 3) FP64 on the device (into `out` if given):
+        features -> MLP -> impulses, three launches on the current stream, no
+        host sync, no allocation after the first call for a shape."""
         E, C = num_envs, max_contacts
         b = self.buffers(E, C)
+        g_out = b["gamma0"] if out is None else out
         P = build_problem(num_envs=E, dof_per_env=dof_per_env, max_contacts=C, **arrays)
         lib, s = load(), _stream(self.device)
         nu = 0 if normal_up is None else _dev_ptr(normal_up, F64, E * C, "normal_up")
@@ -245,8 +257,9 @@ class LearnedWarmStart:
                                           b["x"].data_ptr(), None, s), "sapb_warmstart_features")
         self.mlp.forward(b["x"], b["y"])
         check(lib.sapb_warmstart_impulses(ctypes.byref(P), b["y"].data_ptr(), gp, ctypes.byref(self.norm_struct),
-                                          b["gamma0"].data_ptr(), s), "sapb_warmstart_impulses")
-        return b["gamma0"]
+                                          ctypes.byref(self.solve_options), _dev_ptr(g_out, F64, E * C * 3, "out"), s),
+              "sapb_warmstart_impulses")
+        return g_out
 
     # ---- persistence ------------------------------------------------------------
     def save(self, path: str, **meta) -> None:
@@ -276,10 +289,31 @@ def raw_features(arrays: dict, num_envs: int, dof_per_env: int, max_contacts: in
     return raw
 
 
+def unprojected_targets(arrays: dict, v: torch.Tensor, num_envs: int, dof_per_env: int, max_contacts: int,
+                        contact_beta: float = 1.0, contact_sigma: float = 1.0e-3, tau_fallback: float = 0.0):
+    """(E*C, 3) u = w_eff * y of every slot: y = -R^-1 (J_c v - vhat), SAP's
+    unprojected impulse at the velocity v (sim/contact_solve.py:797-870), with
+    R_t = sigma w, R_n = max(beta^2 w / (4 pi^2), 1 / (dt k (dt + tau)))."""
+    E, n, C = num_envs, dof_per_env, max_contacts
+    J = arrays["jacobian"].reshape(E, C, 3, n)
+    vc = torch.einsum("ecrj,ej->ecr", J, v.reshape(E, n))
+    w = arrays["w_eff"].reshape(E, C).clamp(min=1e-12)
+    tau = arrays["tau_d"].reshape(E, C) if arrays.get("tau_d") is not None else torch.full_like(w, tau_fallback)
+    tau = tau.clamp(min=0.0)
+    k = arrays["stiffness"].reshape(E, C)
+    k = torch.where(k > 0, k, torch.ones_like(k))
+    dt = arrays["dt"].reshape(E, 1)
+    rt = (contact_sigma * w).clamp(min=1e-30)
+    rn = torch.maximum(contact_beta ** 2 / (4.0 * math.pi ** 2) * w, 1.0 / (dt * k * (dt + tau))).clamp(min=1e-30)
+    vhat = -arrays["phi0"].reshape(E, C) / (dt + tau)
+    y = torch.stack([-vc[..., 0] / rt, -vc[..., 1] / rt, (vhat - vc[..., 2]) / rn], -1)
+    return (w[..., None] * y).reshape(E * C, 3)
+
+
 def solver_dataset(problems, device, line_search_variant: str = "armijo_decay"):
-    """(raw inputs (N, 12), targets u = w_eff * gamma* (N, 3)) of every live
-    contact of the given scenes.ContactProblemArrays, gamma* from the
-    converged FP64 GPU solve at the reference tolerances."""
+    """(raw inputs (N, 12), targets u = w_eff * y* (N, 3)) of every live
+    contact of the given scenes.ContactProblemArrays, y* the unprojected
+    impulse at the converged FP64 GPU solve (reference tolerances)."""
     raws, us = [], []
     opts = make_options(line_search_variant)
     for prob in problems:
@@ -290,7 +324,7 @@ def solver_dataset(problems, device, line_search_variant: str = "armijo_decay"):
         contact_solve(**arrays, buffers=buf, options=opts)
         raw = raw_features(arrays, E, n, C, normal_up=nu)
         live = (torch.arange(C, device=device)[None, :] < arrays["contact_count"][:, None]).reshape(-1)
-        u = (arrays["w_eff"][..., None] * buf.contact_gamma[:, :C]).reshape(-1, 3)
+        u = unprojected_targets(arrays, buf.v, E, n, C)
         raws.append(raw[live])
         us.append(u[live].to(F32))
     return torch.cat(raws), torch.cat(us)
@@ -298,11 +332,12 @@ def solver_dataset(problems, device, line_search_variant: str = "armijo_decay"):
 
 def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every: int = 1,
                     hessian_precision: str = "fp64"):
-    """(raw inputs (N, 12), targets u = w_eff * gamma (N, 3)) of the live
+    """(raw inputs (N, 12), targets u = w_eff * y (N, 3)) of the live
     contacts along SolverSAP trajectories (reference warm start, FP64): at
     step k the inputs carry gamma_prev = the impulses of step k-1 in the same
     slot (slot order is canonical, so a persistent contact keeps its slot),
-    the targets are step k's converged impulses.  Every `every`-th step."""
+    the targets are the unprojected impulses y at step k's converged
+    velocity.  Every `every`-th step."""
     from . import models
     from .runtime import SapState
     from .solver import SolverSAP
@@ -329,7 +364,8 @@ def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every:
                 raw = raw_features(arrays, W, n, C, normal_up=normal_up, gamma_prev=gamma_prev)
                 cnt = cr.contact_env_count.clamp(max=C)
                 live = (torch.arange(C, device=device)[None, :] < cnt[:, None]).reshape(-1)
-                u = (cr.contact_env_w_eff[..., None] * solver.contact_solve.contact_gamma).reshape(-1, 3)
+                u = unprojected_targets(arrays, solver.contact_solve.v_flat, W, n, C,
+                                        solver.contact_solve.contact_beta, solver.contact_solve.contact_sigma)
                 raws.append(raw[live])
                 us.append(u[live].to(F32))
             gamma_prev.copy_(solver.contact_solve.contact_gamma)
@@ -337,10 +373,19 @@ def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every:
     return torch.cat(raws), torch.cat(us)
 
 
-def residual_targets(raw: torch.Tensor, u: torch.Tensor) -> torch.Tensor:
-    """w_eff * (gamma* - gamma_prev): the targets u minus the w-scaled
-    previous impulses carried in raw input columns 9..11."""
-    return (u - raw[:, 9:12]).contiguous()
+def residual_targets(raw: torch.Tensor, u: torch.Tensor, clip_quantile: float = 0.005) -> torch.Tensor:
+    """w_eff * (y* - gamma_prev): the targets u minus the w-scaled previous
+    impulses carried in raw input columns 9..11, each component clipped to
+    its [q, 1-q] quantile range (separated contacts have arbitrarily negative
+    y_n, and every value beyond the range projects the same way)."""
+    r = (u - raw[:, 9:12]).contiguous()
+    if clip_quantile > 0.0 and r.shape[0] > 0:
+        k = min(r.shape[0], 1 << 20)
+        sample = r[torch.randperm(r.shape[0], device=r.device)[:k]]
+        lo = torch.quantile(sample, clip_quantile, dim=0)
+        hi = torch.quantile(sample, 1.0 - clip_quantile, dim=0)
+        r = torch.maximum(torch.minimum(r, hi), lo)
+    return r
 
 
 def train(mlp: WarmStartMLP, raw: torch.Tensor, u: torch.Tensor, norm: FeatureNorm, steps: int = 4000,
