@@ -1,21 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the SAP contact step on one node.
 
-Workload (BASELINE metric, config "batched uniform"): 4096 worlds of a 35-DOF
-floating-base humanoid (6 + 29 revolute, serial-chain tree), 8-32 contacts per
-world, phi0 ~ U[-2e-3, 0], mu ~ U[0.3, 1], v* ~ N(0, 0.5); seeded synthetic
-inputs (no dataset exists for this path).  A step is one SAP stage-2 solve of
-all worlds (prepare + Newton + armijo_decay line search to the reference's
-tolerances) from the cold start v0, so every step does the full work.
+Workload (batched uniform humanoids): 4096 worlds of a 35-DOF floating-base
+humanoid (6 + 29 revolute, serial-chain tree), 8-32 body-vs-ground point
+contacts per world on the distal links, phi0 ~ U[-2e-3, 0] m at the start,
+mu ~ U[0.3, 1], pair stiffness 1e5 N/m, dissipation time 0.01 s, joint
+velocities ~ N(0, 0.5), dt = 2 ms; seeded synthetic inputs (no dataset exists
+for this path).  A step is one full SolverSAP.step of all worlds -- free
+motion, contact Jacobian, the stage-2 Newton solve with armijo_decay to the
+reference's tolerances (optimality 1e-14 abs / 1e-6 rel), position
+integration -- and the timed steps continue one rollout.
 
-`value` is world-steps/s of the fast path (FP32 Hessian/factorization, FP64
-gradient/cost/line search/convergence) with inputs resident in HBM; the plain
-FP64 solve is reported beside it.  `e2e` is the same metric through the
-public API with host inputs: pinned host -> device copy of the step's inputs
-and a device -> host read of the solved velocities inside the timed region.
+Arms (same scene, same trajectory up to the solve tolerance):
+  value        learned + FP32: FP32 Hessian / factorization with FP64
+               gradient, cost, line search and convergence test, and the
+               learned warm start (previous impulses and the network's
+               correction tried against the previous velocity);
+  plain_fp64   the reference's method: FP64 throughout, warm start from the
+               previous step's velocity;
+  previous_impulses_fp32   the ablation without the network.
+`e2e` is the headline arm through the public API with host buffers: the
+step's inputs (state and contacts) copied from pinned host memory and the new
+state read back inside the timed region.  `stage2_solve_only` is the contact
+solve alone on the stage-2 snapshot of the same configuration (A, J given).
 
-Multi-GPU (torchrun): worlds are independent, so each rank solves its own
-4096 worlds (weak scaling, no data-path collective); the barrier and the
+Multi-GPU (torchrun): worlds are independent, so each rank steps its own 4096
+worlds (weak scaling, no data-path collective); the barrier and the
 max-over-ranks reduction of the timings are the only collectives.
 """
 
@@ -33,13 +43,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one solve
-# launch on this workload, measured once with ncu.
-NCU_TRAFFIC_BYTES = 117.821440e6 + 5.310464e6
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one contact
+# solve launch of the headline arm on this workload, from one ncu capture.
+NCU_SOLVE_TRAFFIC_BYTES = None
 
 METRIC = "world-steps/s, 4096 humanoids: learned+FP32 vs plain FP64, same B200, same tol"
 WORLDS = 4096
 SEED = 2
+DT = 2.0e-3
+MAX_CONTACTS = 32
 
 
 def parse():
@@ -50,17 +62,21 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--worlds", type=int, default=WORLDS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--weights", default=None, help="warm-start network weights (default: packaged)")
     return ap.parse_args()
 
 
-def algorithmic_bytes(prob) -> int:
-    """Compulsory FP64 I/O of the contact solve, world by world with the actual
-    contact count: 8*[3*C*n + n^2 + 2n + 5C] (A, J, v*, v0, contact params)
-    plus 8*[n + 3C] (v and gamma written)."""
-    n = prob.dof_per_env
-    C = np.clip(prob.contact_count.astype(np.int64), 0, prob.max_contacts)
-    per_world = 8 * (3 * C * n + n * n + 2 * n + 5 * C) + 8 * (n + 3 * C)
-    return int(per_world.sum())
+def solve_bytes_per_world(n: int, counts: np.ndarray, candidate_sets: int) -> np.ndarray:
+    """Compulsory FP64 I/O of the contact solve per world with the actual
+    contact count C: reads A (n^2), J (3Cn), v*, v0, v_guess (3n), 5 contact
+    parameters (5C); writes v, v_guess (2n), gamma (3C), mode (C/2 words);
+    plus for candidate starts the factor (n^2) and the impulse sets (3C
+    each)."""
+    C = counts.astype(np.int64)
+    b = 8 * (n * n + 3 * C * n + 3 * n + 5 * C) + 8 * (2 * n + 3 * C) + 4 * C
+    if candidate_sets:
+        b = b + 8 * (n * n + candidate_sets * 3 * C)
+    return b
 
 
 class ClockSampler:
@@ -140,47 +156,84 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(inside)}
 
 
-def oracle_time(prob, steps: int, threads: int, min_seconds: float = 0.0):
-    """Seconds per full-batch oracle solve (armijo_decay, FP64)."""
-    from oracle import oracle
+# ---- CPU pipeline of the step (oracle restatement), for the baselines ---------
+def cpu_scene(worlds: int, seed: int):
+    """The rollout scene built on the host: same distributions as
+    models.rollout_scene, body poses from the numpy free motion."""
+    from oracle import free_motion as ofm
+    from sap_warp_b200 import models
 
-    oracle.solve(prob.subset(np.arange(min(prob.num_envs, 64))), "armijo_decay", threads=threads)  # warm
-    times = []
-    t_start = time.perf_counter()
-    for _ in range(max(1, steps)):
-        t0 = time.perf_counter()
-        oracle.solve(prob, "armijo_decay", threads=threads)
-        times.append(time.perf_counter() - t0)
-        if min_seconds and time.perf_counter() - t_start > min_seconds:
+    rng = np.random.default_rng(seed)
+    tpl = models.world_template("humanoid", rng)
+    g = models.replicate(tpl, worlds, rng, mu_range=(0.3, 1.0), stiffness=1.0e5, tau_d=0.005)
+    q = models.random_joint_q(tpl, rng, worlds)
+    n, B = tpl["dofs_per_world"], tpl["bodies_per_world"]
+    qd = rng.normal(scale=0.5, size=(worlds, n))
+    om = ofm.Model(dict(tpl, gravity=g["gravity"][0], shape_body_global=g["shape_body"],
+                        shape_mu=g["shape_material_mu"], shape_ke=g["shape_material_ke"],
+                        shape_tau=g["shape_material_tau"]))
+    fm = ofm.free_motion(om, q, qd, np.zeros_like(qd), np.zeros((worlds, B, 6)), np.full(worlds, DT))
+    counts = rng.integers(8, 33, size=worlds)
+    con = models.ground_contacts(rng, fm["pos"], fm["quat"], counts, bodies_from=B // 2, capacity=int(counts.sum()))
+    return dict(tpl=tpl, om=om, q=q, qd=qd, con=con)
+
+
+def cpu_steps(scene: dict, steps: int, threads: int, min_seconds: float = 0.0):
+    """Seconds per world-step of the CPU pipeline (numpy free motion and
+    contact rows, C oracle solve with OpenMP, numpy integration), drake
+    preset, FP64, previous-velocity warm start."""
+    from oracle import free_motion as ofm
+    from oracle import oracle
+    from sap_warp_b200 import scenes
+
+    om, tpl = scene["om"], scene["tpl"]
+    q, qd = scene["q"].copy(), scene["qd"].copy()
+    W, n, B = q.shape[0], tpl["dofs_per_world"], tpl["bodies_per_world"]
+    dt = np.full(W, DT)
+    done, t0 = 0, time.perf_counter()
+    for k in range(max(1, steps)):
+        fm = ofm.free_motion(om, q, qd, np.zeros_like(qd), np.zeros((W, B, 6)), dt)
+        cr = ofm.contact_jacobian(om, fm, scene["con"], MAX_CONTACTS, point_mode="contact_midpoint",
+                                  weight_mode="diag_delassus", fallback_tau=0.0)
+        prob = scenes.ContactProblemArrays(
+            num_envs=W, dof_per_env=n, max_contacts=MAX_CONTACTS, bodies_per_env=B,
+            contact_count=cr["count"].astype(np.int32), dynamics_matrix=fm["A"], jacobian=cr["jac"],
+            phi0=cr["phi0"], w_eff=cr["w"], mu=cr["mu"], stiffness=cr["k"], tau_d=cr["tau"], body0=cr["body0"],
+            body1=cr["body1"], body_dof_start=np.zeros(W * B, np.int32), body_dof_count=np.full(W * B, n, np.int32),
+            v_star=fm["v_star"].reshape(-1), v0=qd.reshape(-1), dt=dt)
+        sol = oracle.solve(prob, "armijo_decay", threads=threads, v_guess=qd.reshape(-1), v_guess_active=k > 0)
+        v = sol["v"].reshape(W, n)
+        q = ofm.integrate(om, q, qd, v, dt, "sap_euler")
+        qd = v
+        done += 1
+        if min_seconds and time.perf_counter() - t0 > min_seconds:
             break
-    return float(np.mean(times)), len(times)
+    return (time.perf_counter() - t0) / done, done
 
 
 def run_reference(args, rank: int, world_size: int):
     """Reference arm: the reference's own implementation is Python + NVIDIA
-    Warp, which cannot be installed here, so the CPU restatement of its
-    algorithm (oracle/, FP64, OpenMP over worlds) is timed on all host cores."""
+    Warp, which cannot be installed here, so the CPU restatement of its step
+    (oracle/, FP64, OpenMP over worlds in the solve) is timed on the host."""
     if rank != 0:
         return
-    from sap_warp_b200 import scenes
-
-    prob = scenes.humanoid_contact_problem(args.worlds, seed=SEED)
     cores = os.cpu_count() or 1
-    for _ in range(max(0, args.warmup)):
-        oracle_time(prob.subset(np.arange(min(256, prob.num_envs))), 1, cores)
-    sec, k = oracle_time(prob, args.steps, cores, min_seconds=60.0)
-    value = prob.num_envs / sec
+    sample_worlds = 128
+    scene = cpu_scene(sample_worlds, SEED)
+    cpu_steps(scene, max(1, min(args.warmup, 2)), cores)
+    sec, k = cpu_steps(scene, max(args.steps, 1), cores, min_seconds=60.0)
+    value = sample_worlds / sec
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "world-steps/s", "n_gpus": args.gpus,
         "steps": k, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, shapes of the batched-uniform config)",
-        "config": {"workload": f"{prob.num_envs} humanoid worlds x 35 DOF, 8-32 contacts, armijo_decay, FP64",
-                   "worlds": prob.num_envs, "dof_per_env": prob.dof_per_env, "max_contacts": prob.max_contacts},
+        "config": {"workload": f"humanoid rollout, 35 DOF, 8-32 contacts, full SAP step, armijo_decay, FP64, "
+                               f"sampled on {sample_worlds} worlds", "worlds": sample_worlds},
         "cpu_baseline": {"value": value, "unit": "world-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"{k} full {prob.num_envs}-world solves"},
+                         "sample": f"{k} steps of a {sample_worlds}-world rollout"},
         "e2e": {"value": value, "unit": "world-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference (Python + NVIDIA Warp) is not installable offline; the FP64 CPU restatement of its "
-                "algorithm is timed instead",
+                "step is timed instead",
     }
     print(json.dumps(line), flush=True)
 
@@ -196,8 +249,11 @@ def main():
 
     import torch
 
-    from sap_warp_b200 import scenes
+    from sap_warp_b200 import models, scenes
     from sap_warp_b200._solve import ContactSolveBuffers, contact_solve, make_options, problem_to_device
+    from sap_warp_b200.runtime import SapState
+    from sap_warp_b200.solver import SolverSAP
+    from sap_warp_b200.warmstart import DEFAULT_WEIGHTS, LearnedWarmStart
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -206,12 +262,6 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-
-    prob = scenes.humanoid_contact_problem(args.worlds, seed=SEED + 1000 * rank)
-    t = problem_to_device(prob, dev)
-    buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, dev)
-    opt_fast = make_options("armijo_decay", hessian_precision="fp32", linear_solve_precision="fp32")
-    opt_fp64 = make_options("armijo_decay")
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
@@ -226,100 +276,165 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         return float(tt.item())
 
-    def timed(opts, steps, warmup, sampler=None):
-        for _ in range(warmup):
-            contact_solve(**t, buffers=buf, options=opts)
+    model, state0, control, contacts, _ = models.rollout_scene("humanoid", args.worlds, SEED + 1000 * rank, dev)
+    W = args.worlds
+    ws = LearnedWarmStart.load(args.weights or DEFAULT_WEIGHTS, dev)
+
+    def fresh_states():
+        a = SapState(joint_q=state0.joint_q.clone(), joint_qd=state0.joint_qd.clone(), body_q=state0.body_q.clone(),
+                     body_f=state0.body_f.clone())
+        b = SapState(joint_q=state0.joint_q.clone(), joint_qd=state0.joint_qd.clone(), body_q=state0.body_q.clone(),
+                     body_f=state0.body_f.clone())
+        return a, b
+
+    def make_solver(prec, warm):
+        return SolverSAP(model, max_rigid_contact=MAX_CONTACTS, contact_preset_variant="drake",
+                         hessian_precision=prec, warm_start=warm, learned_warm_start=ws if warm == "learned" else None)
+
+    def run_arm(prec, warm, sampler=None):
+        solver = make_solver(prec, warm)
+        s_in, s_out = fresh_states()
+        for _ in range(args.warmup):
+            solver.step(s_in, s_out, control, contacts, DT)
+            s_in, s_out = s_out, s_in
         barrier()
+        solver.stage_events = []
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        iters, chosen = [], []
         if sampler:
             sampler.mark_begin()
         ev0.record(stream)
-        for _ in range(steps):
-            contact_solve(**t, buffers=buf, options=opts)
+        for _ in range(args.steps):
+            solver.step(s_in, s_out, control, contacts, DT)
+            iters.append(solver.contact_solve.newton_iterations_env.sum())
+            chosen.append(torch.bincount(solver.contact_solve.warm_start_accepted_env.long(), minlength=3))
+            s_in, s_out = s_out, s_in
         ev1.record(stream)
         barrier()
         if sampler:
             sampler.mark_end()
-        return max_over_ranks(ev0.elapsed_time(ev1) / steps)
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+        stages = {k: v / args.steps for k, v in solver.stage_times().items()}
+        solver.stage_events = None
+        it = float(torch.stack(iters).double().sum().item()) / (args.steps * W)
+        ch = torch.stack(chosen).sum(0).cpu().numpy()
+        conv = bool(solver.contact_solve.converged_env.all())
+        counts = solver.contact_jacobian.contact_env_count.clamp(max=MAX_CONTACTS).cpu().numpy()
+        return dict(ms=ms, stages=stages, iters=it, chosen=ch, converged=conv, counts=counts, solver=solver,
+                    final=s_in)
 
-    # plain FP64 solve
-    ms_fp64 = timed(opt_fp64, args.steps, args.warmup)
-    it_fp64 = float(buf.newton_iterations.double().mean())
-    conv_fp64 = bool(buf.converged.all())
-    v_fp64 = buf.v.clone()
-    # fast path (the headline)
+    plain = run_arm("fp64", "previous_velocity")
+    prev = run_arm("fp32", "previous_impulses")
     sampler = ClockSampler(local_rank)
     sampler.start()
-    ms_fast = timed(opt_fast, args.steps, args.warmup, sampler)
+    fast = run_arm("fp32", "learned", sampler)
     clocks = sampler.stop()
-    it_fast = float(buf.newton_iterations.double().mean())
-    conv_fast = bool(buf.converged.all())
-    rel = float(((buf.v - v_fp64).abs().view(-1, prob.dof_per_env).amax(1) /
-                 v_fp64.abs().view(-1, prob.dof_per_env).amax(1)).max())
+    # final states of the arms agree to the solve tolerance
+    dq = float((fast["final"].joint_qd - plain["final"].joint_qd).abs().max() /
+               plain["final"].joint_qd.abs().max().clamp(min=1e-30))
 
-    # end to end through the public API with host buffers
-    host = {k: v.cpu().pin_memory() for k, v in t.items()}
-    dev_in = {k: torch.empty_like(v) for k, v in t.items()}
-    v_host = torch.empty(buf.v.shape, dtype=buf.v.dtype).pin_memory()
-    h2d = sum(v.numel() * v.element_size() for v in host.values())
-    d2h = v_host.numel() * v_host.element_size()
+    # ---- end to end through the public API with host buffers -----------------
+    solver = make_solver("fp32", "learned")
+    s_in, s_out = fresh_states()
+    host_q = state0.joint_q.cpu().pin_memory()
+    host_qd = state0.joint_qd.cpu().pin_memory()
+    c_names = [k for k in vars(contacts) if isinstance(getattr(contacts, k), torch.Tensor)]
+    host_c = {k: getattr(contacts, k).cpu().pin_memory() for k in c_names}
+    h2d = (host_q.numel() * 8 + host_qd.numel() * 8 + sum(v.numel() * v.element_size() for v in host_c.values()))
+    d2h = host_q.numel() * 8 + host_qd.numel() * 8
 
-    def e2e_step():
-        for k, v in host.items():
-            dev_in[k].copy_(v, non_blocking=True)
-        contact_solve(**dev_in, buffers=buf, options=opt_fast)
-        v_host.copy_(buf.v, non_blocking=True)
+    def e2e_step(a, b):
+        a.joint_q.copy_(host_q, non_blocking=True)
+        a.joint_qd.copy_(host_qd, non_blocking=True)
+        for k, v in host_c.items():
+            getattr(contacts, k).copy_(v, non_blocking=True)
+        solver.step(a, b, control, contacts, DT)
+        host_q.copy_(b.joint_q, non_blocking=True)
+        host_qd.copy_(b.joint_qd, non_blocking=True)
 
     for _ in range(args.warmup):
-        e2e_step()
+        e2e_step(s_in, s_out)
+        s_in, s_out = s_out, s_in
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        e2e_step()
+        e2e_step(s_in, s_out)
+        s_in, s_out = s_out, s_in
     e1.record(stream)
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
 
-    alg = algorithmic_bytes(prob)
-    total_worlds = prob.num_envs * world_size
-    value = total_worlds / (ms_fast * 1e-3)
+    # ---- stage-2 solve alone on the snapshot of the configuration -------------
+    prob = scenes.humanoid_contact_problem(args.worlds, seed=SEED + 1000 * rank)
+    t = problem_to_device(prob, dev)
+    buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, dev)
+    snap = {}
+    for label, opts in (("fp64", make_options("armijo_decay")),
+                        ("fp32", make_options("armijo_decay", hessian_precision="fp32"))):
+        for _ in range(args.warmup):
+            contact_solve(**t, buffers=buf, options=opts)
+        barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k_snap = max(1, min(args.steps, 50))
+        a0.record(stream)
+        for _ in range(k_snap):
+            contact_solve(**t, buffers=buf, options=opts)
+        a1.record(stream)
+        barrier()
+        ms = max_over_ranks(a0.elapsed_time(a1) / k_snap)
+        snap[label] = {"value": prob.num_envs * world_size / (ms * 1e-3), "ms_per_solve": ms,
+                       "mean_newton_iterations": float(buf.newton_iterations.double().mean())}
+
+    total = W * world_size
+    value = total / (fast["ms"] * 1e-3)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = alg / (ms_fast * 1e-3) / 1e9
+    n = 35
+    solve_ms = fast["stages"].get("contact_solve", float("nan"))
+    alg = float(solve_bytes_per_world(n, fast["counts"], 2).sum())
+    achieved = alg / (solve_ms * 1e-3) / 1e9
+    launches_per_step = 8  # scatter, free motion, solve, integrate, features, mlp, impulses, + the solve's memset
     line = {
         "metric": METRIC, "value": value, "unit": "world-steps/s", "n_gpus": world_size, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_fast, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (FP32 Hessian/factor)", "data": "synthetic (seeded)",
-        "config": {"workload": f"{prob.num_envs} humanoid worlds x 35 DOF (6+29 revolute), 8-32 contacts, "
-                               "armijo_decay to reference tolerances, cold start v0",
-                   "worlds_per_gpu": prob.num_envs, "dof_per_env": prob.dof_per_env,
-                   "max_contacts": prob.max_contacts, "parallelism": f"world shards x{world_size}",
-                   "l2": "inputs (A+J = %.0f MB) larger than L2" % (alg / 1e6)},
-        "plain_fp64": {"value": total_worlds / (ms_fp64 * 1e-3), "ms_per_step": ms_fp64,
-                       "mean_newton_iterations": it_fp64, "all_converged": conv_fp64},
-        "fast": {"mean_newton_iterations": it_fast, "all_converged": conv_fast,
-                 "max_rel_v_diff_vs_fp64": rel, "speedup_vs_fp64": ms_fp64 / ms_fast},
-        "e2e": {"value": total_worlds / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak,
-                     "traffic": NCU_TRAFFIC_BYTES if args.worlds == WORLDS else None,
-                     "note": "kernel is FP64/FP32-pipe bound, not HBM bound; achieved = algorithmic bytes / "
-                             "kernel time (of measured peak)"},
-        "gpu_launches": args.steps,
+        "warmup": args.warmup, "ms_per_step": fast["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (FP32 Hessian/factor)", "data": "synthetic (seeded rollout scene)",
+        "config": {"workload": f"{W} humanoid worlds x 35 DOF (6+29 revolute), 8-32 ground contacts, full "
+                               "SolverSAP step (drake preset), armijo_decay to reference tolerances, rollout",
+                   "worlds_per_gpu": W, "dof_per_env": n, "max_contacts": MAX_CONTACTS, "dt": DT,
+                   "parallelism": f"world shards x{world_size}",
+                   "l2": "per-step working set (A, J, factor, rows) larger than L2"},
+        "plain_fp64": {"value": total / (plain["ms"] * 1e-3), "ms_per_step": plain["ms"],
+                       "mean_newton_iterations": plain["iters"], "all_converged": plain["converged"],
+                       "stages_ms": plain["stages"]},
+        "learned_fp32": {"mean_newton_iterations": fast["iters"], "all_converged": fast["converged"],
+                         "chosen_start": {"previous_velocity": int(fast["chosen"][0]),
+                                          "previous_impulses": int(fast["chosen"][1]),
+                                          "network": int(fast["chosen"][2])},
+                         "stages_ms": fast["stages"], "speedup_vs_plain_fp64": plain["ms"] / fast["ms"],
+                         "max_rel_qd_diff_vs_plain_fp64_after_rollout": dq},
+        "previous_impulses_fp32": {"value": total / (prev["ms"] * 1e-3), "ms_per_step": prev["ms"],
+                                   "mean_newton_iterations": prev["iters"], "stages_ms": prev["stages"]},
+        "stage2_solve_only": snap,
+        "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "kernel": "contact_solve_kernel", "achieved": achieved, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": NCU_SOLVE_TRAFFIC_BYTES,
+                     "note": "achieved = algorithmic bytes of the solve launch / its mean duration inside the "
+                             "timed steps (of measured peak); the kernel is latency bound, not HBM bound"},
+        "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        sample = prob.subset(np.arange(min(1024, prob.num_envs)))
-        sec, k = oracle_time(sample, 200, cores, min_seconds=10.0)
-        line["cpu_baseline"] = {"value": sample.num_envs / sec, "unit": "world-steps/s", "cores": cores,
-                                "kind": "port", "sample": f"{k} solves of {sample.num_envs} worlds"}
+        scene = cpu_scene(64, SEED)
+        sec, k = cpu_steps(scene, 1000, cores, min_seconds=10.0)
+        line["cpu_baseline"] = {"value": 64 / sec, "unit": "world-steps/s", "cores": cores, "kind": "port",
+                                "sample": f"{k} steps of a 64-world rollout (numpy free motion and rows, C solve)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -152,6 +152,10 @@ typedef struct sapb_contact_problem {
    * v0) and the candidates.  gamma0_count <= 1 means one set. */
   const double* gamma0;
   int32_t gamma0_count;
+  /* Optional [E,n,n] LDL^T factor of dynamics_matrix as written by
+   * sapb_free_motion_contacts (dynamics_factor output): the candidate starts
+   * solve with it instead of factoring A again.  NULL: factor in the solve. */
+  const double* dynamics_factor;
 } sapb_contact_problem;
 
 /* Outputs: the SapContactSolveResult fields a caller reads
@@ -260,6 +264,8 @@ typedef struct sapb_prepare_outputs {
   double* frame;                    /* [W][C][9] rows t1, t2, n, or NULL */
   int32_t* truncated_count;         /* [1] contacts beyond max_contacts, or NULL */
   double* body_q;                   /* [B][7] start-of-step body poses, or NULL */
+  double* dynamics_factor;          /* [W][n][n] LDL^T of A (below the diagonal L_ik d_k, on it d_k;
+                                       above it unspecified), or NULL */
 } sapb_prepare_outputs;
 
 /* Device workspace bytes of sapb_free_motion_contacts. */

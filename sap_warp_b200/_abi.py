@@ -115,6 +115,7 @@ class ContactProblem(C.Structure):
         ("dof", C.POINTER(DofTerms)),
         ("gamma0", _p),
         ("gamma0_count", C.c_int32),
+        ("dynamics_factor", _p),
     ]
 
 
@@ -220,6 +221,7 @@ class PrepareOutputs(C.Structure):
         ("frame", _p),
         ("truncated_count", _p),
         ("body_q", _p),
+        ("dynamics_factor", _p),
     ]
 
 

@@ -1075,14 +1075,23 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         double best_cost = e4p[0];
         const int ldj = w.ldJ(), ldh = w.ldH();
         for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
-        {
+        if (P.p.dynamics_factor) {
+          // the free motion's LDL^T of A
+          const double* Lg = P.p.dynamics_factor + (size_t)e * n * n;
+          const int lane = tid & 31, warp = tid >> 5;
+          for (int i = warp; i < n; i += NT / 32)
+            for (int j = lane; j <= i; j += 32) w.H[(size_t)i * ldh + j] = HT(__ldg(Lg + (size_t)i * n + j));
+          HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
+          for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
+          __syncthreads();
+        } else {
           const int lane = tid & 31, warp = tid >> 5;
           for (int i = warp; i < n; i += NT / 32)
             for (int j = lane; j <= i; j += 32) w.H[(size_t)i * ldh + j] = HT(__ldg(w.A + (size_t)i * n + j));
+          for (int i = tid; i < n; i += NT) w.V(V_GRAD)[i] = 0.0;
+          __syncthreads();
+          factor_and_solve<NT, HT, NS>(w);  // the factor of A (the solve of a zero rhs is unused)
         }
-        for (int i = tid; i < n; i += NT) w.V(V_GRAD)[i] = 0.0;
-        __syncthreads();
-        factor_and_solve<NT, HT, NS>(w);  // the factor of A (the solve of a zero rhs is unused)
         bool last_is_best = false;
         for (int k = 0; k < K; ++k) {
           const double* g0 = P.p.gamma0 + ((size_t)k * P.p.num_envs + e) * C * 3;

@@ -488,6 +488,13 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     __syncthreads();
   }
   for (int k = tid; k < n; k += kPrepNT) dinv[k] = fast_recip(H[(size_t)k * n + k]);
+  if (P.out.dynamics_factor) {
+    double* Lg = P.out.dynamics_factor + (size_t)e * n * n;
+    for (int k = tid; k < n * n; k += kPrepNT) {
+      const int i = k / n, j = k - i * n;
+      if (j <= i) Lg[k] = H[k];
+    }
+  }
   __syncthreads();
   if (tid < 32) {
     // lanes own rows lane + 32 r (n <= 128): forward z = D^-1 L^-1 tau, then x = L^-T z

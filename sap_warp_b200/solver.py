@@ -222,6 +222,9 @@ class SapContactJacobianResult:
     body_jacobian_local: torch.Tensor | None
     dynamics_matrix_env: torch.Tensor
     contact_env_tau_d: torch.Tensor | None = None
+    # LDL^T of dynamics_matrix_env from the free-motion solve (no counterpart
+    # in the reference's result), or None when not requested
+    dynamics_factor_env: torch.Tensor | None = None
 
 
 @dataclass(frozen=True)
@@ -295,6 +298,7 @@ class SapContactJacobian:
         self.contact_env_R_WC = z(W, C, 3, 3)
         self.truncated = z(1, dt=I32)
         self.body_q_sap = z(v.W * v.Bw, 7)
+        self.dynamics_factor_env = None  # allocated by keep_dynamics_factor()
         self.dt_world = z(W)
         ws = int(load().sapb_prepare_workspace_size(ctypes.byref(v.desc), C))
         self.workspace = torch.zeros(max(ws, 16), dtype=torch.uint8, device=dev)
@@ -308,6 +312,13 @@ class SapContactJacobian:
         o.point, o.frame = _ptr(self.contact_env_point), _ptr(self.contact_env_R_WC)
         o.truncated_count, o.body_q = _ptr(self.truncated), _ptr(self.body_q_sap)
         self.outputs = o
+
+    def keep_dynamics_factor(self) -> None:
+        """Also write the free-motion LDL^T of A (for candidate starts)."""
+        if self.dynamics_factor_env is None:
+            v = self.view
+            self.dynamics_factor_env = torch.zeros(v.W, v.n, v.n, dtype=F64, device=v.device)
+            self.outputs.dynamics_factor = _ptr(self.dynamics_factor_env)
 
     def set_dt(self, dt) -> None:
         """Per-world time step (scalar or [W] tensor), sim/solver_sap.py:975-992."""
@@ -380,7 +391,8 @@ class SapContactJacobian:
             contact_env_R_WC=self.contact_env_R_WC, contact_env_point=self.contact_env_point,
             contact_env_witness0=None, contact_env_witness1=None, contact_env_body0=self.contact_env_body0,
             contact_env_body1=self.contact_env_body1, body_jacobian_local=None,
-            dynamics_matrix_env=self.dynamics_matrix_env, contact_env_tau_d=self.contact_env_tau_d)
+            dynamics_matrix_env=self.dynamics_matrix_env, contact_env_tau_d=self.contact_env_tau_d,
+            dynamics_factor_env=self.dynamics_factor_env)
 
     @property
     def free_motion_result(self) -> SapFreeMotionResult:
@@ -543,6 +555,8 @@ class SapContactSolve:
                 raise TypeError("gamma0 must be a contiguous float64 (W, C, 3) or (K, W, C, 3) tensor")
             P.gamma0 = _ptr(gamma0)
             P.gamma0_count = int(gamma0.numel() // per_set)
+            if getattr(contact_result, "dynamics_factor_env", None) is not None:
+                P.dynamics_factor = _ptr(contact_result.dynamics_factor_env)
         if self.dof is not None:
             self._jq = _f64(state.joint_q)
             self.dof.joint_q = _ptr(self._jq)
@@ -672,6 +686,7 @@ class SolverSAP:
         dev = view.device
         self._v_guess_active = torch.zeros(1, dtype=I32, device=dev)
         self._q_out_tmp = torch.zeros(int(model.joint_coord_count), dtype=F64, device=dev)
+        self.stage_events = None  # list -> per-stage CUDA events (see _mark)
         self.warm_start = str(warm_start).strip().lower().replace("-", "_")
         if self.warm_start not in ("previous_velocity", "previous_impulses", "learned"):
             raise ValueError("warm_start must be 'previous_velocity', 'previous_impulses' or 'learned', "
@@ -691,6 +706,8 @@ class SolverSAP:
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
         if self.learned_warm_start is not None:
             self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
+        if self.warm_start != "previous_velocity":
+            self.contact_jacobian.keep_dynamics_factor()
         self.reset_runtime_state()
 
     @property
@@ -705,6 +722,26 @@ class SolverSAP:
 
     def notify_model_changed(self, flags: int) -> None:
         return
+
+    def _mark(self, stage: str | None) -> None:
+        """Stage timing: when `stage_events` is a list, record a CUDA event on
+        the current stream at each stage boundary as (stage, event); the
+        stage ends at the next record (None closes the step)."""
+        if self.stage_events is not None:
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(torch.cuda.current_stream(self.view.device))
+            self.stage_events.append((stage, ev))
+
+    def stage_times(self) -> dict:
+        """Milliseconds per stage summed over the recorded steps (syncs)."""
+        out: dict = {}
+        ev = self.stage_events or []
+        if ev:
+            ev[-1][1].synchronize()
+        for (name, e0), (_, e1) in zip(ev[:-1], ev[1:]):
+            if name is not None:
+                out[name] = out.get(name, 0.0) + e0.elapsed_time(e1)
+        return out
 
     def reset_runtime_state(self, state: SapState | None = None) -> None:
         """sim/solver_sap.py:1004-1017"""
@@ -741,12 +778,15 @@ class SolverSAP:
                 raise ValueError(f"Unsupported SapState joint_qd_order={s.joint_qd_order!r}.")
         self.contact_jacobian.set_dt(dt)
         self.last_contacts = contacts
+        mark = self._mark
+        mark("free_motion")
         cr = self.contact_jacobian.compute(state_in, contacts, control=control)
         if self.static_substep:
             iters, ls_iters = self.static_substep_iterations, self.static_substep_line_search_iterations
         else:
             iters, ls_iters = self.max_iterations, self.line_search_max_iterations
         v0 = self.contact_jacobian._qd
+        mark("warm_start")
         gamma0 = None
         if self.warm_start == "previous_impulses":
             gamma0 = self._gamma_cand[0]
@@ -761,6 +801,7 @@ class SolverSAP:
                 v_star=self.contact_jacobian.v_star, v0=self.contact_jacobian.v_star,
                 dt=self.contact_jacobian.dt_world)
             gamma0 = self._gamma_cand
+        mark("contact_solve")
         sr = self.contact_solve.solve(
             cr, state_in, control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
             v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, gamma0=gamma0,
@@ -769,6 +810,7 @@ class SolverSAP:
             cost_abs_tol=self.cost_abs_tol, cost_rel_tol=self.cost_rel_tol, line_search_max_iterations=ls_iters,
             armijo_c=self.armijo_c, rho=self.rho, line_search_relative_slop=self.line_search_relative_slop,
             line_search_variant=self.line_search_variant)
+        mark("integrate")
         # position integration (sim/solver_sap.py:1267-1386)
         mode = _abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint" else _abi.SAPB_INTEGRATE_SAP_EULER
         q_in = self.contact_jacobian._q
@@ -784,6 +826,7 @@ class SolverSAP:
         state_out.joint_qd.copy_(sr.v_flat)
         if state_out.body_f is not None and state_in.body_f is not None and state_out.body_f is not state_in.body_f:
             state_out.body_f.copy_(state_in.body_f)
+        mark(None)
         self._v_guess_active.fill_(1)  # warm start from this step's solution (sim/solver_sap.py:1441-1451)
         if self.warm_start != "previous_velocity":
             self._gamma_prev.copy_(sr.contact_gamma)

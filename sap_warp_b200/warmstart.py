@@ -331,9 +331,10 @@ def solver_dataset(problems, device, line_search_variant: str = "armijo_decay"):
 
 
 def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every: int = 1,
-                    hessian_precision: str = "fp64"):
+                    hessian_precision: str = "fp64", contact_preset_variant: str = "drake"):
     """(raw inputs (N, 12), targets u = w_eff * y (N, 3)) of the live
-    contacts along SolverSAP trajectories (reference warm start, FP64): at
+    contacts along SolverSAP trajectories (reference warm start, FP64, the
+    given contact preset): at
     step k the inputs carry gamma_prev = the impulses of step k-1 in the same
     slot (slot order is canonical, so a persistent contact keeps its slot),
     the targets are the unprojected impulses y at step k's converged
@@ -345,7 +346,8 @@ def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every:
     raws, us = [], []
     for seed in seeds:
         model, state, control, con, _ = models.rollout_scene(kind, worlds, seed, device)
-        solver = SolverSAP(model, max_rigid_contact=32, hessian_precision=hessian_precision)
+        solver = SolverSAP(model, max_rigid_contact=32, hessian_precision=hessian_precision,
+                           contact_preset_variant=contact_preset_variant)
         other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(),
                          body_q=state.body_q.clone(), body_f=state.body_f.clone())
         W, n, C = solver.view.W, solver.view.n, solver.max_rigid_contact
