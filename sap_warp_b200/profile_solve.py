@@ -1,11 +1,16 @@
-"""Run the batched contact solve on a fixed workload for profiling.
+"""Run a fixed workload of the contact step for profiling.
 
-    python -m sap_warp_b200.profile_solve --worlds 4096 --precision fp64 --launches 5
+    python -m sap_warp_b200.profile_solve --mode snapshot --worlds 4096 --precision fp64 --launches 5
+    python -m sap_warp_b200.profile_solve --mode rollout --worlds 4096 --steps 8 --warm-start learned \\
+        --precision fp32
 
-Builds the bench's humanoid workload, issues warm-up launches, then times
-`--launches` launches with CUDA events and prints the mean.  Used as the
-target command of ncu captures (select the solve kernel with
-`-k regex:contact_solve` and skip the warm-up launches with `-s`).
+snapshot: the stage-2 solve alone on the batched humanoid problem (A, J
+given): warm-up launches, then `--launches` timed launches.
+rollout: SolverSAP steps (drake preset) of the humanoid rollout scene with
+the given warm start and Hessian precision: `--steps` steps, the last half
+timed.  Each prints the mean time per launch / step.  Used as the target
+command of ncu captures (select a kernel with `-k regex:...` and skip the
+warm-up launches with `-s`).
 """
 
 from __future__ import annotations
@@ -14,20 +19,11 @@ import argparse
 
 import torch
 
-from . import scenes
+from . import models, scenes
 from ._solve import ContactSolveBuffers, contact_solve, make_options, problem_to_device
 
 
-def main() -> None:
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--worlds", type=int, default=4096)
-    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
-    ap.add_argument("--variant", default="armijo_decay")
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--launches", type=int, default=5)
-    ap.add_argument("--seed", type=int, default=2)
-    args = ap.parse_args()
-    dev = torch.device("cuda:0")
+def snapshot(args, dev) -> None:
     prob = scenes.humanoid_contact_problem(args.worlds, seed=args.seed)
     t = problem_to_device(prob, dev)
     buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, dev)
@@ -43,6 +39,46 @@ def main() -> None:
     torch.cuda.synchronize()
     print(f"{args.precision} {args.worlds} worlds: {e0.elapsed_time(e1) / max(args.launches, 1):.4f} ms/launch, "
           f"mean Newton iterations {buf.newton_iterations.double().mean().item():.3f}")
+
+
+def rollout(args, dev) -> None:
+    from .runtime import SapState
+    from .solver import SolverSAP
+
+    model, state, control, contacts, _ = models.rollout_scene("humanoid", args.worlds, args.seed, dev)
+    solver = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", hessian_precision=args.precision,
+                       warm_start=args.warm_start)
+    other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone())
+    half = max(args.steps // 2, 1)
+    for _ in range(args.steps - half):
+        solver.step(state, other, control, contacts, 2.0e-3)
+        state, other = other, state
+    torch.cuda.synchronize()
+    solver.stage_events = []
+    for _ in range(half):
+        solver.step(state, other, control, contacts, 2.0e-3)
+        state, other = other, state
+    stages = {k: round(v / half, 4) for k, v in solver.stage_times().items()}
+    print(f"rollout {args.worlds} worlds, {args.warm_start}, {args.precision}: stages ms/step {stages}, "
+          f"mean Newton iterations {solver.contact_solve.newton_iterations_env.double().mean().item():.3f}")
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", choices=["snapshot", "rollout"], default="snapshot")
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--variant", default="armijo_decay")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--launches", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warm-start", default="learned",
+                    choices=["previous_velocity", "previous_impulses", "learned"])
+    ap.add_argument("--seed", type=int, default=2)
+    args = ap.parse_args()
+    dev = torch.device("cuda:0")
+    (snapshot if args.mode == "snapshot" else rollout)(args, dev)
 
 
 if __name__ == "__main__":
