@@ -284,6 +284,34 @@ __device__ void evaluate(const World<NT, HT, NS>& w, const SolveParams& P, doubl
   out4[3] = r[3];
 }
 
+// H (lower triangle, HT) <- the lower triangle of the FP64 n x n matrix M in
+// global memory (+ diag_add on the diagonal): flat coalesced reads, four
+// loads in flight per thread.
+template <int NT, typename HT, int NS>
+__device__ __forceinline__ void load_lower(const World<NT, HT, NS>& w, const double* M, const double* diag_add,
+                                           double shift) {
+  const int tid = threadIdx.x;
+  const int n = w.dofs(), ldH = w.ldH();
+  const int total = n * n;
+  for (int k0 = tid; k0 < total; k0 += 4 * NT) {
+    double val[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = k0 + u * NT;
+      val[u] = k < total ? __ldg(M + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = k0 + u * NT;
+      if (k < total) {
+        const int i = k / n, j = k - i * n;
+        if (j < i) w.H[(size_t)i * ldH + j] = HT(val[u]);
+        else if (j == i) w.H[(size_t)i * ldH + j] = HT(val[u] + (diag_add ? diag_add[i] : 0.0) + shift);
+      }
+    }
+  }
+}
+
 // H = A + J^T G J + diag(PD + limit + shift), lower triangle, in HT.
 // G (at the stored vc) and G J are formed chunk by chunk; each thread owns one
 // 4x4 tile of H and one of KS slices of a chunk's rows, accumulates in
@@ -303,13 +331,7 @@ __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) 
     for (int k = 0; k < 9; ++k) w.G[9 * c + k] = G[k];
   }
   // H lower = A lower + diagonal terms
-  for (int i = warp; i < n; i += NW) {
-    for (int j = lane; j <= i; j += 32) {
-      double a = __ldg(w.A + (size_t)i * n + j);
-      if (i == j) a += w.V(V_HDIAG)[i] + diag_shift;
-      w.H[(size_t)i * ldH + j] = HT(a);
-    }
-  }
+  load_lower<NT, HT, NS>(w, w.A, w.V(V_HDIAG), diag_shift);
   const int tiles = nb * (nb + 1) / 2;
   int ks = NT / (tiles > 0 ? tiles : 1);
   if (ks < 1) ks = 1;
@@ -381,11 +403,12 @@ __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) 
 }
 
 // In-place LDL^T of the lower triangle of H (unit L stored below the
-// diagonal unscaled as H_ik, D on the diagonal) by one warp, then the solve
-// H dv = -grad.  Mathematically the Cholesky solve of the reference's
-// BlockCholeskySolverBatched (sim/blocked_cholesky.py:414-604).  A pivot that
-// is not positive/finite makes dv NaN, so the line search reports an ascent
-// direction as the reference's NaN factor does.
+// diagonal unscaled as H_ik, D on the diagonal, 1/d_k in V_DINV) by one warp,
+// column by column over the column-descending triangle list (the trailing
+// triangle of step k is its first m(m+1)/2 entries, m = n-k-1), with only
+// warp-level synchronisation; then the solve H dv = -grad.  Mathematically
+// the Cholesky solve of the reference's BlockCholeskySolverBatched
+// (sim/blocked_cholesky.py:414-604).
 template <int NT, typename HT, int NS>
 __device__ void solve_factored(const World<NT, HT, NS>& w);
 
@@ -394,65 +417,21 @@ __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   const int tid = threadIdx.x;
   const int n = w.dofs(), ldH = w.ldH();
   HT* H = w.H;
-  HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));  // 1/d_k, written one step ahead
-  double* dv = w.V(V_DV);
-  // Blocked right-looking LDL^T, 8-column blocks, three barriers per block.
-  // Storage: below the diagonal H[i][k] = L_ik d_k (L unit lower), D on the
-  // diagonal, dinv[k] = 1/d_k -- the layout the triangular solves read.
-  constexpr int B = 8;
-  const int lane = tid & 31;
-  for (int K = 0; K < n; K += B) {
-    const int bs = min(B, n - K);
-    // (1) diagonal block, unblocked, by warp 0
-    if (tid < 32) {
-      for (int s = 0; s < bs; ++s) {
-        const int ks = K + s;
-        const HT rinv = fast_recip(H[(size_t)ks * ldH + ks]);
-        if (lane == 0) dinv[ks] = rinv;
-        const int m = bs - s - 1;  // trailing entries (a, c), s < c <= a < bs
-        for (int q = lane; q < m * (m + 1) / 2; q += 32) {
-          int a = 0;
-          while ((a + 1) * (a + 2) / 2 <= q) ++a;
-          const int c = q - a * (a + 1) / 2;
-          const int i = ks + 1 + a, j = ks + 1 + c;
-          H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + ks] * rinv) * H[(size_t)j * ldH + ks];
-        }
-        __syncwarp();
+  HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
+  if (tid < 32) {
+    const int lane = tid;
+    for (int k = 0; k < n; ++k) {
+      const HT rinv = fast_recip(H[(size_t)k * ldH + k]);
+      if (lane == 0) dinv[k] = rinv;
+      const int m = n - k - 1;
+      const int cnt = m * (m + 1) / 2;
+      for (int e = lane; e < cnt; e += 32) {
+        const int ij = w.tri[e];
+        const int i = ij >> 8, j = ij & 255;
+        H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + k] * rinv) * H[(size_t)j * ldH + k];
       }
+      __syncwarp();
     }
-    __syncthreads();
-    const int rest = n - K - bs;
-    if (rest <= 0) break;
-    // (2) panel rows: P L_K^T = H_panel (forward substitution over the block columns)
-    for (int t = tid; t < rest; t += NT) {
-      const int i = K + bs + t;
-      HT p[B];
-#pragma unroll
-      for (int c = 0; c < B; ++c) {
-        if (c < bs) {
-          HT h = H[(size_t)i * ldH + K + c];
-#pragma unroll
-          for (int m2 = 0; m2 < B; ++m2)
-            if (m2 < c) h -= p[m2] * (H[(size_t)(K + c) * ldH + K + m2] * dinv[K + m2]);
-          p[c] = h;
-          H[(size_t)i * ldH + K + c] = h;
-        }
-      }
-    }
-    __syncthreads();
-    // (3) trailing update of entries (i, j), j >= K + bs: the first
-    // rest*(rest+1)/2 entries of the column-descending triangle list.
-    const int cnt = rest * (rest + 1) / 2;
-    for (int e = tid; e < cnt; e += NT) {
-      const int ij = w.tri[e];
-      const int i = ij >> 8, j = ij & 255;
-      HT acc = H[(size_t)i * ldH + j];
-#pragma unroll
-      for (int c = 0; c < B; ++c)
-        if (c < bs) acc -= H[(size_t)i * ldH + K + c] * dinv[K + c] * H[(size_t)j * ldH + K + c];
-      H[(size_t)i * ldH + j] = acc;
-    }
-    __syncthreads();
   }
   solve_factored<NT, HT, NS>(w);
 }
@@ -573,6 +552,71 @@ __device__ void line_terms(const World<NT, HT, NS>& w, const SolveParams& P, dou
   out3[2] = r[2];
 }
 
+// The regularizer terms of line_terms at four step sizes at once: warp q
+// evaluates alpha[q] (block of 128 threads), lanes over the contacts and
+// DOFs, warp-shuffle sums, one barrier to publish.  reg[q] for every q and
+// the impulse projection onto dv at alpha[0].
+template <int NT, typename HT, int NS>
+__device__ void line_terms4(const World<NT, HT, NS>& w, const SolveParams& P, double dt, const double (&alpha)[4],
+                            double (&reg)[4], double* proj0) {
+  static_assert(NT == 128, "one warp per trial step");
+  const int tid = threadIdx.x, lane = tid & 31, q = tid >> 5;
+  const double a = alpha[q];
+  double rs = 0.0, ps = 0.0;
+  for (int c = lane; c < w.count; c += 32) {
+    const ContactConst cc = w.cc(c);
+    const double dx = w.Cn(C_DVC + 0)[c], dy = w.Cn(C_DVC + 1)[c], dz = w.Cn(C_DVC + 2)[c];
+    double g[3], cost;
+    project_contact(cc, w.Cn(C_VC + 0)[c] + a * dx, w.Cn(C_VC + 1)[c] + a * dy, w.Cn(C_VC + 2)[c] + a * dz, g,
+                    &cost, nullptr);
+    rs += cost;
+    ps += g[0] * dx + g[1] * dy + g[2] * dz;
+  }
+  if (P.dof.has_pd || P.dof.has_limits) {
+    for (int i = lane; i < w.dofs(); i += 32) {
+      const double vi = w.V(V_V)[i] + a * w.V(V_DV)[i];
+      const double dvi = w.V(V_DV)[i];
+      const int fl = w.flags[i];
+      if (P.dof.has_pd && (fl & kFlagPd)) {
+        const double gain = w.V(V_PDGAIN)[i], lim = w.V(V_PDLIM)[i];
+        const double y = w.V(V_PDA)[i] - gain * vi;
+        ps += dvi * dt * clamp_limit(y, lim);
+        if (gain > 0.0) rs += (dt / gain) * clamp_limit_antiderivative(y, lim);
+      }
+      if (P.dof.has_limits) {
+        if (fl & kFlagLo) {
+          const double g = w.V(V_LORINV)[i] * (w.V(V_LOVHAT)[i] - vi);
+          if (g > 0.0) {
+            ps += dvi * g;
+            rs += 0.5 * w.V(V_LOR)[i] * g * g;
+          }
+        }
+        if (fl & kFlagUp) {
+          const double g = w.V(V_UPRINV)[i] * (w.V(V_UPVHAT)[i] + vi);
+          if (g > 0.0) {
+            ps -= dvi * g;
+            rs += 0.5 * w.V(V_UPR)[i] * g * g;
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    rs += __shfl_xor_sync(0xffffffffu, rs, o);
+    ps += __shfl_xor_sync(0xffffffffu, ps, o);
+  }
+  __syncthreads();  // earlier readers of red are done
+  if (lane == 0) {
+    w.red[q] = rs;
+    w.red[4 + q] = ps;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) reg[k] = w.red[k];
+  *proj0 = w.red[4];
+}
+
 struct LsResult {
   int accepted, status, iterations;
   double alpha, accepted_cost;
@@ -629,10 +673,15 @@ __device__ LsResult ls_armijo(const World<NT, HT, NS>& w, const SolveParams& P, 
     r.status = SAPB_LS_ASCENT_DIRECTION;
     return r;
   }
-  double t3[3];
-  line_terms<NT, HT, NS>(w, P, dt, alpha, false, t3);
-  double ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + t3[0];
-  const double deriv = dell_a0 + alpha * d2ell_a - t3[1];
+  // Trial steps amax * rho^k, evaluated four at a time (the same products as
+  // the sequential backtracking, so the same decisions).
+  double al[4], rg[4], p0;
+  al[0] = alpha;
+  for (int q = 1; q < 4; ++q) al[q] = al[q - 1] * o.rho;
+  line_terms4<NT, HT, NS>(w, P, dt, al, rg, &p0);
+  int base = 0;
+  double ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + rg[0];
+  const double deriv = dell_a0 + alpha * d2ell_a - p0;
   {
     const double scale = fmax(1.0, 0.5 * (fabs(ell) + fabs(cost)));
     const double slop = (slop_rel / 10.0) * scale;
@@ -648,8 +697,13 @@ __device__ LsResult ls_armijo(const World<NT, HT, NS>& w, const SolveParams& P, 
   if (o.line_search_max_iterations <= 1) return r;
   for (int iteration = 1;; ++iteration) {
     alpha = alpha * o.rho;
-    line_terms<NT, HT, NS>(w, P, dt, alpha, false, t3);
-    ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + t3[0];
+    if (iteration - base >= 4) {
+      base = iteration;
+      al[0] = alpha;
+      for (int q = 1; q < 4; ++q) al[q] = al[q - 1] * o.rho;
+      line_terms4<NT, HT, NS>(w, P, dt, al, rg, &p0);
+    }
+    ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + rg[iteration - base];
     const double a = alpha, a_prev = alpha_prev, e_prev = ell_prev;
     const double denom = a - a_prev;
     double dell_approx = 0.0;
@@ -693,10 +747,16 @@ __device__ LsResult ls_monotone(const World<NT, HT, NS>& w, const SolveParams& P
   line_coefficients<NT, HT, NS>(w, c4);
   const double base_linear = c4[1], base_quadratic = c4[2], base0 = c4[3];
   double alpha = 1.0, trial = cost;
+  double al[4], rg[4], p0;
+  int base = -4;
   for (int it = 0; it < o.line_search_max_iterations; ++it) {
-    double t3[3];
-    line_terms<NT, HT, NS>(w, P, dt, alpha, false, t3);
-    trial = base0 + alpha * base_linear + 0.5 * alpha * alpha * base_quadratic + t3[0];
+    if (it - base >= 4) {  // halvings evaluated four at a time
+      base = it;
+      al[0] = alpha;
+      for (int q = 1; q < 4; ++q) al[q] = al[q - 1] * 0.5;
+      line_terms4<NT, HT, NS>(w, P, dt, al, rg, &p0);
+    }
+    trial = base0 + alpha * base_linear + 0.5 * alpha * alpha * base_quadratic + rg[it - base];
     r.iterations += 1;
     const double tol = 1.0e-14 + 1.0e-12 * fabs(cost);
     if (trial <= cost + tol) {
@@ -872,6 +932,20 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
           asm volatile("prefetch.global.L2 [%0];" ::"l"(a0 + off));
         for (size_t off = (size_t)tid * 128; off < jbytes; off += (size_t)NT * 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(j0 + off));
+        if (P.p.gamma0) {
+          if (P.p.dynamics_factor) {
+            const char* f0 = reinterpret_cast<const char*>(P.p.dynamics_factor + (size_t)nx * n * n);
+            for (size_t off = (size_t)tid * 128; off < abytes; off += (size_t)NT * 128)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(f0 + off));
+          }
+          const int K = P.p.gamma0_count > 1 ? P.p.gamma0_count : 1;
+          const size_t gbytes = sizeof(double) * (size_t)cnt * 3;
+          for (int k = 0; k < K; ++k) {
+            const char* g0 = reinterpret_cast<const char*>(P.p.gamma0 + ((size_t)k * P.p.num_envs + nx) * C * 3);
+            for (size_t off = (size_t)tid * 128; off < gbytes; off += (size_t)NT * 128)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(g0 + off));
+          }
+        }
       }
     }
 
@@ -1073,21 +1147,17 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         double e4p[4];
         evaluate<NT, HT, NS>(w, P, dt, e4p);
         double best_cost = e4p[0];
-        const int ldj = w.ldJ(), ldh = w.ldH();
+        const int ldj = w.ldJ();
         for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
         if (P.p.dynamics_factor) {
           // the free motion's LDL^T of A
           const double* Lg = P.p.dynamics_factor + (size_t)e * n * n;
-          const int lane = tid & 31, warp = tid >> 5;
-          for (int i = warp; i < n; i += NT / 32)
-            for (int j = lane; j <= i; j += 32) w.H[(size_t)i * ldh + j] = HT(__ldg(Lg + (size_t)i * n + j));
+          load_lower<NT, HT, NS>(w, Lg, nullptr, 0.0);
           HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
           for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
           __syncthreads();
         } else {
-          const int lane = tid & 31, warp = tid >> 5;
-          for (int i = warp; i < n; i += NT / 32)
-            for (int j = lane; j <= i; j += 32) w.H[(size_t)i * ldh + j] = HT(__ldg(w.A + (size_t)i * n + j));
+          load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
           for (int i = tid; i < n; i += NT) w.V(V_GRAD)[i] = 0.0;
           __syncthreads();
           factor_and_solve<NT, HT, NS>(w);  // the factor of A (the solve of a zero rhs is unused)
