@@ -266,6 +266,7 @@ typedef struct sapb_prepare_outputs {
   double* body_q;                   /* [B][7] start-of-step body poses, or NULL */
   double* dynamics_factor;          /* [W][n][n] LDL^T of A (below the diagonal L_ik d_k, on it d_k;
                                        above it unspecified), or NULL */
+  double* vc_star;                  /* [W][C][3] free-motion contact velocities J_c v*, or NULL */
 } sapb_prepare_outputs;
 
 /* Device workspace bytes of sapb_free_motion_contacts. */
@@ -402,10 +403,12 @@ int32_t sapb_mlp_adam(float* params, const float* grad, float* m, float* v, cons
 int32_t sapb_mlp_error(void* stream);
 /* Per-slot network inputs of a stage-2 problem: normalised BF16 rows
  * features [E*C,16] and/or raw FP32 rows raw [E*C,12]; dead slots are zero.
- * normal_up [E,C] (NULL: 1), gamma_prev [E,C,3] (NULL: 0). */
+ * normal_up [E,C] (NULL: 1), gamma_prev [E,C,3] (NULL: 0), vc_star [E,C,3]
+ * the free-motion contact velocities J_c v* (NULL: formed from J and v*). */
 int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const double* normal_up,
-                                const double* gamma_prev, const sapb_warmstart_norm* norm, double tau_fallback,
-                                uint16_t* features, float* raw, void* stream);
+                                const double* gamma_prev, const double* vc_star,
+                                const sapb_warmstart_norm* norm, double tau_fallback, uint16_t* features,
+                                float* raw, void* stream);
 /* gamma0 [E,C,3] from the network output mlp_out [E*C,3] and the previous
  * step's impulses gamma_prev [E,C,3] (NULL: 0); opts supplies the
  * regularization (contact_beta, contact_sigma, contact_tau_d fallback). */

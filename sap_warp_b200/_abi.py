@@ -222,6 +222,7 @@ class PrepareOutputs(C.Structure):
         ("truncated_count", _p),
         ("body_q", _p),
         ("dynamics_factor", _p),
+        ("vc_star", _p),
     ]
 
 
@@ -285,7 +286,7 @@ EXPORTS = {
     "sapb_mlp_adam": (C.c_int32, [_p, _p, _p, _p, C.POINTER(AdamOptions), C.c_int32, _p, _p, _p]),
     "sapb_mlp_error": (C.c_int32, [_p]),
     "sapb_warmstart_features": (
-        C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), C.c_double, _p, _p, _p]
+        C.c_int32, [C.POINTER(ContactProblem), _p, _p, _p, C.POINTER(WarmstartNorm), C.c_double, _p, _p, _p]
     ),
     "sapb_warmstart_impulses": (
         C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), C.POINTER(SolveOptions), _p, _p]

@@ -560,6 +560,7 @@ struct FeatParams {
   sapb_contact_problem p;
   const double* normal_up;
   const double* gamma_prev;
+  const double* vc_star;
   sapb_warmstart_norm norm;
   double tau_fallback;
   uint16_t* x;
@@ -580,20 +581,26 @@ __global__ void features_kernel(const FeatParams P) {
     for (int k = 0; k < kInUsed; ++k) f[k] = 0.f;
     const bool live = c < count;
     if (live) {
-      const double* J = P.p.jacobian + (size_t)s * 3 * n;
-      const double* vs = P.p.v_star + (size_t)e * n;
       double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-      for (int i = lane; i < n; i += 32) {
-        const double v = vs[i];
-        a0 += J[i] * v;
-        a1 += J[n + i] * v;
-        a2 += J[2 * n + i] * v;
-      }
+      if (P.vc_star) {
+        a0 = P.vc_star[3 * s];
+        a1 = P.vc_star[3 * s + 1];
+        a2 = P.vc_star[3 * s + 2];
+      } else {
+        const double* J = P.p.jacobian + (size_t)s * 3 * n;
+        const double* vs = P.p.v_star + (size_t)e * n;
+        for (int i = lane; i < n; i += 32) {
+          const double v = vs[i];
+          a0 += J[i] * v;
+          a1 += J[n + i] * v;
+          a2 += J[2 * n + i] * v;
+        }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        for (int o = 16; o > 0; o >>= 1) {
+          a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+          a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+          a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
       }
       const double w = fmax(P.p.w_eff[s], 1.0e-12);
       f[0] = (float)P.p.phi0[s];
@@ -833,8 +840,9 @@ int32_t sapb_mlp_error(void* stream) {
 }
 
 int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const double* normal_up,
-                                const double* gamma_prev, const sapb_warmstart_norm* norm, double tau_fallback,
-                                uint16_t* features, float* raw, void* stream) {
+                                const double* gamma_prev, const double* vc_star,
+                                const sapb_warmstart_norm* norm, double tau_fallback, uint16_t* features,
+                                float* raw, void* stream) {
   if (!problem || (!features && !raw) || (features && !norm) || problem->num_envs < 0 || problem->dof_per_env < 1 ||
       problem->max_contacts < 0) {
     set_last_error("sapb_warmstart_features: invalid argument");
@@ -856,6 +864,7 @@ int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const doubl
   P.p = *problem;
   P.normal_up = normal_up;
   P.gamma_prev = gamma_prev;
+  P.vc_star = vc_star;
   if (norm) P.norm = *norm;
   P.tau_fallback = tau_fallback;
   P.x = features;

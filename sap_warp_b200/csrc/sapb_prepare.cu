@@ -644,6 +644,16 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     for (int r = 0; r < 3; ++r) Jout[((size_t)c * 3 + r) * n + col] = dot(load3(cs + 12 + 3 * r), rel);
   }
   __syncthreads();
+  if (P.out.vc_star) {
+    // free-motion contact velocities J_c v*, v* = qd + dt vdot
+    const double h = P.in.dt[e];
+    for (int k = tid; k < 3 * cc; k += kPrepNT) {
+      const double* row = Jout + (size_t)k * n;
+      double acc = 0.0;
+      for (int col = 0; col < n; ++col) acc += row[col] * (P.in.joint_qd[d0 + col] + h * vdot[col]);
+      P.out.vc_star[(size_t)e * C * 3 + k] = acc;
+    }
+  }
   // ---- contact weights (sim/contact_jacobian.py:153-251) --------------------
   for (int c = tid; c < cc; c += kPrepNT) {
     const size_t ci = (size_t)e * C + c;

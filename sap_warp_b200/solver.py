@@ -314,11 +314,14 @@ class SapContactJacobian:
         self.outputs = o
 
     def keep_dynamics_factor(self) -> None:
-        """Also write the free-motion LDL^T of A (for candidate starts)."""
+        """Also write the free-motion LDL^T of A and the free-motion contact
+        velocities J_c v* (for candidate starts and the warm-start network)."""
         if self.dynamics_factor_env is None:
             v = self.view
             self.dynamics_factor_env = torch.zeros(v.W, v.n, v.n, dtype=F64, device=v.device)
             self.outputs.dynamics_factor = _ptr(self.dynamics_factor_env)
+            self.contact_env_vc_star = torch.zeros(v.W, self.max_rigid_contact, 3, dtype=F64, device=v.device)
+            self.outputs.vc_star = _ptr(self.contact_env_vc_star)
 
     def set_dt(self, dt) -> None:
         """Per-world time step (scalar or [W] tensor), sim/solver_sap.py:975-992."""
@@ -795,6 +798,7 @@ class SolverSAP:
             self.learned_warm_start.predict(
                 num_envs=self.view.W, dof_per_env=self.view.n, max_contacts=self.max_rigid_contact,
                 normal_up=self._normal_up, gamma_prev=self._gamma_prev, out=self._gamma_cand[1],
+                vc_star=self.contact_jacobian.contact_env_vc_star,
                 contact_count=cr.contact_env_count, dynamics_matrix=cr.dynamics_matrix_env,
                 jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff,
                 mu=cr.contact_env_mu, stiffness=cr.contact_env_stiffness, tau_d=cr.contact_env_tau_d,

@@ -242,7 +242,8 @@ class LearnedWarmStart:
         return self._bufs[key]
 
     def predict(self, *, num_envs: int, dof_per_env: int, max_contacts: int, normal_up: torch.Tensor | None = None,
-                gamma_prev: torch.Tensor | None = None, out: torch.Tensor | None = None, **arrays) -> torch.Tensor:
+                gamma_prev: torch.Tensor | None = None, vc_star: torch.Tensor | None = None,
+                out: torch.Tensor | None = None, **arrays) -> torch.Tensor:
         """gamma0 (E, C, 3) FP64 on the device (into `out` if given):
         features -> MLP -> impulses, three launches on the current stream, no
         host sync, no allocation after the first call for a shape."""
@@ -253,8 +254,9 @@ class LearnedWarmStart:
         lib, s = load(), _stream(self.device)
         nu = 0 if normal_up is None else _dev_ptr(normal_up, F64, E * C, "normal_up")
         gp = 0 if gamma_prev is None else _dev_ptr(gamma_prev, F64, E * C * 3, "gamma_prev")
-        check(lib.sapb_warmstart_features(ctypes.byref(P), nu, gp, ctypes.byref(self.norm_struct), self.tau_fallback,
-                                          b["x"].data_ptr(), None, s), "sapb_warmstart_features")
+        vc = 0 if vc_star is None else _dev_ptr(vc_star, F64, E * C * 3, "vc_star")
+        check(lib.sapb_warmstart_features(ctypes.byref(P), nu, gp, vc, ctypes.byref(self.norm_struct),
+                                          self.tau_fallback, b["x"].data_ptr(), None, s), "sapb_warmstart_features")
         self.mlp.forward(b["x"], b["y"])
         check(lib.sapb_warmstart_impulses(ctypes.byref(P), b["y"].data_ptr(), gp, ctypes.byref(self.norm_struct),
                                           ctypes.byref(self.solve_options), _dev_ptr(g_out, F64, E * C * 3, "out"), s),
@@ -284,7 +286,7 @@ def raw_features(arrays: dict, num_envs: int, dof_per_env: int, max_contacts: in
     P = build_problem(num_envs=E, dof_per_env=dof_per_env, max_contacts=C, **arrays)
     nu = 0 if normal_up is None else _dev_ptr(normal_up, F64, E * C, "normal_up")
     gp = 0 if gamma_prev is None else _dev_ptr(gamma_prev, F64, E * C * 3, "gamma_prev")
-    check(load().sapb_warmstart_features(ctypes.byref(P), nu, gp, None, tau_fallback, None, raw.data_ptr(),
+    check(load().sapb_warmstart_features(ctypes.byref(P), nu, gp, None, None, tau_fallback, None, raw.data_ptr(),
                                          _stream(dev)), "sapb_warmstart_features")
     return raw
 

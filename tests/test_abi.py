@@ -56,7 +56,8 @@ def test_no_compute_entry_points_without_gpu(lib):
     assert lib.sapb_mlp_train_buffer_sizes(300, ctypes.byref(a), ctypes.byref(p)) == _abi.SAPB_OK
     assert a.value == p.value == 3 * 3 * 128 * 128
     assert lib.sapb_mlp_forward(None, None, None, 4, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
-    assert lib.sapb_warmstart_features(None, None, None, None, 0.0, None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert lib.sapb_warmstart_features(None, None, None, None, None, 0.0, None, None, None) == \
+        _abi.SAPB_ERR_INVALID_ARGUMENT
 
 
 def test_struct_layout_matches_header(tmp_path):

@@ -89,6 +89,31 @@ def test_free_motion_and_contact_rows(cuda_device, kind, weight_mode, point_mode
         np.testing.assert_allclose(got["jac"][e, a], ref["jac"][e, b], rtol=1e-9, atol=1e-11)
 
 
+def test_factor_and_free_motion_contact_velocities(cuda_device):
+    """The optional outputs for candidate starts: the LDL^T factor of A
+    (L D L^T reconstructs A) and vc* = J_c v* per live slot."""
+    case = build("humanoid", 16, seed=12)
+    model, state, control = gpu_state(case, cuda_device)
+    cj = SapContactJacobian(model, max_rigid_contact=case["max_contacts"])
+    cj.keep_dynamics_factor()
+    res = cj.compute(state, models.contacts_to_torch(case["con"], cuda_device), control=control, dt=2e-3)
+    torch.cuda.synchronize()
+    A = res.dynamics_matrix_env.cpu().numpy()
+    F = res.dynamics_factor_env.cpu().numpy()
+    n = A.shape[1]
+    for e in range(A.shape[0]):
+        d = np.diag(F[e]).copy()
+        L = np.tril(F[e], -1) / d[None, :] + np.eye(n)
+        np.testing.assert_allclose(L @ np.diag(d) @ L.T, A[e], rtol=1e-10, atol=1e-10 * np.abs(A[e]).max())
+    J = res.contact_env_jacobian.cpu().numpy()
+    vs = cj.v_star.cpu().numpy().reshape(-1, n)
+    vc = cj.contact_env_vc_star.cpu().numpy()
+    cnt = np.minimum(res.contact_env_count.cpu().numpy(), case["max_contacts"])
+    want = np.einsum("ecrj,ej->ecr", J, vs)
+    for e in range(len(cnt)):
+        np.testing.assert_allclose(vc[e, :cnt[e]], want[e, :cnt[e]], rtol=1e-12, atol=1e-12)
+
+
 def test_truncation_counts(cuda_device):
     case = build("quadruped", 8, seed=5, per_world=(20, 40), max_contacts=16)
     model, state, control = gpu_state(case, cuda_device)
