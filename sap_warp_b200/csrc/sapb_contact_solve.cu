@@ -22,6 +22,7 @@
 
 #include "sapb_device.cuh"
 #include "sapb_internal.h"
+#include "sapb_ldlt.cuh"
 
 namespace sapb {
 
@@ -404,84 +405,15 @@ __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) 
 // diagonal unscaled as H_ik (= L_ik d_k), D on the diagonal, 1/d_k in V_DINV.
 // Then the solve H dv = -grad (solve_factored).  Mathematically the Cholesky
 // solve of the reference's BlockCholeskySolverBatched
-// (sim/blocked_cholesky.py:414-604).  Schedule: right-looking with 8-column
-// blocks, the diagonal block by one warp, panel and trailing update by the
-// whole block, three barriers per block.  (A single-warp column-by-column
-// schedule measured no faster in FP32 and slower in FP64 on the 35-DOF
-// humanoid.)
+// (sim/blocked_cholesky.py:414-604), with the blocked schedule of
+// ldlt_blocked (a single-warp column-by-column schedule measured no faster
+// in FP32 and slower in FP64 on the 35-DOF humanoid).
 template <int NT, typename HT, int NS>
 __device__ void solve_factored(const World<NT, HT, NS>& w);
 
 template <int NT, typename HT, int NS>
-__device__ void factor_blocked(const World<NT, HT, NS>& w) {
-  const int tid = threadIdx.x;
-  const int n = w.dofs(), ldH = w.ldH();
-  HT* H = w.H;
-  HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));  // 1/d_k, written one step ahead
-  // Blocked right-looking LDL^T, 8-column blocks, three barriers per block.
-  // Storage: below the diagonal H[i][k] = L_ik d_k (L unit lower), D on the
-  // diagonal, dinv[k] = 1/d_k -- the layout the triangular solves read.
-  constexpr int B = 8;
-  const int lane = tid & 31;
-  for (int K = 0; K < n; K += B) {
-    const int bs = min(B, n - K);
-    // (1) diagonal block, unblocked, by warp 0
-    if (tid < 32) {
-      for (int s = 0; s < bs; ++s) {
-        const int ks = K + s;
-        const HT rinv = fast_recip(H[(size_t)ks * ldH + ks]);
-        if (lane == 0) dinv[ks] = rinv;
-        const int m = bs - s - 1;  // trailing entries (a, c), s < c <= a < bs
-        for (int q = lane; q < m * (m + 1) / 2; q += 32) {
-          int a = 0;
-          while ((a + 1) * (a + 2) / 2 <= q) ++a;
-          const int c = q - a * (a + 1) / 2;
-          const int i = ks + 1 + a, j = ks + 1 + c;
-          H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + ks] * rinv) * H[(size_t)j * ldH + ks];
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    const int rest = n - K - bs;
-    if (rest <= 0) break;
-    // (2) panel rows: P L_K^T = H_panel (forward substitution over the block columns)
-    for (int t = tid; t < rest; t += NT) {
-      const int i = K + bs + t;
-      HT p[B];
-#pragma unroll
-      for (int c = 0; c < B; ++c) {
-        if (c < bs) {
-          HT h = H[(size_t)i * ldH + K + c];
-#pragma unroll
-          for (int m2 = 0; m2 < B; ++m2)
-            if (m2 < c) h -= p[m2] * (H[(size_t)(K + c) * ldH + K + m2] * dinv[K + m2]);
-          p[c] = h;
-          H[(size_t)i * ldH + K + c] = h;
-        }
-      }
-    }
-    __syncthreads();
-    // (3) trailing update of entries (i, j), j >= K + bs: the first
-    // rest*(rest+1)/2 entries of the column-descending triangle list.
-    const int cnt = rest * (rest + 1) / 2;
-    for (int e = tid; e < cnt; e += NT) {
-      const int ij = w.tri[e];
-      const int i = ij >> 8, j = ij & 255;
-      HT acc = H[(size_t)i * ldH + j];
-#pragma unroll
-      for (int c = 0; c < B; ++c)
-        if (c < bs) acc -= H[(size_t)i * ldH + K + c] * dinv[K + c] * H[(size_t)j * ldH + K + c];
-      H[(size_t)i * ldH + j] = acc;
-    }
-    __syncthreads();
-  }
-}
-
-
-template <int NT, typename HT, int NS>
 __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
-  factor_blocked<NT, HT, NS>(w);
+  ldlt_blocked<NT, HT>(w.H, w.dofs(), w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri);
   solve_factored<NT, HT, NS>(w);
 }
 
@@ -950,13 +882,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   const int n = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
   const Layout L = make_layout(n, C, (int)sizeof(HT));
   const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
-  {
-    uint16_t* tri = reinterpret_cast<uint16_t*>(smem + L.off_tri);
-    for (int j = n - 1 - tid; j >= 1; j -= NT) {
-      const int off = (n - 1 - j) * (n - j) / 2;
-      for (int i = j; i < n; ++i) tri[off + (i - j)] = (uint16_t)((i << 8) | j);
-    }
-  }
+  build_triangle_list<NT>(reinterpret_cast<uint16_t*>(smem + L.off_tri), n);
 
   if (tid == 0) s_next = atomicAdd(P.queue, 1);
   for (;;) {

@@ -18,6 +18,7 @@
 
 #include "sapb_device.cuh"
 #include "sapb_internal.h"
+#include "sapb_ldlt.cuh"
 #include "sapb_spatial.cuh"
 
 namespace sapb {
@@ -41,7 +42,7 @@ __host__ __device__ inline size_t prep_align(size_t x) { return (x + 15) / 16 * 
 // ([angular; linear]), so velocities, forces and inertias of different bodies
 // add without shifts.
 struct PrepLayout {
-  size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, dbody, total;
+  size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, dbody, tri, total;
 };
 
 __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C) {
@@ -72,6 +73,7 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C) {
   L.jmp = take(sizeof(int) * 2 * B);        // pointer-jumping parents (two buffers)
   L.bj = take(sizeof(int) * B);             // joint (global index) of each body, -1
   L.dbody = take(sizeof(int) * n);          // body of each DOF
+  L.tri = take(sizeof(uint16_t) * (size_t)(n * (n - 1) / 2 + 1));  // LDL^T triangle list
   L.total = o;
   return L;
 }
@@ -225,6 +227,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   int* jmpB = jmpA + B;
   int* bj = reinterpret_cast<int*>(smem + L.bj);
   int* dbody = reinterpret_cast<int*>(smem + L.dbody);
+  uint16_t* tri = reinterpret_cast<uint16_t*>(smem + L.tri);
   const int j0 = e * Jw, b0g = e * B, d0 = e * n;
   const double* q = P.in.joint_q;
   const double* qd = P.in.joint_qd;
@@ -232,6 +235,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   // ---- topology of this world --------------------------------------------
   for (int b = tid; b < B; b += kPrepNT) bj[b] = -1;
   for (int i = tid; i < n; i += kPrepNT) dbody[i] = -1;
+  build_triangle_list<kPrepNT>(tri, n);
   for (int k = tid; k < 6 * n; k += kPrepNT) S[k] = 0.0;
   __syncthreads();
   for (int jl = tid; jl < Jw; jl += kPrepNT) {
@@ -476,18 +480,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   __syncthreads();
 
   // ---- free-motion solve A vdot = tau: LDL^T (H_ik = L_ik d_k below the diagonal)
-  for (int k = 0; k < n; ++k) {
-    const double rinv = fast_recip(H[(size_t)k * n + k]);
-    const int m = n - k - 1;
-    for (int idx = tid; idx < m * m; idx += kPrepNT) {
-      const int a = idx / m, c = idx - a * m;
-      if (c > a) continue;
-      const int i = k + 1 + a, j = k + 1 + c;
-      H[(size_t)i * n + j] -= H[(size_t)i * n + k] * rinv * H[(size_t)j * n + k];
-    }
-    __syncthreads();
-  }
-  for (int k = tid; k < n; k += kPrepNT) dinv[k] = fast_recip(H[(size_t)k * n + k]);
+  ldlt_blocked<kPrepNT, double>(H, n, n, dinv, tri);
   if (P.out.dynamics_factor) {
     double* Lg = P.out.dynamics_factor + (size_t)e * n * n;
     for (int k = tid; k < n * n; k += kPrepNT) {
@@ -495,7 +488,6 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
       if (j <= i) Lg[k] = H[k];
     }
   }
-  __syncthreads();
   if (tid < 32) {
     // lanes own rows lane + 32 r (n <= 128): forward z = D^-1 L^-1 tau, then x = L^-T z
     double hb[4], sacc[4];
@@ -629,52 +621,76 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     conint[2 * c + 1] = (lb1 >= 0 && lb1 < B) ? lb1 : -1;
   }
   __syncthreads();
+  // ---- contact rows, free-motion contact velocities and diag_delassus
+  // weights, one warp per contact: lanes over the DOF columns, row / weight
+  // partial sums reduced by shuffles.
   double* Jout = P.out.jacobian + (size_t)e * C * 3 * n;
-  for (int k = tid; k < cc * n; k += kPrepNT) {
-    const int c = k / n, col = k - c * n;
-    const double* cs = con + 21 * (size_t)c;
-    V3 rel = v3(0, 0, 0);
-    const int bcol = dbody[col];
-    if (bcol >= 0) {
-      const Sv s = sv_load(S + 6 * col);
+  {
+    const int lane = tid & 31, warp = tid >> 5;
+    const bool dd = P.o.contact_weight_mode == SAPB_WEIGHT_DIAG_DELASSUS;
+    const double h = P.in.dt[e];
+    for (int c = warp; c < cc; c += kPrepNT / 32) {
+      const double* cs = con + 21 * (size_t)c;
       const int lb0 = conint[2 * c], lb1 = conint[2 * c + 1];
-      if (lb1 >= 0 && ((anc[lb1] >> bcol) & 1ull)) rel = rel + (s.v + cross(s.w, load3(cs + 3)));
-      if (lb0 >= 0 && ((anc[lb0] >> bcol) & 1ull)) rel = rel - (s.v + cross(s.w, load3(cs + 0)));
+      double wq[6] = {0, 0, 0, 0, 0, 0}, vq[3] = {0, 0, 0};
+      for (int col = lane; col < n; col += 32) {
+        V3 rel = v3(0, 0, 0);
+        const int bcol = dbody[col];
+        if (bcol >= 0) {
+          const Sv sc = sv_load(S + 6 * col);
+          if (lb1 >= 0 && ((anc[lb1] >> bcol) & 1ull)) rel = rel + (sc.v + cross(sc.w, load3(cs + 3)));
+          if (lb0 >= 0 && ((anc[lb0] >> bcol) & 1ull)) rel = rel - (sc.v + cross(sc.w, load3(cs + 0)));
+        }
+        double rw[3];
+        for (int r = 0; r < 3; ++r) {
+          rw[r] = dot(load3(cs + 12 + 3 * r), rel);
+          Jout[((size_t)c * 3 + r) * n + col] = rw[r];
+        }
+        const double vs = P.in.joint_qd[d0 + col] + h * vdot[col];
+        vq[0] += rw[0] * vs;
+        vq[1] += rw[1] * vs;
+        vq[2] += rw[2] * vs;
+        if (dd) {
+          double aii = adiag[col];
+          if (aii < 1.0e-12) aii = 1.0e-12;
+          const double inv = 1.0 / aii;
+          wq[0] += inv * rw[0] * rw[0];
+          wq[1] += inv * rw[0] * rw[1];
+          wq[2] += inv * rw[0] * rw[2];
+          wq[3] += inv * rw[1] * rw[1];
+          wq[4] += inv * rw[1] * rw[2];
+          wq[5] += inv * rw[2] * rw[2];
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) vq[k] += __shfl_xor_sync(0xffffffffu, vq[k], o);
+        if (dd) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) wq[k] += __shfl_xor_sync(0xffffffffu, wq[k], o);
+        }
+      }
+      if (lane == 0) {
+        const size_t ci = (size_t)e * C + c;
+        if (P.out.vc_star)
+          for (int k = 0; k < 3; ++k) P.out.vc_star[3 * ci + k] = vq[k];
+        if (dd) {
+          // ||J diag(A)^-1 J^T||_F / 3 (sim/contact_jacobian.py:153-251)
+          const double wv = sqrt(wq[0] * wq[0] + wq[3] * wq[3] + wq[5] * wq[5] +
+                                 2.0 * (wq[1] * wq[1] + wq[2] * wq[2] + wq[4] * wq[4])) / 3.0;
+          P.out.w_eff[ci] = wv < 1.0e-12 ? 1.0e-12 : wv;
+        }
+      }
     }
-    for (int r = 0; r < 3; ++r) Jout[((size_t)c * 3 + r) * n + col] = dot(load3(cs + 12 + 3 * r), rel);
   }
   __syncthreads();
-  if (P.out.vc_star) {
-    // free-motion contact velocities J_c v*, v* = qd + dt vdot
-    const double h = P.in.dt[e];
-    for (int k = tid; k < 3 * cc; k += kPrepNT) {
-      const double* row = Jout + (size_t)k * n;
-      double acc = 0.0;
-      for (int col = 0; col < n; ++col) acc += row[col] * (P.in.joint_qd[d0 + col] + h * vdot[col]);
-      P.out.vc_star[(size_t)e * C * 3 + k] = acc;
-    }
-  }
-  // ---- contact weights (sim/contact_jacobian.py:153-251) --------------------
+  // ---- body_inertia contact weights (sim/contact_jacobian.py:153-251) --------
+  if (P.o.contact_weight_mode != SAPB_WEIGHT_DIAG_DELASSUS) {
   for (int c = tid; c < cc; c += kPrepNT) {
     const size_t ci = (size_t)e * C + c;
     double w = 0.0;
-    if (P.o.contact_weight_mode == SAPB_WEIGHT_DIAG_DELASSUS) {
-      double w00 = 0, w01 = 0, w02 = 0, w11 = 0, w12 = 0, w22 = 0;
-      const double* Jc = Jout + (size_t)c * 3 * n;
-      for (int j = 0; j < n; ++j) {
-        double aii = adiag[j];
-        if (aii < 1.0e-12) aii = 1.0e-12;
-        const double inv = 1.0 / aii;
-        const double a0 = Jc[j], a1 = Jc[n + j], a2 = Jc[2 * n + j];
-        w00 += inv * a0 * a0;
-        w01 += inv * a0 * a1;
-        w02 += inv * a0 * a2;
-        w11 += inv * a1 * a1;
-        w12 += inv * a1 * a2;
-        w22 += inv * a2 * a2;
-      }
-      w = sqrt(w00 * w00 + w11 * w11 + w22 * w22 + 2.0 * (w01 * w01 + w02 * w02 + w12 * w12)) / 3.0;
-    } else {
+    {
       const double* cs = con + 21 * (size_t)c;
       const int lbs[2] = {conint[2 * c], conint[2 * c + 1]};
       // body-inertia weights use the witnesses, whatever the point mode
@@ -700,6 +716,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
       w = wsum / 3.0;
     }
     P.out.w_eff[ci] = w < 1.0e-12 ? 1.0e-12 : w;
+  }
   }
 }
 
