@@ -292,36 +292,48 @@ def main():
                          hessian_precision=prec, warm_start=warm, learned_warm_start=ws if warm == "learned" else None)
 
     def run_arm(prec, warm, sampler=None):
+        """Warm-up steps, then the timed steps as replays of a CUDA graph of
+        two whole steps; then the same number of eager steps with per-stage
+        events and per-step statistics (iterations, chosen starts)."""
         solver = make_solver(prec, warm)
         s_in, s_out = fresh_states()
-        for _ in range(args.warmup):
-            solver.step(s_in, s_out, control, contacts, DT)
-            s_in, s_out = s_out, s_in
+        pairs = max(args.steps // 2, 1)
+        graph = solver.capture_steps(s_in, s_out, control, contacts, DT, warmup=max((args.warmup + 1) // 2, 1))
+        graph.replay()
         barrier()
-        solver.stage_events = []
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        iters, chosen = [], []
         if sampler:
             sampler.mark_begin()
         ev0.record(stream)
-        for _ in range(args.steps):
-            solver.step(s_in, s_out, control, contacts, DT)
-            iters.append(solver.contact_solve.newton_iterations_env.sum())
-            chosen.append(torch.bincount(solver.contact_solve.warm_start_accepted_env.long(), minlength=3))
-            s_in, s_out = s_out, s_in
+        for _ in range(pairs):
+            graph.replay()
         ev1.record(stream)
         barrier()
         if sampler:
             sampler.mark_end()
-        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
-        stages = {k: v / args.steps for k, v in solver.stage_times().items()}
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / (2 * pairs))
+        del graph
+        # the same length of rollout again, eager, for the stage split and statistics
+        solver.stage_events = []
+        iters, chosen = [], []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(2 * pairs):
+            solver.step(s_in, s_out, control, contacts, DT)
+            iters.append(solver.contact_solve.newton_iterations_env.sum())
+            chosen.append(torch.bincount(solver.contact_solve.warm_start_accepted_env.long(), minlength=3))
+            s_in, s_out = s_out, s_in
+        e1.record(stream)
+        barrier()
+        ms_eager = max_over_ranks(e0.elapsed_time(e1) / (2 * pairs))
+        stages = {k: v / (2 * pairs) for k, v in solver.stage_times().items()}
         solver.stage_events = None
-        it = float(torch.stack(iters).double().sum().item()) / (args.steps * W)
+        it = float(torch.stack(iters).double().sum().item()) / (2 * pairs * W)
         ch = torch.stack(chosen).sum(0).cpu().numpy()
         conv = bool(solver.contact_solve.converged_env.all())
         counts = solver.contact_jacobian.contact_env_count.clamp(max=MAX_CONTACTS).cpu().numpy()
-        return dict(ms=ms, stages=stages, iters=it, chosen=ch, converged=conv, counts=counts, solver=solver,
-                    final=s_in)
+        return dict(ms=ms, ms_eager=ms_eager, stages=stages, iters=it, chosen=ch, converged=conv, counts=counts,
+                    solver=solver, final=s_in)
 
     plain = run_arm("fp64", "previous_velocity")
     prev = run_arm("fp32", "previous_impulses")
@@ -408,13 +420,17 @@ def main():
                    "worlds_per_gpu": W, "dof_per_env": n, "max_contacts": MAX_CONTACTS, "dt": DT,
                    "parallelism": f"world shards x{world_size}",
                    "l2": "per-step working set (A, J, factor, rows) larger than L2"},
+        "timing": "CUDA graph of two whole steps replayed (steps/2 replays); stages and statistics from the "
+                  "same number of eager steps that follow",
         "plain_fp64": {"value": total / (plain["ms"] * 1e-3), "ms_per_step": plain["ms"],
+                       "ms_per_step_eager": plain["ms_eager"],
                        "mean_newton_iterations": plain["iters"], "all_converged": plain["converged"],
                        "stages_ms": plain["stages"]},
         "learned_fp32": {"mean_newton_iterations": fast["iters"], "all_converged": fast["converged"],
+                         "ms_per_step_eager": fast["ms_eager"],
                          "chosen_start": {"previous_velocity": int(fast["chosen"][0]),
-                                          "previous_impulses": int(fast["chosen"][1]),
-                                          "network": int(fast["chosen"][2])},
+                                          "network": int(fast["chosen"][1]),
+                                          "previous_impulses": int(fast["chosen"][2])},
                          "stages_ms": fast["stages"], "speedup_vs_plain_fp64": plain["ms"] / fast["ms"],
                          "max_rel_qd_diff_vs_plain_fp64_after_rollout": dq},
         "previous_impulses_fp32": {"value": total / (prev["ms"] * 1e-3), "ms_per_step": prev["ms"],

@@ -567,12 +567,17 @@ struct FeatParams {
   float* raw;
 };
 
+// One warp per slot when J_c v* is formed here from J and v*; one thread
+// per slot (every lane its own slot) when vc_star supplies it.
 __global__ void features_kernel(const FeatParams P) {
   const int n = P.p.dof_per_env, C = P.p.max_contacts;
   const long slots = (long)P.p.num_envs * C;
-  const int lane = threadIdx.x & 31;
-  const long warps = (long)gridDim.x * (blockDim.x / 32);
-  for (long s = (long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); s < slots; s += warps) {
+  const bool per_thread = P.vc_star != nullptr;
+  const int lane = per_thread ? 0 : (threadIdx.x & 31);
+  const long stride = per_thread ? (long)gridDim.x * blockDim.x : (long)gridDim.x * (blockDim.x / 32);
+  const long first = per_thread ? (long)blockIdx.x * blockDim.x + threadIdx.x
+                                : (long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  for (long s = first; s < slots; s += stride) {
     const int e = (int)(s / C), c = (int)(s - (long)e * C);
     int count = P.p.contact_count[e];
     count = count < 0 ? 0 : (count > C ? C : count);
@@ -595,7 +600,6 @@ __global__ void features_kernel(const FeatParams P) {
           a1 += J[n + i] * v;
           a2 += J[2 * n + i] * v;
         }
-#pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
           a0 += __shfl_xor_sync(0xffffffffu, a0, o);
           a1 += __shfl_xor_sync(0xffffffffu, a1, o);
@@ -869,7 +873,7 @@ int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const doubl
   P.tau_fallback = tau_fallback;
   P.x = features;
   P.raw = raw;
-  long blocks = (slots + 7) / 8;
+  long blocks = vc_star ? (slots + 255) / 256 : (slots + 7) / 8;
   if (blocks > 8L * sm_count()) blocks = 8L * sm_count();
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   features_kernel<<<(int)blocks, 256, 0, s>>>(P);

@@ -703,9 +703,11 @@ class SolverSAP:
                 lw = LearnedWarmStart.load(DEFAULT_WEIGHTS if lw is None else str(lw), dev)
             self.learned_warm_start = lw
         C = self.max_rigid_contact
-        # candidate impulse sets: [0] the previous step's impulses, [1] the network's
+        # candidate impulse sets: [0] the network's, [1] the previous step's
+        # impulses (evaluated last: it is the usual winner, and the last
+        # candidate's evaluation seeds the first Newton iteration)
         self._gamma_cand = torch.zeros(2, view.W, max(C, 1), 3, dtype=F64, device=dev)
-        self._gamma_prev = self._gamma_cand[0]
+        self._gamma_prev = self._gamma_cand[1]
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
         if self.learned_warm_start is not None:
             self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
@@ -725,6 +727,28 @@ class SolverSAP:
 
     def notify_model_changed(self, flags: int) -> None:
         return
+
+    def capture_steps(self, state_a: SapState, state_b: SapState, control: SapControl | None, contacts, dt,
+                      warmup: int = 1) -> "torch.cuda.CUDAGraph":
+        """Capture two consecutive steps (state_a -> state_b -> state_a) in one
+        CUDA graph; each replay advances the rollout by two steps with every
+        launch of both steps (free motion, warm start, solve, integration)
+        replayed without host work.  `warmup` eager step pairs run first (they
+        advance the rollout too) so the capture sees no first-call setup."""
+        if not isinstance(dt, (int, float)):
+            raise TypeError("capture_steps needs a scalar dt (it is baked into the graph)")
+        side = torch.cuda.Stream(self.view.device)
+        side.wait_stream(torch.cuda.current_stream(self.view.device))
+        with torch.cuda.stream(side):
+            for _ in range(max(int(warmup), 1)):
+                self.step(state_a, state_b, control, contacts, dt)
+                self.step(state_b, state_a, control, contacts, dt)
+        torch.cuda.current_stream(self.view.device).wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+            self.step(state_a, state_b, control, contacts, dt)
+            self.step(state_b, state_a, control, contacts, dt)
+        return graph
 
     def _mark(self, stage: str | None) -> None:
         """Stage timing: when `stage_events` is a list, record a CUDA event on
@@ -792,12 +816,12 @@ class SolverSAP:
         mark("warm_start")
         gamma0 = None
         if self.warm_start == "previous_impulses":
-            gamma0 = self._gamma_cand[0]
+            gamma0 = self._gamma_prev
         elif self.warm_start == "learned":
             self._normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
             self.learned_warm_start.predict(
                 num_envs=self.view.W, dof_per_env=self.view.n, max_contacts=self.max_rigid_contact,
-                normal_up=self._normal_up, gamma_prev=self._gamma_prev, out=self._gamma_cand[1],
+                normal_up=self._normal_up, gamma_prev=self._gamma_prev, out=self._gamma_cand[0],
                 vc_star=self.contact_jacobian.contact_env_vc_star,
                 contact_count=cr.contact_env_count, dynamics_matrix=cr.dynamics_matrix_env,
                 jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff,

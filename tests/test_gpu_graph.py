@@ -1,0 +1,39 @@
+"""The whole SolverSAP step captured in a CUDA graph: replays reproduce the
+eager rollout bit for bit (the step is deterministic: slots are re-ranked,
+reductions have a fixed order, each world is solved by one block)."""
+
+import pytest
+import torch
+
+from sap_warp_b200 import models
+from sap_warp_b200.runtime import SapState
+from sap_warp_b200.solver import SolverSAP
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(state):
+    return (SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone()),
+            SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone()))
+
+
+@pytest.mark.parametrize("warm_start,precision", [("previous_velocity", "fp64"), ("learned", "fp32")])
+def test_graph_replay_matches_eager_steps(cuda_device, warm_start, precision):
+    model, state, control, contacts, _ = models.rollout_scene("humanoid", 256, 7, cuda_device)
+    kw = dict(max_rigid_contact=32, contact_preset_variant="drake", hessian_precision=precision, warm_start=warm_start)
+    eager, graphed = SolverSAP(model, **kw), SolverSAP(model, **kw)
+    ea, eb = pair(state)
+    ga, gb = pair(state)
+    graph = graphed.capture_steps(ga, gb, control, contacts, 2.0e-3, warmup=1)  # 2 eager warm-up steps
+    eager.step(ea, eb, control, contacts, 2.0e-3)  # the two warm-up steps of the capture
+    eager.step(eb, ea, control, contacts, 2.0e-3)
+    for _ in range(3):
+        graph.replay()
+        eager.step(ea, eb, control, contacts, 2.0e-3)
+        eager.step(eb, ea, control, contacts, 2.0e-3)
+    torch.cuda.synchronize()
+    assert torch.equal(ga.joint_q, ea.joint_q) and torch.equal(ga.joint_qd, ea.joint_qd)
+    assert bool(graphed.contact_solve.converged_env.all())
+    del graph

@@ -204,4 +204,4 @@ def test_learned_start_reduces_newton_iterations(cuda_device):
         assert torch.isfinite(state.joint_q).all()
     print(stats)
     assert stats["learned"][0] < 0.8 * stats["previous_velocity"][0], stats
-    assert stats["learned"][1][2] > 0, stats
+    assert stats["learned"][1][1] > 0, stats  # the network's candidate is chosen in some worlds
