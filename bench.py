@@ -292,28 +292,19 @@ def main():
                          hessian_precision=prec, warm_start=warm, learned_warm_start=ws if warm == "learned" else None)
 
     def run_arm(prec, warm, sampler=None):
-        """Warm-up steps, then the timed steps as replays of a CUDA graph of
-        two whole steps; then the same number of eager steps with per-stage
-        events and per-step statistics (iterations, chosen starts)."""
+        """Two passes over the same stretch of the rollout (steps warmup ..
+        warmup + steps of the same trajectory): eager steps with per-stage
+        events and per-step statistics (iterations, chosen starts), then,
+        from the initial state again, the timed steps as replays of a CUDA
+        graph of two whole steps."""
+        pairs = max(args.steps // 2, 1)
+        warm_pairs = max((args.warmup + 1) // 2, 1)
         solver = make_solver(prec, warm)
         s_in, s_out = fresh_states()
-        pairs = max(args.steps // 2, 1)
-        graph = solver.capture_steps(s_in, s_out, control, contacts, DT, warmup=max((args.warmup + 1) // 2, 1))
-        graph.replay()
+        for _ in range(2 * warm_pairs):
+            solver.step(s_in, s_out, control, contacts, DT)
+            s_in, s_out = s_out, s_in
         barrier()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        if sampler:
-            sampler.mark_begin()
-        ev0.record(stream)
-        for _ in range(pairs):
-            graph.replay()
-        ev1.record(stream)
-        barrier()
-        if sampler:
-            sampler.mark_end()
-        ms = max_over_ranks(ev0.elapsed_time(ev1) / (2 * pairs))
-        del graph
-        # the same length of rollout again, eager, for the stage split and statistics
         solver.stage_events = []
         iters, chosen = [], []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -332,8 +323,27 @@ def main():
         ch = torch.stack(chosen).sum(0).cpu().numpy()
         conv = bool(solver.contact_solve.converged_env.all())
         counts = solver.contact_jacobian.contact_env_count.clamp(max=MAX_CONTACTS).cpu().numpy()
+        final_eager = s_in.joint_qd.clone()
+        # timed: graph replays from the initial state
+        solver = make_solver(prec, warm)
+        g_in, g_out = fresh_states()
+        graph = solver.capture_steps(g_in, g_out, control, contacts, DT, warmup=warm_pairs)
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.mark_begin()
+        ev0.record(stream)
+        for _ in range(pairs):
+            graph.replay()
+        ev1.record(stream)
+        barrier()
+        if sampler:
+            sampler.mark_end()
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / (2 * pairs))
+        del graph
+        same = bool(torch.equal(g_in.joint_qd, final_eager))
         return dict(ms=ms, ms_eager=ms_eager, stages=stages, iters=it, chosen=ch, converged=conv, counts=counts,
-                    solver=solver, final=s_in)
+                    solver=solver, final=g_in, graph_matches_eager=same)
 
     plain = run_arm("fp64", "previous_velocity")
     prev = run_arm("fp32", "previous_impulses")
@@ -420,14 +430,15 @@ def main():
                    "worlds_per_gpu": W, "dof_per_env": n, "max_contacts": MAX_CONTACTS, "dt": DT,
                    "parallelism": f"world shards x{world_size}",
                    "l2": "per-step working set (A, J, factor, rows) larger than L2"},
-        "timing": "CUDA graph of two whole steps replayed (steps/2 replays); stages and statistics from the "
-                  "same number of eager steps that follow",
+        "timing": "CUDA graph of two whole steps replayed steps/2 times after the warm-up; stages and "
+                  "statistics from an eager pass over the same steps of the same trajectory",
         "plain_fp64": {"value": total / (plain["ms"] * 1e-3), "ms_per_step": plain["ms"],
                        "ms_per_step_eager": plain["ms_eager"],
                        "mean_newton_iterations": plain["iters"], "all_converged": plain["converged"],
                        "stages_ms": plain["stages"]},
         "learned_fp32": {"mean_newton_iterations": fast["iters"], "all_converged": fast["converged"],
                          "ms_per_step_eager": fast["ms_eager"],
+                         "graph_replay_matches_eager": fast["graph_matches_eager"],
                          "chosen_start": {"previous_velocity": int(fast["chosen"][0]),
                                           "network": int(fast["chosen"][1]),
                                           "previous_impulses": int(fast["chosen"][2])},
