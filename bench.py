@@ -408,6 +408,30 @@ def main():
         snap[label] = {"value": prob.num_envs * world_size / (ms * 1e-3), "ms_per_solve": ms,
                        "mean_newton_iterations": float(buf.newton_iterations.double().mean())}
 
+    # ---- uneven batch: 8192 worlds, a third each 13 / 18 / 35 DOF, one launch ----
+    mix, _ = scenes.mixed_contact_problem(2 * args.worlds, seed=3 + 1000 * rank)
+    tm = problem_to_device(mix, dev)
+    mbuf = ContactSolveBuffers(mix.num_envs, mix.dof_per_env, mix.max_contacts, dev)
+    order = torch.as_tensor(scenes.work_order(mix), dtype=torch.int32).to(dev)
+    uneven = {"worlds": mix.num_envs, "dofs": "13 (arm+box, 2 trees) / 18 / 35, padded to 35",
+              "contacts": "2-8 gripper / min(Poisson(12), 64)"}
+    for label, opts, wo in (("fp64_sorted", make_options("armijo_decay"), order),
+                            ("fp32_sorted", make_options("armijo_decay", hessian_precision="fp32"), order),
+                            ("fp32_index_order", make_options("armijo_decay", hessian_precision="fp32"), None)):
+        for _ in range(max(args.warmup, 1)):
+            contact_solve(**tm, buffers=mbuf, options=opts, world_order=wo)
+        barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k_mix = max(1, min(args.steps, 20))
+        a0.record(stream)
+        for _ in range(k_mix):
+            contact_solve(**tm, buffers=mbuf, options=opts, world_order=wo)
+        a1.record(stream)
+        barrier()
+        ms = max_over_ranks(a0.elapsed_time(a1) / k_mix)
+        uneven[label] = {"value": mix.num_envs * world_size / (ms * 1e-3), "ms_per_solve": ms,
+                         "all_converged": bool(mbuf.converged.all())}
+
     total = W * world_size
     value = total / (fast["ms"] * 1e-3)
     peaks = {}
@@ -447,6 +471,7 @@ def main():
         "previous_impulses_fp32": {"value": total / (prev["ms"] * 1e-3), "ms_per_step": prev["ms"],
                                    "mean_newton_iterations": prev["iters"], "stages_ms": prev["stages"]},
         "stage2_solve_only": snap,
+        "uneven_batch_solve_only": uneven,
         "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "kernel": "contact_solve_kernel", "achieved": achieved, "peak": hbm_peak,

@@ -156,6 +156,10 @@ typedef struct sapb_contact_problem {
    * sapb_free_motion_contacts (dynamics_factor output): the candidate starts
    * solve with it instead of factoring A again.  NULL: factor in the solve. */
   const double* dynamics_factor;
+  /* Optional [E] order in which the persistent kernel takes the worlds (a
+   * permutation of 0..E-1, e.g. by descending estimated work for uneven
+   * batches); entries outside [0, E) are skipped.  NULL: index order. */
+  const int32_t* world_order;
 } sapb_contact_problem;
 
 /* Outputs: the SapContactSolveResult fields a caller reads

@@ -116,6 +116,7 @@ class ContactProblem(C.Structure):
         ("gamma0", _p),
         ("gamma0_count", C.c_int32),
         ("dynamics_factor", _p),
+        ("world_order", _p),
     ]
 
 

@@ -145,6 +145,7 @@ def build_problem(
     v_guess_active: torch.Tensor | None = None,
     dof_terms: DofTermArrays | None = None,
     gamma0: torch.Tensor | None = None,
+    world_order: torch.Tensor | None = None,
 ) -> _abi.ContactProblem:
     """sapb_contact_problem over device tensors (shapes and dtypes checked)."""
     E, n, C = num_envs, dof_per_env, max_contacts
@@ -171,6 +172,7 @@ def build_problem(
     P.gamma0 = _ptr(gamma0, F64, E * C * 3, "gamma0")
     if gamma0 is not None:
         P.gamma0_count = int(gamma0.numel() // (3 * max(E * C, 1)))
+    P.world_order = _ptr(world_order, I32, E, "world_order")
     if dof_terms is not None:
         P.dof = ctypes.pointer(dof_terms.struct)
     return P
@@ -188,7 +190,8 @@ def contact_solve(
     `arrays` are the keyword tensors of `build_problem` (contact_count,
     dynamics_matrix, jacobian, phi0, w_eff, mu, stiffness, tau_d, v_star, v0,
     dt and the optional body maps, v_guess, v_guess_active, dof_terms and the
-    candidate starting impulses gamma0, (E, C, 3) or (K, E, C, 3))."""
+    candidate starting impulses gamma0, (E, C, 3) or (K, E, C, 3), and the
+    persistent kernel's world_order)."""
     lib = load()
     b = buffers
     P = build_problem(num_envs=b.num_envs, dof_per_env=b.dof_per_env, max_contacts=b.max_contacts, **arrays)

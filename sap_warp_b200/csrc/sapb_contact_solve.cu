@@ -889,14 +889,17 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
     // Take the prefetched index, claim the next world and warm L2 with its A
     // and J (prefetch.global.L2 is a hint and has no alignment rule).
     __syncthreads();
-    const int e = s_next;
-    if (e >= P.p.num_envs) break;
+    const int ticket = s_next;
+    if (ticket >= P.p.num_envs) break;
+    const int e = P.p.world_order ? P.p.world_order[ticket] : ticket;
     __syncthreads();
     if (tid == 0) s_next = atomicAdd(P.queue, 1);
     __syncthreads();
+    if (e < 0 || e >= P.p.num_envs) continue;
     {
-      const int nx = s_next;
-      if (nx < P.p.num_envs) {
+      const int nt = s_next;
+      const int nx = nt < P.p.num_envs ? (P.p.world_order ? P.p.world_order[nt] : nt) : P.p.num_envs;
+      if (nx >= 0 && nx < P.p.num_envs) {
         const char* a0 = reinterpret_cast<const char*>(P.p.dynamics_matrix + (size_t)nx * n * n);
         const size_t abytes = sizeof(double) * (size_t)n * n;
         int cnt = P.p.contact_count[nx];

@@ -179,6 +179,7 @@ class ContactProblemArrays:
     v0: np.ndarray
     dt: np.ndarray  # (E,)
     normal_up: np.ndarray | None = None  # (E, C) world-up component of the contact normal
+    dofs_active: np.ndarray | None = None  # (E,) DOFs of each world before padding (mixed batches)
 
     def subset(self, worlds: np.ndarray) -> "ContactProblemArrays":
         """The same problem restricted to a list of worlds (bodies renumbered)."""
@@ -196,6 +197,7 @@ class ContactProblemArrays:
             self.body_dof_start[body_idx].copy(), self.body_dof_count[body_idx].copy(),
             self.v_star[dof_idx].copy(), self.v0[dof_idx].copy(), self.dt[worlds].copy(),
             None if self.normal_up is None else self.normal_up[worlds].copy(),
+            None if self.dofs_active is None else self.dofs_active[worlds].copy(),
         )
 
 
@@ -221,6 +223,7 @@ def humanoid_contact_problem(
     stiffness: float = 1.0e5,
     tau_d: float = 0.01,
     mass_range=(0.5, 2.0),
+    counts: np.ndarray | None = None,
 ) -> ContactProblemArrays:
     """Batched floating-base serial-chain 'humanoid' worlds (6 + `revolute`
     DOFs, one tree per world) with a random pose q, A = M(q) + armature,
@@ -236,6 +239,8 @@ def humanoid_contact_problem(
     A = chain_mass_matrix(model, Rw, ow, Jb)
 
     count = rng.integers(contacts[0], contacts[1] + 1, size=E).astype(np.int32)
+    if counts is not None:
+        count = np.asarray(counts, dtype=np.int32).copy()
     count = np.minimum(count, C)
     # contacts favour the distal half of the chain (feet / hands)
     bodies = rng.integers(B // 2, B, size=(E, C))
@@ -290,3 +295,150 @@ def quadruped_contact_problem(num_worlds: int, seed: int = 1, **kw) -> ContactPr
     kw.setdefault("max_contacts", 16)
     kw.setdefault("mu_range", (0.5, 1.0))
     return humanoid_contact_problem(num_worlds, seed, revolute=12, **kw)
+
+
+def arm_box_contact_problem(num_worlds: int, seed: int = 3, *, contacts=(2, 8), max_contacts: int = 8,
+                            dt: float = 2.0e-3, phi0_range=(-2.0e-3, 0.0), mu_range=(0.3, 1.0),
+                            v_star_std: float = 0.5, stiffness: float = 1.0e5, tau_d: float = 0.01,
+                            counts: np.ndarray | None = None) -> ContactProblemArrays:
+    """A 7-DOF fixed-base arm (serial chain, DOFs 0..6) and a 6-DOF free box
+    (DOFs 7..12, [omega; v] at the box origin) held by gripper contacts
+    between the arm's last link (body 7, shape0) and the box (body 8,
+    shape1): two trees coupled into one clique by J = R (V_box(x) - V_arm(x)).
+    A = blockdiag(M_arm(q), I_box) + armature on the arm."""
+    rng = np.random.default_rng(seed)
+    arm = make_chain(rng, 8)
+    E, C, B = num_worlds, max_contacts, 9
+    base_R = np.broadcast_to(np.eye(3), (E, 3, 3)).copy()
+    base_p = np.tile([0.0, 0.0, 0.5], (E, 1))
+    qj = rng.uniform(-1.0, 1.0, size=(E, 7))
+    Rw, ow, Jb = chain_kinematics(arm, base_R, base_p, qj)
+    A_arm = chain_mass_matrix(arm, Rw, ow, Jb)[:, 6:, 6:]  # the fixed base removes DOFs 0..5
+    J_arm = Jb[:, :, :, 6:]  # (E, 8, 6, 7)
+    m_box = rng.uniform(0.5, 2.0, size=E)
+    R_box = _random_rotations(rng, E)
+    d_box = rng.uniform(0.5, 2.0, size=(E, 3)) * m_box[:, None] * 0.1 ** 2 / 6.0
+    I_box = np.einsum("eij,ej,ekj->eik", R_box, d_box, R_box)
+    p_box = ow[:, 7] + rng.normal(scale=0.03, size=(E, 3))
+    n = 13
+    A = np.zeros((E, n, n))
+    A[:, :7, :7] = A_arm
+    A[:, 7:10, 7:10] = I_box
+    A[:, 10:, 10:] = m_box[:, None, None] * np.eye(3)
+    count = rng.integers(contacts[0], contacts[1] + 1, size=E).astype(np.int32)
+    if counts is not None:
+        count = np.asarray(counts, dtype=np.int32).copy()
+    count = np.minimum(count, C)
+    r_local = rng.normal(size=(E, C, 3))
+    r_local *= (rng.uniform(0.0, 0.05, size=(E, C)) / np.linalg.norm(r_local, axis=-1))[..., None]
+    x = p_box[:, None, :] + r_local
+    normals = rng.normal(size=(E, C, 3))
+    frame = contact_frames(normals)
+    eye = np.broadcast_to(np.eye(3), (E, C, 3, 3))
+    J_box = np.concatenate([-_skew(x - p_box[:, None, :]), eye], -1)  # v + w x r
+    Jl = J_arm[:, 7]  # last link
+    J_a = Jl[:, None, 3:6, :] - np.einsum("ecij,ejk->ecik", _skew(x - ow[:, 7][:, None, :]), Jl[:, 0:3, :])
+    J_point = np.concatenate([-J_a, J_box], -1)  # (E, C, 3, 13): V1 - V0, body1 = box
+    jac = np.einsum("ecrj,ecjk->ecrk", frame, J_point)
+    live = np.arange(C)[None, :] < count[:, None]
+    jac *= live[..., None, None]
+    phi0 = rng.uniform(*phi0_range, size=(E, C)) * live
+    mu = rng.uniform(*mu_range, size=(E, C)) * live
+    w_eff = diag_delassus_weight(jac, A) * live
+    env = np.arange(E)[:, None]
+    body0 = np.where(live, env * B + 7, -1).astype(np.int32)
+    body1 = np.where(live, env * B + 8, -1).astype(np.int32)
+    start = np.tile(np.array([-1, 0, 0, 0, 0, 0, 0, 0, 7], np.int32), E)
+    cnt_dof = np.tile(np.array([0, 7, 7, 7, 7, 7, 7, 7, 6], np.int32), E)
+    v_star = rng.normal(scale=v_star_std, size=(E, n))
+    return ContactProblemArrays(
+        num_envs=E, dof_per_env=n, max_contacts=C, bodies_per_env=B, contact_count=count, dynamics_matrix=A,
+        jacobian=jac, phi0=phi0, w_eff=w_eff, mu=mu, stiffness=np.full((E, C), stiffness) * live,
+        tau_d=np.full((E, C), tau_d) * live, body0=body0, body1=body1, body_dof_start=start,
+        body_dof_count=cnt_dof, v_star=v_star.reshape(-1),
+        v0=(v_star + rng.normal(scale=0.01, size=(E, n))).reshape(-1), dt=np.full(E, dt),
+        normal_up=frame[:, :, 2, 2] * live)
+
+
+def pad_problem(p: ContactProblemArrays, n_max: int, C_max: int, B_max: int) -> ContactProblemArrays:
+    """The same worlds with n_max DOFs, C_max slots and B_max bodies: the
+    extra DOFs get an identity block in A, zero Jacobian columns and
+    v* = v0 = 0, so they take no part in the solve and stay at zero; the
+    solution of the real DOFs is unchanged."""
+    E, n, C, B = p.num_envs, p.dof_per_env, p.max_contacts, p.bodies_per_env
+    assert n <= n_max and C <= C_max and B <= B_max
+    A = np.zeros((E, n_max, n_max))
+    A[:, :n, :n] = p.dynamics_matrix
+    A[:, n:, n:] = np.eye(n_max - n)
+    J = np.zeros((E, C_max, 3, n_max))
+    J[:, :C, :, :n] = p.jacobian
+    pad_c = lambda a: np.pad(a, ((0, 0), (0, C_max - C)))
+    remap = lambda b: np.where(b >= 0, (b // B) * B_max + b % B, -1).astype(np.int32)
+    body_start = np.full((E, B_max), -1, np.int32)
+    body_count = np.zeros((E, B_max), np.int32)
+    body_start[:, :B] = p.body_dof_start.reshape(E, B)
+    body_count[:, :B] = p.body_dof_count.reshape(E, B)
+    pad_v = lambda v: np.pad(v.reshape(E, n), ((0, 0), (0, n_max - n))).reshape(-1)
+    return ContactProblemArrays(
+        num_envs=E, dof_per_env=n_max, max_contacts=C_max, bodies_per_env=B_max,
+        contact_count=p.contact_count.copy(), dynamics_matrix=A, jacobian=J, phi0=pad_c(p.phi0),
+        w_eff=pad_c(p.w_eff), mu=pad_c(p.mu), stiffness=pad_c(p.stiffness), tau_d=pad_c(p.tau_d),
+        body0=np.pad(remap(p.body0), ((0, 0), (0, C_max - C)), constant_values=-1),
+        body1=np.pad(remap(p.body1), ((0, 0), (0, C_max - C)), constant_values=-1),
+        body_dof_start=body_start.reshape(-1), body_dof_count=body_count.reshape(-1), v_star=pad_v(p.v_star),
+        v0=pad_v(p.v0), dt=p.dt.copy(), normal_up=None if p.normal_up is None else pad_c(p.normal_up),
+        dofs_active=np.full(E, n, np.int32) if p.dofs_active is None else p.dofs_active.copy())
+
+
+def concat_problems(parts) -> ContactProblemArrays:
+    """One batch of problems with equal n, C and B (body indices renumbered)."""
+    n, C, B = parts[0].dof_per_env, parts[0].max_contacts, parts[0].bodies_per_env
+    assert all(q.dof_per_env == n and q.max_contacts == C and q.bodies_per_env == B for q in parts)
+    offs = np.cumsum([0] + [q.num_envs for q in parts])
+    shift = lambda b, o: np.where(b >= 0, b + o * B, -1).astype(np.int32)
+    cat = lambda name: np.concatenate([getattr(q, name) for q in parts])
+    return ContactProblemArrays(
+        num_envs=int(offs[-1]), dof_per_env=n, max_contacts=C, bodies_per_env=B, contact_count=cat("contact_count"),
+        dynamics_matrix=cat("dynamics_matrix"), jacobian=cat("jacobian"), phi0=cat("phi0"), w_eff=cat("w_eff"),
+        mu=cat("mu"), stiffness=cat("stiffness"), tau_d=cat("tau_d"),
+        body0=np.concatenate([shift(q.body0, o) for q, o in zip(parts, offs)]),
+        body1=np.concatenate([shift(q.body1, o) for q, o in zip(parts, offs)]),
+        body_dof_start=cat("body_dof_start"), body_dof_count=cat("body_dof_count"), v_star=cat("v_star"),
+        v0=cat("v0"), dt=cat("dt"),
+        normal_up=None if any(q.normal_up is None for q in parts) else cat("normal_up"),
+        dofs_active=np.concatenate([q.dofs_active if q.dofs_active is not None else
+                                    np.full(q.num_envs, q.dof_per_env, np.int32) for q in parts]))
+
+
+def poisson_counts(rng: np.random.Generator, E: int, lam: float = 12.0, lo: int = 1, hi: int = 64) -> np.ndarray:
+    return np.clip(rng.poisson(lam, size=E), lo, hi).astype(np.int32)
+
+
+def mixed_contact_problem(num_worlds: int, seed: int = 3, max_contacts: int = 64):
+    """The uneven batch: a third each of arm + box (13 DOF, 2-8 gripper
+    contacts), quadruped (18 DOF) and humanoid (35 DOF) worlds, contacts of
+    the last two ~ min(Poisson(12), max_contacts) (at least 1), padded to 35
+    DOF and max_contacts slots.  Returns (problem, parts): parts are the
+    unpadded per-kind problems in batch order."""
+    rng = np.random.default_rng(seed)
+    k = num_worlds // 3
+    sizes = [k, k, num_worlds - 2 * k]
+    arm = arm_box_contact_problem(sizes[0], seed=seed)
+    quad = humanoid_contact_problem(sizes[1], seed=seed + 1, revolute=12, max_contacts=max_contacts,
+                                    counts=poisson_counts(rng, sizes[1], hi=max_contacts), mu_range=(0.5, 1.0))
+    hum = humanoid_contact_problem(sizes[2], seed=seed + 2, max_contacts=max_contacts,
+                                   counts=poisson_counts(rng, sizes[2], hi=max_contacts))
+    parts = [arm, quad, hum]
+    B_max = max(q.bodies_per_env for q in parts)
+    prob = concat_problems([pad_problem(q, 35, max_contacts, B_max) for q in parts])
+    return prob, parts
+
+
+def work_order(prob: ContactProblemArrays) -> np.ndarray:
+    """Worlds by descending estimated solve work n^3/3 + C n^2 (n the
+    world's own DOF count): the order a persistent kernel should take them in
+    so the biggest worlds do not finish last."""
+    n = prob.dofs_active if prob.dofs_active is not None else np.full(prob.num_envs, prob.dof_per_env)
+    C = np.minimum(prob.contact_count, prob.max_contacts).astype(np.float64)
+    work = n.astype(np.float64) ** 3 / 3.0 + C * n.astype(np.float64) ** 2
+    return np.argsort(-work, kind="stable").astype(np.int32)

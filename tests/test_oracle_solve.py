@@ -168,3 +168,21 @@ def test_truncated_and_empty_inputs(oracle):
     empty = prob.subset(np.array([], dtype=np.int64))
     res = oracle.solve(empty, "armijo_decay")
     assert res["v"].size == 0
+
+
+def test_padding_to_a_mixed_batch_is_exact(oracle):
+    """Identity-padded DOFs and extra slots change no world's answer or
+    iteration count (the uneven batch runs as one padded launch)."""
+    from sap_warp_b200 import scenes
+
+    prob, parts = scenes.mixed_contact_problem(24, seed=4, max_contacts=16)
+    r = oracle.solve(prob, "armijo_decay")
+    off = 0
+    for q in parts:
+        rq = oracle.solve(q, "armijo_decay")
+        E, n = q.num_envs, q.dof_per_env
+        v = r["v"].reshape(prob.num_envs, -1)
+        np.testing.assert_array_equal(v[off:off + E, :n], rq["v"].reshape(E, n))
+        assert np.all(v[off:off + E, n:] == 0.0)
+        np.testing.assert_array_equal(r["newton_iterations"][off:off + E], rq["newton_iterations"])
+        off += E
