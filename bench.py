@@ -159,8 +159,8 @@ class ClockSampler:
 # ---- CPU pipeline of the step (oracle restatement), for the baselines ---------
 def cpu_scene(worlds: int, seed: int):
     """The rollout scene built on the host: same distributions as
-    models.rollout_scene, body poses from the numpy free motion."""
-    from oracle import free_motion as ofm
+    models.rollout_scene, body poses from the C restatement."""
+    from oracle import oracle
     from sap_warp_b200 import models
 
     rng = np.random.default_rng(seed)
@@ -169,41 +169,42 @@ def cpu_scene(worlds: int, seed: int):
     q = models.random_joint_q(tpl, rng, worlds)
     n, B = tpl["dofs_per_world"], tpl["bodies_per_world"]
     qd = rng.normal(scale=0.5, size=(worlds, n))
-    om = ofm.Model(dict(tpl, gravity=g["gravity"][0], shape_body_global=g["shape_body"],
-                        shape_mu=g["shape_material_mu"], shape_ke=g["shape_material_ke"],
-                        shape_tau=g["shape_material_tau"]))
-    fm = ofm.free_motion(om, q, qd, np.zeros_like(qd), np.zeros((worlds, B, 6)), np.full(worlds, DT))
+    hm = oracle.HostModel(tpl, g)
+    empty = dict(count=np.zeros(1, np.int32), shape0=np.zeros(1, np.int32), shape1=np.zeros(1, np.int32),
+                 point0=np.zeros((1, 3)), point1=np.zeros((1, 3)), normal=np.zeros((1, 3)), margin0=np.zeros(1),
+                 margin1=np.zeros(1))
+    bq = oracle.free_motion_contacts(hm, q, qd, empty, np.full(worlds, DT), 1)["body_q"].reshape(worlds, B, 7)
     counts = rng.integers(8, 33, size=worlds)
-    con = models.ground_contacts(rng, fm["pos"], fm["quat"], counts, bodies_from=B // 2, capacity=int(counts.sum()))
-    return dict(tpl=tpl, om=om, q=q, qd=qd, con=con)
+    con = models.ground_contacts(rng, bq[..., :3], bq[..., 3:], counts, bodies_from=B // 2,
+                                 capacity=int(counts.sum()))
+    return dict(tpl=tpl, hm=hm, q=q, qd=qd, con=con)
 
 
 def cpu_steps(scene: dict, steps: int, threads: int, min_seconds: float = 0.0):
-    """Seconds per world-step of the CPU pipeline (numpy free motion and
-    contact rows, C oracle solve with OpenMP, numpy integration), drake
-    preset, FP64, previous-velocity warm start."""
-    from oracle import free_motion as ofm
+    """Seconds per world-step of the CPU pipeline -- the C restatements of
+    the free motion and contact rows and of the solve (OpenMP over worlds) and
+    of the integration -- drake preset, FP64, previous-velocity warm start."""
     from oracle import oracle
     from sap_warp_b200 import scenes
 
-    om, tpl = scene["om"], scene["tpl"]
+    hm, tpl = scene["hm"], scene["tpl"]
     q, qd = scene["q"].copy(), scene["qd"].copy()
     W, n, B = q.shape[0], tpl["dofs_per_world"], tpl["bodies_per_world"]
     dt = np.full(W, DT)
     done, t0 = 0, time.perf_counter()
     for k in range(max(1, steps)):
-        fm = ofm.free_motion(om, q, qd, np.zeros_like(qd), np.zeros((W, B, 6)), dt)
-        cr = ofm.contact_jacobian(om, fm, scene["con"], MAX_CONTACTS, point_mode="contact_midpoint",
-                                  weight_mode="diag_delassus", fallback_tau=0.0)
+        r = oracle.free_motion_contacts(hm, q, qd, scene["con"], dt, MAX_CONTACTS, point_mode="contact_midpoint",
+                                        weight_mode="diag_delassus", threads=threads)
         prob = scenes.ContactProblemArrays(
             num_envs=W, dof_per_env=n, max_contacts=MAX_CONTACTS, bodies_per_env=B,
-            contact_count=cr["count"].astype(np.int32), dynamics_matrix=fm["A"], jacobian=cr["jac"],
-            phi0=cr["phi0"], w_eff=cr["w"], mu=cr["mu"], stiffness=cr["k"], tau_d=cr["tau"], body0=cr["body0"],
-            body1=cr["body1"], body_dof_start=np.zeros(W * B, np.int32), body_dof_count=np.full(W * B, n, np.int32),
-            v_star=fm["v_star"].reshape(-1), v0=qd.reshape(-1), dt=dt)
+            contact_count=np.minimum(r["count"], MAX_CONTACTS).astype(np.int32), dynamics_matrix=r["A"],
+            jacobian=r["jac"], phi0=r["phi0"], w_eff=r["w"], mu=r["mu"], stiffness=r["k"], tau_d=r["tau"],
+            body0=r["body0"], body1=r["body1"], body_dof_start=np.zeros(W * B, np.int32),
+            body_dof_count=np.full(W * B, n, np.int32), v_star=r["v_star"].reshape(-1), v0=qd.reshape(-1), dt=dt)
         sol = oracle.solve(prob, "armijo_decay", threads=threads, v_guess=qd.reshape(-1), v_guess_active=k > 0)
         v = sol["v"].reshape(W, n)
-        q = ofm.integrate(om, q, qd, v, dt, "sap_euler")
+        q = oracle.integrate_positions(hm, q.reshape(-1), qd.reshape(-1), v.reshape(-1), dt,
+                                       "sap_euler").reshape(W, -1)
         qd = v
         done += 1
         if min_seconds and time.perf_counter() - t0 > min_seconds:
@@ -218,7 +219,7 @@ def run_reference(args, rank: int, world_size: int):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    sample_worlds = 128
+    sample_worlds = 1024
     scene = cpu_scene(sample_worlds, SEED)
     cpu_steps(scene, max(1, min(args.warmup, 2)), cores)
     sec, k = cpu_steps(scene, max(args.steps, 1), cores, min_seconds=60.0)
@@ -232,8 +233,8 @@ def run_reference(args, rank: int, world_size: int):
         "cpu_baseline": {"value": value, "unit": "world-steps/s", "cores": cores, "kind": "port",
                          "sample": f"{k} steps of a {sample_worlds}-world rollout"},
         "e2e": {"value": value, "unit": "world-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference (Python + NVIDIA Warp) is not installable offline; the FP64 CPU restatement of its "
-                "step is timed instead",
+        "note": "reference (Python + NVIDIA Warp) is not installable offline; the FP64 C restatement of its "
+                "step (OpenMP over worlds) is timed instead",
     }
     print(json.dumps(line), flush=True)
 
@@ -483,10 +484,11 @@ def main():
     }
     if rank == 0 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        scene = cpu_scene(64, SEED)
+        scene = cpu_scene(1024, SEED)
         sec, k = cpu_steps(scene, 1000, cores, min_seconds=10.0)
-        line["cpu_baseline"] = {"value": 64 / sec, "unit": "world-steps/s", "cores": cores, "kind": "port",
-                                "sample": f"{k} steps of a 64-world rollout (numpy free motion and rows, C solve)"}
+        line["cpu_baseline"] = {"value": 1024 / sec, "unit": "world-steps/s", "cores": cores, "kind": "port",
+                                "sample": f"{k} steps of a 1024-world rollout (C restatement: free motion, rows, "
+                                          f"solve, integration; OpenMP over worlds)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -56,6 +56,20 @@ int32_t sapo_cholesky(double* a, int32_t n);
 
 void sapo_solve_options_default(sapb_solve_options* opts, int32_t line_search_variant);
 
+/* Free motion, contact rows and weights of every world (host pointers; the
+ * same structs as sapb_free_motion_contacts), contacts in flat order per
+ * world.  Restates SapFreeMotion.compute and SapContactJacobian.compute
+ * (sim/free_motion.py:1804-2178, sim/contact_jacobian.py:153-562,
+ * 1649-1985) with the reference's body-origin recursions.  OpenMP over
+ * worlds; num_threads <= 0: OpenMP default. */
+int32_t sapo_free_motion_contacts(const sapb_model_desc* model, const sapb_step_inputs* in,
+                                  const sapb_prepare_options* opts, const sapb_prepare_outputs* out,
+                                  int32_t num_threads);
+
+/* Position integration (sim/solver_sap.py:144-733), host pointers. */
+int32_t sapo_integrate_positions(const sapb_model_desc* model, const double* q_in, const double* v_prev,
+                                 const double* v_new, const double* dt, int32_t mode, double* q_out);
+
 #ifdef __cplusplus
 }
 #endif
