@@ -872,7 +872,10 @@ __device__ LsResult ls_exact(const World<NT, HT, NS>& w, const SolveParams& P, d
   return r;
 }
 
-template <int NT, typename HT, int MINB, int NS>
+// LSV: the line search, fixed at compile time (SAPB_LS_ARMIJO_DECAY,
+// SAPB_LS_EXACT_ROOT or SAPB_LS_MONOTONE_DECAY) so that one instantiation
+// holds the code of one search only (smaller instruction footprint).
+template <int NT, typename HT, int MINB, int NS, int LSV>
 __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolveParams P) {
   static_assert(NT / 32 <= Layout::kMaxWarps, "partial-sum scratch sized for kMaxWarps warps");
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1176,7 +1179,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         }
         __syncthreads();
       }
-      const double cost_min_alpha = P.o.line_search_variant == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
+      const double cost_min_alpha = LSV == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
       int it = 0;
       bool active = true;
       for (;;) {
@@ -1214,15 +1217,15 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         assemble_hessian<NT, HT, NS>(w, P.o.diag_shift);
         factor_and_solve<NT, HT, NS>(w);
         LsResult r;
-        if (P.o.line_search_variant == SAPB_LS_ARMIJO_DECAY)
+        if constexpr (LSV == SAPB_LS_ARMIJO_DECAY)
           r = ls_armijo<NT, HT, NS>(w, P, dt, cost);
-        else if (P.o.line_search_variant == SAPB_LS_EXACT_ROOT)
+        else if constexpr (LSV == SAPB_LS_EXACT_ROOT)
           r = ls_exact<NT, HT, NS>(w, P, dt, cost);
         else
           r = ls_monotone<NT, HT, NS>(w, P, dt, cost);
         alpha = r.alpha;
         status = r.status;
-        const bool mono = P.o.line_search_variant == SAPB_LS_MONOTONE_DECAY;
+        constexpr bool mono = LSV == SAPB_LS_MONOTONE_DECAY;
         if (r.accepted || mono) ls_total += r.iterations;
         if (r.accepted) {
           previous_cost = cost;
@@ -1266,10 +1269,10 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   }
 }
 
-template <int NT, typename HT, int MINB, int NS>
-static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
+template <int NT, typename HT, int MINB, int NS, int LSV>
+static cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
   const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT));
-  auto kern = contact_solve_kernel<NT, HT, MINB, NS>;
+  auto kern = contact_solve_kernel<NT, HT, MINB, NS, LSV>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (err != cudaSuccess) return err;
   int dev = 0;
@@ -1290,6 +1293,18 @@ static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* 
   if (err != cudaSuccess) return err;
   kern<<<blocks, NT, L.total, stream>>>(P);
   return cudaGetLastError();
+}
+
+template <int NT, typename HT, int MINB, int NS>
+static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
+  switch (P.o.line_search_variant) {
+    case SAPB_LS_ARMIJO_DECAY:
+      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_ARMIJO_DECAY>(P, stream, blocks_out);
+    case SAPB_LS_EXACT_ROOT:
+      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_EXACT_ROOT>(P, stream, blocks_out);
+    default:
+      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_MONOTONE_DECAY>(P, stream, blocks_out);
+  }
 }
 
 size_t contact_solve_smem_bytes(int n, int C, int hessian_precision) {
