@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 2
+#define SAPB_ABI_VERSION 3
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -44,6 +44,9 @@ extern "C" {
 #define SAPB_LS_BAD_BRACKET (-3)
 #define SAPB_LS_BAD_GUESS (-4)
 #define SAPB_LS_ROOT_ITERATION_CAP (-5)
+/* Per-world status of sapb_blocked_contact_solve: the world's block factor
+ * needs more off-diagonal blocks than sapb_blocked_fill_capacity; v = v*. */
+#define SAPB_WORLD_FACTOR_CAPACITY (-10)
 
 /* contact modes (sim/contact_solve.py:60-63) */
 #define SAPB_CONTACT_MODE_NONE 0
@@ -335,6 +338,65 @@ int32_t sapb_contact_solve(const sapb_contact_problem* problem, const sapb_solve
  * (concurrent streams) race: serialize them. */
 int32_t sapb_contact_solve_noalloc(const sapb_contact_problem* problem, const sapb_solve_options* opts,
                                    const sapb_solve_outputs* out, void* stream);
+
+/* ---- worlds of many small trees ---------------------------------------------
+ * The stage-2 problem in a tree-blocked layout, for worlds made of up to 64
+ * trees of tree_dofs DOFs each (for example 64 free bodies: 384 DOFs).  The
+ * reference keeps such worlds dense: A_env with its zero blocks between trees
+ * (sim/contact_jacobian.py:110-150) and J rows over all n DOFs (:404-562).
+ * Here A is its diagonal tree blocks and each contact row holds the columns
+ * of the (at most two) trees the contact touches.  World DOF order is tree
+ * by tree: DOF t * tree_dofs + a is DOF a of tree t.  A contact whose two
+ * sides lie on one tree is given as one side with the summed columns.  No
+ * PD or limit terms (free bodies have none). */
+typedef struct sapb_blocked_problem {
+  int32_t num_envs;
+  int32_t trees_per_env;          /* T <= 64 */
+  int32_t tree_dofs;              /* NB: 6 (a free body) */
+  int32_t max_contacts;           /* C: per-world slot capacity */
+  const int32_t* contact_count;   /* [E] contacts per world (clamped to C) */
+  const double* tree_mass;        /* [E,T,NB,NB] diagonal blocks of A */
+  const double* jacobian;         /* [E,C,3,2*NB]: columns [0,NB) on contact_tree[..,0], [NB,2NB) on [..,1] */
+  const int32_t* contact_tree;    /* [E,C,2] tree of each side, -1: none (static) */
+  const double* phi0;             /* [E,C] */
+  const double* w_eff;            /* [E,C] */
+  const double* mu;               /* [E,C] */
+  const double* stiffness;        /* [E,C] */
+  const double* tau_d;            /* [E,C] or NULL -> options.contact_tau_d */
+  const double* v_star;           /* [E*n] free-motion velocity */
+  const double* v0;               /* [E*n] start-of-step velocity */
+  double* v_guess;                /* [E*n] warm start in / seeded velocity out, or NULL */
+  const int32_t* v_guess_active;  /* [1] nonzero: start from v_guess; NULL: never */
+  const double* dt;               /* [E] */
+  const int32_t* world_order;     /* [E] order of the persistent queue, or NULL */
+} sapb_blocked_problem;
+
+/* Off-diagonal factor blocks one world of this shape can hold on chip
+ * (0: the shape does not fit or tree_dofs != 6).  A world whose
+ * elimination (greedy minimum degree, with fill) needs more gets the
+ * per-world status SAPB_WORLD_FACTOR_CAPACITY. */
+int32_t sapb_blocked_fill_capacity(int32_t trees_per_env, int32_t tree_dofs, int32_t max_contacts,
+                                   int32_t hessian_precision);
+
+/* Bytes of device workspace sapb_blocked_contact_solve needs. */
+size_t sapb_blocked_solve_workspace_size(int32_t num_envs, int32_t trees_per_env, int32_t max_contacts);
+
+/* The solve of sapb_contact_solve on the tree-blocked layout: the same
+ * Newton loop, line searches and convergence test (sim/contact_solve.py:
+ * 6129-6285), the Newton Hessian block sparse (a block per tree and per
+ * pair of trees in contact) and factored by a block LDL^T in
+ * hessian_precision.  Outputs as sapb_contact_solve (v in the tree-by-tree
+ * DOF order; warm_start_accepted written 0). */
+int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* problem, const sapb_solve_options* opts,
+                                   const sapb_solve_outputs* out, void* workspace, size_t workspace_bytes,
+                                   void* stream);
+
+/* Gather a dense problem whose worlds are trees_per_env trees of tree_dofs
+ * DOFs (body_dof_start of a body = its tree's first DOF) into the blocked
+ * layout: tree_mass [E,T,NB,NB], jacobian [E,C,3,2NB], contact_tree [E,C,2]
+ * (device pointers).  The other blocked fields alias the dense ones. */
+int32_t sapb_dense_to_blocked(const sapb_contact_problem* dense, int32_t trees_per_env, int32_t tree_dofs,
+                              double* tree_mass, double* jacobian, int32_t* contact_tree, void* stream);
 
 /* Last CUDA error string seen by the library on this thread ("" if none). */
 const char* sapb_last_error(void);

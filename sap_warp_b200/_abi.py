@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 2
+SAPB_ABI_VERSION = 3
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -22,6 +22,7 @@ SAPB_LS_ALPHA_UNDERFLOW = -2
 SAPB_LS_BAD_BRACKET = -3
 SAPB_LS_BAD_GUESS = -4
 SAPB_LS_ROOT_ITERATION_CAP = -5
+SAPB_WORLD_FACTOR_CAPACITY = -10
 
 SAPB_CONTACT_MODE_NONE = 0
 SAPB_CONTACT_MODE_STICTION = 1
@@ -116,6 +117,30 @@ class ContactProblem(C.Structure):
         ("gamma0", _p),
         ("gamma0_count", C.c_int32),
         ("dynamics_factor", _p),
+        ("world_order", _p),
+    ]
+
+
+class BlockedProblem(C.Structure):
+    _fields_ = [
+        ("num_envs", C.c_int32),
+        ("trees_per_env", C.c_int32),
+        ("tree_dofs", C.c_int32),
+        ("max_contacts", C.c_int32),
+        ("contact_count", _p),
+        ("tree_mass", _p),
+        ("jacobian", _p),
+        ("contact_tree", _p),
+        ("phi0", _p),
+        ("w_eff", _p),
+        ("mu", _p),
+        ("stiffness", _p),
+        ("tau_d", _p),
+        ("v_star", _p),
+        ("v0", _p),
+        ("v_guess", _p),
+        ("v_guess_active", _p),
+        ("dt", _p),
         ("world_order", _p),
     ]
 
@@ -267,6 +292,13 @@ EXPORTS = {
         C.c_int32, [C.POINTER(ContactProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p]
     ),
     "sapb_last_error": (C.c_char_p, []),
+    "sapb_blocked_fill_capacity": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "sapb_blocked_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
+    "sapb_blocked_contact_solve": (
+        C.c_int32,
+        [C.POINTER(BlockedProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p, C.c_size_t, _p],
+    ),
+    "sapb_dense_to_blocked": (C.c_int32, [C.POINTER(ContactProblem), C.c_int32, C.c_int32, _p, _p, _p, _p]),
     "sapb_prepare_workspace_size": (C.c_size_t, [C.POINTER(ModelDesc), C.c_int32]),
     "sapb_free_motion_contacts": (
         C.c_int32,

@@ -235,3 +235,115 @@ def problem_to_device(prob, device) -> dict:
         v0=t(prob.v0, F64),
         dt=t(prob.dt, F64),
     )
+
+
+def blocked_contact_solve(
+    *,
+    buffers: ContactSolveBuffers,
+    options: _abi.SolveOptions,
+    trees_per_env: int,
+    tree_dofs: int = 6,
+    stream: torch.cuda.Stream | None = None,
+    contact_count: torch.Tensor,
+    tree_mass: torch.Tensor,
+    jacobian: torch.Tensor,
+    contact_tree: torch.Tensor,
+    phi0: torch.Tensor,
+    w_eff: torch.Tensor,
+    mu: torch.Tensor,
+    stiffness: torch.Tensor,
+    tau_d: torch.Tensor | None,
+    v_star: torch.Tensor,
+    v0: torch.Tensor,
+    dt: torch.Tensor,
+    v_guess: torch.Tensor | None = None,
+    v_guess_active: torch.Tensor | None = None,
+    world_order: torch.Tensor | None = None,
+) -> ContactSolveBuffers:
+    """Launch the tree-blocked solve (sapb_blocked_contact_solve) for worlds of
+    `trees_per_env` trees of `tree_dofs` DOFs; results land in `buffers`
+    (dof_per_env = trees_per_env * tree_dofs), no host sync."""
+    lib = load()
+    b = buffers
+    E, C, T, NB = b.num_envs, b.max_contacts, trees_per_env, tree_dofs
+    if T * NB != b.dof_per_env:
+        raise ValueError(f"buffers hold {b.dof_per_env} DOFs per world, not {T} trees x {NB}")
+    n = T * NB
+    P = _abi.BlockedProblem()
+    P.num_envs, P.trees_per_env, P.tree_dofs, P.max_contacts = E, T, NB, C
+    P.contact_count = _ptr(contact_count, I32, E, "contact_count")
+    P.tree_mass = _ptr(tree_mass, F64, E * T * NB * NB, "tree_mass")
+    P.jacobian = _ptr(jacobian, F64, E * C * 3 * 2 * NB, "jacobian")
+    P.contact_tree = _ptr(contact_tree, I32, E * C * 2, "contact_tree")
+    P.phi0 = _ptr(phi0, F64, E * C, "phi0")
+    P.w_eff = _ptr(w_eff, F64, E * C, "w_eff")
+    P.mu = _ptr(mu, F64, E * C, "mu")
+    P.stiffness = _ptr(stiffness, F64, E * C, "stiffness")
+    P.tau_d = _ptr(tau_d, F64, E * C, "tau_d")
+    P.v_star = _ptr(v_star, F64, E * n, "v_star")
+    P.v0 = _ptr(v0, F64, E * n, "v0")
+    P.v_guess = _ptr(v_guess, F64, E * n, "v_guess")
+    P.v_guess_active = _ptr(v_guess_active, I32, 1, "v_guess_active")
+    P.dt = _ptr(dt, F64, E, "dt")
+    P.world_order = _ptr(world_order, I32, E, "world_order")
+    out = _abi.SolveOutputs()
+    out.v = b.v.data_ptr()
+    out.contact_gamma = b.contact_gamma.data_ptr()
+    out.contact_mode = b.contact_mode.data_ptr()
+    out.cost = b.cost.data_ptr()
+    out.newton_iterations = b.newton_iterations.data_ptr()
+    out.line_search_iterations = b.line_search_iterations.data_ptr()
+    out.converged = b.converged.data_ptr()
+    out.status = b.status.data_ptr()
+    out.grad_norm = b.grad_norm.data_ptr()
+    out.warm_start_accepted = b.warm_start_accepted.data_ptr()
+    s = stream if stream is not None else torch.cuda.current_stream(b.device)
+    status = lib.sapb_blocked_contact_solve(
+        ctypes.byref(P), ctypes.byref(options), ctypes.byref(out), b.workspace.data_ptr(), b.workspace.numel(),
+        ctypes.c_void_p(s.cuda_stream),
+    )
+    check(status, "sapb_blocked_contact_solve")
+    return buffers
+
+
+def blocked_fill_capacity(trees_per_env: int, tree_dofs: int, max_contacts: int, hessian_precision: str) -> int:
+    """Off-diagonal factor blocks one world of this shape holds on chip."""
+    prec = _abi.SAPB_FP32 if hessian_precision == "fp32" else _abi.SAPB_FP64
+    return int(load().sapb_blocked_fill_capacity(trees_per_env, tree_dofs, max_contacts, prec))
+
+
+def dense_to_blocked(arrays: dict, num_envs: int, dof_per_env: int, max_contacts: int, trees_per_env: int,
+                     tree_dofs: int = 6, stream: torch.cuda.Stream | None = None) -> dict:
+    """Blocked tensors (tree_mass, jacobian, contact_tree) gathered on the
+    device from the dense problem tensors of `build_problem`."""
+    lib = load()
+    E, C, T, NB = num_envs, max_contacts, trees_per_env, tree_dofs
+    dev = arrays["dynamics_matrix"].device
+    P = build_problem(num_envs=E, dof_per_env=dof_per_env, max_contacts=C, **arrays)
+    tm = torch.empty(E, T, NB, NB, dtype=F64, device=dev)
+    jac = torch.empty(E, C, 3, 2 * NB, dtype=F64, device=dev)
+    ct = torch.empty(E, C, 2, dtype=I32, device=dev)
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    status = lib.sapb_dense_to_blocked(ctypes.byref(P), T, NB, tm.data_ptr(), jac.data_ptr(), ct.data_ptr(),
+                                       ctypes.c_void_p(s.cuda_stream))
+    check(status, "sapb_dense_to_blocked")
+    return dict(tree_mass=tm, jacobian=jac, contact_tree=ct)
+
+
+def blocked_problem_to_device(prob, device) -> dict:
+    """Device tensors of a scenes.BlockedProblemArrays."""
+    t = lambda a, dt: torch.as_tensor(a, dtype=dt).contiguous().to(device)
+    return dict(
+        contact_count=t(prob.contact_count, I32),
+        tree_mass=t(prob.tree_mass, F64),
+        jacobian=t(prob.jacobian, F64),
+        contact_tree=t(prob.contact_tree, I32),
+        phi0=t(prob.phi0, F64),
+        w_eff=t(prob.w_eff, F64),
+        mu=t(prob.mu, F64),
+        stiffness=t(prob.stiffness, F64),
+        tau_d=t(prob.tau_d, F64),
+        v_star=t(prob.v_star, F64),
+        v0=t(prob.v0, F64),
+        dt=t(prob.dt, F64),
+    )

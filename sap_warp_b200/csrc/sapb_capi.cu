@@ -111,6 +111,81 @@ int32_t sapb_contact_solve(const sapb_contact_problem* p, const sapb_solve_optio
   return sapb::contact_solve_launch(p, o, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
+int32_t sapb_blocked_fill_capacity(int32_t trees_per_env, int32_t tree_dofs, int32_t max_contacts,
+                                   int32_t hessian_precision) {
+  return sapb::blocked_fill_capacity(trees_per_env, tree_dofs, max_contacts, hessian_precision == SAPB_FP32);
+}
+
+size_t sapb_blocked_solve_workspace_size(int32_t num_envs, int32_t trees_per_env, int32_t max_contacts) {
+  (void)num_envs;
+  (void)trees_per_env;
+  (void)max_contacts;
+  return 256;  // the persistent kernel's work counter, padded
+}
+
+int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* p, const sapb_solve_options* o,
+                                   const sapb_solve_outputs* out, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+  if (!p || !o || !out || !out->v) {
+    sapb::set_last_error("sapb_blocked_contact_solve: null problem, options or output velocity");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->num_envs < 0 || p->trees_per_env < 1 || p->max_contacts < 0) {
+    sapb::set_last_error("sapb_blocked_contact_solve: bad sizes num_envs=%d trees_per_env=%d max_contacts=%d",
+                         p->num_envs, p->trees_per_env, p->max_contacts);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->trees_per_env > 64 || p->tree_dofs != 6) {
+    sapb::set_last_error("sapb_blocked_contact_solve: supported are <= 64 trees of 6 DOFs (got %d of %d)",
+                         p->trees_per_env, p->tree_dofs);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if (p->max_contacts > 32767) {
+    sapb::set_last_error("sapb_blocked_contact_solve: max_contacts=%d > 32767", p->max_contacts);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if (!p->contact_count || !p->tree_mass || !p->v_star || !p->v0 || !p->dt) {
+    sapb::set_last_error("sapb_blocked_contact_solve: missing required input array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->max_contacts > 0 && (!p->jacobian || !p->contact_tree || !p->phi0 || !p->w_eff || !p->mu ||
+                              !p->stiffness)) {
+    sapb::set_last_error("sapb_blocked_contact_solve: missing contact array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (o->line_search_variant < SAPB_LS_MONOTONE_DECAY || o->line_search_variant > SAPB_LS_EXACT_ROOT) {
+    sapb::set_last_error("sapb_blocked_contact_solve: unknown line search variant %d", o->line_search_variant);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (o->line_search_variant == SAPB_LS_ARMIJO_DECAY && !(o->rho > 0.0 && o->rho < 1.0)) {
+    sapb::set_last_error("sapb_blocked_contact_solve: rho must lie in (0, 1), got %g", o->rho);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (!workspace ||
+      workspace_bytes < sapb_blocked_solve_workspace_size(p->num_envs, p->trees_per_env, p->max_contacts)) {
+    sapb::set_last_error("sapb_blocked_contact_solve: workspace missing or too small");
+    return SAPB_ERR_WORKSPACE_TOO_SMALL;
+  }
+  return sapb::blocked_solve_launch(p, o, out, workspace, static_cast<cudaStream_t>(stream));
+}
+
+int32_t sapb_dense_to_blocked(const sapb_contact_problem* d, int32_t trees_per_env, int32_t tree_dofs,
+                              double* tree_mass, double* jacobian, int32_t* contact_tree, void* stream) {
+  if (!d || !tree_mass || !jacobian || !contact_tree || !d->dynamics_matrix || !d->body_dof_start ||
+      (d->max_contacts > 0 && !d->jacobian)) {
+    sapb::set_last_error("sapb_dense_to_blocked: missing array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (trees_per_env < 1 || tree_dofs < 1 || trees_per_env * tree_dofs != d->dof_per_env || d->num_envs < 0 ||
+      d->max_contacts < 0) {
+    sapb::set_last_error("sapb_dense_to_blocked: %d trees of %d DOFs do not make dof_per_env=%d", trees_per_env,
+                         tree_dofs, d->dof_per_env);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::dense_to_blocked_launch(d, trees_per_env, tree_dofs, tree_mass, jacobian, contact_tree,
+                                       static_cast<cudaStream_t>(stream));
+}
+
 size_t sapb_prepare_workspace_size(const sapb_model_desc* m, int32_t max_contacts) {
   if (!m || max_contacts < 0) return 0;
   return sizeof(int32_t) * ((size_t)m->num_worlds * (size_t)(max_contacts + 1) + 1) + 256;

@@ -442,3 +442,206 @@ def work_order(prob: ContactProblemArrays) -> np.ndarray:
     C = np.minimum(prob.contact_count, prob.max_contacts).astype(np.float64)
     work = n.astype(np.float64) ** 3 / 3.0 + C * n.astype(np.float64) ** 2
     return np.argsort(-work, kind="stable").astype(np.int32)
+
+
+@dataclass
+class BlockedProblemArrays:
+    """Host arrays of one sapb_blocked_problem: worlds of `trees_per_env`
+    trees of `tree_dofs` DOFs, DOF order tree by tree (FP64 unless noted)."""
+
+    num_envs: int
+    trees_per_env: int
+    tree_dofs: int
+    max_contacts: int
+    contact_count: np.ndarray  # int32 (E,)
+    tree_mass: np.ndarray  # (E, T, NB, NB) diagonal blocks of A
+    jacobian: np.ndarray  # (E, C, 3, 2 NB): columns of contact_tree[..., 0], then of [..., 1]
+    contact_tree: np.ndarray  # int32 (E, C, 2), -1: static side
+    phi0: np.ndarray  # (E, C)
+    w_eff: np.ndarray
+    mu: np.ndarray
+    stiffness: np.ndarray
+    tau_d: np.ndarray
+    v_star: np.ndarray  # (E*n,)
+    v0: np.ndarray
+    dt: np.ndarray  # (E,)
+
+    @property
+    def dof_per_env(self) -> int:
+        return self.trees_per_env * self.tree_dofs
+
+    def to_dense(self) -> ContactProblemArrays:
+        """The same problem in the dense layout of sapb_contact_problem (A with
+        its zero blocks between trees, J rows over all n DOFs; body = tree)."""
+        E, T, NB, C = self.num_envs, self.trees_per_env, self.tree_dofs, self.max_contacts
+        n = T * NB
+        A = np.zeros((E, T, NB, T, NB))
+        idx = np.arange(T)
+        A[:, idx, :, idx, :] = self.tree_mass.transpose(1, 0, 2, 3)
+        Jd = np.zeros((E, C, 3, T, NB))
+        for s in range(2):
+            t = self.contact_tree[..., s]
+            e_i, c_i = np.nonzero(t >= 0)
+            Jd[e_i, c_i, :, t[e_i, c_i]] += self.jacobian[e_i, c_i, :, s * NB:(s + 1) * NB]
+        body = lambda s: np.where(self.contact_tree[..., s] >= 0,
+                                  self.contact_tree[..., s] + np.arange(E)[:, None] * T, -1).astype(np.int32)
+        return ContactProblemArrays(
+            num_envs=E, dof_per_env=n, max_contacts=C, bodies_per_env=T,
+            contact_count=self.contact_count.astype(np.int32), dynamics_matrix=A.reshape(E, n, n),
+            jacobian=Jd.reshape(E, C, 3, n), phi0=self.phi0, w_eff=self.w_eff, mu=self.mu,
+            stiffness=self.stiffness, tau_d=self.tau_d, body0=body(0), body1=body(1),
+            body_dof_start=np.tile((np.arange(T) * NB).astype(np.int32), E),
+            body_dof_count=np.full(E * T, NB, dtype=np.int32), v_star=self.v_star, v0=self.v0, dt=self.dt,
+        )
+
+    def subset(self, worlds) -> "BlockedProblemArrays":
+        worlds = np.asarray(worlds, dtype=np.int64)
+        n = self.dof_per_env
+        dof_idx = (worlds[:, None] * n + np.arange(n)[None]).reshape(-1)
+        return BlockedProblemArrays(
+            len(worlds), self.trees_per_env, self.tree_dofs, self.max_contacts,
+            self.contact_count[worlds].copy(), self.tree_mass[worlds].copy(), self.jacobian[worlds].copy(),
+            self.contact_tree[worlds].copy(), self.phi0[worlds].copy(), self.w_eff[worlds].copy(),
+            self.mu[worlds].copy(), self.stiffness[worlds].copy(), self.tau_d[worlds].copy(),
+            self.v_star[dof_idx].copy(), self.v0[dof_idx].copy(), self.dt[worlds].copy(),
+        )
+
+
+def _free_body_inertia(m: float, inertia_world: np.ndarray, r: np.ndarray) -> np.ndarray:
+    """6x6 mass matrix of a free body in SAP coordinates [omega; v_origin]
+    (world frame) with the COM at r from the body origin: [[I_c + m [r]x^T [r]x,
+    m [r]x], [-m [r]x, m I]]."""
+    S = _skew(r)
+    M = np.zeros((6, 6))
+    M[:3, :3] = inertia_world + m * S.T @ S
+    M[:3, 3:] = m * S
+    M[3:, :3] = -m * S
+    M[3:, 3:] = m * np.eye(3)
+    return M
+
+
+def box_stack_problem(
+    num_worlds: int,
+    seed: int = 4,
+    *,
+    boxes: int = 64,
+    max_contacts: int = 448,
+    sites: tuple[int, int] = (12, 20),
+    points_per_pair: tuple[int, int] = (4, 8),
+    side_pairs: tuple[int, int] = (2, 8),
+    size_range=(0.05, 0.2),
+    density_range=(500.0, 2000.0),
+    dt: float = 2.0e-3,
+    phi0_range=(-2.0e-3, 0.0),
+    mu_range=(0.3, 1.0),
+    stiffness: float = 1.0e5,
+    tau_d: float = 0.01,
+    v_std: float = 0.05,
+    gravity: float = -9.81,
+) -> BlockedProblemArrays:
+    """Worlds of `boxes` free boxes (6-DOF trees: n = 6 * boxes) stacked on a
+    grid of sites on the ground.  Sizes U[size_range] m per axis, density
+    U[density_range] kg/m^3, small random yaw; body origin at the centre of
+    the bottom face (so each 6x6 block couples rotation and translation).
+    Contacts: 4-8 points (<= 8 per touching pair) between each box and the
+    box below it or the ground, plus a few side contacts (2-4 points,
+    horizontal normal) between boxes of neighbouring stacks, which couple
+    stacks and create fill in the factor.  v0 ~ N(0, v_std); v* = v0 + dt
+    M^-1 f_gravity."""
+    rng = np.random.default_rng(seed)
+    E, T, NB, C = num_worlds, boxes, 6, max_contacts
+    tm = np.zeros((E, T, NB, NB))
+    jac = np.zeros((E, C, 3, 2 * NB))
+    ct = np.full((E, C, 2), -1, dtype=np.int32)
+    count = np.zeros(E, dtype=np.int32)
+    v0 = rng.normal(scale=v_std, size=(E, T * NB))
+    v_star = v0.copy()
+    g = np.array([0.0, 0.0, gravity])
+    for e in range(E):
+        S = int(rng.integers(sites[0], sites[1] + 1))
+        grid = int(np.ceil(np.sqrt(S)))
+        site_xy = np.stack([(np.arange(S) % grid) * 0.35, (np.arange(S) // grid) * 0.35], -1)
+        site_of = rng.integers(0, S, size=T)
+        dims = rng.uniform(*size_range, size=(T, 3))
+        rho = rng.uniform(*density_range, size=T)
+        mass = rho * dims.prod(-1)
+        yaw = rng.uniform(-0.3, 0.3, size=T)
+        R = _axis_angle(np.array([0.0, 0.0, 1.0]), yaw)
+        origin = np.zeros((T, 3))
+        below = np.full(T, -1)
+        top_z = np.zeros(S)
+        top_box = np.full(S, -1)
+        for k in range(T):
+            s = site_of[k]
+            origin[k] = [site_xy[s, 0] + rng.normal(scale=0.01), site_xy[s, 1] + rng.normal(scale=0.01), top_z[s]]
+            below[k] = top_box[s]
+            top_z[s] += dims[k, 2]
+            top_box[s] = k
+        for k in range(T):
+            a, b, c = dims[k]
+            Ic = mass[k] / 12.0 * np.diag([b * b + c * c, a * a + c * c, a * a + b * b])
+            r = R[k] @ np.array([0.0, 0.0, 0.5 * c])
+            M = _free_body_inertia(mass[k], R[k] @ Ic @ R[k].T, r)
+            tm[e, k] = M
+            f = np.concatenate([np.cross(r, mass[k] * g), mass[k] * g])
+            v_star[e, k * NB:(k + 1) * NB] += dt * np.linalg.solve(M, f)
+        rows = []  # (tree0, tree1, point, normal)
+        for k in range(T):
+            lo = below[k]
+            hx = 0.45 * min(dims[k, 0], dims[lo, 0] if lo >= 0 else 1.0)
+            hy = 0.45 * min(dims[k, 1], dims[lo, 1] if lo >= 0 else 1.0)
+            npts = int(rng.integers(points_per_pair[0], points_per_pair[1] + 1))
+            local = np.array([[hx, hy], [-hx, hy], [-hx, -hy], [hx, -hy]])
+            if npts > 4:
+                local = np.concatenate([local, rng.uniform(-1, 1, size=(npts - 4, 2)) * [hx, hy]])
+            for p2 in local[:npts]:
+                p = origin[k] + R[k] @ np.array([p2[0], p2[1], 0.0])
+                nrm = np.array([0.0, 0.0, 1.0]) + (rng.normal(scale=0.02, size=3) if lo >= 0 else 0.0)
+                rows.append((lo, k, p, nrm / np.linalg.norm(nrm)))
+        for _ in range(int(rng.integers(side_pairs[0], side_pairs[1] + 1))):
+            s0 = int(rng.integers(0, S))
+            nb = [s for s in (s0 + 1, s0 + grid) if s < S and (s != s0 + 1 or (s0 + 1) % grid != 0)]
+            if not nb:
+                continue
+            s1 = nb[int(rng.integers(0, len(nb)))]
+            in0, in1 = np.nonzero(site_of == s0)[0], np.nonzero(site_of == s1)[0]
+            if len(in0) == 0 or len(in1) == 0:
+                continue
+            u, w = int(rng.choice(in0)), int(rng.choice(in1))
+            d = origin[w] - origin[u]
+            d[2] = 0.0
+            nrm = d / max(np.linalg.norm(d), 1e-9)
+            mid = 0.5 * (origin[u] + origin[w])
+            zlo = max(origin[u, 2], origin[w, 2])
+            for _p in range(int(rng.integers(2, 5))):
+                p = mid + np.array([0.0, 0.0, zlo + rng.uniform(0.0, 0.05)]) - np.array([0.0, 0.0, mid[2]])
+                p[:2] += rng.normal(scale=0.02, size=2) * np.array([-nrm[1], nrm[0]])
+                rows.append((u, w, p, nrm))
+        cnt = min(len(rows), C)
+        count[e] = cnt
+        for c, (t0, t1, p, nrm) in enumerate(rows[:cnt]):
+            fr = contact_frames(nrm[None])[0]
+            ct[e, c] = (t0, t1)
+            for s, t in ((0, t0), (1, t1)):
+                if t < 0:
+                    continue
+                Jp = np.concatenate([-_skew(p - origin[t]), np.eye(3)], axis=1)  # v_p = v_o + w x (p - o)
+                jac[e, c, :, s * NB:(s + 1) * NB] = (1.0 if s == 1 else -1.0) * fr @ Jp
+    live = np.arange(C)[None, :] < count[:, None]
+    # diag_delassus weights over the columns of the contact's trees
+    dA = np.einsum("etii->eti", tm)
+    dinv = 1.0 / np.clip(dA, 1e-12, None)  # (E, T, NB)
+    W = np.zeros((E, C, 3, 3))
+    for s in range(2):
+        t = np.maximum(ct[..., s], 0)
+        d = np.take_along_axis(dinv, t[..., None], axis=1) * (ct[..., s] >= 0)[..., None]  # (E, C, NB)
+        Js = jac[..., s * NB:(s + 1) * NB]
+        W += np.einsum("ecrj,ecj,eckj->ecrk", Js, d, Js)
+    w_eff = np.maximum(np.linalg.norm(W, axis=(-2, -1)) / 3.0, 1e-12) * live
+    return BlockedProblemArrays(
+        num_envs=E, trees_per_env=T, tree_dofs=NB, max_contacts=C, contact_count=count,
+        tree_mass=tm, jacobian=jac, contact_tree=ct,
+        phi0=rng.uniform(*phi0_range, size=(E, C)) * live, w_eff=w_eff,
+        mu=rng.uniform(*mu_range, size=(E, C)) * live, stiffness=np.full((E, C), stiffness) * live,
+        tau_d=np.full((E, C), tau_d) * live, v_star=v_star.reshape(-1), v0=v0.reshape(-1), dt=np.full(E, dt),
+    )

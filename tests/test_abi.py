@@ -48,6 +48,11 @@ def test_no_compute_entry_points_without_gpu(lib):
     assert lib.sapb_contact_solve_workspace_size(4096, 35, 32) >= 4
     # argument errors are reported before any CUDA call
     assert lib.sapb_contact_solve(None, None, None, None, 0, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert lib.sapb_blocked_contact_solve(None, None, None, None, 0, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert lib.sapb_blocked_fill_capacity(64, 6, 448, _abi.SAPB_FP64) > 100
+    assert lib.sapb_blocked_fill_capacity(64, 6, 448, _abi.SAPB_FP32) > lib.sapb_blocked_fill_capacity(
+        64, 6, 448, _abi.SAPB_FP64)
+    assert lib.sapb_blocked_fill_capacity(64, 5, 448, _abi.SAPB_FP64) == 0
     assert b"null" in lib.sapb_last_error()
     assert lib.sapb_mlp_param_count() == _abi.SAPB_MLP_PARAM_COUNT
     assert lib.sapb_mlp_packed_count() == _abi.SAPB_MLP_PACKED_COUNT
@@ -70,6 +75,7 @@ def test_struct_layout_matches_header(tmp_path):
         " sizeof(sapb_model_desc), sizeof(sapb_step_inputs), sizeof(sapb_prepare_options),"
         " sizeof(sapb_prepare_outputs)); printf(\"%zu %zu %zu %zu\\n\", sizeof(sapb_warmstart_norm),"
         " sizeof(sapb_mlp_train_buffers), sizeof(sapb_adam_options), offsetof(sapb_contact_problem, gamma0));"
+        " printf(\"%zu %zu\\n\", sizeof(sapb_blocked_problem), offsetof(sapb_blocked_problem, world_order));"
         " return 0;}\n"
     )
     exe = tmp_path / "sizes"
@@ -80,5 +86,6 @@ def test_struct_layout_matches_header(tmp_path):
             ctypes.sizeof(_abi.SolveOutputs), _abi.ContactProblem.dof.offset, _abi.SolveOptions.cubic_init.offset,
             ctypes.sizeof(_abi.ModelDesc), ctypes.sizeof(_abi.StepInputs), ctypes.sizeof(_abi.PrepareOptions),
             ctypes.sizeof(_abi.PrepareOutputs), ctypes.sizeof(_abi.WarmstartNorm),
-            ctypes.sizeof(_abi.MlpTrainBuffers), ctypes.sizeof(_abi.AdamOptions), _abi.ContactProblem.gamma0.offset]
+            ctypes.sizeof(_abi.MlpTrainBuffers), ctypes.sizeof(_abi.AdamOptions), _abi.ContactProblem.gamma0.offset,
+            ctypes.sizeof(_abi.BlockedProblem), _abi.BlockedProblem.world_order.offset]
     assert got == want
