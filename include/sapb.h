@@ -373,8 +373,8 @@ typedef struct sapb_blocked_problem {
 
 /* Off-diagonal factor blocks one world of this shape can hold on chip
  * (0: the shape does not fit or tree_dofs != 6).  A world whose
- * elimination (greedy minimum degree, with fill) needs more gets the
- * per-world status SAPB_WORLD_FACTOR_CAPACITY. */
+ * elimination (rounds of independent minimum-degree trees, with fill) needs
+ * more gets the per-world status SAPB_WORLD_FACTOR_CAPACITY. */
 int32_t sapb_blocked_fill_capacity(int32_t trees_per_env, int32_t tree_dofs, int32_t max_contacts,
                                    int32_t hessian_precision);
 

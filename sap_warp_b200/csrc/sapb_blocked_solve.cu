@@ -13,8 +13,9 @@
 // the blocked LDL^T below computes the same factorization up to rounding.
 //
 // Per world and solve (the contact set is fixed during the Newton loop):
-//  - symbolic phase (one warp): 64-bit adjacency masks of the trees, greedy
-//    minimum-degree elimination order with the fill it creates, the
+//  - symbolic phase (one warp): 64-bit adjacency masks of the trees, an
+//    elimination order by rounds of independent low-degree trees (minimum
+//    degree first, shallow elimination tree) with the fill it creates, the
 //    elimination-tree levels, and the slots of the off-diagonal factor blocks;
 //  - per Newton iteration: G_c per contact, diagonal and off-diagonal blocks
 //    of H from per-tree contact lists (fixed summation order: deterministic),
@@ -73,7 +74,7 @@ enum BInt {
 struct BLayout {
   int T, NB, n, C, cap;
   size_t off_vec, off_con, off_G, off_F, off_Y, off_dinv, off_zd, off_flags, off_mask, off_int, off_list, off_tree,
-      off_slot, total;
+      off_slot, off_JA, total;
 };
 
 __host__ __device__ inline size_t balign(size_t x) { return (x + 15) / 16 * 16; }
@@ -111,6 +112,8 @@ __host__ __device__ inline BLayout make_blayout(int T, int NB, int C, int hsize,
   o = balign(o + 2 * (size_t)L.C);
   L.off_slot = o;  // uint8 row tree / column tree of each off-diagonal slot
   o = balign(o + 2 * (size_t)(cap > 0 ? cap : 1));
+  L.off_JA = o;  // FP32 copy of the J row blocks for the FP32 Hessian assembly
+  o = balign(o + (hsize == 4 ? sizeof(float) * (size_t)L.C * 6 * NB : 0));
   L.off_Y = o;
   o = balign(o + bb * (size_t)(cap > 0 ? cap : 1));
   L.total = o;
@@ -159,6 +162,7 @@ struct BWorld {
   const uint16_t* list;  // per-tree (contact << 1 | side)
   uint8_t* slot_row;
   uint8_t* slot_col;
+  float* JA;  // [C][3][2 NB] FP32 copy of J (FP32 Hessian only)
   __device__ __forceinline__ const double* jrow(int c, int k) const { return J + ((size_t)c * 3 + k) * (2 * NB); }
   // slot of the off-diagonal block (row tree i, column block k); i must lie in colm[k]
   __device__ __forceinline__ int slot(int i, int k) const {
@@ -218,11 +222,31 @@ __device__ void bevaluate(const BWorld<NT, HT, NB>& w, double out4[4]) {
       a_v += aij * vt[b];
     }
     double imp = 0.0;
-    for (int q = w.iw[BI_CSTART + t]; q < w.iw[BI_CSTART + t + 1]; ++q) {
-      const int c = w.list[q] >> 1, side = w.list[q] & 1;
-      const double* j0 = w.jrow(c, 0) + side * NB + a;
-      imp += __ldg(j0) * w.Cn(C_GAMMA + 0)[c] + __ldg(j0 + 2 * NB) * w.Cn(C_GAMMA + 1)[c] +
-             __ldg(j0 + 4 * NB) * w.Cn(C_GAMMA + 2)[c];
+    {
+      const int q0 = w.iw[BI_CSTART + t], q1 = w.iw[BI_CSTART + t + 1];
+      int q = q0;
+      for (; q + 4 <= q1; q += 4) {  // four contacts' loads in flight, sum in list order
+        double jv[4][3];
+        int cc[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int ent = w.list[q + u];
+          cc[u] = ent >> 1;
+          const double* j0 = w.jrow(ent >> 1, 0) + (ent & 1) * NB + a;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) jv[u][k] = __ldg(j0 + k * 2 * NB);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          imp += jv[u][0] * w.Cn(C_GAMMA + 0)[cc[u]] + jv[u][1] * w.Cn(C_GAMMA + 1)[cc[u]] +
+                 jv[u][2] * w.Cn(C_GAMMA + 2)[cc[u]];
+      }
+      for (; q < q1; ++q) {
+        const int c = w.list[q] >> 1, side = w.list[q] & 1;
+        const double* j0 = w.jrow(c, 0) + side * NB + a;
+        imp += __ldg(j0) * w.Cn(C_GAMMA + 0)[c] + __ldg(j0 + 2 * NB) * w.Cn(C_GAMMA + 1)[c] +
+               __ldg(j0 + 4 * NB) * w.Cn(C_GAMMA + 2)[c];
+      }
     }
     const double grad = a_res - imp;
     w.V(V_ARES)[i] = a_res;
@@ -275,21 +299,67 @@ __device__ void line_coefficients(const BWorld<NT, HT, NB>& w, double c4[4]) {
   c4[3] = r[3];
 }
 
-// (J_{c,sa}^T G_c J_{c,sb})[a][b]: the contribution of contact c to the H
-// entry (column a of side sa's tree, column b of side sb's tree).
+// Element idx (row k: k * 2 NB + side * NB + column) of contact c's J row
+// block as HT: from the FP32 copy in shared memory when H is FP32, else the
+// FP64 rows in global memory.
 template <int NT, typename HT, int NB>
-__device__ __forceinline__ HT contact_block_entry(const BWorld<NT, HT, NB>& w, int c, int sa, int a, int sb, int b) {
-  const double* j0 = w.jrow(c, 0);
-  const HT* G = w.G + 9 * c;
-  HT ja[3], jb[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    ja[k] = HT(__ldg(j0 + k * 2 * NB + sa * NB + a));
-    jb[k] = HT(__ldg(j0 + k * 2 * NB + sb * NB + b));
-  }
+__device__ __forceinline__ HT jval(const BWorld<NT, HT, NB>& w, int c, int idx) {
+  if constexpr (sizeof(HT) == 4)
+    return w.JA[c * 6 * NB + idx];
+  else
+    return HT(__ldg(w.J + (size_t)c * 6 * NB + idx));
+}
+
+// (J_{c,sa}^T G_c J_{c,sb})[a][b] from the loaded columns ja = J_{c,sa}[:, a],
+// jb = J_{c,sb}[:, b]: contact c's contribution to one H entry.
+template <typename HT>
+__device__ __forceinline__ HT block_term(const HT* G, const HT (&ja)[3], const HT (&jb)[3]) {
   HT acc = HT(0);
 #pragma unroll
   for (int k = 0; k < 3; ++k) acc += ja[k] * (G[3 * k + 0] * jb[0] + G[3 * k + 1] * jb[1] + G[3 * k + 2] * jb[2]);
+  return acc;
+}
+
+// acc += sum over the list entries e0..e1 (contact << 1 | side s) of the H
+// entry (a of side sa, b of side s) where sa = s (diag) or 1 - s with the
+// other side on tree `other` (off-diagonal).  Four contacts per step with
+// their J loads issued together; the sum runs in list order.
+template <int NT, typename HT, int NB, bool kDiag>
+__device__ __forceinline__ HT sum_block_terms(const BWorld<NT, HT, NB>& w, int e0, int e1, int a, int b, int other,
+                                              HT acc) {
+  int e = e0;
+  for (; e + 4 <= e1; e += 4) {
+    int cc[4];
+    bool use[4];
+    HT ja[4][3], jb[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int ent = w.list[e + u];
+      const int c = ent >> 1, sb = ent & 1, sa = kDiag ? sb : 1 - sb;
+      cc[u] = c;
+      use[u] = kDiag || w.tree[2 * c + sa] == other;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        ja[u][k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sa * NB + a);
+        jb[u][k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sb * NB + b);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (use[u]) acc += block_term<HT>(w.G + 9 * cc[u], ja[u], jb[u]);
+  }
+  for (; e < e1; ++e) {
+    const int ent = w.list[e];
+    const int c = ent >> 1, sb = ent & 1, sa = kDiag ? sb : 1 - sb;
+    if (!kDiag && w.tree[2 * c + sa] != other) continue;
+    HT ja[3], jb[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      ja[k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sa * NB + a);
+      jb[k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sb * NB + b);
+    }
+    acc += block_term<HT>(w.G + 9 * c, ja, jb);
+  }
   return acc;
 }
 
@@ -317,23 +387,16 @@ __device__ void bassemble(const BWorld<NT, HT, NB>& w, double diag_shift) {
       int q = item - t * tri, a = 0;
       while ((a + 1) * (a + 2) / 2 <= q) ++a;
       const int b = q - a * (a + 1) / 2;
-      HT acc = HT(__ldg(w.A + ((size_t)t * NB + a) * NB + b) + (a == b ? diag_shift : 0.0));
-      for (int e = w.iw[BI_CSTART + t]; e < w.iw[BI_CSTART + t + 1]; ++e) {
-        const int c = w.list[e] >> 1, s = w.list[e] & 1;
-        acc += contact_block_entry<NT, HT, NB>(w, c, s, a, s, b);
-      }
-      w.F[(t * NB + a) * NB + b] = acc;
+      const HT acc0 = HT(__ldg(w.A + ((size_t)t * NB + a) * NB + b) + (a == b ? diag_shift : 0.0));
+      w.F[(t * NB + a) * NB + b] =
+          sum_block_terms<NT, HT, NB, true>(w, w.iw[BI_CSTART + t], w.iw[BI_CSTART + t + 1], a, b, -1, acc0);
     } else {
       const int q = item - ndiag;
       const int sl = q / (NB * NB), ab = q - sl * NB * NB;
       const int a = ab / NB, b = ab - a * NB;
       const int i = w.slot_row[sl], p = w.slot_col[sl];
-      HT acc = HT(0);
-      for (int e = w.iw[BI_CSTART + p]; e < w.iw[BI_CSTART + p + 1]; ++e) {
-        const int c = w.list[e] >> 1, s = w.list[e] & 1;
-        if (w.tree[2 * c + (1 - s)] == i) acc += contact_block_entry<NT, HT, NB>(w, c, 1 - s, a, s, b);
-      }
-      w.Y[(size_t)sl * NB * NB + ab] = acc;
+      w.Y[(size_t)sl * NB * NB + ab] =
+          sum_block_terms<NT, HT, NB, false>(w, w.iw[BI_CSTART + p], w.iw[BI_CSTART + p + 1], a, b, i, HT(0));
     }
   }
   __syncthreads();
@@ -512,8 +575,11 @@ __device__ void bsolve(const BWorld<NT, HT, NB>& w) {
   }
 }
 
-// Symbolic phase (warp 0): elimination order by greedy minimum degree on the
-// tree adjacency (ties to the lowest tree index), the fill, the row
+// Symbolic phase (warp 0): elimination order on the tree adjacency in rounds
+// -- each round eliminates a greedy independent set (tree order) of the
+// remaining trees whose degree is at most max(minimum degree, 2), so a chain
+// of trees (a stack of boxes) is halved per round instead of peeled from one
+// end, which keeps the elimination tree shallow -- with the fill, the row
 // structure, elimination-tree levels, slot bases and level lists.  Returns
 // false (to every thread) when the factor needs more off-diagonal blocks than
 // the world's capacity.
@@ -524,21 +590,42 @@ __device__ bool bsymbolic(const BWorld<NT, HT, NB>& w, int cap) {
   if (warp == 0) {
     uint64_t rem = T == 64 ? ~0ull : ((1ull << T) - 1ull);
     uint64_t a0 = lane < T ? w.adj[lane] : 0ull, a1 = lane + 32 < T ? w.adj[lane + 32] : 0ull;
-    for (int s = 0; s < T; ++s) {
-      int key = INT_MAX;
-      if (lane < T && ((rem >> lane) & 1ull)) key = (__popcll(a0 & rem) << 7) | lane;
-      if (lane + 32 < T && ((rem >> (lane + 32)) & 1ull)) key = min(key, (__popcll(a1 & rem) << 7) | (lane + 32));
-      key = __reduce_min_sync(0xffffffffu, key);
-      const int p = key & 127;
-      const uint64_t ap = __shfl_sync(0xffffffffu, p < 32 ? a0 : a1, p & 31);
-      const uint64_t col = ap & rem & ~(1ull << p);
-      if (lane == 0) {
-        w.colm[p] = col;
-        w.iw[BI_ORDER + s] = p;
+    const bool own0 = lane < T, own1 = lane + 32 < T;
+    int s = 0;
+    while (rem) {
+      // degrees of the remaining trees and the round's candidates: degree
+      // <= max(minimum degree, 2)
+      const int d0 = own0 && ((rem >> lane) & 1ull) ? __popcll(a0 & rem) : INT_MAX;
+      const int d1 = own1 && ((rem >> (lane + 32)) & 1ull) ? __popcll(a1 & rem) : INT_MAX;
+      const int dmin = __reduce_min_sync(0xffffffffu, min(d0, d1));
+      const int thr = max(dmin, 2);
+      const uint64_t cand = (uint64_t)__ballot_sync(0xffffffffu, d0 <= thr) |
+                            ((uint64_t)__ballot_sync(0xffffffffu, d1 <= thr) << 32);
+      // greedy independent set of candidates in tree order, eliminated together
+      uint64_t sel = 0ull, m = cand;
+      while (m) {
+        const int p = __ffsll((long long)m) - 1;
+        m &= m - 1;
+        const uint64_t ap = __shfl_sync(0xffffffffu, p < 32 ? a0 : a1, p & 31);
+        if (!(ap & sel)) sel |= 1ull << p;
       }
-      if (lane < T && ((col >> lane) & 1ull)) a0 |= col & ~(1ull << lane);
-      if (lane + 32 < T && ((col >> (lane + 32)) & 1ull)) a1 |= col & ~(1ull << (lane + 32));
-      rem &= ~(1ull << p);
+      // their column structures (the selected trees are pairwise non-adjacent,
+      // so one's fill leaves another's adjacency unchanged), then the fill
+      m = sel;
+      while (m) {
+        const int p = __ffsll((long long)m) - 1;
+        m &= m - 1;
+        const uint64_t ap = __shfl_sync(0xffffffffu, p < 32 ? a0 : a1, p & 31);
+        const uint64_t col = ap & rem & ~(1ull << p);
+        if (lane == 0) {
+          w.colm[p] = col;
+          w.iw[BI_ORDER + s] = p;
+        }
+        ++s;
+        if (own0 && ((col >> lane) & 1ull)) a0 |= col & ~(1ull << lane);
+        if (own1 && ((col >> (lane + 32)) & 1ull)) a1 |= col & ~(1ull << (lane + 32));
+      }
+      rem &= ~sel;
     }
     __syncwarp();
     for (int j = lane; j < T; j += 32) {
@@ -642,6 +729,7 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
     w.list = reinterpret_cast<const uint16_t*>(smem + L.off_list);
     w.slot_row = reinterpret_cast<uint8_t*>(smem + L.off_slot);
     w.slot_col = w.slot_row + (L.cap > 0 ? L.cap : 1);
+    w.JA = reinterpret_cast<float*>(smem + L.off_JA);
     int count = P.p.contact_count[e];
     if (count > C) count = C;
     if (count < 0) count = 0;
@@ -671,6 +759,9 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
       if (t1 < 0 || t1 >= T || t1 == t0) t1 = -1;
       tree_w[2 * c] = (int8_t)t0;
       tree_w[2 * c + 1] = (int8_t)t1;
+    }
+    if constexpr (sizeof(HT) == 4) {
+      for (int k = tid; k < count * 6 * NB; k += NT) w.JA[k] = (float)__ldg(w.J + k);
     }
     for (int i = tid; i < n; i += NT) {
       w.V(V_VSTAR)[i] = P.p.v_star[base + i];
