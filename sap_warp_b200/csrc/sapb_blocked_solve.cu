@@ -19,8 +19,9 @@
 //    elimination-tree levels, and the slots of the off-diagonal factor blocks;
 //  - per Newton iteration: G_c per contact, diagonal and off-diagonal blocks
 //    of H from per-tree contact lists (fixed summation order: deterministic),
-//    left-looking block LDL^T level by level (one warp per column block, the
-//    blocks of one level independent), forward / backward block solves.
+//    left-looking block LDL^T level by level (the blocks of one level are
+//    independent; each level runs as block-wide phases over flat work
+//    lists), forward / backward block solves the same way.
 // Precision as in the dense kernel: gradient, costs, line search, update and
 // convergence test in FP64; H and its factor in HT (double or float).
 #include <cuda_runtime.h>
@@ -67,7 +68,9 @@ enum BInt {
   BI_LNODES = BI_LSTART + kBMaxTrees + 1,  // [64] column blocks by level, elimination order within
   BI_CSTART = BI_LNODES + kBMaxTrees,   // [65] tree -> first entry of its contact list
   BI_CNT = BI_CSTART + kBMaxTrees + 1,  // [64] contacts per tree / level cursor
-  BI_MISC = BI_CNT + kBMaxTrees,        // [4] slots used, level count, bad pivot
+  BI_UOFF = BI_CNT + kBMaxTrees,        // [65] by BI_LNODES position: first update item of a block
+  BI_ROFF = BI_UOFF + kBMaxTrees + 1,   // [65] by BI_LNODES position: first off-diagonal row of a block
+  BI_MISC = BI_ROFF + kBMaxTrees + 1,   // [4] slots used, level count, bad pivot
   BI_END = BI_MISC + 4
 };
 
@@ -310,57 +313,33 @@ __device__ __forceinline__ HT jval(const BWorld<NT, HT, NB>& w, int c, int idx) 
     return HT(__ldg(w.J + (size_t)c * 6 * NB + idx));
 }
 
-// (J_{c,sa}^T G_c J_{c,sb})[a][b] from the loaded columns ja = J_{c,sa}[:, a],
-// jb = J_{c,sb}[:, b]: contact c's contribution to one H entry.
-template <typename HT>
-__device__ __forceinline__ HT block_term(const HT* G, const HT (&ja)[3], const HT (&jb)[3]) {
-  HT acc = HT(0);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) acc += ja[k] * (G[3 * k + 0] * jb[0] + G[3 * k + 1] * jb[1] + G[3 * k + 2] * jb[2]);
-  return acc;
-}
-
-// acc += sum over the list entries e0..e1 (contact << 1 | side s) of the H
-// entry (a of side sa, b of side s) where sa = s (diag) or 1 - s with the
-// other side on tree `other` (off-diagonal).  Four contacts per step with
-// their J loads issued together; the sum runs in list order.
+// Row a of one H block: acc[b] += sum over the list entries e0..e1
+// (contact << 1 | side sb) of (J_{c,sa}[:, a])^T G_c J_{c,sb}[:, b], with
+// sa = sb (a tree's diagonal block) or sa = 1 - sb restricted to contacts
+// whose side sa lies on tree `other` (an off-diagonal block).  y = ja^T G is
+// formed once per contact and shared by the NB entries of the row; the sum
+// runs in list order.
 template <int NT, typename HT, int NB, bool kDiag>
-__device__ __forceinline__ HT sum_block_terms(const BWorld<NT, HT, NB>& w, int e0, int e1, int a, int b, int other,
-                                              HT acc) {
-  int e = e0;
-  for (; e + 4 <= e1; e += 4) {
-    int cc[4];
-    bool use[4];
-    HT ja[4][3], jb[4][3];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int ent = w.list[e + u];
-      const int c = ent >> 1, sb = ent & 1, sa = kDiag ? sb : 1 - sb;
-      cc[u] = c;
-      use[u] = kDiag || w.tree[2 * c + sa] == other;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        ja[u][k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sa * NB + a);
-        jb[u][k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sb * NB + b);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (use[u]) acc += block_term<HT>(w.G + 9 * cc[u], ja[u], jb[u]);
-  }
-  for (; e < e1; ++e) {
+__device__ __forceinline__ void sum_block_row(const BWorld<NT, HT, NB>& w, int e0, int e1, int a, int other,
+                                              HT (&acc)[NB]) {
+  for (int e = e0; e < e1; ++e) {
     const int ent = w.list[e];
     const int c = ent >> 1, sb = ent & 1, sa = kDiag ? sb : 1 - sb;
     if (!kDiag && w.tree[2 * c + sa] != other) continue;
-    HT ja[3], jb[3];
+    const HT* G = w.G + 9 * c;
+    HT ja[3], jb[3][NB];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       ja[k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sa * NB + a);
-      jb[k] = jval<NT, HT, NB>(w, c, k * 2 * NB + sb * NB + b);
+#pragma unroll
+      for (int b = 0; b < NB; ++b) jb[k][b] = jval<NT, HT, NB>(w, c, k * 2 * NB + sb * NB + b);
     }
-    acc += block_term<HT>(w.G + 9 * c, ja, jb);
+    HT y[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y[k] = ja[0] * G[k] + ja[1] * G[3 + k] + ja[2] * G[6 + k];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) acc[b] += y[0] * jb[0][b] + y[1] * jb[1][b] + y[2] * jb[2][b];
   }
-  return acc;
 }
 
 // H = A + J^T G J + shift I in the block layout: F (tree blocks, lower
@@ -377,200 +356,252 @@ __device__ void bassemble(const BWorld<NT, HT, NB>& w, double diag_shift) {
     for (int k = 0; k < 9; ++k) w.G[9 * c + k] = HT(G[k]);
   }
   __syncthreads();
-  constexpr int tri = NB * (NB + 1) / 2;
-  const int ndiag = w.T * tri;
+  // one item per block row: the NB rows of each tree's diagonal block, then
+  // the NB rows of each off-diagonal slot
+  const int ndiag = w.T * NB;
   const int nslots = w.iw[BI_MISC + 0];
-  const int total = ndiag + nslots * NB * NB;
+  const int total = ndiag + nslots * NB;
   for (int item = tid; item < total; item += NT) {
+    HT acc[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) acc[b] = HT(0);
     if (item < ndiag) {
-      const int t = item / tri;
-      int q = item - t * tri, a = 0;
-      while ((a + 1) * (a + 2) / 2 <= q) ++a;
-      const int b = q - a * (a + 1) / 2;
-      const HT acc0 = HT(__ldg(w.A + ((size_t)t * NB + a) * NB + b) + (a == b ? diag_shift : 0.0));
-      w.F[(t * NB + a) * NB + b] =
-          sum_block_terms<NT, HT, NB, true>(w, w.iw[BI_CSTART + t], w.iw[BI_CSTART + t + 1], a, b, -1, acc0);
+      const int t = item / NB, a = item - t * NB;
+      sum_block_row<NT, HT, NB, true>(w, w.iw[BI_CSTART + t], w.iw[BI_CSTART + t + 1], a, -1, acc);
+      const double* Ar = w.A + ((size_t)t * NB + a) * NB;
+      HT* Fr = w.F + (t * NB + a) * NB;
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+        if (b <= a) Fr[b] = HT(__ldg(Ar + b) + (a == b ? diag_shift : 0.0)) + acc[b];
     } else {
       const int q = item - ndiag;
-      const int sl = q / (NB * NB), ab = q - sl * NB * NB;
-      const int a = ab / NB, b = ab - a * NB;
+      const int sl = q / NB, a = q - sl * NB;
       const int i = w.slot_row[sl], p = w.slot_col[sl];
-      w.Y[(size_t)sl * NB * NB + ab] =
-          sum_block_terms<NT, HT, NB, false>(w, w.iw[BI_CSTART + p], w.iw[BI_CSTART + p + 1], a, b, i, HT(0));
+      sum_block_row<NT, HT, NB, false>(w, w.iw[BI_CSTART + p], w.iw[BI_CSTART + p + 1], a, i, acc);
+      HT* Yr = w.Y + ((size_t)sl * NB + a) * NB;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) Yr[b] = acc[b];
     }
   }
   __syncthreads();
 }
 
-// Left-looking block LDL^T, one elimination-tree level at a time; a warp per
-// column block j: subtract the contributions of the blocks k below it
-// (rowm[j]), factor the NB x NB diagonal block, then Y_ij <- M_ij L_jj^-T for
-// the blocks i of its column (colm[j]).
+// Position idx in [b0, b1) of BI_LNODES whose work range [off[idx],
+// off[idx + 1]) holds flat item u (off = BI_UOFF or BI_ROFF; blocks with no
+// work have empty ranges and are never returned).
+__device__ __forceinline__ int find_block(const int* off, int b0, int b1, int u) {
+  int lo = b0, hi = b1 - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= u) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The m-th tree (in increasing index) of the mask cj.
+__device__ __forceinline__ int nth_tree(uint64_t cj, int m) {
+  for (int z = 0; z < m; ++z) cj &= cj - 1;
+  return __ffsll((long long)cj) - 1;
+}
+
+// Left-looking block LDL^T, one elimination-tree level at a time.  Each level
+// is three block-wide phases over flat work lists (no per-block loops that
+// diverge within a warp): (A) every entry of the level's column blocks j
+// minus the contributions of the finished blocks k below them (rowm[j]);
+// (B) a thread per block factors its NB x NB diagonal block in registers;
+// (C) every row of the off-diagonal blocks, Y_ij <- M_ij L_jj^-T.
 template <int NT, typename HT, int NB>
 __device__ void bfactor(const BWorld<NT, HT, NB>& w) {
-  constexpr int NW = NT / 32;
   constexpr int tri = NB * (NB + 1) / 2;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tid = threadIdx.x;
   const int nlev = w.iw[BI_MISC + 1];
+  const int* uoff = w.iw + BI_UOFF;
+  const int* roff = w.iw + BI_ROFF;
   for (int l = 0; l < nlev; ++l) {
     const int b0 = w.iw[BI_LSTART + l], b1 = w.iw[BI_LSTART + l + 1];
-    for (int idx = b0 + warp; idx < b1; idx += NW) {
+    // (A) updates
+    const int u0 = uoff[b0], u1 = uoff[b1];
+    for (int u = u0 + tid; u < u1; u += NT) {
+      const int idx = find_block(uoff, b0, b1, u);
       const int j = w.iw[BI_LNODES + idx];
-      const uint64_t rj = w.rowm[j], cj = w.colm[j];
-      const int ncol = __popcll(cj);
-      // (1) updates from the finished blocks k < j
-      if (rj) {
-        for (int item = lane; item < tri + ncol * NB * NB; item += 32) {
-          if (item < tri) {
-            int a = 0;
-            while ((a + 1) * (a + 2) / 2 <= item) ++a;
-            const int b = item - a * (a + 1) / 2;
-            HT s = HT(0);
-            uint64_t r = rj;
-            while (r) {
-              const int k = __ffsll((long long)r) - 1;
-              r &= r - 1;
-              const HT* Yjk = w.Y + (size_t)w.slot(j, k) * NB * NB;
-              const HT* dk = w.dinv + k * NB;
+      const uint64_t rj = w.rowm[j];
+      const int item = u - uoff[idx];
+      if (item < tri) {
+        int a = 0;
+        while ((a + 1) * (a + 2) / 2 <= item) ++a;
+        const int b = item - a * (a + 1) / 2;
+        HT sum = HT(0);
+        uint64_t r = rj;
+        while (r) {
+          const int k = __ffsll((long long)r) - 1;
+          r &= r - 1;
+          const HT* Yjk = w.Y + (size_t)w.slot(j, k) * NB * NB;
+          const HT* dk = w.dinv + k * NB;
 #pragma unroll
-              for (int e = 0; e < NB; ++e) s += Yjk[a * NB + e] * dk[e] * Yjk[b * NB + e];
-            }
-            w.F[(j * NB + a) * NB + b] -= s;
-          } else {
-            const int q = item - tri;
-            const int m = q / (NB * NB), ab = q - m * NB * NB;
-            const int a = ab / NB, b = ab - a * NB;
-            // the m-th tree of cj
-            uint64_t cc = cj;
-            for (int z = 0; z < m; ++z) cc &= cc - 1;
-            const int i = __ffsll((long long)cc) - 1;
-            HT s = HT(0);
-            uint64_t r = rj;
-            while (r) {
-              const int k = __ffsll((long long)r) - 1;
-              r &= r - 1;
-              if (!((w.colm[k] >> i) & 1ull)) continue;
-              const HT* Yik = w.Y + (size_t)w.slot(i, k) * NB * NB;
-              const HT* Yjk = w.Y + (size_t)w.slot(j, k) * NB * NB;
-              const HT* dk = w.dinv + k * NB;
-#pragma unroll
-              for (int e = 0; e < NB; ++e) s += Yik[a * NB + e] * dk[e] * Yjk[b * NB + e];
-            }
-            w.Y[(size_t)w.slot(i, j) * NB * NB + ab] -= s;
-          }
+          for (int e = 0; e < NB; ++e) sum += Yjk[a * NB + e] * dk[e] * Yjk[b * NB + e];
         }
-        __syncwarp();
-      }
-      // (2) the diagonal block: column by column, lane a owns row a
-      HT* Fj = w.F + j * NB * NB;
-      for (int b = 0; b < NB; ++b) {
-        HT val = HT(0);
-        if (lane >= b && lane < NB) {
-          val = Fj[lane * NB + b];
-          for (int e = 0; e < b; ++e) val -= Fj[lane * NB + e] * Fj[e * NB + e] * Fj[b * NB + e];
-        }
-        const HT d = __shfl_sync(0xffffffffu, val, b);
-        const HT rinv = fast_recip(d);
-        __syncwarp();
-        if (lane == b) {
-          Fj[b * NB + b] = d;
-          w.dinv[j * NB + b] = rinv;
-          if (!(d > HT(0)) || !isfinite(double(d))) w.iw[BI_MISC + 2] = 1;
-        } else if (lane > b && lane < NB) {
-          Fj[lane * NB + b] = val * rinv;
-        }
-        __syncwarp();
-      }
-      // (3) Y_ij <- M_ij L_jj^-T, one row per lane
-      for (int row = lane; row < ncol * NB; row += 32) {
-        const int m = row / NB, a = row - m * NB;
-        uint64_t cc = cj;
-        for (int z = 0; z < m; ++z) cc &= cc - 1;
-        const int i = __ffsll((long long)cc) - 1;
-        HT* y = w.Y + (size_t)w.slot(i, j) * NB * NB + a * NB;
-        HT yv[NB];
+        w.F[(j * NB + a) * NB + b] -= sum;
+      } else {
+        const int q = item - tri;
+        const int m = q / (NB * NB), ab = q - m * NB * NB;
+        const int a = ab / NB, b = ab - a * NB;
+        const int i = nth_tree(w.colm[j], m);
+        HT sum = HT(0);
+        uint64_t r = rj;
+        while (r) {
+          const int k = __ffsll((long long)r) - 1;
+          r &= r - 1;
+          if (!((w.colm[k] >> i) & 1ull)) continue;
+          const HT* Yik = w.Y + (size_t)w.slot(i, k) * NB * NB;
+          const HT* Yjk = w.Y + (size_t)w.slot(j, k) * NB * NB;
+          const HT* dk = w.dinv + k * NB;
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
-          HT s = y[b];
-#pragma unroll
-          for (int e = 0; e < b; ++e) s -= yv[e] * Fj[b * NB + e];
-          yv[b] = s;
+          for (int e = 0; e < NB; ++e) sum += Yik[a * NB + e] * dk[e] * Yjk[b * NB + e];
         }
-#pragma unroll
-        for (int b = 0; b < NB; ++b) y[b] = yv[b];
+        w.Y[(size_t)w.slot(i, j) * NB * NB + ab] -= sum;
       }
     }
+    if (u1 > u0) __syncthreads();
+    // (B) diagonal blocks, a thread per block, in registers
+    for (int idx = b0 + tid; idx < b1; idx += NT) {
+      const int j = w.iw[BI_LNODES + idx];
+      HT* Fj = w.F + j * NB * NB;
+      HT Lr[NB][NB], Dr[NB], Rr[NB];
+#pragma unroll
+      for (int a = 0; a < NB; ++a)
+#pragma unroll
+        for (int b = 0; b <= a; ++b) Lr[a][b] = Fj[a * NB + b];
+      bool ok = true;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        HT d = Lr[b][b];
+#pragma unroll
+        for (int e = 0; e < b; ++e) d -= Lr[b][e] * Lr[b][e] * Dr[e];
+        Dr[b] = d;
+        Rr[b] = fast_recip(d);
+        ok = ok && d > HT(0) && isfinite(double(d));
+#pragma unroll
+        for (int a = b + 1; a < NB; ++a) {
+          HT v = Lr[a][b];
+#pragma unroll
+          for (int e = 0; e < b; ++e) v -= Lr[a][e] * Lr[b][e] * Dr[e];
+          Lr[a][b] = v * Rr[b];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < NB; ++a) {
+#pragma unroll
+        for (int b = 0; b < a; ++b) Fj[a * NB + b] = Lr[a][b];
+        Fj[a * NB + a] = Dr[a];
+        w.dinv[j * NB + a] = Rr[a];
+      }
+      if (!ok) w.iw[BI_MISC + 2] = 1;
+    }
     __syncthreads();
+    // (C) off-diagonal rows
+    const int r0 = roff[b0], r1 = roff[b1];
+    for (int u = r0 + tid; u < r1; u += NT) {
+      const int idx = find_block(roff, b0, b1, u);
+      const int j = w.iw[BI_LNODES + idx];
+      const int row = u - roff[idx];
+      const int m = row / NB, a = row - m * NB;
+      const int i = nth_tree(w.colm[j], m);
+      const HT* Fj = w.F + j * NB * NB;
+      HT* y = w.Y + (size_t)w.slot(i, j) * NB * NB + a * NB;
+      HT yv[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        HT sum = y[b];
+#pragma unroll
+        for (int e = 0; e < b; ++e) sum -= yv[e] * Fj[b * NB + e];
+        yv[b] = sum;
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) y[b] = yv[b];
+    }
+    if (r1 > r0) __syncthreads();
   }
 }
 
 // dv = -H^-1 grad with the block factor: forward L z = b (levels up), then
-// L^T x = D^-1 z (levels down); a warp per column block, lane a owns row a.
-// A bad pivot makes dv NaN (as in the dense kernel).
+// L^T x = D^-1 z (levels down).  Per level: a thread per block row gathers
+// the off-diagonal products, then a thread per block solves with its
+// diagonal block.  A bad pivot makes dv NaN (as in the dense kernel).
 template <int NT, typename HT, int NB>
 __device__ void bsolve(const BWorld<NT, HT, NB>& w) {
-  constexpr int NW = NT / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tid = threadIdx.x;
   const int nlev = w.iw[BI_MISC + 1];
   double* dv = w.V(V_DV);
   const double* grad = w.V(V_GRAD);
   for (int l = 0; l < nlev; ++l) {
     const int b0 = w.iw[BI_LSTART + l], b1 = w.iw[BI_LSTART + l + 1];
-    for (int idx = b0 + warp; idx < b1; idx += NW) {
-      const int j = w.iw[BI_LNODES + idx];
-      HT z = HT(0);
-      if (lane < NB) {
-        z = HT(-grad[j * NB + lane]);
-        uint64_t r = w.rowm[j];
-        while (r) {
-          const int k = __ffsll((long long)r) - 1;
-          r &= r - 1;
-          const HT* Yjk = w.Y + (size_t)w.slot(j, k) * NB * NB + lane * NB;
-          const HT* zk = w.zd + k * NB;
+    for (int u = tid; u < (b1 - b0) * NB; u += NT) {
+      const int j = w.iw[BI_LNODES + b0 + u / NB], a = u % NB;
+      HT z = HT(-grad[j * NB + a]);
+      uint64_t r = w.rowm[j];
+      while (r) {
+        const int k = __ffsll((long long)r) - 1;
+        r &= r - 1;
+        const HT* Yjk = w.Y + (size_t)w.slot(j, k) * NB * NB + a * NB;
+        const HT* zk = w.zd + k * NB;
 #pragma unroll
-          for (int e = 0; e < NB; ++e) z -= Yjk[e] * zk[e];
-        }
+        for (int e = 0; e < NB; ++e) z -= Yjk[e] * zk[e];
       }
+      w.zd[j * NB + a] = z;  // the block's own zd is not read in this level
+    }
+    __syncthreads();
+    for (int idx = b0 + tid; idx < b1; idx += NT) {
+      const int j = w.iw[BI_LNODES + idx];
       const HT* Fj = w.F + j * NB * NB;
+      HT z[NB];
 #pragma unroll
       for (int a = 0; a < NB; ++a) {
-        const HT za = __shfl_sync(0xffffffffu, z, a);
-        if (lane > a && lane < NB) z -= Fj[lane * NB + a] * za;
+        HT v = w.zd[j * NB + a];
+#pragma unroll
+        for (int e = 0; e < a; ++e) v -= Fj[a * NB + e] * z[e];
+        z[a] = v;
       }
-      if (lane < NB) w.zd[j * NB + lane] = z * w.dinv[j * NB + lane];
+#pragma unroll
+      for (int a = 0; a < NB; ++a) w.zd[j * NB + a] = z[a] * w.dinv[j * NB + a];
     }
     __syncthreads();
   }
   for (int l = nlev - 1; l >= 0; --l) {
     const int b0 = w.iw[BI_LSTART + l], b1 = w.iw[BI_LSTART + l + 1];
-    for (int idx = b0 + warp; idx < b1; idx += NW) {
-      const int j = w.iw[BI_LNODES + idx];
-      HT t = HT(0);
-      if (lane < NB) {
-        HT s = HT(0);
-        uint64_t cc = w.colm[j];
-        while (cc) {
-          const int i = __ffsll((long long)cc) - 1;
-          cc &= cc - 1;
-          const HT* Yij = w.Y + (size_t)w.slot(i, j) * NB * NB + lane;
+    for (int u = tid; u < (b1 - b0) * NB; u += NT) {
+      const int j = w.iw[BI_LNODES + b0 + u / NB], b = u % NB;
+      HT sum = HT(0);
+      uint64_t cc = w.colm[j];
+      while (cc) {
+        const int i = __ffsll((long long)cc) - 1;
+        cc &= cc - 1;
+        const HT* Yij = w.Y + (size_t)w.slot(i, j) * NB * NB + b;
 #pragma unroll
-          for (int a = 0; a < NB; ++a) s += Yij[a * NB] * HT(dv[i * NB + a]);
-        }
-        t = w.zd[j * NB + lane] - w.dinv[j * NB + lane] * s;
+        for (int a = 0; a < NB; ++a) sum += Yij[a * NB] * HT(dv[i * NB + a]);
       }
+      dv[j * NB + b] = double(w.zd[j * NB + b] - w.dinv[j * NB + b] * sum);
+    }
+    __syncthreads();
+    for (int idx = b0 + tid; idx < b1; idx += NT) {
+      const int j = w.iw[BI_LNODES + idx];
       const HT* Fj = w.F + j * NB * NB;
+      HT x[NB];
 #pragma unroll
       for (int a = NB - 1; a >= 0; --a) {
-        const HT xa = __shfl_sync(0xffffffffu, t, a);
-        if (lane < a) t -= Fj[a * NB + lane] * xa;
+        HT v = HT(dv[j * NB + a]);
+#pragma unroll
+        for (int c = a + 1; c < NB; ++c) v -= Fj[c * NB + a] * x[c];
+        x[a] = v;
       }
-      if (lane < NB) dv[j * NB + lane] = double(t);
+#pragma unroll
+      for (int a = 0; a < NB; ++a) dv[j * NB + a] = double(x[a]);
     }
     __syncthreads();
   }
   if (w.iw[BI_MISC + 2]) {
     const double nanv = __longlong_as_double(0x7ff8000000000000ULL);
-    for (int i = threadIdx.x; i < w.n; i += NT) dv[i] = nanv;
+    for (int i = tid; i < w.n; i += NT) dv[i] = nanv;
     __syncthreads();
   }
 }
@@ -663,6 +694,19 @@ __device__ bool bsymbolic(const BWorld<NT, HT, NB>& w, int cap) {
         const int p = w.iw[BI_ORDER + s];
         w.iw[BI_LNODES + w.iw[BI_CNT + w.iw[BI_LVL + p]]++] = p;
       }
+      // flat work offsets of the factorization's update and row phases
+      constexpr int tri = NB * (NB + 1) / 2;
+      int u = 0, r = 0;
+      for (int idx = 0; idx < T; ++idx) {
+        const int p = w.iw[BI_LNODES + idx];
+        const int nc = __popcll(w.colm[p]);
+        w.iw[BI_UOFF + idx] = u;
+        w.iw[BI_ROFF + idx] = r;
+        if (w.rowm[p]) u += tri + nc * NB * NB;
+        r += nc * NB;
+      }
+      w.iw[BI_UOFF + T] = u;
+      w.iw[BI_ROFF + T] = r;
     }
   }
   __syncthreads();
