@@ -251,7 +251,8 @@ def main():
     import torch
 
     from sap_warp_b200 import models, scenes
-    from sap_warp_b200._solve import ContactSolveBuffers, contact_solve, make_options, problem_to_device
+    from sap_warp_b200._solve import (ContactSolveBuffers, blocked_contact_solve, blocked_problem_to_device,
+                                      contact_solve, make_options, problem_to_device)
     from sap_warp_b200.runtime import SapState
     from sap_warp_b200.solver import SolverSAP
     from sap_warp_b200.warmstart import DEFAULT_WEIGHTS, LearnedWarmStart
@@ -433,6 +434,29 @@ def main():
         uneven[label] = {"value": mix.num_envs * world_size / (ms * 1e-3), "ms_per_solve": ms,
                          "all_converged": bool(mbuf.converged.all())}
 
+    # ---- worlds of 64 free boxes (384 DOFs, ~400 contacts): tree-blocked solve ----
+    boxes = scenes.box_stack_problem(512, seed=4 + 1000 * rank)
+    tb = blocked_problem_to_device(boxes, dev)
+    bbuf = ContactSolveBuffers(boxes.num_envs, boxes.dof_per_env, boxes.max_contacts, dev)
+    box_line = {"worlds": boxes.num_envs, "trees": "64 free boxes (6 DOF each, n = 384)",
+                "contacts": f"mean {float(boxes.contact_count.mean()):.0f} per world (stacks + side contacts)"}
+    for label, prec in (("fp64", "fp64"), ("fp32", "fp32")):
+        opts = make_options("armijo_decay", hessian_precision=prec, linear_solve_precision=prec)
+        for _ in range(max(args.warmup, 1)):
+            blocked_contact_solve(buffers=bbuf, options=opts, trees_per_env=64, **tb)
+        barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k_box = max(1, min(args.steps, 5))
+        a0.record(stream)
+        for _ in range(k_box):
+            blocked_contact_solve(buffers=bbuf, options=opts, trees_per_env=64, **tb)
+        a1.record(stream)
+        barrier()
+        ms = max_over_ranks(a0.elapsed_time(a1) / k_box)
+        box_line[label] = {"value": boxes.num_envs * world_size / (ms * 1e-3), "ms_per_solve": ms,
+                           "mean_newton_iterations": float(bbuf.newton_iterations.double().mean()),
+                           "all_converged": bool(bbuf.converged.all())}
+
     total = W * world_size
     value = total / (fast["ms"] * 1e-3)
     peaks = {}
@@ -473,6 +497,7 @@ def main():
                                    "mean_newton_iterations": prev["iters"], "stages_ms": prev["stages"]},
         "stage2_solve_only": snap,
         "uneven_batch_solve_only": uneven,
+        "box_worlds_solve_only": box_line,
         "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "kernel": "contact_solve_kernel", "achieved": achieved, "peak": hbm_peak,

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 3
+#define SAPB_ABI_VERSION 4
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -248,6 +248,14 @@ typedef struct sapb_prepare_options {
   double fallback_mu;
   double fallback_stiffness;
   double fallback_tau_d;
+  /* Nonzero: tree-blocked outputs for worlds whose every body is a free body
+   * (a free joint to the world: one tree of 6 DOFs per body, DOF order body
+   * by body).  tree_mass and contact_tree are written, jacobian is
+   * [W][C][3][12] in the layout of sapb_blocked_problem, and
+   * dynamics_matrix / dynamics_factor are not written (may be NULL).  No
+   * counterpart in the reference, which keeps such worlds dense
+   * (sim/contact_jacobian.py:110-150, 404-562).  At most 64 bodies. */
+  int32_t tree_blocked;
 } sapb_prepare_options;
 
 /* Outputs: SapFreeMotionResult (sim/free_motion.py:63-68) and the
@@ -274,6 +282,8 @@ typedef struct sapb_prepare_outputs {
   double* dynamics_factor;          /* [W][n][n] LDL^T of A (below the diagonal L_ik d_k, on it d_k;
                                        above it unspecified), or NULL */
   double* vc_star;                  /* [W][C][3] free-motion contact velocities J_c v*, or NULL */
+  double* tree_mass;                /* [W][B][6][6] diagonal blocks of A (tree_blocked only) */
+  int32_t* contact_tree;            /* [W][C][2] tree of each contact side, -1 static (tree_blocked only) */
 } sapb_prepare_outputs;
 
 /* Device workspace bytes of sapb_free_motion_contacts. */
@@ -287,7 +297,8 @@ size_t sapb_prepare_workspace_size(const sapb_model_desc* model, int32_t max_con
  * claimed atomically like the reference's scatter (:470), then ordered by
  * flat contact index within each world, so an untruncated world's slot order
  * is the flat buffer's.  At most 64 bodies and 128 DOFs per world
- * (SAPB_ERR_UNSUPPORTED otherwise). */
+ * (SAPB_ERR_UNSUPPORTED otherwise); with opts->tree_blocked, worlds of up
+ * to 64 free bodies (384 DOFs) in the tree-blocked layout. */
 int32_t sapb_free_motion_contacts(const sapb_model_desc* model, const sapb_step_inputs* in,
                                   const sapb_prepare_options* opts, const sapb_prepare_outputs* out,
                                   void* workspace, size_t workspace_bytes, void* stream);

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 3
+SAPB_ABI_VERSION = 4
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -226,6 +226,7 @@ class PrepareOptions(C.Structure):
         ("fallback_mu", C.c_double),
         ("fallback_stiffness", C.c_double),
         ("fallback_tau_d", C.c_double),
+        ("tree_blocked", C.c_int32),
     ]
 
 
@@ -249,6 +250,8 @@ class PrepareOutputs(C.Structure):
         ("body_q", _p),
         ("dynamics_factor", _p),
         ("vc_star", _p),
+        ("tree_mass", _p),
+        ("contact_tree", _p),
     ]
 
 

@@ -211,7 +211,9 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inpu
                                   void* workspace, size_t workspace_bytes, void* stream) {
   const int32_t st = check_model(m, "sapb_free_motion_contacts");
   if (st != SAPB_OK) return st;
-  if (!in || !o || !out || !in->joint_q || !in->joint_qd || !in->dt || !out->v_star || !out->dynamics_matrix) {
+  const bool blk = o && o->tree_blocked;
+  if (!in || !o || !out || !in->joint_q || !in->joint_qd || !in->dt || !out->v_star ||
+      (blk ? (!out->tree_mass || !out->contact_tree) : !out->dynamics_matrix)) {
     sapb::set_last_error("sapb_free_motion_contacts: missing input or output array");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
@@ -230,12 +232,19 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inpu
     sapb::set_last_error("sapb_free_motion_contacts: missing contact output array");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
-  if (m->bodies_per_world > 64 || m->dofs_per_world > 128) {
+  if (blk && (m->bodies_per_world > 64 || m->dofs_per_world != 6 * m->bodies_per_world ||
+              m->joints_per_world != m->bodies_per_world || out->dynamics_factor)) {
+    sapb::set_last_error("sapb_free_motion_contacts: tree-blocked outputs need worlds of <= 64 free bodies "
+                         "(got %d bodies, %d joints, %d DOFs) and no dynamics_factor output",
+                         m->bodies_per_world, m->joints_per_world, m->dofs_per_world);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if (!blk && (m->bodies_per_world > 64 || m->dofs_per_world > 128)) {
     sapb::set_last_error("sapb_free_motion_contacts: at most 64 bodies and 128 DOFs per world (got %d, %d)",
                          m->bodies_per_world, m->dofs_per_world);
     return SAPB_ERR_UNSUPPORTED;
   }
-  const size_t smem = sapb::prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, o->max_contacts);
+  const size_t smem = sapb::prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, o->max_contacts, blk);
   if (smem > sapb::kMaxSmemPerBlock) {
     sapb::set_last_error("sapb_free_motion_contacts: world too large for one block (%zu bytes of shared memory)",
                          smem);

@@ -45,7 +45,7 @@ struct PrepLayout {
   size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, dbody, tri, total;
 };
 
-__host__ __device__ inline PrepLayout prep_layout(int B, int n, int C) {
+__host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk) {
   PrepLayout L;
   const size_t Cc = (size_t)(C > 0 ? C : 1);
   size_t o = 0;
@@ -66,14 +66,14 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C) {
   L.S = take(sizeof(double) * 6 * n);       // motion subspace columns
   L.F = take(sizeof(double) * 6 * n);       // composite inertia times S
   L.vec = take(sizeof(double) * 4 * n);     // tau, vdot, diag(A), 1/d
-  L.H = take(sizeof(double) * (size_t)n * n);
+  L.H = take(sizeof(double) * (blk ? (size_t)36 * B : (size_t)n * n));  // A (tree blocks when blocked)
   L.con = take(sizeof(double) * 21 * Cc);   // per contact: x0 3, x1 3, -, -, frame 9
   L.conint = take(sizeof(int) * 2 * Cc);    // local bodies lb0, lb1
   L.anc = take(sizeof(uint64_t) * 2 * B);   // ancestor-or-self masks (two buffers)
   L.jmp = take(sizeof(int) * 2 * B);        // pointer-jumping parents (two buffers)
   L.bj = take(sizeof(int) * B);             // joint (global index) of each body, -1
   L.dbody = take(sizeof(int) * n);          // body of each DOF
-  L.tri = take(sizeof(uint16_t) * (size_t)(n * (n - 1) / 2 + 1));  // LDL^T triangle list
+  L.tri = take(sizeof(uint16_t) * (blk ? 1 : (size_t)(n * (n - 1) / 2 + 1)));  // LDL^T triangle list
   L.total = o;
   return L;
 }
@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   const int e = blockIdx.x;
   const int B = P.m.bodies_per_world, n = P.m.dofs_per_world, C = P.o.max_contacts;
   const int Jw = P.m.joints_per_world;
-  const PrepLayout L = prep_layout(B, n, C);
+  const bool blk = P.o.tree_blocked != 0;  // worlds of free bodies, tree-blocked outputs
+  const PrepLayout L = prep_layout(B, n, C, blk);
   double* poseA = reinterpret_cast<double*>(smem + L.pose);
   double* poseB = reinterpret_cast<double*>(smem + L.pose2);
   double* fm = reinterpret_cast<double*>(smem + L.fm);
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   // ---- topology of this world --------------------------------------------
   for (int b = tid; b < B; b += kPrepNT) bj[b] = -1;
   for (int i = tid; i < n; i += kPrepNT) dbody[i] = -1;
-  build_triangle_list<kPrepNT>(tri, n);
+  if (!blk) build_triangle_list<kPrepNT>(tri, n);
   for (int k = tid; k < 6 * n; k += kPrepNT) S[k] = 0.0;
   __syncthreads();
   for (int jl = tid; jl < Jw; jl += kPrepNT) {
@@ -459,8 +460,28 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   }
   __syncthreads();
   // ---- A = composite-rigid-body pairs + armature ------------------------------
-  double* Ag = P.out.dynamics_matrix + (size_t)e * n * n;
-  for (int k = tid; k < n * n; k += kPrepNT) {
+  if (blk) {
+    // free bodies: the 6 x 6 block of each tree (DOFs 6 t .. 6 t + 5)
+    double* Tm = P.out.tree_mass + (size_t)e * 36 * B;
+    for (int k = tid; k < 36 * B; k += kPrepNT) {
+      const int t = k / 36, a = (k / 6) % 6, b = k % 6;
+      const int i = 6 * t + (a > b ? a : b), j = 6 * t + (a > b ? b : a);
+      const int bi = dbody[i], bjj = dbody[j];
+      double v = 0.0;
+      if (bi >= 0 && bjj >= 0) {
+        if ((anc[bi] >> bjj) & 1ull) v = sdot(sv_load(S + 6 * j), sv_load(Fi + 6 * i));
+        else if ((anc[bjj] >> bi) & 1ull) v = sdot(sv_load(S + 6 * i), sv_load(Fi + 6 * j));
+      }
+      if (a == b) {
+        v += P.m.joint_armature[d0 + i];
+        adiag[i] = v;
+      }
+      H[k] = v;
+      Tm[k] = v;
+    }
+  }
+  double* Ag = blk ? nullptr : P.out.dynamics_matrix + (size_t)e * n * n;
+  for (int k = tid; k < (blk ? 0 : n * n); k += kPrepNT) {
     const int i = k / n, j = k - i * n;
     if (j > i) continue;
     const int bi = dbody[i], bjj = dbody[j];
@@ -480,6 +501,49 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   __syncthreads();
 
   // ---- free-motion solve A vdot = tau: LDL^T (H_ik = L_ik d_k below the diagonal)
+  if (blk) {
+    // a thread per tree: LDL^T of its 6 x 6 block and the solve, in registers
+    for (int t = tid; t < B; t += kPrepNT) {
+      double Lr[6][6], Dr[6], z[6];
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = 0; b <= a; ++b) Lr[a][b] = H[36 * t + 6 * a + b];
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        double d = Lr[b][b];
+#pragma unroll
+        for (int q = 0; q < b; ++q) d -= Lr[b][q] * Lr[b][q] * Dr[q];
+        Dr[b] = d;
+        const double r = 1.0 / d;
+#pragma unroll
+        for (int a = b + 1; a < 6; ++a) {
+          double v = Lr[a][b];
+#pragma unroll
+          for (int q = 0; q < b; ++q) v -= Lr[a][q] * Lr[b][q] * Dr[q];
+          Lr[a][b] = v * r;
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        double v = tau[6 * t + a];
+#pragma unroll
+        for (int q = 0; q < a; ++q) v -= Lr[a][q] * z[q];
+        z[a] = v;
+      }
+#pragma unroll
+      for (int a = 0; a < 6; ++a) z[a] /= Dr[a];
+#pragma unroll
+      for (int a = 5; a >= 0; --a) {
+        double v = z[a];
+#pragma unroll
+        for (int q = a + 1; q < 6; ++q) v -= Lr[q][a] * z[q];
+        z[a] = v;
+      }
+#pragma unroll
+      for (int a = 0; a < 6; ++a) vdot[6 * t + a] = z[a];
+    }
+  } else {
   ldlt_blocked<kPrepNT, double>(H, n, n, dinv, tri);
   if (P.out.dynamics_factor) {
     double* Lg = P.out.dynamics_factor + (size_t)e * n * n;
@@ -535,6 +599,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
       const int i = lane + 32 * r;
       if (i < n) vdot[i] = hb[r];
     }
+  }
   }
   __syncthreads();
   for (int i = tid; i < n; i += kPrepNT) {
@@ -624,7 +689,16 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   // ---- contact rows, free-motion contact velocities and diag_delassus
   // weights, one warp per contact: lanes over the DOF columns, row / weight
   // partial sums reduced by shuffles.
-  double* Jout = P.out.jacobian + (size_t)e * C * 3 * n;
+  // Tree-blocked rows hold 12 columns: the 6 DOFs of side 0's tree, then
+  // side 1's (a contact between two shapes of one tree keeps the combined
+  // columns on side 0).
+  const int ncols = blk ? 12 : n;
+  double* Jout = P.out.jacobian + (size_t)e * C * 3 * ncols;
+  auto tree_of = [&](int lb) {
+    if (lb < 0 || bj[lb] < 0) return -1;
+    const int t = (P.m.joint_qd_start[bj[lb]] - d0) / 6;
+    return (t >= 0 && t < B) ? t : -1;
+  };
   {
     const int lane = tid & 31, warp = tid >> 5;
     const bool dd = P.o.contact_weight_mode == SAPB_WEIGHT_DIAG_DELASSUS;
@@ -632,26 +706,47 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     for (int c = warp; c < cc; c += kPrepNT / 32) {
       const double* cs = con + 21 * (size_t)c;
       const int lb0 = conint[2 * c], lb1 = conint[2 * c + 1];
+      int t0 = -1, t1 = -1;
+      if (blk) {
+        t0 = tree_of(lb0);
+        t1 = tree_of(lb1);
+        if (t1 == t0) t1 = -1;
+        if (t0 < 0) {
+          t0 = t1;
+          t1 = -1;
+        }
+        if (lane == 0) {
+          // the side order of the rows: the body of side 0 (or the only one)
+          P.out.contact_tree[2 * ((size_t)e * C + c)] = t0;
+          P.out.contact_tree[2 * ((size_t)e * C + c) + 1] = t1;
+        }
+      }
       double wq[6] = {0, 0, 0, 0, 0, 0}, vq[3] = {0, 0, 0};
-      for (int col = lane; col < n; col += 32) {
+      for (int col = lane; col < ncols; col += 32) {
         V3 rel = v3(0, 0, 0);
-        const int bcol = dbody[col];
+        int dof = col;
+        if (blk) {
+          const int ts = col < 6 ? t0 : t1;
+          dof = ts >= 0 ? 6 * ts + col % 6 : -1;
+        }
+        const int bcol = dof >= 0 ? dbody[dof] : -1;
         if (bcol >= 0) {
-          const Sv sc = sv_load(S + 6 * col);
+          const Sv sc = sv_load(S + 6 * dof);
           if (lb1 >= 0 && ((anc[lb1] >> bcol) & 1ull)) rel = rel + (sc.v + cross(sc.w, load3(cs + 3)));
           if (lb0 >= 0 && ((anc[lb0] >> bcol) & 1ull)) rel = rel - (sc.v + cross(sc.w, load3(cs + 0)));
         }
         double rw[3];
         for (int r = 0; r < 3; ++r) {
           rw[r] = dot(load3(cs + 12 + 3 * r), rel);
-          Jout[((size_t)c * 3 + r) * n + col] = rw[r];
+          Jout[((size_t)c * 3 + r) * ncols + col] = rw[r];
         }
-        const double vs = P.in.joint_qd[d0 + col] + h * vdot[col];
+        if (dof < 0) continue;
+        const double vs = P.in.joint_qd[d0 + dof] + h * vdot[dof];
         vq[0] += rw[0] * vs;
         vq[1] += rw[1] * vs;
         vq[2] += rw[2] * vs;
         if (dd) {
-          double aii = adiag[col];
+          double aii = adiag[dof];
           if (aii < 1.0e-12) aii = 1.0e-12;
           const double inv = 1.0 / aii;
           wq[0] += inv * rw[0] * rw[0];
@@ -720,7 +815,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   }
 }
 
-size_t prepare_smem_bytes(int B, int n, int C) { return prep_layout(B, n, C).total; }
+size_t prepare_smem_bytes(int B, int n, int C, bool blk) { return prep_layout(B, n, C, blk).total; }
 
 int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, const sapb_prepare_options* o,
                        const sapb_prepare_outputs* out, void* workspace, size_t workspace_bytes,
@@ -745,7 +840,7 @@ int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, con
     err = cudaGetLastError();
   }
   if (err == cudaSuccess) {
-    const size_t smem = prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, C);
+    const size_t smem = prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, C, o->tree_blocked != 0);
     err = cudaFuncSetAttribute(prepare_world_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err == cudaSuccess) {
       prepare_world_kernel<<<W, kPrepNT, smem, stream>>>(P);

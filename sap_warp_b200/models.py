@@ -43,10 +43,12 @@ def _spd_inertia(rng, m, link):
     return R @ np.diag(d) @ R.T + 1e-4 * np.eye(3)
 
 
-def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: bool = False) -> dict:
+def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: bool = False,
+                   boxes: int = 64) -> dict:
     """One world's topology and inertia (numpy).  kind: 'humanoid' (free base
     + 29-revolute serial chain, 35 DOF), 'quadruped' (free base + 4 legs x 3
-    revolute, 18 DOF), 'box' (one free box, 6 DOF), 'arm_box' (7-revolute
+    revolute, 18 DOF), 'box' (one free box, 6 DOF), 'boxes' (`boxes` free
+    bodies, each its own tree: 6 * boxes DOF), 'arm_box' (7-revolute
     fixed-base arm + free box, 13 DOF), 'slider' (free base + prismatic +
     revolute chain)."""
     joints = []  # (type, parent_body, axis or None, X_p, X_c)
@@ -63,6 +65,9 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
                 joints.append((SAP_JOINT_REVOLUTE, parent, None))
     elif kind == "box":
         joints.append((SAP_JOINT_FREE, -1, None))
+    elif kind == "boxes":
+        for _ in range(boxes):
+            joints.append((SAP_JOINT_FREE, -1, None))
     elif kind == "arm_box":
         for k in range(7):
             joints.append((SAP_JOINT_REVOLUTE, k - 1, None))
@@ -324,3 +329,122 @@ def rollout_scene(kind: str, worlds: int, seed: int, device, *, contacts=(8, 32)
     con = ground_contacts(rng, bq[..., :3], bq[..., 3:], counts, bodies_from=B // 2, phi0_range=phi0_range,
                           tilt=tilt, capacity=int(counts.sum()))
     return model, state, control, contacts_to_torch(con, device), con
+
+
+def _quat_z(yaw: np.ndarray) -> np.ndarray:
+    """Quaternions (x, y, z, w) of rotations about +z."""
+    z = np.zeros_like(yaw)
+    return np.stack([z, z, np.sin(0.5 * yaw), np.cos(0.5 * yaw)], -1)
+
+
+def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20), points_per_pair=(4, 8),
+              side_pairs=(2, 8), size_range=(0.05, 0.2), density_range=(500.0, 2000.0), v_std: float = 0.05,
+              phi0_range=(-2.0e-3, 0.0), mu_range=(0.3, 1.0), stiffness: float = 1.0e5, tau_d: float = 0.01):
+    """Worlds of `boxes` free boxes stacked on a grid of sites on the ground
+    (the model behind scenes.box_stack_problem, as a SapModel with a flat
+    contact buffer): box sizes U[size_range] m per axis, density
+    U[density_range], small random yaw, body origin at the centre of the
+    bottom face; 4-8 contact points between each box and the box below it
+    (or the ground), plus a few side contacts between boxes of neighbouring
+    stacks; witness points in the body frames of their shapes, normal from
+    shape0 to shape1, phi0 ~ U[phi0_range]; joint velocities ~ N(0, v_std).
+    Returns (model, state, control, contacts, host contact dict, host arrays
+    dict(tpl, g, q, qd))."""
+    from .runtime import SapControl, SapState
+    from .scenes import _axis_angle
+
+    rng = np.random.default_rng(seed)
+    E, B = worlds, boxes
+    tpl = world_template("boxes", rng, boxes=B)
+    g = replicate(tpl, E, rng, mu_range=mu_range, stiffness=stiffness, tau_d=0.5 * tau_d)
+    q = np.zeros((E, 7 * B))
+    ground = E * B
+    rows = []  # (world, shape0, shape1, x1 world, normal, lower body or -1, upper body)
+    pos_all = np.zeros((E, B, 3))
+    R_all = np.zeros((E, B, 3, 3))
+    for e in range(E):
+        S = int(rng.integers(sites[0], sites[1] + 1))
+        grid = int(np.ceil(np.sqrt(S)))
+        site_xy = np.stack([(np.arange(S) % grid) * 0.35, (np.arange(S) // grid) * 0.35], -1)
+        site_of = rng.integers(0, S, size=B)
+        dims = rng.uniform(*size_range, size=(B, 3))
+        mass = rng.uniform(*density_range, size=B) * dims.prod(-1)
+        yaw = rng.uniform(-0.3, 0.3, size=B)
+        R = _axis_angle(np.array([0.0, 0.0, 1.0]), yaw)
+        origin = np.zeros((B, 3))
+        below = np.full(B, -1)
+        top_z = np.zeros(S)
+        top_box = np.full(S, -1)
+        for k in range(B):
+            st = site_of[k]
+            origin[k] = [site_xy[st, 0] + rng.normal(scale=0.01), site_xy[st, 1] + rng.normal(scale=0.01), top_z[st]]
+            below[k] = top_box[st]
+            top_z[st] += dims[k, 2]
+            top_box[st] = k
+        sl = slice(e * B, (e + 1) * B)
+        a, b, c = dims[:, 0], dims[:, 1], dims[:, 2]
+        g["body_mass"][sl] = mass
+        g["body_inertia"][sl] = (mass / 12.0)[:, None, None] * np.stack(
+            [np.diag(v) for v in np.stack([b * b + c * c, a * a + c * c, a * a + b * b], -1)])
+        g["body_com"][sl] = np.stack([np.zeros(B), np.zeros(B), 0.5 * c], -1)
+        q7 = q[e].reshape(B, 7)
+        q7[:, :3] = origin
+        q7[:, 3:] = _quat_z(yaw)
+        pos_all[e], R_all[e] = origin, R
+        for k in range(B):
+            lo = below[k]
+            hx = 0.45 * min(dims[k, 0], dims[lo, 0] if lo >= 0 else 1.0)
+            hy = 0.45 * min(dims[k, 1], dims[lo, 1] if lo >= 0 else 1.0)
+            npts = int(rng.integers(points_per_pair[0], points_per_pair[1] + 1))
+            local = np.array([[hx, hy], [-hx, hy], [-hx, -hy], [hx, -hy]])
+            if npts > 4:
+                local = np.concatenate([local, rng.uniform(-1, 1, size=(npts - 4, 2)) * [hx, hy]])
+            for p2 in local[:npts]:
+                x1 = origin[k] + R[k] @ np.array([p2[0], p2[1], 0.0])
+                nrm = np.array([0.0, 0.0, 1.0]) + (rng.normal(scale=0.02, size=3) if lo >= 0 else 0.0)
+                rows.append((e, lo, k, x1, nrm / np.linalg.norm(nrm)))
+        for _ in range(int(rng.integers(side_pairs[0], side_pairs[1] + 1))):
+            s0 = int(rng.integers(0, S))
+            nb = [t for t in (s0 + 1, s0 + grid) if t < S and (t != s0 + 1 or (s0 + 1) % grid != 0)]
+            if not nb:
+                continue
+            s1 = nb[int(rng.integers(0, len(nb)))]
+            in0, in1 = np.nonzero(site_of == s0)[0], np.nonzero(site_of == s1)[0]
+            if len(in0) == 0 or len(in1) == 0:
+                continue
+            u, w = int(rng.choice(in0)), int(rng.choice(in1))
+            d = origin[w] - origin[u]
+            d[2] = 0.0
+            nrm = d / max(np.linalg.norm(d), 1e-9)
+            mid = 0.5 * (origin[u] + origin[w])
+            zlo = max(origin[u, 2], origin[w, 2])
+            for _p in range(int(rng.integers(2, 5))):
+                x1 = np.array([mid[0], mid[1], zlo + rng.uniform(0.0, 0.05)])
+                x1[:2] += rng.normal(scale=0.02, size=2) * np.array([-nrm[1], nrm[0]])
+                rows.append((e, u, w, x1, nrm))
+    N = len(rows)
+    phi0 = rng.uniform(*phi0_range, size=N)
+    shape0 = np.array([r[0] * B + r[1] if r[1] >= 0 else ground for r in rows], np.int32)
+    shape1 = np.array([r[0] * B + r[2] for r in rows], np.int32)
+    x1 = np.stack([r[3] for r in rows])
+    nrm = np.stack([r[4] for r in rows])
+    x0 = x1 - phi0[:, None] * nrm
+    ew = np.array([r[0] for r in rows])
+    lo = np.array([r[1] for r in rows])
+    up = np.array([r[2] for r in rows])
+    Ru = R_all[ew, up]
+    p1 = np.einsum("nji,nj->ni", Ru, x1 - pos_all[ew, up])
+    Rl = R_all[ew, np.maximum(lo, 0)]
+    p0 = np.where((lo >= 0)[:, None], np.einsum("nji,nj->ni", Rl, x0 - pos_all[ew, np.maximum(lo, 0)]), x0)
+    z = np.zeros(N)
+    con = dict(count=np.array([N], np.int32), shape0=shape0, shape1=shape1, point0=p0.astype(np.float32),
+               point1=p1.astype(np.float32), normal=nrm.astype(np.float32), margin0=z.astype(np.float32),
+               margin1=z.astype(np.float32), point0d=p0, point1d=p1, normald=nrm, margin0d=z, margin1d=z.copy())
+    qd = rng.normal(scale=v_std, size=(E, 6 * B))
+    model = to_model(tpl, g, q, device)
+    state = SapState(joint_q=torch.as_tensor(q.reshape(-1), dtype=torch.float64, device=device),
+                     joint_qd=torch.as_tensor(qd.reshape(-1), dtype=torch.float64, device=device),
+                     body_q=model.body_q.clone(),
+                     body_f=torch.zeros(model.body_count, 6, dtype=torch.float64, device=device))
+    control = SapControl(joint_f=torch.zeros(model.joint_dof_count, dtype=torch.float64, device=device))
+    return model, state, control, contacts_to_torch(con, device), con, dict(tpl=tpl, g=g, q=q, qd=qd)

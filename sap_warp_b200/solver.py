@@ -107,6 +107,13 @@ class _ModelView:
         if np.any(parent_joint >= np.arange(J)):
             raise ValueError("joints must be ordered parents before children")
         self.device = model.joint_type.device
+        # worlds made only of free bodies (one 6-DOF tree per body) may use the
+        # tree-blocked layout; by default those beyond the dense solve's 60
+        # DOFs do
+        jp = model.joint_parent.cpu().numpy()
+        self.free_bodies = bool(self.Jw == self.Bw and self.n == 6 * self.Bw and self.Bw <= 64
+                                and np.all(jt == SAP_JOINT_FREE) and np.all(jp < 0))
+        self.tree_blocked = self.free_bodies and self.n > 60
         d = _abi.ModelDesc()
         d.num_worlds, d.joints_per_world, d.bodies_per_world = W, self.Jw, self.Bw
         d.dofs_per_world, d.coords_per_world, d.articulations_per_world = self.n, self.Qw, self.Aw
@@ -192,6 +199,14 @@ class _ModelView:
         self.has_limits = bool(np.any((limit_ok != 0) & (lke > 0) & (np.isfinite(lo) | np.isfinite(hi))))
 
 
+def _pick_tree_blocked(view: _ModelView, tree_blocked: bool | None) -> bool:
+    if tree_blocked is None:
+        return view.tree_blocked
+    if tree_blocked and not view.free_bodies:
+        raise ValueError("the tree-blocked layout needs worlds made only of free bodies (<= 64 per world)")
+    return bool(tree_blocked)
+
+
 @dataclass(frozen=True)
 class SapFreeMotionResult:
     """sim/free_motion.py:63-68"""
@@ -225,6 +240,12 @@ class SapContactJacobianResult:
     # LDL^T of dynamics_matrix_env from the free-motion solve (no counterpart
     # in the reference's result), or None when not requested
     dynamics_factor_env: torch.Tensor | None = None
+    # tree-blocked layout (worlds of free bodies; no counterpart in the
+    # reference): the diagonal 6 x 6 blocks of A [W, B, 6, 6] and the tree of
+    # each contact side [W, C, 2]; contact_env_jacobian is then [W, C, 3, 12]
+    # and dynamics_matrix_env is None
+    tree_mass_env: torch.Tensor | None = None
+    contact_env_tree: torch.Tensor | None = None
 
 
 @dataclass(frozen=True)
@@ -256,9 +277,13 @@ class SapContactJacobian:
                  contact_weight_mode: str = "diag_delassus", contact_point_mode: str = "contact_midpoint",
                  capture_local_snapshots: bool = False, use_f64_boundary_pose: bool = True,
                  free_motion_solve_precision: str = "fp64", sap_contact_weight_precision: str = "fp64",
-                 _view: _ModelView | None = None):
+                 tree_blocked: bool | None = None, _view: _ModelView | None = None):
+        """tree_blocked: None picks the tree-blocked layout for worlds of free
+        bodies with more than 60 DOFs; True asks for it (worlds of free
+        bodies only), False for the dense one."""
         self.view = _view or _ModelView(model)
         v = self.view
+        self.tree_blocked = _pick_tree_blocked(v, tree_blocked)
         self.model = model
         self.max_rigid_contact = max(int(max_rigid_contact), 1)
         wm = str(contact_weight_mode).strip().lower()
@@ -280,12 +305,20 @@ class SapContactJacobian:
         self.opts.fallback_mu = float(fallback_mu)
         self.opts.fallback_stiffness = float(fallback_stiffness)
         self.opts.fallback_tau_d = float(fallback_tau_d)
+        self.opts.tree_blocked = 1 if self.tree_blocked else 0
         W, n, C, dev = v.W, v.n, self.max_rigid_contact, v.device
         z = lambda *s, dt=F64: torch.zeros(*s, dtype=dt, device=dev)
         self.v_star = z(W * n)
         self.vdot = z(W * n)
-        self.dynamics_matrix_env = z(W, n, n)
-        self.contact_env_jacobian = z(W, C, 3, n)
+        if self.tree_blocked:
+            self.dynamics_matrix_env = None
+            self.tree_mass_env = z(W, v.Bw, 6, 6)
+            self.contact_env_tree = torch.full((W, C, 2), -1, dtype=I32, device=dev)
+            self.contact_env_jacobian = z(W, C, 3, 12)
+        else:
+            self.dynamics_matrix_env = z(W, n, n)
+            self.tree_mass_env = self.contact_env_tree = None
+            self.contact_env_jacobian = z(W, C, 3, n)
         self.contact_env_count = z(W, dt=I32)
         self.contact_env_phi0 = z(W, C)
         self.contact_env_w_eff = z(W, C)
@@ -311,11 +344,14 @@ class SapContactJacobian:
         o.body0, o.body1 = _ptr(self.contact_env_body0), _ptr(self.contact_env_body1)
         o.point, o.frame = _ptr(self.contact_env_point), _ptr(self.contact_env_R_WC)
         o.truncated_count, o.body_q = _ptr(self.truncated), _ptr(self.body_q_sap)
+        o.tree_mass, o.contact_tree = _ptr(self.tree_mass_env), _ptr(self.contact_env_tree)
         self.outputs = o
 
     def keep_dynamics_factor(self) -> None:
         """Also write the free-motion LDL^T of A and the free-motion contact
         velocities J_c v* (for candidate starts and the warm-start network)."""
+        if self.tree_blocked:
+            raise NotImplementedError("the tree-blocked layout keeps no dense factor of A")
         if self.dynamics_factor_env is None:
             v = self.view
             self.dynamics_factor_env = torch.zeros(v.W, v.n, v.n, dtype=F64, device=v.device)
@@ -395,7 +431,8 @@ class SapContactJacobian:
             contact_env_witness0=None, contact_env_witness1=None, contact_env_body0=self.contact_env_body0,
             contact_env_body1=self.contact_env_body1, body_jacobian_local=None,
             dynamics_matrix_env=self.dynamics_matrix_env, contact_env_tau_d=self.contact_env_tau_d,
-            dynamics_factor_env=self.dynamics_factor_env)
+            dynamics_factor_env=self.dynamics_factor_env, tree_mass_env=self.tree_mass_env,
+            contact_env_tree=self.contact_env_tree)
 
     @property
     def free_motion_result(self) -> SapFreeMotionResult:
@@ -416,6 +453,8 @@ class SapFreeMotion:
         self._cj.compute(state, SapContacts(), control=control, dt=dt)
         r = self._cj.free_motion_result
         if assemble_dynamics_matrix:
+            if self._cj.tree_blocked:
+                raise NotImplementedError("assemble_dynamics_matrix is not available in the tree-blocked layout")
             W, n = self._cj.view.W, self._cj.view.n
             A = torch.zeros(W * n, W * n, dtype=F64, device=self._cj.view.device)
             for e in range(W):
@@ -431,11 +470,15 @@ class SapContactSolve:
                  contact_sigma: float = 1.0e-3, contact_tau_d: float = 0.1, block_size: int | None = None,
                  diag_shift: float = 0.0, contact_assembly_tile_size: int = 256, solve_precision: str = "fp64",
                  linear_solve_precision: str = "fp64", hessian_precision: str | None = None,
-                 _view: _ModelView | None = None):
+                 tree_blocked: bool | None = None, _view: _ModelView | None = None):
         self.view = _view or _ModelView(model)
         v = self.view
-        if v.n > 60:
-            raise NotImplementedError(f"the on-chip solve supports up to 60 DOFs per world, got {v.n}")
+        self.tree_blocked = _pick_tree_blocked(v, tree_blocked)
+        if v.n > 60 and not self.tree_blocked:
+            raise NotImplementedError(f"the dense on-chip solve supports up to 60 DOFs per world, got {v.n} "
+                                      "(worlds of free bodies use the tree-blocked solve)")
+        if self.tree_blocked and (v.has_pd or v.has_limits):
+            raise NotImplementedError("the tree-blocked solve has no joint drive or limit terms")
         self.model = model
         self.max_rigid_contact = max(int(max_rigid_contact), 1)
         self.contact_beta, self.contact_sigma = float(contact_beta), float(contact_sigma)
@@ -461,7 +504,8 @@ class SapContactSolve:
         self.grad_norm = z(W)
         self.warm_start_accepted_env = z(W, dt=I32)
         self.dt_world = z(W)
-        ws = int(load().sapb_contact_solve_workspace_size(W, n, C))
+        ws = int(load().sapb_blocked_solve_workspace_size(W, v.Bw, C) if self.tree_blocked
+                 else load().sapb_contact_solve_workspace_size(W, n, C))
         self.workspace = torch.zeros(max(ws, 16), dtype=torch.uint8, device=dev)
         self.zero_f32 = z(W * n, dt=F32)
         out = _abi.SolveOutputs()
@@ -536,6 +580,10 @@ class SapContactSolve:
                             rho=float(rho), line_search_relative_slop=float(line_search_relative_slop))
         v = self.view
         W, n, C = v.W, v.n, self.max_rigid_contact
+        if self.tree_blocked:
+            if gamma0 is not None:
+                raise NotImplementedError("candidate starting impulses need the dense layout")
+            return self._solve_blocked(contact_result, opts, v_star, v0, v_guess, v_guess_active)
         P = _abi.ContactProblem()
         P.num_envs, P.dof_per_env, P.max_contacts = W, n, int(contact_result.contact_env_jacobian.shape[1])
         P.num_bodies = int(v.body_dof_start.numel())
@@ -576,6 +624,32 @@ class SapContactSolve:
         check(status, "sapb_contact_solve")
         return self.result()
 
+    def _solve_blocked(self, r: SapContactJacobianResult, opts, v_star, v0, v_guess, v_guess_active):
+        """The tree-blocked solve (sapb_blocked_contact_solve) on the
+        tree-blocked result of SapContactJacobian."""
+        if r.tree_mass_env is None or r.contact_env_tree is None:
+            raise ValueError("the tree-blocked solve needs a tree-blocked SapContactJacobianResult")
+        v = self.view
+        P = _abi.BlockedProblem()
+        P.num_envs, P.trees_per_env, P.tree_dofs = v.W, v.Bw, 6
+        P.max_contacts = int(r.contact_env_jacobian.shape[1])
+        P.contact_count, P.tree_mass = _ptr(r.contact_env_count), _ptr(r.tree_mass_env)
+        P.jacobian, P.contact_tree = _ptr(r.contact_env_jacobian), _ptr(r.contact_env_tree)
+        P.phi0, P.w_eff, P.mu = _ptr(r.contact_env_phi0), _ptr(r.contact_env_w_eff), _ptr(r.contact_env_mu)
+        P.stiffness, P.tau_d = _ptr(r.contact_env_stiffness), _ptr(r.contact_env_tau_d)
+        self._vs, self._v0 = _f64(v_star), _f64(v0)
+        P.v_star, P.v0, P.dt = _ptr(self._vs), _ptr(self._v0), _ptr(self.dt_world)
+        if v_guess is not None:
+            if v_guess.dtype != F64 or not v_guess.is_contiguous():
+                raise TypeError("v_guess must be a contiguous float64 tensor (it is written back)")
+            P.v_guess = _ptr(v_guess)
+            P.v_guess_active = _ptr(v_guess_active)
+        status = load().sapb_blocked_contact_solve(ctypes.byref(P), ctypes.byref(opts), ctypes.byref(self.outputs),
+                                                   self.workspace.data_ptr(), self.workspace.numel(),
+                                                   ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream))
+        check(status, "sapb_blocked_contact_solve")
+        return self.result()
+
     def result(self) -> SapContactSolveResult:
         return SapContactSolveResult(
             v_env=self.v_env, v_flat=self.v_flat, cost=self.cost, contact_gamma=self.contact_gamma,
@@ -606,7 +680,7 @@ class SolverSAP:
                  static_substep: bool = False, static_substep_iterations: int = 8,
                  static_substep_line_search_iterations: int = 6, position_integration: str | None = None,
                  hessian_precision: str | None = None, warm_start: str = "previous_velocity",
-                 learned_warm_start=None):
+                 learned_warm_start=None, tree_blocked: bool | None = None):
         """Keyword arguments of the reference's SolverSAP (sim/solver_sap.py:
         749-791) plus: hessian_precision ("fp64" / "fp32": J^T G J assembly and
         factorization precision; the gradient, cost, line search and
@@ -619,8 +693,14 @@ class SolverSAP:
                                LearnedWarmStart, a weights path, or None for
                                the packaged weights);
         the lowest-cost start among the previous-velocity one and the
-        candidates is taken, and Newton always runs to the same tolerance."""
+        candidates is taken, and Newton always runs to the same tolerance;
+        tree_blocked (None: automatic) selects the tree-blocked layout for
+        worlds made only of free bodies (default beyond 60 DOFs per world:
+        A as 6 x 6 blocks, contact rows over the two touching bodies, a block
+        sparse Newton factorization), which takes the previous-velocity warm
+        start only."""
         view = _ModelView(model)
+        tree_blocked = _pick_tree_blocked(view, tree_blocked)
         preset = dict(_CONTACT_PRESET_KWARGS[_normalize_contact_preset_variant(contact_preset_variant)])
         self.contact_preset_variant = _normalize_contact_preset_variant(contact_preset_variant)
         pick = lambda v, k: preset[k] if v is None else v
@@ -677,13 +757,13 @@ class SolverSAP:
         self.contact_jacobian = SapContactJacobian(
             model, max_rigid_contact=self.max_rigid_contact, fallback_mu=fallback_mu,
             fallback_stiffness=fallback_stiffness, fallback_tau_d=shape_tau, contact_weight_mode=contact_weight_mode,
-            contact_point_mode=contact_point_mode, _view=view)
+            contact_point_mode=contact_point_mode, tree_blocked=tree_blocked, _view=view)
         # the solve-side fallback is per pair: tau(shape0) + tau(shape1) (sim/solver_sap.py:945-955)
         self.contact_solve = SapContactSolve(
             model, max_rigid_contact=self.max_rigid_contact, contact_beta=contact_beta, contact_sigma=contact_sigma,
             contact_tau_d=2.0 * shape_tau, block_size=block_size, diag_shift=diag_shift,
             solve_precision=self.contact_solve_precision, linear_solve_precision=self.contact_linear_solve_precision,
-            hessian_precision=hessian_precision, _view=view)
+            hessian_precision=hessian_precision, tree_blocked=tree_blocked, _view=view)
         self.view = view
         self.num_envs, self.dof_count, self.dof_per_env = view.W, int(model.joint_dof_count), view.n
         dev = view.device
@@ -694,6 +774,8 @@ class SolverSAP:
         if self.warm_start not in ("previous_velocity", "previous_impulses", "learned"):
             raise ValueError("warm_start must be 'previous_velocity', 'previous_impulses' or 'learned', "
                              f"got {warm_start!r}.")
+        if tree_blocked and self.warm_start != "previous_velocity":
+            raise NotImplementedError("the tree-blocked layout takes the previous-velocity warm start only")
         self.learned_warm_start = None
         if self.warm_start == "learned":
             from .warmstart import DEFAULT_WEIGHTS, LearnedWarmStart
