@@ -3,12 +3,14 @@
     python -m sap_warp_b200.profile_solve --mode snapshot --worlds 4096 --precision fp64 --launches 5
     python -m sap_warp_b200.profile_solve --mode rollout --worlds 4096 --steps 8 --warm-start learned \\
         --precision fp32
+    python -m sap_warp_b200.profile_solve --mode boxes --worlds 512 --precision fp32 --launches 3
 
 snapshot: the stage-2 solve alone on the batched humanoid problem (A, J
 given): warm-up launches, then `--launches` timed launches.
 rollout: SolverSAP steps (drake preset) of the humanoid rollout scene with
 the given warm start and Hessian precision: `--steps` steps, the last half
-timed.  Each prints the mean time per launch / step.  Used as the target
+timed.  boxes: the tree-blocked solve alone on worlds of 64 free boxes
+(scenes.box_stack_problem).  Each prints the mean time per launch / step.  Used as the target
 command of ncu captures (select a kernel with `-k regex:...` and skip the
 warm-up launches with `-s`).
 """
@@ -41,6 +43,26 @@ def snapshot(args, dev) -> None:
           f"mean Newton iterations {buf.newton_iterations.double().mean().item():.3f}")
 
 
+def boxes(args, dev) -> None:
+    from ._solve import blocked_contact_solve, blocked_problem_to_device
+
+    prob = scenes.box_stack_problem(args.worlds, seed=args.seed)
+    t = blocked_problem_to_device(prob, dev)
+    buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, dev)
+    opt = make_options(args.variant, hessian_precision=args.precision, linear_solve_precision=args.precision)
+    for _ in range(args.warmup):
+        blocked_contact_solve(**t, buffers=buf, options=opt, trees_per_env=prob.trees_per_env)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.launches):
+        blocked_contact_solve(**t, buffers=buf, options=opt, trees_per_env=prob.trees_per_env)
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"boxes {args.precision} {args.worlds} worlds: {e0.elapsed_time(e1) / max(args.launches, 1):.4f} "
+          f"ms/launch, mean Newton iterations {buf.newton_iterations.double().mean().item():.3f}")
+
+
 def rollout(args, dev) -> None:
     from .runtime import SapState
     from .solver import SolverSAP
@@ -66,7 +88,7 @@ def rollout(args, dev) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", choices=["snapshot", "rollout"], default="snapshot")
+    ap.add_argument("--mode", choices=["snapshot", "rollout", "boxes"], default="snapshot")
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--variant", default="armijo_decay")
@@ -78,7 +100,7 @@ def main() -> None:
     ap.add_argument("--seed", type=int, default=2)
     args = ap.parse_args()
     dev = torch.device("cuda:0")
-    (snapshot if args.mode == "snapshot" else rollout)(args, dev)
+    {"snapshot": snapshot, "rollout": rollout, "boxes": boxes}[args.mode](args, dev)
 
 
 if __name__ == "__main__":
