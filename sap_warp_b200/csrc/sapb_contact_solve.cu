@@ -495,6 +495,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[8 * (NT / 32)];
   __shared__ int s_next;
+  __shared__ unsigned long long s_partmask;
   const int tid = threadIdx.x;
   const int n = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
   const Layout L = make_layout(n, C, (int)sizeof(HT));
@@ -691,28 +692,38 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
     }
     __syncthreads();
     // ---- participating DOFs (sim/contact_solve.py:423-488) ------------------
+    // A DOF takes part if a model term acts on it or a contact's body DOF
+    // range or J column covers it.  The contacts mark their DOFs in a 64-bit
+    // mask in parallel (n <= 60 here).
+    if (tid == 0) s_partmask = 0ull;
+    __syncthreads();
+    for (int c = tid; c < count; c += NT) {
+      const size_t ci = (size_t)e * C + c;
+      unsigned long long mk = 0ull;
+      if (P.p.body_dof_start) {
+        const int bs[2] = {P.p.body0 ? P.p.body0[ci] : -1, P.p.body1 ? P.p.body1[ci] : -1};
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int b = bs[q];
+          if (b < 0 || b >= P.p.num_bodies) continue;
+          const int s = P.p.body_dof_start[b], m = P.p.body_dof_count[b];
+          if (s < 0 || m <= 0 || s >= n) continue;
+          const int hi = s + m < n ? s + m : n;
+          mk |= ((1ull << (hi - s)) - 1ull) << s;
+        }
+      }
+      const double* Jc = w.J + (size_t)(3 * c) * L.ldJ;
+      if (mk != (1ull << n) - 1ull)
+        for (int j = 0; j < n; ++j)
+          if (Jc[j] != 0.0 || Jc[L.ldJ + j] != 0.0 || Jc[2 * L.ldJ + j] != 0.0) mk |= 1ull << j;
+      atomicOr(&s_partmask, mk);
+    }
+    __syncthreads();
     int any_model_term = 0;
     for (int i = tid; i < n; i += NT) {
-      int part = (w.flags[i] & (kFlagPd | kFlagLo | kFlagUp)) ? 1 : 0;
-      any_model_term |= part;
-      for (int c = 0; c < count && !part; ++c) {
-        const size_t ci = (size_t)e * C + c;
-        const int b0 = P.p.body0 ? P.p.body0[ci] : -1;
-        const int b1 = P.p.body1 ? P.p.body1[ci] : -1;
-        if (P.p.body_dof_start) {
-          if (b0 >= 0 && b0 < P.p.num_bodies) {
-            const int s = P.p.body_dof_start[b0], m = P.p.body_dof_count[b0];
-            if (s >= 0 && m > 0 && i >= s && i < s + m) part = 1;
-          }
-          if (b1 >= 0 && b1 < P.p.num_bodies) {
-            const int s = P.p.body_dof_start[b1], m = P.p.body_dof_count[b1];
-            if (s >= 0 && m > 0 && i >= s && i < s + m) part = 1;
-          }
-        }
-        const double* Jc = w.J + (size_t)(3 * c) * L.ldJ;
-        if (Jc[i] != 0.0 || Jc[L.ldJ + i] != 0.0 || Jc[2 * L.ldJ + i] != 0.0) part = 1;
-      }
-      if (part) w.flags[i] |= kFlagPart;
+      const int model = (w.flags[i] & (kFlagPd | kFlagLo | kFlagUp)) ? 1 : 0;
+      any_model_term |= model;
+      if (model || ((s_partmask >> i) & 1ull)) w.flags[i] |= kFlagPart;
     }
     const int model_terms = __syncthreads_or(any_model_term);
     const bool unconstrained = (count == 0) && !model_terms;

@@ -23,36 +23,56 @@ __device__ __forceinline__ void build_triangle_list(uint16_t* tri, int n) {
 
 // In-place right-looking LDL^T of the lower triangle of H (row stride ldH):
 // afterwards H_ik = L_ik d_k below the diagonal (L unit lower), d_k on it,
-// dinv[k] = 1/d_k.  8-column blocks: the diagonal block by warp 0, the panel
-// and the trailing update by the whole block, three barriers per block.
+// dinv[k] = 1/d_k.  8-column blocks (6 in FP64), two barriers per block:
+// every thread factors the block's diagonal block in registers (it is final
+// once the previous trailing update is done), threads below bs write its rows,
+// the rows under it (the panel) are solved against it in registers, one per
+// thread; then the trailing update.  The arithmetic is the right-looking
+// recurrence on the stored form W_ik = L_ik d_k:
+//   d_k = H_kk - sum_{e<k} W_ke^2 / d_e,  W_ik = H_ik - sum_{e<k} W_ie W_ke / d_e.
 // H must be complete when called (barrier before); complete on return.
 template <int NT, typename T>
 __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri) {
   const int tid = threadIdx.x;
-  constexpr int B = 8;
-  const int lane = tid & 31;
+  constexpr int B = sizeof(T) == 4 ? 8 : 6;  // FP64 blocks of 6: the register block stays small
   for (int K = 0; K < n; K += B) {
     const int bs = min(B, n - K);
-    // (1) diagonal block, unblocked, by warp 0
-    if (tid < 32) {
-      for (int s = 0; s < bs; ++s) {
-        const int ks = K + s;
-        const T rinv = fast_recip(H[(size_t)ks * ldH + ks]);
-        if (lane == 0) dinv[ks] = rinv;
-        const int m = bs - s - 1;  // trailing entries (a, c), s < c <= a < bs
-        for (int q = lane; q < m * (m + 1) / 2; q += 32) {
-          int a = 0;
-          while ((a + 1) * (a + 2) / 2 <= q) ++a;
-          const int c = q - a * (a + 1) / 2;
-          const int i = ks + 1 + a, j = ks + 1 + c;
-          H[(size_t)i * ldH + j] -= (H[(size_t)i * ldH + ks] * rinv) * H[(size_t)j * ldH + ks];
-        }
-        __syncwarp();
+    const int rest = n - K - bs;
+    // (1) the diagonal block, in registers (padding rows: identity)
+    T W[B][B], R[B];
+#pragma unroll
+    for (int a = 0; a < B; ++a)
+#pragma unroll
+      for (int b = 0; b <= a; ++b)
+        W[a][b] = (a < bs) ? H[(size_t)(K + a) * ldH + K + b] : (a == b ? T(1) : T(0));
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      T d = W[b][b];
+#pragma unroll
+      for (int e = 0; e < b; ++e) d -= W[b][e] * R[e] * W[b][e];
+      W[b][b] = d;
+      R[b] = fast_recip(d);
+#pragma unroll
+      for (int a = b + 1; a < B; ++a) {
+        T v = W[a][b];
+#pragma unroll
+        for (int e = 0; e < b; ++e) v -= W[a][e] * R[e] * W[b][e];
+        W[a][b] = v;
       }
     }
-    __syncthreads();
-    const int rest = n - K - bs;
-    if (rest <= 0) break;
+    if (tid < bs) {
+#pragma unroll
+      for (int a = 0; a < B; ++a) {
+        if (a != tid) continue;
+#pragma unroll
+        for (int b = 0; b <= a; ++b) H[(size_t)(K + a) * ldH + K + b] = W[a][b];
+        dinv[K + a] = R[a];
+      }
+    }
+    if (rest <= 0) {
+      __syncthreads();
+      break;
+    }
     // (2) panel rows: P L_K^T = H_panel (forward substitution over the block columns)
     for (int t = tid; t < rest; t += NT) {
       const int i = K + bs + t;
@@ -62,8 +82,7 @@ __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri)
         if (c < bs) {
           T h = H[(size_t)i * ldH + K + c];
 #pragma unroll
-          for (int m2 = 0; m2 < B; ++m2)
-            if (m2 < c) h -= p[m2] * (H[(size_t)(K + c) * ldH + K + m2] * dinv[K + m2]);
+          for (int m2 = 0; m2 < c; ++m2) h -= p[m2] * (W[c][m2] * R[m2]);
           p[c] = h;
           H[(size_t)i * ldH + K + c] = h;
         }
@@ -79,7 +98,7 @@ __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri)
       T acc = H[(size_t)i * ldH + j];
 #pragma unroll
       for (int c = 0; c < B; ++c)
-        if (c < bs) acc -= H[(size_t)i * ldH + K + c] * dinv[K + c] * H[(size_t)j * ldH + K + c];
+        if (c < bs) acc -= H[(size_t)i * ldH + K + c] * R[c] * H[(size_t)j * ldH + K + c];
       H[(size_t)i * ldH + j] = acc;
     }
     __syncthreads();

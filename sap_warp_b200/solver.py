@@ -199,6 +199,12 @@ class _ModelView:
         self.has_limits = bool(np.any((limit_ok != 0) & (lke > 0) & (np.isfinite(lo) | np.isfinite(hi))))
 
 
+def _checked_order(order: torch.Tensor | None, W: int) -> torch.Tensor | None:
+    if order is not None and (order.dtype != I32 or not order.is_contiguous() or order.numel() != W):
+        raise TypeError(f"world_order must be a contiguous int32 tensor of {W} world indices")
+    return order
+
+
 def _pick_tree_blocked(view: _ModelView, tree_blocked: bool | None) -> bool:
     if tree_blocked is None:
         return view.tree_blocked
@@ -549,10 +555,12 @@ class SapContactSolve:
               line_search_relative_slop: float | None = None, line_search_variant: str = "monotone_decay",
               collect_iteration_stats: bool = True, check_line_search_errors: bool = True,
               graph_conditional: bool = True, static_loop: bool = False,
-              gamma0: torch.Tensor | None = None) -> SapContactSolveResult:
+              gamma0: torch.Tensor | None = None, world_order: torch.Tensor | None = None) -> SapContactSolveResult:
         """sim/contact_solve.py:6129-6285.  gamma0 (W, C, 3) FP64: learned
         starting impulses (no counterpart in the reference), tried against the
-        plain start on the cost."""
+        plain start on the cost.  world_order (W,) int32: the order in which
+        the persistent kernel takes the worlds (a permutation; results do not
+        depend on it)."""
         variant = normalize_sap_line_search_mode(line_search_variant)
         if not bool(graph_conditional):
             raise ValueError("SapContactSolve only supports graph_conditional=True; "
@@ -583,12 +591,13 @@ class SapContactSolve:
         if self.tree_blocked:
             if gamma0 is not None:
                 raise NotImplementedError("candidate starting impulses need the dense layout")
-            return self._solve_blocked(contact_result, opts, v_star, v0, v_guess, v_guess_active)
+            return self._solve_blocked(contact_result, opts, v_star, v0, v_guess, v_guess_active, world_order)
         P = _abi.ContactProblem()
         P.num_envs, P.dof_per_env, P.max_contacts = W, n, int(contact_result.contact_env_jacobian.shape[1])
         P.num_bodies = int(v.body_dof_start.numel())
         r = contact_result
         P.contact_count, P.dynamics_matrix = _ptr(r.contact_env_count), _ptr(r.dynamics_matrix_env)
+        P.world_order = _ptr(_checked_order(world_order, W))
         P.jacobian, P.phi0, P.w_eff = _ptr(r.contact_env_jacobian), _ptr(r.contact_env_phi0), _ptr(r.contact_env_w_eff)
         P.mu, P.stiffness, P.tau_d = _ptr(r.contact_env_mu), _ptr(r.contact_env_stiffness), _ptr(r.contact_env_tau_d)
         P.body0, P.body1 = _ptr(r.contact_env_body0), _ptr(r.contact_env_body1)
@@ -624,7 +633,8 @@ class SapContactSolve:
         check(status, "sapb_contact_solve")
         return self.result()
 
-    def _solve_blocked(self, r: SapContactJacobianResult, opts, v_star, v0, v_guess, v_guess_active):
+    def _solve_blocked(self, r: SapContactJacobianResult, opts, v_star, v0, v_guess, v_guess_active,
+                       world_order=None):
         """The tree-blocked solve (sapb_blocked_contact_solve) on the
         tree-blocked result of SapContactJacobian."""
         if r.tree_mass_env is None or r.contact_env_tree is None:
@@ -634,6 +644,7 @@ class SapContactSolve:
         P.num_envs, P.trees_per_env, P.tree_dofs = v.W, v.Bw, 6
         P.max_contacts = int(r.contact_env_jacobian.shape[1])
         P.contact_count, P.tree_mass = _ptr(r.contact_env_count), _ptr(r.tree_mass_env)
+        P.world_order = _ptr(_checked_order(world_order, v.W))
         P.jacobian, P.contact_tree = _ptr(r.contact_env_jacobian), _ptr(r.contact_env_tree)
         P.phi0, P.w_eff, P.mu = _ptr(r.contact_env_phi0), _ptr(r.contact_env_w_eff), _ptr(r.contact_env_mu)
         P.stiffness, P.tau_d = _ptr(r.contact_env_stiffness), _ptr(r.contact_env_tau_d)
@@ -680,7 +691,7 @@ class SolverSAP:
                  static_substep: bool = False, static_substep_iterations: int = 8,
                  static_substep_line_search_iterations: int = 6, position_integration: str | None = None,
                  hessian_precision: str | None = None, warm_start: str = "previous_velocity",
-                 learned_warm_start=None, tree_blocked: bool | None = None):
+                 learned_warm_start=None, tree_blocked: bool | None = None, work_order: str = "previous_iterations"):
         """Keyword arguments of the reference's SolverSAP (sim/solver_sap.py:
         749-791) plus: hessian_precision ("fp64" / "fp32": J^T G J assembly and
         factorization precision; the gradient, cost, line search and
@@ -694,7 +705,11 @@ class SolverSAP:
                                the packaged weights);
         the lowest-cost start among the previous-velocity one and the
         candidates is taken, and Newton always runs to the same tolerance;
-        tree_blocked (None: automatic) selects the tree-blocked layout for
+        work_order ("previous_iterations", the default, or "index"): the
+        order in which the persistent solve kernel takes the worlds -- by the
+        previous step's Newton iterations, most first, so long solves start
+        early instead of trailing at the end of the launch (results do not
+        depend on it); tree_blocked (None: automatic) selects the tree-blocked layout for
         worlds made only of free bodies (default beyond 60 DOFs per world:
         A as 6 x 6 blocks, contact rows over the two touching bodies, a block
         sparse Newton factorization), which takes the previous-velocity warm
@@ -795,6 +810,12 @@ class SolverSAP:
             self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
         if self.warm_start != "previous_velocity":
             self.contact_jacobian.keep_dynamics_factor()
+        self.work_order = str(work_order).strip().lower().replace("-", "_")
+        if self.work_order not in ("previous_iterations", "index"):
+            raise ValueError(f"work_order must be 'previous_iterations' or 'index', got {work_order!r}.")
+        self._world_order = torch.arange(view.W, dtype=I32, device=dev)
+        self._order_keys = torch.zeros(view.W, dtype=I32, device=dev)
+        self._order_idx = torch.zeros(view.W, dtype=torch.int64, device=dev)
         self.reset_runtime_state()
 
     @property
@@ -864,6 +885,8 @@ class SolverSAP:
         self._v_guess_active.zero_()
         if hasattr(self, "_gamma_cand"):
             self._gamma_cand.zero_()
+        if hasattr(self, "_world_order"):
+            torch.arange(self.view.W, dtype=I32, device=self.view.device, out=self._world_order)
         self.last_contacts = None
         self.last_contact_jacobian_result = None
         self.last_contact_solve_result = None
@@ -919,7 +942,12 @@ class SolverSAP:
             optimality_abs_tol=self.optimality_abs_tol, optimality_rel_tol=self.optimality_rel_tol,
             cost_abs_tol=self.cost_abs_tol, cost_rel_tol=self.cost_rel_tol, line_search_max_iterations=ls_iters,
             armijo_c=self.armijo_c, rho=self.rho, line_search_relative_slop=self.line_search_relative_slop,
-            line_search_variant=self.line_search_variant)
+            line_search_variant=self.line_search_variant,
+            world_order=self._world_order if self.work_order == "previous_iterations" else None)
+        if self.work_order == "previous_iterations":
+            # next step's queue: most Newton iterations first (stable: ties keep index order)
+            torch.sort(sr.newton_iterations_env, descending=True, stable=True, out=(self._order_keys, self._order_idx))
+            self._world_order.copy_(self._order_idx)
         mark("integrate")
         # position integration (sim/solver_sap.py:1267-1386)
         mode = _abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint" else _abi.SAPB_INTEGRATE_SAP_EULER
