@@ -902,11 +902,11 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
         line_coefficients<NT, HT, NB>(w, c4);
         LsResult r;
         if constexpr (LSV == SAPB_LS_ARMIJO_DECAY)
-          r = ls_armijo<NT>(w, P, dt, cost, c4);
+          r = ls_armijo<NT, 1>(w, P, dt, cost, c4);
         else if constexpr (LSV == SAPB_LS_EXACT_ROOT)
           r = ls_exact<NT>(w, P, dt, cost, c4);
         else
-          r = ls_monotone<NT>(w, P, dt, cost, c4);
+          r = ls_monotone<NT, 1>(w, P, dt, cost, c4);
         alpha = r.alpha;
         status = r.status;
         constexpr bool mono = LSV == SAPB_LS_MONOTONE_DECAY;

@@ -38,16 +38,13 @@ struct SolveParams {
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// Contacts per G J chunk of the Hessian assembly.
-constexpr int kChunk = 16;
-
 // Shared-memory layout of one world.  ldJ: room for the 4-wide Hessian tiles
 // and odd, so thread-per-row reads of J are free of bank conflicts.  ldH odd
 // for conflict-free column reads in the factorization.
 struct Layout {
   int n, C, ldJ, ldH, nb;
   size_t off_J, off_scr, off_H, off_G, off_vec, off_con, off_flags, off_tri, total;
-  static constexpr int kVecs = 22;
+  static constexpr int kVecs = 23;
   static constexpr int kConPer = 17;
   static constexpr int kMaxWarps = 4;  // partial-sum scratch (blocks of <= 128 threads)
 };
@@ -62,12 +59,11 @@ __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
   size_t o = 0;
   L.off_J = o;
   o = align_up(o + sizeof(double) * (size_t)3 * C * L.ldJ, 16);
-  L.off_scr = o;  // one chunk of G J rows, or the partial sums of the DOF products
+  L.off_scr = o;  // the partial sums of the DOF products, or two staged impulse sets
   {
-    const int ch = C < kChunk ? C : kChunk;
-    const size_t gj = (size_t)hsize * 3 * ch * L.ldJ;
     const size_t part = sizeof(double) * 3 * Layout::kMaxWarps * 64;
-    o = align_up(o + (gj > part ? gj : part), 16);
+    const size_t gam = sizeof(double) * 6 * (size_t)(C > 0 ? C : 1);
+    o = align_up(o + (part > gam ? part : gam), 16);
   }
   L.off_H = o;
   o = align_up(o + (size_t)hsize * n * L.ldH, 16);
@@ -93,7 +89,7 @@ struct World {
   Layout L;
   const double* A;  // global, this world's [n][n]
   double* J;
-  HT* GJ;           // chunk rows, aliased with the partial sums
+  HT* GJ;           // scratch: the partial sums of the DOF products, or staged impulse sets
   HT* H;
   double* G;        // [C][9]
   double* vec;
@@ -302,14 +298,16 @@ __device__ __forceinline__ void load_lower(const World<NT, HT, NS>& w, const dou
 }
 
 // H = A + J^T G J + diag(PD + limit + shift), lower triangle, in HT.
-// G (at the stored vc) and G J are formed chunk by chunk; each thread owns one
-// 4x4 tile of H and one of KS slices of a chunk's rows, accumulates in
-// registers across chunks, and the slices add into H in turn (deterministic).
+// G at the stored vc per contact; each thread owns one 4x4 tile of H and one
+// of KS slices of the contacts and accumulates J_c^T (G_c J_c) for its tile
+// in registers (G J formed per contact for the tile's columns: no staging,
+// no barriers between contacts); the slices of a tile are summed by warp
+// shuffles (KS a power of two) or add into H in turn, in a fixed order
+// (deterministic).
 template <int NT, typename HT, int NS>
 __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) {
   const int tid = threadIdx.x;
   const int n = w.dofs(), ldJ = w.ldJ(), ldH = w.ldH(), nb = w.nb();
-  const int ncol = 4 * nb;
   // G at the current contact velocities (sim/contact_solve.py:1071-1217).
   for (int c = tid; c < w.count; c += NT) {
     double g[3], cost, G[9];
@@ -339,53 +337,65 @@ __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) 
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = HT(0);
-  for (int cb = 0; cb < w.count; cb += kChunk) {
-    const int cn = min(kChunk, w.count - cb);
-    __syncthreads();  // G ready / previous chunk consumed
-    for (int rr = tid; rr < 3 * cn; rr += NT) {
-      const int c = cb + rr / 3, k = rr - 3 * (rr / 3);
+  __syncthreads();  // G ready, H initialised
+  if (has_item) {
+    // this slice's contacts; per contact G J for the tile's 4 columns, then
+    // the tile's rank-3 update J_c[:, 4 bi..]^T (G J_c)[:, 4 bj..]
+    const int per = (w.count + ks - 1) / ks;
+    const int c0 = slice * per, c1 = min(w.count, c0 + per);
+    for (int c = c0; c < c1; ++c) {
       const double* Jc = w.J + (size_t)(3 * c) * ldJ;
-      const double g0 = w.G[9 * c + 3 * k + 0], g1 = w.G[9 * c + 3 * k + 1], g2 = w.G[9 * c + 3 * k + 2];
-      HT* out = w.GJ + (size_t)rr * ldJ;
-      for (int j = 0; j < ncol; ++j) out[j] = HT(g0 * Jc[j] + g1 * Jc[ldJ + j] + g2 * Jc[2 * ldJ + j]);
-    }
-    __syncthreads();
-    if (has_item) {
-      const int rows = 3 * cn;
-      const int per = (rows + ks - 1) / ks;
-      const int r0 = slice * per, r1 = min(rows, r0 + per);
-      for (int r = r0; r < r1; ++r) {
-        const double* jr = w.J + (size_t)(3 * cb + r) * ldJ + 4 * bi;
-        const HT* gr = w.GJ + (size_t)r * ldJ + 4 * bj;
-        HT x[4], y[4];
+      HT ja[3][4], jb[3][4], G[9];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          x[a] = HT(jr[a]);
-          y[a] = gr[a];
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          ja[k][q] = HT(Jc[(size_t)k * ldJ + 4 * bi + q]);
+          jb[k][q] = HT(Jc[(size_t)k * ldJ + 4 * bj + q]);
         }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) G[k] = HT(w.G[9 * c + k]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        HT gj[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gj[q] = G[3 * k] * jb[0][q] + G[3 * k + 1] * jb[1][q] + G[3 * k + 2] * jb[2][q];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
+          for (int q = 0; q < 4; ++q) acc[a][q] += ja[k][a] * gj[q];
       }
     }
   }
-  __syncthreads();  // H init visible
-  for (int s = 0; s < ks; ++s) {
-    if (has_item && slice == s) {
+  auto add_tile = [&]() {
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = 4 * bi + a;
-        if (i >= n) continue;
+    for (int a = 0; a < 4; ++a) {
+      const int i = 4 * bi + a;
+      if (i >= n) continue;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int j = 4 * bj + b;
-          if (j > i || j >= n) continue;
-          w.H[(size_t)i * ldH + j] += acc[a][b];
-        }
+      for (int b = 0; b < 4; ++b) {
+        const int j = 4 * bj + b;
+        if (j > i || j >= n) continue;
+        w.H[(size_t)i * ldH + j] += acc[a][b];
       }
     }
+  };
+  if ((ks & (ks - 1)) == 0) {
+    // the ks slices of a tile are ks consecutive lanes of one warp: sum them
+    // by shuffles (fixed order), slice 0 adds the tile
+    for (int o = ks >> 1; o > 0; o >>= 1) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += __shfl_down_sync(0xffffffffu, acc[a][b], o);
+    }
+    if (has_item && slice == 0) add_tile();
     __syncthreads();
+  } else {
+    for (int s = 0; s < ks; ++s) {
+      if (has_item && slice == s) add_tile();
+      __syncthreads();
+    }
   }
 }
 
@@ -405,27 +415,28 @@ __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   solve_factored<NT, HT, NS>(w);
 }
 
-// dv = -H^-1 grad with the LDL^T that factor_and_solve left in H and V_DINV
-// (one warp; lanes own rows lane, lane + 32).  A pivot that is not
-// positive / finite makes dv NaN.
+// out = -H^-1 rhs (vector slots) with the LDL^T that factor_and_solve left
+// in H and V_DINV, by warp `warp` alone (lanes own rows lane, lane + 32; no
+// block barrier).  A pivot that is not positive / finite makes out NaN.
 template <int NT, typename HT, int NS>
-__device__ void solve_factored(const World<NT, HT, NS>& w) {
+__device__ void solve_warp(const World<NT, HT, NS>& w, int rhs_slot, int out_slot, int warp) {
   const int tid = threadIdx.x;
   const int n = w.dofs(), ldH = w.ldH();
   const HT* H = w.H;
   const HT* dinv = reinterpret_cast<const HT*>(w.V(V_DINV));
-  double* dv = w.V(V_DV);
-  if (tid < 32) {
+  double* dv = w.V(out_slot);
+  const double* rhs = w.V(rhs_slot);
+  if ((tid >> 5) == warp) {
     bool ok = true;
     for (int k = 0; k < n; ++k) {
       const HT d = H[(size_t)k * ldH + k];
       if (!(d > HT(0)) || !isfinite(double(d))) ok = false;
     }
     // Forward z = D^-1 (L^-1 b), backward x = L^-T z; lanes own rows lane, lane+32.
-    const int lane = tid;
+    const int lane = tid & 31;
     HT hb0 = HT(0), hb1 = HT(0);
-    if (lane < n) hb0 = HT(-w.V(V_GRAD)[lane]);
-    if (lane + 32 < n) hb1 = HT(-w.V(V_GRAD)[lane + 32]);
+    if (lane < n) hb0 = HT(-rhs[lane]);
+    if (lane + 32 < n) hb1 = HT(-rhs[lane + 32]);
     for (int k = 0; k < n; ++k) {
       const HT bk = __shfl_sync(0xffffffffu, k < 32 ? hb0 : hb1, k & 31);
       const HT zk = bk * dinv[k];
@@ -454,6 +465,14 @@ __device__ void solve_factored(const World<NT, HT, NS>& w) {
     if (lane < n) dv[lane] = ok ? double(hb0) : nanv;
     if (lane + 32 < n) dv[lane + 32] = ok ? double(hb1) : nanv;
   }
+}
+
+// dv = -H^-1 grad (warp 0), then a block barrier.  (One warp's serial
+// substitution beats a block-wide blocked solve here: the latter's two
+// barriers per block cost more than the warp's chain on the 35-DOF worlds.)
+template <int NT, typename HT, int NS>
+__device__ void solve_factored(const World<NT, HT, NS>& w) {
+  solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
   __syncthreads();
 }
 
@@ -570,24 +589,16 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       const int rows = 3 * count;
       const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n;
       const int ldj = w.ldJ();
-      // Flat copy of the contiguous rows*n block, 4 loads in flight per thread.
+      // Flat copy of the contiguous rows*n block by asynchronous 8-byte
+      // copies (all in flight at once, completed before the barrier after the
+      // per-DOF setup below; the rows land at stride ldj).
       const int total = rows * n;
-      for (int k0 = tid; k0 < total; k0 += 4 * NT) {
-        double val[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int k = k0 + u * NT;
-          val[u] = k < total ? __ldg(Jg + k) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int k = k0 + u * NT;
-          if (k < total) {
-            const int r = k / n, j = k - r * n;
-            w.J[(size_t)r * ldj + j] = val[u];
-          }
-        }
+      for (int k = tid; k < total; k += NT) {
+        const int r = k / n, j = k - r * n;
+        const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(w.J + (size_t)r * ldj + j));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(Jg + k) : "memory");
       }
+      asm volatile("cp.async.commit_group;" ::: "memory");
       // zero padding columns n..ldj-1
       for (int k = tid; k < rows * (ldj - n); k += NT) {
         const int r = k / (ldj - n), j = n + (k - r * (ldj - n));
@@ -690,6 +701,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       }
       w.flags[i] = fl;
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's J copies
     __syncthreads();
     // ---- participating DOFs (sim/contact_solve.py:423-488) ------------------
     // A DOF takes part if a model term acts on it or a contact's body DOF
@@ -769,31 +781,50 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
           factor_and_solve<NT, HT, NS>(w);  // the factor of A (the solve of a zero rhs is unused)
         }
         bool last_is_best = false;
-        for (int k = 0; k < K; ++k) {
-          const double* g0 = P.p.gamma0 + ((size_t)k * P.p.num_envs + e) * C * 3;
-          for (int i = tid; i < n; i += NT) {
-            double acc = 0.0;
-            for (int c = 0; c < count; ++c) {
-              const double* Jc = w.J + (size_t)(3 * c) * ldj;
-              acc += Jc[i] * __ldg(g0 + 3 * c) + Jc[ldj + i] * __ldg(g0 + 3 * c + 1) +
-                     Jc[2 * ldj + i] * __ldg(g0 + 3 * c + 2);
-            }
-            w.V(V_GRAD)[i] = -acc;  // solve_factored solves H dv = -grad
+        // Two sets at a time: stage their impulses in the (here unused)
+        // scratch, form J^T gamma for both (threads 0-63 set k0, 64-127 set
+        // k0+1), solve both with the factor on warps 0 and 1, then evaluate
+        // the candidates in order.
+        double* gs = reinterpret_cast<double*>(w.GJ);
+        for (int k0 = 0; k0 < K; k0 += 2) {
+          const int nk = K - k0 < 2 ? K - k0 : 2;
+          for (int q = tid; q < nk * 3 * count; q += NT) {
+            const int kk = q / (3 * count), r = q - kk * 3 * count;
+            gs[q] = __ldg(P.p.gamma0 + ((size_t)(k0 + kk) * P.p.num_envs + e) * C * 3 + r);
           }
           __syncthreads();
-          solve_factored<NT, HT, NS>(w);
-          for (int i = tid; i < n; i += NT)
-            w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? w.V(V_VSTAR)[i] + w.V(V_DV)[i] : w.V(V_VSTAR)[i];
+          {
+            const int kk = tid >> 6, i = tid & 63;
+            if (kk < nk && i < n) {
+              const double* g = gs + kk * 3 * count;
+              double acc = 0.0;
+              for (int c = 0; c < count; ++c) {
+                const double* Jc = w.J + (size_t)(3 * c) * ldj;
+                acc += Jc[i] * g[3 * c] + Jc[ldj + i] * g[3 * c + 1] + Jc[2 * ldj + i] * g[3 * c + 2];
+              }
+              w.V(kk == 0 ? V_GRAD : V_DP)[i] = -acc;  // the solves give -H^-1 rhs
+            }
+          }
           __syncthreads();
-          double e4c[4];
-          evaluate<NT, HT, NS>(w, P, dt, e4c);
-          last_is_best = false;
-          if (e4c[0] < best_cost) {
-            best_cost = e4c[0];
-            ws_accepted = k + 1;
-            last_is_best = true;
-            for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
-            for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
+          solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
+          if (nk > 1) solve_warp<NT, HT, NS>(w, V_DP, V_DV2, 1);
+          __syncthreads();
+          for (int kk = 0; kk < nk; ++kk) {
+            const int k = k0 + kk;
+            const double* dvk = w.V(kk == 0 ? V_DV : V_DV2);
+            for (int i = tid; i < n; i += NT)
+              w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? w.V(V_VSTAR)[i] + dvk[i] : w.V(V_VSTAR)[i];
+            __syncthreads();
+            double e4c[4];
+            evaluate<NT, HT, NS>(w, P, dt, e4c);
+            last_is_best = false;
+            if (e4c[0] < best_cost) {
+              best_cost = e4c[0];
+              ws_accepted = k + 1;
+              last_is_best = true;
+              for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
+              for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
+            }
           }
         }
         if (last_is_best) {
@@ -845,11 +876,11 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         double c4[4];
         line_coefficients<NT, HT, NS>(w, c4);
         if constexpr (LSV == SAPB_LS_ARMIJO_DECAY)
-          r = ls_armijo<NT>(w, P, dt, cost, c4);
+          r = ls_armijo<NT, 3>(w, P, dt, cost, c4);
         else if constexpr (LSV == SAPB_LS_EXACT_ROOT)
           r = ls_exact<NT>(w, P, dt, cost, c4);
         else
-          r = ls_monotone<NT>(w, P, dt, cost, c4);
+          r = ls_monotone<NT, 3>(w, P, dt, cost, c4);
         alpha = r.alpha;
         status = r.status;
         constexpr bool mono = LSV == SAPB_LS_MONOTONE_DECAY;

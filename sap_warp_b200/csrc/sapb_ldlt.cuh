@@ -105,4 +105,91 @@ __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri)
   }
 }
 
+// x <- -A^-1 x (neg) or A^-1 x with the LDL^T that ldlt_blocked left in H
+// and dinv, by the whole block: forward L z = b, zd = D^-1 z, backward
+// L^T x = zd, over the same blocks as the factorization.  Per block every
+// thread solves the small diagonal system in registers, then threads update
+// the remaining rows (one row each); two barriers per block.  x (FP64 or T)
+// holds the intermediate vectors; the arithmetic is in T.  A pivot that is
+// not positive / finite makes x NaN.  x complete on entry (barrier before)
+// and on return.
+template <int NT, typename T, typename X>
+__device__ void ldlt_solve_blocked(const T* H, int n, int ldH, const T* dinv, X* x, bool neg) {
+  const int tid = threadIdx.x;
+  constexpr int B = sizeof(T) == 4 ? 8 : 6;
+  bool ok = true;
+  for (int k = 0; k < n; ++k) {
+    const T d = H[(size_t)k * ldH + k];
+    if (!(d > T(0)) || !isfinite(double(d))) ok = false;
+  }
+  const T sgn = neg ? T(-1) : T(1);
+  // forward
+  for (int K = 0; K < n; K += B) {
+    const int bs = min(B, n - K);
+    T z[B], R[B];
+#pragma unroll
+    for (int a = 0; a < B; ++a) {
+      R[a] = a < bs ? dinv[K + a] : T(0);
+      T v = a < bs ? T(x[K + a]) : T(0);
+      if (K == 0) v *= sgn;
+#pragma unroll
+      for (int e = 0; e < a; ++e)
+        if (a < bs) v -= H[(size_t)(K + a) * ldH + K + e] * R[e] * z[e];
+      z[a] = v;
+    }
+    __syncthreads();  // every thread has read the block's entries of x
+    if (tid < bs) {
+#pragma unroll
+      for (int a = 0; a < B; ++a)
+        if (a == tid) x[K + a] = X(z[a] * R[a]);
+    }
+    for (int i = K + bs + tid; i < n; i += NT) {
+      T acc = T(x[i]);
+      if (K == 0) acc *= sgn;
+#pragma unroll
+      for (int c = 0; c < B; ++c)
+        if (c < bs) acc -= H[(size_t)i * ldH + K + c] * R[c] * z[c];
+      x[i] = X(acc);
+    }
+    __syncthreads();
+  }
+  // backward
+  const int last = ((n - 1) / B) * B;
+  for (int K = last; K >= 0; K -= B) {
+    const int bs = min(B, n - K);
+    T xb[B];
+#pragma unroll
+    for (int a = B - 1; a >= 0; --a) {
+      if (a >= bs) {
+        xb[a] = T(0);
+        continue;
+      }
+      T v = T(x[K + a]);
+      const T ra = dinv[K + a];
+#pragma unroll
+      for (int c = a + 1; c < B; ++c)
+        if (c < bs) v -= H[(size_t)(K + c) * ldH + K + a] * ra * xb[c];
+      xb[a] = v;
+    }
+    __syncthreads();
+    if (tid < bs) {
+#pragma unroll
+      for (int a = 0; a < B; ++a)
+        if (a == tid) x[K + a] = X(xb[a]);
+    }
+    for (int i = tid; i < K; i += NT) {
+      T acc = T(0);
+#pragma unroll
+      for (int c = 0; c < B; ++c)
+        if (c < bs) acc += H[(size_t)(K + c) * ldH + i] * xb[c];
+      x[i] = X(T(x[i]) - dinv[i] * acc);
+    }
+    __syncthreads();
+  }
+  if (!ok) {
+    for (int i = tid; i < n; i += NT) x[i] = X(__longlong_as_double(0x7ff8000000000000ULL));
+    __syncthreads();
+  }
+}
+
 }  // namespace sapb

@@ -20,7 +20,7 @@ constexpr int kFlagPd = 1, kFlagLo = 2, kFlagUp = 4, kFlagPart = 8;
 // Vector slots inside off_vec (each ldJ doubles).
 enum Vec {
   V_V = 0, V_VSTAR, V_DV, V_GRAD, V_ARES, V_DP, V_DSCALE, V_AINV, V_PDA, V_PDGAIN, V_PDLIM,
-  V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_SAVE, V_BEST, V_DINV, V_END
+  V_LOVHAT, V_UPVHAT, V_LOR, V_UPR, V_LORINV, V_UPRINV, V_HDIAG, V_TMP0, V_SAVE, V_BEST, V_DINV, V_DV2, V_END
 };
 // Contact slots inside off_con (each C doubles).
 enum Con {
@@ -92,54 +92,69 @@ __device__ void line_terms(const W& w, const PP& P, double dt, double alpha, boo
   out3[2] = r[2];
 }
 
-// The regularizer terms of line_terms at four step sizes at once: warp q of
-// each group of four warps evaluates alpha[q], the groups split the contacts
-// and DOFs, lanes stride over them, warp-shuffle sums, one barrier to
-// publish.  reg[q] for every q and the impulse projection onto dv at
-// alpha[0].  (With 128 threads: one group, warp q sums everything.)
-template <int NT, class W, class PP>
-__device__ void line_terms4(const W& w, const PP& P, double dt, const double (&alpha)[4],
-                            double (&reg)[4], double* proj0) {
-  static_assert(NT % 128 == 0, "groups of four warps, one warp per trial step");
+// The regularizer terms of line_terms at 4 KT step sizes at once: warp q of
+// each group of four warps evaluates alpha[q], alpha[q + 4], ...,
+// alpha[q + 4 (KT - 1)] (the same per-step sums and order for any KT), the
+// groups split the contacts and DOFs, lanes stride over them, warp-shuffle
+// sums, one barrier to publish.  reg[k] for every k and the impulse
+// projection onto dv at alpha[0].  (With 128 threads: one group, warp q sums
+// everything.)
+template <int NT, int KT, class W, class PP>
+__device__ void line_termsK(const W& w, const PP& P, double dt, const double (&alpha)[4 * KT],
+                            double (&reg)[4 * KT], double* proj0) {
+  static_assert(NT % 128 == 0, "groups of four warps");
   constexpr int NG = NT / 128;
+  constexpr int NR = 4 * KT + 4;  // reduction slots per group
+  static_assert(NG * NR <= 8 * (NT / 32), "reduction scratch");
   const int tid = threadIdx.x, lane = tid & 31, q = (tid >> 5) & 3, grp = tid >> 7;
   const int first = grp * 32 + lane;
   constexpr int stride = 32 * NG;
-  const double a = alpha[q];
-  double rs = 0.0, ps = 0.0;
+  double a[KT], rs[KT];
+#pragma unroll
+  for (int t = 0; t < KT; ++t) {
+    a[t] = alpha[q + 4 * t];
+    rs[t] = 0.0;
+  }
+  double ps = 0.0;
   for (int c = first; c < w.count; c += stride) {
     const ContactConst cc = w.cc(c);
     const double dx = w.Cn(C_DVC + 0)[c], dy = w.Cn(C_DVC + 1)[c], dz = w.Cn(C_DVC + 2)[c];
-    double g[3], cost;
-    project_contact(cc, w.Cn(C_VC + 0)[c] + a * dx, w.Cn(C_VC + 1)[c] + a * dy, w.Cn(C_VC + 2)[c] + a * dz, g,
-                    &cost, nullptr);
-    rs += cost;
-    ps += g[0] * dx + g[1] * dy + g[2] * dz;
+    const double vx = w.Cn(C_VC + 0)[c], vy = w.Cn(C_VC + 1)[c], vz = w.Cn(C_VC + 2)[c];
+#pragma unroll
+    for (int t = 0; t < KT; ++t) {
+      double g[3], cost;
+      project_contact(cc, vx + a[t] * dx, vy + a[t] * dy, vz + a[t] * dz, g, &cost, nullptr);
+      rs[t] += cost;
+      if (t == 0) ps += g[0] * dx + g[1] * dy + g[2] * dz;
+    }
   }
   if (P.dof.has_pd || P.dof.has_limits) {
     for (int i = first; i < w.dofs(); i += stride) {
-      const double vi = w.V(V_V)[i] + a * w.V(V_DV)[i];
       const double dvi = w.V(V_DV)[i];
       const int fl = w.flags[i];
-      if (P.dof.has_pd && (fl & kFlagPd)) {
-        const double gain = w.V(V_PDGAIN)[i], lim = w.V(V_PDLIM)[i];
-        const double y = w.V(V_PDA)[i] - gain * vi;
-        ps += dvi * dt * clamp_limit(y, lim);
-        if (gain > 0.0) rs += (dt / gain) * clamp_limit_antiderivative(y, lim);
-      }
-      if (P.dof.has_limits) {
-        if (fl & kFlagLo) {
-          const double g = w.V(V_LORINV)[i] * (w.V(V_LOVHAT)[i] - vi);
-          if (g > 0.0) {
-            ps += dvi * g;
-            rs += 0.5 * w.V(V_LOR)[i] * g * g;
-          }
+#pragma unroll
+      for (int t = 0; t < KT; ++t) {
+        const double vi = w.V(V_V)[i] + a[t] * dvi;
+        if (P.dof.has_pd && (fl & kFlagPd)) {
+          const double gain = w.V(V_PDGAIN)[i], lim = w.V(V_PDLIM)[i];
+          const double y = w.V(V_PDA)[i] - gain * vi;
+          if (t == 0) ps += dvi * dt * clamp_limit(y, lim);
+          if (gain > 0.0) rs[t] += (dt / gain) * clamp_limit_antiderivative(y, lim);
         }
-        if (fl & kFlagUp) {
-          const double g = w.V(V_UPRINV)[i] * (w.V(V_UPVHAT)[i] + vi);
-          if (g > 0.0) {
-            ps -= dvi * g;
-            rs += 0.5 * w.V(V_UPR)[i] * g * g;
+        if (P.dof.has_limits) {
+          if (fl & kFlagLo) {
+            const double g = w.V(V_LORINV)[i] * (w.V(V_LOVHAT)[i] - vi);
+            if (g > 0.0) {
+              if (t == 0) ps += dvi * g;
+              rs[t] += 0.5 * w.V(V_LOR)[i] * g * g;
+            }
+          }
+          if (fl & kFlagUp) {
+            const double g = w.V(V_UPRINV)[i] * (w.V(V_UPVHAT)[i] + vi);
+            if (g > 0.0) {
+              if (t == 0) ps -= dvi * g;
+              rs[t] += 0.5 * w.V(V_UPR)[i] * g * g;
+            }
           }
         }
       }
@@ -147,25 +162,27 @@ __device__ void line_terms4(const W& w, const PP& P, double dt, const double (&a
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    rs += __shfl_xor_sync(0xffffffffu, rs, o);
+#pragma unroll
+    for (int t = 0; t < KT; ++t) rs[t] += __shfl_xor_sync(0xffffffffu, rs[t], o);
     ps += __shfl_xor_sync(0xffffffffu, ps, o);
   }
   __syncthreads();  // earlier readers of red are done
   if (lane == 0) {
-    w.red[grp * 8 + q] = rs;
-    w.red[grp * 8 + 4 + q] = ps;
+#pragma unroll
+    for (int t = 0; t < KT; ++t) w.red[grp * NR + 4 * t + q] = rs[t];
+    w.red[grp * NR + 4 * KT + q] = ps;
   }
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < 4 * KT; ++k) {
     double s = w.red[k];
 #pragma unroll
-    for (int g = 1; g < NG; ++g) s += w.red[g * 8 + k];
+    for (int g = 1; g < NG; ++g) s += w.red[g * NR + k];
     reg[k] = s;
   }
-  double p0 = w.red[4];
+  double p0 = w.red[4 * KT];
 #pragma unroll
-  for (int g = 1; g < NG; ++g) p0 += w.red[g * 8 + 4];
+  for (int g = 1; g < NG; ++g) p0 += w.red[g * NR + 4 * KT];
   *proj0 = p0;
 }
 
@@ -179,7 +196,7 @@ __device__ __forceinline__ bool armijo_ok(double alpha, double ell, double ell0,
 }
 
 // armijo_decay backtracking (sim/contact_solve.py:2670-2904, driver :5108-5305).
-template <int NT, class W, class PP>
+template <int NT, int KT, class W, class PP>
 __device__ LsResult ls_armijo(const W& w, const PP& P, double dt, double cost, const double (&c4)[4]) {
   const sapb_solve_options& o = P.o;
   LsResult r{0, 0, 0, 0.0, cost};
@@ -194,12 +211,13 @@ __device__ LsResult ls_armijo(const W& w, const PP& P, double dt, double cost, c
     r.status = SAPB_LS_ASCENT_DIRECTION;
     return r;
   }
-  // Trial steps amax * rho^k, evaluated four at a time (the same products as
+  // Trial steps amax * rho^k, evaluated 4 KT at a time (the same products as
   // the sequential backtracking, so the same decisions).
-  double al[4], rg[4], p0;
+  constexpr int NB = 4 * KT;
+  double al[NB], rg[NB], p0;
   al[0] = alpha;
-  for (int q = 1; q < 4; ++q) al[q] = al[q - 1] * o.rho;
-  line_terms4<NT>(w, P, dt, al, rg, &p0);
+  for (int q = 1; q < NB; ++q) al[q] = al[q - 1] * o.rho;
+  line_termsK<NT, KT>(w, P, dt, al, rg, &p0);
   int base = 0;
   double ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + rg[0];
   const double deriv = dell_a0 + alpha * d2ell_a - p0;
@@ -218,11 +236,11 @@ __device__ LsResult ls_armijo(const W& w, const PP& P, double dt, double cost, c
   if (o.line_search_max_iterations <= 1) return r;
   for (int iteration = 1;; ++iteration) {
     alpha = alpha * o.rho;
-    if (iteration - base >= 4) {
+    if (iteration - base >= NB) {
       base = iteration;
       al[0] = alpha;
-      for (int q = 1; q < 4; ++q) al[q] = al[q - 1] * o.rho;
-      line_terms4<NT>(w, P, dt, al, rg, &p0);
+      for (int q = 1; q < NB; ++q) al[q] = al[q - 1] * o.rho;
+      line_termsK<NT, KT>(w, P, dt, al, rg, &p0);
     }
     ell = mom0 + alpha * dell_a0 + 0.5 * alpha * alpha * d2ell_a + rg[iteration - base];
     const double a = alpha, a_prev = alpha_prev, e_prev = ell_prev;
@@ -260,20 +278,21 @@ __device__ LsResult ls_armijo(const W& w, const PP& P, double dt, double cost, c
 }
 
 // monotone_decay (fused kernel sim/contact_solve.py:2483-2667).
-template <int NT, class W, class PP>
+template <int NT, int KT, class W, class PP>
 __device__ LsResult ls_monotone(const W& w, const PP& P, double dt, double cost, const double (&c4)[4]) {
   const sapb_solve_options& o = P.o;
   LsResult r{0, 0, 0, 1.0, cost};
   const double base_linear = c4[1], base_quadratic = c4[2], base0 = c4[3];
   double alpha = 1.0, trial = cost;
-  double al[4], rg[4], p0;
-  int base = -4;
+  constexpr int NB = 4 * KT;
+  double al[NB], rg[NB], p0;
+  int base = -NB;
   for (int it = 0; it < o.line_search_max_iterations; ++it) {
-    if (it - base >= 4) {  // halvings evaluated four at a time
+    if (it - base >= NB) {  // halvings evaluated 4 KT at a time
       base = it;
       al[0] = alpha;
-      for (int q = 1; q < 4; ++q) al[q] = al[q - 1] * 0.5;
-      line_terms4<NT>(w, P, dt, al, rg, &p0);
+      for (int q = 1; q < NB; ++q) al[q] = al[q - 1] * 0.5;
+      line_termsK<NT, KT>(w, P, dt, al, rg, &p0);
     }
     trial = base0 + alpha * base_linear + 0.5 * alpha * alpha * base_quadratic + rg[it - base];
     r.iterations += 1;

@@ -198,7 +198,7 @@ __device__ __forceinline__ void pose_store(double* p, Xf x) {
 // columns (sim/contact_jacobian.py:404-562).
 __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int tid = threadIdx.x;
   const int e = blockIdx.x;
   const int B = P.m.bodies_per_world, n = P.m.dofs_per_world, C = P.o.max_contacts;
   const int Jw = P.m.joints_per_world;
@@ -552,54 +552,9 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
       if (j <= i) Lg[k] = H[k];
     }
   }
-  if (tid < 32) {
-    // lanes own rows lane + 32 r (n <= 128): forward z = D^-1 L^-1 tau, then x = L^-T z
-    double hb[4], sacc[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = lane + 32 * r;
-      hb[r] = i < n ? tau[i] : 0.0;
-      sacc[r] = 0.0;
-    }
-    for (int k = 0; k < n; ++k) {
-      const int kr = k >> 5;
-      double bk = 0.0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (r == kr) bk = hb[r];
-      bk = __shfl_sync(0xffffffffu, bk, k & 31);
-      const double zk = bk * dinv[k];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int i = lane + 32 * r;
-        if (i == k) hb[r] = zk;
-        else if (i > k && i < n) hb[r] -= H[(size_t)i * n + k] * zk;
-      }
-    }
-    for (int i = n - 1; i >= 0; --i) {
-      const int ir = i >> 5;
-      double xi = 0.0;
-      if (lane == (i & 31)) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-          if (r == ir) {
-            xi = hb[r] - sacc[r] * dinv[i];
-            hb[r] = xi;
-          }
-      }
-      xi = __shfl_sync(0xffffffffu, xi, i & 31);
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int l = lane + 32 * r;
-        if (l < i) sacc[r] += H[(size_t)i * n + l] * xi;
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = lane + 32 * r;
-      if (i < n) vdot[i] = hb[r];
-    }
-  }
+  for (int i = tid; i < n; i += kPrepNT) vdot[i] = tau[i];
+  __syncthreads();
+  ldlt_solve_blocked<kPrepNT, double>(H, n, n, dinv, vdot, false);
   }
   __syncthreads();
   for (int i = tid; i < n; i += kPrepNT) {
