@@ -42,7 +42,7 @@ __host__ __device__ inline size_t prep_align(size_t x) { return (x + 15) / 16 * 
 // ([angular; linear]), so velocities, forces and inertias of different bodies
 // add without shifts.
 struct PrepLayout {
-  size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, dbody, tri, total;
+  size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, par, dbody, tri, total;
 };
 
 __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk) {
@@ -69,9 +69,10 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk)
   L.H = take(sizeof(double) * (blk ? (size_t)36 * B : (size_t)n * n));  // A (tree blocks when blocked)
   L.con = take(sizeof(double) * 21 * Cc);   // per contact: x0 3, x1 3, -, -, frame 9
   L.conint = take(sizeof(int) * 2 * Cc);    // local bodies lb0, lb1
-  L.anc = take(sizeof(uint64_t) * 2 * B);   // ancestor-or-self masks (two buffers)
+  L.anc = take(sizeof(uint64_t) * 2 * B);   // ancestor-or-self masks (two buffers; then bodies by depth)
   L.jmp = take(sizeof(int) * 2 * B);        // pointer-jumping parents (two buffers)
   L.bj = take(sizeof(int) * B);             // joint (global index) of each body, -1
+  L.par = take(sizeof(int) * B);            // parent body, -1
   L.dbody = take(sizeof(int) * n);          // body of each DOF
   L.tri = take(sizeof(uint16_t) * (blk ? 1 : (size_t)(n * (n - 1) / 2 + 1)));  // LDL^T triangle list
   L.total = o;
@@ -191,9 +192,9 @@ __device__ __forceinline__ void pose_store(double* p, Xf x) {
 // (sim/free_motion.py:412-1249, 1804-2178) become: poses by pointer jumping
 // over the parent links (log depth rounds), per-joint motion subspaces and
 // joint velocities in parallel, body velocities / bias accelerations as sums
-// over ancestor masks, subtree forces and composite inertias as sums over
-// descendants, A by the composite-rigid-body pairs H_ij = S_j . (I^c S_i),
-// then a one-barrier-per-column LDL^T and warp-parallel triangular solves.
+// over ancestor masks, subtree forces and composite inertias by one pass
+// from the deepest bodies up, A by the composite-rigid-body pairs H_ij = S_j . (I^c S_i),
+// then a blocked LDL^T (diagonal blocks in registers) and block triangular solves.
 // The contact rows are J_c = R_WC (v_O + w x x_c) of the ancestor DOFs' S
 // columns (sim/contact_jacobian.py:404-562).
 __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams P) {
@@ -227,6 +228,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   int* jmpA = reinterpret_cast<int*>(smem + L.jmp);
   int* jmpB = jmpA + B;
   int* bj = reinterpret_cast<int*>(smem + L.bj);
+  int* par = reinterpret_cast<int*>(smem + L.par);
   int* dbody = reinterpret_cast<int*>(smem + L.dbody);
   uint16_t* tri = reinterpret_cast<uint16_t*>(smem + L.tri);
   const int j0 = e * Jw, b0g = e * B, d0 = e * n;
@@ -278,6 +280,7 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     pose_store(poseA + 8 * b, T);
     pose_store(fm + 8 * b, X_FM);
     jmpA[b] = parent;
+    par[b] = parent;
     ancA[b] = 1ull << b;
   }
   __syncthreads();
@@ -316,8 +319,20 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
   }
   const double* pose = cur;
   const uint64_t* anc = ac;
+  // bodies by descending depth (children before their parents; equal depths
+  // by index) for the subtree sums, in the pointer-jumping buffer left free
+  int* deep_order = reinterpret_cast<int*>(an);
 
   // ---- motion subspaces, joint velocities, body inertias ------------------
+  for (int b = tid; b < B; b += kPrepNT) {
+    const int db = __popcll(anc[b]);  // depth + 1
+    int rank = 0;
+    for (int d = 0; d < B; ++d) {
+      const int dd = __popcll(anc[d]);
+      rank += (dd > db || (dd == db && d < b)) ? 1 : 0;
+    }
+    deep_order[rank] = b;
+  }
   // S in world-origin coordinates of the reference's mobilizer columns
   // (sim/sap_helpers.py:1289-1433): revolute [w; p_F x w], prismatic [0; a],
   // ball [w_k; p_F x w_k], free [w_k; p_M x w_k] and [0; a_k], all axes
@@ -436,13 +451,19 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     sv_store(fb + 6 * b, f);
   }
   __syncthreads();
-  // ---- subtree forces and composite inertias --------------------------------
+  // ---- subtree forces and composite inertias: own values, then one pass
+  // from the deepest bodies up, each adding its subtree into its parent
   for (int k = tid; k < 16 * B; k += kPrepNT) {
     const int b = k >> 4, comp = k & 15;
-    double acc = 0.0;
-    for (int d = 0; d < B; ++d)
-      if ((anc[d] >> b) & 1ull) acc += comp < 6 ? fb[6 * d + comp] : ib[10 * d + comp - 6];
-    fs[16 * b + comp] = acc;
+    fs[k] = comp < 6 ? fb[6 * b + comp] : ib[10 * b + comp - 6];
+  }
+  __syncthreads();
+  for (int comp = tid; comp < 16; comp += kPrepNT) {
+    for (int idx = 0; idx < B; ++idx) {
+      const int b = deep_order[idx];
+      const int p = par[b];
+      if (p >= 0) fs[16 * p + comp] += fs[16 * b + comp];
+    }
   }
   __syncthreads();
   // ---- tau = joint_f - S^T f_subtree, F_i = I^c S_i (sim/sap_helpers.py:2090-2118)
