@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 4
+#define SAPB_ABI_VERSION 5
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -313,6 +313,35 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* model, const sapb_step_
 int32_t sapb_integrate_positions(const sapb_model_desc* model, const double* joint_q_in, const double* v_prev,
                                  const double* v_new, const double* dt, int32_t mode, double* joint_q_out,
                                  void* stream);
+
+/* ---- public-order boundary ------------------------------------------------
+ * Newton-style callers hold joint velocities / forces in the public order
+ * (free and distance joints: [v_com; w] and [f; tau_com]) and body forces as
+ * [f; tau] at the COM; the step runs in SAP order ([w; v_origin], body-origin
+ * wrenches).  These restate the boundary of SolverSAP.step
+ * (sim/solver_sap.py:1198-1261, 1467-1469).  All arrays FP64, device. */
+
+/* Public -> SAP order (copy_public_to_sap_velocity_f64_from_joint_pose,
+ * _copy_public_to_sap_force_kernel_f64_from_joint_pose and
+ * _copy_public_body_force_to_sap_body_origin_kernel, sim/sap_helpers.py:
+ * 1481-1622, 1811-2095).  joint_q [coords] gives the free joints' rotation;
+ * body_q [B][7] the bodies' (for body forces).  Any of the three public
+ * inputs may be NULL (its output is then not written). */
+int32_t sapb_public_to_sap(const sapb_model_desc* model, const double* joint_q, const double* body_q,
+                           const double* joint_qd_public, const double* joint_f_public,
+                           const double* body_f_public, double* joint_qd_sap, double* joint_f_sap,
+                           double* body_f_sap, void* stream);
+
+/* SAP -> public joint velocities with the pose joint_q
+ * (_copy_sap_to_public_velocity_f64_from_joint_pose, sim/sap_helpers.py:1711-1760). */
+int32_t sapb_sap_to_public_velocity(const sapb_model_desc* model, const double* joint_q,
+                                    const double* joint_qd_sap, double* joint_qd_public, void* stream);
+
+/* Forward kinematics of public coordinates: body poses [B][7] and public body
+ * velocities [B][6] ([v; w], may be NULL) articulation by articulation
+ * (sap_eval_fk, sim/sap_kinematics.py:85-341; FP64 here, FP32 there). */
+int32_t sapb_eval_fk(const sapb_model_desc* model, const double* joint_q, const double* joint_qd_public,
+                     double* body_q, double* body_qd, void* stream);
 
 /* Fill the reference defaults of SapContactSolve for a line-search variant.
  * Replaces the Python defaults of solve(), sim/contact_solve.py:6129-6182. */

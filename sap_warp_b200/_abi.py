@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 4
+SAPB_ABI_VERSION = 5
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -308,6 +308,9 @@ EXPORTS = {
         [C.POINTER(ModelDesc), C.POINTER(StepInputs), C.POINTER(PrepareOptions), C.POINTER(PrepareOutputs), _p,
          C.c_size_t, _p],
     ),
+    "sapb_public_to_sap": (C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "sapb_sap_to_public_velocity": (C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p]),
+    "sapb_eval_fk": (C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, _p]),
     "sapb_integrate_positions": (
         C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, C.c_int32, _p, _p]
     ),

@@ -257,6 +257,43 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inpu
   return sapb::prepare_launch(m, in, o, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
+int32_t sapb_public_to_sap(const sapb_model_desc* m, const double* joint_q, const double* body_q,
+                           const double* joint_qd_public, const double* joint_f_public,
+                           const double* body_f_public, double* joint_qd_sap, double* joint_f_sap,
+                           double* body_f_sap, void* stream) {
+  const int32_t st = check_model(m, "sapb_public_to_sap");
+  if (st != SAPB_OK) return st;
+  if ((joint_qd_public && !joint_qd_sap) || (joint_f_public && !joint_f_sap) || (body_f_public && !body_f_sap) ||
+      ((joint_qd_public || joint_f_public) && !joint_q) || (body_f_public && !body_q)) {
+    sapb::set_last_error("sapb_public_to_sap: an input without its output or pose array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::public_to_sap_launch(m, joint_q, body_q, joint_qd_public, joint_f_public, body_f_public, joint_qd_sap,
+                                    joint_f_sap, body_f_sap, static_cast<cudaStream_t>(stream));
+}
+
+int32_t sapb_sap_to_public_velocity(const sapb_model_desc* m, const double* joint_q, const double* joint_qd_sap,
+                                    double* joint_qd_public, void* stream) {
+  const int32_t st = check_model(m, "sapb_sap_to_public_velocity");
+  if (st != SAPB_OK) return st;
+  if (!joint_q || !joint_qd_sap || !joint_qd_public) {
+    sapb::set_last_error("sapb_sap_to_public_velocity: missing array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::sap_to_public_launch(m, joint_q, joint_qd_sap, joint_qd_public, static_cast<cudaStream_t>(stream));
+}
+
+int32_t sapb_eval_fk(const sapb_model_desc* m, const double* joint_q, const double* joint_qd_public, double* body_q,
+                     double* body_qd, void* stream) {
+  const int32_t st = check_model(m, "sapb_eval_fk");
+  if (st != SAPB_OK) return st;
+  if (!joint_q || !body_q || (body_qd && !joint_qd_public)) {
+    sapb::set_last_error("sapb_eval_fk: missing array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::eval_fk_launch(m, joint_q, joint_qd_public, body_q, body_qd, static_cast<cudaStream_t>(stream));
+}
+
 int32_t sapb_integrate_positions(const sapb_model_desc* m, const double* q_in, const double* v_prev,
                                  const double* v_new, const double* dt, int32_t mode, double* q_out, void* stream) {
   const int32_t st = check_model(m, "sapb_integrate_positions");

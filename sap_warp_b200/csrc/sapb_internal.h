@@ -26,6 +26,14 @@ int32_t blocked_solve_launch(const sapb_blocked_problem* p, const sapb_solve_opt
 int32_t dense_to_blocked_launch(const sapb_contact_problem* d, int T, int NB, double* tree_mass, double* jac,
                                 int32_t* contact_tree, cudaStream_t stream);
 
+int32_t public_to_sap_launch(const sapb_model_desc* m, const double* joint_q, const double* body_q,
+                             const double* qd_pub, const double* f_pub, const double* bf_pub, double* qd_sap,
+                             double* f_sap, double* bf_sap, cudaStream_t stream);
+int32_t sap_to_public_launch(const sapb_model_desc* m, const double* joint_q, const double* qd_sap, double* qd_pub,
+                             cudaStream_t stream);
+int32_t eval_fk_launch(const sapb_model_desc* m, const double* joint_q, const double* qd_pub, double* body_q,
+                       double* body_qd, cudaStream_t stream);
+
 size_t prepare_smem_bytes(int B, int n, int C, bool tree_blocked);
 int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, const sapb_prepare_options* o,
                        const sapb_prepare_outputs* out, void* workspace, size_t workspace_bytes,

@@ -784,6 +784,15 @@ class SolverSAP:
         dev = view.device
         self._v_guess_active = torch.zeros(1, dtype=I32, device=dev)
         self._q_out_tmp = torch.zeros(int(model.joint_coord_count), dtype=F64, device=dev)
+        # public-order boundary (sim/solver_sap.py:1198-1261): SAP-order copies of
+        # public inputs, and FP64 staging of public outputs
+        D, Bt = int(model.joint_dof_count), int(model.body_count)
+        self._qd_sap_in = torch.zeros(D, dtype=F64, device=dev)
+        self._f_sap_in = torch.zeros(D, dtype=F64, device=dev)
+        self._bf_sap_in = torch.zeros(Bt, 6, dtype=F64, device=dev)
+        self._qd_pub_out = torch.zeros(D, dtype=F64, device=dev)
+        self._body_q_out = torch.zeros(Bt, 7, dtype=F64, device=dev)
+        self._body_qd_out = torch.zeros(Bt, 6, dtype=F64, device=dev)
         self.stage_events = None  # list -> per-stage CUDA events (see _mark)
         self.warm_start = str(warm_start).strip().lower().replace("-", "_")
         if self.warm_start not in ("previous_velocity", "previous_impulses", "learned"):
@@ -911,8 +920,9 @@ class SolverSAP:
         self.contact_jacobian.set_dt(dt)
         self.last_contacts = contacts
         mark = self._mark
+        solve_state, solve_control, output_public = self._boundary_in(state_in, state_out, control)
         mark("free_motion")
-        cr = self.contact_jacobian.compute(state_in, contacts, control=control)
+        cr = self.contact_jacobian.compute(solve_state, contacts, control=solve_control)
         if self.static_substep:
             iters, ls_iters = self.static_substep_iterations, self.static_substep_line_search_iterations
         else:
@@ -936,7 +946,7 @@ class SolverSAP:
             gamma0 = self._gamma_cand
         mark("contact_solve")
         sr = self.contact_solve.solve(
-            cr, state_in, control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
+            cr, solve_state, solve_control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
             v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, gamma0=gamma0,
             max_iterations=iters,
             optimality_abs_tol=self.optimality_abs_tol, optimality_rel_tol=self.optimality_rel_tol,
@@ -961,7 +971,10 @@ class SolverSAP:
         check(status, "sapb_integrate_positions")
         if q_out is not state_out.joint_q:
             state_out.joint_q.copy_(q_out)
-        state_out.joint_qd.copy_(sr.v_flat)
+        if output_public:
+            self._boundary_out(state_out, q_out, sr.v_flat)
+        else:
+            state_out.joint_qd.copy_(sr.v_flat)
         if state_out.body_f is not None and state_in.body_f is not None and state_out.body_f is not state_in.body_f:
             state_out.body_f.copy_(state_in.body_f)
         mark(None)
@@ -977,6 +990,51 @@ class SolverSAP:
             self.sim_time += float(dt)
         self.frame_id += 1
         return state_out
+
+    def _boundary_in(self, state_in: SapState, state_out: SapState, control: SapControl | None):
+        """Public-order inputs -> SAP order (sim/solver_sap.py:1198-1261):
+        returns the SAP-order state and control the step runs on, and whether
+        the output is public."""
+        lib, stream = load(), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)
+        desc = ctypes.byref(self.view.desc)
+        if getattr(state_in, "joint_qd_order", "sap") == "public":
+            q = _f64(state_in.joint_q)
+            bf_pub = None
+            if state_in.body_f is not None and getattr(state_in, "body_f_order", "sap") == "public":
+                bf_pub = _f64(state_in.body_f.reshape(-1, 6))
+            bq = _f64(state_in.body_q.reshape(-1, 7)) if bf_pub is not None else None
+            check(lib.sapb_public_to_sap(desc, _ptr(q), _ptr(bq), _ptr(_f64(state_in.joint_qd)), None,
+                                         _ptr(bf_pub), _ptr(self._qd_sap_in), None, _ptr(self._bf_sap_in), stream),
+                  "sapb_public_to_sap")
+            state_in = SapState(joint_q=state_in.joint_q, joint_qd=self._qd_sap_in, body_q=state_in.body_q,
+                                body_qd=getattr(state_in, "body_qd", None),
+                                body_f=self._bf_sap_in if bf_pub is not None else state_in.body_f,
+                                joint_qd_order="sap", body_f_order="sap")
+        if control is not None and getattr(control, "joint_f_order", "sap") == "public" and control.joint_f is not None:
+            q = _f64(state_in.joint_q)
+            check(lib.sapb_public_to_sap(desc, _ptr(q), None, None, _ptr(_f64(control.joint_f)), None, None,
+                                         _ptr(self._f_sap_in), None, stream), "sapb_public_to_sap")
+            control = SapControl(joint_f=self._f_sap_in, joint_target_pos=control.joint_target_pos,
+                                 joint_target_vel=control.joint_target_vel, joint_act=control.joint_act,
+                                 joint_f_order="sap")
+        return state_in, control, getattr(state_out, "joint_qd_order", "sap") == "public"
+
+    def _boundary_out(self, state_out: SapState, q_out: torch.Tensor, v_sap: torch.Tensor) -> None:
+        """SAP-order result -> public output (sim/solver_sap.py:1467-1469): the
+        public joint velocities at the new pose, then the forward kinematics
+        of the new public coordinates into body_q / body_qd."""
+        lib, stream = load(), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)
+        desc = ctypes.byref(self.view.desc)
+        check(lib.sapb_sap_to_public_velocity(desc, _ptr(q_out), _ptr(v_sap), _ptr(self._qd_pub_out), stream),
+              "sapb_sap_to_public_velocity")
+        state_out.joint_qd.copy_(self._qd_pub_out)
+        want_qd = getattr(state_out, "body_qd", None) is not None
+        check(lib.sapb_eval_fk(desc, _ptr(q_out), _ptr(self._qd_pub_out), _ptr(self._body_q_out),
+                               _ptr(self._body_qd_out) if want_qd else None, stream), "sapb_eval_fk")
+        if state_out.body_q is not None:
+            state_out.body_q.copy_(self._body_q_out.reshape(state_out.body_q.shape))
+        if want_qd:
+            state_out.body_qd.copy_(self._body_qd_out.reshape(state_out.body_qd.shape))
 
     def update_contacts(self, contacts: SapContacts) -> None:
         raise NotImplementedError("SolverSAP does not expose contact-force writeback yet.")
