@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 5
+#define SAPB_ABI_VERSION 6
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -342,6 +342,54 @@ int32_t sapb_sap_to_public_velocity(const sapb_model_desc* model, const double* 
  * (sap_eval_fk, sim/sap_kinematics.py:85-341; FP64 here, FP32 there). */
 int32_t sapb_eval_fk(const sapb_model_desc* model, const double* joint_q, const double* joint_qd_public,
                      double* body_q, double* body_qd, void* stream);
+
+/* ---- contact generation for primitive shapes ------------------------------
+ * Planes, spheres and boxes: plane-sphere, plane-box (corners), sphere-sphere,
+ * sphere-box (closest point), box-box (corners against faces, both ways; no
+ * edge-edge).  Writes the flat contact buffer as the reference's
+ * sap_write_contact does (sim/collision/pipeline.py:52-118): shape pair,
+ * witness points in the body frames of their shapes (world frame for static
+ * shapes), unit normal from shape0 to shape1, margins (a sphere's radius is
+ * in its margin, its witness point the centre).  A covering of the synthetic
+ * scenes' pairs, not the reference's general narrow phase (GJK / MPR,
+ * meshes, SDFs, contact reduction).  Deterministic order: pairs by world,
+ * then shape index, contacts of a pair in a fixed order. */
+#define SAPB_SHAPE_PLANE 0
+#define SAPB_SHAPE_SPHERE 1
+#define SAPB_SHAPE_BOX 2
+
+typedef struct sapb_collision_shapes {
+  int32_t num_worlds;
+  int32_t shapes_per_world;         /* local shapes, contiguous per world */
+  int32_t num_global_shapes;        /* static shapes after all worlds' shapes, met by every world (the ground) */
+  const int32_t* shape_type;        /* [S] SAPB_SHAPE_* */
+  const double* shape_scale;        /* [S][3] sphere radius in [0]; box half extents */
+  const double* shape_X_bs;         /* [S][7] shape frame in its body frame (world frame for static shapes);
+                                       a plane is z = 0 of its frame with normal +z */
+  const int32_t* shape_body;        /* [S] body, -1 static */
+  const double* shape_margin;       /* [S] or NULL */
+  double gap;                       /* emit contacts whose signed distance is below gap */
+} sapb_collision_shapes;
+
+typedef struct sapb_contact_outputs {
+  int32_t capacity;
+  int32_t* count;                   /* [1] contacts written (clamped to capacity) */
+  int32_t* shape0;                  /* [capacity] */
+  int32_t* shape1;
+  double* point0;                   /* [capacity][3] */
+  double* point1;
+  double* normal;
+  double* margin0;                  /* [capacity] */
+  double* margin1;
+} sapb_contact_outputs;
+
+/* Device workspace bytes of sapb_generate_contacts. */
+size_t sapb_contacts_workspace_size(const sapb_collision_shapes* shapes);
+
+/* Contacts of every world at the body poses body_q [B][7] (device). */
+int32_t sapb_generate_contacts(const sapb_collision_shapes* shapes, const double* body_q,
+                               const sapb_contact_outputs* out, void* workspace, size_t workspace_bytes,
+                               void* stream);
 
 /* Fill the reference defaults of SapContactSolve for a line-search variant.
  * Replaces the Python defaults of solve(), sim/contact_solve.py:6129-6182. */

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 5
+SAPB_ABI_VERSION = 6
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -142,6 +142,37 @@ class BlockedProblem(C.Structure):
         ("v_guess_active", _p),
         ("dt", _p),
         ("world_order", _p),
+    ]
+
+
+SAPB_SHAPE_PLANE, SAPB_SHAPE_SPHERE, SAPB_SHAPE_BOX = 0, 1, 2
+
+
+class CollisionShapes(C.Structure):
+    _fields_ = [
+        ("num_worlds", C.c_int32),
+        ("shapes_per_world", C.c_int32),
+        ("num_global_shapes", C.c_int32),
+        ("shape_type", _p),
+        ("shape_scale", _p),
+        ("shape_X_bs", _p),
+        ("shape_body", _p),
+        ("shape_margin", _p),
+        ("gap", C.c_double),
+    ]
+
+
+class ContactOutputs(C.Structure):
+    _fields_ = [
+        ("capacity", C.c_int32),
+        ("count", _p),
+        ("shape0", _p),
+        ("shape1", _p),
+        ("point0", _p),
+        ("point1", _p),
+        ("normal", _p),
+        ("margin0", _p),
+        ("margin1", _p),
     ]
 
 
@@ -311,6 +342,10 @@ EXPORTS = {
     "sapb_public_to_sap": (C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "sapb_sap_to_public_velocity": (C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p]),
     "sapb_eval_fk": (C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, _p]),
+    "sapb_contacts_workspace_size": (C.c_size_t, [C.POINTER(CollisionShapes)]),
+    "sapb_generate_contacts": (
+        C.c_int32, [C.POINTER(CollisionShapes), _p, C.POINTER(ContactOutputs), _p, C.c_size_t, _p]
+    ),
     "sapb_integrate_positions": (
         C.c_int32, [C.POINTER(ModelDesc), _p, _p, _p, _p, C.c_int32, _p, _p]
     ),

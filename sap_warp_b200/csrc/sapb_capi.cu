@@ -294,6 +294,39 @@ int32_t sapb_eval_fk(const sapb_model_desc* m, const double* joint_q, const doub
   return sapb::eval_fk_launch(m, joint_q, joint_qd_public, body_q, body_qd, static_cast<cudaStream_t>(stream));
 }
 
+size_t sapb_contacts_workspace_size(const sapb_collision_shapes* shapes) {
+  if (!shapes || shapes->num_worlds < 0 || shapes->shapes_per_world < 0 || shapes->num_global_shapes < 0) return 0;
+  return sapb::contacts_workspace_bytes(shapes);
+}
+
+int32_t sapb_generate_contacts(const sapb_collision_shapes* sh, const double* body_q, const sapb_contact_outputs* out,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  if (!sh || !out || !out->count || sh->num_worlds < 0 || sh->shapes_per_world < 0 || sh->num_global_shapes < 0 ||
+      out->capacity < 0) {
+    sapb::set_last_error("sapb_generate_contacts: bad arguments");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (sh->shapes_per_world > 4096) {
+    sapb::set_last_error("sapb_generate_contacts: shapes_per_world=%d > 4096", sh->shapes_per_world);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if ((sh->num_worlds * sh->shapes_per_world + sh->num_global_shapes) > 0 &&
+      (!sh->shape_type || !sh->shape_scale || !sh->shape_X_bs || !sh->shape_body || !body_q)) {
+    sapb::set_last_error("sapb_generate_contacts: missing shape array or body poses");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (out->capacity > 0 && (!out->shape0 || !out->shape1 || !out->point0 || !out->point1 || !out->normal ||
+                            !out->margin0 || !out->margin1)) {
+    sapb::set_last_error("sapb_generate_contacts: missing output array");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (!workspace || workspace_bytes < sapb::contacts_workspace_bytes(sh)) {
+    sapb::set_last_error("sapb_generate_contacts: workspace missing or smaller than sapb_contacts_workspace_size");
+    return SAPB_ERR_WORKSPACE_TOO_SMALL;
+  }
+  return sapb::contacts_launch(sh, body_q, out, workspace, static_cast<cudaStream_t>(stream));
+}
+
 int32_t sapb_integrate_positions(const sapb_model_desc* m, const double* q_in, const double* v_prev,
                                  const double* v_new, const double* dt, int32_t mode, double* q_out, void* stream) {
   const int32_t st = check_model(m, "sapb_integrate_positions");

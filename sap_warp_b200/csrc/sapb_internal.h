@@ -34,6 +34,10 @@ int32_t sap_to_public_launch(const sapb_model_desc* m, const double* joint_q, co
 int32_t eval_fk_launch(const sapb_model_desc* m, const double* joint_q, const double* qd_pub, double* body_q,
                        double* body_qd, cudaStream_t stream);
 
+size_t contacts_workspace_bytes(const sapb_collision_shapes* s);
+int32_t contacts_launch(const sapb_collision_shapes* s, const double* body_q, const sapb_contact_outputs* out,
+                        void* workspace, cudaStream_t stream);
+
 size_t prepare_smem_bytes(int B, int n, int C, bool tree_blocked);
 int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, const sapb_prepare_options* o,
                        const sapb_prepare_outputs* out, void* workspace, size_t workspace_bytes,

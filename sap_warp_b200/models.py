@@ -362,12 +362,14 @@ def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20)
     rows = []  # (world, shape0, shape1, x1 world, normal, lower body or -1, upper body)
     pos_all = np.zeros((E, B, 3))
     R_all = np.zeros((E, B, 3, 3))
+    dims_all = np.zeros((E, B, 3))
     for e in range(E):
         S = int(rng.integers(sites[0], sites[1] + 1))
         grid = int(np.ceil(np.sqrt(S)))
         site_xy = np.stack([(np.arange(S) % grid) * 0.35, (np.arange(S) // grid) * 0.35], -1)
         site_of = rng.integers(0, S, size=B)
         dims = rng.uniform(*size_range, size=(B, 3))
+        dims_all[e] = dims
         mass = rng.uniform(*density_range, size=B) * dims.prod(-1)
         yaw = rng.uniform(-0.3, 0.3, size=B)
         R = _axis_angle(np.array([0.0, 0.0, 1.0]), yaw)
@@ -447,4 +449,24 @@ def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20)
                      body_q=model.body_q.clone(),
                      body_f=torch.zeros(model.body_count, 6, dtype=torch.float64, device=device))
     control = SapControl(joint_f=torch.zeros(model.joint_dof_count, dtype=torch.float64, device=device))
-    return model, state, control, contacts_to_torch(con, device), con, dict(tpl=tpl, g=g, q=q, qd=qd)
+    return model, state, control, contacts_to_torch(con, device), con, dict(tpl=tpl, g=g, q=q, qd=qd, dims=dims_all)
+
+
+def box_shapes(host: dict):
+    """collision.ShapeSet of a box_scene: one box shape per body (centred half
+    a height above the body origin, which sits at the bottom face) and a
+    static ground plane z = 0 shared by all worlds."""
+    from .collision import ShapeSet
+    from ._abi import SAPB_SHAPE_BOX, SAPB_SHAPE_PLANE
+
+    dims = host["dims"]
+    E, B = dims.shape[:2]
+    X = np.zeros((E * B + 1, 7))
+    X[:, 6] = 1.0
+    X[:E * B, 2] = 0.5 * dims.reshape(-1, 3)[:, 2]
+    scale = np.zeros((E * B + 1, 3))
+    scale[:E * B] = 0.5 * dims.reshape(-1, 3)
+    return ShapeSet(num_worlds=E, shapes_per_world=B, num_global_shapes=1,
+                    shape_type=np.concatenate([np.full(E * B, SAPB_SHAPE_BOX), [SAPB_SHAPE_PLANE]]).astype(np.int32),
+                    shape_scale=scale, shape_X_bs=X,
+                    shape_body=np.concatenate([np.arange(E * B), [-1]]).astype(np.int32))
