@@ -386,7 +386,11 @@ typedef struct sapb_contact_outputs {
 /* Device workspace bytes of sapb_generate_contacts. */
 size_t sapb_contacts_workspace_size(const sapb_collision_shapes* shapes);
 
-/* Contacts of every world at the body poses body_q [B][7] (device). */
+/* Contacts of every world at the body poses body_q [B][7] (device), in the
+ * format the reference's collision pipeline writes with sap_write_contact
+ * (sim/collision/pipeline.py:52-118); the primitive pairs of
+ * sim/collision/primitive.py (plane-sphere :89-97, sphere-sphere :99-130,
+ * plane-box :354-428, sphere-box :1150-1205; box-box as vertex-face). */
 int32_t sapb_generate_contacts(const sapb_collision_shapes* shapes, const double* body_q,
                                const sapb_contact_outputs* out, void* workspace, size_t workspace_bytes,
                                void* stream);
