@@ -24,10 +24,11 @@ __device__ __forceinline__ void build_triangle_list(uint16_t* tri, int n) {
 // In-place right-looking LDL^T of the lower triangle of H (row stride ldH):
 // afterwards H_ik = L_ik d_k below the diagonal (L unit lower), d_k on it,
 // dinv[k] = 1/d_k.  8-column blocks (6 in FP64), two barriers per block:
-// every thread factors the block's diagonal block in registers (it is final
-// once the previous trailing update is done), threads below bs write its rows,
-// the rows under it (the panel) are solved against it in registers, one per
-// thread; then the trailing update.  The arithmetic is the right-looking
+// every thread factors the block's diagonal block in
+// registers (it is final once the previous trailing update is done), the rows
+// under it (the panel) are solved against it in registers, one per thread;
+// after the panel's barrier threads below bs write the block's rows back
+// while the trailing update runs.  The arithmetic is the right-looking
 // recurrence on the stored form W_ik = L_ik d_k:
 //   d_k = H_kk - sum_{e<k} W_ke^2 / d_e,  W_ik = H_ik - sum_{e<k} W_ie W_ke / d_e.
 // H must be complete when called (barrier before); complete on return.
@@ -60,16 +61,23 @@ __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri)
         W[a][b] = v;
       }
     }
-    if (tid < bs) {
+    // The factored rows go back to H only once every thread has read the
+    // block: after the panel's barrier (the trailing update never touches
+    // the diagonal block), or after a barrier of its own for the last block.
+    auto store_block = [&]() {
+      if (tid < bs) {
 #pragma unroll
-      for (int a = 0; a < B; ++a) {
-        if (a != tid) continue;
+        for (int a = 0; a < B; ++a) {
+          if (a != tid) continue;
 #pragma unroll
-        for (int b = 0; b <= a; ++b) H[(size_t)(K + a) * ldH + K + b] = W[a][b];
-        dinv[K + a] = R[a];
+          for (int b = 0; b <= a; ++b) H[(size_t)(K + a) * ldH + K + b] = W[a][b];
+          dinv[K + a] = R[a];
+        }
       }
-    }
+    };
     if (rest <= 0) {
+      __syncthreads();
+      store_block();
       __syncthreads();
       break;
     }
@@ -89,6 +97,7 @@ __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri)
       }
     }
     __syncthreads();
+    store_block();
     // (3) trailing update of entries (i, j), j >= K + bs: the first
     // rest*(rest+1)/2 entries of the column-descending triangle list.
     const int cnt = rest * (rest + 1) / 2;

@@ -37,3 +37,23 @@ def test_graph_replay_matches_eager_steps(cuda_device, warm_start, precision):
     assert torch.equal(ga.joint_q, ea.joint_q) and torch.equal(ga.joint_qd, ea.joint_qd)
     assert bool(graphed.contact_solve.converged_env.all())
     del graph
+
+
+def test_learned_fp32_rollouts_repeat_bit_for_bit(cuda_device):
+    """Two solvers stepping the same 4096 worlds (learned warm start, FP32
+    factor: the fastest factor, so the one where a shared-memory race in the
+    blocked LDL^T would show first) give identical trajectories."""
+    def run():
+        model, state, control, contacts, _ = models.rollout_scene("humanoid", 4096, 20240, cuda_device)
+        solver = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32",
+                           warm_start="learned")
+        a, b = pair(state)
+        out = []
+        for _ in range(40):
+            solver.step(a, b, control, contacts, 2.0e-3)
+            out.append(b.joint_qd.clone())
+            a, b = b, a
+        return out
+    r1, r2 = run(), run()
+    first = next((k for k in range(len(r1)) if not torch.equal(r1[k], r2[k])), None)
+    assert first is None, f"the rollouts part at step {first}"
