@@ -360,14 +360,40 @@ def main():
                plain["final"].joint_qd.abs().max().clamp(min=1e-30))
 
     # ---- end to end through the public API with host buffers -----------------
+    # Every step copies its state (joint_q, joint_qd) and its contacts from
+    # pinned host memory and its new state back to the host.  Headline: two
+    # whole steps and their copies in one graph (capture_host_steps), each
+    # step's contacts copied while the step before it computes.  Beside it:
+    # the same copies and eager steps serialised on one stream.
+    from sap_warp_b200.runtime import SapContacts
+
+    c_names = [k for k in vars(contacts) if isinstance(getattr(contacts, k), torch.Tensor)]
+    host_state = {"joint_q": state0.joint_q.cpu().pin_memory(), "joint_qd": state0.joint_qd.cpu().pin_memory()}
+    host_cs = tuple(SapContacts(**{k: getattr(contacts, k).cpu().pin_memory() for k in c_names}) for _ in range(2))
+    h2d = (host_state["joint_q"].numel() * 8 + host_state["joint_qd"].numel() * 8
+           + sum(getattr(host_cs[0], k).numel() * getattr(host_cs[0], k).element_size() for k in c_names))
+    d2h = host_state["joint_q"].numel() * 8 + host_state["joint_qd"].numel() * 8
+    solver = make_solver("fp32", "learned")
+    s_in, s_out = fresh_states()
+    pairs = max(args.steps // 2, 1)
+    hg = solver.capture_host_steps(host_state, host_cs, s_in, s_out, control, DT,
+                                   warmup=max((args.warmup + 1) // 2, 1))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(pairs):
+        hg.replay()
+    e1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / (2 * pairs))
+    e2e_final_q = host_state["joint_q"].clone()
+    del hg
+
     solver = make_solver("fp32", "learned")
     s_in, s_out = fresh_states()
     host_q = state0.joint_q.cpu().pin_memory()
     host_qd = state0.joint_qd.cpu().pin_memory()
-    c_names = [k for k in vars(contacts) if isinstance(getattr(contacts, k), torch.Tensor)]
-    host_c = {k: getattr(contacts, k).cpu().pin_memory() for k in c_names}
-    h2d = (host_q.numel() * 8 + host_qd.numel() * 8 + sum(v.numel() * v.element_size() for v in host_c.values()))
-    d2h = host_q.numel() * 8 + host_qd.numel() * 8
+    host_c = {k: getattr(host_cs[0], k) for k in c_names}
 
     def e2e_step(a, b):
         a.joint_q.copy_(host_q, non_blocking=True)
@@ -378,18 +404,19 @@ def main():
         host_q.copy_(b.joint_q, non_blocking=True)
         host_qd.copy_(b.joint_qd, non_blocking=True)
 
-    for _ in range(args.warmup):
+    for _ in range(2 * max((args.warmup + 1) // 2, 1)):
         e2e_step(s_in, s_out)
         s_in, s_out = s_out, s_in
     barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(2 * pairs):
         e2e_step(s_in, s_out)
         s_in, s_out = s_out, s_in
     e1.record(stream)
     barrier()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ms_e2e_serial = max_over_ranks(e0.elapsed_time(e1) / (2 * pairs))
+    torch.cuda.synchronize()
+    e2e_same = bool(torch.equal(host_q, e2e_final_q))
 
     # ---- stage-2 solve alone on the snapshot of the configuration -------------
     prob = scenes.humanoid_contact_problem(args.worlds, seed=SEED + 1000 * rank)
@@ -501,7 +528,11 @@ def main():
         "uneven_batch_solve_only": uneven,
         "box_worlds_solve_only": box_line,
         "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
+                "path": "SolverSAP.capture_host_steps: two steps and their host copies per graph replay, "
+                        "contacts copied on a second stream during the previous step",
+                "serial_eager": {"value": total / (ms_e2e_serial * 1e-3), "ms_per_step": ms_e2e_serial},
+                "matches_serial_eager": e2e_same},
         "roofline": {"bound": "hbm", "kernel": "contact_solve_kernel", "achieved": achieved, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": NCU_SOLVE_TRAFFIC_BYTES,
                      "note": "achieved = algorithmic bytes of the solve launch / its mean duration inside the "

@@ -670,6 +670,19 @@ class SapContactSolve:
             iterations=-1, line_search_iterations=-1, converged=True)
 
 
+class HostStepGraph:
+    """A captured pair of host-fed steps (SolverSAP.capture_host_steps):
+    replay() advances the rollout by two steps, copies included."""
+
+    def __init__(self, graph: "torch.cuda.CUDAGraph", device_contacts: tuple, copy_stream: "torch.cuda.Stream"):
+        self.graph = graph
+        self.device_contacts = device_contacts  # the two device contact buffers the graph reads
+        self.copy_stream = copy_stream
+
+    def replay(self) -> None:
+        self.graph.replay()
+
+
 class SolverSAP:
     """SAP timestepper (sim/solver_sap.py:736-1512): free motion and contact
     Jacobian, the stage-2 solve and position integration, three native
@@ -861,6 +874,71 @@ class SolverSAP:
             self.step(state_a, state_b, control, contacts, dt)
             self.step(state_b, state_a, control, contacts, dt)
         return graph
+
+    def capture_host_steps(self, host_state: dict, host_contacts: tuple, state_a: SapState, state_b: SapState,
+                           control: SapControl | None, dt, warmup: int = 1) -> "HostStepGraph":
+        """Two consecutive steps fed from and returned to pinned host memory,
+        captured in one CUDA graph.  Every step copies its state
+        (`host_state["joint_q"]`, `["joint_qd"]`) host -> device, steps, and
+        copies the new state back into the same host tensors; step k of a
+        pair takes its contacts from `host_contacts[k]` (SapContacts of
+        pinned host tensors).  Each step's contacts are copied into one of
+        two device buffers on a second stream while the step before it
+        computes, so that copy overlaps the step; the graph joins the copy
+        stream before it ends, so one replay holds all the copies of its two
+        steps.  The host contacts of the first step of a pair are read
+        during the second step of the previous replay.  `warmup` eager pairs
+        (the same copies and steps) run first and advance the rollout."""
+        if not isinstance(dt, (int, float)):
+            raise TypeError("capture_host_steps needs a scalar dt (it is baked into the graph)")
+        if len(host_contacts) != 2:
+            raise ValueError("host_contacts holds the contacts of the two steps of a pair")
+        for name in ("joint_q", "joint_qd"):
+            if not host_state[name].is_pinned():
+                raise ValueError(f"host_state[{name!r}] must be pinned host memory")
+        fields = [k for k, v in vars(host_contacts[0]).items() if isinstance(v, torch.Tensor)]
+        for hc in host_contacts:
+            for k in fields:
+                t = getattr(hc, k)
+                if t is None or not t.is_pinned():
+                    raise ValueError(f"host contacts {k!r} must be pinned host tensors in both sets")
+        dev = self.view.device
+        dev_contacts = tuple(SapContacts(**{k: getattr(hc, k).to(dev) for k in fields}) for hc in host_contacts)
+        main = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(dev)
+
+        def put(dst: SapContacts, src: SapContacts):
+            for k in fields:
+                getattr(dst, k).copy_(getattr(src, k), non_blocking=True)
+
+        def pair():
+            cur = torch.cuda.current_stream(dev)
+            for k, (a, b) in enumerate(((state_a, state_b), (state_b, state_a))):
+                # the state first (the step waits for it), then the other
+                # buffer's contacts on the copy stream while this step runs:
+                # the second step's, then the next pair's first step's
+                a.joint_q.copy_(host_state["joint_q"], non_blocking=True)
+                a.joint_qd.copy_(host_state["joint_qd"], non_blocking=True)
+                if k == 1:
+                    cur.wait_stream(copy)  # this step's contacts (copied during the first step)
+                copy.wait_stream(cur)  # the buffer is free once the step before this one ended
+                with torch.cuda.stream(copy):
+                    put(dev_contacts[1 - k], host_contacts[1 - k])
+                self.step(a, b, control, dev_contacts[k], dt)
+                host_state["joint_q"].copy_(b.joint_q, non_blocking=True)
+                host_state["joint_qd"].copy_(b.joint_qd, non_blocking=True)
+            cur.wait_stream(copy)
+
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            for _ in range(max(int(warmup), 1)):
+                pair()
+        main.wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, capture_error_mode="thread_local"):
+            pair()
+        return HostStepGraph(graph, dev_contacts, copy)
 
     def _mark(self, stage: str | None) -> None:
         """Stage timing: when `stage_events` is a list, record a CUDA event on

@@ -57,3 +57,44 @@ def test_learned_fp32_rollouts_repeat_bit_for_bit(cuda_device):
     r1, r2 = run(), run()
     first = next((k for k in range(len(r1)) if not torch.equal(r1[k], r2[k])), None)
     assert first is None, f"the rollouts part at step {first}"
+
+
+def test_host_step_graph_matches_eager_steps(cuda_device):
+    """capture_host_steps: state and contacts from pinned host memory each
+    step, the new state back to the host; its replays reproduce eager steps
+    bit for bit, with the second contact set really used by the second step
+    of each pair (a set with every contact moved away gives other results)."""
+    from sap_warp_b200.runtime import SapContacts
+
+    model, state, control, contacts, _ = models.rollout_scene("humanoid", 256, 11, cuda_device)
+    kw = dict(max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32", warm_start="learned")
+    names = [k for k in vars(contacts) if isinstance(getattr(contacts, k), torch.Tensor)]
+    far = SapContacts(**{k: getattr(contacts, k).clone() for k in names})
+    far.rigid_contact_point0[:, 2] -= 1.0  # separated by a metre: no contact force
+    far.rigid_contact_point0d[:, 2] -= 1.0
+    sets = (contacts, far)
+    host_sets = tuple(SapContacts(**{k: getattr(c, k).cpu().pin_memory() for k in names}) for c in sets)
+    host_state = {"joint_q": state.joint_q.cpu().pin_memory(), "joint_qd": state.joint_qd.cpu().pin_memory()}
+
+    hs = SolverSAP(model, **kw)
+    ha, hb = pair(state)
+    graph = hs.capture_host_steps(host_state, host_sets, ha, hb, control, 2.0e-3, warmup=1)
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+
+    es = SolverSAP(model, **kw)
+    ea, eb = pair(state)
+    for _ in range(4):  # the warm-up pair and three replays
+        es.step(ea, eb, control, sets[0], 2.0e-3)
+        es.step(eb, ea, control, sets[1], 2.0e-3)
+    torch.cuda.synchronize()
+    assert torch.equal(host_state["joint_q"], ea.joint_q.cpu())
+    assert torch.equal(host_state["joint_qd"], ea.joint_qd.cpu())
+    ref = SolverSAP(model, **kw)
+    ra, rb = pair(state)
+    for _ in range(8):
+        ref.step(ra, rb, control, contacts, 2.0e-3)
+        ra, rb = rb, ra
+    assert not torch.equal(ra.joint_qd, ea.joint_qd)
+    del graph
