@@ -201,4 +201,47 @@ __device__ void ldlt_solve_blocked(const T* H, int n, int ldH, const T* dinv, X*
   }
 }
 
+// x = A^-1 b by the calling warp alone (all 32 lanes; no block barrier) with
+// the LDL^T that ldlt_blocked left in H and dinv: lanes own rows lane and
+// lane + 32 (n <= 64); forward z = D^-1 L^-1 b with the pivot broadcast by
+// shuffles, then backward x = L^-T z.  b is read before x is written (they
+// may alias).  A pivot that is not positive / finite makes x NaN.
+template <typename T>
+__device__ void ldlt_solve_warp(const T* H, int n, int ldH, const T* dinv, const double* b, double* x) {
+  const int lane = threadIdx.x & 31;
+  bool ok = true;
+  for (int k = lane; k < n; k += 32) {
+    const T d = H[(size_t)k * ldH + k];
+    if (!(d > T(0)) || !isfinite(double(d))) ok = false;
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  T h0 = lane < n ? T(b[lane]) : T(0);
+  T h1 = lane + 32 < n ? T(b[lane + 32]) : T(0);
+  for (int k = 0; k < n; ++k) {
+    const T zk = __shfl_sync(0xffffffffu, k < 32 ? h0 : h1, k & 31) * dinv[k];
+    if (lane == (k & 31)) {
+      if (k < 32) h0 = zk;
+      else h1 = zk;
+    }
+    if (lane > k && lane < n) h0 -= H[(size_t)lane * ldH + k] * zk;
+    if (lane + 32 > k && lane + 32 < n) h1 -= H[(size_t)(lane + 32) * ldH + k] * zk;
+  }
+  T s0 = T(0), s1 = T(0);
+  for (int i = n - 1; i >= 0; --i) {
+    T xi_local = T(0);
+    if (lane == (i & 31)) {
+      xi_local = i < 32 ? h0 - s0 * dinv[i] : h1 - s1 * dinv[i];
+      if (i < 32) h0 = xi_local;
+      else h1 = xi_local;
+    }
+    const T xi = __shfl_sync(0xffffffffu, xi_local, i & 31);
+    if (lane < i) s0 += H[(size_t)i * ldH + lane] * xi;
+    if (lane + 32 < i) s1 += H[(size_t)i * ldH + lane + 32] * xi;
+  }
+  const double nanv = __longlong_as_double(0x7ff8000000000000ULL);
+  __syncwarp();
+  if (lane < n) x[lane] = ok ? double(h0) : nanv;
+  if (lane + 32 < n) x[lane + 32] = ok ? double(h1) : nanv;
+}
+
 }  // namespace sapb

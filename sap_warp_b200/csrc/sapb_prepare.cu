@@ -197,7 +197,7 @@ __device__ __forceinline__ void pose_store(double* p, Xf x) {
 // then a blocked LDL^T (diagonal blocks in registers) and block triangular solves.
 // The contact rows are J_c = R_WC (v_O + w x x_c) of the ancestor DOFs' S
 // columns (sim/contact_jacobian.py:404-562).
-__global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams P) {
+__global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x;
   const int e = blockIdx.x;
@@ -573,45 +573,49 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
       if (j <= i) Lg[k] = H[k];
     }
   }
-  for (int i = tid; i < n; i += kPrepNT) vdot[i] = tau[i];
-  __syncthreads();
-  ldlt_solve_blocked<kPrepNT, double>(H, n, n, dinv, vdot, false);
   }
-  __syncthreads();
-  for (int i = tid; i < n; i += kPrepNT) {
-    const double vd = vdot[i];
-    P.out.v_star[d0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vd;
-    if (P.out.vdot) P.out.vdot[d0 + i] = vd;
+  // The free-motion solve A vdot = tau and the contact set-up below need
+  // nothing of each other: with n <= 64, warp 0 solves by itself (shuffles,
+  // no block barrier) while warps 1-3 rank and set up the contacts, synced by
+  // a named barrier of their own; otherwise the whole block solves first.
+  const bool split = !blk && n <= 64;
+  if (!blk && !split) {
+    for (int i = tid; i < n; i += kPrepNT) vdot[i] = tau[i];
+    __syncthreads();
+    ldlt_solve_blocked<kPrepNT, double>(H, n, n, dinv, vdot, false);
   }
-  if (P.out.body_q) {
-    for (int k = tid; k < 7 * B; k += kPrepNT) {
-      const int b = k / 7, c = k - 7 * b;
-      P.out.body_q[7 * (size_t)(b0g + b) + c] = pose[8 * b + c];
-    }
-  }
-
-  // ---- contacts of this world ---------------------------------------------
+  if (!split) __syncthreads();
   const int total = P.env_count[e];
   const int cc = total < C ? total : C;
-  if (tid == 0 && P.out.contact_count) P.out.contact_count[e] = total;
+  auto POSE_P = [&](int b) { return v3(pose[8 * b], pose[8 * b + 1], pose[8 * b + 2]); };
+  auto POSE_Q = [&](int b) { return qnormalize(Q4{pose[8 * b + 3], pose[8 * b + 4], pose[8 * b + 5], pose[8 * b + 6]}); };
+  if (split && tid < 32) {
+    ldlt_solve_warp<double>(H, n, n, dinv, tau, vdot);
+  } else {
+  const int wt = split ? tid - 32 : tid;                // worker thread index
+  const int wn = split ? kPrepNT - 32 : kPrepNT;        // worker threads
+  auto wsync = [&]() {
+    if (split) asm volatile("bar.sync 1, %0;" ::"n"(kPrepNT - 32) : "memory");
+    else __syncthreads();
+  };
+  // ---- contacts of this world ---------------------------------------------
+  if (wt == 0 && P.out.contact_count) P.out.contact_count[e] = total;
   // Canonical slot order: the slots the scatter claimed in arrival order are
   // re-ranked by flat contact index (distinct), so an untruncated world's
   // slots follow the flat buffer's order on every step.
   {
     int* tmp = conint;  // 2*C ints, free until the rows below use them
-    for (int c = tid; c < cc; c += kPrepNT) tmp[c] = P.env_src[(size_t)e * C + c];
-    __syncthreads();
-    for (int c = tid; c < cc; c += kPrepNT) {
+    for (int c = wt; c < cc; c += wn) tmp[c] = P.env_src[(size_t)e * C + c];
+    wsync();
+    for (int c = wt; c < cc; c += wn) {
       const int v = tmp[c];
       int rank = 0;
       for (int j = 0; j < cc; ++j) rank += tmp[j] < v ? 1 : 0;
       P.env_src[(size_t)e * C + rank] = v;
     }
-    __syncthreads();
+    wsync();
   }
-  auto POSE_P = [&](int b) { return v3(pose[8 * b], pose[8 * b + 1], pose[8 * b + 2]); };
-  auto POSE_Q = [&](int b) { return qnormalize(Q4{pose[8 * b + 3], pose[8 * b + 4], pose[8 * b + 5], pose[8 * b + 6]}); };
-  for (int c = tid; c < cc; c += kPrepNT) {
+  for (int c = wt; c < cc; c += wn) {
     const int src = P.env_src[(size_t)e * C + c];
     const int sh0 = P.in.contact_shape0[src], sh1 = P.in.contact_shape1[src];
     const int S_ = P.m.num_shapes;
@@ -661,7 +665,19 @@ __global__ void __launch_bounds__(kPrepNT) prepare_world_kernel(const PrepParams
     conint[2 * c] = (lb0 >= 0 && lb0 < B) ? lb0 : -1;
     conint[2 * c + 1] = (lb1 >= 0 && lb1 < B) ? lb1 : -1;
   }
+  }
   __syncthreads();
+  for (int i = tid; i < n; i += kPrepNT) {
+    const double vd = vdot[i];
+    P.out.v_star[d0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vd;
+    if (P.out.vdot) P.out.vdot[d0 + i] = vd;
+  }
+  if (P.out.body_q) {
+    for (int k = tid; k < 7 * B; k += kPrepNT) {
+      const int b = k / 7, c = k - 7 * b;
+      P.out.body_q[7 * (size_t)(b0g + b) + c] = pose[8 * b + c];
+    }
+  }
   // ---- contact rows, free-motion contact velocities and diag_delassus
   // weights, one warp per contact: lanes over the DOF columns, row / weight
   // partial sums reduced by shuffles.
