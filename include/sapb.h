@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 6
+#define SAPB_ABI_VERSION 7
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -461,6 +461,13 @@ typedef struct sapb_blocked_problem {
   const int32_t* v_guess_active;  /* [1] nonzero: start from v_guess; NULL: never */
   const double* dt;               /* [E] */
   const int32_t* world_order;     /* [E] order of the persistent queue, or NULL */
+  /* A candidate start (no counterpart in the reference): starting impulses
+   * [E,C,3] (for example the previous step's), or NULL.  The solve forms
+   * v_c = v* + A^-1 J^T gamma0 tree by tree (A is block diagonal) and starts
+   * Newton from v_c when its cost is below the plain start's (v_guess or
+   * v0); warm_start_accepted reports 1 then.  gamma0_count must be <= 1. */
+  const double* gamma0;
+  int32_t gamma0_count;
 } sapb_blocked_problem;
 
 /* Off-diagonal factor blocks one world of this shape can hold on chip
@@ -478,7 +485,7 @@ size_t sapb_blocked_solve_workspace_size(int32_t num_envs, int32_t trees_per_env
  * 6129-6285), the Newton Hessian block sparse (a block per tree and per
  * pair of trees in contact) and factored by a block LDL^T in
  * hessian_precision.  Outputs as sapb_contact_solve (v in the tree-by-tree
- * DOF order; warm_start_accepted written 0). */
+ * DOF order; warm_start_accepted 0 plain start, 1 the gamma0 candidate). */
 int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* problem, const sapb_solve_options* opts,
                                    const sapb_solve_outputs* out, void* workspace, size_t workspace_bytes,
                                    void* stream);

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 6
+SAPB_ABI_VERSION = 7
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -142,6 +142,8 @@ class BlockedProblem(C.Structure):
         ("v_guess_active", _p),
         ("dt", _p),
         ("world_order", _p),
+        ("gamma0", _p),
+        ("gamma0_count", C.c_int32),
     ]
 
 

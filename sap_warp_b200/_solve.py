@@ -259,10 +259,12 @@ def blocked_contact_solve(
     v_guess: torch.Tensor | None = None,
     v_guess_active: torch.Tensor | None = None,
     world_order: torch.Tensor | None = None,
+    gamma0: torch.Tensor | None = None,
 ) -> ContactSolveBuffers:
     """Launch the tree-blocked solve (sapb_blocked_contact_solve) for worlds of
     `trees_per_env` trees of `tree_dofs` DOFs; results land in `buffers`
-    (dof_per_env = trees_per_env * tree_dofs), no host sync."""
+    (dof_per_env = trees_per_env * tree_dofs), no host sync.  gamma0 (E, C, 3):
+    starting impulses of a candidate start v* + A^-1 J^T gamma0."""
     lib = load()
     b = buffers
     E, C, T, NB = b.num_envs, b.max_contacts, trees_per_env, tree_dofs
@@ -286,6 +288,8 @@ def blocked_contact_solve(
     P.v_guess_active = _ptr(v_guess_active, I32, 1, "v_guess_active")
     P.dt = _ptr(dt, F64, E, "dt")
     P.world_order = _ptr(world_order, I32, E, "world_order")
+    P.gamma0 = _ptr(gamma0, F64, E * C * 3, "gamma0")
+    P.gamma0_count = 1 if gamma0 is not None else 0
     out = _abi.SolveOutputs()
     out.v = b.v.data_ptr()
     out.contact_gamma = b.contact_gamma.data_ptr()

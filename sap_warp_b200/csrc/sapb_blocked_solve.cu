@@ -51,12 +51,15 @@ struct BlockedParams {
 };
 
 // The per-DOF vectors the blocked kernel keeps, mapped from the V_* slots the
-// line searches name.  Slot kBVecs-1 absorbs the PD / limit slots, which the
-// line searches only touch when PD or limit terms exist (never here).
+// line searches name.  Slot kBVecs-1 holds the saved plain start while a
+// candidate start is evaluated (V_SAVE) and absorbs the PD / limit slots,
+// which the line searches only touch when PD or limit terms exist (never
+// here).
 __host__ __device__ constexpr int bslot(int k) {
   return k == V_V ? 0 : k == V_VSTAR ? 1 : k == V_DV ? 2 : k == V_GRAD ? 3 : k == V_ARES ? 4 : k == V_DP ? 5
        : k == V_DSCALE ? 6 : k == V_TMP0 ? 7 : 8;
 }
+static_assert(bslot(V_SAVE) == 8, "the saved start has the spare slot");
 constexpr int kBVecs = 9;
 
 // Integer scratch inside off_int.
@@ -857,7 +860,7 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
     __syncthreads();
     const bool fits = bsymbolic<NT, HT, NB>(w, L.cap);
 
-    int newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
+    int newton_iterations = 0, ls_total = 0, converged = 0, status = 0, accepted = 0;
     double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
     bool evaluated = false;
     if (!fits) {
@@ -872,10 +875,88 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
       for (int i = tid; i < n; i += NT)
         if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
+      // Candidate start (no counterpart in the reference): v_c = v* +
+      // A^-1 J^T gamma0, tree by tree since A is block diagonal (one thread
+      // per tree with contacts: J_t^T gamma over its contact list, then its
+      // 6x6 block factored and solved in registers, FP64).  Taken when its
+      // cost is below the plain start's; its evaluation then seeds
+      // iteration 0.
+      bool have_e4 = false;
+      double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
+      if (P.p.gamma0) {
+        double e4p[4];
+        bevaluate<NT, HT, NB>(w, e4p);
+        for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
+        for (int t = tid; t < T; t += NT) {
+          const int q0 = w.iw[BI_CSTART + t], q1 = w.iw[BI_CSTART + t + 1];
+          if (q1 == q0) continue;  // no contact: v* already
+          double r[NB];
+#pragma unroll
+          for (int a = 0; a < NB; ++a) r[a] = 0.0;
+          for (int q = q0; q < q1; ++q) {
+            const int ent = w.list[q];
+            const int c = ent >> 1, side = ent & 1;
+            const double* Jc = w.J + (size_t)c * 3 * 2 * NB + side * NB;
+            const double* g = P.p.gamma0 + ((size_t)e * C + c) * 3;
+            const double g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+              r[a] += __ldg(Jc + a) * g0 + __ldg(Jc + 2 * NB + a) * g1 + __ldg(Jc + 4 * NB + a) * g2;
+          }
+          double Lr[NB][NB], Dr[NB];
+          const double* At = w.A + (size_t)t * NB * NB;
+#pragma unroll
+          for (int a = 0; a < NB; ++a)
+#pragma unroll
+            for (int b = 0; b <= a; ++b) Lr[a][b] = __ldg(At + a * NB + b);
+#pragma unroll
+          for (int b = 0; b < NB; ++b) {
+            double d = Lr[b][b];
+#pragma unroll
+            for (int q = 0; q < b; ++q) d -= Lr[b][q] * Lr[b][q] * Dr[q];
+            Dr[b] = d;
+#pragma unroll
+            for (int a = b + 1; a < NB; ++a) {
+              double v = Lr[a][b];
+#pragma unroll
+              for (int q = 0; q < b; ++q) v -= Lr[a][q] * Lr[b][q] * Dr[q];
+              Lr[a][b] = v / d;
+            }
+          }
+#pragma unroll
+          for (int a = 0; a < NB; ++a)
+#pragma unroll
+            for (int q = 0; q < a; ++q) r[a] -= Lr[a][q] * r[q];
+#pragma unroll
+          for (int a = 0; a < NB; ++a) r[a] /= Dr[a];
+#pragma unroll
+          for (int a = NB - 1; a >= 0; --a)
+#pragma unroll
+            for (int q = a + 1; q < NB; ++q) r[a] -= Lr[q][a] * r[q];
+#pragma unroll
+          for (int a = 0; a < NB; ++a) w.V(V_V)[t * NB + a] = w.V(V_VSTAR)[t * NB + a] + r[a];
+        }
+        __syncthreads();
+        double e4c[4];
+        bevaluate<NT, HT, NB>(w, e4c);
+        if (e4c[0] < e4p[0]) {
+          accepted = 1;
+          have_e4 = true;
+          for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
+        } else {
+          for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_SAVE)[i];
+          __syncthreads();
+        }
+      }
       const double cost_min_alpha = LSV == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
       for (int it = 0;; ++it) {
         double e4[4];
-        bevaluate<NT, HT, NB>(w, e4);
+        if (have_e4) {
+          for (int q = 0; q < 4; ++q) e4[q] = e4_seed[q];
+          have_e4 = false;
+        } else {
+          bevaluate<NT, HT, NB>(w, e4);
+        }
         evaluated = true;
         cost = e4[0];
         // convergence test (sim/contact_solve.py:2043-2087)
@@ -946,7 +1027,7 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
       if (P.out.converged) P.out.converged[e] = converged;
       if (P.out.status) P.out.status[e] = status;
       if (P.out.grad_norm) P.out.grad_norm[e] = grad_norm;
-      if (P.out.warm_start_accepted) P.out.warm_start_accepted[e] = 0;
+      if (P.out.warm_start_accepted) P.out.warm_start_accepted[e] = accepted;
     }
     __syncthreads();
   }

@@ -153,6 +153,11 @@ int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* p, const sapb_sol
     sapb::set_last_error("sapb_blocked_contact_solve: missing contact array");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
+  if (p->gamma0 && p->gamma0_count > 1) {
+    sapb::set_last_error("sapb_blocked_contact_solve: one candidate impulse set at most (gamma0_count=%d)",
+                         p->gamma0_count);
+    return SAPB_ERR_UNSUPPORTED;
+  }
   if (o->line_search_variant < SAPB_LS_MONOTONE_DECAY || o->line_search_variant > SAPB_LS_EXACT_ROOT) {
     sapb::set_last_error("sapb_blocked_contact_solve: unknown line search variant %d", o->line_search_variant);
     return SAPB_ERR_INVALID_ARGUMENT;

@@ -589,9 +589,8 @@ class SapContactSolve:
         v = self.view
         W, n, C = v.W, v.n, self.max_rigid_contact
         if self.tree_blocked:
-            if gamma0 is not None:
-                raise NotImplementedError("candidate starting impulses need the dense layout")
-            return self._solve_blocked(contact_result, opts, v_star, v0, v_guess, v_guess_active, world_order)
+            return self._solve_blocked(contact_result, opts, v_star, v0, v_guess, v_guess_active, world_order,
+                                       gamma0)
         P = _abi.ContactProblem()
         P.num_envs, P.dof_per_env, P.max_contacts = W, n, int(contact_result.contact_env_jacobian.shape[1])
         P.num_bodies = int(v.body_dof_start.numel())
@@ -634,9 +633,10 @@ class SapContactSolve:
         return self.result()
 
     def _solve_blocked(self, r: SapContactJacobianResult, opts, v_star, v0, v_guess, v_guess_active,
-                       world_order=None):
+                       world_order=None, gamma0=None):
         """The tree-blocked solve (sapb_blocked_contact_solve) on the
-        tree-blocked result of SapContactJacobian."""
+        tree-blocked result of SapContactJacobian; gamma0 (W, C, 3): one set
+        of candidate starting impulses."""
         if r.tree_mass_env is None or r.contact_env_tree is None:
             raise ValueError("the tree-blocked solve needs a tree-blocked SapContactJacobianResult")
         v = self.view
@@ -655,6 +655,11 @@ class SapContactSolve:
                 raise TypeError("v_guess must be a contiguous float64 tensor (it is written back)")
             P.v_guess = _ptr(v_guess)
             P.v_guess_active = _ptr(v_guess_active)
+        if gamma0 is not None:
+            per_set = v.W * int(P.max_contacts) * 3
+            if gamma0.dtype != F64 or not gamma0.is_contiguous() or gamma0.numel() != per_set:
+                raise TypeError("the tree-blocked solve takes one contiguous float64 (W, C, 3) impulse set")
+            P.gamma0, P.gamma0_count = _ptr(gamma0), 1
         status = load().sapb_blocked_contact_solve(ctypes.byref(P), ctypes.byref(opts), ctypes.byref(self.outputs),
                                                    self.workspace.data_ptr(), self.workspace.numel(),
                                                    ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream))
@@ -811,8 +816,9 @@ class SolverSAP:
         if self.warm_start not in ("previous_velocity", "previous_impulses", "learned"):
             raise ValueError("warm_start must be 'previous_velocity', 'previous_impulses' or 'learned', "
                              f"got {warm_start!r}.")
-        if tree_blocked and self.warm_start != "previous_velocity":
-            raise NotImplementedError("the tree-blocked layout takes the previous-velocity warm start only")
+        if self.contact_solve.tree_blocked and self.warm_start == "learned":
+            raise NotImplementedError("the tree-blocked layout takes the previous-velocity or previous-impulses "
+                                      "warm start")
         self.learned_warm_start = None
         if self.warm_start == "learned":
             from .warmstart import DEFAULT_WEIGHTS, LearnedWarmStart
@@ -830,8 +836,8 @@ class SolverSAP:
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
         if self.learned_warm_start is not None:
             self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
-        if self.warm_start != "previous_velocity":
-            self.contact_jacobian.keep_dynamics_factor()
+        if self.warm_start != "previous_velocity" and not self.contact_solve.tree_blocked:
+            self.contact_jacobian.keep_dynamics_factor()  # the blocked solve solves with A's tree blocks
         self.work_order = str(work_order).strip().lower().replace("-", "_")
         if self.work_order not in ("previous_iterations", "index"):
             raise ValueError(f"work_order must be 'previous_iterations' or 'index', got {work_order!r}.")

@@ -122,3 +122,76 @@ def test_fill_capacity_status(cuda_device):
     n = bp.dof_per_env
     np.testing.assert_array_equal(gpu["v"].reshape(-1, n)[1], bp.v_star.reshape(-1, n)[1])
     assert gpu["converged"][0] == 1 and gpu["converged"][2] == 1
+
+
+def test_blocked_candidate_start_matches_dense_kernel(cuda_device):
+    """One set of candidate impulses (the plain solution, scaled near 1 in
+    half the worlds and by 4 in the others): the blocked solve takes the
+    same starts as the dense kernel (both FP64) and reaches the same answer."""
+    bp = scenes.box_stack_problem(64, seed=45, boxes=8, max_contacts=64, sites=(2, 4))
+    d = bp.to_dense()
+    t = problem_to_device(d, cuda_device)
+    buf = ContactSolveBuffers(d.num_envs, d.dof_per_env, d.max_contacts, cuda_device)
+    contact_solve(**t, buffers=buf, options=make_options("armijo_decay"))
+    torch.cuda.synchronize()
+    scale = torch.where(torch.arange(d.num_envs, device=cuda_device) % 2 == 0, 1.02, 4.0).double()
+    gamma0 = (buf.contact_gamma.reshape(d.num_envs, d.max_contacts, 3) * scale[:, None, None]).contiguous()
+    buf_d = ContactSolveBuffers(d.num_envs, d.dof_per_env, d.max_contacts, cuda_device)
+    contact_solve(**t, buffers=buf_d, options=make_options("armijo_decay"), gamma0=gamma0)
+    torch.cuda.synchronize()
+    dense = {k: getattr(buf_d, k).cpu().numpy() for k in KEYS + ("warm_start_accepted",)}
+    tb = blocked_problem_to_device(bp, cuda_device)
+    buf_b = ContactSolveBuffers(bp.num_envs, bp.dof_per_env, bp.max_contacts, cuda_device)
+    blocked_contact_solve(buffers=buf_b, options=make_options("armijo_decay"), trees_per_env=bp.trees_per_env,
+                          tree_dofs=bp.tree_dofs, gamma0=gamma0, **tb)
+    torch.cuda.synchronize()
+    blocked = {k: getattr(buf_b, k).cpu().numpy() for k in KEYS + ("warm_start_accepted",)}
+    acc = blocked["warm_start_accepted"]
+    np.testing.assert_array_equal(acc, dense["warm_start_accepted"])
+    assert acc[0::2].mean() > 0.9 and acc[1::2].mean() < acc[0::2].mean()  # near-solution sets taken
+    assert_parity(d, blocked, dense, tight=1e-8, loose=1e-4)
+    np.testing.assert_array_equal(blocked["converged"], 1)
+    # near the solution a world needs fewer iterations than from the plain start
+    assert blocked["newton_iterations"][0::2].mean() < dense_plain_iterations(buf)
+
+
+def dense_plain_iterations(buf):
+    return float(buf.newton_iterations.double().mean())
+
+
+def test_box_rollout_previous_impulses(cuda_device):
+    """64-box worlds stepped by SolverSAP with the previous step's impulses
+    as a candidate start: every step converges, the candidate is taken in
+    most worlds after the first step, Newton iterations drop against the
+    previous-velocity start (by about an eighth on these stacks: stiction
+    keeps Newton long even near the solution), and both runs end at the same
+    state to the solve tolerance."""
+    from sap_warp_b200 import models
+    from sap_warp_b200.runtime import SapState
+    from sap_warp_b200.solver import SolverSAP
+
+    model, state, control, con, _, _ = models.box_scene(16, 74, cuda_device)
+    runs = {}
+    for warm in ("previous_velocity", "previous_impulses"):
+        solver = SolverSAP(model, max_rigid_contact=512, contact_preset_variant="drake", hessian_precision="fp32",
+                           warm_start=warm)
+        assert solver.contact_solve.tree_blocked
+        a = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone())
+        b = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone())
+        iters, taken = [], []
+        for k in range(12):
+            solver.step(a, b, control, con, 2e-3)
+            assert bool(solver.contact_solve.converged_env.all())
+            if k >= 2:
+                iters.append(float(solver.contact_solve.newton_iterations_env.double().mean()))
+                taken.append(float(solver.contact_solve.warm_start_accepted_env.double().mean()))
+            a, b = b, a
+        runs[warm] = (np.mean(iters), np.mean(taken), a.joint_qd.clone())
+    it_v, _, qd_v = runs["previous_velocity"]
+    it_i, taken_i, qd_i = runs["previous_impulses"]
+    assert taken_i > 0.5
+    assert it_i < it_v
+    rel = float((qd_i - qd_v).abs().max() / qd_v.abs().max().clamp(min=1e-30))
+    assert rel < 1e-3
