@@ -486,6 +486,40 @@ def main():
                            "mean_newton_iterations": float(bbuf.newton_iterations.double().mean()),
                            "all_converged": bool(bbuf.converged.all())}
 
+    # ---- the whole step on 512 worlds of 64 free boxes (tree-blocked free
+    # motion and solve, FP32 Hessian), previous-velocity vs previous-impulses start
+    bmodel, bstate, bcontrol, bcon, _, _ = models.box_scene(512, 75 + 1000 * rank, dev)
+    box_step = {"worlds": 512, "trees": "64 free boxes per world (n = 384)",
+                "contacts": f"{int(bcon.rigid_contact_count.item())} in all"}
+    for warm in ("previous_velocity", "previous_impulses"):
+        bsolver = SolverSAP(bmodel, max_rigid_contact=512, contact_preset_variant="drake", hessian_precision="fp32",
+                            warm_start=warm)
+        ba = SapState(joint_q=bstate.joint_q.clone(), joint_qd=bstate.joint_qd.clone(), body_q=bstate.body_q.clone(),
+                      body_f=bstate.body_f.clone())
+        bb = SapState(joint_q=bstate.joint_q.clone(), joint_qd=bstate.joint_qd.clone(), body_q=bstate.body_q.clone(),
+                      body_f=bstate.body_f.clone())
+        for _ in range(2):
+            bsolver.step(ba, bb, bcontrol, bcon, DT)
+            ba, bb = bb, ba
+        barrier()
+        k_bs = max(1, min(args.steps, 10))
+        its, acc = [], []
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(k_bs):
+            bsolver.step(ba, bb, bcontrol, bcon, DT)
+            its.append(bsolver.contact_solve.newton_iterations_env.sum())
+            acc.append(bsolver.contact_solve.warm_start_accepted_env.sum())
+            ba, bb = bb, ba
+        a1.record(stream)
+        barrier()
+        ms = max_over_ranks(a0.elapsed_time(a1) / k_bs)
+        box_step[warm] = {"value": 512 * world_size / (ms * 1e-3), "ms_per_step": ms,
+                          "mean_newton_iterations": float(torch.stack(its).double().sum()) / (512 * k_bs),
+                          "candidate_taken": float(torch.stack(acc).double().sum()) / (512 * k_bs),
+                          "all_converged": bool(bsolver.contact_solve.converged_env.all())}
+    del bsolver, bmodel, bstate, bcon
+
     total = W * world_size
     value = total / (fast["ms"] * 1e-3)
     peaks = {}
@@ -527,6 +561,7 @@ def main():
         "stage2_solve_only": snap,
         "uneven_batch_solve_only": uneven,
         "box_worlds_solve_only": box_line,
+        "box_worlds_step": box_step,
         "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
                 "path": "SolverSAP.capture_host_steps: two steps and their host copies per graph replay, "
