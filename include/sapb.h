@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 7
+#define SAPB_ABI_VERSION 8
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -94,6 +94,8 @@ typedef struct sapb_solve_options {
   int32_t linear_solve_precision; /* SAPB_FP64 / SAPB_FP32: Newton-direction Cholesky */
   int32_t hessian_precision;      /* SAPB_FP64 / SAPB_FP32: J^T G J assembly */
   int32_t cubic_init;             /* exact_root cubic seed, sim/contact_solve.py:55-58 (1) */
+  int32_t ctas_per_sm;            /* resident CTAs per SM of the persistent dense solve: 0 as many as fit
+                                   * (sapb_contact_solve_occupancy), k at most k; results do not depend on it */
 } sapb_solve_options;
 
 /* Per-DOF drive and limit model (the arrays SapContactSolve.prepare reads,
@@ -394,6 +396,11 @@ size_t sapb_contacts_workspace_size(const sapb_collision_shapes* shapes);
 int32_t sapb_generate_contacts(const sapb_collision_shapes* shapes, const double* body_q,
                                const sapb_contact_outputs* out, void* workspace, size_t workspace_bytes,
                                void* stream);
+
+/* Resident CTAs per SM the dense contact solve can hold for this world shape
+ * (the upper end of sapb_solve_options.ctas_per_sm), or a negative status. */
+int32_t sapb_contact_solve_occupancy(int32_t dof_per_env, int32_t max_contacts, int32_t hessian_precision,
+                                     int32_t line_search_variant);
 
 /* Fill the reference defaults of SapContactSolve for a line-search variant.
  * Replaces the Python defaults of solve(), sim/contact_solve.py:6129-6182. */

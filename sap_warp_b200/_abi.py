@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 7
+SAPB_ABI_VERSION = 8
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -64,6 +64,7 @@ class SolveOptions(C.Structure):
         ("linear_solve_precision", C.c_int32),
         ("hessian_precision", C.c_int32),
         ("cubic_init", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
     ]
 
 
@@ -320,6 +321,7 @@ EXPORTS = {
     "sapb_solve_options_default": (None, [C.POINTER(SolveOptions), C.c_int32]),
     "sapb_abi_version": (C.c_int32, []),
     "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
+    "sapb_contact_solve_occupancy": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve": (
         C.c_int32,
         [C.POINTER(ContactProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p, C.c_size_t, _p],

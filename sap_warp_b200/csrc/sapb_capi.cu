@@ -26,6 +26,15 @@ int32_t sapb_abi_version(void) { return SAPB_ABI_VERSION; }
 
 const char* sapb_last_error(void) { return sapb::g_last_error; }
 
+int32_t sapb_contact_solve_occupancy(int32_t dof_per_env, int32_t max_contacts, int32_t hessian_precision,
+                                     int32_t line_search_variant) {
+  if (line_search_variant < SAPB_LS_MONOTONE_DECAY || line_search_variant > SAPB_LS_EXACT_ROOT) {
+    sapb::set_last_error("sapb_contact_solve_occupancy: unknown line search variant %d", line_search_variant);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::contact_solve_occupancy(dof_per_env, max_contacts, hessian_precision, line_search_variant);
+}
+
 void sapb_solve_options_default(sapb_solve_options* o, int32_t variant) {
   // SapContactSolve defaults: sim/contact_solve.py:3299-3316 and 6129-6182.
   if (!o) return;

@@ -943,7 +943,12 @@ static cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, in
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, L.total);
   if (err != cudaSuccess) return err;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  int blocks = sms * per_sm;
+  if (blocks_out && P.p.num_envs == 0) {  // occupancy query only
+    *blocks_out = per_sm;
+    return cudaSuccess;
+  }
+  const int k = (P.o.ctas_per_sm > 0 && P.o.ctas_per_sm < per_sm) ? P.o.ctas_per_sm : per_sm;
+  int blocks = sms * k;
   if (blocks > P.p.num_envs) blocks = P.p.num_envs;
   if (blocks < 1) blocks = 1;
   if (blocks_out) *blocks_out = blocks;
@@ -969,6 +974,47 @@ size_t contact_solve_smem_bytes(int n, int C, int hessian_precision) {
   return make_layout(n, C, hessian_precision == SAPB_FP32 ? 4 : 8).total;
 }
 
+// Resident CTAs per SM of the kernel a problem of this shape launches: the
+// same dispatch with num_envs = 0, which stops at the occupancy query.
+static cudaError_t solve_dispatch(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out);
+
+int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant) {
+  if (n < 1 || C < 0) return SAPB_ERR_INVALID_ARGUMENT;
+  const bool fp32 = hessian_precision == SAPB_FP32;
+  if (contact_solve_smem_bytes(n, C, fp32 ? SAPB_FP32 : SAPB_FP64) > kMaxSmemPerBlock) return SAPB_ERR_UNSUPPORTED;
+  SolveParams P;
+  memset(&P, 0, sizeof(P));
+  P.p.dof_per_env = n;
+  P.p.max_contacts = C;
+  P.o.line_search_variant = variant;
+  int per_sm = 0;
+  const cudaError_t err = solve_dispatch(P, fp32, nullptr, &per_sm);
+  if (err != cudaSuccess) {
+    set_last_error("contact solve occupancy: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  return per_sm;
+}
+
+static cudaError_t solve_dispatch(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
+  // Kernels specialised on the DOF count of the common trees (humanoid 35,
+  // quadruped 18, arm + box 13, single free body 6); a generic one otherwise.
+  switch (P.p.dof_per_env) {
+#define SAPB_DISPATCH_N(NV)                                                              \
+  case NV:                                                                               \
+    return fp32 ? launch_solve<128, float, 4, NV>(P, stream, blocks_out)                 \
+                : launch_solve<128, double, 3, NV>(P, stream, blocks_out);
+    SAPB_DISPATCH_N(35)
+    SAPB_DISPATCH_N(18)
+    SAPB_DISPATCH_N(13)
+    SAPB_DISPATCH_N(6)
+#undef SAPB_DISPATCH_N
+    default:
+      return fp32 ? launch_solve<128, float, 4, 0>(P, stream, blocks_out)
+                  : launch_solve<128, double, 3, 0>(P, stream, blocks_out);
+  }
+}
+
 int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_options* o, const sapb_solve_outputs* out,
                              void* workspace, size_t workspace_bytes, cudaStream_t stream) {
   SolveParams P;
@@ -990,24 +1036,7 @@ int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_opt
                    (size_t)kMaxSmemPerBlock);
     return SAPB_ERR_UNSUPPORTED;
   }
-  cudaError_t err;
-  // Kernels specialised on the DOF count of the common trees (humanoid 35,
-  // quadruped 18, arm + box 13, single free body 6); a generic one otherwise.
-  switch (p->dof_per_env) {
-#define SAPB_DISPATCH_N(NV)                                                              \
-  case NV:                                                                               \
-    err = fp32 ? launch_solve<128, float, 4, NV>(P, stream, nullptr)                     \
-               : launch_solve<128, double, 3, NV>(P, stream, nullptr);                   \
-    break;
-    SAPB_DISPATCH_N(35)
-    SAPB_DISPATCH_N(18)
-    SAPB_DISPATCH_N(13)
-    SAPB_DISPATCH_N(6)
-#undef SAPB_DISPATCH_N
-    default:
-      err = fp32 ? launch_solve<128, float, 4, 0>(P, stream, nullptr)
-                 : launch_solve<128, double, 3, 0>(P, stream, nullptr);
-  }
+  const cudaError_t err = solve_dispatch(P, fp32, stream, nullptr);
   if (err != cudaSuccess) {
     set_last_error("contact solve launch: %s", cudaGetErrorString(err));
     return SAPB_ERR_CUDA;

@@ -479,6 +479,8 @@ class SapContactSolve:
                  tree_blocked: bool | None = None, _view: _ModelView | None = None):
         self.view = _view or _ModelView(model)
         v = self.view
+        self.autotuner = None  # autotune.SolveAutotuner: picks the dense solve's resident CTAs per SM
+        self._device_props = None
         self.tree_blocked = _pick_tree_blocked(v, tree_blocked)
         if v.n > 60 and not self.tree_blocked:
             raise NotImplementedError(f"the dense on-chip solve supports up to 60 DOFs per world, got {v.n} "
@@ -545,6 +547,49 @@ class SapContactSolve:
                             contact_tau_d=self.contact_tau_d, diag_shift=self.diag_shift,
                             linear_solve_precision=self.linear_solve_precision,
                             hessian_precision=self.hessian_precision, **kw)
+
+    def _launch_shape(self, P, opts, variant: str, stream) -> int:
+        """Resident CTAs per SM for this problem: 0 (the occupancy bound)
+        without an autotuner; with one, its choice for the problem's key,
+        timed here on this very problem the first time the key is seen
+        (never while a graph is being captured: then the bound)."""
+        from .autotune import tuning_key
+
+        if self.autotuner is None:
+            return 0
+        v = self.view
+        fp32 = opts.hessian_precision == _abi.SAPB_FP32 or opts.linear_solve_precision == _abi.SAPB_FP32
+        if self._device_props is None:
+            self._device_props = torch.cuda.get_device_properties(v.device)
+        props = self._device_props
+        key = tuning_key(v.n, P.max_contacts, "fp32" if fp32 else "fp64", variant, props.name,
+                         props.multi_processor_count)
+        known = self.autotuner.lookup(key)
+        if known is not None:
+            return known
+        if torch.cuda.is_current_stream_capturing():
+            return 0
+        lib = load()
+        occ = int(lib.sapb_contact_solve_occupancy(v.n, int(P.max_contacts),
+                                                   _abi.SAPB_FP32 if fp32 else _abi.SAPB_FP64,
+                                                   int(opts.line_search_variant)))
+        if occ < 1:
+            check(occ, "sapb_contact_solve_occupancy")
+        cur = torch.cuda.current_stream(v.device)
+
+        def time_ms(k: int) -> float:
+            o = _abi.SolveOptions.from_buffer_copy(opts)
+            o.ctas_per_sm = k
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(cur)
+            check(lib.sapb_contact_solve(ctypes.byref(P), ctypes.byref(o), ctypes.byref(self.outputs),
+                                         self.workspace.data_ptr(), self.workspace.numel(), stream),
+                  "sapb_contact_solve")
+            e1.record(cur)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
+        return self.autotuner.tune(key, list(range(1, occ + 1)), time_ms)
 
     def solve(self, contact_result: SapContactJacobianResult, state: SapState, control: SapControl | None, dt,
               v_star: torch.Tensor, *, v0: torch.Tensor | None = None, v_guess: torch.Tensor | None = None,
@@ -626,9 +671,10 @@ class SapContactSolve:
                 self._dof_keep["_" + name] = tt
                 setattr(self.dof, name, _ptr(tt))
             P.dof = ctypes.pointer(self.dof)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream)
+        opts.ctas_per_sm = self._launch_shape(P, opts, variant, stream)
         status = load().sapb_contact_solve(ctypes.byref(P), ctypes.byref(opts), ctypes.byref(self.outputs),
-                                           self.workspace.data_ptr(), self.workspace.numel(),
-                                           ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream))
+                                           self.workspace.data_ptr(), self.workspace.numel(), stream)
         check(status, "sapb_contact_solve")
         return self.result()
 
@@ -709,7 +755,8 @@ class SolverSAP:
                  static_substep: bool = False, static_substep_iterations: int = 8,
                  static_substep_line_search_iterations: int = 6, position_integration: str | None = None,
                  hessian_precision: str | None = None, warm_start: str = "previous_velocity",
-                 learned_warm_start=None, tree_blocked: bool | None = None, work_order: str = "previous_iterations"):
+                 learned_warm_start=None, tree_blocked: bool | None = None, work_order: str = "previous_iterations",
+                 autotune: bool | str | os.PathLike | None = None):
         """Keyword arguments of the reference's SolverSAP (sim/solver_sap.py:
         749-791) plus: hessian_precision ("fp64" / "fp32": J^T G J assembly and
         factorization precision; the gradient, cost, line search and
@@ -730,8 +777,11 @@ class SolverSAP:
         depend on it); tree_blocked (None: automatic) selects the tree-blocked layout for
         worlds made only of free bodies (default beyond 60 DOFs per world:
         A as 6 x 6 blocks, contact rows over the two touching bodies, a block
-        sparse Newton factorization), which takes the previous-velocity warm
-        start only."""
+        sparse Newton factorization), which takes the previous-velocity or
+        previous-impulses warm start; autotune (True, or a JSON cache path)
+        times the dense solve's resident CTAs per SM on the first solve of
+        each problem shape and keeps the fastest (autotune.SolveAutotuner;
+        results do not depend on it)."""
         view = _ModelView(model)
         tree_blocked = _pick_tree_blocked(view, tree_blocked)
         preset = dict(_CONTACT_PRESET_KWARGS[_normalize_contact_preset_variant(contact_preset_variant)])
@@ -844,6 +894,10 @@ class SolverSAP:
         self._world_order = torch.arange(view.W, dtype=I32, device=dev)
         self._order_keys = torch.zeros(view.W, dtype=I32, device=dev)
         self._order_idx = torch.zeros(view.W, dtype=torch.int64, device=dev)
+        if autotune:
+            from .autotune import SolveAutotuner
+
+            self.contact_solve.autotuner = SolveAutotuner(None if autotune is True else autotune)
         self.reset_runtime_state()
 
     @property
