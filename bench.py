@@ -293,7 +293,8 @@ def main():
 
     def make_solver(prec, warm):
         return SolverSAP(model, max_rigid_contact=MAX_CONTACTS, contact_preset_variant="drake",
-                         hessian_precision=prec, warm_start=warm, learned_warm_start=ws if warm == "learned" else None)
+                         hessian_precision=prec, warm_start=warm, learned_warm_start=ws if warm == "learned" else None,
+                         autotune=True)
 
     def run_arm(prec, warm, sampler=None):
         """Two passes over the same stretch of the rollout (steps warmup ..
@@ -463,6 +464,32 @@ def main():
         uneven[label] = {"value": mix.num_envs * world_size / (ms * 1e-3), "ms_per_solve": ms,
                          "all_converged": bool(mbuf.converged.all())}
 
+    # ---- the launch-shape autotuner's view: each resident-CTA count per SM
+    # timed on the snapshot and on the uneven batch (SolveAutotuner's rule) ----
+    from sap_warp_b200._lib import load as _load_lib
+    from sap_warp_b200.autotune import SolveAutotuner
+
+    tuned = {}
+    for label, tt, bb, opts, wo in (
+            ("humanoid_fp32", t, buf, make_options("armijo_decay", hessian_precision="fp32"), None),
+            ("humanoid_fp64", t, buf, make_options("armijo_decay"), None),
+            ("uneven_fp32", tm, mbuf, make_options("armijo_decay", hessian_precision="fp32"), order)):
+        occ = int(_load_lib().sapb_contact_solve_occupancy(bb.dof_per_env, bb.max_contacts, opts.hessian_precision,
+                                                            opts.line_search_variant))
+
+        def time_ms(k, tt=tt, bb=bb, opts=opts, wo=wo):
+            opts.ctas_per_sm = k
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            contact_solve(**tt, buffers=bb, options=opts, world_order=wo)
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
+        tuner = SolveAutotuner(repeats=5)
+        chosen = tuner.tune(label, list(range(1, occ + 1)), time_ms)
+        tuned[label] = {"occupancy": occ, "chosen": chosen, "ms": tuner.table[label]["ms"]}
+
     # ---- worlds of 64 free boxes (384 DOFs, ~400 contacts): tree-blocked solve ----
     boxes = scenes.box_stack_problem(512, seed=4 + 1000 * rank)
     tb = blocked_problem_to_device(boxes, dev)
@@ -562,6 +589,7 @@ def main():
         "uneven_batch_solve_only": uneven,
         "box_worlds_solve_only": box_line,
         "box_worlds_step": box_step,
+        "autotune_ctas_per_sm": tuned,
         "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
                 "path": "SolverSAP.capture_host_steps: two steps and their host copies per graph replay, "

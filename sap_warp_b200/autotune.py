@@ -40,9 +40,10 @@ class SolveAutotuner:
     each new choice (None: this process only).  repeats: timed runs per
     candidate (the minimum counts)."""
 
-    def __init__(self, cache_path: str | os.PathLike | None = None, repeats: int = 3):
+    def __init__(self, cache_path: str | os.PathLike | None = None, repeats: int = 3, margin: float = 0.03):
         self.cache_path = None if cache_path is None else os.fspath(cache_path)
         self.repeats = max(int(repeats), 1)
+        self.margin = float(margin)
         self.table: dict = {}
         if self.cache_path and os.path.exists(self.cache_path):
             with open(self.cache_path) as f:
@@ -56,8 +57,10 @@ class SolveAutotuner:
         return None if entry is None else int(entry["ctas_per_sm"])
 
     def tune(self, key: str, candidates: list[int], time_ms: Callable[[int], float]) -> int:
-        """The cached choice for `key`, else the candidate with the least time
-        (ties: the larger k), recorded with every candidate's time."""
+        """The cached choice for `key`, else the candidate with the least time,
+        recorded with every candidate's time.  The largest candidate (the
+        occupancy bound, the launch without tuning) is kept unless another
+        beats it by more than `margin` (a short sample decides)."""
         known = self.lookup(key)
         if known is not None:
             return known
@@ -66,6 +69,8 @@ class SolveAutotuner:
             raise ValueError("no candidate launch shape")
         times = {k: min(float(time_ms(k)) for _ in range(self.repeats)) for k in cands}
         best = min(cands, key=lambda k: (times[k], -k))
+        if times[cands[-1]] <= times[best] * (1.0 + self.margin):
+            best = cands[-1]
         self.table[key] = {"ctas_per_sm": best, "ms": {str(k): times[k] for k in cands}}
         self.save()
         return best

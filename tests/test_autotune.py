@@ -18,7 +18,7 @@ def test_keys_bucket_contacts_and_name_the_gpu():
 def test_tune_picks_the_fastest_and_caches(tmp_path):
     path = tmp_path / "tune.json"
     tuner = SolveAutotuner(path, repeats=2)
-    times = {1: 3.0, 2: 1.5, 3: 1.2, 4: 1.3}
+    times = {1: 3.0, 2: 1.5, 3: 1.2, 4: 1.3}  # 3 beats the bound 4 by more than the 3 % margin
     calls = []
 
     def time_ms(k):
@@ -39,3 +39,9 @@ def test_ties_take_more_ctas_and_bad_candidates_fail():
     assert tuner.tune("s", [1, 2, 3], lambda k: 1.0) == 3
     with pytest.raises(ValueError):
         tuner.tune("t", [0, -1], lambda k: 1.0)
+
+
+def test_the_occupancy_bound_stays_within_the_margin():
+    tuner = SolveAutotuner(margin=0.05)
+    assert tuner.tune("s", [1, 2, 3, 4], {1: 2.0, 2: 1.0, 3: 0.99, 4: 1.03}.get) == 4
+    assert tuner.tune("t", [1, 2, 3, 4], {1: 2.0, 2: 1.0, 3: 0.90, 4: 1.03}.get) == 3
