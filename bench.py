@@ -242,10 +242,10 @@ def run_reference(args, rank: int, world_size: int):
 
 
 def main():
+    from sap_warp_b200.shards import RankGroup, env_ranks, shard_of
+
     args = parse()
-    world_size = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world_size, local_rank = env_ranks()
     if args.impl == "reference":
         run_reference(args, rank, world_size)
         return
@@ -267,20 +267,11 @@ def main():
 
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     stream = torch.cuda.current_stream(dev)
+    group = RankGroup(dist, dev)
+    barrier, max_over_ranks = group.barrier, group.max_over_ranks
+    shard = shard_of(rank, world_size, args.worlds, SEED)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        tt = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
-
-    model, state0, control, contacts, _ = models.rollout_scene("humanoid", args.worlds, SEED + 1000 * rank, dev)
+    model, state0, control, contacts, _ = models.rollout_scene("humanoid", shard.worlds, shard.seed, dev)
     W = args.worlds
     ws = LearnedWarmStart.load(args.weights or DEFAULT_WEIGHTS, dev)
 
