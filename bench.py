@@ -506,7 +506,7 @@ def main():
 
     # ---- the whole step on 512 worlds of 64 free boxes (tree-blocked free
     # motion and solve, FP32 Hessian), previous-velocity vs previous-impulses start
-    bmodel, bstate, bcontrol, bcon, _, _ = models.box_scene(512, 75 + 1000 * rank, dev)
+    bmodel, bstate, bcontrol, bcon, _, bhost = models.box_scene(512, 75 + 1000 * rank, dev)
     box_step = {"worlds": 512, "trees": "64 free boxes per world (n = 384)",
                 "contacts": f"{int(bcon.rigid_contact_count.item())} in all"}
     for warm in ("previous_velocity", "previous_impulses"):
@@ -536,7 +536,30 @@ def main():
                           "mean_newton_iterations": float(torch.stack(its).double().sum()) / (512 * k_bs),
                           "candidate_taken": float(torch.stack(acc).double().sum()) / (512 * k_bs),
                           "all_converged": bool(bsolver.contact_solve.converged_env.all())}
-    del bsolver, bmodel, bstate, bcon
+    # ---- contact generation for the same worlds' shapes (64 boxes each + a
+    # ground plane): forward kinematics, count, scan, write ----
+    from sap_warp_b200.collision import ContactGenerator
+    from sap_warp_b200.solver import _ModelView
+
+    bshapes = models.box_shapes(bhost)
+    gen = ContactGenerator(bshapes, _ModelView(bmodel), capacity=512 * 1024, gap=2.0e-3)
+    for _ in range(3):
+        gen.generate(bstate.joint_q)
+    barrier()
+    k_gen = max(1, min(args.steps, 20))
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(k_gen):
+        gen.generate(bstate.joint_q)
+    a1.record(stream)
+    barrier()
+    ms = max_over_ranks(a0.elapsed_time(a1) / k_gen)
+    pairs = 512 * (64 * 1 + 64 * 63 // 2)
+    contact_gen = {"worlds": 512, "shapes": "64 boxes per world + a shared ground plane",
+                   "candidate_pairs": pairs, "contacts": int(gen.count.item()), "ms_per_call": ms,
+                   "value": 512 * world_size / (ms * 1e-3), "unit": "world-generations/s",
+                   "pairs_per_s": pairs * world_size / (ms * 1e-3)}
+    del gen, bsolver, bmodel, bstate, bcon
 
     total = W * world_size
     value = total / (fast["ms"] * 1e-3)
@@ -580,6 +603,7 @@ def main():
         "uneven_batch_solve_only": uneven,
         "box_worlds_solve_only": box_line,
         "box_worlds_step": box_step,
+        "contact_generation": contact_gen,
         "autotune_ctas_per_sm": tuned,
         "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,

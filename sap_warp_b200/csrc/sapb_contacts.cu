@@ -159,6 +159,18 @@ __device__ void pair_contacts(const GenParams& P, int sa, int sb, Emit& emit) {
   const Xf Xa = shape_world(P, a), Xb = shape_world(P, b);
   const V3 sa3 = load3(P.s.shape_scale + 3 * (size_t)a), sb3 = load3(P.s.shape_scale + 3 * (size_t)b);
   if (t1 == SAPB_SHAPE_PLANE && t2 == SAPB_SHAPE_PLANE) return;
+  if (t1 != SAPB_SHAPE_PLANE) {
+    // bounding spheres (a sphere's radius, a box's half diagonal): pairs
+    // farther apart than both plus sqrt(3) x (margins + gap) cannot touch
+    // (the box tests accept a corner up to that far out on every axis at
+    // once); the slack keeps the cut conservative under rounding
+    const double ra = t1 == SAPB_SHAPE_SPHERE ? sa3.x : sqrt(dot(sa3, sa3));
+    const double rb = t2 == SAPB_SHAPE_SPHERE ? sb3.x : sqrt(dot(sb3, sb3));
+    const V3 d = Xb.p - Xa.p;
+    const double reach =
+        (ra + rb + 1.7320508075688772 * (fabs(m1) + fabs(m2) + fabs(gap))) * (1.0 + 1.0e-12) + 1.0e-12;
+    if (dot(d, d) > reach * reach) return;
+  }
   if (t1 == SAPB_SHAPE_PLANE) {
     const V3 n = qrot(Xa.q, v3(0, 0, 1));
     if (t2 == SAPB_SHAPE_SPHERE) {
@@ -254,7 +266,7 @@ __global__ void count_kernel(const GenParams P, int32_t* counts) {
 }
 
 // Exclusive scan of counts in blocks of kScanBlock (block sums out), then of
-// the block sums by one block, then the offsets added.
+// the block sums by one block, then the offsets added in the write pass.
 __global__ void scan_blocks_kernel(const int32_t* in, int64_t n, int64_t* out, int64_t* block_sums) {
   __shared__ int64_t s[kScanBlock];
   const int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
@@ -272,15 +284,31 @@ __global__ void scan_blocks_kernel(const int32_t* in, int64_t n, int64_t* out, i
 }
 
 __global__ void scan_sums_kernel(int64_t* block_sums, int64_t nb, int32_t* total_out, int32_t capacity) {
-  // one thread: nb is small (pairs / 1024)
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int64_t acc = 0;
-  for (int64_t b = 0; b < nb; ++b) {
+  // one block: thread t sums a run of consecutive block sums, the runs'
+  // totals are scanned in shared memory, then each run is rewritten as
+  // exclusive offsets (integer sums: the same on every run)
+  __shared__ int64_t s[kScanBlock];
+  const int t = threadIdx.x;
+  const int64_t per = (nb + kScanBlock - 1) / kScanBlock;
+  const int64_t b0 = (int64_t)t * per;
+  const int64_t b1 = b0 + per < nb ? b0 + per : nb;
+  int64_t local = 0;
+  for (int64_t b = b0; b < b1; ++b) local += block_sums[b];
+  s[t] = local;
+  __syncthreads();
+  for (int o = 1; o < kScanBlock; o <<= 1) {
+    const int64_t x = t >= o ? s[t - o] : 0;
+    __syncthreads();
+    s[t] += x;
+    __syncthreads();
+  }
+  int64_t acc = s[t] - local;
+  for (int64_t b = b0; b < b1; ++b) {
     const int64_t v = block_sums[b];
     block_sums[b] = acc;
     acc += v;
   }
-  *total_out = (int32_t)(acc < capacity ? acc : capacity);
+  if (t == kScanBlock - 1) *total_out = (int32_t)(s[t] < capacity ? s[t] : capacity);
 }
 
 __global__ void write_kernel(const GenParams P, const int64_t* offsets, const int64_t* block_offsets,
@@ -331,7 +359,7 @@ int32_t contacts_launch(const sapb_collision_shapes* s, const double* body_q, co
   const unsigned blocks = (unsigned)((P.num_pairs + threads - 1) / threads);
   count_kernel<<<blocks, threads, 0, stream>>>(P, counts);
   scan_blocks_kernel<<<(unsigned)nb, kScanBlock, 0, stream>>>(counts, P.num_pairs, offsets, block_sums);
-  scan_sums_kernel<<<1, 1, 0, stream>>>(block_sums, nb, out->count, out->capacity);
+  scan_sums_kernel<<<1, kScanBlock, 0, stream>>>(block_sums, nb, out->count, out->capacity);
   write_kernel<<<blocks, threads, 0, stream>>>(P, offsets, block_sums, *out);
   const cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
