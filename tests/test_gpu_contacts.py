@@ -100,3 +100,37 @@ def test_box_worlds_step_with_generated_contacts(cuda_device):
     p1 = q1.reshape(-1, 7)[:, :3]
     assert float(p1[:, 2].min()) > -5e-3
     assert float((p1 - p0).norm(dim=1).max()) < 5e-2
+
+
+def test_capacity_clamps_and_keeps_the_prefix(cuda_device):
+    """More contacts than slots: the count is the capacity, the slots hold
+    the oracle's first contacts in order, and nothing past them is written."""
+    model, state, control, con, _, host = models.box_scene(2, 76, cuda_device, boxes=8, sites=(2, 3))
+    shapes = models.box_shapes(host)
+    bq, _ = ob.eval_fk(host["g"], host["q"].reshape(-1), np.zeros(model.joint_dof_count))
+    ref = oc.generate(shapes, bq, gap=2.0e-3)
+    total = len(ref["shape0"])
+    cap = total // 2
+    gen = ContactGenerator(shapes, _ModelView(model), capacity=cap + 5, gap=2.0e-3)
+    gen.outputs.capacity = cap  # the last five slots stay outside the buffer the kernel may write
+    gen.shape0.fill_(-7)
+    gen.generate(state.joint_q)
+    torch.cuda.synchronize()
+    assert int(gen.count.item()) == cap
+    np.testing.assert_array_equal(gen.shape0[:cap].cpu().numpy(), ref["shape0"][:cap])
+    np.testing.assert_allclose(gen.point1[:cap].cpu().numpy(), ref["point1"][:cap], rtol=1e-12, atol=1e-12)
+    assert bool((gen.shape0[cap:] == -7).all())
+
+
+def test_no_candidate_pairs(cuda_device):
+    """One shape per world and no static shape: no pair, count 0."""
+    model, state, control, con, _, host = models.box_scene(2, 77, cuda_device, boxes=1, sites=(1, 1))
+    shapes = models.box_shapes(host)
+    one = ShapeSet(num_worlds=2, shapes_per_world=1, num_global_shapes=0, shape_type=shapes.shape_type[:2],
+                   shape_scale=shapes.shape_scale[:2], shape_X_bs=shapes.shape_X_bs[:2],
+                   shape_body=shapes.shape_body[:2])
+    gen = ContactGenerator(one, _ModelView(model), capacity=16)
+    gen.count.fill_(3)
+    gen.generate(state.joint_q)
+    torch.cuda.synchronize()
+    assert int(gen.count.item()) == 0
