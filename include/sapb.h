@@ -375,7 +375,8 @@ typedef struct sapb_collision_shapes {
 
 typedef struct sapb_contact_outputs {
   int32_t capacity;
-  int32_t* count;                   /* [1] contacts written (clamped to capacity) */
+  int32_t* count;                   /* [1] contacts found (may exceed capacity: then only the first
+                                       capacity, in pair order, are written; INT32_MAX saturates) */
   int32_t* shape0;                  /* [capacity] */
   int32_t* shape1;
   double* point0;                   /* [capacity][3] */

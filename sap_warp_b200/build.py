@@ -2,7 +2,9 @@
 
 ``python -m sap_warp_b200.build`` compiles every ``csrc/*.cu`` into
 ``sap_warp_b200/libsapb.so``.  The library is built in the source tree so it
-travels with the repository to the machine that runs it.
+travels with the repository to the machine that runs it.  Each source is
+compiled to a relocatable-free object in parallel (one nvcc per source), then
+the objects are linked into the shared library.
 """
 
 from __future__ import annotations
@@ -11,6 +13,8 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG_DIR = Path(__file__).resolve().parent
@@ -20,7 +24,7 @@ LIB_NAME = "libsapb.so"
 LIB_PATH = PKG_DIR / LIB_NAME
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
+COMPILE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 
 def _nvcc() -> str:
@@ -42,17 +46,30 @@ def needs_build() -> bool:
     return any(p.stat().st_mtime > lib_mtime for p in deps)
 
 
-def build_library(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the CUDA sources into the in-tree shared library."""
-    if not force and not needs_build():
-        return LIB_PATH
-    tmp = LIB_PATH.with_suffix(".so.tmp")
-    cmd = [_nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, "-I", str(INCLUDE), "-o", str(tmp), *map(str, sources())]
+def _run(cmd: list[str], verbose: bool) -> None:
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
+        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+
+
+def build_library(force: bool = False, verbose: bool = False, jobs: int | None = None) -> Path:
+    """Compile the CUDA sources into the in-tree shared library."""
+    if not force and not needs_build():
+        return LIB_PATH
+    nvcc = _nvcc()
+    srcs = sources()
+    jobs = jobs or min(len(srcs), max(os.cpu_count() or 1, 1))
+    with tempfile.TemporaryDirectory(prefix="sapb_build_") as tmpdir:
+        objs = [Path(tmpdir) / (s.stem + ".o") for s in srcs]
+        cmds = [[nvcc, *ARCH_FLAGS, *COMPILE_FLAGS, "-I", str(INCLUDE), "-c", "-o", str(o), str(s)]
+                for s, o in zip(srcs, objs)]
+        with ThreadPoolExecutor(max_workers=jobs) as ex:
+            for f in [ex.submit(_run, c, verbose) for c in cmds]:
+                f.result()
+        tmp = LIB_PATH.with_suffix(".so.tmp")
+        _run([nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *map(str, objs)], verbose)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 

@@ -39,6 +39,10 @@ class ShapeSet:
     shape_margin: np.ndarray | None = None  # [S]
 
 
+class ContactOverflowError(RuntimeError):
+    """More contacts were found than the contact buffer holds."""
+
+
 class ContactGenerator:
     """Owns the device buffers of contact generation for one ShapeSet and a
     model view; `generate(joint_q)` runs the forward kinematics of the
@@ -80,7 +84,13 @@ class ContactGenerator:
         O.margin0, O.margin1 = self.margin0.data_ptr(), self.margin1.data_ptr()
         self.outputs = O
 
-    def generate(self, joint_q: torch.Tensor) -> SapContacts:
+    def generate(self, joint_q: torch.Tensor, *, check_capacity: bool = False) -> SapContacts:
+        """Contacts at the coordinates joint_q.  The count buffer receives
+        the number of contacts found, which exceeds the capacity when the
+        buffer overflowed (only the first `capacity`, in pair order, are
+        written; the step reads at most that many).  check_capacity=True reads
+        the count back (a host synchronisation) and raises ContactOverflowError
+        on overflow; otherwise call `overflowed()` when convenient."""
         lib = load()
         stream = ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)
         q = joint_q if (joint_q.dtype == F64 and joint_q.is_contiguous()) else joint_q.to(F64).contiguous()
@@ -94,6 +104,10 @@ class ContactGenerator:
         self.normalf.copy_(self.normal)
         self.margin0f.copy_(self.margin0)
         self.margin1f.copy_(self.margin1)
+        if check_capacity and self.overflowed():
+            raise ContactOverflowError(
+                f"contact generation found {int(self.count.item())} contacts for {self.outputs.capacity} slots; "
+                "the contacts past the capacity were dropped")
         return SapContacts(rigid_contact_count=self.count, rigid_contact_shape0=self.shape0,
                            rigid_contact_shape1=self.shape1, rigid_contact_point0=self.point0f,
                            rigid_contact_point1=self.point1f, rigid_contact_normal=self.normalf,
@@ -101,3 +115,11 @@ class ContactGenerator:
                            rigid_contact_point0d=self.point0, rigid_contact_point1d=self.point1,
                            rigid_contact_normald=self.normal, rigid_contact_margin0d=self.margin0,
                            rigid_contact_margin1d=self.margin1)
+
+    def found(self) -> int:
+        """Contacts found by the last generate() (reads the device count)."""
+        return int(self.count.item())
+
+    def overflowed(self) -> bool:
+        """Whether the last generate() found more contacts than the capacity."""
+        return self.found() > int(self.outputs.capacity)

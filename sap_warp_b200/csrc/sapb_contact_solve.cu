@@ -1,974 +1,9 @@
-// sapb_contact_solve.cu -- fused SAP stage-2 Newton solve, one CTA per world.
-//
-// Restates SapContactSolve.solve (sim/contact_solve.py:6129-6285) as ONE
-// persistent launch.  A CTA pulls a world index from a device counter, stages
-// the world's contact Jacobian J in shared memory once, and runs prepare
-// (:4285-4429), the Newton loop (:5474-5655) and the chosen line search
-// (:2207-3175) on chip.  The dynamics matrix A is read through L1 (it is the
-// only per-world array re-read from outside shared memory; 3-4 passes per
-// Newton iteration hit L1/L2).  Per line-search trial the kernel touches
-// O(contacts + DOFs) data because the contact velocity along the search line
-// is vc + alpha * (J dv) (vc is linear in v); the reference issues ~35
-// launches per Newton iteration and re-reads A and J on every trial.
-//
-// Precision: the gradient, costs, line search, velocity update and the
-// convergence test are FP64.  The Hessian H = A + J^T G J + diag and its LDL^T
-// factorization run in HT (double, or float for the mixed path).
-#include <cuda_runtime.h>
-
-#include <cstdint>
-#include <cstdio>
-#include <cstring>
-
-#include "sapb_device.cuh"
-#include "sapb_internal.h"
-#include "sapb_ldlt.cuh"
-#include "sapb_linesearch.cuh"
+// sapb_contact_solve.cu -- host side of the fused contact solve: shared-
+// memory size, occupancy query and the dispatch to the DOF specialisations
+// (kernels in sapb_contact_solve.cuh, instantiated in sapb_solve_n*.cu).
+#include "sapb_contact_solve.cuh"
 
 namespace sapb {
-
-struct SolveParams {
-  sapb_contact_problem p;
-  sapb_dof_terms dof;  // copy of *p.dof (has_pd/has_limits 0 if none)
-  sapb_solve_options o;
-  sapb_solve_outputs out;
-  int32_t use_guess_flag_ptr_valid;
-  int32_t* queue;      // work counter (zeroed before launch)
-};
-
-__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
-// Shared-memory layout of one world.  ldJ: room for the 4-wide Hessian tiles
-// and odd, so thread-per-row reads of J are free of bank conflicts.  ldH odd
-// for conflict-free column reads in the factorization.
-struct Layout {
-  int n, C, ldJ, ldH, nb;
-  size_t off_J, off_scr, off_H, off_G, off_vec, off_con, off_flags, off_tri, total;
-  static constexpr int kVecs = 23;
-  static constexpr int kConPer = 17;
-  static constexpr int kMaxWarps = 4;  // partial-sum scratch (blocks of <= 128 threads)
-};
-
-__host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
-  Layout L;
-  L.n = n;
-  L.C = C;
-  L.ldJ = (n + 3) / 4 * 4 + 1;
-  L.ldH = (n % 2 == 0) ? n + 1 : n;
-  L.nb = (n + 3) / 4;
-  size_t o = 0;
-  L.off_J = o;
-  o = align_up(o + sizeof(double) * (size_t)3 * C * L.ldJ, 16);
-  L.off_scr = o;  // the partial sums of the DOF products, or two staged impulse sets
-  {
-    const size_t part = sizeof(double) * 3 * Layout::kMaxWarps * 64;
-    const size_t gam = sizeof(double) * 6 * (size_t)(C > 0 ? C : 1);
-    o = align_up(o + (part > gam ? part : gam), 16);
-  }
-  L.off_H = o;
-  o = align_up(o + (size_t)hsize * n * L.ldH, 16);
-  L.off_G = o;
-  o = align_up(o + sizeof(double) * 9 * (size_t)(C > 0 ? C : 1), 16);
-  L.off_vec = o;
-  o = align_up(o + sizeof(double) * (size_t)Layout::kVecs * L.ldJ, 16);
-  L.off_con = o;
-  o = align_up(o + sizeof(double) * (size_t)Layout::kConPer * (C > 0 ? C : 1), 16);
-  L.off_flags = o;
-  o = align_up(o + sizeof(int) * (size_t)L.ldJ, 16);
-  L.off_tri = o;  // (i << 8 | j) of the lower triangle below row 0, columns descending
-  o = align_up(o + sizeof(uint16_t) * (size_t)(n * (n - 1) / 2 + 1), 16);
-  L.total = o;
-  return L;
-}
-
-static_assert(V_END <= Layout::kVecs, "vector slots");
-static_assert(C_END <= Layout::kConPer, "contact slots");
-
-template <int NT, typename HT, int NS>
-struct World {
-  Layout L;
-  const double* A;  // global, this world's [n][n]
-  double* J;
-  HT* GJ;           // scratch: the partial sums of the DOF products, or staged impulse sets
-  HT* H;
-  double* G;        // [C][9]
-  double* vec;
-  double* con;
-  int* flags;
-  const uint16_t* tri;
-  double* red;
-  int n, count;
-  // DOF count and leading dimensions: compile-time constants when NS > 0.
-  __device__ __forceinline__ int dofs() const { return NS > 0 ? NS : n; }
-  __device__ __forceinline__ int ldJ() const { return NS > 0 ? (NS + 3) / 4 * 4 + 1 : L.ldJ; }
-  __device__ __forceinline__ int ldH() const { return NS > 0 ? ((NS % 2 == 0) ? NS + 1 : NS) : L.ldH; }
-  __device__ __forceinline__ int nb() const { return NS > 0 ? (NS + 3) / 4 : L.nb; }
-  __device__ double* V(int k) const { return vec + (size_t)k * ldJ(); }
-  __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
-  __device__ double* part(int which, int warp) const {
-    return reinterpret_cast<double*>(GJ) + ((size_t)which * Layout::kMaxWarps + warp) * 64;
-  }
-  __device__ ContactConst cc(int c) const {
-    ContactConst x;
-    x.rt = Cn(C_RT)[c];
-    x.rn = Cn(C_RN)[c];
-    x.rt_inv = Cn(C_RTINV)[c];
-    x.rn_inv = Cn(C_RNINV)[c];
-    x.vhat_n = Cn(C_VHAT)[c];
-    x.mu = Cn(C_MU)[c];
-    x.mu_hat = Cn(C_MUHAT)[c];
-    x.factor = Cn(C_FACTOR)[c];
-    return x;
-  }
-};
-
-// vc-type products: rows r < 3*count of J times x (length n, shared) into the
-// contact slots `slot..slot+2`.  One thread per row.
-template <int NT, typename HT, int NS>
-__device__ void contact_rows_times(const World<NT, HT, NS>& w, const double* x, int slot) {
-  const int rows = 3 * w.count;
-  for (int r = threadIdx.x; r < rows; r += NT) {
-    const double* row = w.J + (size_t)r * w.ldJ();
-    double s0 = 0.0, s1 = 0.0;
-    int j = 0;
-    for (; j + 1 < w.dofs(); j += 2) {
-      s0 += row[j] * x[j];
-      s1 += row[j + 1] * x[j + 1];
-    }
-    if (j < w.dofs()) s0 += row[j] * x[j];
-    const int c = r / 3, k = r - 3 * c;
-    w.Cn(slot + k)[c] = s0 + s1;
-  }
-}
-
-// Partial sums of the per-DOF products over a warp's share of the columns of
-// A and of the contacts: part(0)[i] = sum_j A[j][i] x[j], part(1)[i] =
-// sum_j A[j][i] y[j], part(2)[i] = sum_c J_c[:, i] . gamma_c.  Lanes own DOFs
-// i = lane and lane + 32, so a warp reads consecutive addresses.
-template <int NT, typename HT, int NS>
-__device__ void dof_partials(const World<NT, HT, NS>& w, const double* x, const double* y, bool with_gamma) {
-  constexpr int NW = NT / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int n = w.dofs();
-  const int jchunk = (n + NW - 1) / NW;
-  const int j0 = warp * jchunk, j1 = min(n, j0 + jchunk);
-  const int cchunk = (w.count + NW - 1) / NW;
-  const int c0 = warp * cchunk, c1 = min(w.count, c0 + cchunk);
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int i = lane + 32 * h;
-    if (i >= n) continue;
-    double a = 0.0, b = 0.0, g = 0.0;
-    for (int j = j0; j < j1; ++j) {
-      const double aij = __ldg(w.A + (size_t)j * n + i);
-      a += aij * x[j];
-      if (y) b += aij * y[j];
-    }
-    if (with_gamma) {
-      const int ld = w.ldJ();
-      for (int c = c0; c < c1; ++c) {
-        const double* Jc = w.J + (size_t)(3 * c) * ld + i;
-        g += Jc[0] * w.Cn(C_GAMMA + 0)[c] + Jc[ld] * w.Cn(C_GAMMA + 1)[c] + Jc[2 * ld] * w.Cn(C_GAMMA + 2)[c];
-      }
-    }
-    w.part(0, warp)[i] = a;
-    w.part(1, warp)[i] = b;
-    w.part(2, warp)[i] = g;
-  }
-}
-
-template <int NT, typename HT, int NS>
-__device__ __forceinline__ double sum_partials(const World<NT, HT, NS>& w, int which, int i) {
-  constexpr int NW = NT / 32;
-  double s = 0.0;
-#pragma unroll
-  for (int k = 0; k < NW; ++k) s += w.part(which, k)[i];
-  return s;
-}
-
-// Objective at the current v (shared V_V): contact gamma and cost, A(v-v*),
-// J^T gamma, PD and limit terms, gradient.  Returns {cost, |g|^2, |p|^2, |jc|^2}
-// (scaled, over participating DOFs) to every thread.  Restates
-// _solver_update_active sim/contact_solve.py:4080-4136.
-template <int NT, typename HT, int NS>
-__device__ void evaluate(const World<NT, HT, NS>& w, const SolveParams& P, double dt, double out4[4]) {
-  const int tid = threadIdx.x;
-  contact_rows_times<NT, HT, NS>(w, w.V(V_V), C_VC);
-  for (int i = tid; i < w.dofs(); i += NT) w.V(V_TMP0)[i] = w.V(V_V)[i] - w.V(V_VSTAR)[i];
-  __syncthreads();
-  double csum = 0.0;
-  for (int c = tid; c < w.count; c += NT) {
-    double g[3], cost;
-    project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cost, nullptr);
-    w.Cn(C_GAMMA + 0)[c] = g[0];
-    w.Cn(C_GAMMA + 1)[c] = g[1];
-    w.Cn(C_GAMMA + 2)[c] = g[2];
-    csum += cost;
-  }
-  __syncthreads();
-  dof_partials<NT, HT, NS>(w, w.V(V_TMP0), w.V(V_V), true);
-  __syncthreads();
-  double model_cost = 0.0, g2 = 0.0, p2 = 0.0, j2 = 0.0;
-  const double* v = w.V(V_V);
-  const double* vs = w.V(V_VSTAR);
-  for (int i = tid; i < w.dofs(); i += NT) {
-    const double a_res = sum_partials<NT, HT, NS>(w, 0, i);
-    const double a_v = sum_partials<NT, HT, NS>(w, 1, i);
-    double imp = sum_partials<NT, HT, NS>(w, 2, i);
-    const double vi = v[i];
-    double mc = 0.5 * (vi - vs[i]) * a_res;
-    const int fl = w.flags[i];
-    double pdg = 0.0, hd = 0.0;
-    if (P.dof.has_pd && (fl & kFlagPd)) {
-      const double gain = w.V(V_PDGAIN)[i], lim = w.V(V_PDLIM)[i];
-      const double y = w.V(V_PDA)[i] - gain * vi;
-      pdg = dt * clamp_limit(y, lim);
-      hd += dt * gain * clamp_limit_derivative(y, lim);
-      if (gain > 0.0) mc += (dt / gain) * clamp_limit_antiderivative(y, lim);
-    }
-    double lg = 0.0;
-    if (P.dof.has_limits) {
-      double lc = 0.0;
-      if (fl & kFlagLo) {
-        const double g = w.V(V_LORINV)[i] * (w.V(V_LOVHAT)[i] - vi);
-        if (g > 0.0) {
-          lg += g;
-          hd += w.V(V_LORINV)[i];
-          lc += 0.5 * w.V(V_LOR)[i] * g * g;
-        }
-      }
-      if (fl & kFlagUp) {
-        const double g = w.V(V_UPRINV)[i] * (w.V(V_UPVHAT)[i] + vi);
-        if (g > 0.0) {
-          lg -= g;
-          hd += w.V(V_UPRINV)[i];
-          lc += 0.5 * w.V(V_UPR)[i] * g * g;
-        }
-      }
-      mc += lc;
-    }
-    imp += pdg + lg;
-    const double grad = a_res - imp;
-    w.V(V_ARES)[i] = a_res;
-    w.V(V_GRAD)[i] = grad;
-    w.V(V_HDIAG)[i] = hd;
-    model_cost += mc;
-    if (fl & kFlagPart) {
-      const double s = w.V(V_DSCALE)[i];
-      const double gs = s * grad, ps = s * a_v, js = s * imp;
-      g2 += gs * gs;
-      p2 += ps * ps;
-      j2 += js * js;
-    }
-  }
-  double r[4] = {csum + model_cost, g2, p2, j2};
-  block_sum<NT, 4>(r, w.red);
-  out4[0] = r[0];
-  out4[1] = r[1];
-  out4[2] = r[2];
-  out4[3] = r[3];
-}
-
-// H (lower triangle, HT) <- the lower triangle of the FP64 n x n matrix M in
-// global memory (+ diag_add on the diagonal): flat coalesced reads, four
-// loads in flight per thread.
-template <int NT, typename HT, int NS>
-__device__ __forceinline__ void load_lower(const World<NT, HT, NS>& w, const double* M, const double* diag_add,
-                                           double shift) {
-  const int tid = threadIdx.x;
-  const int n = w.dofs(), ldH = w.ldH();
-  const int total = n * n;
-  for (int k0 = tid; k0 < total; k0 += 4 * NT) {
-    double val[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int k = k0 + u * NT;
-      val[u] = k < total ? __ldg(M + k) : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int k = k0 + u * NT;
-      if (k < total) {
-        const int i = k / n, j = k - i * n;
-        if (j < i) w.H[(size_t)i * ldH + j] = HT(val[u]);
-        else if (j == i) w.H[(size_t)i * ldH + j] = HT(val[u] + (diag_add ? diag_add[i] : 0.0) + shift);
-      }
-    }
-  }
-}
-
-// H = A + J^T G J + diag(PD + limit + shift), lower triangle, in HT.
-// G at the stored vc per contact; each thread owns one 4x4 tile of H and one
-// of KS slices of the contacts and accumulates J_c^T (G_c J_c) for its tile
-// in registers (G J formed per contact for the tile's columns: no staging,
-// no barriers between contacts); the slices of a tile are summed by warp
-// shuffles (KS a power of two) or add into H in turn, in a fixed order
-// (deterministic).
-template <int NT, typename HT, int NS>
-__device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) {
-  const int tid = threadIdx.x;
-  const int n = w.dofs(), ldJ = w.ldJ(), ldH = w.ldH(), nb = w.nb();
-  // G at the current contact velocities (sim/contact_solve.py:1071-1217).
-  for (int c = tid; c < w.count; c += NT) {
-    double g[3], cost, G[9];
-    project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cost, G);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) w.G[9 * c + k] = G[k];
-  }
-  // H lower = A lower + diagonal terms
-  load_lower<NT, HT, NS>(w, w.A, w.V(V_HDIAG), diag_shift);
-  const int tiles = nb * (nb + 1) / 2;
-  int ks = NT / (tiles > 0 ? tiles : 1);
-  if (ks < 1) ks = 1;
-  if (ks > 4) ks = 4;
-  const int items = tiles * ks;
-  // This thread's item (a thread holds at most one: items <= NT is checked
-  // on the host; n <= 64 gives tiles <= 136, ks >= 1).
-  const bool has_item = tid < items;
-  int bi = 0, bj = 0, slice = 0;
-  if (has_item) {
-    const int t = tid / ks;
-    slice = tid - t * ks;
-    while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
-    bj = t - bi * (bi + 1) / 2;
-  }
-  HT acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = HT(0);
-  __syncthreads();  // G ready, H initialised
-  if (has_item) {
-    // this slice's contacts; per contact G J for the tile's 4 columns, then
-    // the tile's rank-3 update J_c[:, 4 bi..]^T (G J_c)[:, 4 bj..]
-    const int per = (w.count + ks - 1) / ks;
-    const int c0 = slice * per, c1 = min(w.count, c0 + per);
-    for (int c = c0; c < c1; ++c) {
-      const double* Jc = w.J + (size_t)(3 * c) * ldJ;
-      HT ja[3][4], jb[3][4], G[9];
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          ja[k][q] = HT(Jc[(size_t)k * ldJ + 4 * bi + q]);
-          jb[k][q] = HT(Jc[(size_t)k * ldJ + 4 * bj + q]);
-        }
-#pragma unroll
-      for (int k = 0; k < 9; ++k) G[k] = HT(w.G[9 * c + k]);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        HT gj[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) gj[q] = G[3 * k] * jb[0][q] + G[3 * k + 1] * jb[1][q] + G[3 * k + 2] * jb[2][q];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) acc[a][q] += ja[k][a] * gj[q];
-      }
-    }
-  }
-  auto add_tile = [&]() {
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int i = 4 * bi + a;
-      if (i >= n) continue;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int j = 4 * bj + b;
-        if (j > i || j >= n) continue;
-        w.H[(size_t)i * ldH + j] += acc[a][b];
-      }
-    }
-  };
-  if ((ks & (ks - 1)) == 0) {
-    // the ks slices of a tile are ks consecutive lanes of one warp: sum them
-    // by shuffles (fixed order), slice 0 adds the tile
-    for (int o = ks >> 1; o > 0; o >>= 1) {
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] += __shfl_down_sync(0xffffffffu, acc[a][b], o);
-    }
-    if (has_item && slice == 0) add_tile();
-    __syncthreads();
-  } else {
-    for (int s = 0; s < ks; ++s) {
-      if (has_item && slice == s) add_tile();
-      __syncthreads();
-    }
-  }
-}
-
-// In-place LDL^T of the lower triangle of H: unit L stored below the
-// diagonal unscaled as H_ik (= L_ik d_k), D on the diagonal, 1/d_k in V_DINV.
-// Then the solve H dv = -grad (solve_factored).  Mathematically the Cholesky
-// solve of the reference's BlockCholeskySolverBatched
-// (sim/blocked_cholesky.py:414-604), with the blocked schedule of
-// ldlt_blocked (a single-warp column-by-column schedule measured no faster
-// in FP32 and slower in FP64 on the 35-DOF humanoid).
-template <int NT, typename HT, int NS>
-__device__ void solve_factored(const World<NT, HT, NS>& w);
-
-template <int NT, typename HT, int NS>
-__device__ void factor_and_solve(const World<NT, HT, NS>& w) {
-  ldlt_blocked<NT, HT>(w.H, w.dofs(), w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri);
-  solve_factored<NT, HT, NS>(w);
-}
-
-// out = -H^-1 rhs (vector slots) with the LDL^T that factor_and_solve left
-// in H and V_DINV, by warp `warp` alone (lanes own rows lane, lane + 32; no
-// block barrier).  A pivot that is not positive / finite makes out NaN.
-template <int NT, typename HT, int NS>
-__device__ void solve_warp(const World<NT, HT, NS>& w, int rhs_slot, int out_slot, int warp) {
-  const int tid = threadIdx.x;
-  const int n = w.dofs(), ldH = w.ldH();
-  const HT* H = w.H;
-  const HT* dinv = reinterpret_cast<const HT*>(w.V(V_DINV));
-  double* dv = w.V(out_slot);
-  const double* rhs = w.V(rhs_slot);
-  if ((tid >> 5) == warp) {
-    bool ok = true;
-    for (int k = 0; k < n; ++k) {
-      const HT d = H[(size_t)k * ldH + k];
-      if (!(d > HT(0)) || !isfinite(double(d))) ok = false;
-    }
-    // Forward z = D^-1 (L^-1 b), backward x = L^-T z; lanes own rows lane, lane+32.
-    const int lane = tid & 31;
-    HT hb0 = HT(0), hb1 = HT(0);
-    if (lane < n) hb0 = HT(-rhs[lane]);
-    if (lane + 32 < n) hb1 = HT(-rhs[lane + 32]);
-    for (int k = 0; k < n; ++k) {
-      const HT bk = __shfl_sync(0xffffffffu, k < 32 ? hb0 : hb1, k & 31);
-      const HT zk = bk * dinv[k];
-      if (lane == (k & 31)) {
-        if (k < 32) hb0 = zk;
-        else hb1 = zk;
-      }
-      if (lane > k && lane < n) hb0 -= H[(size_t)lane * ldH + k] * zk;
-      if (lane + 32 > k && lane + 32 < n) hb1 -= H[(size_t)(lane + 32) * ldH + k] * zk;
-    }
-    HT s0 = HT(0), s1 = HT(0);
-    for (int i = n - 1; i >= 0; --i) {
-      HT xi_local = HT(0);
-      if (lane == (i & 31)) {
-        const HT zi = i < 32 ? hb0 : hb1;
-        const HT si = i < 32 ? s0 : s1;
-        xi_local = zi - si * dinv[i];
-        if (i < 32) hb0 = xi_local;
-        else hb1 = xi_local;
-      }
-      const HT xi = __shfl_sync(0xffffffffu, xi_local, i & 31);
-      if (lane < i) s0 += H[(size_t)i * ldH + lane] * xi;
-      if (lane + 32 < i) s1 += H[(size_t)i * ldH + lane + 32] * xi;
-    }
-    const double nanv = __longlong_as_double(0x7ff8000000000000ULL);
-    if (lane < n) dv[lane] = ok ? double(hb0) : nanv;
-    if (lane + 32 < n) dv[lane + 32] = ok ? double(hb1) : nanv;
-  }
-}
-
-// dv = -H^-1 grad (warp 0), then a block barrier.  (One warp's serial
-// substitution beats a block-wide blocked solve here: the latter's two
-// barriers per block cost more than the warp's chain on the 35-DOF worlds.)
-template <int NT, typename HT, int NS>
-__device__ void solve_factored(const World<NT, HT, NS>& w) {
-  solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
-  __syncthreads();
-}
-
-// Line coefficients (sim/contact_solve.py:2234-2263, 1657-1692):
-// dp = A dv, dvc = J dv and {dell0, dell_a0, d2ell_a, mom0}.
-template <int NT, typename HT, int NS>
-__device__ void line_coefficients(const World<NT, HT, NS>& w, double c4[4]) {
-  const int tid = threadIdx.x;
-  contact_rows_times<NT, HT, NS>(w, w.V(V_DV), C_DVC);
-  dof_partials<NT, HT, NS>(w, w.V(V_DV), nullptr, false);
-  __syncthreads();
-  double d0 = 0.0, da0 = 0.0, d2 = 0.0, m0 = 0.0;
-  const double* v = w.V(V_V);
-  const double* vs = w.V(V_VSTAR);
-  const double* dv = w.V(V_DV);
-  for (int i = tid; i < w.dofs(); i += NT) {
-    const double acc = sum_partials<NT, HT, NS>(w, 0, i);
-    w.V(V_DP)[i] = acc;
-    const double ri = v[i] - vs[i];
-    d0 += w.V(V_GRAD)[i] * dv[i];
-    da0 += acc * ri;
-    d2 += dv[i] * acc;
-    m0 += 0.5 * ri * w.V(V_ARES)[i];
-  }
-  double r[4] = {d0, da0, d2, m0};
-  block_sum<NT, 4>(r, w.red);  // its barriers also publish dvc / dp
-  c4[0] = r[0];
-  c4[1] = r[1];
-  c4[2] = r[2];
-  c4[3] = r[3];
-}
-
-// LSV: the line search, fixed at compile time (SAPB_LS_ARMIJO_DECAY,
-// SAPB_LS_EXACT_ROOT or SAPB_LS_MONOTONE_DECAY) so that one instantiation
-// holds the code of one search only (smaller instruction footprint).
-template <int NT, typename HT, int MINB, int NS, int LSV>
-__global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolveParams P) {
-  static_assert(NT / 32 <= Layout::kMaxWarps, "partial-sum scratch sized for kMaxWarps warps");
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double red[8 * (NT / 32)];
-  __shared__ int s_next;
-  __shared__ unsigned long long s_partmask;
-  const int tid = threadIdx.x;
-  const int n = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
-  const Layout L = make_layout(n, C, (int)sizeof(HT));
-  const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
-  build_triangle_list<NT>(reinterpret_cast<uint16_t*>(smem + L.off_tri), n);
-
-  if (tid == 0) s_next = atomicAdd(P.queue, 1);
-  for (;;) {
-    // Take the prefetched index, claim the next world and warm L2 with its A
-    // and J (prefetch.global.L2 is a hint and has no alignment rule).
-    __syncthreads();
-    const int ticket = s_next;
-    if (ticket >= P.p.num_envs) break;
-    const int e = P.p.world_order ? P.p.world_order[ticket] : ticket;
-    __syncthreads();
-    if (tid == 0) s_next = atomicAdd(P.queue, 1);
-    __syncthreads();
-    if (e < 0 || e >= P.p.num_envs) continue;
-    {
-      const int nt = s_next;
-      const int nx = nt < P.p.num_envs ? (P.p.world_order ? P.p.world_order[nt] : nt) : P.p.num_envs;
-      if (nx >= 0 && nx < P.p.num_envs) {
-        const char* a0 = reinterpret_cast<const char*>(P.p.dynamics_matrix + (size_t)nx * n * n);
-        const size_t abytes = sizeof(double) * (size_t)n * n;
-        int cnt = P.p.contact_count[nx];
-        cnt = cnt < 0 ? 0 : (cnt > C ? C : cnt);
-        const char* j0 = reinterpret_cast<const char*>(P.p.jacobian + (size_t)nx * C * 3 * n);
-        const size_t jbytes = sizeof(double) * (size_t)cnt * 3 * n;
-        for (size_t off = (size_t)tid * 128; off < abytes; off += (size_t)NT * 128)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(a0 + off));
-        for (size_t off = (size_t)tid * 128; off < jbytes; off += (size_t)NT * 128)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(j0 + off));
-        if (P.p.gamma0) {
-          if (P.p.dynamics_factor) {
-            const char* f0 = reinterpret_cast<const char*>(P.p.dynamics_factor + (size_t)nx * n * n);
-            for (size_t off = (size_t)tid * 128; off < abytes; off += (size_t)NT * 128)
-              asm volatile("prefetch.global.L2 [%0];" ::"l"(f0 + off));
-          }
-          const int K = P.p.gamma0_count > 1 ? P.p.gamma0_count : 1;
-          const size_t gbytes = sizeof(double) * (size_t)cnt * 3;
-          for (int k = 0; k < K; ++k) {
-            const char* g0 = reinterpret_cast<const char*>(P.p.gamma0 + ((size_t)k * P.p.num_envs + nx) * C * 3);
-            for (size_t off = (size_t)tid * 128; off < gbytes; off += (size_t)NT * 128)
-              asm volatile("prefetch.global.L2 [%0];" ::"l"(g0 + off));
-          }
-        }
-      }
-    }
-
-    World<NT, HT, NS> w{L,
-                    P.p.dynamics_matrix + (size_t)e * n * n,
-                    reinterpret_cast<double*>(smem + L.off_J),
-                    reinterpret_cast<HT*>(smem + L.off_scr),
-                    reinterpret_cast<HT*>(smem + L.off_H),
-                    reinterpret_cast<double*>(smem + L.off_G),
-                    reinterpret_cast<double*>(smem + L.off_vec),
-                    reinterpret_cast<double*>(smem + L.off_con),
-                    reinterpret_cast<int*>(smem + L.off_flags),
-                    reinterpret_cast<const uint16_t*>(smem + L.off_tri),
-                    red,
-                    n,
-                    0};
-    int count = P.p.contact_count[e];
-    if (count > C) count = C;
-    if (count < 0) count = 0;
-    w.count = count;
-    const double dt = P.p.dt[e];
-    const size_t base = (size_t)e * n;
-
-    // ---- stage J, per-contact constants and vectors -------------------------
-    {
-      const int rows = 3 * count;
-      const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n;
-      const int ldj = w.ldJ();
-      // Flat copy of the contiguous rows*n block by asynchronous 8-byte
-      // copies (all in flight at once, completed before the barrier after the
-      // per-DOF setup below; the rows land at stride ldj).
-      const int total = rows * n;
-      for (int k = tid; k < total; k += NT) {
-        const int r = k / n, j = k - r * n;
-        const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(w.J + (size_t)r * ldj + j));
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(Jg + k) : "memory");
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      // zero padding columns n..ldj-1
-      for (int k = tid; k < rows * (ldj - n); k += NT) {
-        const int r = k / (ldj - n), j = n + (k - r * (ldj - n));
-        w.J[(size_t)r * ldj + j] = 0.0;
-      }
-      for (int c = tid; c < count; c += NT) {
-        const size_t ci = (size_t)e * C + c;
-        const double tau = P.p.tau_d ? P.p.tau_d[ci] : P.o.contact_tau_d;
-        const ContactConst cc = make_contact_const(P.p.phi0[ci], P.p.w_eff[ci], P.p.mu[ci], P.p.stiffness[ci], tau,
-                                                   P.o.contact_beta, P.o.contact_sigma, dt);
-        w.Cn(C_RT)[c] = cc.rt;
-        w.Cn(C_RN)[c] = cc.rn;
-        w.Cn(C_RTINV)[c] = cc.rt_inv;
-        w.Cn(C_RNINV)[c] = cc.rn_inv;
-        w.Cn(C_VHAT)[c] = cc.vhat_n;
-        w.Cn(C_MU)[c] = cc.mu;
-        w.Cn(C_MUHAT)[c] = cc.mu_hat;
-        w.Cn(C_FACTOR)[c] = cc.factor;
-      }
-      for (int i = tid; i < L.ldJ; i += NT) {
-        if (i < n) {
-          w.V(V_VSTAR)[i] = P.p.v_star[base + i];
-          double v = P.p.v0[base + i];
-          if (P.p.v_guess) {
-            if (use_guess) v = P.p.v_guess[base + i];
-            P.p.v_guess[base + i] = v;
-          }
-          w.V(V_V)[i] = v;
-          double d = __ldg(w.A + (size_t)i * n + i);
-          if (d < 1.0e-12 || !isfinite(d)) d = 1.0e-12;
-          w.V(V_AINV)[i] = 1.0 / d;
-          w.V(V_DSCALE)[i] = 1.0 / sqrt(d);
-        } else {
-          for (int k = 0; k < Layout::kVecs; ++k) w.V(k)[i] = 0.0;
-        }
-      }
-    }
-    // ---- PD and limit terms (sim/contact_solve.py:490-683) ------------------
-    for (int i = tid; i < n; i += NT) {
-      int fl = 0;
-      const size_t dof = base + i;
-      const sapb_dof_terms& D = P.dof;
-      if (D.has_pd) {
-        int coord = D.dof_coord_index[dof];
-        if (coord >= D.joint_coord_count) coord = -1;
-        int target = D.dof_target_index[dof];
-        if (target < 0 || target >= P.p.num_envs * n) target = (int)dof;
-        if (D.joint_target_mode[target] != 0) {
-          const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
-          if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {
-            double kpe, kde;
-            effective_pd_gains(kp, kd, dt, w.V(V_AINV)[i], &kpe, &kde);
-            const double gain = dt * kpe + kde;
-            if (gain > 0.0) {
-              double q0 = 0.0, qd = 0.0;
-              if (coord >= 0) {
-                q0 = D.joint_q[coord];
-                qd = D.joint_target_pos ? (double)D.joint_target_pos[target] : 0.0;
-              }
-              const double vd = D.joint_target_vel ? (double)D.joint_target_vel[target] : 0.0;
-              const double u0 = D.joint_act ? (double)D.joint_act[target] : 0.0;
-              fl |= kFlagPd;
-              w.V(V_PDA)[i] = kpe * (qd - q0) + kde * vd + u0;
-              w.V(V_PDGAIN)[i] = gain;
-              w.V(V_PDLIM)[i] = (double)D.joint_effort_limit[target];
-            }
-          }
-        }
-      }
-      w.V(V_LOR)[i] = 1.0;
-      w.V(V_UPR)[i] = 1.0;
-      if (D.has_limits) {
-        int coord = D.dof_coord_index[dof];
-        if (coord >= D.joint_coord_count) coord = -1;
-        const double ke = coord >= 0 ? D.joint_limit_ke[dof] : 0.0;
-        if (coord >= 0 && D.limit_supported[dof] != 0 && ke > 0.0) {
-          const double q0 = D.joint_q[coord];
-          const double lower = D.joint_limit_lower[dof], upper = D.joint_limit_upper[dof];
-          const double speed = fmax(fabs(P.p.v0[base + i]), fabs(w.V(V_VSTAR)[i]));
-          const double window = kLimitWindow * dt * speed;
-          const double kd = D.joint_limit_kd[dof];
-          const double tau_d = kd > 0.0 ? kd / ke : 0.0;
-          const double bf = kLimitBeta * kLimitBeta / (4.0 * kPi * kPi);
-          const double r_nr = bf * fmax(w.V(V_AINV)[i], 1.0e-12);
-          const double r_soft = 1.0 / (dt * ke * (dt + tau_d));
-          const double rr = fmax(r_nr, r_soft);
-          if (isfinite(lower) && q0 - lower <= window) {
-            fl |= kFlagLo;
-            w.V(V_LOVHAT)[i] = -(q0 - lower) / (dt + tau_d);
-            w.V(V_LOR)[i] = rr;
-            w.V(V_LORINV)[i] = 1.0 / rr;
-          }
-          if (isfinite(upper) && upper - q0 <= window) {
-            fl |= kFlagUp;
-            w.V(V_UPVHAT)[i] = -(upper - q0) / (dt + tau_d);
-            w.V(V_UPR)[i] = rr;
-            w.V(V_UPRINV)[i] = 1.0 / rr;
-          }
-        }
-      }
-      w.flags[i] = fl;
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's J copies
-    __syncthreads();
-    // ---- participating DOFs (sim/contact_solve.py:423-488) ------------------
-    // A DOF takes part if a model term acts on it or a contact's body DOF
-    // range or J column covers it.  The contacts mark their DOFs in a 64-bit
-    // mask in parallel (n <= 60 here).
-    if (tid == 0) s_partmask = 0ull;
-    __syncthreads();
-    for (int c = tid; c < count; c += NT) {
-      const size_t ci = (size_t)e * C + c;
-      unsigned long long mk = 0ull;
-      if (P.p.body_dof_start) {
-        const int bs[2] = {P.p.body0 ? P.p.body0[ci] : -1, P.p.body1 ? P.p.body1[ci] : -1};
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int b = bs[q];
-          if (b < 0 || b >= P.p.num_bodies) continue;
-          const int s = P.p.body_dof_start[b], m = P.p.body_dof_count[b];
-          if (s < 0 || m <= 0 || s >= n) continue;
-          const int hi = s + m < n ? s + m : n;
-          mk |= ((1ull << (hi - s)) - 1ull) << s;
-        }
-      }
-      const double* Jc = w.J + (size_t)(3 * c) * L.ldJ;
-      if (mk != (1ull << n) - 1ull)
-        for (int j = 0; j < n; ++j)
-          if (Jc[j] != 0.0 || Jc[L.ldJ + j] != 0.0 || Jc[2 * L.ldJ + j] != 0.0) mk |= 1ull << j;
-      atomicOr(&s_partmask, mk);
-    }
-    __syncthreads();
-    int any_model_term = 0;
-    for (int i = tid; i < n; i += NT) {
-      const int model = (w.flags[i] & (kFlagPd | kFlagLo | kFlagUp)) ? 1 : 0;
-      any_model_term |= model;
-      if (model || ((s_partmask >> i) & 1ull)) w.flags[i] |= kFlagPart;
-    }
-    const int model_terms = __syncthreads_or(any_model_term);
-    const bool unconstrained = (count == 0) && !model_terms;
-
-    int newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
-    double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
-    int ws_accepted = 0;
-    bool evaluated = false;
-    if (unconstrained) {
-      converged = 1;
-      for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
-      __syncthreads();
-    } else {
-      for (int i = tid; i < n; i += NT)
-        if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
-      __syncthreads();
-      // Candidate starts (no counterpart in the reference): for each of the
-      // gamma0_count impulse sets, v_c = v* + A^-1 J^T gamma_c on the
-      // participating DOFs with A factored once in this kernel's factor
-      // precision; the start with the lowest cost among the plain start and
-      // the candidates is taken.  Its evaluation seeds iteration 0 when it
-      // was the last one evaluated.
-      bool have_e4 = false;
-      double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
-      if (P.p.gamma0 && count > 0) {
-        const int K = P.p.gamma0_count > 1 ? P.p.gamma0_count : 1;
-        double e4p[4];
-        evaluate<NT, HT, NS>(w, P, dt, e4p);
-        double best_cost = e4p[0];
-        const int ldj = w.ldJ();
-        for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
-        if (P.p.dynamics_factor) {
-          // the free motion's LDL^T of A
-          const double* Lg = P.p.dynamics_factor + (size_t)e * n * n;
-          load_lower<NT, HT, NS>(w, Lg, nullptr, 0.0);
-          HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
-          for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
-          __syncthreads();
-        } else {
-          load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
-          for (int i = tid; i < n; i += NT) w.V(V_GRAD)[i] = 0.0;
-          __syncthreads();
-          factor_and_solve<NT, HT, NS>(w);  // the factor of A (the solve of a zero rhs is unused)
-        }
-        bool last_is_best = false;
-        // Two sets at a time: stage their impulses in the (here unused)
-        // scratch, form J^T gamma for both (threads 0-63 set k0, 64-127 set
-        // k0+1), solve both with the factor on warps 0 and 1, then evaluate
-        // the candidates in order.
-        double* gs = reinterpret_cast<double*>(w.GJ);
-        for (int k0 = 0; k0 < K; k0 += 2) {
-          const int nk = K - k0 < 2 ? K - k0 : 2;
-          for (int q = tid; q < nk * 3 * count; q += NT) {
-            const int kk = q / (3 * count), r = q - kk * 3 * count;
-            gs[q] = __ldg(P.p.gamma0 + ((size_t)(k0 + kk) * P.p.num_envs + e) * C * 3 + r);
-          }
-          __syncthreads();
-          {
-            const int kk = tid >> 6, i = tid & 63;
-            if (kk < nk && i < n) {
-              const double* g = gs + kk * 3 * count;
-              double acc = 0.0;
-              for (int c = 0; c < count; ++c) {
-                const double* Jc = w.J + (size_t)(3 * c) * ldj;
-                acc += Jc[i] * g[3 * c] + Jc[ldj + i] * g[3 * c + 1] + Jc[2 * ldj + i] * g[3 * c + 2];
-              }
-              w.V(kk == 0 ? V_GRAD : V_DP)[i] = -acc;  // the solves give -H^-1 rhs
-            }
-          }
-          __syncthreads();
-          solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
-          if (nk > 1) solve_warp<NT, HT, NS>(w, V_DP, V_DV2, 1);
-          __syncthreads();
-          for (int kk = 0; kk < nk; ++kk) {
-            const int k = k0 + kk;
-            const double* dvk = w.V(kk == 0 ? V_DV : V_DV2);
-            for (int i = tid; i < n; i += NT)
-              w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? w.V(V_VSTAR)[i] + dvk[i] : w.V(V_VSTAR)[i];
-            __syncthreads();
-            double e4c[4];
-            evaluate<NT, HT, NS>(w, P, dt, e4c);
-            last_is_best = false;
-            if (e4c[0] < best_cost) {
-              best_cost = e4c[0];
-              ws_accepted = k + 1;
-              last_is_best = true;
-              for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
-              for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
-            }
-          }
-        }
-        if (last_is_best) {
-          have_e4 = true;
-        } else {
-          const int src = ws_accepted > 0 ? V_BEST : V_SAVE;
-          for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(src)[i];
-        }
-        __syncthreads();
-      }
-      const double cost_min_alpha = LSV == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
-      int it = 0;
-      bool active = true;
-      for (;;) {
-        double e4[4];
-        if (have_e4) {
-          for (int k = 0; k < 4; ++k) e4[k] = e4_seed[k];
-          have_e4 = false;
-        } else {
-          evaluate<NT, HT, NS>(w, P, dt, e4);
-        }
-        evaluated = true;
-        cost = e4[0];
-        // convergence test (sim/contact_solve.py:2043-2087)
-        const double gn = sqrt(fmax(e4[1], 0.0)), pn = sqrt(fmax(e4[2], 0.0)), jn = sqrt(fmax(e4[3], 0.0));
-        grad_norm = gn;
-        const double opt_tol = P.o.optimality_abs_tol + P.o.optimality_rel_tol * fmax(pn, jn);
-        const bool opt = gn <= opt_tol;
-        bool cost_ok = false;
-        if (it > 0 && alpha > cost_min_alpha) {
-          const double sc = 0.5 * (fabs(cost) + fabs(previous_cost));
-          const double tol = P.o.cost_abs_tol + P.o.cost_rel_tol * sc;
-          if (fabs(cost - previous_cost) < tol) cost_ok = true;
-        }
-        newton_iterations = it;
-        if (opt || cost_ok) {
-          converged = 1;
-          active = false;
-        } else if (it >= P.o.max_iterations) {
-          active = false;
-        } else {
-          converged = 0;
-        }
-        if (!active) break;
-        // Newton direction
-        assemble_hessian<NT, HT, NS>(w, P.o.diag_shift);
-        factor_and_solve<NT, HT, NS>(w);
-        LsResult r;
-        double c4[4];
-        line_coefficients<NT, HT, NS>(w, c4);
-        if constexpr (LSV == SAPB_LS_ARMIJO_DECAY)
-          r = ls_armijo<NT, 3>(w, P, dt, cost, c4);
-        else if constexpr (LSV == SAPB_LS_EXACT_ROOT)
-          r = ls_exact<NT>(w, P, dt, cost, c4);
-        else
-          r = ls_monotone<NT, 3>(w, P, dt, cost, c4);
-        alpha = r.alpha;
-        status = r.status;
-        constexpr bool mono = LSV == SAPB_LS_MONOTONE_DECAY;
-        if (r.accepted || mono) ls_total += r.iterations;
-        if (r.accepted) {
-          previous_cost = cost;
-          for (int i = tid; i < n; i += NT) w.V(V_V)[i] += r.alpha * w.V(V_DV)[i];
-        } else if (mono) {
-          previous_cost = cost;
-        }
-        __syncthreads();
-        ++it;
-      }
-    }
-    // ---- outputs ------------------------------------------------------------
-    for (int i = tid; i < n; i += NT) P.out.v[base + i] = w.V(V_V)[i];
-    for (int c = tid; c < C; c += NT) {
-      const size_t ci = (size_t)e * C + c;
-      const bool live = evaluated && c < count;
-      if (P.out.contact_gamma) {
-        P.out.contact_gamma[ci * 3 + 0] = live ? w.Cn(C_GAMMA + 0)[c] : 0.0;
-        P.out.contact_gamma[ci * 3 + 1] = live ? w.Cn(C_GAMMA + 1)[c] : 0.0;
-        P.out.contact_gamma[ci * 3 + 2] = live ? w.Cn(C_GAMMA + 2)[c] : 0.0;
-      }
-      if (P.out.contact_mode) {
-        int mode = SAPB_CONTACT_MODE_NONE;
-        if (live) {
-          double g[3], cst;
-          mode = project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cst, nullptr);
-        }
-        P.out.contact_mode[ci] = mode;
-      }
-    }
-    if (tid == 0) {
-      if (P.out.cost) P.out.cost[e] = evaluated ? cost : 0.0;
-      if (P.out.newton_iterations) P.out.newton_iterations[e] = newton_iterations;
-      if (P.out.line_search_iterations) P.out.line_search_iterations[e] = ls_total;
-      if (P.out.converged) P.out.converged[e] = converged;
-      if (P.out.status) P.out.status[e] = status;
-      if (P.out.grad_norm) P.out.grad_norm[e] = grad_norm;
-      if (P.out.warm_start_accepted) P.out.warm_start_accepted[e] = ws_accepted;
-    }
-    __syncthreads();
-  }
-}
-
-template <int NT, typename HT, int MINB, int NS, int LSV>
-static cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
-  const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT));
-  auto kern = contact_solve_kernel<NT, HT, MINB, NS, LSV>;
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
-  if (err != cudaSuccess) return err;
-  int dev = 0;
-  err = cudaGetDevice(&dev);
-  if (err != cudaSuccess) return err;
-  int sms = 0;
-  err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (err != cudaSuccess) return err;
-  int per_sm = 0;
-  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, L.total);
-  if (err != cudaSuccess) return err;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  if (blocks_out && P.p.num_envs == 0) {  // occupancy query only
-    *blocks_out = per_sm;
-    return cudaSuccess;
-  }
-  const int k = (P.o.ctas_per_sm > 0 && P.o.ctas_per_sm < per_sm) ? P.o.ctas_per_sm : per_sm;
-  int blocks = sms * k;
-  if (blocks > P.p.num_envs) blocks = P.p.num_envs;
-  if (blocks < 1) blocks = 1;
-  if (blocks_out) *blocks_out = blocks;
-  err = cudaMemsetAsync(P.queue, 0, sizeof(int32_t), stream);
-  if (err != cudaSuccess) return err;
-  kern<<<blocks, NT, L.total, stream>>>(P);
-  return cudaGetLastError();
-}
-
-template <int NT, typename HT, int MINB, int NS>
-static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
-  switch (P.o.line_search_variant) {
-    case SAPB_LS_ARMIJO_DECAY:
-      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_ARMIJO_DECAY>(P, stream, blocks_out);
-    case SAPB_LS_EXACT_ROOT:
-      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_EXACT_ROOT>(P, stream, blocks_out);
-    default:
-      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_MONOTONE_DECAY>(P, stream, blocks_out);
-  }
-}
 
 size_t contact_solve_smem_bytes(int n, int C, int hessian_precision) {
   return make_layout(n, C, hessian_precision == SAPB_FP32 ? 4 : 8).total;
@@ -1000,18 +35,16 @@ static cudaError_t solve_dispatch(const SolveParams& P, bool fp32, cudaStream_t 
   // Kernels specialised on the DOF count of the common trees (humanoid 35,
   // quadruped 18, arm + box 13, single free body 6); a generic one otherwise.
   switch (P.p.dof_per_env) {
-#define SAPB_DISPATCH_N(NV)                                                              \
-  case NV:                                                                               \
-    return fp32 ? launch_solve<128, float, 4, NV>(P, stream, blocks_out)                 \
-                : launch_solve<128, double, 3, NV>(P, stream, blocks_out);
+#define SAPB_DISPATCH_N(NV) \
+  case NV:                  \
+    return launch_solve_ns<NV>(P, fp32, stream, blocks_out);
     SAPB_DISPATCH_N(35)
     SAPB_DISPATCH_N(18)
     SAPB_DISPATCH_N(13)
     SAPB_DISPATCH_N(6)
 #undef SAPB_DISPATCH_N
     default:
-      return fp32 ? launch_solve<128, float, 4, 0>(P, stream, blocks_out)
-                  : launch_solve<128, double, 3, 0>(P, stream, blocks_out);
+      return launch_solve_ns<0>(P, fp32, stream, blocks_out);
   }
 }
 
@@ -1046,3 +79,4 @@ int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_opt
 }
 
 }  // namespace sapb
+

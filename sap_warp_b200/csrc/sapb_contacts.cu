@@ -308,7 +308,13 @@ __global__ void scan_sums_kernel(int64_t* block_sums, int64_t nb, int32_t* total
     block_sums[b] = acc;
     acc += v;
   }
-  if (t == kScanBlock - 1) *total_out = (int32_t)(s[t] < capacity ? s[t] : capacity);
+  // The full number of contacts found, like the reference's writer, whose
+  // atomic count keeps growing past the buffer (sim/collision/pipeline.py:
+  // 87-90): consumers cap it at the buffer length themselves (the step's
+  // scatter does), and a count above the capacity tells the caller that the
+  // contacts past it were dropped.  Saturates at INT32_MAX.
+  (void)capacity;
+  if (t == kScanBlock - 1) *total_out = (int32_t)(s[t] < INT32_MAX ? s[t] : INT32_MAX);
 }
 
 __global__ void write_kernel(const GenParams P, const int64_t* offsets, const int64_t* block_offsets,

@@ -201,22 +201,19 @@ __device__ void ldlt_solve_blocked(const T* H, int n, int ldH, const T* dinv, X*
   }
 }
 
-// x = A^-1 b by the calling warp alone (all 32 lanes; no block barrier) with
-// the LDL^T that ldlt_blocked left in H and dinv: lanes own rows lane and
-// lane + 32 (n <= 64); forward z = D^-1 L^-1 b with the pivot broadcast by
-// shuffles, then backward x = L^-T z.  b is read before x is written (they
-// may alias).  A pivot that is not positive / finite makes x NaN.
+// x = A^-1 b (or -A^-1 b with neg) by the calling warp alone (all 32 lanes;
+// no block barrier) with the LDL^T that ldlt_blocked left in H and dinv:
+// lanes own rows lane and lane + 32 (n <= 64); forward z = D^-1 L^-1 b with
+// the pivot broadcast by shuffles, then backward x = L^-T z.  b is read before
+// x is written (they may alias).  `ok` false (a pivot not positive / finite,
+// ldlt_pivots_ok_warp) makes x NaN.
 template <typename T>
-__device__ void ldlt_solve_warp(const T* H, int n, int ldH, const T* dinv, const double* b, double* x) {
+__device__ void ldlt_solve_warp(const T* H, int n, int ldH, const T* dinv, const double* b, double* x,
+                                bool neg, bool ok) {
   const int lane = threadIdx.x & 31;
-  bool ok = true;
-  for (int k = lane; k < n; k += 32) {
-    const T d = H[(size_t)k * ldH + k];
-    if (!(d > T(0)) || !isfinite(double(d))) ok = false;
-  }
-  ok = __all_sync(0xffffffffu, ok);
-  T h0 = lane < n ? T(b[lane]) : T(0);
-  T h1 = lane + 32 < n ? T(b[lane + 32]) : T(0);
+  const T sg = neg ? T(-1) : T(1);
+  T h0 = lane < n ? sg * T(b[lane]) : T(0);
+  T h1 = lane + 32 < n ? sg * T(b[lane + 32]) : T(0);
   for (int k = 0; k < n; ++k) {
     const T zk = __shfl_sync(0xffffffffu, k < 32 ? h0 : h1, k & 31) * dinv[k];
     if (lane == (k & 31)) {
@@ -242,6 +239,19 @@ __device__ void ldlt_solve_warp(const T* H, int n, int ldH, const T* dinv, const
   __syncwarp();
   if (lane < n) x[lane] = ok ? double(h0) : nanv;
   if (lane + 32 < n) x[lane + 32] = ok ? double(h1) : nanv;
+}
+
+// Whether every pivot of a stored LDL^T is positive and finite (the warp's
+// lanes check two each), returned to every lane.
+template <typename T>
+__device__ bool ldlt_pivots_ok_warp(const T* H, int n, int ldH) {
+  const int lane = threadIdx.x & 31;
+  bool ok = true;
+  for (int k = lane; k < n; k += 32) {
+    const T d = H[(size_t)k * ldH + k];
+    if (!(d > T(0)) || !isfinite(double(d))) ok = false;
+  }
+  return __all_sync(0xffffffffu, ok);
 }
 
 }  // namespace sapb

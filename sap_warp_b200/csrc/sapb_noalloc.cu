@@ -7,6 +7,7 @@
 // runtime that owns every device allocation, or a foreign-language binding
 // with no device allocator of its own) has no way to provide one.  This entry
 // point uses a fixed array compiled into the library instead.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -24,6 +25,40 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void* g_scratch_device_ptr[kMaxDevices] = {};
+// Identity of the context each cached address belongs to: a device reset
+// (cudaDeviceReset) ends that context, and the next call on the device then
+// looks the address up again in the new one.
+unsigned long long g_scratch_ctx_id[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context (0 if none or the
+// driver cannot say), through the runtime's driver entry points: no link
+// against the driver library.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    looked_up = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+  unsigned long long id = 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 }  // namespace
 
@@ -53,8 +88,11 @@ extern "C" int32_t sapb_contact_solve_noalloc(const sapb_contact_problem* p, con
   {
     // Set-up once per device, with that device current: the array's name is
     // a host-side stand-in, so its device address must come from the runtime.
+    // The address is cached with the id of its context and looked up again
+    // when the device's context has changed since (after a device reset).
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_device_ptr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_device_ptr[dev] || ctx == 0 || ctx != g_scratch_ctx_id[dev]) {
       void* ptr = nullptr;
       err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
       if (err != cudaSuccess || ptr == nullptr) {
@@ -62,6 +100,7 @@ extern "C" int32_t sapb_contact_solve_noalloc(const sapb_contact_problem* p, con
         return SAPB_ERR_CUDA;
       }
       g_scratch_device_ptr[dev] = ptr;
+      g_scratch_ctx_id[dev] = current_context_id();  // the lookup made the context current if it was not
     }
     scratch = g_scratch_device_ptr[dev];
   }

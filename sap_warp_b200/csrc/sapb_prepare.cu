@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   auto POSE_P = [&](int b) { return v3(pose[8 * b], pose[8 * b + 1], pose[8 * b + 2]); };
   auto POSE_Q = [&](int b) { return qnormalize(Q4{pose[8 * b + 3], pose[8 * b + 4], pose[8 * b + 5], pose[8 * b + 6]}); };
   if (split && tid < 32) {
-    ldlt_solve_warp<double>(H, n, n, dinv, tau, vdot);
+    ldlt_solve_warp<double>(H, n, n, dinv, tau, vdot, false, ldlt_pivots_ok_warp<double>(H, n, n));
   } else {
   const int wt = split ? tid - 32 : tid;                // worker thread index
   const int wn = split ? kPrepNT - 32 : kPrepNT;        // worker threads

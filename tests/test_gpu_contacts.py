@@ -9,8 +9,8 @@ import torch
 from oracle import boundary as ob
 from oracle import contacts as oc
 from sap_warp_b200 import _abi, models
-from sap_warp_b200.collision import ContactGenerator, ShapeSet
-from sap_warp_b200.runtime import SapState
+from sap_warp_b200.collision import ContactGenerator, ContactOverflowError, ShapeSet
+from sap_warp_b200.runtime import SapContacts, SapState
 from sap_warp_b200.solver import SolverSAP, _ModelView
 
 pytestmark = pytest.mark.gpu
@@ -103,8 +103,10 @@ def test_box_worlds_step_with_generated_contacts(cuda_device):
 
 
 def test_capacity_clamps_and_keeps_the_prefix(cuda_device):
-    """More contacts than slots: the count is the capacity, the slots hold
-    the oracle's first contacts in order, and nothing past them is written."""
+    """More contacts than slots: the count is the number found (as the
+    reference's writer counts), the slots hold the oracle's first contacts in
+    order, nothing past them is written, and the generator reports the
+    overflow."""
     model, state, control, con, _, host = models.box_scene(2, 76, cuda_device, boxes=8, sites=(2, 3))
     shapes = models.box_shapes(host)
     bq, _ = ob.eval_fk(host["g"], host["q"].reshape(-1), np.zeros(model.joint_dof_count))
@@ -116,10 +118,21 @@ def test_capacity_clamps_and_keeps_the_prefix(cuda_device):
     gen.shape0.fill_(-7)
     gen.generate(state.joint_q)
     torch.cuda.synchronize()
-    assert int(gen.count.item()) == cap
+    assert int(gen.count.item()) == total
+    assert gen.overflowed()
     np.testing.assert_array_equal(gen.shape0[:cap].cpu().numpy(), ref["shape0"][:cap])
     np.testing.assert_allclose(gen.point1[:cap].cpu().numpy(), ref["point1"][:cap], rtol=1e-12, atol=1e-12)
     assert bool((gen.shape0[cap:] == -7).all())
+    with pytest.raises(ContactOverflowError):
+        gen.generate(state.joint_q, check_capacity=True)
+    # the step reads only the slots the buffer holds
+    from sap_warp_b200.solver import SapContactJacobian
+    cj = SapContactJacobian(model, max_rigid_contact=64, fallback_tau_d=0.0)
+    contacts = gen.generate(state.joint_q)
+    cj.compute(state, SapContacts(**{k: (v[:cap] if (v is not None and v.dim() > 0 and v.shape[0] == cap + 5)
+                                         else v) for k, v in vars(contacts).items()}), control=control, dt=2.0e-3)
+    torch.cuda.synchronize()
+    assert int(cj.contact_env_count.sum()) <= cap
 
 
 def test_no_candidate_pairs(cuda_device):
