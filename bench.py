@@ -11,6 +11,11 @@ motion, contact Jacobian, the stage-2 Newton solve with armijo_decay to the
 reference's tolerances (optimality 1e-14 abs / 1e-6 rel), position
 integration -- and the timed steps continue one rollout.
 
+The timed window starts after a fixed settling prefix of SETTLE_STEPS steps
+(plain FP64 solver, untimed), so a short run measures the steady rollout
+rather than its easy first steps; every arm starts from the same settled
+state.
+
 Arms (same scene, same trajectory up to the solve tolerance):
   value        learned + FP32: FP32 Hessian / factorization with FP64
                gradient, cost, line search and convergence test, and the
@@ -54,6 +59,7 @@ WORLDS = 4096
 SEED = 2
 DT = 2.0e-3
 MAX_CONTACTS = 32
+SETTLE_STEPS = 100
 
 
 def parse():
@@ -214,6 +220,57 @@ def cpu_steps(scene: dict, steps: int, threads: int, min_seconds: float = 0.0):
     return (time.perf_counter() - t0) / done, done
 
 
+def oracle_errors(dev) -> dict:
+    """Error of the GPU solve against the FP64 oracle per configuration, on
+    samples the oracle finishes in seconds: the stage-2 solve (armijo_decay,
+    the reference's tolerances) of the same seeded problem on the GPU in FP64
+    and with the FP32 Hessian / factorization, and in the oracle (FP64).
+    Per world: max |v - v_oracle| / max |v_oracle|; reported as the max and
+    the 99th percentile over the sample.  Part of the CPU-baseline leg (the
+    oracle runs on the host)."""
+    import torch
+
+    from oracle import oracle
+    from sap_warp_b200 import scenes
+    from sap_warp_b200._solve import (ContactSolveBuffers, blocked_contact_solve, blocked_problem_to_device,
+                                      contact_solve, make_options, problem_to_device)
+
+    def rel(vg, vo, n):
+        vg, vo = vg.reshape(-1, n), vo.reshape(-1, n)
+        e = np.abs(vg - vo).max(1) / np.maximum(np.abs(vo).max(1), 1e-300)
+        return {"max": float(e.max()), "p99": float(np.quantile(e, 0.99)), "worlds": int(e.size)}
+
+    out = {}
+    cases = (("humanoid_35dof", scenes.humanoid_contact_problem(256, seed=SEED + 17), None),
+             ("quadruped_18dof", scenes.quadruped_contact_problem(256, seed=SEED + 18), None))
+    mix, _ = scenes.mixed_contact_problem(384, seed=SEED + 19)
+    cases = cases + (("uneven_13_18_35dof", mix, scenes.work_order(mix)),)
+    for name, prob, order in cases:
+        ref = oracle.solve(prob, "armijo_decay")
+        t = problem_to_device(prob, dev)
+        wo = None if order is None else torch.as_tensor(order, dtype=torch.int32, device=dev)
+        row = {}
+        for prec in ("fp64", "fp32"):
+            buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, dev)
+            contact_solve(**t, buffers=buf, options=make_options("armijo_decay", hessian_precision=prec,
+                                                                 linear_solve_precision=prec), world_order=wo)
+            torch.cuda.synchronize()
+            row[prec] = rel(buf.v.cpu().numpy(), ref["v"], prob.dof_per_env)
+        out[name] = row
+    boxes = scenes.box_stack_problem(2, seed=SEED + 20)
+    ref = oracle.solve(boxes.to_dense(), "armijo_decay")
+    tb = blocked_problem_to_device(boxes, dev)
+    row = {}
+    for prec in ("fp64", "fp32"):
+        buf = ContactSolveBuffers(boxes.num_envs, boxes.dof_per_env, boxes.max_contacts, dev)
+        blocked_contact_solve(buffers=buf, options=make_options("armijo_decay", hessian_precision=prec,
+                                                                linear_solve_precision=prec), trees_per_env=64, **tb)
+        torch.cuda.synchronize()
+        row[prec] = rel(buf.v.cpu().numpy(), ref["v"], boxes.dof_per_env)
+    out["boxes_384dof"] = row
+    return out
+
+
 def run_reference(args, rank: int, world_size: int):
     """Reference arm: the reference's own implementation is Python + NVIDIA
     Warp, which cannot be installed here, so the CPU restatement of its step
@@ -271,9 +328,21 @@ def main():
     barrier, max_over_ranks = group.barrier, group.max_over_ranks
     shard = shard_of(rank, world_size, args.worlds, SEED)
 
-    model, state0, control, contacts, _ = models.rollout_scene("humanoid", shard.worlds, shard.seed, dev)
+    model, state_init, control, contacts, _ = models.rollout_scene("humanoid", shard.worlds, shard.seed, dev)
     W = args.worlds
     ws = LearnedWarmStart.load(args.weights or DEFAULT_WEIGHTS, dev)
+    # settle: SETTLE_STEPS untimed steps of the plain FP64 solver; every arm
+    # starts its warm-up and timed window from the settled state
+    settler = SolverSAP(model, max_rigid_contact=MAX_CONTACTS, contact_preset_variant="drake", hessian_precision="fp64")
+    s_a = SapState(joint_q=state_init.joint_q.clone(), joint_qd=state_init.joint_qd.clone(),
+                   body_q=state_init.body_q.clone(), body_f=state_init.body_f.clone())
+    s_b = SapState(joint_q=state_init.joint_q.clone(), joint_qd=state_init.joint_qd.clone(),
+                   body_q=state_init.body_q.clone(), body_f=state_init.body_f.clone())
+    for _ in range(SETTLE_STEPS):
+        settler.step(s_a, s_b, control, contacts, DT)
+        s_a, s_b = s_b, s_a
+    state0 = s_a
+    del settler, s_b
 
     def fresh_states():
         a = SapState(joint_q=state0.joint_q.clone(), joint_qd=state0.joint_qd.clone(), body_q=state0.body_q.clone(),
@@ -302,13 +371,21 @@ def main():
             s_in, s_out = s_out, s_in
         barrier()
         solver.stage_events = []
-        iters, chosen = [], []
+        iters, chosen, flops = [], [], []
+        nd = 35.0
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(2 * pairs):
             solver.step(s_in, s_out, control, contacts, DT)
-            iters.append(solver.contact_solve.newton_iterations_env.sum())
-            chosen.append(torch.bincount(solver.contact_solve.warm_start_accepted_env.long(), minlength=3))
+            cs = solver.contact_solve
+            k = cs.newton_iterations_env.double()
+            iters.append(k.sum())
+            chosen.append(torch.bincount(cs.warm_start_accepted_env.long(), minlength=3))
+            # algorithmic FP64-equivalent arithmetic of this step's solve (see roofline.fp64)
+            Cw = solver.contact_jacobian.contact_env_count.clamp(0, MAX_CONTACTS).double()
+            t = cs.ls_iterations_total.double()
+            flops.append((k * (6 * Cw * nd * nd + nd ** 3 / 3 + 2 * nd * nd + 6 * Cw * nd)
+                          + (k + 1) * (4 * nd * nd + 12 * Cw * nd) + 80 * Cw * t).sum())
             s_in, s_out = s_out, s_in
         e1.record(stream)
         barrier()
@@ -316,6 +393,7 @@ def main():
         stages = {k: v / (2 * pairs) for k, v in solver.stage_times().items()}
         solver.stage_events = None
         it = float(torch.stack(iters).double().sum().item()) / (2 * pairs * W)
+        solve_flops = float(torch.stack(flops).sum().item()) / (2 * pairs)
         ch = torch.stack(chosen).sum(0).cpu().numpy()
         conv = bool(solver.contact_solve.converged_env.all())
         counts = solver.contact_jacobian.contact_env_count.clamp(max=MAX_CONTACTS).cpu().numpy()
@@ -339,7 +417,7 @@ def main():
         del graph
         same = bool(torch.equal(g_in.joint_qd, final_eager))
         return dict(ms=ms, ms_eager=ms_eager, stages=stages, iters=it, chosen=ch, converged=conv, counts=counts,
-                    solver=solver, final=g_in, graph_matches_eager=same)
+                    solver=solver, final=g_in, graph_matches_eager=same, solve_flops_fp64=solve_flops)
 
     plain = run_arm("fp64", "previous_velocity")
     prev = run_arm("fp32", "previous_impulses")
@@ -457,6 +535,7 @@ def main():
 
     # ---- the launch-shape autotuner's view: each resident-CTA count per SM
     # timed on the snapshot and on the uneven batch (SolveAutotuner's rule) ----
+    from sap_warp_b200 import _abi as _abi_mod
     from sap_warp_b200._lib import load as _load_lib
     from sap_warp_b200.autotune import SolveAutotuner
 
@@ -563,6 +642,13 @@ def main():
 
     total = W * world_size
     value = total / (fast["ms"] * 1e-3)
+    # measured FMA rates of this GPU (the FP64 pipe's roofline denominator)
+    fma = {}
+    for label, prec in (("fp64", _abi_mod.SAPB_FP64), ("fp32", _abi_mod.SAPB_FP32)):
+        rate = __import__("ctypes").c_double(0.0)
+        st = _load_lib().sapb_measure_fma_rate(prec, 1 << 14, __import__("ctypes").byref(rate),
+                                               __import__("ctypes").c_void_p(stream.cuda_stream))
+        fma[label] = rate.value if st == 0 else float("nan")
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -573,16 +659,34 @@ def main():
     solve_ms = fast["stages"].get("contact_solve", float("nan"))
     alg = float(solve_bytes_per_world(n, fast["counts"], 2).sum())
     achieved = alg / (solve_ms * 1e-3) / 1e9
+    # FP64 arithmetic of the plain arm's solve (algorithmic count from its
+    # measured Newton iterations and line-search trials) against the measured
+    # FP64 FMA rate
+    pf = plain["solve_flops_fp64"]
+    plain_solve_ms = plain["stages"].get("contact_solve", float("nan"))
+    fp64_achieved = pf / (plain_solve_ms * 1e-3) / 1e12
+    fp64_peak = fma["fp64"] / 1e12
     launches_per_step = 8  # scatter, free motion, solve, integrate, features, mlp, impulses, + the solve's memset
     line = {
         "metric": METRIC, "value": value, "unit": "world-steps/s", "n_gpus": world_size, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": fast["ms"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (FP32 Hessian/factor)", "data": "synthetic (seeded rollout scene)",
+        "vs_baseline": plain["ms"] / fast["ms"],
+        "vs_baseline_basis": "the metric's own baseline: the plain FP64 arm (the reference's method: FP64 "
+                             "throughout, previous-velocity warm start) on the same B200, same scene, window and "
+                             "tolerance -- its ms_per_step over this arm's (no published number exists)",
+        "plain_fp64_value": total / (plain["ms"] * 1e-3), "plain_fp64_ms_per_step": plain["ms"],
+        "speedup_vs_plain_fp64": plain["ms"] / fast["ms"],
+        "solve_stage_speedup_vs_plain_fp64": plain["stages"].get("contact_solve", float("nan")) / max(
+            fast["stages"].get("contact_solve", float("nan")) + fast["stages"].get("warm_start", 0.0), 1e-9),
+        "newton_iterations_per_world_step": {"learned_fp32": fast["iters"], "plain_fp64": plain["iters"],
+                                             "previous_impulses_fp32": prev["iters"]},
+        "dtype": "f64 (FP32 Hessian/factor)", "data": "synthetic (seeded rollout scene)",
         "config": {"workload": f"{W} humanoid worlds x 35 DOF (6+29 revolute), 8-32 ground contacts, full "
                                "SolverSAP step (drake preset), armijo_decay to reference tolerances, rollout",
                    "worlds_per_gpu": W, "dof_per_env": n, "max_contacts": MAX_CONTACTS, "dt": DT,
                    "parallelism": f"world shards x{world_size}",
-                   "l2": "per-step working set (A, J, factor, rows) larger than L2"},
+                   "l2": "per-step working set (A, J, factor, rows) larger than L2",
+                   "window": f"steps {SETTLE_STEPS}+ of the rollout (after an untimed settling prefix)"},
         "timing": "CUDA graph of two whole steps replayed steps/2 times after the warm-up; stages and "
                   "statistics from an eager pass over the same steps of the same trajectory",
         "plain_fp64": {"value": total / (plain["ms"] * 1e-3), "ms_per_step": plain["ms"],
@@ -614,7 +718,13 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "contact_solve_kernel", "achieved": achieved, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": NCU_SOLVE_TRAFFIC_BYTES,
                      "note": "achieved = algorithmic bytes of the solve launch / its mean duration inside the "
-                             "timed steps (of measured peak); the kernel is latency bound, not HBM bound"},
+                             "timed steps (of measured peak); the kernel is latency bound, not HBM bound",
+                     "fp64": {"kernel": "contact_solve_kernel (plain FP64 arm)", "achieved": fp64_achieved,
+                              "peak": fp64_peak, "unit": "TFLOP/s", "frac": fp64_achieved / fp64_peak,
+                              "peak_source": "sapb_measure_fma_rate on this GPU (FP64 FMA chains), this run",
+                              "flops": "algorithmic: per world k (6 C n^2 + n^3/3 + 2 n^2 + 6 C n) + "
+                                       "(k + 1)(4 n^2 + 12 C n) + 80 C t, k Newton iterations, t trials"}},
+        "fma_rate_tflops": {k: v / 1e12 for k, v in fma.items()},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
     }
@@ -625,6 +735,7 @@ def main():
         line["cpu_baseline"] = {"value": 1024 / sec, "unit": "world-steps/s", "cores": cores, "kind": "port",
                                 "sample": f"{k} steps of a 1024-world rollout (C restatement: free motion, rows, "
                                           f"solve, integration; OpenMP over worlds)"}
+        line["error_vs_fp64_oracle"] = oracle_errors(dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

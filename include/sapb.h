@@ -407,6 +407,14 @@ int32_t sapb_contact_solve_occupancy(int32_t dof_per_env, int32_t max_contacts, 
  * Replaces the Python defaults of solve(), sim/contact_solve.py:6129-6182. */
 void sapb_solve_options_default(sapb_solve_options* opts, int32_t line_search_variant);
 
+/* Measured fused multiply-add rate of the current GPU in the given precision
+ * (SAPB_FP64 / SAPB_FP32), in FLOP/s: eight independent FMA chains per
+ * thread, 2048 threads per SM, `iters` steps each, timed with CUDA events on
+ * `stream` after a warm-up launch (synchronises the stream).  The FP64 figure
+ * is the denominator of the contact solve's FP64-pipe fraction.  No
+ * counterpart in the reference (a measurement of this build's roofline). */
+int32_t sapb_measure_fma_rate(int32_t precision, int32_t iters, double* flops_per_s, void* stream);
+
 /* ABI version of the loaded library (SAPB_ABI_VERSION). */
 int32_t sapb_abi_version(void);
 

@@ -320,6 +320,7 @@ class AdamOptions(C.Structure):
 EXPORTS = {
     "sapb_solve_options_default": (None, [C.POINTER(SolveOptions), C.c_int32]),
     "sapb_abi_version": (C.c_int32, []),
+    "sapb_measure_fma_rate": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(C.c_double), _p]),
     "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_occupancy": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve": (
