@@ -47,6 +47,14 @@ extern "C" {
 /* Per-world status of sapb_blocked_contact_solve: the world's block factor
  * needs more off-diagonal blocks than sapb_blocked_fill_capacity; v = v*. */
 #define SAPB_WORLD_FACTOR_CAPACITY (-10)
+/* Per-world statuses of sapb_contact_solve (no counterpart in the reference,
+ * whose solve carries NaNs to the iteration cap): a NaN / Inf in the world's
+ * inputs (A, J, phi0, w_eff, mu, stiffness, tau_d, v*, start velocity) --
+ * the world is not solved, v = its start velocity, no iterations; a Newton
+ * factorization met a pivot that is not positive and finite (H not SPD) --
+ * the solve stops there, v = the last accepted iterate. */
+#define SAPB_WORLD_NOT_FINITE (-11)
+#define SAPB_WORLD_NOT_SPD (-12)
 
 /* contact modes (sim/contact_solve.py:60-63) */
 #define SAPB_CONTACT_MODE_NONE 0
@@ -582,6 +590,14 @@ int32_t sapb_mlp_adam(float* params, const float* grad, float* m, float* v, cons
 /* Reads and clears the MLP kernels' timeout flag (synchronises `stream`):
  * SAPB_OK or SAPB_ERR_TIMEOUT. */
 int32_t sapb_mlp_error(void* stream);
+/* Failure-detection hooks of the MLP kernels (no counterpart in the
+ * reference): every mbarrier wait of the forward / backward kernels gives up
+ * after wait_polls polls (0: the default bound of 2^22 polls), after which
+ * the kernel sets the timeout flag, waits (bounded) for any commit still in
+ * flight, frees its tensor memory and exits; with drop_first_commit each
+ * forward CTA issues no MMA commit for its first layer, so that wait cannot
+ * complete (a deterministic timeout for tests).  Applies to later launches. */
+int32_t sapb_mlp_test_hooks(int32_t wait_polls, int32_t drop_first_commit);
 /* Per-slot network inputs of a stage-2 problem: normalised BF16 rows
  * features [E*C,16] and/or raw FP32 rows raw [E*C,12]; dead slots are zero.
  * normal_up [E,C] (NULL: 1), gamma_prev [E,C,3] (NULL: 0), vc_star [E,C,3]

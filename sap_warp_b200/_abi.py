@@ -23,6 +23,8 @@ SAPB_LS_BAD_BRACKET = -3
 SAPB_LS_BAD_GUESS = -4
 SAPB_LS_ROOT_ITERATION_CAP = -5
 SAPB_WORLD_FACTOR_CAPACITY = -10
+SAPB_WORLD_NOT_FINITE = -11
+SAPB_WORLD_NOT_SPD = -12
 
 SAPB_CONTACT_MODE_NONE = 0
 SAPB_CONTACT_MODE_STICTION = 1
@@ -364,6 +366,7 @@ EXPORTS = {
     "sapb_mlp_backward": (C.c_int32, [_p, _p, C.c_int32, C.POINTER(MlpTrainBuffers), _p, _p]),
     "sapb_mlp_adam": (C.c_int32, [_p, _p, _p, _p, C.POINTER(AdamOptions), C.c_int32, _p, _p, _p]),
     "sapb_mlp_error": (C.c_int32, [_p]),
+    "sapb_mlp_test_hooks": (C.c_int32, [C.c_int32, C.c_int32]),
     "sapb_warmstart_features": (
         C.c_int32, [C.POINTER(ContactProblem), _p, _p, _p, C.POINTER(WarmstartNorm), C.c_double, _p, _p, _p]
     ),

@@ -99,6 +99,7 @@ struct World {
   int* flags;
   const uint16_t* tri;
   double* red;
+  int* factor_ok;  // shared: whether the last Newton factorization's pivots were all positive and finite
   int n, count;
   // DOF count and leading dimensions: compile-time constants when NS > 0.
   __device__ __forceinline__ int dofs() const { return NS > 0 ? NS : n; }
@@ -417,6 +418,7 @@ __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   ldlt_blocked<NT, HT>(w.H, w.dofs(), w.ldH(), dinv, w.tri);
   if ((threadIdx.x >> 5) == 0) {
     const bool ok = ldlt_pivots_ok_warp<HT>(w.H, w.dofs(), w.ldH());
+    if (threadIdx.x == 0) *w.factor_ok = ok ? 1 : 0;
     ldlt_solve_warp<HT>(w.H, w.dofs(), w.ldH(), dinv, w.V(V_GRAD), w.V(V_DV), true, ok);
   }
   __syncthreads();
@@ -473,6 +475,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   __shared__ double red[8 * (NT / 32)];
   __shared__ int s_next;
   __shared__ unsigned long long s_partmask;
+  __shared__ int s_factor_ok;
   const int tid = threadIdx.x;
   const int n = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
   const Layout L = make_layout(n, C, (int)sizeof(HT));
@@ -533,6 +536,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
                     reinterpret_cast<int*>(smem + L.off_flags),
                     reinterpret_cast<const uint16_t*>(smem + L.off_tri),
                     red,
+                    &s_factor_ok,
                     n,
                     0};
     int count = P.p.contact_count[e];
@@ -697,12 +701,35 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
     }
     const int model_terms = __syncthreads_or(any_model_term);
     const bool unconstrained = (count == 0) && !model_terms;
+    // ---- input check: a NaN / Inf in A, J, the contact parameters, v* or
+    // the start velocity leaves the world unsolved (SAPB_WORLD_NOT_FINITE)
+    int bad = 0;
+    for (int k = tid; k < n * n; k += NT)
+      if (!isfinite(__ldg(w.A + k))) bad = 1;
+    {
+      const int ldj = w.ldJ(), tot = 3 * count * n;
+      for (int k = tid; k < tot; k += NT) {
+        const int r = k / n, j = k - r * n;
+        if (!isfinite(w.J[(size_t)r * ldj + j])) bad = 1;
+      }
+    }
+    for (int c = tid; c < count; c += NT) {
+      const size_t ci = (size_t)e * C + c;
+      if (!isfinite(P.p.phi0[ci]) || !isfinite(P.p.w_eff[ci]) || !isfinite(P.p.mu[ci]) ||
+          !isfinite(P.p.stiffness[ci]) || (P.p.tau_d && !isfinite(P.p.tau_d[ci])))
+        bad = 1;
+    }
+    for (int i = tid; i < n; i += NT)
+      if (!isfinite(w.V(V_VSTAR)[i]) || !isfinite(w.V(V_V)[i])) bad = 1;
+    const bool not_finite = __syncthreads_or(bad) != 0;
 
     int newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
     double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
     int ws_accepted = 0;
     bool evaluated = false;
-    if (unconstrained) {
+    if (not_finite) {
+      status = SAPB_WORLD_NOT_FINITE;  // v stays the start velocity
+    } else if (unconstrained) {
       converged = 1;
       for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
@@ -829,6 +856,11 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         // Newton direction
         assemble_hessian<NT, HT, NS>(w, P.o.diag_shift);
         factor_and_solve<NT, HT, NS>(w);
+        if (!*w.factor_ok) {  // H not SPD (uniform: published by the barrier above)
+          status = SAPB_WORLD_NOT_SPD;
+          converged = 0;
+          break;
+        }
         LsResult r;
         double c4[4];
         line_coefficients<NT, HT, NS>(w, c4);

@@ -93,6 +93,8 @@ __device__ __forceinline__ void copy_bytes(void* dst, const void* src, int bytes
 
 // ---- forward ----------------------------------------------------------------
 struct FwdParams {
+  uint32_t polls;          // bound of each mbarrier wait (polls)
+  int drop_first_commit;   // test hook: each CTA's first MMA commit is not issued
   const uint16_t* wp;
   const float* bias;
   const uint16_t* x;  // [rows][16] BF16
@@ -153,10 +155,11 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
   constexpr uint32_t kIdesc = umma::idesc_bf16(128, 128, false, false);
 
   uint32_t phase = 0;
-  bool ok = true;
+  bool ok = true, outstanding = false;
   const int tiles = (P.rows + kRows - 1) / kRows;
   for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
     const int row0 = tile * kRows;
+    const bool first_tile = tile == (int)blockIdx.x;
     {
       const int rr = tid >> 1, ch = tid & 1;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
@@ -167,7 +170,10 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
     __syncthreads();
     float y0 = 0.f, y1 = 0.f, y2 = 0.f;
     for (int layer = 0; layer < 3; ++layer) {
-      if (tid == 0) {
+      // the test hook leaves this layer's barrier phase without a commit, so
+      // its bounded wait cannot complete (nothing is left in flight)
+      const bool drop = P.drop_first_commit && first_tile && layer == 0;
+      if (tid == 0 && !drop) {
         umma::fence_after_sync();
         // A = X or H (K-major, 128 rows), B = W (K-major, 128 output rows).
         if (layer == 0)
@@ -176,10 +182,13 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
           umma::mma_chain(tmem, aH, 2048, 128, 4096, aW[layer], 2048, 128, 4096, 8, kIdesc, 0);
         umma::commit(&bar);
       }
-      const bool got = umma::mbar_wait(&bar, phase, kPolls);
+      const bool got = umma::mbar_wait(&bar, phase, P.polls);
       phase ^= 1u;
       ok = __syncthreads_and(got) != 0;
-      if (!ok) break;
+      if (!ok) {
+        outstanding = !drop;  // a commit was issued and not yet seen
+        break;
+      }
       umma::fence_after_sync();
       const float* b = Bs + kB1 + layer * kHid;
 #pragma unroll 1
@@ -249,7 +258,8 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
   }
   if (!ok) {
     if (tid == 0) atomicExch(&g_mlp_error, 1);
-    umma::mbar_wait(&bar, phase ^ 1u, kPolls);  // the commit still outstanding, if any
+    // the commit still outstanding, if any, before the accumulator is freed
+    if (outstanding) umma::mbar_wait(&bar, phase ^ 1u, kPolls);
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -261,6 +271,7 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
 
 // ---- backward ---------------------------------------------------------------
 struct BwdParams {
+  uint32_t polls;  // bound of each mbarrier wait (polls)
   const uint16_t* wp;
   const uint16_t* x;
   int rows;
@@ -357,7 +368,7 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_backward_kernel(const BwdPara
     *reinterpret_cast<uint4*>(D + umma::core_off(r, col + 8, kRows)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
   };
   auto wait_mma = [&]() -> bool {
-    const bool got = umma::mbar_wait(&bar, phase, kPolls);
+    const bool got = umma::mbar_wait(&bar, phase, P.polls);
     phase ^= 1u;
     const bool all = __syncthreads_and(got) != 0;
     if (all) umma::fence_after_sync();
@@ -688,6 +699,11 @@ __global__ void impulses_kernel(const ImpulseParams P) {
 }
 
 // ---- launch helpers -----------------------------------------------------------
+// Wait bound of the MLP kernels (polls of an mbarrier), and the test hook
+// that drops each forward CTA's first commit; set by sapb_mlp_test_hooks.
+static uint32_t g_host_polls = kPolls;
+static int g_host_drop_first_commit = 0;
+
 static int sm_count() {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -751,6 +767,8 @@ static int32_t forward_common(const uint16_t* packed, const float* bias, const u
   }
   FwdParams P;
   memset(&P, 0, sizeof(P));
+  P.polls = g_host_polls;
+  P.drop_first_commit = g_host_drop_first_commit;
   P.wp = packed;
   P.bias = bias;
   P.x = x;
@@ -797,6 +815,7 @@ int32_t sapb_mlp_backward(const uint16_t* packed, const uint16_t* x, int32_t row
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   BwdParams P;
+  P.polls = g_host_polls;
   P.wp = packed;
   P.x = x;
   P.rows = rows;
@@ -831,6 +850,16 @@ int32_t sapb_mlp_adam(float* params, const float* grad, float* m, float* v, cons
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   adam_kernel<<<(kParams + 255) / 256, 256, 0, s>>>(params, grad, m, v, a, packed, bias);
   return cuda_status(cudaGetLastError(), "sapb_mlp_adam");
+}
+
+int32_t sapb_mlp_test_hooks(int32_t wait_polls, int32_t drop_first_commit) {
+  if (wait_polls < 0) {
+    set_last_error("sapb_mlp_test_hooks: wait_polls must be >= 0");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  g_host_polls = wait_polls == 0 ? kPolls : (uint32_t)wait_polls;
+  g_host_drop_first_commit = drop_first_commit != 0;
+  return SAPB_OK;
 }
 
 int32_t sapb_mlp_error(void* stream) {

@@ -548,11 +548,15 @@ class SapContactSolve:
                             linear_solve_precision=self.linear_solve_precision,
                             hessian_precision=self.hessian_precision, **kw)
 
-    def _launch_shape(self, P, opts, variant: str, stream) -> int:
+    def _launch_shape(self, P, opts, variant: str, stream, guess: torch.Tensor | None = None) -> int:
         """Resident CTAs per SM for this problem: 0 (the occupancy bound)
         without an autotuner; with one, its choice for the problem's key,
         timed here on this very problem the first time the key is seen
-        (never while a graph is being captured: then the bound)."""
+        (never while a graph is being captured: then the bound).  The solve
+        writes its start back into the warm-start guess `guess` (and the
+        guess may be the output velocity itself), so the guess is saved
+        before the timed solves and restored before each of them and after:
+        every timed solve, and the real one, starts from the same guess."""
         from .autotune import tuning_key
 
         if self.autotuner is None:
@@ -576,10 +580,13 @@ class SapContactSolve:
         if occ < 1:
             check(occ, "sapb_contact_solve_occupancy")
         cur = torch.cuda.current_stream(v.device)
+        saved = guess.clone() if guess is not None else None
 
         def time_ms(k: int) -> float:
             o = _abi.SolveOptions.from_buffer_copy(opts)
             o.ctas_per_sm = k
+            if saved is not None:
+                guess.copy_(saved)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(cur)
             check(lib.sapb_contact_solve(ctypes.byref(P), ctypes.byref(o), ctypes.byref(self.outputs),
@@ -589,7 +596,10 @@ class SapContactSolve:
             e1.synchronize()
             return e0.elapsed_time(e1)
 
-        return self.autotuner.tune(key, list(range(1, occ + 1)), time_ms)
+        chosen = self.autotuner.tune(key, list(range(1, occ + 1)), time_ms)
+        if saved is not None:
+            guess.copy_(saved)
+        return chosen
 
     def solve(self, contact_result: SapContactJacobianResult, state: SapState, control: SapControl | None, dt,
               v_star: torch.Tensor, *, v0: torch.Tensor | None = None, v_guess: torch.Tensor | None = None,
@@ -672,7 +682,7 @@ class SapContactSolve:
                 setattr(self.dof, name, _ptr(tt))
             P.dof = ctypes.pointer(self.dof)
         stream = ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream)
-        opts.ctas_per_sm = self._launch_shape(P, opts, variant, stream)
+        opts.ctas_per_sm = self._launch_shape(P, opts, variant, stream, v_guess)
         status = load().sapb_contact_solve(ctypes.byref(P), ctypes.byref(opts), ctypes.byref(self.outputs),
                                            self.workspace.data_ptr(), self.workspace.numel(), stream)
         check(status, "sapb_contact_solve")

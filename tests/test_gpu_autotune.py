@@ -68,3 +68,31 @@ def test_solver_autotune_writes_its_choice(cuda_device, tmp_path):
     assert set(entry["ms"]) == {str(k) for k in range(1, occ + 1)}
     assert 1 <= entry["ctas_per_sm"] <= occ
     assert all(np.isfinite(float(v)) and float(v) > 0 for v in entry["ms"].values())
+
+
+def test_tuning_after_the_first_step_keeps_the_answer(cuda_device, tmp_path):
+    """Tuning on a later step (warm-start guess active, the guess being the
+    output velocity): every timed solve starts from the same guess, and the
+    step's answer equals an untuned run's bit for bit."""
+    from sap_warp_b200.autotune import SolveAutotuner
+
+    model, state, control, contacts, _ = models.rollout_scene("humanoid", 512, 83, cuda_device)
+    kw = dict(max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32")
+
+    def run(tune_at):
+        solver = SolverSAP(model, **kw)
+        a = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone())
+        b = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone())
+        for k in range(4):
+            if k == tune_at:
+                solver.contact_solve.autotuner = SolveAutotuner(str(tmp_path / "late.json"))
+            solver.step(a, b, control, contacts, 2e-3)
+            a, b = b, a
+        torch.cuda.synchronize()
+        return a.joint_qd.clone(), solver.contact_solve.newton_iterations_env.clone()
+
+    qd0, it0 = run(None)
+    qd1, it1 = run(2)
+    assert torch.equal(qd0, qd1) and torch.equal(it0, it1)
