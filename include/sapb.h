@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 8
+#define SAPB_ABI_VERSION 9
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -323,6 +323,67 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* model, const sapb_step_
 int32_t sapb_integrate_positions(const sapb_model_desc* model, const double* joint_q_in, const double* v_prev,
                                  const double* v_new, const double* dt, int32_t mode, double* joint_q_out,
                                  void* stream);
+
+/* ---- the whole step behind a handle -----------------------------------------
+ * SolverSAP (sim/solver_sap.py:736-1512) as a C API: sapb_create allocates
+ * every work buffer (SolverSAP.__init__, :749-968); sapb_step runs one step
+ * (SolverSAP.step, :1388-1494) -- free motion and contact rows, the contact
+ * solve warm-started from the previous solution, position integration --
+ * on `stream`, without host synchronisation and without allocating, so a
+ * caller may capture it in a CUDA graph; sapb_get_status reads the per-world
+ * solve status; sapb_destroy frees the buffers.  SAP-order state (the public
+ * boundary is sapb_public_to_sap / sapb_sap_to_public_velocity / sapb_eval_fk). */
+typedef struct sapb_handle sapb_handle;
+
+#define SAPB_WARM_START_PREVIOUS_VELOCITY 0  /* the reference's: start from the last solution */
+#define SAPB_WARM_START_PREVIOUS_IMPULSES 1  /* also try v* + A^-1 J^T gamma_prev (candidate start) */
+#define SAPB_WORK_ORDER_INDEX 0
+#define SAPB_WORK_ORDER_PREVIOUS_ITERATIONS 1  /* most Newton iterations of the last step first */
+
+typedef struct sapb_step_options {
+  sapb_prepare_options prepare;     /* max_contacts, weight / point modes, fallbacks; tree_blocked = 0 */
+  sapb_solve_options solve;         /* the contact solve's options (line search, precisions, tolerances) */
+  int32_t position_integration;     /* SAPB_INTEGRATE_SAP_EULER / SAPB_INTEGRATE_MIDPOINT */
+  int32_t warm_start;               /* SAPB_WARM_START_* */
+  int32_t work_order;               /* SAPB_WORK_ORDER_* */
+} sapb_step_options;
+
+/* One step's device arrays: the start-of-step state, control and contacts
+ * (in), the drive / limit model (NULL: none; its joint_q is replaced by
+ * in.joint_q) and the new state (out; q_out must not alias in.joint_q). */
+typedef struct sapb_step_io {
+  sapb_step_inputs in;
+  const sapb_dof_terms* dof;
+  double* joint_q_out;              /* [coords] */
+  double* joint_qd_out;             /* [dofs] SAP order */
+} sapb_step_io;
+
+/* Fill the defaults of SolverSAP's keywords for a drake-preset step
+ * (sim/solver_sap.py:749-791): 128 contact slots, armijo_decay, FP64,
+ * sap_euler, previous-velocity warm start, work order by previous iterations. */
+void sapb_step_options_default(sapb_step_options* opts);
+/* Allocate the step's buffers for `model` (device arrays the caller keeps
+ * alive while the handle lives); reads the model's index arrays once
+ * (synchronous).  SAPB_ERR_UNSUPPORTED for shapes the on-chip solve cannot
+ * hold. */
+int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts, sapb_handle** out);
+/* One step on `stream` (see above). */
+int32_t sapb_step(sapb_handle* handle, const sapb_step_io* io, void* stream);
+/* Copy the last step's per-world solve status (0, SAPB_LS_* or SAPB_WORLD_*),
+ * convergence flags and Newton iterations into [W] arrays (host or device;
+ * any may be NULL), asynchronously on `stream`. */
+int32_t sapb_get_status(const sapb_handle* handle, int32_t* status, int32_t* converged, int32_t* newton_iterations,
+                        void* stream);
+/* Device pointers of the handle's solve outputs (SapContactSolveResult views,
+ * sim/contact_solve.py:188-232): valid until sapb_destroy. */
+int32_t sapb_step_solve_outputs(const sapb_handle* handle, sapb_solve_outputs* out);
+void sapb_destroy(sapb_handle* handle);
+
+/* The order in which the persistent solve should take the worlds next step:
+ * by the last Newton iterations, most first, ties in index order (stable),
+ * sorted on the device by one CTA (at most 32768 worlds).  No counterpart in
+ * the reference (its solve has no work queue). */
+int32_t sapb_world_order(const int32_t* newton_iterations, int32_t num_envs, int32_t* order, void* stream);
 
 /* ---- public-order boundary ------------------------------------------------
  * Newton-style callers hold joint velocities / forces in the public order

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 8
+SAPB_ABI_VERSION = 9
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -318,11 +318,33 @@ class AdamOptions(C.Structure):
                 ("weight_decay", C.c_float)]
 
 
+SAPB_WARM_START_PREVIOUS_VELOCITY = 0
+SAPB_WARM_START_PREVIOUS_IMPULSES = 1
+SAPB_WORK_ORDER_INDEX = 0
+SAPB_WORK_ORDER_PREVIOUS_ITERATIONS = 1
+
+
+class StepOptions(C.Structure):
+    _fields_ = [("prepare", PrepareOptions), ("solve", SolveOptions), ("position_integration", C.c_int32),
+                ("warm_start", C.c_int32), ("work_order", C.c_int32)]
+
+
+class StepIO(C.Structure):
+    _fields_ = [("inp", StepInputs), ("dof", C.POINTER(DofTerms)), ("joint_q_out", _p), ("joint_qd_out", _p)]
+
+
 # name -> (restype, argtypes) of every symbol include/sapb.h declares.
 EXPORTS = {
     "sapb_solve_options_default": (None, [C.POINTER(SolveOptions), C.c_int32]),
     "sapb_abi_version": (C.c_int32, []),
     "sapb_measure_fma_rate": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(C.c_double), _p]),
+    "sapb_step_options_default": (None, [C.POINTER(StepOptions)]),
+    "sapb_create": (C.c_int32, [C.POINTER(ModelDesc), C.POINTER(StepOptions), C.POINTER(_p)]),
+    "sapb_step": (C.c_int32, [_p, C.POINTER(StepIO), _p]),
+    "sapb_get_status": (C.c_int32, [_p, _p, _p, _p, _p]),
+    "sapb_step_solve_outputs": (C.c_int32, [_p, C.POINTER(SolveOutputs)]),
+    "sapb_destroy": (None, [_p]),
+    "sapb_world_order": (C.c_int32, [_p, C.c_int32, _p, _p]),
     "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_occupancy": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve": (

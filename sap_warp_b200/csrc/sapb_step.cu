@@ -1,0 +1,442 @@
+// sapb_step.cu -- the whole SAP step behind one handle, for hosts that drive
+// the step from C (SolverSAP.__init__ / .step, sim/solver_sap.py:749-968 and
+// :1388-1494, as a C API): sapb_create allocates every work buffer once,
+// sapb_step runs free motion + contact rows, the contact solve (with the
+// previous-velocity or previous-impulse warm start) and the position
+// integration on the caller's stream without host synchronisation (so a
+// caller may capture it in a CUDA graph), sapb_get_status copies the
+// per-world solve statuses, sapb_destroy frees the buffers.
+//
+// Also the stable work-order sort (sapb_world_order): the persistent solve
+// takes the worlds in the order of the previous step's Newton iterations,
+// most first; one CTA sorts keys (iterations descending, world index
+// ascending) by a bitonic network in shared memory.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "sapb_internal.h"
+
+namespace sapb {
+namespace {
+
+constexpr int kOrderThreads = 1024;
+constexpr int kOrderMaxWorlds = 32768;  // 2^15 keys of 4 bytes: 128 KB of shared memory
+constexpr uint32_t kIndexBits = 16;     // world index in the low bits (< 2^16 after the check)
+
+// Keys (0x7fff - min(iterations, 0x7fff)) << 16 | index sorted ascending:
+// iterations descending, ties in index order (stable).  Padding keys
+// 0xffffffff sort last.
+__global__ void __launch_bounds__(kOrderThreads) world_order_kernel(const int32_t* iters, int32_t W, int32_t N,
+                                                                    int32_t* order) {
+  extern __shared__ uint32_t keys[];
+  for (int i = threadIdx.x; i < N; i += kOrderThreads) {
+    uint32_t key = 0xffffffffu;
+    if (i < W) {
+      int it = iters[i];
+      it = it < 0 ? 0 : (it > 0x7fff ? 0x7fff : it);
+      key = ((uint32_t)(0x7fff - it) << kIndexBits) | (uint32_t)i;
+    }
+    keys[i] = key;
+  }
+  __syncthreads();
+  for (int k = 2; k <= N; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < N; i += kOrderThreads) {
+        const int p = i ^ j;
+        if (p > i) {
+          const uint32_t a = keys[i], b = keys[p];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) {
+            keys[i] = b;
+            keys[p] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < W; i += kOrderThreads) order[i] = (int32_t)(keys[i] & 0xffffu);
+}
+
+template <typename T>
+cudaError_t dev_alloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count);
+}
+
+}  // namespace
+}  // namespace sapb
+
+using namespace sapb;
+
+struct sapb_handle {
+  sapb_model_desc model;
+  sapb_step_options opts;
+  int32_t W, n, C, B, Q;
+  // free motion + contact rows
+  double *v_star, *vdot, *A, *J, *phi0, *w_eff, *mu, *stiffness, *tau_d, *factor, *vc_star;
+  int32_t *count, *body0, *body1, *truncated;
+  void* prep_ws;
+  size_t prep_ws_bytes;
+  // solve
+  double *v, *gamma, *gamma_prev, *cost, *grad_norm;
+  int32_t *mode, *iters, *ls_iters, *converged, *status, *ws_accepted, *guess_flag, *order;
+  int32_t *body_dof_start, *body_dof_count;
+  void* solve_ws;
+  size_t solve_ws_bytes;
+};
+
+extern "C" {
+
+int32_t sapb_world_order(const int32_t* newton_iterations, int32_t num_envs, int32_t* order, void* stream) {
+  if (num_envs < 0 || (num_envs > 0 && (!newton_iterations || !order))) {
+    set_last_error("sapb_world_order: invalid argument");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (num_envs > kOrderMaxWorlds) {
+    set_last_error("sapb_world_order: %d worlds above the supported %d", num_envs, kOrderMaxWorlds);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if (num_envs == 0) return SAPB_OK;
+  int N = 1;
+  while (N < num_envs) N <<= 1;
+  const size_t smem = sizeof(uint32_t) * (size_t)N;
+  cudaError_t err = cudaFuncSetAttribute(world_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err == cudaSuccess) {
+    world_order_kernel<<<1, kOrderThreads, smem, static_cast<cudaStream_t>(stream)>>>(newton_iterations, num_envs,
+                                                                                       N, order);
+    err = cudaGetLastError();
+  }
+  if (err != cudaSuccess) {
+    set_last_error("sapb_world_order: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  return SAPB_OK;
+}
+
+void sapb_step_options_default(sapb_step_options* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->prepare.max_contacts = 128;
+  o->prepare.contact_weight_mode = SAPB_WEIGHT_DIAG_DELASSUS;
+  o->prepare.contact_point_mode = SAPB_POINT_MIDPOINT;
+  o->prepare.fallback_mu = 0.1;
+  o->prepare.fallback_stiffness = 1.0e10;
+  o->prepare.fallback_tau_d = 0.0;
+  o->prepare.tree_blocked = 0;
+  sapb_solve_options_default(&o->solve, SAPB_LS_ARMIJO_DECAY);
+  o->position_integration = SAPB_INTEGRATE_SAP_EULER;
+  o->warm_start = SAPB_WARM_START_PREVIOUS_VELOCITY;
+  o->work_order = SAPB_WORK_ORDER_PREVIOUS_ITERATIONS;
+}
+
+void sapb_destroy(sapb_handle* h) {
+  if (!h) return;
+  void* ptrs[] = {h->v_star, h->vdot, h->A, h->J, h->phi0, h->w_eff, h->mu, h->stiffness, h->tau_d, h->factor,
+                  h->vc_star, h->count, h->body0, h->body1, h->truncated, h->prep_ws, h->v, h->gamma,
+                  h->gamma_prev, h->cost, h->grad_norm, h->mode, h->iters, h->ls_iters, h->converged, h->status,
+                  h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete h;
+}
+
+int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts, sapb_handle** out) {
+  if (!model || !opts || !out) {
+    set_last_error("sapb_create: null argument");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  const int32_t W = model->num_worlds, n = model->dofs_per_world, C = opts->prepare.max_contacts;
+  const int32_t B = W * model->bodies_per_world, Q = W * model->coords_per_world;
+  const int32_t J = W * model->joints_per_world, A = W * model->articulations_per_world;
+  if (W < 1 || n < 1 || C < 1 || model->bodies_per_world < 1 || J < 1 || A < 1 || !model->joint_child ||
+      !model->joint_qd_start || !model->joint_dof_dim || !model->articulation_start) {
+    set_last_error("sapb_create: invalid model description");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (opts->prepare.tree_blocked) {
+    set_last_error("sapb_create: the handle runs the dense layout (tree_blocked must be 0)");
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  if (opts->position_integration != SAPB_INTEGRATE_SAP_EULER && opts->position_integration != SAPB_INTEGRATE_MIDPOINT) {
+    set_last_error("sapb_create: position_integration must be SAPB_INTEGRATE_SAP_EULER or _MIDPOINT");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (opts->warm_start != SAPB_WARM_START_PREVIOUS_VELOCITY && opts->warm_start != SAPB_WARM_START_PREVIOUS_IMPULSES) {
+    set_last_error("sapb_create: warm_start must be SAPB_WARM_START_PREVIOUS_VELOCITY or _PREVIOUS_IMPULSES");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (opts->work_order == SAPB_WORK_ORDER_PREVIOUS_ITERATIONS && W > kOrderMaxWorlds) {
+    set_last_error("sapb_create: work_order by previous iterations supports at most %d worlds", kOrderMaxWorlds);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  const size_t solve_smem = contact_solve_smem_bytes(n, C, opts->solve.hessian_precision == SAPB_FP32 ||
+                                                                   opts->solve.linear_solve_precision == SAPB_FP32
+                                                               ? SAPB_FP32
+                                                               : SAPB_FP64);
+  if (solve_smem > kMaxSmemPerBlock) {
+    set_last_error("sapb_create: worlds of %d DOFs and %d contact slots exceed the on-chip solve", n, C);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  // body -> world-local DOF range of its articulation (the reference's
+  // _build_body_dof_maps, sim/contact_solve.py:3724-3758), from the model's
+  // index arrays (copied to the host once)
+  std::vector<int32_t> child(J), qd_start(J + 1), dim(2 * J), art(A + 1);
+  cudaError_t err = cudaMemcpy(child.data(), model->joint_child, sizeof(int32_t) * J, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(qd_start.data(), model->joint_qd_start, sizeof(int32_t) * (J + 1), cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(dim.data(), model->joint_dof_dim, sizeof(int32_t) * 2 * J, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(art.data(), model->articulation_start, sizeof(int32_t) * (A + 1), cudaMemcpyDeviceToHost);
+  if (err != cudaSuccess) {
+    set_last_error("sapb_create: reading the model: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  std::vector<int32_t> bstart(B, -1), bcount(B, 0);
+  for (int a = 0; a < A; ++a) {
+    int s0 = -1, tot = 0;
+    for (int j = art[a]; j < art[a + 1] && j < J; ++j) {
+      const int cnt = dim[2 * j] + dim[2 * j + 1];
+      if (cnt > 0 && (s0 < 0 || qd_start[j] < s0)) s0 = qd_start[j];
+      tot += cnt;
+    }
+    if (s0 < 0 || tot <= 0) continue;
+    for (int j = art[a]; j < art[a + 1] && j < J; ++j) {
+      const int b = child[j];
+      if (b >= 0 && b < B) {
+        bstart[b] = s0 - (b / model->bodies_per_world) * n;
+        bcount[b] = tot;
+      }
+    }
+  }
+  sapb_handle* h = new sapb_handle;
+  memset(h, 0, sizeof(*h));
+  h->model = *model;
+  h->opts = *opts;
+  h->W = W;
+  h->n = n;
+  h->C = C;
+  h->B = B;
+  h->Q = Q;
+  const size_t Wn = (size_t)W * n, WC = (size_t)W * C;
+  const bool cand = opts->warm_start == SAPB_WARM_START_PREVIOUS_IMPULSES;
+  err = cudaSuccess;
+  auto take = [&](cudaError_t e) {
+    if (err == cudaSuccess) err = e;
+  };
+  take(dev_alloc(&h->v_star, Wn));
+  take(dev_alloc(&h->vdot, Wn));
+  take(dev_alloc(&h->A, Wn * n));
+  take(dev_alloc(&h->J, WC * 3 * n));
+  take(dev_alloc(&h->phi0, WC));
+  take(dev_alloc(&h->w_eff, WC));
+  take(dev_alloc(&h->mu, WC));
+  take(dev_alloc(&h->stiffness, WC));
+  take(dev_alloc(&h->tau_d, WC));
+  take(dev_alloc(&h->count, W));
+  take(dev_alloc(&h->body0, WC));
+  take(dev_alloc(&h->body1, WC));
+  take(dev_alloc(&h->truncated, 1));
+  if (cand) {
+    take(dev_alloc(&h->factor, Wn * n));
+    take(dev_alloc(&h->vc_star, WC * 3));
+    take(dev_alloc(&h->gamma_prev, WC * 3));
+  }
+  take(dev_alloc(&h->v, Wn));
+  take(dev_alloc(&h->gamma, WC * 3));
+  take(dev_alloc(&h->cost, W));
+  take(dev_alloc(&h->grad_norm, W));
+  take(dev_alloc(&h->mode, WC));
+  take(dev_alloc(&h->iters, W));
+  take(dev_alloc(&h->ls_iters, W));
+  take(dev_alloc(&h->converged, W));
+  take(dev_alloc(&h->status, W));
+  take(dev_alloc(&h->ws_accepted, W));
+  take(dev_alloc(&h->guess_flag, 1));
+  take(dev_alloc(&h->order, W));
+  take(dev_alloc(&h->body_dof_start, B));
+  take(dev_alloc(&h->body_dof_count, B));
+  h->prep_ws_bytes = sapb_prepare_workspace_size(model, C);
+  h->solve_ws_bytes = sapb_contact_solve_workspace_size(W, n, C);
+  if (err == cudaSuccess) err = cudaMalloc(&h->prep_ws, h->prep_ws_bytes > 0 ? h->prep_ws_bytes : 16);
+  if (err == cudaSuccess) err = cudaMalloc(&h->solve_ws, h->solve_ws_bytes > 0 ? h->solve_ws_bytes : 16);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(h->body_dof_start, bstart.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(h->body_dof_count, bcount.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemset(h->guess_flag, 0, sizeof(int32_t));
+  if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_prev, 0, sizeof(double) * WC * 3);
+  if (err == cudaSuccess) err = cudaMemset(h->iters, 0, sizeof(int32_t) * W);
+  if (err == cudaSuccess) {
+    std::vector<int32_t> idx(W);
+    for (int i = 0; i < W; ++i) idx[i] = i;
+    err = cudaMemcpy(h->order, idx.data(), sizeof(int32_t) * W, cudaMemcpyHostToDevice);
+  }
+  if (err != cudaSuccess) {
+    set_last_error("sapb_create: %s", cudaGetErrorString(err));
+    sapb_destroy(h);
+    return SAPB_ERR_CUDA;
+  }
+  *out = h;
+  return SAPB_OK;
+}
+
+int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
+  if (!h || !io || !io->in.joint_q || !io->in.joint_qd || !io->in.dt || !io->joint_q_out || !io->joint_qd_out) {
+    set_last_error("sapb_step: null argument");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (io->joint_q_out == io->in.joint_q) {
+    set_last_error("sapb_step: joint_q_out must not alias the input coordinates");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool cand = h->opts.warm_start == SAPB_WARM_START_PREVIOUS_IMPULSES;
+  const bool order = h->opts.work_order == SAPB_WORK_ORDER_PREVIOUS_ITERATIONS;
+  // free motion and contact rows (sim/solver_sap.py:1415-1433)
+  sapb_prepare_outputs po;
+  memset(&po, 0, sizeof(po));
+  po.v_star = h->v_star;
+  po.vdot = h->vdot;
+  po.dynamics_matrix = h->A;
+  po.jacobian = h->J;
+  po.contact_count = h->count;
+  po.phi0 = h->phi0;
+  po.w_eff = h->w_eff;
+  po.mu = h->mu;
+  po.stiffness = h->stiffness;
+  po.tau_d = h->tau_d;
+  po.body0 = h->body0;
+  po.body1 = h->body1;
+  po.truncated_count = h->truncated;
+  po.dynamics_factor = h->factor;
+  po.vc_star = h->vc_star;
+  int32_t st = sapb_free_motion_contacts(&h->model, &io->in, &h->opts.prepare, &po, h->prep_ws, h->prep_ws_bytes,
+                                         stream);
+  if (st != SAPB_OK) return st;
+  // contact solve (sim/solver_sap.py:1434-1460), warm start from the last
+  // solution once a step has run
+  sapb_contact_problem p;
+  memset(&p, 0, sizeof(p));
+  p.num_envs = h->W;
+  p.dof_per_env = h->n;
+  p.max_contacts = h->C;
+  p.num_bodies = h->B;
+  p.contact_count = h->count;
+  p.dynamics_matrix = h->A;
+  p.jacobian = h->J;
+  p.phi0 = h->phi0;
+  p.w_eff = h->w_eff;
+  p.mu = h->mu;
+  p.stiffness = h->stiffness;
+  p.tau_d = h->tau_d;
+  p.body0 = h->body0;
+  p.body1 = h->body1;
+  p.body_dof_start = h->body_dof_start;
+  p.body_dof_count = h->body_dof_count;
+  p.v_star = h->v_star;
+  p.v0 = io->in.joint_qd;
+  p.v_guess = h->v;
+  p.v_guess_active = h->guess_flag;
+  p.dt = io->in.dt;
+  // the drive / limit terms act at this step's coordinates (the solve copies
+  // the struct into its launch parameters)
+  sapb_dof_terms dof_local;
+  if (io->dof) {
+    dof_local = *io->dof;
+    dof_local.joint_q = io->in.joint_q;
+    dof_local.joint_coord_count = h->Q;
+    p.dof = &dof_local;
+  }
+  if (cand) {
+    p.gamma0 = h->gamma_prev;
+    p.gamma0_count = 1;
+    p.dynamics_factor = h->factor;
+  }
+  p.world_order = order ? h->order : nullptr;
+  sapb_solve_outputs so;
+  memset(&so, 0, sizeof(so));
+  so.v = h->v;
+  so.contact_gamma = h->gamma;
+  so.contact_mode = h->mode;
+  so.cost = h->cost;
+  so.newton_iterations = h->iters;
+  so.line_search_iterations = h->ls_iters;
+  so.converged = h->converged;
+  so.status = h->status;
+  so.grad_norm = h->grad_norm;
+  so.warm_start_accepted = h->ws_accepted;
+  st = sapb_contact_solve(&p, &h->opts.solve, &so, h->solve_ws, h->solve_ws_bytes, stream);
+  if (st != SAPB_OK) return st;
+  if (order) {
+    st = sapb_world_order(h->iters, h->W, h->order, stream);
+    if (st != SAPB_OK) return st;
+  }
+  // position integration (sim/solver_sap.py:1267-1386); joints without
+  // coordinates to integrate keep theirs
+  cudaError_t err = cudaMemcpyAsync(io->joint_q_out, io->in.joint_q, sizeof(double) * h->Q, cudaMemcpyDeviceToDevice, s);
+  if (err != cudaSuccess) {
+    set_last_error("sapb_step: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  st = sapb_integrate_positions(&h->model, io->in.joint_q, io->in.joint_qd, h->v, io->in.dt,
+                                h->opts.position_integration, io->joint_q_out, stream);
+  if (st != SAPB_OK) return st;
+  err = cudaMemcpyAsync(io->joint_qd_out, h->v, sizeof(double) * (size_t)h->W * h->n, cudaMemcpyDeviceToDevice, s);
+  if (err == cudaSuccess) err = cudaMemsetAsync(h->guess_flag, 1, sizeof(int32_t), s);  // nonzero: warm start on
+  if (err == cudaSuccess && cand)
+    err = cudaMemcpyAsync(h->gamma_prev, h->gamma, sizeof(double) * (size_t)h->W * h->C * 3, cudaMemcpyDeviceToDevice,
+                          s);
+  if (err != cudaSuccess) {
+    set_last_error("sapb_step: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  return SAPB_OK;
+}
+
+int32_t sapb_get_status(const sapb_handle* h, int32_t* status, int32_t* converged, int32_t* newton_iterations,
+                        void* stream) {
+  if (!h) {
+    set_last_error("sapb_get_status: null handle");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t bytes = sizeof(int32_t) * (size_t)h->W;
+  cudaError_t err = cudaSuccess;
+  if (status) err = cudaMemcpyAsync(status, h->status, bytes, cudaMemcpyDefault, s);
+  if (err == cudaSuccess && converged) err = cudaMemcpyAsync(converged, h->converged, bytes, cudaMemcpyDefault, s);
+  if (err == cudaSuccess && newton_iterations)
+    err = cudaMemcpyAsync(newton_iterations, h->iters, bytes, cudaMemcpyDefault, s);
+  if (err != cudaSuccess) {
+    set_last_error("sapb_get_status: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  return SAPB_OK;
+}
+
+int32_t sapb_step_solve_outputs(const sapb_handle* h, sapb_solve_outputs* out) {
+  if (!h || !out) {
+    set_last_error("sapb_step_solve_outputs: null argument");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  memset(out, 0, sizeof(*out));
+  out->v = h->v;
+  out->contact_gamma = h->gamma;
+  out->contact_mode = h->mode;
+  out->cost = h->cost;
+  out->newton_iterations = h->iters;
+  out->line_search_iterations = h->ls_iters;
+  out->converged = h->converged;
+  out->status = h->status;
+  out->grad_norm = h->grad_norm;
+  out->warm_start_accepted = h->ws_accepted;
+  return SAPB_OK;
+}
+
+}  // extern "C"

@@ -548,6 +548,31 @@ class SapContactSolve:
                             linear_solve_precision=self.linear_solve_precision,
                             hessian_precision=self.hessian_precision, **kw)
 
+    def solve_options(self, line_search_variant: str = "monotone_decay", *, max_iterations: int = 100,
+                      optimality_abs_tol: float = 1.0e-14, optimality_rel_tol: float = 1.0e-6,
+                      cost_abs_tol: float | None = None, cost_rel_tol: float | None = None,
+                      line_search_max_iterations: int = 40, armijo_c: float = 1.0e-4, rho: float = 0.8,
+                      line_search_relative_slop: float | None = None):
+        """(variant, sapb_solve_options) of solve() with the reference's
+        variant-dependent defaults (sim/contact_solve.py:6163-6182)."""
+        variant = normalize_sap_line_search_mode(line_search_variant)
+        if variant == "armijo_decay" and not (0.0 < float(rho) < 1.0):
+            raise ValueError(f"rho must lie in (0, 1), got {rho!r}.")
+        if variant == "exact_root" and int(line_search_max_iterations) == 40:
+            line_search_max_iterations = 100
+        if cost_abs_tol is None:
+            cost_abs_tol = 0.0 if variant == "monotone_decay" else 1.0e-30
+        if cost_rel_tol is None:
+            cost_rel_tol = 5.0e-3 if variant == "monotone_decay" else 1.0e-15
+        if line_search_relative_slop is None:
+            line_search_relative_slop = 1000.0 * np.finfo(np.float64).eps
+        opts = self.options(variant, max_iterations=int(max_iterations), optimality_abs_tol=float(optimality_abs_tol),
+                            optimality_rel_tol=float(optimality_rel_tol), cost_abs_tol=float(cost_abs_tol),
+                            cost_rel_tol=float(cost_rel_tol),
+                            line_search_max_iterations=int(line_search_max_iterations), armijo_c=float(armijo_c),
+                            rho=float(rho), line_search_relative_slop=float(line_search_relative_slop))
+        return variant, opts
+
     def _launch_shape(self, P, opts, variant: str, stream, guess: torch.Tensor | None = None) -> int:
         """Resident CTAs per SM for this problem: 0 (the occupancy bound)
         without an autotuner; with one, its choice for the problem's key,
@@ -616,31 +641,20 @@ class SapContactSolve:
         plain start on the cost.  world_order (W,) int32: the order in which
         the persistent kernel takes the worlds (a permutation; results do not
         depend on it)."""
-        variant = normalize_sap_line_search_mode(line_search_variant)
         if not bool(graph_conditional):
             raise ValueError("SapContactSolve only supports graph_conditional=True; "
                              "the Python Newton-loop fallback has been removed.")
-        if variant == "armijo_decay" and not (0.0 < float(rho) < 1.0):
-            raise ValueError(f"rho must lie in (0, 1), got {rho!r}.")
-        if variant == "exact_root" and int(line_search_max_iterations) == 40:
-            line_search_max_iterations = 100
-        if cost_abs_tol is None:
-            cost_abs_tol = 0.0 if variant == "monotone_decay" else 1.0e-30
-        if cost_rel_tol is None:
-            cost_rel_tol = 5.0e-3 if variant == "monotone_decay" else 1.0e-15
-        if line_search_relative_slop is None:
-            line_search_relative_slop = 1000.0 * np.finfo(np.float64).eps
+        variant, opts = self.solve_options(
+            line_search_variant, max_iterations=max_iterations, optimality_abs_tol=optimality_abs_tol,
+            optimality_rel_tol=optimality_rel_tol, cost_abs_tol=cost_abs_tol, cost_rel_tol=cost_rel_tol,
+            line_search_max_iterations=line_search_max_iterations, armijo_c=armijo_c, rho=rho,
+            line_search_relative_slop=line_search_relative_slop)
         if isinstance(dt, torch.Tensor):
             self.dt_world.copy_(dt.reshape(-1))
         else:
             self.dt_world.fill_(float(dt))
         if v0 is None:
             v0 = v_guess if v_guess is not None else v_star
-        opts = self.options(variant, max_iterations=int(max_iterations), optimality_abs_tol=float(optimality_abs_tol),
-                            optimality_rel_tol=float(optimality_rel_tol), cost_abs_tol=float(cost_abs_tol),
-                            cost_rel_tol=float(cost_rel_tol),
-                            line_search_max_iterations=int(line_search_max_iterations), armijo_c=float(armijo_c),
-                            rho=float(rho), line_search_relative_slop=float(line_search_relative_slop))
         v = self.view
         W, n, C = v.W, v.n, self.max_rigid_contact
         if self.tree_blocked:
@@ -901,9 +915,9 @@ class SolverSAP:
         self.work_order = str(work_order).strip().lower().replace("-", "_")
         if self.work_order not in ("previous_iterations", "index"):
             raise ValueError(f"work_order must be 'previous_iterations' or 'index', got {work_order!r}.")
+        if self.work_order == "previous_iterations" and view.W > 32768:
+            self.work_order = "index"  # the device sort of the work order holds at most 32768 worlds
         self._world_order = torch.arange(view.W, dtype=I32, device=dev)
-        self._order_keys = torch.zeros(view.W, dtype=I32, device=dev)
-        self._order_idx = torch.zeros(view.W, dtype=torch.int64, device=dev)
         if autotune:
             from .autotune import SolveAutotuner
 
@@ -922,6 +936,36 @@ class SolverSAP:
 
     def notify_model_changed(self, flags: int) -> None:
         return
+
+    def c_step_options(self) -> _abi.StepOptions:
+        """This solver's configuration as the options of the C step handle
+        (sapb_create / sapb_step): the same contact preparation, solve
+        options, integrator, warm start (previous velocity or previous
+        impulses) and work order, so a C host stepping the same model gets
+        the same trajectory."""
+        if self.contact_solve.tree_blocked:
+            raise NotImplementedError("the C step handle runs the dense layout")
+        if self.warm_start == "learned":
+            raise NotImplementedError("the C step handle takes the previous-velocity or previous-impulses warm start")
+        if self.static_substep:
+            iters, ls_iters = self.static_substep_iterations, self.static_substep_line_search_iterations
+        else:
+            iters, ls_iters = self.max_iterations, self.line_search_max_iterations
+        _, solve = self.contact_solve.solve_options(
+            self.line_search_variant, max_iterations=iters, optimality_abs_tol=self.optimality_abs_tol,
+            optimality_rel_tol=self.optimality_rel_tol, cost_abs_tol=self.cost_abs_tol,
+            cost_rel_tol=self.cost_rel_tol, line_search_max_iterations=ls_iters, armijo_c=self.armijo_c,
+            rho=self.rho, line_search_relative_slop=self.line_search_relative_slop)
+        o = _abi.StepOptions()
+        o.prepare = _abi.PrepareOptions.from_buffer_copy(self.contact_jacobian.opts)
+        o.solve = solve
+        o.position_integration = (_abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint"
+                                  else _abi.SAPB_INTEGRATE_SAP_EULER)
+        o.warm_start = (_abi.SAPB_WARM_START_PREVIOUS_IMPULSES if self.warm_start == "previous_impulses"
+                        else _abi.SAPB_WARM_START_PREVIOUS_VELOCITY)
+        o.work_order = (_abi.SAPB_WORK_ORDER_PREVIOUS_ITERATIONS if self.work_order == "previous_iterations"
+                        else _abi.SAPB_WORK_ORDER_INDEX)
+        return o
 
     def capture_steps(self, state_a: SapState, state_b: SapState, control: SapControl | None, contacts, dt,
                       warmup: int = 1) -> "torch.cuda.CUDAGraph":
@@ -1104,8 +1148,9 @@ class SolverSAP:
             world_order=self._world_order if self.work_order == "previous_iterations" else None)
         if self.work_order == "previous_iterations":
             # next step's queue: most Newton iterations first (stable: ties keep index order)
-            torch.sort(sr.newton_iterations_env, descending=True, stable=True, out=(self._order_keys, self._order_idx))
-            self._world_order.copy_(self._order_idx)
+            check(load().sapb_world_order(_ptr(sr.newton_iterations_env), self.view.W, _ptr(self._world_order),
+                                          ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)),
+                  "sapb_world_order")
         mark("integrate")
         # position integration (sim/solver_sap.py:1267-1386)
         mode = _abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint" else _abi.SAPB_INTEGRATE_SAP_EULER

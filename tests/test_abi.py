@@ -62,6 +62,19 @@ def test_no_compute_entry_points_without_gpu(lib):
     assert lib.sapb_mlp_forward(None, None, None, 4, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
     assert lib.sapb_warmstart_features(None, None, None, None, None, 0.0, None, None, None) == \
         _abi.SAPB_ERR_INVALID_ARGUMENT
+    # the whole-step handle, the world order and the FMA-rate probe reject bad arguments before any CUDA call
+    so = _abi.StepOptions()
+    lib.sapb_step_options_default(ctypes.byref(so))
+    assert so.prepare.max_contacts == 128 and so.solve.line_search_variant == _abi.SAPB_LS_ARMIJO_DECAY
+    assert so.work_order == _abi.SAPB_WORK_ORDER_PREVIOUS_ITERATIONS
+    assert lib.sapb_create(None, ctypes.byref(so), None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert lib.sapb_step(None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert lib.sapb_get_status(None, None, None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    lib.sapb_destroy(None)
+    assert lib.sapb_world_order(None, 4, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert lib.sapb_world_order(None, 0, None, None) == _abi.SAPB_OK
+    rate = ctypes.c_double()
+    assert lib.sapb_measure_fma_rate(7, 16, ctypes.byref(rate), None) == _abi.SAPB_ERR_INVALID_ARGUMENT
 
 
 def test_struct_layout_matches_header(tmp_path):
@@ -75,6 +88,8 @@ def test_struct_layout_matches_header(tmp_path):
         " sizeof(sapb_prepare_outputs)); printf(\"%zu %zu %zu %zu\\n\", sizeof(sapb_warmstart_norm),"
         " sizeof(sapb_mlp_train_buffers), sizeof(sapb_adam_options), offsetof(sapb_contact_problem, gamma0));"
         " printf(\"%zu %zu\\n\", sizeof(sapb_blocked_problem), offsetof(sapb_blocked_problem, world_order));"
+        " printf(\"%zu %zu %zu %zu\\n\", sizeof(sapb_step_options), offsetof(sapb_step_options, work_order),"
+        " sizeof(sapb_step_io), offsetof(sapb_step_io, joint_qd_out));"
         " return 0;}\n"
     )
     exe = tmp_path / "sizes"
@@ -86,5 +101,7 @@ def test_struct_layout_matches_header(tmp_path):
             ctypes.sizeof(_abi.ModelDesc), ctypes.sizeof(_abi.StepInputs), ctypes.sizeof(_abi.PrepareOptions),
             ctypes.sizeof(_abi.PrepareOutputs), ctypes.sizeof(_abi.WarmstartNorm),
             ctypes.sizeof(_abi.MlpTrainBuffers), ctypes.sizeof(_abi.AdamOptions), _abi.ContactProblem.gamma0.offset,
-            ctypes.sizeof(_abi.BlockedProblem), _abi.BlockedProblem.world_order.offset]
+            ctypes.sizeof(_abi.BlockedProblem), _abi.BlockedProblem.world_order.offset,
+            ctypes.sizeof(_abi.StepOptions), _abi.StepOptions.work_order.offset, ctypes.sizeof(_abi.StepIO),
+            _abi.StepIO.joint_qd_out.offset]
     assert got == want

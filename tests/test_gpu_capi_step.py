@@ -1,0 +1,99 @@
+"""The whole step through the C ABI (sapb_create / sapb_step /
+sapb_get_status / sapb_destroy) against SolverSAP on the same model, and the
+device work-order sort against a stable host sort."""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from sap_warp_b200 import _abi, models
+from sap_warp_b200._lib import check, load
+from sap_warp_b200.runtime import SapState
+from sap_warp_b200.solver import SolverSAP
+
+pytestmark = pytest.mark.gpu
+
+
+def _p(t):
+    return 0 if t is None else t.data_ptr()
+
+
+def test_world_order_is_a_stable_descending_sort(cuda_device):
+    lib = load()
+    rng = np.random.default_rng(5)
+    for W in (1, 7, 1000, 4096, 32768):
+        it = rng.integers(0, 12, size=W).astype(np.int32)
+        it[::97] = 40000  # clamped keys still sort first
+        d_it = torch.as_tensor(it, device=cuda_device)
+        order = torch.full((W,), -1, dtype=torch.int32, device=cuda_device)
+        check(lib.sapb_world_order(d_it.data_ptr(), W, order.data_ptr(),
+                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), "sapb_world_order")
+        torch.cuda.synchronize()
+        want = np.argsort(-np.minimum(it.astype(np.int64), 0x7FFF), kind="stable")
+        np.testing.assert_array_equal(order.cpu().numpy(), want)
+    assert lib.sapb_world_order(d_it.data_ptr(), 32769, order.data_ptr(), None) == _abi.SAPB_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("warm", ["previous_velocity", "previous_impulses"])
+def test_c_step_equals_solver_steps(cuda_device, warm):
+    W, dt, steps = 256, 2.0e-3, 4
+    model, state, control, contacts, _ = models.rollout_scene("humanoid", W, 61, cuda_device)
+    solver = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32",
+                       warm_start=warm)
+    a = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                 body_f=state.body_f.clone())
+    b = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                 body_f=state.body_f.clone())
+    for _ in range(steps):
+        solver.step(a, b, control, contacts, dt)
+        a, b = b, a
+    torch.cuda.synchronize()
+    ref_q, ref_qd = a.joint_q.clone(), a.joint_qd.clone()
+    ref_status = solver.contact_solve.ls_status.clone()
+    ref_iters = solver.contact_solve.newton_iterations_env.clone()
+
+    lib = load()
+    opts = solver.c_step_options()
+    handle = ctypes.c_void_p()
+    check(lib.sapb_create(ctypes.byref(solver.view.desc), ctypes.byref(opts), ctypes.byref(handle)), "sapb_create")
+    try:
+        q = [state.joint_q.to(torch.float64).clone(), state.joint_q.to(torch.float64).clone()]
+        qd = [state.joint_qd.to(torch.float64).clone(), state.joint_qd.to(torch.float64).clone()]
+        dt_w = torch.full((W,), dt, dtype=torch.float64, device=cuda_device)
+        jf = control.joint_f.to(torch.float64).contiguous()
+        bf = state.body_f.to(torch.float64).reshape(-1, 6).contiguous()
+        io = _abi.StepIO()
+        inp = io.inp
+        inp.joint_f, inp.body_f, inp.dt = _p(jf), _p(bf), _p(dt_w)
+        inp.contact_capacity = int(contacts.rigid_contact_shape0.numel())
+        inp.contact_count = _p(contacts.rigid_contact_count)
+        inp.contact_shape0, inp.contact_shape1 = _p(contacts.rigid_contact_shape0), _p(contacts.rigid_contact_shape1)
+        inp.contact_point0, inp.contact_point1 = _p(contacts.rigid_contact_point0d), _p(contacts.rigid_contact_point1d)
+        inp.contact_normal = _p(contacts.rigid_contact_normald)
+        inp.contact_margin0, inp.contact_margin1 = (_p(contacts.rigid_contact_margin0d),
+                                                    _p(contacts.rigid_contact_margin1d))
+        if solver.contact_solve.dof is not None:
+            io.dof = ctypes.pointer(solver.contact_solve.dof)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for k in range(steps):
+            src, dst = k % 2, 1 - k % 2
+            inp.joint_q, inp.joint_qd = _p(q[src]), _p(qd[src])
+            io.joint_q_out, io.joint_qd_out = _p(q[dst]), _p(qd[dst])
+            check(lib.sapb_step(handle, ctypes.byref(io), stream), "sapb_step")
+        status = torch.zeros(W, dtype=torch.int32, device=cuda_device)
+        conv = np.zeros(W, np.int32)
+        iters = torch.zeros(W, dtype=torch.int32, device=cuda_device)
+        check(lib.sapb_get_status(handle, status.data_ptr(), conv.ctypes.data, iters.data_ptr(), stream),
+              "sapb_get_status")
+        torch.cuda.synchronize()
+        out = _abi.SolveOutputs()
+        check(lib.sapb_step_solve_outputs(handle, ctypes.byref(out)), "sapb_step_solve_outputs")
+        assert out.v and out.contact_gamma and out.status
+    finally:
+        lib.sapb_destroy(handle)
+    last = steps % 2
+    assert torch.equal(q[last], ref_q.to(torch.float64)) and torch.equal(qd[last], ref_qd.to(torch.float64))
+    assert torch.equal(status, ref_status) and torch.equal(iters, ref_iters)
+    assert np.all(conv == 1)
