@@ -294,6 +294,7 @@ typedef struct sapb_prepare_outputs {
   double* vc_star;                  /* [W][C][3] free-motion contact velocities J_c v*, or NULL */
   double* tree_mass;                /* [W][B][6][6] diagonal blocks of A (tree_blocked only) */
   int32_t* contact_tree;            /* [W][C][2] tree of each contact side, -1 static (tree_blocked only) */
+  int32_t* contact_source;          /* [W][C] flat contact index of each slot, -1 past the world's count, or NULL */
 } sapb_prepare_outputs;
 
 /* Device workspace bytes of sapb_free_motion_contacts. */
@@ -323,6 +324,35 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* model, const sapb_step_
 int32_t sapb_integrate_positions(const sapb_model_desc* model, const double* joint_q_in, const double* v_prev,
                                  const double* v_new, const double* dt, int32_t mode, double* joint_q_out,
                                  void* stream);
+
+/* ---- contact history ------------------------------------------------------
+ * Impulses carried from one step's contact slots to the next step's by
+ * contact identity (no counterpart in the reference, which warm-starts from
+ * the previous velocity only): a contact is the same if its shape pair
+ * matches and its shape1 witness point in shape1's body frame (the stable
+ * feature of every primitive pair: sphere centre, box corner) is the mutually
+ * nearest among the pair's contacts, looked for within 64 slots of its own.
+ * Slots shift when contacts appear or vanish; with an unchanged contact
+ * buffer every slot maps to itself.  One CTA per world; the keys are
+ * updated in place (this step's replace the previous step's). */
+typedef struct sapb_contact_history {
+  int32_t num_envs;
+  int32_t max_contacts;             /* C */
+  int32_t num_flat;                 /* length of the flat contact arrays */
+  const int32_t* contact_count;     /* [W] this step's contacts per world (clamped to C) */
+  const int32_t* contact_source;    /* [W][C] flat index of each slot (sapb_prepare_outputs) */
+  const int32_t* flat_shape0;       /* [N] */
+  const int32_t* flat_shape1;       /* [N] */
+  const double* flat_point1;        /* [N][3] shape1 witness in its body frame */
+  int32_t* key_shape;               /* [W][C][2] in: the previous step's keys; out: this step's */
+  double* key_point;                /* [W][C][3] */
+  int32_t* key_count;               /* [W] in: previous counts (0 before the first step); out: this step's */
+  const double* gamma_prev;         /* [W][C][3] the previous step's impulses by its slots */
+  double* gamma_hist;               /* [W][C][3] out: carried impulses (0 for new contacts) */
+  int32_t* has_history;             /* [W][C] out: 1 carried, 0 new or empty slot */
+} sapb_contact_history;
+
+int32_t sapb_contact_history_update(const sapb_contact_history* hist, void* stream);
 
 /* ---- the whole step behind a handle -----------------------------------------
  * SolverSAP (sim/solver_sap.py:736-1512) as a C API: sapb_create allocates
@@ -440,6 +470,11 @@ typedef struct sapb_collision_shapes {
   const int32_t* shape_body;        /* [S] body, -1 static */
   const double* shape_margin;       /* [S] or NULL */
   double gap;                       /* emit contacts whose signed distance is below gap */
+  /* [S] collision groups or NULL (every pair is tested): the rule of
+   * sap_test_group_pair (sim/collision/broad_phase_common.py:133-150) --
+   * 0 meets nothing, a positive group meets itself and negative groups, a
+   * negative group meets every group but itself. */
+  const int32_t* shape_collision_group;
 } sapb_collision_shapes;
 
 typedef struct sapb_contact_outputs {
@@ -638,6 +673,10 @@ int32_t sapb_mlp_pack(const float* params, uint16_t* packed, float* bias, void* 
 /* y[rows,3] = MLP(x), x [rows,16] BF16 (16-byte aligned, columns 12..15 zero). */
 int32_t sapb_mlp_forward(const uint16_t* packed, const float* bias, const uint16_t* x, int32_t rows, float* y,
                          void* stream);
+/* sapb_mlp_forward over the 128-row tiles whose tile_active[tile] is nonzero
+ * only (the other tiles' rows of y are not written). */
+int32_t sapb_mlp_forward_tiles(const uint16_t* packed, const float* bias, const uint16_t* x, int32_t rows, float* y,
+                               const int32_t* tile_active, void* stream);
 /* Training forward: saves buf->act / buf->pre, writes buf->dy and adds the
  * squared error to buf->loss; y optional. */
 int32_t sapb_mlp_forward_train(const uint16_t* packed, const float* bias, const uint16_t* x, const float* target,
@@ -667,12 +706,20 @@ int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const doubl
                                 const double* gamma_prev, const double* vc_star,
                                 const sapb_warmstart_norm* norm, double tau_fallback, uint16_t* features,
                                 float* raw, void* stream);
+/* Per tile of 128 slot rows (E*C rows, world-major): 1 if a live slot has no
+ * history (has_history [E,C] zero or NULL), i.e. the network has a row to
+ * predict there; for sapb_mlp_forward_tiles. */
+int32_t sapb_warmstart_active_tiles(const sapb_contact_problem* problem, const int32_t* has_history,
+                                    int32_t* tile_active, void* stream);
 /* gamma0 [E,C,3] from the network output mlp_out [E*C,3] and the previous
  * step's impulses gamma_prev [E,C,3] (NULL: 0); opts supplies the
- * regularization (contact_beta, contact_sigma, contact_tau_d fallback). */
+ * regularization (contact_beta, contact_sigma, contact_tau_d fallback).
+ * With has_history [E,C] (NULL: none), slots whose contact has history keep
+ * gamma_prev and the network's prediction serves the others. */
 int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float* mlp_out,
-                                const double* gamma_prev, const sapb_warmstart_norm* norm,
-                                const sapb_solve_options* opts, double* gamma0, void* stream);
+                                const double* gamma_prev, const int32_t* has_history,
+                                const sapb_warmstart_norm* norm, const sapb_solve_options* opts, double* gamma0,
+                                void* stream);
 
 #ifdef __cplusplus
 }

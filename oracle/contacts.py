@@ -73,7 +73,18 @@ def generate(shapes, body_q, gap=1.0e-3):
             face[k] = s * ha[k]
             emit(a, b, Xa[0] + qrot(Xa[1], face), vw, qrot(Xa[1], nl), ma, mb)
 
+    groups = getattr(shapes, "shape_collision_group", None)
+
+    def groups_meet(ga, gb):  # sim/collision/broad_phase_common.py:133-150
+        if ga == 0 or gb == 0:
+            return False
+        if ga > 0:
+            return ga == gb or gb < 0
+        return ga != gb
+
     def pair(sa, sb):
+        if groups is not None and not groups_meet(int(groups[sa]), int(groups[sb])):
+            return
         a, b = sa, sb
         if shapes.shape_type[a] > shapes.shape_type[b]:
             a, b = b, a

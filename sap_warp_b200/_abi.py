@@ -164,6 +164,7 @@ class CollisionShapes(C.Structure):
         ("shape_body", _p),
         ("shape_margin", _p),
         ("gap", C.c_double),
+        ("shape_collision_group", _p),
     ]
 
 
@@ -288,6 +289,7 @@ class PrepareOutputs(C.Structure):
         ("vc_star", _p),
         ("tree_mass", _p),
         ("contact_tree", _p),
+        ("contact_source", _p),
     ]
 
 
@@ -333,6 +335,13 @@ class StepIO(C.Structure):
     _fields_ = [("inp", StepInputs), ("dof", C.POINTER(DofTerms)), ("joint_q_out", _p), ("joint_qd_out", _p)]
 
 
+class ContactHistory(C.Structure):
+    _fields_ = [("num_envs", C.c_int32), ("max_contacts", C.c_int32), ("num_flat", C.c_int32),
+                ("contact_count", _p), ("contact_source", _p), ("flat_shape0", _p), ("flat_shape1", _p),
+                ("flat_point1", _p), ("key_shape", _p), ("key_point", _p), ("key_count", _p), ("gamma_prev", _p),
+                ("gamma_hist", _p), ("has_history", _p)]
+
+
 # name -> (restype, argtypes) of every symbol include/sapb.h declares.
 EXPORTS = {
     "sapb_solve_options_default": (None, [C.POINTER(SolveOptions), C.c_int32]),
@@ -345,6 +354,7 @@ EXPORTS = {
     "sapb_step_solve_outputs": (C.c_int32, [_p, C.POINTER(SolveOutputs)]),
     "sapb_destroy": (None, [_p]),
     "sapb_world_order": (C.c_int32, [_p, C.c_int32, _p, _p]),
+    "sapb_contact_history_update": (C.c_int32, [C.POINTER(ContactHistory), _p]),
     "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_occupancy": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve": (
@@ -393,8 +403,10 @@ EXPORTS = {
         C.c_int32, [C.POINTER(ContactProblem), _p, _p, _p, C.POINTER(WarmstartNorm), C.c_double, _p, _p, _p]
     ),
     "sapb_warmstart_impulses": (
-        C.c_int32, [C.POINTER(ContactProblem), _p, _p, C.POINTER(WarmstartNorm), C.POINTER(SolveOptions), _p, _p]
+        C.c_int32, [C.POINTER(ContactProblem), _p, _p, _p, C.POINTER(WarmstartNorm), C.POINTER(SolveOptions), _p, _p]
     ),
+    "sapb_warmstart_active_tiles": (C.c_int32, [C.POINTER(ContactProblem), _p, _p, _p]),
+    "sapb_mlp_forward_tiles": (C.c_int32, [_p, _p, _p, C.c_int32, _p, _p, _p]),
 }
 
 

@@ -37,6 +37,7 @@ class ShapeSet:
     shape_X_bs: np.ndarray  # [S, 7] shape frame in its body frame (world frame if static)
     shape_body: np.ndarray  # int32 [S], -1 static
     shape_margin: np.ndarray | None = None  # [S]
+    shape_collision_group: np.ndarray | None = None  # int32 [S] (sim/collision/broad_phase_common.py:133-150)
 
 
 class ContactOverflowError(RuntimeError):
@@ -55,7 +56,9 @@ class ContactGenerator:
         t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
         self._keep = dict(type=t(shapes.shape_type, I32), scale=t(shapes.shape_scale, F64),
                           X=t(shapes.shape_X_bs, F64), body=t(shapes.shape_body, I32),
-                          margin=None if shapes.shape_margin is None else t(shapes.shape_margin, F64))
+                          margin=None if shapes.shape_margin is None else t(shapes.shape_margin, F64),
+                          group=None if shapes.shape_collision_group is None
+                          else t(shapes.shape_collision_group, I32))
         S = _abi.CollisionShapes()
         S.num_worlds, S.shapes_per_world, S.num_global_shapes = (shapes.num_worlds, shapes.shapes_per_world,
                                                                   shapes.num_global_shapes)
@@ -63,6 +66,7 @@ class ContactGenerator:
         S.shape_X_bs, S.shape_body = self._keep["X"].data_ptr(), self._keep["body"].data_ptr()
         S.shape_margin = 0 if self._keep["margin"] is None else self._keep["margin"].data_ptr()
         S.gap = float(gap)
+        S.shape_collision_group = 0 if self._keep["group"] is None else self._keep["group"].data_ptr()
         self.shapes = S
         lib = load()
         ws = int(lib.sapb_contacts_workspace_size(ctypes.byref(S)))

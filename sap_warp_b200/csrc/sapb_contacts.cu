@@ -139,7 +139,17 @@ __device__ void box_corners_vs_box(const GenParams& P, int sa_box, int sb_vert, 
   }
 }
 
+// sap_test_group_pair (sim/collision/broad_phase_common.py:133-150)
+__device__ __forceinline__ bool groups_meet(int ga, int gb) {
+  if (ga == 0 || gb == 0) return false;
+  if (ga > 0) return ga == gb || gb < 0;
+  return ga != gb;
+}
+
 __device__ void pair_contacts(const GenParams& P, int sa, int sb, Emit& emit) {
+  if (P.s.shape_collision_group &&
+      !groups_meet(P.s.shape_collision_group[sa], P.s.shape_collision_group[sb]))
+    return;
   const int ta = P.s.shape_type[sa], tb = P.s.shape_type[sb];
   const double gap = P.s.gap;
   const double mga = P.s.shape_margin ? P.s.shape_margin[sa] : 0.0;

@@ -1,0 +1,153 @@
+// sapb_history.cu -- impulses carried across steps by contact identity.
+//
+// The previous-impulse warm start needs, for each of this step's contact
+// slots, the impulse the same contact had at the end of the previous step.
+// Slots are the contacts of a world in flat-buffer order, so when a contact
+// appears or vanishes the later slots shift.  A contact is recognised by its
+// key: the shape pair and the shape1 witness point in shape1's body frame
+// (constant for a sphere centre or a box corner).  Per world (one CTA) the
+// previous keys and this step's are staged in shared memory; a slot takes
+// the impulse of the previous slot with the same pair whose point is the
+// nearest to its own, provided that it is also the nearest of this step's
+// slots to that previous contact (mutual nearest, searched within 64 slots
+// of each side); then this step's keys replace the previous ones.  No
+// counterpart in the reference, whose warm start is the previous velocity.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "sapb_internal.h"
+
+namespace sapb {
+namespace {
+
+constexpr int kHistThreads = 128;
+constexpr int kHistWindow = 64;
+
+struct Key {
+  int s0, s1;
+  double x, y, z;
+};
+
+__device__ __forceinline__ double dist2(const Key& a, const Key& b) {
+  const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  return dx * dx + dy * dy + dz * dz;
+}
+
+__global__ void __launch_bounds__(kHistThreads) history_kernel(const sapb_contact_history H) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int C = H.max_contacts, e = blockIdx.x;
+  Key* prev = reinterpret_cast<Key*>(smem);
+  Key* cur = prev + C;
+  int np = H.key_count[e];
+  np = np < 0 ? 0 : (np > C ? C : np);
+  int nc = H.contact_count[e];
+  nc = nc < 0 ? 0 : (nc > C ? C : nc);
+  const size_t base = (size_t)e * C;
+  for (int c = threadIdx.x; c < np; c += kHistThreads) {
+    Key k;
+    k.s0 = H.key_shape[2 * (base + c)];
+    k.s1 = H.key_shape[2 * (base + c) + 1];
+    k.x = H.key_point[3 * (base + c)];
+    k.y = H.key_point[3 * (base + c) + 1];
+    k.z = H.key_point[3 * (base + c) + 2];
+    prev[c] = k;
+  }
+  for (int c = threadIdx.x; c < nc; c += kHistThreads) {
+    const int src = H.contact_source[base + c];
+    Key k{-2, -2, 0.0, 0.0, 0.0};
+    if (src >= 0 && src < H.num_flat) {
+      k.s0 = H.flat_shape0[src];
+      k.s1 = H.flat_shape1[src];
+      k.x = H.flat_point1[3 * (size_t)src];
+      k.y = H.flat_point1[3 * (size_t)src + 1];
+      k.z = H.flat_point1[3 * (size_t)src + 2];
+    }
+    cur[c] = k;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += kHistThreads) {
+    int best = -1;
+    if (c < nc && cur[c].s0 != -2) {
+      const Key k = cur[c];
+      double bd = DBL_MAX;
+      const int lo = c - kHistWindow > 0 ? c - kHistWindow : 0;
+      const int hi = c + kHistWindow + 1 < np ? c + kHistWindow + 1 : np;
+      for (int p = lo; p < hi; ++p) {
+        if (prev[p].s0 != k.s0 || prev[p].s1 != k.s1) continue;
+        const double d = dist2(k, prev[p]);
+        if (d < bd) {
+          bd = d;
+          best = p;
+        }
+      }
+      if (best >= 0) {  // mutual: this slot is the nearest of this step's to it
+        const Key kp = prev[best];
+        const int lo2 = best - kHistWindow > 0 ? best - kHistWindow : 0;
+        const int hi2 = best + kHistWindow + 1 < nc ? best + kHistWindow + 1 : nc;
+        for (int q = lo2; q < hi2; ++q) {
+          if (q == c || cur[q].s0 != kp.s0 || cur[q].s1 != kp.s1) continue;
+          const double d = dist2(kp, cur[q]);
+          if (d < bd || (d == bd && q < c)) {
+            best = -1;
+            break;
+          }
+        }
+      }
+    }
+    const size_t s = base + c;
+    if (best >= 0) {
+      const size_t ps = base + best;
+      H.gamma_hist[3 * s] = H.gamma_prev[3 * ps];
+      H.gamma_hist[3 * s + 1] = H.gamma_prev[3 * ps + 1];
+      H.gamma_hist[3 * s + 2] = H.gamma_prev[3 * ps + 2];
+    } else {
+      H.gamma_hist[3 * s] = 0.0;
+      H.gamma_hist[3 * s + 1] = 0.0;
+      H.gamma_hist[3 * s + 2] = 0.0;
+    }
+    if (H.has_history) H.has_history[s] = best >= 0 ? 1 : 0;
+  }
+  __syncthreads();  // every slot has read the previous keys
+  for (int c = threadIdx.x; c < nc; c += kHistThreads) {
+    const size_t s = base + c;
+    H.key_shape[2 * s] = cur[c].s0;
+    H.key_shape[2 * s + 1] = cur[c].s1;
+    H.key_point[3 * s] = cur[c].x;
+    H.key_point[3 * s + 1] = cur[c].y;
+    H.key_point[3 * s + 2] = cur[c].z;
+  }
+  if (threadIdx.x == 0) H.key_count[e] = nc;
+}
+
+}  // namespace
+}  // namespace sapb
+
+using namespace sapb;
+
+extern "C" int32_t sapb_contact_history_update(const sapb_contact_history* h, void* stream) {
+  if (!h || h->num_envs < 0 || h->max_contacts < 1 || h->num_flat < 0 ||
+      (h->num_envs > 0 && (!h->contact_count || !h->contact_source || !h->key_shape || !h->key_point ||
+                           !h->key_count || !h->gamma_prev || !h->gamma_hist ||
+                           (h->num_flat > 0 && (!h->flat_shape0 || !h->flat_shape1 || !h->flat_point1))))) {
+    set_last_error("sapb_contact_history_update: invalid argument");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (h->num_envs == 0) return SAPB_OK;
+  const size_t smem = sizeof(Key) * 2 * (size_t)h->max_contacts;
+  if (smem > kMaxSmemPerBlock) {
+    set_last_error("sapb_contact_history_update: %d slots per world exceed shared memory", h->max_contacts);
+    return SAPB_ERR_UNSUPPORTED;
+  }
+  cudaError_t err = cudaFuncSetAttribute(history_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err == cudaSuccess) {
+    history_kernel<<<h->num_envs, kHistThreads, smem, static_cast<cudaStream_t>(stream)>>>(*h);
+    err = cudaGetLastError();
+  }
+  if (err != cudaSuccess) {
+    set_last_error("sapb_contact_history_update: %s", cudaGetErrorString(err));
+    return SAPB_ERR_CUDA;
+  }
+  return SAPB_OK;
+}

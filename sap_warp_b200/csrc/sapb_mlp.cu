@@ -95,6 +95,7 @@ __device__ __forceinline__ void copy_bytes(void* dst, const void* src, int bytes
 struct FwdParams {
   uint32_t polls;          // bound of each mbarrier wait (polls)
   int drop_first_commit;   // test hook: each CTA's first MMA commit is not issued
+  const int32_t* tile_active;  // [tiles] 0: skip the tile (its outputs are not written); NULL: every tile
   const uint16_t* wp;
   const float* bias;
   const uint16_t* x;  // [rows][16] BF16
@@ -134,6 +135,12 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int q = warp & 3, hf = warp >> 2;
   const int r = 32 * q + lane;  // tile row of this thread
+  if (P.tile_active) {  // a CTA with no active tile returns before staging the weights (uniform)
+    bool any = false;
+    const int ntiles = (P.rows + kRows - 1) / kRows;
+    for (int t = blockIdx.x; t < ntiles && !any; t += gridDim.x) any = P.tile_active[t] != 0;
+    if (!any) return;
+  }
 
   copy_bytes(W1s, P.wp + kPW1, kHid * kIn * 2);
   copy_bytes(W2s, P.wp + kPW2, kImg * 2);
@@ -157,9 +164,12 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
   uint32_t phase = 0;
   bool ok = true, outstanding = false;
   const int tiles = (P.rows + kRows - 1) / kRows;
+  bool first_tile = true;
   for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    if (P.tile_active && P.tile_active[tile] == 0) continue;  // uniform over the CTA, before any barrier
     const int row0 = tile * kRows;
-    const bool first_tile = tile == (int)blockIdx.x;
+    const bool drop_here = first_tile;
+    first_tile = false;
     {
       const int rr = tid >> 1, ch = tid & 1;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
@@ -172,7 +182,7 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_forward_kernel(const FwdParam
     for (int layer = 0; layer < 3; ++layer) {
       // the test hook leaves this layer's barrier phase without a commit, so
       // its bounded wait cannot complete (nothing is left in flight)
-      const bool drop = P.drop_first_commit && first_tile && layer == 0;
+      const bool drop = P.drop_first_commit && drop_here && layer == 0;
       if (tid == 0 && !drop) {
         umma::fence_after_sync();
         // A = X or H (K-major, 128 rows), B = W (K-major, 128 output rows).
@@ -660,6 +670,7 @@ struct ImpulseParams {
   sapb_contact_problem p;
   const float* y;
   const double* gamma_prev;  // residual base (NULL: 0)
+  const int32_t* has_history;  // [E*C] 1: the slot keeps gamma_prev (NULL: the network everywhere)
   sapb_warmstart_norm norm;
   double beta, sigma, tau_fallback;
   double* gamma0;
@@ -678,7 +689,11 @@ __global__ void impulses_kernel(const ImpulseParams P) {
     int count = P.p.contact_count[e];
     count = count < 0 ? 0 : (count > C ? C : count);
     double g[3] = {0.0, 0.0, 0.0};
-    if (c < count) {
+    if (c < count && P.has_history && P.has_history[s] && P.gamma_prev) {
+      g[0] = P.gamma_prev[3 * s];
+      g[1] = P.gamma_prev[3 * s + 1];
+      g[2] = P.gamma_prev[3 * s + 2];
+    } else if (c < count) {
       const double w = fmax(P.p.w_eff[s], 1.0e-12);
       double y[3];
 #pragma unroll
@@ -695,6 +710,26 @@ __global__ void impulses_kernel(const ImpulseParams P) {
     P.gamma0[3 * s + 0] = g[0];
     P.gamma0[3 * s + 1] = g[1];
     P.gamma0[3 * s + 2] = g[2];
+  }
+}
+
+// Tiles of kRows slot rows that hold a live contact without history (the
+// rows the network must predict).
+__global__ void active_tiles_kernel(const sapb_contact_problem p, const int32_t* has_history, int32_t* tile_active) {
+  const int C = p.max_contacts;
+  const long slots = (long)p.num_envs * C;
+  const long tiles = (slots + kRows - 1) / kRows;
+  for (long t = (long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); t < tiles;
+       t += (long)gridDim.x * (blockDim.x / 32)) {
+    bool need = false;
+    for (long s = t * kRows + (threadIdx.x & 31); s < (t + 1) * kRows && s < slots; s += 32) {
+      const int e = (int)(s / C), c = (int)(s - (long)e * C);
+      int count = p.contact_count[e];
+      count = count < 0 ? 0 : (count > C ? C : count);
+      if (c < count && !(has_history && has_history[s])) need = true;
+    }
+    need = __any_sync(0xffffffffu, need);
+    if ((threadIdx.x & 31) == 0) tile_active[t] = need ? 1 : 0;
   }
 }
 
@@ -754,7 +789,8 @@ int32_t sapb_mlp_pack(const float* params, uint16_t* packed, float* bias, void* 
 }
 
 static int32_t forward_common(const uint16_t* packed, const float* bias, const uint16_t* x, int32_t rows, float* y,
-                              const float* target, const sapb_mlp_train_buffers* buf, void* stream, bool train) {
+                              const float* target, const sapb_mlp_train_buffers* buf, void* stream, bool train,
+                              const int32_t* tile_active = nullptr) {
   if (!packed || !bias || rows < 0 || (rows > 0 && !x) || (!train && rows > 0 && !y) ||
       (train && (!buf || !target || !buf->act || !buf->pre || !buf->dy || !buf->loss))) {
     set_last_error("sapb_mlp_forward: invalid argument");
@@ -769,6 +805,7 @@ static int32_t forward_common(const uint16_t* packed, const float* bias, const u
   memset(&P, 0, sizeof(P));
   P.polls = g_host_polls;
   P.drop_first_commit = g_host_drop_first_commit;
+  P.tile_active = tile_active;
   P.wp = packed;
   P.bias = bias;
   P.x = x;
@@ -796,6 +833,28 @@ static int32_t forward_common(const uint16_t* packed, const float* bias, const u
 int32_t sapb_mlp_forward(const uint16_t* packed, const float* bias, const uint16_t* x, int32_t rows, float* y,
                          void* stream) {
   return forward_common(packed, bias, x, rows, y, nullptr, nullptr, stream, false);
+}
+
+int32_t sapb_mlp_forward_tiles(const uint16_t* packed, const float* bias, const uint16_t* x, int32_t rows, float* y,
+                               const int32_t* tile_active, void* stream) {
+  return forward_common(packed, bias, x, rows, y, nullptr, nullptr, stream, false, tile_active);
+}
+
+int32_t sapb_warmstart_active_tiles(const sapb_contact_problem* problem, const int32_t* has_history,
+                                    int32_t* tile_active, void* stream) {
+  if (!problem || !tile_active || problem->num_envs < 0 || problem->max_contacts < 0 ||
+      (problem->num_envs > 0 && !problem->contact_count)) {
+    set_last_error("sapb_warmstart_active_tiles: invalid argument");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  const long slots = (long)problem->num_envs * problem->max_contacts;
+  if (slots == 0) return SAPB_OK;
+  const long tiles = (slots + kRows - 1) / kRows;
+  long blocks = (tiles + 7) / 8;
+  if (blocks > 8L * sm_count()) blocks = 8L * sm_count();
+  active_tiles_kernel<<<(int)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(*problem, has_history,
+                                                                                      tile_active);
+  return cuda_status(cudaGetLastError(), "sapb_warmstart_active_tiles");
 }
 
 int32_t sapb_mlp_forward_train(const uint16_t* packed, const float* bias, const uint16_t* x, const float* target,
@@ -910,8 +969,9 @@ int32_t sapb_warmstart_features(const sapb_contact_problem* problem, const doubl
 }
 
 int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float* mlp_out,
-                                const double* gamma_prev, const sapb_warmstart_norm* norm,
-                                const sapb_solve_options* opts, double* gamma0, void* stream) {
+                                const double* gamma_prev, const int32_t* has_history,
+                                const sapb_warmstart_norm* norm, const sapb_solve_options* opts, double* gamma0,
+                                void* stream) {
   if (!problem || !mlp_out || !norm || !opts || !gamma0 || problem->num_envs < 0 || problem->max_contacts < 0) {
     set_last_error("sapb_warmstart_impulses: invalid argument");
     return SAPB_ERR_INVALID_ARGUMENT;
@@ -927,6 +987,7 @@ int32_t sapb_warmstart_impulses(const sapb_contact_problem* problem, const float
   P.p = *problem;
   P.y = mlp_out;
   P.gamma_prev = gamma_prev;
+  P.has_history = has_history;
   P.norm = *norm;
   P.beta = opts->contact_beta;
   P.sigma = opts->contact_sigma;

@@ -615,6 +615,8 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     }
     wsync();
   }
+  if (P.out.contact_source)
+    for (int c = wt; c < C; c += wn) P.out.contact_source[(size_t)e * C + c] = c < cc ? P.env_src[(size_t)e * C + c] : -1;
   for (int c = wt; c < cc; c += wn) {
     const int src = P.env_src[(size_t)e * C + c];
     const int sh0 = P.in.contact_shape0[src], sh1 = P.in.contact_shape1[src];

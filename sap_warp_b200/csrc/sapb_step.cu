@@ -82,6 +82,9 @@ struct sapb_handle {
   int32_t *count, *body0, *body1, *truncated;
   void* prep_ws;
   size_t prep_ws_bytes;
+  // contact history (previous-impulse warm start): keys, carried impulses
+  int32_t *source, *key_shape, *key_count, *has_history;
+  double *key_point, *gamma_last;
   // solve
   double *v, *gamma, *gamma_prev, *cost, *grad_norm;
   int32_t *mode, *iters, *ls_iters, *converged, *status, *ws_accepted, *guess_flag, *order;
@@ -139,7 +142,8 @@ void sapb_destroy(sapb_handle* h) {
   void* ptrs[] = {h->v_star, h->vdot, h->A, h->J, h->phi0, h->w_eff, h->mu, h->stiffness, h->tau_d, h->factor,
                   h->vc_star, h->count, h->body0, h->body1, h->truncated, h->prep_ws, h->v, h->gamma,
                   h->gamma_prev, h->cost, h->grad_norm, h->mode, h->iters, h->ls_iters, h->converged, h->status,
-                  h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws};
+                  h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws,
+                  h->source, h->key_shape, h->key_count, h->has_history, h->key_point, h->gamma_last};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -247,6 +251,12 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     take(dev_alloc(&h->factor, Wn * n));
     take(dev_alloc(&h->vc_star, WC * 3));
     take(dev_alloc(&h->gamma_prev, WC * 3));
+    take(dev_alloc(&h->gamma_last, WC * 3));
+    take(dev_alloc(&h->source, WC));
+    take(dev_alloc(&h->key_shape, WC * 2));
+    take(dev_alloc(&h->key_point, WC * 3));
+    take(dev_alloc(&h->key_count, W));
+    take(dev_alloc(&h->has_history, WC));
   }
   take(dev_alloc(&h->v, Wn));
   take(dev_alloc(&h->gamma, WC * 3));
@@ -272,6 +282,8 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     err = cudaMemcpy(h->body_dof_count, bcount.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemset(h->guess_flag, 0, sizeof(int32_t));
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_prev, 0, sizeof(double) * WC * 3);
+  if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_last, 0, sizeof(double) * WC * 3);
+  if (err == cudaSuccess && cand) err = cudaMemset(h->key_count, 0, sizeof(int32_t) * W);
   if (err == cudaSuccess) err = cudaMemset(h->iters, 0, sizeof(int32_t) * W);
   if (err == cudaSuccess) {
     std::vector<int32_t> idx(W);
@@ -317,9 +329,30 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   po.truncated_count = h->truncated;
   po.dynamics_factor = h->factor;
   po.vc_star = h->vc_star;
+  po.contact_source = h->source;
   int32_t st = sapb_free_motion_contacts(&h->model, &io->in, &h->opts.prepare, &po, h->prep_ws, h->prep_ws_bytes,
                                          stream);
   if (st != SAPB_OK) return st;
+  if (cand) {  // the last solve's impulses carried to this step's slots by contact identity
+    sapb_contact_history hist;
+    memset(&hist, 0, sizeof(hist));
+    hist.num_envs = h->W;
+    hist.max_contacts = h->C;
+    hist.num_flat = io->in.contact_capacity;
+    hist.contact_count = h->count;
+    hist.contact_source = h->source;
+    hist.flat_shape0 = io->in.contact_shape0;
+    hist.flat_shape1 = io->in.contact_shape1;
+    hist.flat_point1 = io->in.contact_point1;
+    hist.key_shape = h->key_shape;
+    hist.key_point = h->key_point;
+    hist.key_count = h->key_count;
+    hist.gamma_prev = h->gamma_last;
+    hist.gamma_hist = h->gamma_prev;
+    hist.has_history = h->has_history;
+    st = sapb_contact_history_update(&hist, stream);
+    if (st != SAPB_OK) return st;
+  }
   // contact solve (sim/solver_sap.py:1434-1460), warm start from the last
   // solution once a step has run
   sapb_contact_problem p;
@@ -391,7 +424,7 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   err = cudaMemcpyAsync(io->joint_qd_out, h->v, sizeof(double) * (size_t)h->W * h->n, cudaMemcpyDeviceToDevice, s);
   if (err == cudaSuccess) err = cudaMemsetAsync(h->guess_flag, 1, sizeof(int32_t), s);  // nonzero: warm start on
   if (err == cudaSuccess && cand)
-    err = cudaMemcpyAsync(h->gamma_prev, h->gamma, sizeof(double) * (size_t)h->W * h->C * 3, cudaMemcpyDeviceToDevice,
+    err = cudaMemcpyAsync(h->gamma_last, h->gamma, sizeof(double) * (size_t)h->W * h->C * 3, cudaMemcpyDeviceToDevice,
                           s);
   if (err != cudaSuccess) {
     set_last_error("sapb_step: %s", cudaGetErrorString(err));

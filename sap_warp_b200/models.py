@@ -331,6 +331,100 @@ def rollout_scene(kind: str, worlds: int, seed: int, device, *, contacts=(8, 32)
     return model, state, control, contacts_to_torch(con, device), con
 
 
+def _quat_from_z(n: np.ndarray) -> np.ndarray:
+    """Unit quaternions (xyzw) rotating +z onto the unit vectors n (N, 3)."""
+    z = np.array([0.0, 0.0, 1.0])
+    axis = np.cross(z, n)
+    s = np.linalg.norm(axis, axis=1)
+    c = n[:, 2]
+    ang = np.arctan2(s, c)
+    u = np.where(s[:, None] > 1e-15, axis / np.maximum(s, 1e-300)[:, None], np.array([1.0, 0.0, 0.0]))
+    return np.concatenate([u * np.sin(0.5 * ang)[:, None], np.cos(0.5 * ang)[:, None]], axis=1)
+
+
+def site_scene(kind: str, worlds: int, seed: int, device, *, sites: int = 32, contacts=(8, 32),
+               radius: float = 0.01, qd_std: float = 0.5, phi0_range=(-2.0e-3, 0.0), lift_range=(5.0e-3, 3.0e-2),
+               mu_range=(0.3, 1.0), stiffness: float = 1.0e5, tau_d: float = 0.01, tilt: float = 0.1):
+    """A batch of `kind` worlds whose contacts come from collision shapes and
+    are regenerated from the pose every step: `sites` spheres of radius
+    `radius` on the distal half of each world's bodies, each over its own
+    static ground patch (a plane through a ground point, normal ~ +z tilted
+    by `tilt`), a sphere and its patch sharing a collision group so that
+    only those pairs are tested.  At the start C ~ U{contacts} sites per
+    world touch their patch (phi0 ~ U[phi0_range]) and the others hover
+    U[lift_range] above theirs; as the bodies move, contacts vanish and
+    appear.  Materials as rollout_scene's (pair stiffness, dissipation).
+    Returns (model, state, control, shapes (collision.ShapeSet), host)."""
+    from ._abi import SAPB_SHAPE_PLANE, SAPB_SHAPE_SPHERE
+    from .collision import ShapeSet
+    from .runtime import SapContacts, SapControl, SapState
+    from .solver import SapContactJacobian
+
+    rng = np.random.default_rng(seed)
+    tpl = world_template(kind, rng)
+    g = replicate(tpl, worlds, rng, mu_range=mu_range, stiffness=stiffness, tau_d=0.5 * tau_d)
+    q = random_joint_q(tpl, rng, worlds)
+    n, B = tpl["dofs_per_world"], tpl["bodies_per_world"]
+    E, K = worlds, int(sites)
+    # shapes: per world K spheres (on bodies), then K static patches
+    S = E * 2 * K
+    shape_body = np.full(S, -1, np.int32)
+    bodies = rng.integers(B // 2, B, size=(E, K))
+    gidx = (np.arange(E)[:, None] * B + bodies)
+    sph = (np.arange(E)[:, None] * 2 * K + np.arange(K)[None, :])
+    shape_body[sph.reshape(-1)] = gidx.reshape(-1)
+    g["shape_body"] = shape_body
+    g["shape_material_mu"] = np.ones(S)
+    g["shape_material_mu"][sph.reshape(-1)] = rng.uniform(*mu_range, E * K)
+    g["shape_material_ke"] = np.full(S, 2.0 * stiffness)
+    g["shape_material_tau"] = np.full(S, 0.5 * tau_d)
+    g["counts"] = dict(g["counts"], shapes=S)
+    model = to_model(tpl, g, q, device)
+    qd = rng.normal(scale=qd_std, size=(worlds, n))
+    state = SapState(joint_q=torch.as_tensor(q.reshape(-1), dtype=torch.float64, device=device),
+                     joint_qd=torch.as_tensor(qd.reshape(-1), dtype=torch.float64, device=device),
+                     body_q=model.body_q.clone(),
+                     body_f=torch.zeros(model.body_count, 6, dtype=torch.float64, device=device))
+    control = SapControl(joint_f=torch.zeros(model.joint_dof_count, dtype=torch.float64, device=device))
+    cj = SapContactJacobian(model, max_rigid_contact=1, fallback_tau_d=0.0)
+    cj.compute(state, SapContacts(), control=control, dt=2.0e-3)
+    bq = cj.body_q_sap.reshape(worlds, B, 7).cpu().numpy()
+    counts = rng.integers(contacts[0], contacts[1] + 1, size=worlds)
+    # sites: a point on the body (within 5 cm of its origin), its patch
+    # through the point moved by phi along the patch normal
+    r_local = rng.normal(size=(E, K, 3))
+    r_local *= (rng.uniform(0.0, 0.05, size=(E, K)) / np.linalg.norm(r_local, axis=2))[..., None]
+    bp = bq[np.arange(E)[:, None], bodies]
+    bquat = bp[..., 3:] / np.linalg.norm(bp[..., 3:], axis=-1, keepdims=True)
+    x1 = bp[..., :3] + _qrot(bquat, r_local)
+    nrm = np.array([0.0, 0.0, 1.0]) + rng.normal(scale=tilt, size=(E, K, 3))
+    nrm /= np.linalg.norm(nrm, axis=2, keepdims=True)
+    touching = np.arange(K)[None, :] < counts[:, None]
+    phi = np.where(touching, rng.uniform(*phi0_range, size=(E, K)), rng.uniform(*lift_range, size=(E, K)))
+    x0 = x1 - phi[..., None] * nrm
+    # sphere centre = the site point plus the radius along the normal, in the body frame
+    conj = bquat * np.array([-1.0, -1.0, -1.0, 1.0])
+    centre_local = r_local + _qrot(conj, radius * nrm)
+    X = np.zeros((S, 7))
+    scale = np.zeros((S, 3))
+    types = np.full(S, SAPB_SHAPE_PLANE, np.int32)
+    groups = np.zeros(S, np.int32)
+    for w in range(E):
+        base = w * 2 * K
+        X[base:base + K, :3] = centre_local[w]
+        X[base:base + K, 6] = 1.0
+        X[base + K:base + 2 * K, :3] = x0[w]
+        X[base + K:base + 2 * K, 3:] = _quat_from_z(nrm[w])
+        scale[base:base + K, 0] = radius
+        types[base:base + K] = SAPB_SHAPE_SPHERE
+        groups[base:base + K] = 1 + np.arange(K)
+        groups[base + K:base + 2 * K] = 1 + np.arange(K)
+    shapes = ShapeSet(num_worlds=E, shapes_per_world=2 * K, num_global_shapes=0, shape_type=types,
+                      shape_scale=scale, shape_X_bs=X, shape_body=shape_body, shape_collision_group=groups)
+    host = dict(tpl=tpl, g=g, q=q, qd=qd, counts=counts, phi=phi, sites=K)
+    return model, state, control, shapes, host
+
+
 def _quat_z(yaw: np.ndarray) -> np.ndarray:
     """Quaternions (x, y, z, w) of rotations about +z."""
     z = np.zeros_like(yaw)

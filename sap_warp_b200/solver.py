@@ -365,6 +365,14 @@ class SapContactJacobian:
             self.contact_env_vc_star = torch.zeros(v.W, self.max_rigid_contact, 3, dtype=F64, device=v.device)
             self.outputs.vc_star = _ptr(self.contact_env_vc_star)
 
+    def keep_contact_source(self) -> None:
+        """Also write the flat contact index of each slot (contact_env_source,
+        [W][C], -1 past a world's count): the key of the contact history."""
+        if getattr(self, "contact_env_source", None) is None:
+            v = self.view
+            self.contact_env_source = torch.full((v.W, self.max_rigid_contact), -1, dtype=I32, device=v.device)
+            self.outputs.contact_source = _ptr(self.contact_env_source)
+
     def set_dt(self, dt) -> None:
         """Per-world time step (scalar or [W] tensor), sim/solver_sap.py:975-992."""
         if isinstance(dt, torch.Tensor):
@@ -779,19 +787,28 @@ class SolverSAP:
                  static_substep: bool = False, static_substep_iterations: int = 8,
                  static_substep_line_search_iterations: int = 6, position_integration: str | None = None,
                  hessian_precision: str | None = None, warm_start: str = "previous_velocity",
-                 learned_warm_start=None, tree_blocked: bool | None = None, work_order: str = "previous_iterations",
-                 autotune: bool | str | os.PathLike | None = None):
+                 learned_warm_start=None, learned_candidates: str = "new_contacts", tree_blocked: bool | None = None,
+                 work_order: str = "previous_iterations", autotune: bool | str | os.PathLike | None = None):
         """Keyword arguments of the reference's SolverSAP (sim/solver_sap.py:
         749-791) plus: hessian_precision ("fp64" / "fp32": J^T G J assembly and
         factorization precision; the gradient, cost, line search and
         convergence test stay FP64); warm_start, one of
           "previous_velocity"  the reference's: start from the last solution;
           "previous_impulses"  also try v* + A^-1 J^T gamma_prev;
-          "learned"            also try v* + A^-1 J^T gamma_prev and
-                               v* + A^-1 J^T gamma0, gamma0 from the
-                               per-contact network (learned_warm_start: a
-                               LearnedWarmStart, a weights path, or None for
-                               the packaged weights);
+          "learned"            also try starts from the per-contact network
+                               (learned_warm_start: a LearnedWarmStart, a
+                               weights path, or None for the packaged
+                               weights); learned_candidates "new_contacts"
+                               (default): one start v* + A^-1 J^T gamma0 with
+                               gamma0 the carried impulse where the contact
+                               existed last step and the network's where it
+                               is new (tiles without a new contact skip the
+                               network); "all_contacts": two starts, the
+                               network's gamma0 on every contact and the
+                               carried impulses;
+        previous impulses are carried to this step's contact slots by
+        contact identity (shape pair and witness point), so slots may shift
+        as contacts appear and vanish;
         the lowest-cost start among the previous-velocity one and the
         candidates is taken, and Newton always runs to the same tolerance;
         work_order ("previous_iterations", the default, or "index"): the
@@ -893,6 +910,9 @@ class SolverSAP:
         if self.contact_solve.tree_blocked and self.warm_start == "learned":
             raise NotImplementedError("the tree-blocked layout takes the previous-velocity or previous-impulses "
                                       "warm start")
+        self.learned_candidates = str(learned_candidates).strip().lower().replace("-", "_")
+        if self.learned_candidates not in ("new_contacts", "all_contacts"):
+            raise ValueError(f"learned_candidates must be 'new_contacts' or 'all_contacts', got {learned_candidates!r}.")
         self.learned_warm_start = None
         if self.warm_start == "learned":
             from .warmstart import DEFAULT_WEIGHTS, LearnedWarmStart
@@ -906,8 +926,18 @@ class SolverSAP:
         # impulses (evaluated last: it is the usual winner, and the last
         # candidate's evaluation seeds the first Newton iteration)
         self._gamma_cand = torch.zeros(2, view.W, max(C, 1), 3, dtype=F64, device=dev)
+        # [1] holds the previous step's impulses carried to this step's slots
+        # by contact identity (sapb_contact_history_update), from the last
+        # solve's impulses by its own slots (_gamma_last)
         self._gamma_prev = self._gamma_cand[1]
+        self._gamma_last = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
+        if self.warm_start != "previous_velocity":
+            self._hist_key_shape = torch.zeros(view.W, max(C, 1), 2, dtype=I32, device=dev)
+            self._hist_key_point = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
+            self._hist_key_count = torch.zeros(view.W, dtype=I32, device=dev)
+            self.has_history = torch.zeros(view.W, max(C, 1), dtype=I32, device=dev)
+            self.contact_jacobian.keep_contact_source()
         if self.learned_warm_start is not None:
             self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
         if self.warm_start != "previous_velocity" and not self.contact_solve.tree_blocked:
@@ -1086,6 +1116,9 @@ class SolverSAP:
         self._v_guess_active.zero_()
         if hasattr(self, "_gamma_cand"):
             self._gamma_cand.zero_()
+            self._gamma_last.zero_()
+        if hasattr(self, "_hist_key_count"):
+            self._hist_key_count.zero_()
         if hasattr(self, "_world_order"):
             torch.arange(self.view.W, dtype=I32, device=self.view.device, out=self._world_order)
         self.last_contacts = None
@@ -1122,6 +1155,8 @@ class SolverSAP:
         v0 = self.contact_jacobian._qd
         mark("warm_start")
         gamma0 = None
+        if self.warm_start != "previous_velocity":
+            self._carry_impulses(cr)
         if self.warm_start == "previous_impulses":
             gamma0 = self._gamma_prev
         elif self.warm_start == "learned":
@@ -1134,8 +1169,9 @@ class SolverSAP:
                 jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff,
                 mu=cr.contact_env_mu, stiffness=cr.contact_env_stiffness, tau_d=cr.contact_env_tau_d,
                 v_star=self.contact_jacobian.v_star, v0=self.contact_jacobian.v_star,
-                dt=self.contact_jacobian.dt_world)
-            gamma0 = self._gamma_cand
+                dt=self.contact_jacobian.dt_world,
+                has_history=self.has_history if self.learned_candidates == "new_contacts" else None)
+            gamma0 = self._gamma_cand[0:1] if self.learned_candidates == "new_contacts" else self._gamma_cand
         mark("contact_solve")
         sr = self.contact_solve.solve(
             cr, solve_state, solve_control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
@@ -1173,7 +1209,7 @@ class SolverSAP:
         mark(None)
         self._v_guess_active.fill_(1)  # warm start from this step's solution (sim/solver_sap.py:1441-1451)
         if self.warm_start != "previous_velocity":
-            self._gamma_prev.copy_(sr.contact_gamma)
+            self._gamma_last.copy_(sr.contact_gamma)
         self.last_contact_jacobian_result = cr
         self.last_contact_solve_result = sr
         self.last_solve_iterations = -1
@@ -1183,6 +1219,25 @@ class SolverSAP:
             self.sim_time += float(dt)
         self.frame_id += 1
         return state_out
+
+    def _carry_impulses(self, cr: SapContactJacobianResult) -> None:
+        """The last solve's impulses carried to this step's contact slots by
+        contact identity (shape pair + shape1 witness point), into
+        _gamma_prev; has_history marks the slots that found their contact."""
+        cj = self.contact_jacobian
+        inp = cj._inputs
+        H = _abi.ContactHistory()
+        H.num_envs, H.max_contacts = self.view.W, self.max_rigid_contact
+        H.num_flat = int(inp.contact_capacity)
+        H.contact_count, H.contact_source = _ptr(cr.contact_env_count), _ptr(cj.contact_env_source)
+        H.flat_shape0, H.flat_shape1, H.flat_point1 = inp.contact_shape0, inp.contact_shape1, inp.contact_point1
+        H.key_shape, H.key_point = _ptr(self._hist_key_shape), _ptr(self._hist_key_point)
+        H.key_count = _ptr(self._hist_key_count)
+        H.gamma_prev, H.gamma_hist, H.has_history = _ptr(self._gamma_last), _ptr(self._gamma_prev), _ptr(
+            self.has_history)
+        check(load().sapb_contact_history_update(
+            ctypes.byref(H), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)),
+            "sapb_contact_history_update")
 
     def _boundary_in(self, state_in: SapState, state_out: SapState, control: SapControl | None):
         """Public-order inputs -> SAP order (sim/solver_sap.py:1198-1261):

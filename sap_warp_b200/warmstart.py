@@ -160,13 +160,23 @@ class WarmStartMLP:
         check(load().sapb_mlp_pack(self.params.data_ptr(), self.packed.data_ptr(), self.bias.data_ptr(),
                                    _stream(self.device)), "sapb_mlp_pack")
 
-    def forward(self, x: torch.Tensor, y: torch.Tensor | None = None) -> torch.Tensor:
+    def forward(self, x: torch.Tensor, y: torch.Tensor | None = None,
+                tile_active: torch.Tensor | None = None) -> torch.Tensor:
+        """y = MLP(x); with tile_active (int32 per 128-row tile), only the
+        tiles whose flag is nonzero are computed (the others' rows of y are
+        left as they are)."""
         rows = x.shape[0]
         xp = _dev_ptr(x, I16, rows * IN_PAD, "x")
         if y is None:
             y = torch.empty(rows, OUT, dtype=F32, device=self.device)
-        check(load().sapb_mlp_forward(self.packed.data_ptr(), self.bias.data_ptr(), xp, rows,
-                                      _dev_ptr(y, F32, rows * OUT, "y"), _stream(self.device)), "sapb_mlp_forward")
+        yp = _dev_ptr(y, F32, rows * OUT, "y")
+        if tile_active is None:
+            check(load().sapb_mlp_forward(self.packed.data_ptr(), self.bias.data_ptr(), xp, rows, yp,
+                                          _stream(self.device)), "sapb_mlp_forward")
+        else:
+            tp = _dev_ptr(tile_active, torch.int32, (rows + 127) // 128, "tile_active")
+            check(load().sapb_mlp_forward_tiles(self.packed.data_ptr(), self.bias.data_ptr(), xp, rows, yp, tp,
+                                                _stream(self.device)), "sapb_mlp_forward_tiles")
         return y
 
     def forward_train(self, x: torch.Tensor, target: torch.Tensor, buf: TrainBuffers,
@@ -238,15 +248,20 @@ class LearnedWarmStart:
             self._bufs[key] = dict(
                 x=torch.zeros(slots, IN_PAD, dtype=I16, device=self.device),
                 y=torch.zeros(slots, OUT, dtype=F32, device=self.device),
+                tiles=torch.zeros((slots + 127) // 128, dtype=torch.int32, device=self.device),
                 gamma0=torch.zeros(num_envs, max_contacts, 3, dtype=F64, device=self.device))
         return self._bufs[key]
 
     def predict(self, *, num_envs: int, dof_per_env: int, max_contacts: int, normal_up: torch.Tensor | None = None,
                 gamma_prev: torch.Tensor | None = None, vc_star: torch.Tensor | None = None,
-                out: torch.Tensor | None = None, **arrays) -> torch.Tensor:
+                out: torch.Tensor | None = None, has_history: torch.Tensor | None = None,
+                **arrays) -> torch.Tensor:
         """gamma0 (E, C, 3) FP64 on the device (into `out` if given):
-        features -> MLP -> impulses, three launches on the current stream, no
-        host sync, no allocation after the first call for a shape."""
+        features -> MLP -> impulses on the current stream, no host sync, no
+        allocation after the first call for a shape.  With has_history
+        ((E, C) int32: the slot's contact carries gamma_prev from the
+        previous step), those slots keep gamma_prev and the network predicts
+        only the new contacts (tiles of 128 rows without one are skipped)."""
         E, C = num_envs, max_contacts
         b = self.buffers(E, C)
         g_out = b["gamma0"] if out is None else out
@@ -257,8 +272,14 @@ class LearnedWarmStart:
         vc = 0 if vc_star is None else _dev_ptr(vc_star, F64, E * C * 3, "vc_star")
         check(lib.sapb_warmstart_features(ctypes.byref(P), nu, gp, vc, ctypes.byref(self.norm_struct),
                                           self.tau_fallback, b["x"].data_ptr(), None, s), "sapb_warmstart_features")
-        self.mlp.forward(b["x"], b["y"])
-        check(lib.sapb_warmstart_impulses(ctypes.byref(P), b["y"].data_ptr(), gp, ctypes.byref(self.norm_struct),
+        hh = 0 if has_history is None else _dev_ptr(has_history, torch.int32, E * C, "has_history")
+        if has_history is None:
+            self.mlp.forward(b["x"], b["y"])
+        else:
+            check(lib.sapb_warmstart_active_tiles(ctypes.byref(P), hh, b["tiles"].data_ptr(), s),
+                  "sapb_warmstart_active_tiles")
+            self.mlp.forward(b["x"], b["y"], tile_active=b["tiles"])
+        check(lib.sapb_warmstart_impulses(ctypes.byref(P), b["y"].data_ptr(), gp, hh, ctypes.byref(self.norm_struct),
                                           ctypes.byref(self.solve_options), _dev_ptr(g_out, F64, E * C * 3, "out"), s),
               "sapb_warmstart_impulses")
         return g_out
@@ -373,6 +394,50 @@ def rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, every:
                 raws.append(raw[live])
                 us.append(u[live].to(F32))
             gamma_prev.copy_(solver.contact_solve.contact_gamma)
+            state, other = other, state
+    return torch.cat(raws), torch.cat(us)
+
+
+def site_rollout_dataset(kind: str, worlds: int, seeds, steps: int, device, *, hessian_precision: str = "fp64",
+                         contact_preset_variant: str = "drake"):
+    """(raw inputs (N, 12), targets u = w_eff * y (N, 3)) of the NEW contacts
+    (no contact with the same identity at the previous step) along SolverSAP
+    trajectories of models.site_scene, whose contacts are regenerated from
+    the pose every step: the rows the learned start's network predicts when
+    it serves new contacts only (their gamma_prev input is zero).  Targets:
+    the unprojected impulses y at the step's converged velocity."""
+    from . import models
+    from .collision import ContactGenerator
+    from .runtime import SapState
+    from .solver import SolverSAP
+
+    raws, us = [], []
+    for seed in seeds:
+        model, state, control, shapes, _ = models.site_scene(kind, worlds, seed, device)
+        solver = SolverSAP(model, max_rigid_contact=32, hessian_precision=hessian_precision,
+                           contact_preset_variant=contact_preset_variant, warm_start="previous_impulses")
+        gen = ContactGenerator(shapes, solver.view, capacity=worlds * 32, gap=1.0e-3)
+        other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(),
+                         body_q=state.body_q.clone(), body_f=state.body_f.clone())
+        W, n, C = solver.view.W, solver.view.n, solver.max_rigid_contact
+        normal_up = torch.zeros(W, C, dtype=F64, device=device)
+        for k in range(steps):
+            solver.step(state, other, control, gen.generate(state.joint_q), 2.0e-3)
+            cr = solver.last_contact_jacobian_result
+            normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
+            arrays = dict(contact_count=cr.contact_env_count, dynamics_matrix=cr.dynamics_matrix_env,
+                          jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff,
+                          mu=cr.contact_env_mu, stiffness=cr.contact_env_stiffness, tau_d=cr.contact_env_tau_d,
+                          v_star=solver.contact_jacobian.v_star, v0=solver.contact_jacobian.v_star,
+                          dt=solver.contact_jacobian.dt_world)
+            raw = raw_features(arrays, W, n, C, normal_up=normal_up)
+            cnt = cr.contact_env_count.clamp(max=C)
+            live = torch.arange(C, device=device)[None, :] < cnt[:, None]
+            new = (live & (solver.has_history == 0)).reshape(-1)
+            u = unprojected_targets(arrays, solver.contact_solve.v_flat, W, n, C,
+                                    solver.contact_solve.contact_beta, solver.contact_solve.contact_sigma)
+            raws.append(raw[new])
+            us.append(u[new].to(F32))
             state, other = other, state
     return torch.cat(raws), torch.cat(us)
 

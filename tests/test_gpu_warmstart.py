@@ -115,7 +115,7 @@ def test_unprojected_targets_project_to_the_solution(cuda_device):
     import ctypes
     y = u.to(torch.float32).contiguous()
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    assert load().sapb_warmstart_impulses(ctypes.byref(P), y.data_ptr(), None, ctypes.byref(ws.norm_struct),
+    assert load().sapb_warmstart_impulses(ctypes.byref(P), y.data_ptr(), None, None, ctypes.byref(ws.norm_struct),
                                           ctypes.byref(ws.solve_options), b["gamma0"].data_ptr(), s) == 0
     g = b["gamma0"].cpu().numpy()
     want = sol["contact_gamma"][:, :C]
@@ -166,42 +166,52 @@ def test_exact_impulses_start_at_the_solution(cuda_device, oracle):
         assert got["converged"].all()
 
 
-def test_learned_start_reduces_newton_iterations(cuda_device):
-    """Ablation along trajectories: a network trained in-test on
-    solver-generated humanoid rollouts, used as SolverSAP's learned warm start
-    (previous impulses and the network's correction tried against the
-    previous velocity), cuts the mean Newton iterations of a held-out rollout
-    against the reference's previous-velocity start, every world converging
-    at the same tolerance; the network's own candidate is the chosen start in
-    part of the worlds."""
+def test_learned_start_against_previous_impulses(cuda_device):
+    """Ablation on rollouts whose contacts are regenerated from the pose every
+    step (models.site_scene: contacts appear and vanish).  A network trained
+    in-test on the new contacts of solver rollouts serves SolverSAP's learned
+    start (carried impulses for contacts that existed last step, the
+    network's prediction for new ones).  Against the same method without
+    the network (previous impulses, new contacts starting at zero) it must
+    not cost Newton iterations, and both cut the reference's
+    previous-velocity start's iterations; every world converges at the same
+    tolerance and the network predicts some contacts.  (Measured gain over
+    previous impulses: under 1 %; the carried impulses give the reduction.)"""
     from sap_warp_b200 import models
+    from sap_warp_b200.collision import ContactGenerator
     from sap_warp_b200.runtime import SapState
     from sap_warp_b200.solver import SolverSAP
+    from sap_warp_b200.warmstart import site_rollout_dataset
 
-    raw, u = rollout_dataset("humanoid", 1024, (400, 401), 40, cuda_device)
-    res = residual_targets(raw, u)
-    norm = FeatureNorm.from_data(raw.cpu().numpy(), res.cpu().numpy())
+    raw, u = site_rollout_dataset("humanoid", 1024, (400, 401), 30, cuda_device)
+    assert raw.shape[0] > 500, raw.shape
+    norm = FeatureNorm.from_data(raw.cpu().numpy(), residual_targets(raw, u).cpu().numpy())
     mlp = WarmStartMLP(cuda_device, seed=0)
-    log = train(mlp, raw, u, norm, steps=2000, batch=8192, lr=2e-3, log_every=500)
+    log = train(mlp, raw, u, norm, steps=1500, batch=4096, lr=2e-3, log_every=500)
     assert log[-1][1] < 0.8 * log[0][1], log
     ws = LearnedWarmStart(mlp, norm)
     stats = {}
-    for mode in ("previous_velocity", "learned"):
-        model, state, control, con, _ = models.rollout_scene("humanoid", 1024, 402, cuda_device)
+    for mode in ("previous_velocity", "previous_impulses", "learned"):
+        model, state, control, shapes, _ = models.site_scene("humanoid", 1024, 402, cuda_device)
         solver = SolverSAP(model, max_rigid_contact=32, hessian_precision="fp32", warm_start=mode,
                            learned_warm_start=ws if mode == "learned" else None)
+        gen = ContactGenerator(shapes, solver.view, capacity=1024 * 32, gap=1.0e-3)
         other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
                          body_f=state.body_f.clone())
-        its, chosen = [], []
+        its, predicted = [], 0
         for k in range(30):
-            solver.step(state, other, control, con, 2.0e-3)
+            solver.step(state, other, control, gen.generate(state.joint_q), 2.0e-3)
             cs = solver.contact_solve
             assert bool(cs.converged_env.all()), (mode, k)
             its.append(cs.newton_iterations_env.double().mean().item())
-            chosen.append(torch.bincount(cs.warm_start_accepted_env.long(), minlength=3).cpu().numpy())
+            if mode == "learned":
+                cnt = solver.contact_jacobian.contact_env_count.clamp(max=32)
+                live = torch.arange(32, device=cuda_device)[None, :] < cnt[:, None]
+                predicted += int((live & (solver.has_history == 0)).sum())
             state, other = other, state
-        stats[mode] = (float(np.mean(its[3:])), np.sum(chosen, 0))
+        stats[mode] = (float(np.mean(its[3:])), predicted)
         assert torch.isfinite(state.joint_q).all()
     print(stats)
-    assert stats["learned"][0] < 0.8 * stats["previous_velocity"][0], stats
-    assert stats["learned"][1][1] > 0, stats  # the network's candidate is chosen in some worlds
+    assert stats["learned"][1] > 0, stats  # the network served new contacts
+    assert stats["previous_impulses"][0] < 0.8 * stats["previous_velocity"][0], stats
+    assert stats["learned"][0] <= 1.02 * stats["previous_impulses"][0], stats
