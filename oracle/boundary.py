@@ -19,7 +19,7 @@ from __future__ import annotations
 
 import numpy as np
 
-FREE, DISTANCE, PRISMATIC, REVOLUTE, BALL = 4, 5, 0, 1, 2
+FREE, DISTANCE, PRISMATIC, REVOLUTE, BALL, D6 = 4, 5, 0, 1, 2, 6
 
 
 def qrot(q, v):
@@ -129,6 +129,18 @@ def eval_fk(g: dict, joint_q, qd_pub):
             elif jt in (FREE, DISTANCE):
                 X_j = (np.asarray(joint_q[qs:qs + 3], dtype=np.float64), np.asarray(joint_q[qs + 3:qs + 7]))
                 vj, wj = np.asarray(qd_pub[ds:ds + 3]), np.asarray(qd_pub[ds + 3:ds + 6])
+            elif jt == D6:  # sim/sap_kinematics.py:170-215
+                from oracle.free_motion import d6_transform_and_axes
+
+                lin, ang = int(g["joint_dof_dim"][i][0]), int(g["joint_dof_dim"][i][1])
+                p_, r_, ax = d6_transform_and_axes(g["joint_axis"][ds:ds + lin + ang],
+                                                   np.asarray(joint_q[qs:qs + lin + ang], dtype=np.float64)[None],
+                                                   lin, ang)
+                X_j = (p_[0], r_[0])
+                for k in range(lin):
+                    vj = vj + qd_pub[ds + k] * g["joint_axis"][ds + k]
+                for k in range(ang):
+                    wj = wj + qd_pub[ds + lin + k] * ax[0, k]
             X_wc = tmul(tmul(X_wpj, X_j), tinv(X_cj))
             body_q[child, :3], body_q[child, 3:] = X_wc
             body_qd[child, :3] = v_wpj + qrot(X_wpj[1], vj)

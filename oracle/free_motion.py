@@ -107,6 +107,58 @@ def mobilizer_accel_bias_to_body(R_WF_q, p_MoBo_F, V_FM_F):
     return np.concatenate([qrotate(R_WF_q, sh[..., :3]), qrotate(R_WF_q, sh[..., 3:])], -1)
 
 
+def quat_from_cols(c0, c1, c2):
+    """_quatd_from_matrix_cols (sim/sap_helpers.py:608-655), one rotation."""
+    r00, r10, r20 = c0
+    r01, r11, r21 = c1
+    r02, r12, r22 = c2
+    tr = r00 + r11 + r22
+    if tr > 0.0:
+        s = np.sqrt(tr + 1.0) * 2.0
+        return np.array([(r21 - r12) / s, (r02 - r20) / s, (r10 - r01) / s, 0.25 * s])
+    if r00 > r11 and r00 > r22:
+        s = np.sqrt(1.0 + r00 - r11 - r22) * 2.0
+        return np.array([0.25 * s, (r01 + r10) / s, (r02 + r20) / s, (r21 - r12) / s])
+    if r11 > r22:
+        s = np.sqrt(1.0 + r11 - r00 - r22) * 2.0
+        return np.array([(r01 + r10) / s, 0.25 * s, (r12 + r21) / s, (r02 - r20) / s])
+    s = np.sqrt(1.0 + r22 - r00 - r11) * 2.0
+    return np.array([(r02 + r20) / s, (r12 + r21) / s, 0.25 * s, (r10 - r01) / s])
+
+
+def d6_transform_and_axes(axes, q, lin, ang):
+    """D6 across-mobilizer transform and angular DOF axes per world
+    (sim/sap_helpers.py:1109-1161 rotations, :1204-1241 X_FM, :1247-1286
+    angular axes).  axes (lin + ang, 3) in F; q (E, lin + ang).  Returns
+    (pos (E, 3), rot (E, 4), angular axes (E, ang, 3))."""
+    E = q.shape[0]
+    pos = np.zeros((E, 3))
+    for k in range(lin):
+        pos = pos + axes[k] * q[:, k:k + 1]
+    rot = np.tile([0.0, 0.0, 0.0, 1.0], (E, 1))
+    out = np.zeros((E, max(ang, 1), 3))
+    if ang == 1:
+        out[:, 0] = axes[lin]
+        rot = q_axis_angle(axes[lin], q[:, lin])
+    elif ang in (2, 3):
+        c0, c1 = axes[lin], axes[lin + 1]
+        c2 = axes[lin + 2] if ang == 3 else np.cross(c0, c1)
+        off = np.broadcast_to(quat_from_cols(c0, c1, c2), (E, 4))
+        l0 = qrotate(off, np.broadcast_to([1.0, 0.0, 0.0], (E, 3)))
+        l1 = qrotate(off, np.broadcast_to([0.0, 1.0, 0.0], (E, 3)))
+        l2 = qrotate(off, np.broadcast_to([0.0, 0.0, 1.0], (E, 3)))
+        q0 = q_axis_angle(l0, q[:, lin])
+        a1 = qrotate(q0, l1)
+        q10 = qmul(q_axis_angle(a1, q[:, lin + 1]), q0)
+        out[:, 0], out[:, 1] = l0, a1
+        rot = q10
+        if ang == 3:
+            a2 = qrotate(q10, l2)
+            out[:, 2] = a2
+            rot = qmul(q_axis_angle(a2, q[:, lin + 2]), q10)
+    return pos, rot, out
+
+
 def spatial_inertia_body_origin(R, Icom, m, c_body):
     """(sim/sap_helpers.py:1027-1062) 6x6 [[I_Bo, m[c]x], [-m[c]x, m I]]."""
     c = np.einsum("...ij,...j->...i", R, c_body)
@@ -161,6 +213,10 @@ def free_motion(m: Model, joint_q, joint_qd, joint_f, body_f, dt):
         elif jt in (JOINT_FREE, JOINT_DISTANCE):
             fm_p = joint_q[:, qs:qs + 3].copy()
             fm_q = joint_q[:, qs + 3:qs + 7].copy()
+        elif jt == JOINT_D6:
+            lin, ang = int(m.joint_dof_dim[j, 0]), int(m.joint_dof_dim[j, 1])
+            fm_p, fm_q, d6_axes = d6_transform_and_axes(m.joint_axis[ds:ds + lin + ang], joint_q[:, qs:qs + lin + ang],
+                                                        lin, ang)
         elif jt != JOINT_FIXED:
             raise NotImplementedError(f"joint type {jt}")
         wm_p, wm_q = tcompose(wf_p, wf_q, fm_p, fm_q)
@@ -190,6 +246,20 @@ def free_motion(m: Model, joint_q, joint_qd, joint_f, body_f, dt):
             eye = np.eye(6)
             Sj = [mobilizer_velocity_to_body(R_WF, p_MoBo_F, np.broadcast_to(eye[k], (E, 6))) for k in range(6)]
             V_FM = joint_qd[:, ds:ds + 6].copy()
+        elif jt == JOINT_D6:
+            # sim/sap_helpers.py:1387-1431: translation columns, then the
+            # angular axes at the current angles; V_FM their combination
+            Sj = []
+            V_FM = np.zeros((E, 6))
+            for k in range(lin):
+                a = np.broadcast_to(m.joint_axis[ds + k], (E, 3))
+                col = np.concatenate([np.zeros((E, 3)), a], -1)
+                Sj.append(mobilizer_velocity_to_body(R_WF, p_MoBo_F, col))
+                V_FM = V_FM + col * joint_qd[:, ds + k:ds + k + 1]
+            for k in range(ang):
+                col = np.concatenate([d6_axes[:, k], np.zeros((E, 3))], -1)
+                Sj.append(mobilizer_velocity_to_body(R_WF, p_MoBo_F, col))
+                V_FM = V_FM + col * joint_qd[:, ds + lin + k:ds + lin + k + 1]
         else:
             Sj = []
             V_FM = zero
@@ -425,6 +495,9 @@ def integrate(m: Model, joint_q, v_prev, v_new, dt, mode="sap_euler"):
                 r = q_axis_angle(axis, ang)
                 qn = qnormalize(qmul(r, qq))
                 q[:, qs + o:qs + o + 4] = np.where((ang > 1e-12)[:, None], qn, qq)
+        elif jt == JOINT_D6:  # scalar coordinates, one per axis (sim/solver_sap.py:379-383, 504-510)
+            dim = int(m.joint_dof_dim[j, 0] + m.joint_dof_dim[j, 1])
+            q[:, qs:qs + dim] = joint_q[:, qs:qs + dim] + h * vel[:, ds:ds + dim]
         elif jt == JOINT_FIXED:
             pass
     return q

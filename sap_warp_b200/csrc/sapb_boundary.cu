@@ -148,6 +148,12 @@ __global__ void eval_fk_kernel(const BoundaryParams P, const double* joint_q, co
                Q4{joint_q[qs + 3], joint_q[qs + 4], joint_q[qs + 5], joint_q[qs + 6]}};
       vj = v3(qd(ds), qd(ds + 1), qd(ds + 2));
       wj = v3(qd(ds + 3), qd(ds + 4), qd(ds + 5));
+    } else if (jt == SAPB_JOINT_D6) {  // sim/sap_kinematics.py:170-215
+      const int lin = P.m.joint_dof_dim[2 * i], ang = P.m.joint_dof_dim[2 * i + 1];
+      V3 ax[3];
+      d6_mobilizer(P.m.joint_axis + 3 * (size_t)ds, joint_q + qs, lin, ang, &X_j, ax);
+      for (int k = 0; k < lin && k < 3; ++k) vj = vj + qd(ds + k) * load3(P.m.joint_axis + 3 * (size_t)(ds + k));
+      for (int k = 0; k < ang && k < 3; ++k) wj = wj + qd(ds + lin + k) * ax[k];
     }
     const Xf X_wc = xf_mul(xf_mul(X_wpj, X_j), xf_inv(X_cj));
     const V3 lin = v_wpj + qrot(X_wpj.q, vj), ang = w_wpj + qrot(X_wpj.q, wj);

@@ -271,6 +271,10 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
       } else if (jt == SAPB_JOINT_FREE || jt == SAPB_JOINT_DISTANCE) {
         X_FM.p = v3(q[qs], q[qs + 1], q[qs + 2]);
         X_FM.q = Q4{q[qs + 3], q[qs + 4], q[qs + 5], q[qs + 6]};
+      } else if (jt == SAPB_JOINT_D6) {
+        V3 ax[3];
+        d6_mobilizer(P.m.joint_axis + 3 * (size_t)ds, q + qs, P.m.joint_dof_dim[2 * j], P.m.joint_dof_dim[2 * j + 1],
+                     &X_FM, ax);
       }
       T = xf_compose(xf_compose(xf_load(P.m.joint_X_p + 7 * (size_t)j), X_FM),
                      xf_inverse(xf_load(P.m.joint_X_c + 7 * (size_t)j)));
@@ -373,6 +377,26 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
         // translation gives [0; v_rel x w_rel]
         const V3 w_rel = qrot(R, v3(qd[ds], qd[ds + 1], qd[ds + 2]));
         const V3 v_rel = qrot(R, v3(qd[ds + 3], qd[ds + 4], qd[ds + 5]));
+        c = sv(v3(0, 0, 0), cross(v_rel, w_rel));
+      } else if (jt == SAPB_JOINT_D6) {
+        // translations [0; a_k], then rotations about M's origin [w_k; p_M x w_k]
+        // (the rotation axes at the current angles, held fixed in the bias
+        // like the reference, sim/sap_helpers.py:1387-1431)
+        const int lin = P.m.joint_dof_dim[2 * j], ang = P.m.joint_dof_dim[2 * j + 1];
+        Xf X_tmp;
+        V3 ax[3];
+        d6_mobilizer(P.m.joint_axis + 3 * (size_t)ds, q + P.m.joint_q_start[j], lin, ang, &X_tmp, ax);
+        V3 v_rel = v3(0, 0, 0), w_rel = v3(0, 0, 0);
+        for (int k = 0; k < lin && k < 3; ++k) {
+          const V3 a = qrot(R, load3(P.m.joint_axis + 3 * (size_t)(ds + k)));
+          put(k, sv(v3(0, 0, 0), a));
+          v_rel = v_rel + qd[ds + k] * a;
+        }
+        for (int k = 0; k < ang && k < 3; ++k) {
+          const V3 w = qrot(R, ax[k]);
+          put(lin + k, sv(w, cross(X_WM.p, w)));
+          w_rel = w_rel + qd[ds + lin + k] * w;
+        }
         c = sv(v3(0, 0, 0), cross(v_rel, w_rel));
       }
     }

@@ -104,4 +104,62 @@ __device__ __forceinline__ Sv mobilizer_accel_bias_to_body(Q4 R_WF, V3 p_MoBo_F,
   return Sv{v3(0, 0, 0), qrot(R_WF, cross(w_FM_F, cross(w_FM_F, p_MoBo_F)))};
 }
 
+// Rotation with the given columns (the reference's _quatd_from_matrix_cols,
+// sim/sap_helpers.py:608-655: the trace branch, else the largest diagonal).
+__device__ inline Q4 quat_from_cols(V3 c0, V3 c1, V3 c2) {
+  const double r00 = c0.x, r10 = c0.y, r20 = c0.z, r01 = c1.x, r11 = c1.y, r21 = c1.z, r02 = c2.x, r12 = c2.y,
+               r22 = c2.z;
+  const double tr = r00 + r11 + r22;
+  if (tr > 0.0) {
+    const double s = sqrt(tr + 1.0) * 2.0;
+    return Q4{(r21 - r12) / s, (r02 - r20) / s, (r10 - r01) / s, 0.25 * s};
+  }
+  if (r00 > r11 && r00 > r22) {
+    const double s = sqrt(1.0 + r00 - r11 - r22) * 2.0;
+    return Q4{0.25 * s, (r01 + r10) / s, (r02 + r20) / s, (r21 - r12) / s};
+  }
+  if (r11 > r22) {
+    const double s = sqrt(1.0 + r11 - r00 - r22) * 2.0;
+    return Q4{(r01 + r10) / s, 0.25 * s, (r12 + r21) / s, (r02 - r20) / s};
+  }
+  const double s = sqrt(1.0 + r22 - r00 - r11) * 2.0;
+  return Q4{(r02 + r20) / s, (r12 + r21) / s, 0.25 * s, (r10 - r01) / s};
+}
+
+// D6 mobilizer (sim/sap_helpers.py:1109-1161, 1204-1241, 1247-1286,
+// 1387-1431): `lin` translation axes a_k (coordinates q[0..lin)), then `ang`
+// rotation axes; with two or three rotation axes each axis is carried by the
+// rotations before it (axes e_x, e_y, e_z of the frame whose columns are the
+// joint axes).  Writes the transform X_FM and the angular DOF axes in F.
+__device__ inline void d6_mobilizer(const double* axes, const double* q, int lin, int ang, Xf* X, V3 ang_axis[3]) {
+  V3 pos = v3(0, 0, 0);
+  for (int k = 0; k < lin && k < 3; ++k) pos = pos + q[k] * load3(axes + 3 * k);
+  Q4 rot = qident();
+  const double* aa = axes + 3 * lin;
+  const double* qa = q + lin;
+  if (ang == 1) {
+    ang_axis[0] = load3(aa);
+    rot = qaxis_angle(ang_axis[0], qa[0]);
+  } else if (ang == 2 || ang == 3) {
+    const V3 c0 = load3(aa), c1 = load3(aa + 3);
+    const V3 c2 = ang == 3 ? load3(aa + 6) : cross(c0, c1);
+    const Q4 off = quat_from_cols(c0, c1, c2);
+    const V3 l0 = qrot(off, v3(1, 0, 0)), l1 = qrot(off, v3(0, 1, 0)), l2 = qrot(off, v3(0, 0, 1));
+    const Q4 q0 = qaxis_angle(l0, qa[0]);
+    const V3 a1 = qrot(q0, l1);
+    const Q4 q1 = qaxis_angle(a1, qa[1]);
+    const Q4 q10 = qmul(q1, q0);
+    ang_axis[0] = l0;
+    ang_axis[1] = a1;
+    rot = q10;
+    if (ang == 3) {
+      const V3 a2 = qrot(q10, l2);
+      ang_axis[2] = a2;
+      rot = qmul(qaxis_angle(a2, qa[2]), q10);
+    }
+  }
+  X->p = pos;
+  X->q = rot;
+}
+
 }  // namespace sapb

@@ -15,6 +15,9 @@ import numpy as np
 import torch
 
 from .runtime import (
+    SAP_JOINT_BALL,
+    SAP_JOINT_D6,
+    SAP_JOINT_DISTANCE,
     SAP_JOINT_FREE,
     SAP_JOINT_PRISMATIC,
     SAP_JOINT_REVOLUTE,
@@ -50,7 +53,9 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
     revolute, 18 DOF), 'box' (one free box, 6 DOF), 'boxes' (`boxes` free
     bodies, each its own tree: 6 * boxes DOF), 'arm_box' (7-revolute
     fixed-base arm + free box, 13 DOF), 'slider' (free base + prismatic +
-    revolute chain)."""
+    revolute chain), 'joints' (a chain through every mobilizer kind: free
+    base, ball, D6 (1 translation + 2 rotations), distance, D6 (2 + 1), D6
+    (3 rotations), revolute, D6 (3 translations), prismatic; 29 DOF)."""
     joints = []  # (type, parent_body, axis or None, X_p, X_c)
     link = 0.12
     if kind == "humanoid":
@@ -77,6 +82,16 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
         joints.append((SAP_JOINT_PRISMATIC, 0, None))
         for b in range(2, 6):
             joints.append((SAP_JOINT_REVOLUTE, b - 1, None))
+    elif kind == "joints":
+        joints.append((SAP_JOINT_FREE, -1, None))
+        joints.append((SAP_JOINT_BALL, 0, None))
+        joints.append((SAP_JOINT_D6, 1, (1, 2)))
+        joints.append((SAP_JOINT_DISTANCE, 2, None))
+        joints.append((SAP_JOINT_D6, 3, (2, 1)))
+        joints.append((SAP_JOINT_D6, 4, (0, 3)))
+        joints.append((SAP_JOINT_REVOLUTE, 5, None))
+        joints.append((SAP_JOINT_D6, 6, (3, 0)))
+        joints.append((SAP_JOINT_PRISMATIC, 7, None))
     else:
         raise ValueError(kind)
     B = len(joints)
@@ -96,7 +111,7 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
             X_c[k, :3] = _random_unit(rng, 1)[0] * 0.03
             X_c[k, 3:] = _random_quat(rng, 1)[0]
     mass = rng.uniform(0.5, 2.0, size=B)
-    if kind in ("humanoid", "quadruped", "slider"):
+    if kind in ("humanoid", "quadruped", "slider", "joints"):
         mass[0] *= 4.0
     inertia = np.stack([_spd_inertia(rng, mass[b], link) for b in range(B)])
     com = rng.uniform(-0.5, 0.5, size=(B, 3)) * link * 0.5
@@ -112,6 +127,15 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
         elif jtype[k] == SAP_JOINT_PRISMATIC:
             dofdim[k] = (1, 0)
             ncoord[k] = 1
+        elif jtype[k] == SAP_JOINT_BALL:
+            dofdim[k] = (0, 3)
+            ncoord[k] = 4
+        elif jtype[k] == SAP_JOINT_DISTANCE:
+            dofdim[k] = (3, 3)
+            ncoord[k] = 7
+        elif jtype[k] == SAP_JOINT_D6:
+            dofdim[k] = joints[k][2]
+            ncoord[k] = sum(joints[k][2])
     ndof = dofdim.sum(1)
     qd_start = np.concatenate([[0], np.cumsum(ndof)]).astype(np.int32)
     q_start = np.concatenate([[0], np.cumsum(ncoord)]).astype(np.int32)
@@ -120,6 +144,13 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
     for k in range(B):
         if jtype[k] in (SAP_JOINT_REVOLUTE, SAP_JOINT_PRISMATIC):
             axis[qd_start[k]] = axis_per_joint[k]
+        elif jtype[k] == SAP_JOINT_D6:
+            lin, ang = joints[k][2]
+            axis[qd_start[k]:qd_start[k] + lin] = _random_unit(rng, lin) if lin else axis[:0]
+            if ang:  # rotation axes: columns of a random rotation
+                qr = _random_quat(rng, 1)[0]
+                cols = np.stack([_qrot(qr, e) for e in np.eye(3)])
+                axis[qd_start[k] + lin:qd_start[k] + lin + ang] = cols[:ang]
     # joint ancestor: the joint whose child is this joint's parent body
     child = np.arange(B, dtype=np.int32)
     ancestor = np.array([parent[k] if parent[k] >= 0 else -1 for k in range(B)], np.int32)
@@ -145,6 +176,14 @@ def random_joint_q(tpl: dict, rng: np.random.Generator, worlds: int, spread: flo
             q[:, qs:qs + 3] = np.stack([rng.uniform(-1, 1, worlds), rng.uniform(-1, 1, worlds),
                                         rng.uniform(0.8, 1.2, worlds)], -1)
             q[:, qs + 3:qs + 7] = _random_quat(rng, worlds)
+        elif jt == SAP_JOINT_BALL:
+            q[:, qs:qs + 4] = _random_quat(rng, worlds)
+        elif jt == SAP_JOINT_DISTANCE:
+            q[:, qs:qs + 3] = rng.normal(scale=0.05, size=(worlds, 3))
+            q[:, qs + 3:qs + 7] = _random_quat(rng, worlds)
+        elif jt == SAP_JOINT_D6:
+            dim = int(tpl["joint_dof_dim"][k].sum())
+            q[:, qs:qs + dim] = rest[qs:qs + dim] + rng.normal(scale=spread, size=(worlds, dim))
         else:
             q[:, qs] = rest[qs] + rng.normal(scale=spread, size=worlds)
     return q

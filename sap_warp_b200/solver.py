@@ -101,8 +101,6 @@ class _ModelView:
         self.W, self.Jw, self.Bw, self.n, self.Qw = W, J // W, B // W, D // W, Q // W
         self.Aw = int(model.articulation_count) // W
         jt = model.joint_type.cpu().numpy()
-        if np.any(jt == SAP_JOINT_D6):
-            raise NotImplementedError("D6 joints are not supported by the native free motion.")
         parent_joint = model.joint_ancestor.cpu().numpy()
         if np.any(parent_joint >= np.arange(J)):
             raise ValueError("joints must be ordered parents before children")

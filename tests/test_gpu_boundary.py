@@ -30,7 +30,7 @@ def _t(a, dev):
     return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
 
 
-@pytest.mark.parametrize("kind", ["humanoid", "arm_box", "slider", "quadruped"])
+@pytest.mark.parametrize("kind", ["humanoid", "arm_box", "slider", "quadruped", "joints"])
 def test_conversions_and_fk_match_oracle(cuda_device, kind):
     rng, tpl, g, q = _case(kind, 11)
     model = models.to_model(tpl, g, q.reshape(4, -1), cuda_device)

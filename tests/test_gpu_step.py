@@ -13,7 +13,7 @@ from sap_warp_b200.solver import SapContactJacobian, SolverSAP
 
 pytestmark = pytest.mark.gpu
 
-KINDS = ["humanoid", "quadruped", "slider", "arm_box"]
+KINDS = ["humanoid", "quadruped", "slider", "arm_box", "joints"]
 
 
 def build(kind, worlds, seed, per_world=(8, 24), random_child_frames=False, max_contacts=32):
@@ -126,10 +126,13 @@ def test_truncation_counts(cuda_device):
 
 
 @pytest.mark.parametrize("mode", ["sap_euler", "midpoint"])
-def test_full_step_matches_oracle_pipeline(cuda_device, oracle, mode):
+@pytest.mark.parametrize("kind", ["humanoid", "joints"])
+def test_full_step_matches_oracle_pipeline(cuda_device, oracle, mode, kind):
     """SolverSAP.step == numpy free motion + contact rows -> C oracle solve ->
-    numpy integration, for a humanoid batch (drake-like preset, FP64)."""
-    case = build("humanoid", 32, seed=41, random_child_frames=True)
+    numpy integration, for a humanoid batch and a batch of chains through
+    every mobilizer kind (ball, distance, D6 with 1-3 rotation / translation
+    axes; drake-like preset, FP64)."""
+    case = build(kind, 32, seed=41, random_child_frames=True)
     model, state, control = gpu_state(case, cuda_device)
     solver = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", position_integration=mode,
                        contact_tau_d=0.0)

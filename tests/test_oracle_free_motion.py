@@ -49,3 +49,46 @@ def test_c_and_numpy_restatements_agree(oracle, kind):
         qn = oracle.integrate_positions(hm, q.reshape(-1), qd.reshape(-1), 1.1 * qd.reshape(-1), dt, mode)
         np.testing.assert_allclose(qn.reshape(E, -1), ofm.integrate(om, q, qd, 1.1 * qd, dt, mode), rtol=0,
                                    atol=1e-15)
+
+
+def test_motion_subspaces_are_pose_derivatives_for_every_mobilizer():
+    """Pins the numpy restatement of every mobilizer (free, ball, distance,
+    D6 with 1-3 rotation axes and 1-3 translations, revolute, prismatic) to
+    calculus: for joints whose velocity is the derivative of their
+    coordinates (scalar coordinates: revolute, prismatic, D6), the motion
+    subspace column S_k at a body origin equals the finite difference of
+    that body's pose with respect to coordinate k."""
+    from oracle.free_motion import JOINT_D6, JOINT_PRISMATIC, JOINT_REVOLUTE, qconj, qmul
+
+    rng = np.random.default_rng(13)
+    tpl = models.world_template("joints", rng)
+    g = models.replicate(tpl, 1, rng)
+    q = models.random_joint_q(tpl, rng, 1)
+    n, B = tpl["dofs_per_world"], tpl["bodies_per_world"]
+    om = ofm.Model(dict(tpl, gravity=g["gravity"][0]))
+    zero = np.zeros((1, n))
+    base = ofm.free_motion(om, q, zero, zero, np.zeros((1, B, 6)), np.full(1, 2e-3))
+    checked = 0
+    for j, jt in enumerate(tpl["joint_type"]):
+        if jt not in (JOINT_REVOLUTE, JOINT_PRISMATIC, JOINT_D6):
+            continue
+        qs, ds = tpl["joint_q_start"][j], tpl["joint_qd_start"][j]
+        for k in range(int(tpl["joint_dof_dim"][j].sum())):
+            eps = 1e-6
+            qp = q.copy()
+            qp[0, qs + k] += eps
+            qm = q.copy()
+            qm[0, qs + k] -= eps
+            fp = ofm.free_motion(om, qp, zero, zero, np.zeros((1, B, 6)), np.full(1, 2e-3))
+            fmn = ofm.free_motion(om, qm, zero, zero, np.zeros((1, B, 6)), np.full(1, 2e-3))
+            child = tpl["joint_child"][j]
+            for b in range(B):  # every body the column moves (its own and the subtree)
+                dp = (fp["pos"][0, b] - fmn["pos"][0, b]) / (2 * eps)
+                dq = qmul(fp["quat"][0, b], qconj(fmn["quat"][0, b]))
+                dw = 2.0 * dq[:3] * np.sign(dq[3]) / (2 * eps)
+                Jcol = base["Jb"][0, b, :, ds + k]
+                np.testing.assert_allclose(Jcol[:3], dw, rtol=1e-6, atol=1e-7, err_msg=f"joint {j} dof {k} body {b}")
+                np.testing.assert_allclose(Jcol[3:], dp, rtol=1e-6, atol=1e-7, err_msg=f"joint {j} dof {k} body {b}")
+            assert child >= 0
+            checked += 1
+    assert checked == 1 + 1 + 4 * 3  # revolute, prismatic, the four D6 joints of three axes each
