@@ -7,6 +7,12 @@ them down different paths they still agree to the conditioning times that
 tolerance.  The test therefore requires (per world) either a 1e-6 relative
 match with the oracle's v, or, for at most 2% of worlds, a 1e-4 match plus the
 stationarity of the GPU answer checked independently in numpy.
+
+Tie policy for the active set: a contact's mode may differ from the
+oracle's only where a regime boundary of the projection (stiction /
+sliding / separation, sim/contact_solve.py:856-907) lies between the two
+answers -- the numpy projection at the GPU's velocity gives the GPU's mode
+and at the oracle's velocity the oracle's.  Every other mode is identical.
 """
 
 import numpy as np
@@ -58,9 +64,21 @@ def assert_parity(prob, gpu, ref, tight=1e-6, loose=1e-4, max_loose_frac=0.02):
     g_scale = np.maximum(np.abs(ref["contact_gamma"]).max(axis=(1, 2)), 1e-12)
     g_err = np.abs(gpu["contact_gamma"] - ref["contact_gamma"]).max(axis=(1, 2)) / g_scale
     assert np.all(g_err[tight_worlds] <= 1e-5), f"gamma error {g_err[tight_worlds].max():.3e}"
-    # active set: identical contact modes except at a regime boundary
+    # active set: identical contact modes except at a regime boundary that
+    # lies between the two answers (the tie policy above)
     mism = (gpu["contact_mode"] != ref["contact_mode"])[tight_worlds].sum()
     assert mism <= max(1, 0.002 * tight_worlds.sum() * prob.max_contacts), f"{mism} mode mismatches"
+    for e in np.nonzero(tight_worlds)[0]:
+        c = int(min(prob.contact_count[e], prob.max_contacts))
+        diff = np.nonzero(gpu["contact_mode"][e, :c] != ref["contact_mode"][e, :c])[0]
+        if diff.size == 0:
+            continue
+        rt, rn, vhat = sn.contact_constants(prob.phi0[e, :c], prob.w_eff[e, :c], prob.mu[e, :c],
+                                            prob.stiffness[e, :c], prob.tau_d[e, :c])
+        for vv, want in ((Vg[e], gpu["contact_mode"][e, :c]), (Vr[e], ref["contact_mode"][e, :c])):
+            vc = np.einsum("crj,j->cr", prob.jacobian[e, :c], vv)
+            _, mode = sn.project(vc, prob.mu[e, :c], rt, rn, vhat)
+            np.testing.assert_array_equal(mode[diff], want[diff], err_msg=f"world {e}: a mode differs off a boundary")
     np.testing.assert_array_equal(gpu["converged"], ref["converged"])
     np.testing.assert_allclose(gpu["cost"], ref["cost"], rtol=1e-6, atol=1e-12)
 
@@ -71,8 +89,18 @@ def test_humanoid_parity_fp64(cuda_device, oracle, variant):
     ref = oracle.solve(prob, variant)
     gpu = run_gpu(prob, cuda_device, variant)
     if variant == "monotone_decay":
-        # the loose cost test makes early stops path-sensitive: compare where
-        # the iteration counts agree, and require the same counts almost everywhere
+        # the loose cost test (|dl| < 5e-3 mean|l|) stops early and path-
+        # dependently: check every world path-independently against the
+        # optimum (the oracle run to a tight tolerance): both answers are
+        # within the same band of the optimal cost, and identical where the
+        # paths agree (same iteration counts)
+        opt = oracle.solve(prob, "armijo_decay", optimality_rel_tol=1e-12, cost_rel_tol=0.0, max_iterations=200)
+        lo = opt["cost"]
+        gap_g, gap_r = gpu["cost"] - lo, ref["cost"] - lo
+        band = np.maximum(2.0 * np.abs(gap_r), 5e-3 * np.abs(lo)) + 1e-12
+        assert np.all(gap_g >= -1e-9 * np.abs(lo) - 1e-12), "a GPU cost below the optimum"
+        assert np.all(np.abs(gap_g) <= band), np.abs(gap_g / band).max()
+        np.testing.assert_array_equal(gpu["converged"], ref["converged"])
         same = gpu["newton_iterations"] == ref["newton_iterations"]
         assert same.mean() > 0.95
         idx = np.nonzero(same)[0]
@@ -101,7 +129,16 @@ def test_mixed_precision_matches_fp64_oracle(cuda_device, oracle):
     assert np.all(gpu["converged"] == 1)
     n = prob.dof_per_env
     err = np.abs(gpu["v"] - ref["v"]).reshape(-1, n).max(1) / np.abs(ref["v"]).reshape(-1, n).max(1)
-    assert np.quantile(err, 0.98) <= 1e-6 and err.max() <= 1e-4
+    assert np.quantile(err, 0.99) <= 1e-6 and err.max() <= 1e-5, (np.quantile(err, 0.99), err.max())
+    # every world above 1e-6 is itself stationary to the solve's tolerance (FP64 numpy check)
+    Vg = gpu["v"].reshape(-1, n)
+    for e in np.nonzero(err > 1e-6)[0]:
+        c = prob.contact_count[e]
+        _, grad, _, _ = sn.objective(Vg[e], prob.dynamics_matrix[e], prob.v_star.reshape(-1, n)[e], prob.jacobian[e],
+                                     prob.phi0[e], prob.w_eff[e], prob.mu[e], prob.stiffness[e], prob.tau_d[e], c)
+        d = 1.0 / np.sqrt(np.diag(prob.dynamics_matrix[e]))
+        s_ = max(np.linalg.norm(d * (prob.dynamics_matrix[e] @ Vg[e])), 1.0)
+        assert np.linalg.norm(d * grad) <= 1e-6 * s_ * 1.01 + 1e-12
 
 
 def test_unconstrained_and_truncated(cuda_device, oracle):
