@@ -488,6 +488,52 @@ def main():
     torch.cuda.synchronize()
     e2e_same = bool(torch.equal(host_q, e2e_final_q))
 
+    # ---- contacts regenerated from the pose every step (models.site_scene):
+    # contact generation + the step, the three arms, eager steps timed by
+    # events after a settling prefix ----
+    from sap_warp_b200.collision import ContactGenerator
+
+    smodel, sstate0, scontrol, sshapes, _ = models.site_scene("humanoid", shard.worlds, shard.seed + 7, dev)
+    site = {"worlds": W, "contacts": "32 sphere sites per world over per-site ground patches, 8-32 touching at "
+                                     "the start; contacts regenerated from the pose every step (they appear and "
+                                     "vanish)"}
+    for label, prec, warm in (("plain_fp64", "fp64", "previous_velocity"),
+                              ("previous_impulses_fp32", "fp32", "previous_impulses"),
+                              ("learned_fp32", "fp32", "learned")):
+        ssolver = SolverSAP(smodel, max_rigid_contact=MAX_CONTACTS, contact_preset_variant="drake",
+                            hessian_precision=prec, warm_start=warm, learned_warm_start=ws if warm == "learned" else None)
+        sgen = ContactGenerator(sshapes, ssolver.view, capacity=shard.worlds * MAX_CONTACTS, gap=1.0e-3)
+        sa = SapState(joint_q=sstate0.joint_q.clone(), joint_qd=sstate0.joint_qd.clone(),
+                      body_q=sstate0.body_q.clone(), body_f=sstate0.body_f.clone())
+        sb = SapState(joint_q=sstate0.joint_q.clone(), joint_qd=sstate0.joint_qd.clone(),
+                      body_q=sstate0.body_q.clone(), body_f=sstate0.body_f.clone())
+        for _ in range(20 + args.warmup):
+            ssolver.step(sa, sb, scontrol, sgen.generate(sa.joint_q), DT)
+            sa, sb = sb, sa
+        barrier()
+        k_site = max(1, min(args.steps, 40))
+        its, cnt = [], []
+        ssolver.stage_events = []
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(k_site):
+            c = sgen.generate(sa.joint_q)
+            ssolver.step(sa, sb, scontrol, c, DT)
+            its.append(ssolver.contact_solve.newton_iterations_env.double().mean())
+            cnt.append(c.rigid_contact_count.double())
+            sa, sb = sb, sa
+        a1.record(stream)
+        barrier()
+        ms = max_over_ranks(a0.elapsed_time(a1) / k_site)
+        site[label] = {"value": W * world_size / (ms * 1e-3), "ms_per_step_with_generation": ms,
+                       "stages_ms": {k: v / k_site for k, v in ssolver.stage_times().items()},
+                       "mean_newton_iterations": float(torch.stack(its).mean()),
+                       "mean_contacts_per_world": float(torch.stack(cnt).mean()) / shard.worlds,
+                       "all_converged": bool(ssolver.contact_solve.converged_env.all())}
+        del ssolver, sgen
+    site["speedup_vs_plain_fp64"] = (site["plain_fp64"]["ms_per_step_with_generation"]
+                                     / site["learned_fp32"]["ms_per_step_with_generation"])
+
     # ---- stage-2 solve alone on the snapshot of the configuration -------------
     prob = scenes.humanoid_contact_problem(args.worlds, seed=SEED + 1000 * rank)
     t = problem_to_device(prob, dev)
@@ -547,8 +593,8 @@ def main():
         occ = int(_load_lib().sapb_contact_solve_occupancy(bb.dof_per_env, bb.max_contacts, opts.hessian_precision,
                                                             opts.line_search_variant))
 
-        def time_ms(k, tt=tt, bb=bb, opts=opts, wo=wo):
-            opts.ctas_per_sm = k
+        def time_ms(shape, tt=tt, bb=bb, opts=opts, wo=wo):
+            opts.ctas_per_sm, opts.ldlt_block = shape
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             contact_solve(**tt, buffers=bb, options=opts, world_order=wo)
@@ -556,9 +602,14 @@ def main():
             e1.synchronize()
             return e0.elapsed_time(e1)
 
+        wl = (__import__("ctypes").c_int32 * 8)()
+        nw = max(min(int(_load_lib().sapb_contact_solve_ldlt_blocks(bb.dof_per_env, wl, 8)), 8), 1)
         tuner = SolveAutotuner(repeats=5)
-        chosen = tuner.tune(label, list(range(1, occ + 1)), time_ms)
-        tuned[label] = {"occupancy": occ, "chosen": chosen, "ms": tuner.table[label]["ms"]}
+        chosen = tuner.tune(label, [(k, int(wl[w])) for w in range(nw) for k in range(1, occ + 1)], time_ms,
+                            default=(occ, int(wl[0])))
+        opts.ctas_per_sm, opts.ldlt_block = 0, 0
+        tuned[label] = {"occupancy": occ, "ldlt_blocks": [int(wl[w]) for w in range(nw)], "chosen": list(chosen),
+                        "ms": tuner.table[label]["ms"]}
 
     # ---- worlds of 64 free boxes (384 DOFs, ~400 contacts): tree-blocked solve ----
     boxes = scenes.box_stack_problem(512, seed=4 + 1000 * rank)
@@ -697,8 +748,7 @@ def main():
                          "ms_per_step_eager": fast["ms_eager"],
                          "graph_replay_matches_eager": fast["graph_matches_eager"],
                          "chosen_start": {"previous_velocity": int(fast["chosen"][0]),
-                                          "network": int(fast["chosen"][1]),
-                                          "previous_impulses": int(fast["chosen"][2])},
+                                          "carried_impulses_and_network": int(fast["chosen"][1])},
                          "stages_ms": fast["stages"], "speedup_vs_plain_fp64": plain["ms"] / fast["ms"],
                          "max_rel_qd_diff_vs_plain_fp64_after_rollout": dq},
         "previous_impulses_fp32": {"value": total / (prev["ms"] * 1e-3), "ms_per_step": prev["ms"],
@@ -707,8 +757,9 @@ def main():
         "uneven_batch_solve_only": uneven,
         "box_worlds_solve_only": box_line,
         "box_worlds_step": box_step,
+        "regenerated_contacts_rollout": site,
         "contact_generation": contact_gen,
-        "autotune_ctas_per_sm": tuned,
+        "autotune_launch_shape": tuned,
         "e2e": {"value": total / (ms_e2e * 1e-3), "unit": "world-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e,
                 "path": "SolverSAP.capture_host_steps: two steps and their host copies per graph replay, "

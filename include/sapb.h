@@ -104,6 +104,9 @@ typedef struct sapb_solve_options {
   int32_t cubic_init;             /* exact_root cubic seed, sim/contact_solve.py:55-58 (1) */
   int32_t ctas_per_sm;            /* resident CTAs per SM of the persistent dense solve: 0 as many as fit
                                    * (sapb_contact_solve_occupancy), k at most k; results do not depend on it */
+  int32_t ldlt_block;             /* column-block width of the dense solve's LDL^T: 0 the default for the DOF
+                                   * count, else one of sapb_contact_solve_ldlt_blocks (others: the default);
+                                   * the width changes the factorization's rounding, not the tolerance */
 } sapb_solve_options;
 
 /* Per-DOF drive and limit model (the arrays SapContactSolve.prepare reads,
@@ -506,6 +509,11 @@ int32_t sapb_generate_contacts(const sapb_collision_shapes* shapes, const double
  * (the upper end of sapb_solve_options.ctas_per_sm), or a negative status. */
 int32_t sapb_contact_solve_occupancy(int32_t dof_per_env, int32_t max_contacts, int32_t hessian_precision,
                                      int32_t line_search_variant);
+
+/* The LDL^T column-block widths the dense solve is built with for worlds of
+ * dof_per_env DOFs (the first is the default), written to widths (at most
+ * capacity); returns their count.  The autotuner's compile-time variants. */
+int32_t sapb_contact_solve_ldlt_blocks(int32_t dof_per_env, int32_t* widths, int32_t capacity);
 
 /* Fill the reference defaults of SapContactSolve for a line-search variant.
  * Replaces the Python defaults of solve(), sim/contact_solve.py:6129-6182. */

@@ -67,6 +67,7 @@ class SolveOptions(C.Structure):
         ("hessian_precision", C.c_int32),
         ("cubic_init", C.c_int32),
         ("ctas_per_sm", C.c_int32),
+        ("ldlt_block", C.c_int32),
     ]
 
 
@@ -357,6 +358,7 @@ EXPORTS = {
     "sapb_contact_history_update": (C.c_int32, [C.POINTER(ContactHistory), _p]),
     "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_occupancy": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "sapb_contact_solve_ldlt_blocks": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.c_int32]),
     "sapb_contact_solve": (
         C.c_int32,
         [C.POINTER(ContactProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p, C.c_size_t, _p],

@@ -1,14 +1,18 @@
-"""Autotuner of the persistent dense contact solve's launch shape.
+"""Autotuner of the persistent dense contact solve's launch shape and its
+compile-time variants.
 
 The solve kernel is persistent: sms x k CTAs take worlds from a device work
 counter, and each world is solved by one CTA, so results do not depend on k
-(the resident CTAs per SM).  The best k is the occupancy maximum for most
-shapes, but not for every one (fewer resident worlds share the SM's
-instruction cache and issue slots).  The tuner times each k from 1 to the
-occupancy bound on the caller's own first solve (CUDA events, best of a few
-runs each) and keeps the fastest in a table keyed by (DOFs per world,
-contact-slot bucket, precision, line search, GPU name, SM count), which it
-can persist as JSON.
+(the resident CTAs per SM).  The kernel is also built in variants of the
+LDL^T factorization's column-block width b (sapb_contact_solve_ldlt_blocks):
+the best width depends on the DOF count (35 DOFs: seven blocks of 5), and
+the width changes the factorization's rounding (not the tolerance the
+solve reaches).  The tuner times every (k, b) on the caller's own first
+solve (CUDA events, best of a few runs each) and keeps the fastest in a
+table keyed by (DOFs per world, contact-slot bucket, precision, line search,
+GPU name, SM count), which it can persist as JSON.  The default shape (the
+occupancy bound, the first width) is kept unless another beats it by more
+than a margin.
 """
 
 from __future__ import annotations
@@ -33,8 +37,17 @@ def tuning_key(dof_per_env: int, max_contacts: int, precision: str, line_search:
             f"{int(sm_count)}sm")
 
 
+def _label(shape) -> str:
+    return ",".join(str(int(x)) for x in shape) if isinstance(shape, (tuple, list)) else str(int(shape))
+
+
+def _shape(value):
+    return tuple(int(x) for x in value) if isinstance(value, (tuple, list)) else int(value)
+
+
 class SolveAutotuner:
-    """Choice of resident CTAs per SM per problem key.
+    """Choice of launch shape per problem key: an int (resident CTAs per SM)
+    or a tuple (CTAs per SM, LDL^T block width).
 
     cache_path: a JSON file to load the table from and write it back to after
     each new choice (None: this process only).  repeats: timed runs per
@@ -52,26 +65,38 @@ class SolveAutotuner:
                 raise ValueError(f"{self.cache_path}: not an autotuning table")
             self.table = data
 
-    def lookup(self, key: str) -> int | None:
+    def lookup(self, key: str):
         entry = self.table.get(key)
-        return None if entry is None else int(entry["ctas_per_sm"])
+        if entry is None:
+            return None
+        return _shape(entry["choice"]) if "choice" in entry else int(entry["ctas_per_sm"])
 
-    def tune(self, key: str, candidates: list[int], time_ms: Callable[[int], float]) -> int:
+    def tune(self, key: str, candidates: list, time_ms: Callable, default=None):
         """The cached choice for `key`, else the candidate with the least time,
-        recorded with every candidate's time.  The largest candidate (the
-        occupancy bound, the launch without tuning) is kept unless another
-        beats it by more than `margin` (a short sample decides)."""
+        recorded with every candidate's time.  The default (given, or for
+        plain ints the largest: the occupancy bound, the launch without
+        tuning) is kept unless another beats it by more than `margin` (a
+        short sample decides)."""
         known = self.lookup(key)
         if known is not None:
             return known
-        cands = sorted({int(k) for k in candidates if int(k) >= 1})
+        cands = [_shape(c) for c in candidates]
+        cands = [c for c in dict.fromkeys(cands) if (min(c) if isinstance(c, tuple) else c) >= 1]
         if not cands:
             raise ValueError("no candidate launch shape")
-        times = {k: min(float(time_ms(k)) for _ in range(self.repeats)) for k in cands}
-        best = min(cands, key=lambda k: (times[k], -k))
-        if times[cands[-1]] <= times[best] * (1.0 + self.margin):
-            best = cands[-1]
-        self.table[key] = {"ctas_per_sm": best, "ms": {str(k): times[k] for k in cands}}
+        if default is None:
+            default = max(cands) if all(isinstance(c, int) for c in cands) else cands[-1]
+        default = _shape(default)
+        if default not in cands:
+            raise ValueError("the default shape is not a candidate")
+        times = {c: min(float(time_ms(c)) for _ in range(self.repeats)) for c in cands}
+        best = min(cands, key=lambda c: times[c])
+        if times[default] <= times[best] * (1.0 + self.margin):
+            best = default
+        entry = {"choice": list(best) if isinstance(best, tuple) else best,
+                 "ctas_per_sm": best[0] if isinstance(best, tuple) else best,
+                 "ms": {_label(c): times[c] for c in cands}}
+        self.table[key] = entry
         self.save()
         return best
 

@@ -35,6 +35,14 @@ int32_t sapb_contact_solve_occupancy(int32_t dof_per_env, int32_t max_contacts, 
   return sapb::contact_solve_occupancy(dof_per_env, max_contacts, hessian_precision, line_search_variant);
 }
 
+int32_t sapb_contact_solve_ldlt_blocks(int32_t dof_per_env, int32_t* widths, int32_t capacity) {
+  if (dof_per_env < 1 || capacity < 0 || (capacity > 0 && !widths)) {
+    sapb::set_last_error("sapb_contact_solve_ldlt_blocks: invalid argument");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::ldlt_block_widths(dof_per_env, widths, capacity);
+}
+
 void sapb_solve_options_default(sapb_solve_options* o, int32_t variant) {
   // SapContactSolve defaults: sim/contact_solve.py:3299-3316 and 6129-6182.
   if (!o) return;

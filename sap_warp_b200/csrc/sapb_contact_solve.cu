@@ -31,6 +31,23 @@ int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant
   return per_sm;
 }
 
+template <int NS>
+static int widths_of(int32_t* out, int capacity) {
+  int k = 0;
+  for (; k < LdltBlocks<NS>::kCount && k < capacity; ++k) out[k] = LdltBlocks<NS>::kW[k];
+  return LdltBlocks<NS>::kCount;
+}
+
+int ldlt_block_widths(int n, int32_t* out, int capacity) {
+  switch (n) {
+    case 35: return widths_of<35>(out, capacity);
+    case 18: return widths_of<18>(out, capacity);
+    case 13: return widths_of<13>(out, capacity);
+    case 6: return widths_of<6>(out, capacity);
+    default: return widths_of<0>(out, capacity);
+  }
+}
+
 static cudaError_t solve_dispatch(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
   // Kernels specialised on the DOF count of the common trees (humanoid 35,
   // quadruped 18, arm + box 13, single free body 6); a generic one otherwise.

@@ -412,10 +412,10 @@ __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) 
 // wait on a shuffle and a shared-memory round trip.  A four-column blocked
 // warp solve measured no faster than the column-by-column one.)  A pivot
 // that is not positive / finite makes dv NaN.
-template <int NT, typename HT, int NS>
+template <int NT, typename HT, int NS, int LB>
 __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
-  ldlt_blocked<NT, HT>(w.H, w.dofs(), w.ldH(), dinv, w.tri);
+  ldlt_blocked<NT, HT, LB>(w.H, w.dofs(), w.ldH(), dinv, w.tri);
   if ((threadIdx.x >> 5) == 0) {
     const bool ok = ldlt_pivots_ok_warp<HT>(w.H, w.dofs(), w.ldH());
     if (threadIdx.x == 0) *w.factor_ok = ok ? 1 : 0;
@@ -467,8 +467,10 @@ __device__ void line_coefficients(const World<NT, HT, NS>& w, double c4[4]) {
 
 // LSV: the line search, fixed at compile time (SAPB_LS_ARMIJO_DECAY,
 // SAPB_LS_EXACT_ROOT or SAPB_LS_MONOTONE_DECAY) so that one instantiation
-// holds the code of one search only (smaller instruction footprint).
-template <int NT, typename HT, int MINB, int NS, int LSV>
+// holds the code of one search only (smaller instruction footprint).  LB:
+// the column-block width of the LDL^T factorization (a variant the
+// autotuner chooses: the best width depends on the DOF count).
+template <int NT, typename HT, int MINB, int NS, int LSV, int LB>
 __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolveParams P) {
   static_assert(NT / 32 <= Layout::kMaxWarps, "partial-sum scratch sized for kMaxWarps warps");
   extern __shared__ __align__(16) unsigned char smem[];
@@ -762,7 +764,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         } else {
           load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
           __syncthreads();
-          ldlt_blocked<NT, HT>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri);  // the factor of A
+          ldlt_blocked<NT, HT, LB>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri);  // the factor of A
         }
         bool last_is_best = false;
         // Two sets at a time: stage their impulses in the (here unused)
@@ -855,7 +857,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         if (!active) break;
         // Newton direction
         assemble_hessian<NT, HT, NS>(w, P.o.diag_shift);
-        factor_and_solve<NT, HT, NS>(w);
+        factor_and_solve<NT, HT, NS, LB>(w);
         if (!*w.factor_ok) {  // H not SPD (uniform: published by the barrier above)
           status = SAPB_WORLD_NOT_SPD;
           converged = 0;
@@ -865,11 +867,11 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         double c4[4];
         line_coefficients<NT, HT, NS>(w, c4);
         if constexpr (LSV == SAPB_LS_ARMIJO_DECAY)
-          r = ls_armijo<NT, 3>(w, P, dt, cost, c4);
+          r = ls_armijo<NT, 1>(w, P, dt, cost, c4);
         else if constexpr (LSV == SAPB_LS_EXACT_ROOT)
           r = ls_exact<NT>(w, P, dt, cost, c4);
         else
-          r = ls_monotone<NT, 3>(w, P, dt, cost, c4);
+          r = ls_monotone<NT, 1>(w, P, dt, cost, c4);
         alpha = r.alpha;
         status = r.status;
         constexpr bool mono = LSV == SAPB_LS_MONOTONE_DECAY;
@@ -916,10 +918,10 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   }
 }
 
-template <int NT, typename HT, int MINB, int NS, int LSV>
+template <int NT, typename HT, int MINB, int NS, int LSV, int LB>
 static cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
   const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT));
-  auto kern = contact_solve_kernel<NT, HT, MINB, NS, LSV>;
+  auto kern = contact_solve_kernel<NT, HT, MINB, NS, LSV, LB>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (err != cudaSuccess) return err;
   int dev = 0;
@@ -947,16 +949,32 @@ static cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, in
   return cudaGetLastError();
 }
 
-template <int NT, typename HT, int MINB, int NS>
+template <int NT, typename HT, int MINB, int NS, int LB>
 static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
   switch (P.o.line_search_variant) {
     case SAPB_LS_ARMIJO_DECAY:
-      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_ARMIJO_DECAY>(P, stream, blocks_out);
+      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_ARMIJO_DECAY, LB>(P, stream, blocks_out);
     case SAPB_LS_EXACT_ROOT:
-      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_EXACT_ROOT>(P, stream, blocks_out);
+      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_EXACT_ROOT, LB>(P, stream, blocks_out);
     default:
-      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_MONOTONE_DECAY>(P, stream, blocks_out);
+      return launch_solve_ls<NT, HT, MINB, NS, SAPB_LS_MONOTONE_DECAY, LB>(P, stream, blocks_out);
   }
+}
+
+// LDL^T block widths instantiated per DOF specialisation (the first is the
+// default), from measurements on B200: 35 DOFs = 7 blocks of 5 is fastest
+// in both precisions; wider blocks lengthen the serial diagonal chain and
+// the register block, narrower ones add barriers.
+template <int NS> struct LdltBlocks { static constexpr int kCount = 1; static constexpr int kW[1] = {4}; };
+template <> struct LdltBlocks<35> { static constexpr int kCount = 2; static constexpr int kW[2] = {5, 4}; };
+template <> struct LdltBlocks<18> { static constexpr int kCount = 2; static constexpr int kW[2] = {6, 4}; };
+template <> struct LdltBlocks<13> { static constexpr int kCount = 2; static constexpr int kW[2] = {4, 5}; };
+template <> struct LdltBlocks<6> { static constexpr int kCount = 1; static constexpr int kW[1] = {6}; };
+
+template <int NS, int LB>
+static cudaError_t launch_solve_lb(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
+  return fp32 ? launch_solve<128, float, 4, NS, LB>(P, stream, blocks_out)
+              : launch_solve<128, double, 3, NS, LB>(P, stream, blocks_out);
 }
 
 // The kernels of one DOF specialisation NS (both Hessian precisions, every
@@ -964,9 +982,13 @@ static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* 
 // (sapb_solve_n*.cu) so the specialisations compile in parallel.
 template <int NS>
 cudaError_t launch_solve_ns(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
-  return fp32 ? launch_solve<128, float, 4, NS>(P, stream, blocks_out)
-              : launch_solve<128, double, 3, NS>(P, stream, blocks_out);
+  constexpr int n = LdltBlocks<NS>::kCount;
+  const int want = P.o.ldlt_block;
+  if (n > 1 && want == LdltBlocks<NS>::kW[n > 1 ? 1 : 0])
+    return launch_solve_lb<NS, LdltBlocks<NS>::kW[n > 1 ? 1 : 0]>(P, fp32, stream, blocks_out);
+  return launch_solve_lb<NS, LdltBlocks<NS>::kW[0]>(P, fp32, stream, blocks_out);  // the default (0 or unknown)
 }
+
 
 extern template cudaError_t launch_solve_ns<35>(const SolveParams&, bool, cudaStream_t, int*);
 extern template cudaError_t launch_solve_ns<18>(const SolveParams&, bool, cudaStream_t, int*);

@@ -18,6 +18,7 @@ void set_last_error(const char* fmt, ...);
 
 size_t contact_solve_smem_bytes(int n, int C, int hessian_precision);
 int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant);
+int ldlt_block_widths(int n, int32_t* out, int capacity);
 int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_options* o, const sapb_solve_outputs* out,
                              void* workspace, size_t workspace_bytes, cudaStream_t stream);
 

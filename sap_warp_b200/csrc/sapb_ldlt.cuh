@@ -23,7 +23,7 @@ __device__ __forceinline__ void build_triangle_list(uint16_t* tri, int n) {
 
 // In-place right-looking LDL^T of the lower triangle of H (row stride ldH):
 // afterwards H_ik = L_ik d_k below the diagonal (L unit lower), d_k on it,
-// dinv[k] = 1/d_k.  8-column blocks (6 in FP64), two barriers per block:
+// dinv[k] = 1/d_k.  B-column blocks, two barriers per block:
 // every thread factors the block's diagonal block in
 // registers (it is final once the previous trailing update is done), the rows
 // under it (the panel) are solved against it in registers, one per thread;
@@ -32,10 +32,10 @@ __device__ __forceinline__ void build_triangle_list(uint16_t* tri, int n) {
 // recurrence on the stored form W_ik = L_ik d_k:
 //   d_k = H_kk - sum_{e<k} W_ke^2 / d_e,  W_ik = H_ik - sum_{e<k} W_ie W_ke / d_e.
 // H must be complete when called (barrier before); complete on return.
-template <int NT, typename T>
+template <int NT, typename T, int B>
 __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri) {
+  static_assert(B >= 1 && B <= 8, "block width");
   const int tid = threadIdx.x;
-  constexpr int B = sizeof(T) == 4 ? 8 : 6;  // FP64 blocks of 6: the register block stays small
   for (int K = 0; K < n; K += B) {
     const int bs = min(B, n - K);
     const int rest = n - K - bs;

@@ -579,11 +579,13 @@ class SapContactSolve:
                             rho=float(rho), line_search_relative_slop=float(line_search_relative_slop))
         return variant, opts
 
-    def _launch_shape(self, P, opts, variant: str, stream, guess: torch.Tensor | None = None) -> int:
-        """Resident CTAs per SM for this problem: 0 (the occupancy bound)
-        without an autotuner; with one, its choice for the problem's key,
+    def _launch_shape(self, P, opts, variant: str, stream, guess: torch.Tensor | None = None) -> tuple[int, int]:
+        """(resident CTAs per SM, LDL^T block width) for this problem: (0, 0)
+        -- the occupancy bound and the default width -- without an
+        autotuner; with one, its choice for the problem's key among every
+        CTA count up to the bound and every width the kernel is built with,
         timed here on this very problem the first time the key is seen
-        (never while a graph is being captured: then the bound).  The solve
+        (never while a graph is being captured: then the defaults).  The solve
         writes its start back into the warm-start guess `guess` (and the
         guess may be the output velocity itself), so the guess is saved
         before the timed solves and restored before each of them and after:
@@ -591,7 +593,7 @@ class SapContactSolve:
         from .autotune import tuning_key
 
         if self.autotuner is None:
-            return 0
+            return 0, 0
         v = self.view
         fp32 = opts.hessian_precision == _abi.SAPB_FP32 or opts.linear_solve_precision == _abi.SAPB_FP32
         if self._device_props is None:
@@ -601,9 +603,9 @@ class SapContactSolve:
                          props.multi_processor_count)
         known = self.autotuner.lookup(key)
         if known is not None:
-            return known
+            return known if isinstance(known, tuple) else (known, 0)
         if torch.cuda.is_current_stream_capturing():
-            return 0
+            return 0, 0
         lib = load()
         occ = int(lib.sapb_contact_solve_occupancy(v.n, int(P.max_contacts),
                                                    _abi.SAPB_FP32 if fp32 else _abi.SAPB_FP64,
@@ -612,10 +614,12 @@ class SapContactSolve:
             check(occ, "sapb_contact_solve_occupancy")
         cur = torch.cuda.current_stream(v.device)
         saved = guess.clone() if guess is not None else None
+        widths = (ctypes.c_int32 * 8)()
+        nw = max(min(int(lib.sapb_contact_solve_ldlt_blocks(v.n, widths, 8)), 8), 1)
 
-        def time_ms(k: int) -> float:
+        def time_ms(shape) -> float:
             o = _abi.SolveOptions.from_buffer_copy(opts)
-            o.ctas_per_sm = k
+            o.ctas_per_sm, o.ldlt_block = shape
             if saved is not None:
                 guess.copy_(saved)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -627,7 +631,8 @@ class SapContactSolve:
             e1.synchronize()
             return e0.elapsed_time(e1)
 
-        chosen = self.autotuner.tune(key, list(range(1, occ + 1)), time_ms)
+        cands = [(k, int(widths[b])) for b in range(nw) for k in range(1, occ + 1)]
+        chosen = self.autotuner.tune(key, cands, time_ms, default=(occ, int(widths[0])))
         if saved is not None:
             guess.copy_(saved)
         return chosen
@@ -702,7 +707,7 @@ class SapContactSolve:
                 setattr(self.dof, name, _ptr(tt))
             P.dof = ctypes.pointer(self.dof)
         stream = ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream)
-        opts.ctas_per_sm = self._launch_shape(P, opts, variant, stream, v_guess)
+        opts.ctas_per_sm, opts.ldlt_block = self._launch_shape(P, opts, variant, stream, v_guess)
         status = load().sapb_contact_solve(ctypes.byref(P), ctypes.byref(opts), ctypes.byref(self.outputs),
                                            self.workspace.data_ptr(), self.workspace.numel(), stream)
         check(status, "sapb_contact_solve")

@@ -1,7 +1,9 @@
-"""The dense solve's launch shape (resident CTAs per SM) on the GPU: the
-occupancy bound, results independent of the shape, and SolverSAP's
-autotuner timing the candidates on its first solve."""
+"""The dense solve's launch shape (resident CTAs per SM) and LDL^T block
+width on the GPU: the occupancy bound, results independent of the CTA
+count (bit for bit) and of the block width (to the solve's tolerance), and
+SolverSAP's autotuner timing the candidates on its first solve."""
 
+import ctypes
 import json
 
 import numpy as np
@@ -59,14 +61,21 @@ def test_solver_autotune_writes_its_choice(cuda_device, tmp_path):
 
     q0, qd0 = run()
     q1, qd1 = run(autotune=str(path))
-    assert torch.equal(q0, q1) and torch.equal(qd0, qd1)
+    q2, qd2 = run(autotune=str(path))  # the saved choice, no timing
+    assert torch.equal(q1, q2) and torch.equal(qd1, qd2)
+    scale = float(qd0.abs().max())
+    assert float((qd1 - qd0).abs().max()) <= 1e-6 * scale  # a different block width: same tolerance
     table = json.loads(path.read_text())
     assert len(table) == 1
     (key, entry), = table.items()
     assert key.startswith("n35-c32-fp32-armijo_decay-")
     occ = load().sapb_contact_solve_occupancy(35, 32, _abi.SAPB_FP32, _abi.LINE_SEARCH_VARIANTS["armijo_decay"])
-    assert set(entry["ms"]) == {str(k) for k in range(1, occ + 1)}
-    assert 1 <= entry["ctas_per_sm"] <= occ
+    widths = (ctypes.c_int32 * 8)()
+    nw = load().sapb_contact_solve_ldlt_blocks(35, widths, 8)
+    assert nw >= 2 and widths[0] == 5
+    assert set(entry["ms"]) == {f"{k},{widths[b]}" for b in range(nw) for k in range(1, occ + 1)}
+    k, b = entry["choice"]
+    assert 1 <= k <= occ and b in list(widths)[:nw] and entry["ctas_per_sm"] == k
     assert all(np.isfinite(float(v)) and float(v) > 0 for v in entry["ms"].values())
 
 
@@ -93,6 +102,29 @@ def test_tuning_after_the_first_step_keeps_the_answer(cuda_device, tmp_path):
         torch.cuda.synchronize()
         return a.joint_qd.clone(), solver.contact_solve.newton_iterations_env.clone()
 
-    qd0, it0 = run(None)
-    qd1, it1 = run(2)
+    qd1, it1 = run(2)  # tunes on step 2 (and saves its choice)
+    qd0, it0 = run(2)  # step 2 takes the saved choice without timing
     assert torch.equal(qd0, qd1) and torch.equal(it0, it1)
+
+
+def test_every_ldlt_block_width_reaches_the_tolerance(cuda_device, oracle):
+    """Each LDL^T block width the kernel is built with solves the humanoid
+    batch to the same tolerance: the answers agree with the FP64 oracle
+    like the default width's."""
+    prob = scenes.humanoid_contact_problem(256, seed=84)
+    ref = oracle.solve(prob, "armijo_decay")
+    t = problem_to_device(prob, cuda_device)
+    widths = (ctypes.c_int32 * 8)()
+    nw = load().sapb_contact_solve_ldlt_blocks(35, widths, 8)
+    assert load().sapb_contact_solve_ldlt_blocks(36, widths, 8) >= 1 and widths[0] >= 1
+    nw = load().sapb_contact_solve_ldlt_blocks(35, widths, 8)
+    for prec in ("fp64", "fp32"):
+        for b in list(widths)[:nw]:
+            buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, cuda_device)
+            contact_solve(**t, buffers=buf, options=make_options("armijo_decay", hessian_precision=prec,
+                                                                 linear_solve_precision=prec, ldlt_block=b))
+            torch.cuda.synchronize()
+            assert bool(buf.converged.all()), (prec, b)
+            n = prob.dof_per_env
+            err = np.abs(buf.v.cpu().numpy() - ref["v"]).reshape(-1, n).max(1) / np.abs(ref["v"]).reshape(-1, n).max(1)
+            assert np.quantile(err, 0.98) <= 1e-6 and err.max() <= 1e-4, (prec, b, err.max())
