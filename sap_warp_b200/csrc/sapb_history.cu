@@ -22,7 +22,7 @@
 namespace sapb {
 namespace {
 
-constexpr int kHistThreads = 128;
+constexpr int kHistMaxThreads = 128;  // a CTA per world: one warp per 32 slots, at most four
 constexpr int kHistWindow = 64;
 
 struct Key {
@@ -35,7 +35,8 @@ __device__ __forceinline__ double dist2(const Key& a, const Key& b) {
   return dx * dx + dy * dy + dz * dz;
 }
 
-__global__ void __launch_bounds__(kHistThreads) history_kernel(const sapb_contact_history H) {
+__global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_contact_history H) {
+  const int kHistThreads = blockDim.x;
   extern __shared__ __align__(16) unsigned char smem[];
   const int C = H.max_contacts, e = blockIdx.x;
   Key* prev = reinterpret_cast<Key*>(smem);
@@ -142,7 +143,9 @@ extern "C" int32_t sapb_contact_history_update(const sapb_contact_history* h, vo
   }
   cudaError_t err = cudaFuncSetAttribute(history_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err == cudaSuccess) {
-    history_kernel<<<h->num_envs, kHistThreads, smem, static_cast<cudaStream_t>(stream)>>>(*h);
+    int threads = (h->max_contacts + 31) / 32 * 32;
+    if (threads > kHistMaxThreads) threads = kHistMaxThreads;
+    history_kernel<<<h->num_envs, threads, smem, static_cast<cudaStream_t>(stream)>>>(*h);
     err = cudaGetLastError();
   }
   if (err != cudaSuccess) {
