@@ -19,11 +19,15 @@ state.
 Arms (same scene, same trajectory up to the solve tolerance):
   value        learned + FP32: FP32 Hessian / factorization with FP64
                gradient, cost, line search and convergence test, and the
-               learned warm start (previous impulses and the network's
-               correction tried against the previous velocity);
+               learned warm start (each contact's start impulse: the
+               quadratic extrapolation of its last three solves' impulses
+               where it has that history, the network's prediction where it
+               is new; tried against the previous velocity);
   plain_fp64   the reference's method: FP64 throughout, warm start from the
                previous step's velocity;
-  previous_impulses_fp32   the ablation without the network.
+  previous_impulses_fp32   the ablation without the network;
+  carried_impulses_fp32    the ablation without the network and without
+               extrapolation (the last solve's impulses as they were).
 `e2e` is the headline arm through the public API with host buffers: the
 step's inputs (state and contacts) copied from pinned host memory and the new
 state read back inside the timed region.  `stage2_solve_only` is the contact
@@ -351,12 +355,12 @@ def main():
                      body_f=state0.body_f.clone())
         return a, b
 
-    def make_solver(prec, warm):
+    def make_solver(prec, warm, history=3):
         return SolverSAP(model, max_rigid_contact=MAX_CONTACTS, contact_preset_variant="drake",
                          hessian_precision=prec, warm_start=warm, learned_warm_start=ws if warm == "learned" else None,
-                         autotune=True)
+                         impulse_history=history, autotune=True)
 
-    def run_arm(prec, warm, sampler=None):
+    def run_arm(prec, warm, sampler=None, history=3):
         """Two passes over the same stretch of the rollout (steps warmup ..
         warmup + steps of the same trajectory): eager steps with per-stage
         events and per-step statistics (iterations, chosen starts), then,
@@ -364,7 +368,7 @@ def main():
         graph of two whole steps."""
         pairs = max(args.steps // 2, 1)
         warm_pairs = max((args.warmup + 1) // 2, 1)
-        solver = make_solver(prec, warm)
+        solver = make_solver(prec, warm, history)
         s_in, s_out = fresh_states()
         for _ in range(2 * warm_pairs):
             solver.step(s_in, s_out, control, contacts, DT)
@@ -399,7 +403,7 @@ def main():
         counts = solver.contact_jacobian.contact_env_count.clamp(max=MAX_CONTACTS).cpu().numpy()
         final_eager = s_in.joint_qd.clone()
         # timed: graph replays from the initial state
-        solver = make_solver(prec, warm)
+        solver = make_solver(prec, warm, history)
         g_in, g_out = fresh_states()
         graph = solver.capture_steps(g_in, g_out, control, contacts, DT, warmup=warm_pairs)
         barrier()
@@ -421,6 +425,7 @@ def main():
 
     plain = run_arm("fp64", "previous_velocity")
     prev = run_arm("fp32", "previous_impulses")
+    carried = run_arm("fp32", "previous_impulses", history=1)
     sampler = ClockSampler(local_rank)
     sampler.start()
     fast = run_arm("fp32", "learned", sampler)
@@ -730,7 +735,8 @@ def main():
         "solve_stage_speedup_vs_plain_fp64": plain["stages"].get("contact_solve", float("nan")) / max(
             fast["stages"].get("contact_solve", float("nan")) + fast["stages"].get("warm_start", 0.0), 1e-9),
         "newton_iterations_per_world_step": {"learned_fp32": fast["iters"], "plain_fp64": plain["iters"],
-                                             "previous_impulses_fp32": prev["iters"]},
+                                             "previous_impulses_fp32": prev["iters"],
+                                             "carried_impulses_fp32": carried["iters"]},
         "dtype": "f64 (FP32 Hessian/factor)", "data": "synthetic (seeded rollout scene)",
         "config": {"workload": f"{W} humanoid worlds x 35 DOF (6+29 revolute), 8-32 ground contacts, full "
                                "SolverSAP step (drake preset), armijo_decay to reference tolerances, rollout",
@@ -748,11 +754,15 @@ def main():
                          "ms_per_step_eager": fast["ms_eager"],
                          "graph_replay_matches_eager": fast["graph_matches_eager"],
                          "chosen_start": {"previous_velocity": int(fast["chosen"][0]),
-                                          "carried_impulses_and_network": int(fast["chosen"][1])},
+                                          "history_impulses_and_network": int(fast["chosen"][1])},
                          "stages_ms": fast["stages"], "speedup_vs_plain_fp64": plain["ms"] / fast["ms"],
                          "max_rel_qd_diff_vs_plain_fp64_after_rollout": dq},
         "previous_impulses_fp32": {"value": total / (prev["ms"] * 1e-3), "ms_per_step": prev["ms"],
-                                   "mean_newton_iterations": prev["iters"], "stages_ms": prev["stages"]},
+                                   "mean_newton_iterations": prev["iters"], "stages_ms": prev["stages"],
+                                   "impulse_history": 3},
+        "carried_impulses_fp32": {"value": total / (carried["ms"] * 1e-3), "ms_per_step": carried["ms"],
+                                  "mean_newton_iterations": carried["iters"], "stages_ms": carried["stages"],
+                                  "impulse_history": 1},
         "stage2_solve_only": snap,
         "uneven_batch_solve_only": uneven,
         "box_worlds_solve_only": box_line,

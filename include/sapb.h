@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 9
+#define SAPB_ABI_VERSION 10
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -337,7 +337,18 @@ int32_t sapb_integrate_positions(const sapb_model_desc* model, const double* joi
  * nearest among the pair's contacts, looked for within 64 slots of its own.
  * Slots shift when contacts appear or vanish; with an unchanged contact
  * buffer every slot maps to itself.  One CTA per world; the keys are
- * updated in place (this step's replace the previous step's). */
+ * updated in place (this step's replace the previous step's).
+ *
+ * Start impulses (`order` 2 or 3): along each contact's identity the
+ * history keeps the impulses of up to `order` past steps, and the start is
+ * their polynomial extrapolation to this step -- 2 g1 - g2 from two,
+ * 3 g1 - 3 g2 + g3 from three (g1 the last solve's impulse, g2 the one
+ * before, g3 the one before that), the carried g1 from one, zero for a new
+ * contact.  Impulses of a persistent contact change smoothly from step to
+ * step, so the extrapolation lands nearer this step's solution than g1;
+ * the solve compares the start's cost with the plain start's anyway.  With
+ * order 2 or 3, gamma_hist and has_history are in/out (the previous call's
+ * outputs, by the previous slots) and must persist between calls. */
 typedef struct sapb_contact_history {
   int32_t num_envs;
   int32_t max_contacts;             /* C */
@@ -351,8 +362,12 @@ typedef struct sapb_contact_history {
   double* key_point;                /* [W][C][3] */
   int32_t* key_count;               /* [W] in: previous counts (0 before the first step); out: this step's */
   const double* gamma_prev;         /* [W][C][3] the previous step's impulses by its slots */
-  double* gamma_hist;               /* [W][C][3] out: carried impulses (0 for new contacts) */
-  int32_t* has_history;             /* [W][C] out: 1 carried, 0 new or empty slot */
+  double* gamma_hist;               /* [W][C][3] out: carried impulses g1 (0 for new contacts); order >= 2: in */
+  int32_t* has_history;             /* [W][C] out: past impulses known for the slot's contact, 1..order (1 with
+                                     * order <= 1), 0 new or empty slot; order >= 2: in */
+  int32_t order;                    /* 0 or 1: carried impulses; 2: linear extrapolation; 3: quadratic */
+  double* gamma_older;              /* [W][C][3] order 3: in/out g2 by slot (the impulses two solves back) */
+  double* gamma_start;              /* [W][C][3] out: the start impulses (NULL: not written) */
 } sapb_contact_history;
 
 int32_t sapb_contact_history_update(const sapb_contact_history* hist, void* stream);
@@ -369,7 +384,8 @@ int32_t sapb_contact_history_update(const sapb_contact_history* hist, void* stre
 typedef struct sapb_handle sapb_handle;
 
 #define SAPB_WARM_START_PREVIOUS_VELOCITY 0  /* the reference's: start from the last solution */
-#define SAPB_WARM_START_PREVIOUS_IMPULSES 1  /* also try v* + A^-1 J^T gamma_prev (candidate start) */
+#define SAPB_WARM_START_PREVIOUS_IMPULSES 1  /* also try v* + A^-1 J^T gamma0, gamma0 the start impulses
+                                               * of the contact history (candidate start) */
 #define SAPB_WORK_ORDER_INDEX 0
 #define SAPB_WORK_ORDER_PREVIOUS_ITERATIONS 1  /* most Newton iterations of the last step first */
 
@@ -379,6 +395,8 @@ typedef struct sapb_step_options {
   int32_t position_integration;     /* SAPB_INTEGRATE_SAP_EULER / SAPB_INTEGRATE_MIDPOINT */
   int32_t warm_start;               /* SAPB_WARM_START_* */
   int32_t work_order;               /* SAPB_WORK_ORDER_* */
+  int32_t impulse_history;          /* previous impulses: the contact history's order (1 carried, 2 linear,
+                                     * 3 quadratic extrapolation; 0 = 3) */
 } sapb_step_options;
 
 /* One step's device arrays: the start-of-step state, control and contacts
@@ -393,7 +411,8 @@ typedef struct sapb_step_io {
 
 /* Fill the defaults of SolverSAP's keywords for a drake-preset step
  * (sim/solver_sap.py:749-791): 128 contact slots, armijo_decay, FP64,
- * sap_euler, previous-velocity warm start, work order by previous iterations. */
+ * sap_euler, previous-velocity warm start, work order by previous iterations,
+ * impulse history of order 3. */
 void sapb_step_options_default(sapb_step_options* opts);
 /* Allocate the step's buffers for `model` (device arrays the caller keeps
  * alive while the handle lives); reads the model's index arrays once

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 9
+SAPB_ABI_VERSION = 10
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -329,7 +329,7 @@ SAPB_WORK_ORDER_PREVIOUS_ITERATIONS = 1
 
 class StepOptions(C.Structure):
     _fields_ = [("prepare", PrepareOptions), ("solve", SolveOptions), ("position_integration", C.c_int32),
-                ("warm_start", C.c_int32), ("work_order", C.c_int32)]
+                ("warm_start", C.c_int32), ("work_order", C.c_int32), ("impulse_history", C.c_int32)]
 
 
 class StepIO(C.Structure):
@@ -340,7 +340,8 @@ class ContactHistory(C.Structure):
     _fields_ = [("num_envs", C.c_int32), ("max_contacts", C.c_int32), ("num_flat", C.c_int32),
                 ("contact_count", _p), ("contact_source", _p), ("flat_shape0", _p), ("flat_shape1", _p),
                 ("flat_point1", _p), ("key_shape", _p), ("key_point", _p), ("key_count", _p), ("gamma_prev", _p),
-                ("gamma_hist", _p), ("has_history", _p)]
+                ("gamma_hist", _p), ("has_history", _p), ("order", C.c_int32), ("gamma_older", _p),
+                ("gamma_start", _p)]
 
 
 # name -> (restype, argtypes) of every symbol include/sapb.h declares.

@@ -10,7 +10,12 @@
 // the impulse of the previous slot with the same pair whose point is the
 // nearest to its own, provided that it is also the nearest of this step's
 // slots to that previous contact (mutual nearest, searched within 64 slots
-// of each side); then this step's keys replace the previous ones.  No
+// of each side); then this step's keys replace the previous ones.  With an
+// order of 2 or 3 the slots also carry the impulses of the steps before
+// (the previous call's carried impulses and their predecessors, by the
+// previous slots), and the start impulse is the polynomial through the last
+// `order` impulses of the contact evaluated one step on: 2 g1 - g2 (linear),
+// 3 g1 - 3 g2 + g3 (quadratic), g1 with one known, 0 for a new contact.  No
 // counterpart in the reference, whose warm start is the previous velocity.
 #include <cuda_runtime.h>
 
@@ -24,6 +29,7 @@ namespace {
 
 constexpr int kHistMaxThreads = 128;  // a CTA per world: one warp per 32 slots, at most four
 constexpr int kHistWindow = 64;
+constexpr int kHistMaxOrder = 3;
 
 struct Key {
   int s0, s1;
@@ -41,6 +47,12 @@ __global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_con
   const int C = H.max_contacts, e = blockIdx.x;
   Key* prev = reinterpret_cast<Key*>(smem);
   Key* cur = prev + C;
+  const int order = H.order < 1 ? 1 : (H.order > kHistMaxOrder ? kHistMaxOrder : H.order);
+  // order >= 2: the previous call's carried impulses (and order 3: the ones
+  // before them) and known-impulse counts, staged before any slot is rewritten
+  double* pg1 = reinterpret_cast<double*>(cur + C);
+  double* pg2 = pg1 + 3 * C;
+  int* pdepth = reinterpret_cast<int*>(pg2 + 3 * C);
   int np = H.key_count[e];
   np = np < 0 ? 0 : (np > C ? C : np);
   int nc = H.contact_count[e];
@@ -54,6 +66,14 @@ __global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_con
     k.y = H.key_point[3 * (base + c) + 1];
     k.z = H.key_point[3 * (base + c) + 2];
     prev[c] = k;
+    if (order >= 2) {
+      const int d = H.has_history[base + c];
+      pdepth[c] = d < 0 ? 0 : (d > order ? order : d);
+      for (int r = 0; r < 3; ++r) {
+        pg1[3 * c + r] = H.gamma_hist[3 * (base + c) + r];
+        pg2[3 * c + r] = order >= 3 ? H.gamma_older[3 * (base + c) + r] : 0.0;
+      }
+    }
   }
   for (int c = threadIdx.x; c < nc; c += kHistThreads) {
     const int src = H.contact_source[base + c];
@@ -98,17 +118,35 @@ __global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_con
       }
     }
     const size_t s = base + c;
+    // g1: the last solve's impulse; g2, g3: the ones before (known when the
+    // matched previous slot knew them)
+    double g1[3] = {0.0, 0.0, 0.0}, g2[3] = {0.0, 0.0, 0.0}, g3[3] = {0.0, 0.0, 0.0};
+    int depth = 0;
     if (best >= 0) {
       const size_t ps = base + best;
-      H.gamma_hist[3 * s] = H.gamma_prev[3 * ps];
-      H.gamma_hist[3 * s + 1] = H.gamma_prev[3 * ps + 1];
-      H.gamma_hist[3 * s + 2] = H.gamma_prev[3 * ps + 2];
-    } else {
-      H.gamma_hist[3 * s] = 0.0;
-      H.gamma_hist[3 * s + 1] = 0.0;
-      H.gamma_hist[3 * s + 2] = 0.0;
+      for (int r = 0; r < 3; ++r) g1[r] = H.gamma_prev[3 * ps + r];
+      depth = 1;
+      if (order >= 2) {
+        depth = pdepth[best] + 1 < order ? pdepth[best] + 1 : order;
+        for (int r = 0; r < 3; ++r) {
+          g2[r] = pg1[3 * best + r];
+          g3[r] = pg2[3 * best + r];
+        }
+      }
     }
-    if (H.has_history) H.has_history[s] = best >= 0 ? 1 : 0;
+    for (int r = 0; r < 3; ++r) {
+      H.gamma_hist[3 * s + r] = g1[r];
+      if (order >= 3) H.gamma_older[3 * s + r] = depth >= 2 ? g2[r] : 0.0;
+    }
+    if (H.has_history) H.has_history[s] = depth;
+    if (H.gamma_start) {
+      for (int r = 0; r < 3; ++r) {
+        double g = g1[r];  // depth 1 (0 for a new contact)
+        if (depth == 2) g = 2.0 * g1[r] - g2[r];
+        else if (depth == 3) g = 3.0 * g1[r] - 3.0 * g2[r] + g3[r];
+        H.gamma_start[3 * s + r] = g;
+      }
+    }
   }
   __syncthreads();  // every slot has read the previous keys
   for (int c = threadIdx.x; c < nc; c += kHistThreads) {
@@ -128,15 +166,16 @@ __global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_con
 using namespace sapb;
 
 extern "C" int32_t sapb_contact_history_update(const sapb_contact_history* h, void* stream) {
-  if (!h || h->num_envs < 0 || h->max_contacts < 1 || h->num_flat < 0 ||
+  if (!h || h->num_envs < 0 || h->max_contacts < 1 || h->num_flat < 0 || h->order < 0 || h->order > kHistMaxOrder ||
       (h->num_envs > 0 && (!h->contact_count || !h->contact_source || !h->key_shape || !h->key_point ||
                            !h->key_count || !h->gamma_prev || !h->gamma_hist ||
+                           (h->order >= 2 && !h->has_history) || (h->order >= 3 && !h->gamma_older) ||
                            (h->num_flat > 0 && (!h->flat_shape0 || !h->flat_shape1 || !h->flat_point1))))) {
     set_last_error("sapb_contact_history_update: invalid argument");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   if (h->num_envs == 0) return SAPB_OK;
-  const size_t smem = sizeof(Key) * 2 * (size_t)h->max_contacts;
+  const size_t smem = (sizeof(Key) * 2 + sizeof(double) * 6 + sizeof(int)) * (size_t)h->max_contacts;
   if (smem > kMaxSmemPerBlock) {
     set_last_error("sapb_contact_history_update: %d slots per world exceed shared memory", h->max_contacts);
     return SAPB_ERR_UNSUPPORTED;

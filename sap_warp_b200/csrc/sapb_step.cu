@@ -82,9 +82,10 @@ struct sapb_handle {
   int32_t *count, *body0, *body1, *truncated;
   void* prep_ws;
   size_t prep_ws_bytes;
-  // contact history (previous-impulse warm start): keys, carried impulses
+  // contact history (previous-impulse warm start): keys, carried impulses,
+  // the impulses before them, the extrapolated start impulses
   int32_t *source, *key_shape, *key_count, *has_history;
-  double *key_point, *gamma_last;
+  double *key_point, *gamma_last, *gamma_older, *gamma_start;
   // solve
   double *v, *gamma, *gamma_prev, *cost, *grad_norm;
   int32_t *mode, *iters, *ls_iters, *converged, *status, *ws_accepted, *guess_flag, *order;
@@ -135,6 +136,7 @@ void sapb_step_options_default(sapb_step_options* o) {
   o->position_integration = SAPB_INTEGRATE_SAP_EULER;
   o->warm_start = SAPB_WARM_START_PREVIOUS_VELOCITY;
   o->work_order = SAPB_WORK_ORDER_PREVIOUS_ITERATIONS;
+  o->impulse_history = 3;
 }
 
 void sapb_destroy(sapb_handle* h) {
@@ -143,7 +145,8 @@ void sapb_destroy(sapb_handle* h) {
                   h->vc_star, h->count, h->body0, h->body1, h->truncated, h->prep_ws, h->v, h->gamma,
                   h->gamma_prev, h->cost, h->grad_norm, h->mode, h->iters, h->ls_iters, h->converged, h->status,
                   h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws,
-                  h->source, h->key_shape, h->key_count, h->has_history, h->key_point, h->gamma_last};
+                  h->source, h->key_shape, h->key_count, h->has_history, h->key_point, h->gamma_last,
+                  h->gamma_older, h->gamma_start};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -173,6 +176,10 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   }
   if (opts->warm_start != SAPB_WARM_START_PREVIOUS_VELOCITY && opts->warm_start != SAPB_WARM_START_PREVIOUS_IMPULSES) {
     set_last_error("sapb_create: warm_start must be SAPB_WARM_START_PREVIOUS_VELOCITY or _PREVIOUS_IMPULSES");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (opts->impulse_history < 0 || opts->impulse_history > 3) {
+    set_last_error("sapb_create: impulse_history must be 0 (default), 1, 2 or 3");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   if (opts->work_order == SAPB_WORK_ORDER_PREVIOUS_ITERATIONS && W > kOrderMaxWorlds) {
@@ -223,6 +230,7 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   memset(h, 0, sizeof(*h));
   h->model = *model;
   h->opts = *opts;
+  if (h->opts.impulse_history == 0) h->opts.impulse_history = 3;
   h->W = W;
   h->n = n;
   h->C = C;
@@ -257,6 +265,8 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     take(dev_alloc(&h->key_point, WC * 3));
     take(dev_alloc(&h->key_count, W));
     take(dev_alloc(&h->has_history, WC));
+    take(dev_alloc(&h->gamma_older, WC * 3));
+    take(dev_alloc(&h->gamma_start, WC * 3));
   }
   take(dev_alloc(&h->v, Wn));
   take(dev_alloc(&h->gamma, WC * 3));
@@ -284,6 +294,9 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_prev, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_last, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess && cand) err = cudaMemset(h->key_count, 0, sizeof(int32_t) * W);
+  if (err == cudaSuccess && cand) err = cudaMemset(h->has_history, 0, sizeof(int32_t) * WC);
+  if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_older, 0, sizeof(double) * WC * 3);
+  if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_start, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess) err = cudaMemset(h->iters, 0, sizeof(int32_t) * W);
   if (err == cudaSuccess) {
     std::vector<int32_t> idx(W);
@@ -333,7 +346,7 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   int32_t st = sapb_free_motion_contacts(&h->model, &io->in, &h->opts.prepare, &po, h->prep_ws, h->prep_ws_bytes,
                                          stream);
   if (st != SAPB_OK) return st;
-  if (cand) {  // the last solve's impulses carried to this step's slots by contact identity
+  if (cand) {  // the last solves' impulses carried to this step's slots by contact identity, extrapolated
     sapb_contact_history hist;
     memset(&hist, 0, sizeof(hist));
     hist.num_envs = h->W;
@@ -350,6 +363,9 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     hist.gamma_prev = h->gamma_last;
     hist.gamma_hist = h->gamma_prev;
     hist.has_history = h->has_history;
+    hist.order = h->opts.impulse_history;
+    hist.gamma_older = h->gamma_older;
+    hist.gamma_start = h->gamma_start;
     st = sapb_contact_history_update(&hist, stream);
     if (st != SAPB_OK) return st;
   }
@@ -388,7 +404,7 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     p.dof = &dof_local;
   }
   if (cand) {
-    p.gamma0 = h->gamma_prev;
+    p.gamma0 = h->gamma_start;
     p.gamma0_count = 1;
     p.dynamics_factor = h->factor;
   }

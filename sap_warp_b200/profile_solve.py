@@ -9,7 +9,8 @@ snapshot: the stage-2 solve alone on the batched humanoid problem (A, J
 given): warm-up launches, then `--launches` timed launches.
 rollout: SolverSAP steps (drake preset) of the humanoid rollout scene with
 the given warm start and Hessian precision: `--steps` steps, the last half
-timed.  boxes: the tree-blocked solve alone on worlds of 64 free boxes
+timed, after `--settle` steps of a plain FP64 solver (the bench's settling
+prefix).  boxes: the tree-blocked solve alone on worlds of 64 free boxes
 (scenes.box_stack_problem).  Each prints the mean time per launch / step.  Used as the target
 command of ncu captures (select a kernel with `-k regex:...` and skip the
 warm-up launches with `-s`).
@@ -72,6 +73,12 @@ def rollout(args, dev) -> None:
                        warm_start=args.warm_start)
     other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
                      body_f=state.body_f.clone())
+    if args.settle > 0:
+        settler = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp64")
+        for _ in range(args.settle):
+            settler.step(state, other, control, contacts, 2.0e-3)
+            state, other = other, state
+        del settler
     half = max(args.steps // 2, 1)
     for _ in range(args.steps - half):
         solver.step(state, other, control, contacts, 2.0e-3)
@@ -95,6 +102,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--launches", type=int, default=5)
     ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--settle", type=int, default=0,
+                    help="rollout: untimed steps of a plain FP64 solver first (its solve launches come first)")
     ap.add_argument("--warm-start", default="learned",
                     choices=["previous_velocity", "previous_impulses", "learned"])
     ap.add_argument("--seed", type=int, default=2)

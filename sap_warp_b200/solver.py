@@ -790,28 +790,33 @@ class SolverSAP:
                  static_substep: bool = False, static_substep_iterations: int = 8,
                  static_substep_line_search_iterations: int = 6, position_integration: str | None = None,
                  hessian_precision: str | None = None, warm_start: str = "previous_velocity",
-                 learned_warm_start=None, learned_candidates: str = "new_contacts", tree_blocked: bool | None = None,
+                 learned_warm_start=None, learned_candidates: str = "new_contacts", impulse_history: int = 3,
+                 tree_blocked: bool | None = None,
                  work_order: str = "previous_iterations", autotune: bool | str | os.PathLike | None = None):
         """Keyword arguments of the reference's SolverSAP (sim/solver_sap.py:
         749-791) plus: hessian_precision ("fp64" / "fp32": J^T G J assembly and
         factorization precision; the gradient, cost, line search and
         convergence test stay FP64); warm_start, one of
           "previous_velocity"  the reference's: start from the last solution;
-          "previous_impulses"  also try v* + A^-1 J^T gamma_prev;
+          "previous_impulses"  also try v* + A^-1 J^T gamma0, gamma0 the
+                               start impulses of the contact history;
           "learned"            also try starts from the per-contact network
                                (learned_warm_start: a LearnedWarmStart, a
                                weights path, or None for the packaged
                                weights); learned_candidates "new_contacts"
                                (default): one start v* + A^-1 J^T gamma0 with
-                               gamma0 the carried impulse where the contact
-                               existed last step and the network's where it
-                               is new (tiles without a new contact skip the
-                               network); "all_contacts": two starts, the
-                               network's gamma0 on every contact and the
-                               carried impulses;
+                               gamma0 the history's start impulse where the
+                               contact existed last step and the network's
+                               where it is new (tiles without a new contact
+                               skip the network); "all_contacts": two starts,
+                               the network's gamma0 on every contact and the
+                               history's start impulses;
         previous impulses are carried to this step's contact slots by
         contact identity (shape pair and witness point), so slots may shift
-        as contacts appear and vanish;
+        as contacts appear and vanish; impulse_history (1, 2 or 3, default
+        3): how many past impulses of each contact make its start impulse --
+        1 the last one, 2 their linear extrapolation to this step, 3 the
+        quadratic one (fewer where the contact is younger);
         the lowest-cost start among the previous-velocity one and the
         candidates is taken, and Newton always runs to the same tolerance;
         work_order ("previous_iterations", the default, or "index"): the
@@ -925,15 +930,22 @@ class SolverSAP:
                 lw = LearnedWarmStart.load(DEFAULT_WEIGHTS if lw is None else str(lw), dev)
             self.learned_warm_start = lw
         C = self.max_rigid_contact
-        # candidate impulse sets: [0] the network's, [1] the previous step's
+        self.impulse_history = int(impulse_history)
+        if self.impulse_history not in (1, 2, 3):
+            raise ValueError(f"impulse_history must be 1, 2 or 3, got {impulse_history!r}.")
+        # candidate impulse sets: [0] the network's, [1] the history's start
         # impulses (evaluated last: it is the usual winner, and the last
         # candidate's evaluation seeds the first Newton iteration)
         self._gamma_cand = torch.zeros(2, view.W, max(C, 1), 3, dtype=F64, device=dev)
-        # [1] holds the previous step's impulses carried to this step's slots
-        # by contact identity (sapb_contact_history_update), from the last
-        # solve's impulses by its own slots (_gamma_last)
+        # [1] holds the start impulses of this step's slots: the last solves'
+        # impulses carried by contact identity (sapb_contact_history_update)
+        # from the last solve's impulses by its own slots (_gamma_last) and
+        # extrapolated over the impulses before them (_gamma_carried: the
+        # last solve's by this step's slots, _gamma_older: the one before)
         self._gamma_prev = self._gamma_cand[1]
         self._gamma_last = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
+        self._gamma_carried = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
+        self._gamma_older = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
         if self.warm_start != "previous_velocity":
             self._hist_key_shape = torch.zeros(view.W, max(C, 1), 2, dtype=I32, device=dev)
@@ -974,7 +986,7 @@ class SolverSAP:
         """This solver's configuration as the options of the C step handle
         (sapb_create / sapb_step): the same contact preparation, solve
         options, integrator, warm start (previous velocity or previous
-        impulses) and work order, so a C host stepping the same model gets
+        impulses, with the same impulse history) and work order, so a C host stepping the same model gets
         the same trajectory."""
         if self.contact_solve.tree_blocked:
             raise NotImplementedError("the C step handle runs the dense layout")
@@ -998,6 +1010,7 @@ class SolverSAP:
                         else _abi.SAPB_WARM_START_PREVIOUS_VELOCITY)
         o.work_order = (_abi.SAPB_WORK_ORDER_PREVIOUS_ITERATIONS if self.work_order == "previous_iterations"
                         else _abi.SAPB_WORK_ORDER_INDEX)
+        o.impulse_history = self.impulse_history
         return o
 
     def capture_steps(self, state_a: SapState, state_b: SapState, control: SapControl | None, contacts, dt,
@@ -1120,8 +1133,11 @@ class SolverSAP:
         if hasattr(self, "_gamma_cand"):
             self._gamma_cand.zero_()
             self._gamma_last.zero_()
+            self._gamma_carried.zero_()
+            self._gamma_older.zero_()
         if hasattr(self, "_hist_key_count"):
             self._hist_key_count.zero_()
+            self.has_history.zero_()
         if hasattr(self, "_world_order"):
             torch.arange(self.view.W, dtype=I32, device=self.view.device, out=self._world_order)
         self.last_contacts = None
@@ -1164,9 +1180,13 @@ class SolverSAP:
             gamma0 = self._gamma_prev
         elif self.warm_start == "learned":
             self._normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
+            # new_contacts: slots with history keep their start impulse;
+            # all_contacts: the network corrects the carried impulses
             self.learned_warm_start.predict(
                 num_envs=self.view.W, dof_per_env=self.view.n, max_contacts=self.max_rigid_contact,
-                normal_up=self._normal_up, gamma_prev=self._gamma_prev, out=self._gamma_cand[0],
+                normal_up=self._normal_up,
+                gamma_prev=self._gamma_prev if self.learned_candidates == "new_contacts" else self._gamma_carried,
+                out=self._gamma_cand[0],
                 vc_star=self.contact_jacobian.contact_env_vc_star,
                 contact_count=cr.contact_env_count, dynamics_matrix=cr.dynamics_matrix_env,
                 jacobian=cr.contact_env_jacobian, phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff,
@@ -1224,9 +1244,11 @@ class SolverSAP:
         return state_out
 
     def _carry_impulses(self, cr: SapContactJacobianResult) -> None:
-        """The last solve's impulses carried to this step's contact slots by
-        contact identity (shape pair + shape1 witness point), into
-        _gamma_prev; has_history marks the slots that found their contact."""
+        """The last solves' impulses carried to this step's contact slots by
+        contact identity (shape pair + shape1 witness point) and extrapolated
+        over impulse_history steps, into _gamma_prev (the start impulses);
+        has_history counts the past impulses known for each slot's contact
+        (0: new)."""
         cj = self.contact_jacobian
         inp = cj._inputs
         H = _abi.ContactHistory()
@@ -1236,8 +1258,9 @@ class SolverSAP:
         H.flat_shape0, H.flat_shape1, H.flat_point1 = inp.contact_shape0, inp.contact_shape1, inp.contact_point1
         H.key_shape, H.key_point = _ptr(self._hist_key_shape), _ptr(self._hist_key_point)
         H.key_count = _ptr(self._hist_key_count)
-        H.gamma_prev, H.gamma_hist, H.has_history = _ptr(self._gamma_last), _ptr(self._gamma_prev), _ptr(
+        H.gamma_prev, H.gamma_hist, H.has_history = _ptr(self._gamma_last), _ptr(self._gamma_carried), _ptr(
             self.has_history)
+        H.order, H.gamma_older, H.gamma_start = self.impulse_history, _ptr(self._gamma_older), _ptr(self._gamma_prev)
         check(load().sapb_contact_history_update(
             ctypes.byref(H), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)),
             "sapb_contact_history_update")

@@ -66,7 +66,7 @@ def test_no_compute_entry_points_without_gpu(lib):
     so = _abi.StepOptions()
     lib.sapb_step_options_default(ctypes.byref(so))
     assert so.prepare.max_contacts == 128 and so.solve.line_search_variant == _abi.SAPB_LS_ARMIJO_DECAY
-    assert so.work_order == _abi.SAPB_WORK_ORDER_PREVIOUS_ITERATIONS
+    assert so.work_order == _abi.SAPB_WORK_ORDER_PREVIOUS_ITERATIONS and so.impulse_history == 3
     assert lib.sapb_create(None, ctypes.byref(so), None) == _abi.SAPB_ERR_INVALID_ARGUMENT
     assert lib.sapb_step(None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
     assert lib.sapb_get_status(None, None, None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
@@ -90,6 +90,8 @@ def test_struct_layout_matches_header(tmp_path):
         " printf(\"%zu %zu\\n\", sizeof(sapb_blocked_problem), offsetof(sapb_blocked_problem, world_order));"
         " printf(\"%zu %zu %zu %zu\\n\", sizeof(sapb_step_options), offsetof(sapb_step_options, work_order),"
         " sizeof(sapb_step_io), offsetof(sapb_step_io, joint_qd_out));"
+        " printf(\"%zu %zu %zu %zu\\n\", sizeof(sapb_contact_history), offsetof(sapb_contact_history, order),"
+        " offsetof(sapb_contact_history, gamma_start), offsetof(sapb_step_options, impulse_history));"
         " return 0;}\n"
     )
     exe = tmp_path / "sizes"
@@ -103,5 +105,6 @@ def test_struct_layout_matches_header(tmp_path):
             ctypes.sizeof(_abi.MlpTrainBuffers), ctypes.sizeof(_abi.AdamOptions), _abi.ContactProblem.gamma0.offset,
             ctypes.sizeof(_abi.BlockedProblem), _abi.BlockedProblem.world_order.offset,
             ctypes.sizeof(_abi.StepOptions), _abi.StepOptions.work_order.offset, ctypes.sizeof(_abi.StepIO),
-            _abi.StepIO.joint_qd_out.offset]
+            _abi.StepIO.joint_qd_out.offset, ctypes.sizeof(_abi.ContactHistory), _abi.ContactHistory.order.offset,
+            _abi.ContactHistory.gamma_start.offset, _abi.StepOptions.impulse_history.offset]
     assert got == want

@@ -21,11 +21,12 @@ pytestmark = pytest.mark.gpu
 
 
 class _Hist:
-    def __init__(self, W, C, dev):
+    def __init__(self, W, C, dev, order=1):
         z = lambda *s, dt=torch.float64: torch.zeros(*s, dtype=dt, device=dev)
-        self.W, self.C = W, C
+        self.W, self.C, self.order = W, C, order
         self.key_shape, self.key_point, self.key_count = z(W, C, 2, dt=torch.int32), z(W, C, 3), z(W, dt=torch.int32)
         self.gamma_hist, self.has = z(W, C, 3), z(W, C, dt=torch.int32)
+        self.gamma_older, self.gamma_start = z(W, C, 3), z(W, C, 3)
 
     def update(self, counts, source, s0, s1, p1, gamma_prev):
         H = _abi.ContactHistory()
@@ -36,6 +37,7 @@ class _Hist:
                                                  self.key_count.data_ptr())
         H.gamma_prev, H.gamma_hist, H.has_history = gamma_prev.data_ptr(), self.gamma_hist.data_ptr(), \
             self.has.data_ptr()
+        H.order, H.gamma_older, H.gamma_start = self.order, self.gamma_older.data_ptr(), self.gamma_start.data_ptr()
         check(load().sapb_contact_history_update(ctypes.byref(H), None), "sapb_contact_history_update")
         torch.cuda.synchronize()
 
@@ -81,6 +83,40 @@ def test_history_follows_contacts_across_slot_shifts(cuda_device):
     np.testing.assert_array_equal(gh[1, 0], gp[1, 1])
     np.testing.assert_array_equal(gh[1, 1], gp[1, 0])
     np.testing.assert_array_equal(h.key_count.cpu().numpy(), [4, 2])
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_start_impulses_extrapolate_each_contacts_history(cuda_device, order):
+    """Three solves' impulses along each contact's identity, through slot
+    shifts: the start is the carried impulse (1 known), 2 g1 - g2 (2 known),
+    3 g1 - 3 g2 + g3 (3 known), capped at the order; a contact that vanished
+    for a step starts its history again; new contacts start at zero."""
+    h = _Hist(1, 8, cuda_device, order=order)
+    A, B, Cc, D = (1, 10, (0, 0, 0)), (1, 11, (1, 0, 0)), (1, 12, (2, 0, 0)), (1, 13, (3, 0, 0))
+    # the contact sets of steps 0..3 (slots follow list order)
+    steps = [[A, B, Cc], [D, A, B, Cc], [A, Cc, D], [B, A, Cc, D]]
+    rng = np.random.default_rng(order)
+    sol = {}  # contact -> list of its solves' impulses, most recent last
+    gamma_prev = torch.zeros(1, 8, 3, dtype=torch.float64, device=cuda_device)
+    prev_list = []
+    for k, cur in enumerate(steps):
+        h.update(*_flat(cuda_device, [cur]), gamma_prev)
+        start, has = h.gamma_start.cpu().numpy()[0], h.has.cpu().numpy()[0]
+        for slot, c in enumerate(cur):
+            past = sol.get(c, []) if c in prev_list else []
+            depth = min(len(past), order)
+            assert has[slot] == depth, (k, slot, has[slot], depth)
+            g = [np.asarray(x) for x in past[::-1]]  # g1, g2, g3
+            want = np.zeros(3) if depth == 0 else g[0] if depth == 1 else \
+                2.0 * g[0] - g[1] if depth == 2 else 3.0 * g[0] - 3.0 * g[1] + g[2]
+            np.testing.assert_allclose(start[slot], want, rtol=0, atol=1e-12)
+        assert np.all(start[len(cur):] == 0.0) and np.all(has[len(cur):] == 0)
+        # this step's solve: a new impulse per live contact; a contact absent
+        # at this step loses its history
+        g = rng.normal(size=(8, 3))
+        gamma_prev = torch.as_tensor(g[None], device=cuda_device).contiguous()
+        sol = {c: (sol.get(c, []) if c in prev_list else []) + [g[slot]] for slot, c in enumerate(cur)}
+        prev_list = list(cur)
 
 
 def test_site_scene_contacts_match_the_restatement(cuda_device):
