@@ -54,9 +54,9 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one contact
 # solve launch of the headline arm on this workload (4096 humanoids, learned
-# start, FP32 Hessian; step 7 of the rollout), from one ncu capture:
-# 175.93 MB read + 15.12 MB written.
-NCU_SOLVE_TRAFFIC_BYTES = 191_042_560
+# start, FP32 Hessian; the fifth step after the 100-step settling prefix),
+# from one ncu capture: 167.60 MB read + 9.28 MB written.
+NCU_SOLVE_TRAFFIC_BYTES = 176_878_592
 
 METRIC = "world-steps/s, 4096 humanoids: learned+FP32 vs plain FP64, same B200, same tol"
 WORLDS = 4096
