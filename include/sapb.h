@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 10
+#define SAPB_ABI_VERSION 11
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -176,6 +176,17 @@ typedef struct sapb_contact_problem {
    * permutation of 0..E-1, e.g. by descending estimated work for uneven
    * batches); entries outside [0, E) are skipped.  NULL: index order. */
   const int32_t* world_order;
+  /* Candidate start velocities [K][E*n] back to back (v_candidate_count <= 1
+   * means one), or NULL: each is taken on the participating DOFs (v* on the
+   * others) and tried like the impulse candidates, before them -- e.g. the
+   * v_start output of sapb_free_motion_contacts.  Chosen-start numbering:
+   * 0 plain, 1..K the velocity candidates, K+1.. the impulse sets. */
+  const double* v_candidates;
+  int32_t v_candidate_count;
+  /* Optional [E*n] base velocity of the impulse candidates: v_c = base +
+   * A^-1 J^T gamma_c (NULL: base = v*).  A world whose candidate impulses are
+   * all zero then starts at the base without reading dynamics_factor. */
+  const double* gamma0_base;
 } sapb_contact_problem;
 
 /* Outputs: the SapContactSolveResult fields a caller reads
@@ -190,7 +201,8 @@ typedef struct sapb_solve_outputs {
   int32_t* converged;             /* [E] 1 if optimality or cost test met */
   int32_t* status;                /* [E] last line-search status (0 or SAPB_LS_*) */
   double* grad_norm;              /* [E] ||D^-1/2 grad|| over participating DOFs */
-  int32_t* warm_start_accepted;   /* [E] chosen start: 0 plain, k = candidate set k (NULL: not written) */
+  int32_t* warm_start_accepted;   /* [E] chosen start: 0 plain, then the velocity candidates, then the impulse
+                                   * sets, counted from 1 (NULL: not written) */
 } sapb_solve_outputs;
 
 /* ---- free motion + contact Jacobian ---------------------------------------
@@ -269,12 +281,19 @@ typedef struct sapb_prepare_options {
    * counterpart in the reference, which keeps such worlds dense
    * (sim/contact_jacobian.py:110-150, 404-562).  At most 64 bodies. */
   int32_t tree_blocked;
+  /* Nonzero (with a history whose has_history marks new contacts): write
+   * dynamics_factor only for worlds with a new contact in a live slot, the
+   * only worlds whose network-predicted impulses need it; other worlds'
+   * factors are left unwritten. */
+  int32_t factor_new_contacts_only;
 } sapb_prepare_options;
 
 /* Outputs: SapFreeMotionResult (sim/free_motion.py:63-68) and the
  * SapContactJacobianResult arrays the contact solve reads
  * (sim/contact_jacobian.py:51-84).  Any pointer but v_star,
  * dynamics_matrix, jacobian and the contact arrays may be NULL. */
+struct sapb_contact_history;
+
 typedef struct sapb_prepare_outputs {
   double* v_star;                   /* [dofs] */
   double* vdot;                     /* [dofs] */
@@ -298,6 +317,17 @@ typedef struct sapb_prepare_outputs {
   double* tree_mass;                /* [W][B][6][6] diagonal blocks of A (tree_blocked only) */
   int32_t* contact_tree;            /* [W][C][2] tree of each contact side, -1 static (tree_blocked only) */
   int32_t* contact_source;          /* [W][C] flat contact index of each slot, -1 past the world's count, or NULL */
+  /* The contact history (sapb_contact_history_update), run by this launch
+   * between the contact scatter and the free motion, on this launch's slots
+   * and contact buffer: its num_envs, max_contacts, num_flat, contact_count,
+   * contact_source and flat_* fields are ignored (filled here), the others
+   * are as sapb_contact_history documents.  NULL: no history. */
+  const struct sapb_contact_history* history;
+  /* [W][n] the candidate start v* + A^-1 J^T gamma_start of each world
+   * (gamma_start of the history by this launch's slots; FP64, through the
+   * free motion's own LDL^T), or NULL.  Dense layout; needs history with
+   * gamma_start. */
+  double* v_start;
 } sapb_prepare_outputs;
 
 /* Device workspace bytes of sapb_free_motion_contacts. */

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 10
+SAPB_ABI_VERSION = 11
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -122,6 +122,9 @@ class ContactProblem(C.Structure):
         ("gamma0_count", C.c_int32),
         ("dynamics_factor", _p),
         ("world_order", _p),
+        ("v_candidates", _p),
+        ("v_candidate_count", C.c_int32),
+        ("gamma0_base", _p),
     ]
 
 
@@ -265,6 +268,7 @@ class PrepareOptions(C.Structure):
         ("fallback_stiffness", C.c_double),
         ("fallback_tau_d", C.c_double),
         ("tree_blocked", C.c_int32),
+        ("factor_new_contacts_only", C.c_int32),
     ]
 
 
@@ -291,6 +295,8 @@ class PrepareOutputs(C.Structure):
         ("tree_mass", _p),
         ("contact_tree", _p),
         ("contact_source", _p),
+        ("history", _p),
+        ("v_start", _p),
     ]
 
 

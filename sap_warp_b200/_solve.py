@@ -146,6 +146,9 @@ def build_problem(
     dof_terms: DofTermArrays | None = None,
     gamma0: torch.Tensor | None = None,
     world_order: torch.Tensor | None = None,
+    v_candidates: torch.Tensor | None = None,
+    gamma0_base: torch.Tensor | None = None,
+    dynamics_factor: torch.Tensor | None = None,
 ) -> _abi.ContactProblem:
     """sapb_contact_problem over device tensors (shapes and dtypes checked)."""
     E, n, C = num_envs, dof_per_env, max_contacts
@@ -173,6 +176,11 @@ def build_problem(
     if gamma0 is not None:
         P.gamma0_count = int(gamma0.numel() // (3 * max(E * C, 1)))
     P.world_order = _ptr(world_order, I32, E, "world_order")
+    P.v_candidates = _ptr(v_candidates, F64, E * n, "v_candidates")
+    if v_candidates is not None:
+        P.v_candidate_count = int(v_candidates.numel() // max(E * n, 1))
+    P.gamma0_base = _ptr(gamma0_base, F64, E * n, "gamma0_base")
+    P.dynamics_factor = _ptr(dynamics_factor, F64, E * n * n, "dynamics_factor")
     if dof_terms is not None:
         P.dof = ctypes.pointer(dof_terms.struct)
     return P
@@ -190,7 +198,9 @@ def contact_solve(
     `arrays` are the keyword tensors of `build_problem` (contact_count,
     dynamics_matrix, jacobian, phi0, w_eff, mu, stiffness, tau_d, v_star, v0,
     dt and the optional body maps, v_guess, v_guess_active, dof_terms and the
-    candidate starting impulses gamma0, (E, C, 3) or (K, E, C, 3), and the
+    candidate starting impulses gamma0, (E, C, 3) or (K, E, C, 3), their
+    base velocity gamma0_base (E*n), the candidate start velocities
+    v_candidates, (E*n) or (K, E*n), the LDL^T dynamics_factor and the
     persistent kernel's world_order)."""
     lib = load()
     b = buffers

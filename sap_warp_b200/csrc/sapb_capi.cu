@@ -84,6 +84,10 @@ int32_t sapb_contact_solve(const sapb_contact_problem* p, const sapb_solve_optio
                          p->dof_per_env, p->max_contacts);
     return SAPB_ERR_INVALID_ARGUMENT;
   }
+  if (p->gamma0_count < 0 || p->v_candidate_count < 0) {
+    sapb::set_last_error("sapb_contact_solve: negative candidate count");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
   if (p->dof_per_env > 60) {
     sapb::set_last_error("sapb_contact_solve: dof_per_env=%d > 60 is not supported by the on-chip solve",
                          p->dof_per_env);

@@ -510,6 +510,15 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
           asm volatile("prefetch.global.L2 [%0];" ::"l"(a0 + off));
         for (size_t off = (size_t)tid * 128; off < jbytes; off += (size_t)NT * 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(j0 + off));
+        if (P.p.v_candidates) {
+          const int KV = P.p.v_candidate_count > 1 ? P.p.v_candidate_count : 1;
+          const size_t vbytes = sizeof(double) * (size_t)n;
+          for (int k = 0; k < KV; ++k) {
+            const char* v0p = reinterpret_cast<const char*>(P.p.v_candidates + ((size_t)k * P.p.num_envs + nx) * n);
+            for (size_t off = (size_t)tid * 128; off < vbytes; off += (size_t)NT * 128)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(v0p + off));
+          }
+        }
         if (P.p.gamma0) {
           if (P.p.dynamics_factor) {
             const char* f0 = reinterpret_cast<const char*>(P.p.dynamics_factor + (size_t)nx * n * n);
@@ -739,77 +748,105 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       for (int i = tid; i < n; i += NT)
         if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
-      // Candidate starts (no counterpart in the reference): for each of the
-      // gamma0_count impulse sets, v_c = v* + A^-1 J^T gamma_c on the
-      // participating DOFs with A factored once in this kernel's factor
-      // precision; the start with the lowest cost among the plain start and
-      // the candidates is taken.  Its evaluation seeds iteration 0 when it
-      // was the last one evaluated.
+      // Candidate starts (no counterpart in the reference): v_candidate_count
+      // start velocities, then gamma0_count impulse sets with v_c = base +
+      // A^-1 J^T gamma_c (base v* or gamma0_base), each taken on the
+      // participating DOFs (v* on the others), A factored once in this
+      // kernel's factor precision or read from the free motion's factor;
+      // the start with the lowest cost among the plain start and the
+      // candidates is taken.  Its evaluation seeds iteration 0 when it was
+      // the last one evaluated.
       bool have_e4 = false;
       double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
-      if (P.p.gamma0 && count > 0) {
-        const int K = P.p.gamma0_count > 1 ? P.p.gamma0_count : 1;
+      const int KV = P.p.v_candidates ? (P.p.v_candidate_count > 1 ? P.p.v_candidate_count : 1) : 0;
+      const int KG = P.p.gamma0 ? (P.p.gamma0_count > 1 ? P.p.gamma0_count : 1) : 0;
+      if ((KV > 0 || KG > 0) && count > 0) {
         double e4p[4];
         evaluate<NT, HT, NS>(w, P, dt, e4p);
         double best_cost = e4p[0];
-        const int ldj = w.ldJ();
         for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
-        if (P.p.dynamics_factor) {
-          // the free motion's LDL^T of A
-          const double* Lg = P.p.dynamics_factor + (size_t)e * n * n;
-          load_lower<NT, HT, NS>(w, Lg, nullptr, 0.0);
-          HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
-          for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
-          __syncthreads();
-        } else {
-          load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
-          __syncthreads();
-          ldlt_blocked<NT, HT, LB>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri);  // the factor of A
-        }
         bool last_is_best = false;
-        // Two sets at a time: stage their impulses in the (here unused)
-        // scratch, form J^T gamma for both (threads 0-63 set k0, 64-127 set
-        // k0+1), solve both with the factor on warps 0 and 1, then evaluate
-        // the candidates in order.
-        double* gs = reinterpret_cast<double*>(w.GJ);
-        for (int k0 = 0; k0 < K; k0 += 2) {
-          const int nk = K - k0 < 2 ? K - k0 : 2;
-          for (int q = tid; q < nk * 3 * count; q += NT) {
+        auto try_start = [&](int index) {  // V(V_V) holds the candidate
+          __syncthreads();
+          double e4c[4];
+          evaluate<NT, HT, NS>(w, P, dt, e4c);
+          last_is_best = false;
+          if (e4c[0] < best_cost) {
+            best_cost = e4c[0];
+            ws_accepted = index;
+            last_is_best = true;
+            for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
+            for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
+          }
+        };
+        for (int k = 0; k < KV; ++k) {
+          const double* vk = P.p.v_candidates + ((size_t)k * P.p.num_envs + e) * n;
+          for (int i = tid; i < n; i += NT)
+            w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? __ldg(vk + i) : w.V(V_VSTAR)[i];
+          try_start(k + 1);
+        }
+        if (KG > 0) {
+          const double* base_g = P.p.gamma0_base ? P.p.gamma0_base + (size_t)e * n : nullptr;
+          // a world whose candidate impulses are all zero starts at the base
+          int nz = 0;
+          for (int q = tid; q < KG * 3 * count; q += NT) {
             const int kk = q / (3 * count), r = q - kk * 3 * count;
-            gs[q] = __ldg(P.p.gamma0 + ((size_t)(k0 + kk) * P.p.num_envs + e) * C * 3 + r);
+            if (__ldg(P.p.gamma0 + ((size_t)kk * P.p.num_envs + e) * C * 3 + r) != 0.0) nz = 1;
           }
-          __syncthreads();
-          {
-            const int kk = tid >> 6, i = tid & 63;
-            if (kk < nk && i < n) {
-              const double* g = gs + kk * 3 * count;
-              double acc = 0.0;
-              for (int c = 0; c < count; ++c) {
-                const double* Jc = w.J + (size_t)(3 * c) * ldj;
-                acc += Jc[i] * g[3 * c] + Jc[ldj + i] * g[3 * c + 1] + Jc[2 * ldj + i] * g[3 * c + 2];
-              }
-              w.V(kk == 0 ? V_GRAD : V_DP)[i] = -acc;  // the solves give -H^-1 rhs
-            }
-          }
-          __syncthreads();
-          solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
-          if (nk > 1) solve_warp<NT, HT, NS>(w, V_DP, V_DV2, 1);
-          __syncthreads();
-          for (int kk = 0; kk < nk; ++kk) {
-            const int k = k0 + kk;
-            const double* dvk = w.V(kk == 0 ? V_DV : V_DV2);
+          if (!__syncthreads_or(nz)) {
             for (int i = tid; i < n; i += NT)
-              w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? w.V(V_VSTAR)[i] + dvk[i] : w.V(V_VSTAR)[i];
-            __syncthreads();
-            double e4c[4];
-            evaluate<NT, HT, NS>(w, P, dt, e4c);
-            last_is_best = false;
-            if (e4c[0] < best_cost) {
-              best_cost = e4c[0];
-              ws_accepted = k + 1;
-              last_is_best = true;
-              for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
-              for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
+              w.V(V_V)[i] = (w.flags[i] & kFlagPart) && base_g ? __ldg(base_g + i) : w.V(V_VSTAR)[i];
+            try_start(KV + 1);
+          } else {
+            const int ldj = w.ldJ();
+            if (P.p.dynamics_factor) {
+              // the free motion's LDL^T of A
+              const double* Lg = P.p.dynamics_factor + (size_t)e * n * n;
+              load_lower<NT, HT, NS>(w, Lg, nullptr, 0.0);
+              HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
+              for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
+              __syncthreads();
+            } else {
+              load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
+              __syncthreads();
+              ldlt_blocked<NT, HT, LB>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri);  // the factor of A
+            }
+            // Two sets at a time: stage their impulses in the (here unused)
+            // scratch, form J^T gamma for both (threads 0-63 set k0, 64-127
+            // set k0+1), solve both with the factor on warps 0 and 1, then
+            // evaluate the candidates in order.
+            double* gs = reinterpret_cast<double*>(w.GJ);
+            for (int k0 = 0; k0 < KG; k0 += 2) {
+              const int nk = KG - k0 < 2 ? KG - k0 : 2;
+              for (int q = tid; q < nk * 3 * count; q += NT) {
+                const int kk = q / (3 * count), r = q - kk * 3 * count;
+                gs[q] = __ldg(P.p.gamma0 + ((size_t)(k0 + kk) * P.p.num_envs + e) * C * 3 + r);
+              }
+              __syncthreads();
+              {
+                const int kk = tid >> 6, i = tid & 63;
+                if (kk < nk && i < n) {
+                  const double* g = gs + kk * 3 * count;
+                  double acc = 0.0;
+                  for (int c = 0; c < count; ++c) {
+                    const double* Jc = w.J + (size_t)(3 * c) * ldj;
+                    acc += Jc[i] * g[3 * c] + Jc[ldj + i] * g[3 * c + 1] + Jc[2 * ldj + i] * g[3 * c + 2];
+                  }
+                  w.V(kk == 0 ? V_GRAD : V_DP)[i] = -acc;  // the solves give -H^-1 rhs
+                }
+              }
+              __syncthreads();
+              solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
+              if (nk > 1) solve_warp<NT, HT, NS>(w, V_DP, V_DV2, 1);
+              __syncthreads();
+              for (int kk = 0; kk < nk; ++kk) {
+                const double* dvk = w.V(kk == 0 ? V_DV : V_DV2);
+                for (int i = tid; i < n; i += NT)
+                  w.V(V_V)[i] = (w.flags[i] & kFlagPart)
+                                    ? (base_g ? __ldg(base_g + i) : w.V(V_VSTAR)[i]) + dvk[i]
+                                    : w.V(V_VSTAR)[i];
+                try_start(KV + k0 + kk + 1);
+              }
             }
           }
         }

@@ -41,7 +41,10 @@ __device__ __forceinline__ double dist2(const Key& a, const Key& b) {
   return dx * dx + dy * dy + dz * dz;
 }
 
-__global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_contact_history H) {
+// rank_src (the free-motion launch's slot list, [W][C] flat indices in
+// arrival order): ranked by flat index in place first and used as the slots'
+// sources; NULL: the sources are H.contact_source.
+__global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_contact_history H, int32_t* rank_src) {
   const int kHistThreads = blockDim.x;
   extern __shared__ __align__(16) unsigned char smem[];
   const int C = H.max_contacts, e = blockIdx.x;
@@ -53,11 +56,25 @@ __global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_con
   double* pg1 = reinterpret_cast<double*>(cur + C);
   double* pg2 = pg1 + 3 * C;
   int* pdepth = reinterpret_cast<int*>(pg2 + 3 * C);
+  int* srcs = pdepth + C;  // arrival order [C], then ranked [C]
   int np = H.key_count[e];
   np = np < 0 ? 0 : (np > C ? C : np);
   int nc = H.contact_count[e];
   nc = nc < 0 ? 0 : (nc > C ? C : nc);
   const size_t base = (size_t)e * C;
+  if (rank_src) {
+    // the canonical slot order: this step's contacts by flat index (distinct)
+    for (int c = threadIdx.x; c < nc; c += kHistThreads) srcs[c] = rank_src[base + c];
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += kHistThreads) {
+      const int v = srcs[c];
+      int rank = 0;
+      for (int j = 0; j < nc; ++j) rank += srcs[j] < v ? 1 : 0;
+      srcs[C + rank] = v;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += kHistThreads) rank_src[base + c] = srcs[C + c];
+  }
   for (int c = threadIdx.x; c < np; c += kHistThreads) {
     Key k;
     k.s0 = H.key_shape[2 * (base + c)];
@@ -76,7 +93,7 @@ __global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_con
     }
   }
   for (int c = threadIdx.x; c < nc; c += kHistThreads) {
-    const int src = H.contact_source[base + c];
+    const int src = rank_src ? srcs[C + c] : H.contact_source[base + c];
     Key k{-2, -2, 0.0, 0.0, 0.0};
     if (src >= 0 && src < H.num_flat) {
       k.s0 = H.flat_shape0[src];
@@ -165,17 +182,19 @@ __global__ void __launch_bounds__(kHistMaxThreads) history_kernel(const sapb_con
 
 using namespace sapb;
 
-extern "C" int32_t sapb_contact_history_update(const sapb_contact_history* h, void* stream) {
+namespace sapb {
+
+int32_t history_launch(const sapb_contact_history* h, int32_t* rank_src, cudaStream_t stream) {
   if (!h || h->num_envs < 0 || h->max_contacts < 1 || h->num_flat < 0 || h->order < 0 || h->order > kHistMaxOrder ||
-      (h->num_envs > 0 && (!h->contact_count || !h->contact_source || !h->key_shape || !h->key_point ||
-                           !h->key_count || !h->gamma_prev || !h->gamma_hist ||
+      (h->num_envs > 0 && (!h->contact_count || (!h->contact_source && !rank_src) || !h->key_shape ||
+                           !h->key_point || !h->key_count || !h->gamma_prev || !h->gamma_hist ||
                            (h->order >= 2 && !h->has_history) || (h->order >= 3 && !h->gamma_older) ||
                            (h->num_flat > 0 && (!h->flat_shape0 || !h->flat_shape1 || !h->flat_point1))))) {
     set_last_error("sapb_contact_history_update: invalid argument");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   if (h->num_envs == 0) return SAPB_OK;
-  const size_t smem = (sizeof(Key) * 2 + sizeof(double) * 6 + sizeof(int)) * (size_t)h->max_contacts;
+  const size_t smem = (sizeof(Key) * 2 + sizeof(double) * 6 + sizeof(int) * 3) * (size_t)h->max_contacts;
   if (smem > kMaxSmemPerBlock) {
     set_last_error("sapb_contact_history_update: %d slots per world exceed shared memory", h->max_contacts);
     return SAPB_ERR_UNSUPPORTED;
@@ -184,7 +203,7 @@ extern "C" int32_t sapb_contact_history_update(const sapb_contact_history* h, vo
   if (err == cudaSuccess) {
     int threads = (h->max_contacts + 31) / 32 * 32;
     if (threads > kHistMaxThreads) threads = kHistMaxThreads;
-    history_kernel<<<h->num_envs, threads, smem, static_cast<cudaStream_t>(stream)>>>(*h);
+    history_kernel<<<h->num_envs, threads, smem, stream>>>(*h, rank_src);
     err = cudaGetLastError();
   }
   if (err != cudaSuccess) {
@@ -192,4 +211,10 @@ extern "C" int32_t sapb_contact_history_update(const sapb_contact_history* h, vo
     return SAPB_ERR_CUDA;
   }
   return SAPB_OK;
+}
+
+}  // namespace sapb
+
+extern "C" int32_t sapb_contact_history_update(const sapb_contact_history* h, void* stream) {
+  return history_launch(h, nullptr, static_cast<cudaStream_t>(stream));
 }

@@ -41,6 +41,9 @@ int32_t contacts_launch(const sapb_collision_shapes* s, const double* body_q, co
                         void* workspace, cudaStream_t stream);
 
 size_t prepare_smem_bytes(int B, int n, int C, bool tree_blocked);
+// The contact history; rank_src non-NULL: the free-motion launch's slot
+// list, ranked in place and used as the slots' sources (sapb_history.cu).
+int32_t history_launch(const sapb_contact_history* h, int32_t* rank_src, cudaStream_t stream);
 int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, const sapb_prepare_options* o,
                        const sapb_prepare_outputs* out, void* workspace, size_t workspace_bytes,
                        cudaStream_t stream);

@@ -33,6 +33,11 @@ struct PrepParams {
   int32_t* env_count;  // [W]
   int32_t* env_src;    // [W][C]
   int32_t* truncated;  // [1]
+  // the contact history run before this kernel: slots already ranked, the
+  // start impulses and known-impulse counts by slot (NULL: no history)
+  bool ranked;
+  const double* gamma_start;  // [W][C][3]
+  const int32_t* hist_depth;  // [W][C]
 };
 
 __host__ __device__ inline size_t prep_align(size_t x) { return (x + 15) / 16 * 16; }
@@ -42,7 +47,8 @@ __host__ __device__ inline size_t prep_align(size_t x) { return (x + 15) / 16 * 
 // ([angular; linear]), so velocities, forces and inertias of different bodies
 // add without shifts.
 struct PrepLayout {
-  size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, par, dbody, tri, total;
+  size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, par, dbody, tri, jg,
+      total;
 };
 
 __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk) {
@@ -75,6 +81,7 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk)
   L.par = take(sizeof(int) * B);            // parent body, -1
   L.dbody = take(sizeof(int) * n);          // body of each DOF
   L.tri = take(sizeof(uint16_t) * (blk ? 1 : (size_t)(n * (n - 1) / 2 + 1)));  // LDL^T triangle list
+  L.jg = take(sizeof(double) * (blk ? 1 : (size_t)(kPrepNT / 32) * n));  // per-warp J^T gamma_start partials
   L.total = o;
   return L;
 }
@@ -197,6 +204,9 @@ __device__ __forceinline__ void pose_store(double* p, Xf x) {
 // then a blocked LDL^T (diagonal blocks in registers) and block triangular solves.
 // The contact rows are J_c = R_WC (v_O + w x x_c) of the ancestor DOFs' S
 // columns (sim/contact_jacobian.py:404-562).
+// VS: the candidate start velocity is written (v_start; a separate
+// instantiation keeps its registers off the plain path).
+template <bool VS>
 __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x;
@@ -231,6 +241,8 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   int* par = reinterpret_cast<int*>(smem + L.par);
   int* dbody = reinterpret_cast<int*>(smem + L.dbody);
   uint16_t* tri = reinterpret_cast<uint16_t*>(smem + L.tri);
+  double* jg = reinterpret_cast<double*>(smem + L.jg);
+  const bool want_vstart = VS && !blk && P.out.v_start && P.gamma_start;
   const int j0 = e * Jw, b0g = e * B, d0 = e * n;
   const double* q = P.in.joint_q;
   const double* qd = P.in.joint_qd;
@@ -240,6 +252,19 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   for (int i = tid; i < n; i += kPrepNT) dbody[i] = -1;
   if (!blk) build_triangle_list<kPrepNT>(tri, n);
   for (int k = tid; k < 6 * n; k += kPrepNT) S[k] = 0.0;
+  if (want_vstart)
+    for (int k = tid; k < (kPrepNT / 32) * n; k += kPrepNT) jg[k] = 0.0;
+  // whether a live slot holds a new contact (the factor is then written
+  // under factor_new_contacts_only)
+  int newc = 0;
+  if (P.o.factor_new_contacts_only && P.hist_depth) {
+    const int tot = P.env_count[e];
+    const int c0 = tot < C ? tot : C;
+    for (int c = tid; c < c0; c += kPrepNT)
+      if (P.hist_depth[(size_t)e * C + c] == 0) newc = 1;
+  } else {
+    newc = 1;
+  }
   __syncthreads();
   for (int jl = tid; jl < Jw; jl += kPrepNT) {
     const int j = j0 + jl;
@@ -251,7 +276,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     for (int k = 0; k < dim; ++k)
       if (dl + k >= 0 && dl + k < n) dbody[dl + k] = cb;
   }
-  __syncthreads();
+  const bool write_factor = P.out.dynamics_factor && __syncthreads_or(newc) != 0;
 
   // ---- local transforms X_{parent body, body} = X_p X_FM(q) X_c^-1 ---------
   // (sim/sap_helpers.py:1164-1243)
@@ -590,7 +615,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     }
   } else {
   ldlt_blocked<kPrepNT, double, 5>(H, n, n, dinv, tri);  // width 5: measured fastest for 35 DOFs
-  if (P.out.dynamics_factor) {
+  if (write_factor) {
     double* Lg = P.out.dynamics_factor + (size_t)e * n * n;
     for (int k = tid; k < n * n; k += kPrepNT) {
       const int i = k / n, j = k - i * n;
@@ -627,7 +652,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   // Canonical slot order: the slots the scatter claimed in arrival order are
   // re-ranked by flat contact index (distinct), so an untruncated world's
   // slots follow the flat buffer's order on every step.
-  {
+  if (!P.ranked) {  // (the contact history ranks them when it runs first)
     int* tmp = conint;  // 2*C ints, free until the rows below use them
     for (int c = wt; c < cc; c += wn) tmp[c] = P.env_src[(size_t)e * C + c];
     wsync();
@@ -720,6 +745,9 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   {
     const int lane = tid & 31, warp = tid >> 5;
     const bool dd = P.o.contact_weight_mode == SAPB_WEIGHT_DIAG_DELASSUS;
+    // this warp's partial of J^T gamma_start (its contacts, in order): in
+    // registers, columns lane and lane + 32, up to 64 DOFs; in shared memory beyond
+    double jgr0 = 0.0, jgr1 = 0.0;
     const double h = P.in.dt[e];
     for (int c = warp; c < cc; c += kPrepNT / 32) {
       const double* cs = con + 21 * (size_t)c;
@@ -740,6 +768,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
         }
       }
       double wq[6] = {0, 0, 0, 0, 0, 0}, vq[3] = {0, 0, 0};
+      const double* gst = want_vstart ? P.gamma_start + 3 * ((size_t)e * C + c) : nullptr;
       for (int col = lane; col < ncols; col += 32) {
         V3 rel = v3(0, 0, 0);
         int dof = col;
@@ -759,6 +788,15 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
           Jout[((size_t)c * 3 + r) * ncols + col] = rw[r];
         }
         if (dof < 0) continue;
+        if (want_vstart) {
+          const double t = rw[0] * __ldg(gst) + rw[1] * __ldg(gst + 1) + rw[2] * __ldg(gst + 2);
+          if (n <= 64) {
+            if (col < 32) jgr0 += t;
+            else jgr1 += t;
+          } else {
+            jg[warp * n + dof] += t;
+          }
+        }
         const double vs = P.in.joint_qd[d0 + dof] + h * vdot[dof];
         vq[0] += rw[0] * vs;
         vq[1] += rw[1] * vs;
@@ -796,6 +834,10 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
         }
       }
     }
+    if (want_vstart && n <= 64) {
+      if (lane < n) jg[warp * n + lane] = jgr0;
+      if (lane + 32 < n) jg[warp * n + lane + 32] = jgr1;
+    }
   }
   __syncthreads();
   // ---- body_inertia contact weights (sim/contact_jacobian.py:153-251) --------
@@ -831,6 +873,42 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     P.out.w_eff[ci] = w < 1.0e-12 ? 1.0e-12 : w;
   }
   }
+  // ---- candidate start v* + A^-1 J^T gamma_start through this kernel's
+  // LDL^T of A (H, dinv): the warps' partials summed in warp order, then the
+  // triangular solves (one warp up to 64 DOFs, the block beyond)
+  if (want_vstart && n <= 64) {
+    __syncthreads();
+    if (tid < 32) {  // warp 0 alone: no block barrier after the partials
+      double* z = jg + n;
+      for (int i = tid; i < n; i += 32) {
+        double r = 0.0;
+        for (int q = 0; q < kPrepNT / 32; ++q) r += jg[q * n + i];
+        jg[i] = r;
+      }
+      __syncwarp();
+      ldlt_solve_warp<double>(H, n, n, dinv, jg, z, false, ldlt_pivots_ok_warp<double>(H, n, n));
+      __syncwarp();
+      for (int i = tid; i < n; i += 32)
+        P.out.v_start[d0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vdot[i] + z[i];
+    }
+  } else if (want_vstart) {
+    __syncthreads();
+    for (int i = tid; i < n; i += kPrepNT) {
+      double r = 0.0;
+      for (int q = 0; q < kPrepNT / 32; ++q) r += jg[q * n + i];
+      jg[i] = r;
+    }
+    __syncthreads();
+    double* z = jg + n;
+    {
+      for (int i = tid; i < n; i += kPrepNT) z[i] = jg[i];
+      __syncthreads();
+      ldlt_solve_blocked<kPrepNT, double>(H, n, n, dinv, z, false);
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += kPrepNT)
+      P.out.v_start[d0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vdot[i] + z[i];
+  }
 }
 
 size_t prepare_smem_bytes(int B, int n, int C, bool blk) { return prep_layout(B, n, C, blk).total; }
@@ -857,11 +935,31 @@ int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, con
     scatter_contacts_kernel<<<blocks, 256, 0, stream>>>(P);
     err = cudaGetLastError();
   }
+  if (err == cudaSuccess && out->history) {
+    // the contact history on this launch's slots, which it ranks by flat index
+    sapb_contact_history hh = *out->history;
+    hh.num_envs = W;
+    hh.max_contacts = C > 0 ? C : 1;
+    hh.num_flat = in->contact_capacity;
+    hh.contact_count = P.env_count;
+    hh.contact_source = nullptr;
+    hh.flat_shape0 = in->contact_shape0;
+    hh.flat_shape1 = in->contact_shape1;
+    hh.flat_point1 = in->contact_point1;
+    const int32_t st = history_launch(&hh, P.env_src, stream);
+    if (st != SAPB_OK) return st;
+    P.ranked = true;
+    P.gamma_start = hh.gamma_start;
+    P.hist_depth = hh.has_history;
+  }
   if (err == cudaSuccess) {
     const size_t smem = prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, C, o->tree_blocked != 0);
-    err = cudaFuncSetAttribute(prepare_world_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool vs = out->v_start && P.gamma_start && !o->tree_blocked;
+    err = cudaFuncSetAttribute(vs ? prepare_world_kernel<true> : prepare_world_kernel<false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err == cudaSuccess) {
-      prepare_world_kernel<<<W, kPrepNT, smem, stream>>>(P);
+      if (vs) prepare_world_kernel<true><<<W, kPrepNT, smem, stream>>>(P);
+      else prepare_world_kernel<false><<<W, kPrepNT, smem, stream>>>(P);
       err = cudaGetLastError();
     }
   }

@@ -78,14 +78,14 @@ struct sapb_handle {
   sapb_step_options opts;
   int32_t W, n, C, B, Q;
   // free motion + contact rows
-  double *v_star, *vdot, *A, *J, *phi0, *w_eff, *mu, *stiffness, *tau_d, *factor, *vc_star;
+  double *v_star, *vdot, *A, *J, *phi0, *w_eff, *mu, *stiffness, *tau_d, *factor, *vc_star;  // (factor, vc_star: unused)
   int32_t *count, *body0, *body1, *truncated;
   void* prep_ws;
   size_t prep_ws_bytes;
   // contact history (previous-impulse warm start): keys, carried impulses,
   // the impulses before them, the extrapolated start impulses
   int32_t *source, *key_shape, *key_count, *has_history;
-  double *key_point, *gamma_last, *gamma_older, *gamma_start;
+  double *key_point, *gamma_last, *gamma_older, *gamma_start, *v_start;
   // solve
   double *v, *gamma, *gamma_prev, *cost, *grad_norm;
   int32_t *mode, *iters, *ls_iters, *converged, *status, *ws_accepted, *guess_flag, *order;
@@ -146,7 +146,7 @@ void sapb_destroy(sapb_handle* h) {
                   h->gamma_prev, h->cost, h->grad_norm, h->mode, h->iters, h->ls_iters, h->converged, h->status,
                   h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws,
                   h->source, h->key_shape, h->key_count, h->has_history, h->key_point, h->gamma_last,
-                  h->gamma_older, h->gamma_start};
+                  h->gamma_older, h->gamma_start, h->v_start};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -256,11 +256,9 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   take(dev_alloc(&h->body1, WC));
   take(dev_alloc(&h->truncated, 1));
   if (cand) {
-    take(dev_alloc(&h->factor, Wn * n));
-    take(dev_alloc(&h->vc_star, WC * 3));
+    take(dev_alloc(&h->v_start, Wn));
     take(dev_alloc(&h->gamma_prev, WC * 3));
     take(dev_alloc(&h->gamma_last, WC * 3));
-    take(dev_alloc(&h->source, WC));
     take(dev_alloc(&h->key_shape, WC * 2));
     take(dev_alloc(&h->key_point, WC * 3));
     take(dev_alloc(&h->key_count, W));
@@ -340,23 +338,12 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   po.body0 = h->body0;
   po.body1 = h->body1;
   po.truncated_count = h->truncated;
-  po.dynamics_factor = h->factor;
-  po.vc_star = h->vc_star;
-  po.contact_source = h->source;
-  int32_t st = sapb_free_motion_contacts(&h->model, &io->in, &h->opts.prepare, &po, h->prep_ws, h->prep_ws_bytes,
-                                         stream);
-  if (st != SAPB_OK) return st;
-  if (cand) {  // the last solves' impulses carried to this step's slots by contact identity, extrapolated
-    sapb_contact_history hist;
-    memset(&hist, 0, sizeof(hist));
-    hist.num_envs = h->W;
-    hist.max_contacts = h->C;
-    hist.num_flat = io->in.contact_capacity;
-    hist.contact_count = h->count;
-    hist.contact_source = h->source;
-    hist.flat_shape0 = io->in.contact_shape0;
-    hist.flat_shape1 = io->in.contact_shape1;
-    hist.flat_point1 = io->in.contact_point1;
+  // previous impulses: the contact history runs inside the launch (the last
+  // solves' impulses carried to this step's slots by contact identity and
+  // extrapolated), and the free motion forms the start v* + A^-1 J^T gamma
+  sapb_contact_history hist;
+  memset(&hist, 0, sizeof(hist));
+  if (cand) {
     hist.key_shape = h->key_shape;
     hist.key_point = h->key_point;
     hist.key_count = h->key_count;
@@ -366,9 +353,12 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     hist.order = h->opts.impulse_history;
     hist.gamma_older = h->gamma_older;
     hist.gamma_start = h->gamma_start;
-    st = sapb_contact_history_update(&hist, stream);
-    if (st != SAPB_OK) return st;
+    po.history = &hist;
+    po.v_start = h->v_start;
   }
+  int32_t st = sapb_free_motion_contacts(&h->model, &io->in, &h->opts.prepare, &po, h->prep_ws, h->prep_ws_bytes,
+                                         stream);
+  if (st != SAPB_OK) return st;
   // contact solve (sim/solver_sap.py:1434-1460), warm start from the last
   // solution once a step has run
   sapb_contact_problem p;
@@ -404,9 +394,8 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     p.dof = &dof_local;
   }
   if (cand) {
-    p.gamma0 = h->gamma_start;
-    p.gamma0_count = 1;
-    p.dynamics_factor = h->factor;
+    p.v_candidates = h->v_start;
+    p.v_candidate_count = 1;
   }
   p.world_order = order ? h->order : nullptr;
   sapb_solve_outputs so;

@@ -371,6 +371,17 @@ class SapContactJacobian:
             self.contact_env_source = torch.full((v.W, self.max_rigid_contact), -1, dtype=I32, device=v.device)
             self.outputs.contact_source = _ptr(self.contact_env_source)
 
+    def set_history(self, history, v_start: torch.Tensor | None = None, factor_new_contacts_only: bool = False) -> None:
+        """Run the contact history (an _abi.ContactHistory over persistent
+        buffers, or None) inside the launch, between the contact scatter and
+        the free motion; with v_start ((W*n,) FP64) also write the candidate
+        start v* + A^-1 J^T gamma_start there; factor_new_contacts_only: the
+        kept LDL^T factor only for worlds with a new contact."""
+        self._history = history  # the launch reads it by address
+        self.outputs.history = ctypes.addressof(history) if history is not None else None
+        self.outputs.v_start = _ptr(v_start)
+        self.opts.factor_new_contacts_only = 1 if factor_new_contacts_only else 0
+
     def set_dt(self, dt) -> None:
         """Per-world time step (scalar or [W] tensor), sim/solver_sap.py:975-992."""
         if isinstance(dt, torch.Tensor):
@@ -646,12 +657,16 @@ class SapContactSolve:
               line_search_relative_slop: float | None = None, line_search_variant: str = "monotone_decay",
               collect_iteration_stats: bool = True, check_line_search_errors: bool = True,
               graph_conditional: bool = True, static_loop: bool = False,
-              gamma0: torch.Tensor | None = None, world_order: torch.Tensor | None = None) -> SapContactSolveResult:
-        """sim/contact_solve.py:6129-6285.  gamma0 (W, C, 3) FP64: learned
-        starting impulses (no counterpart in the reference), tried against the
-        plain start on the cost.  world_order (W,) int32: the order in which
-        the persistent kernel takes the worlds (a permutation; results do not
-        depend on it)."""
+              gamma0: torch.Tensor | None = None, world_order: torch.Tensor | None = None,
+              v_candidates: torch.Tensor | None = None,
+              gamma0_base: torch.Tensor | None = None) -> SapContactSolveResult:
+        """sim/contact_solve.py:6129-6285.  Candidate starts (no counterpart
+        in the reference), tried against the plain start on the cost:
+        v_candidates (W*n,) or (K, W*n) FP64 start velocities, then gamma0
+        (W, C, 3) or (K, W, C, 3) FP64 starting impulses, each mapped to
+        gamma0_base (or v*) + A^-1 J^T gamma.  world_order (W,) int32: the
+        order in which the persistent kernel takes the worlds (a permutation;
+        results do not depend on it)."""
         if not bool(graph_conditional):
             raise ValueError("SapContactSolve only supports graph_conditional=True; "
                              "the Python Newton-loop fallback has been removed.")
@@ -696,6 +711,16 @@ class SapContactSolve:
             P.gamma0_count = int(gamma0.numel() // per_set)
             if getattr(contact_result, "dynamics_factor_env", None) is not None:
                 P.dynamics_factor = _ptr(contact_result.dynamics_factor_env)
+            if gamma0_base is not None:
+                if gamma0_base.dtype != F64 or not gamma0_base.is_contiguous() or gamma0_base.numel() != W * n:
+                    raise TypeError("gamma0_base must be a contiguous float64 (W*n,) tensor")
+                P.gamma0_base = _ptr(gamma0_base)
+        if v_candidates is not None:
+            if v_candidates.dtype != F64 or not v_candidates.is_contiguous() or v_candidates.numel() % (W * n) != 0 \
+                    or v_candidates.numel() == 0:
+                raise TypeError("v_candidates must be a contiguous float64 (W*n,) or (K, W*n) tensor")
+            P.v_candidates = _ptr(v_candidates)
+            P.v_candidate_count = int(v_candidates.numel() // (W * n))
         if self.dof is not None:
             self._jq = _f64(state.joint_q)
             self.dof.joint_q = _ptr(self._jq)
@@ -947,16 +972,35 @@ class SolverSAP:
         self._gamma_carried = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self._gamma_older = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
+        self._v_start = None
         if self.warm_start != "previous_velocity":
             self._hist_key_shape = torch.zeros(view.W, max(C, 1), 2, dtype=I32, device=dev)
             self._hist_key_point = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
             self._hist_key_count = torch.zeros(view.W, dtype=I32, device=dev)
             self.has_history = torch.zeros(view.W, max(C, 1), dtype=I32, device=dev)
-            self.contact_jacobian.keep_contact_source()
+            # the contact history, run by the free-motion launch on its slots:
+            # the last solve's impulses (_gamma_last, by its slots) carried by
+            # contact identity and extrapolated into the start impulses
+            H = _abi.ContactHistory()
+            H.key_shape, H.key_point = _ptr(self._hist_key_shape), _ptr(self._hist_key_point)
+            H.key_count = _ptr(self._hist_key_count)
+            H.gamma_prev, H.gamma_hist, H.has_history = (_ptr(self._gamma_last), _ptr(self._gamma_carried),
+                                                         _ptr(self.has_history))
+            H.order, H.gamma_older, H.gamma_start = (self.impulse_history, _ptr(self._gamma_older),
+                                                     _ptr(self._gamma_prev))
+            if not self.contact_solve.tree_blocked:
+                # the start velocity v* + A^-1 J^T gamma_start, formed by the
+                # free motion with its own factor of A
+                self._v_start = torch.zeros(view.W * view.n, dtype=F64, device=dev)
+            self.contact_jacobian.set_history(
+                H, v_start=self._v_start,
+                factor_new_contacts_only=self.warm_start == "learned" and self.learned_candidates == "new_contacts")
         if self.learned_warm_start is not None:
             self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
-        if self.warm_start != "previous_velocity" and not self.contact_solve.tree_blocked:
-            self.contact_jacobian.keep_dynamics_factor()  # the blocked solve solves with A's tree blocks
+            # network inputs J_c v* and, for the network's impulses, the
+            # factor of A (new contacts only in the new_contacts mode)
+            self.contact_jacobian.keep_dynamics_factor()
+            self._gamma_zero = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self.work_order = str(work_order).strip().lower().replace("-", "_")
         if self.work_order not in ("previous_iterations", "index"):
             raise ValueError(f"work_order must be 'previous_iterations' or 'index', got {work_order!r}.")
@@ -1173,19 +1217,25 @@ class SolverSAP:
             iters, ls_iters = self.max_iterations, self.line_search_max_iterations
         v0 = self.contact_jacobian._qd
         mark("warm_start")
-        gamma0 = None
-        if self.warm_start != "previous_velocity":
-            self._carry_impulses(cr)
+        # the contact history ran inside the free-motion launch: _gamma_prev
+        # holds the start impulses, _v_start the start velocity
+        gamma0 = v_cands = gamma0_base = None
         if self.warm_start == "previous_impulses":
-            gamma0 = self._gamma_prev
+            if self._v_start is not None:
+                v_cands = self._v_start
+            else:
+                gamma0 = self._gamma_prev  # tree-blocked: the solve maps them tree by tree
         elif self.warm_start == "learned":
             self._normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
-            # new_contacts: slots with history keep their start impulse;
-            # all_contacts: the network corrects the carried impulses
+            # new_contacts: the network's impulses on new contacts only (zero
+            # where the start velocity already holds the history's), added to
+            # the start velocity through A^-1 J^T; all_contacts: the network
+            # corrects the carried impulses, a set of its own beside the
+            # start velocity
+            new_only = self.learned_candidates == "new_contacts"
             self.learned_warm_start.predict(
                 num_envs=self.view.W, dof_per_env=self.view.n, max_contacts=self.max_rigid_contact,
-                normal_up=self._normal_up,
-                gamma_prev=self._gamma_prev if self.learned_candidates == "new_contacts" else self._gamma_carried,
+                normal_up=self._normal_up, gamma_prev=self._gamma_zero if new_only else self._gamma_carried,
                 out=self._gamma_cand[0],
                 vc_star=self.contact_jacobian.contact_env_vc_star,
                 contact_count=cr.contact_env_count, dynamics_matrix=cr.dynamics_matrix_env,
@@ -1194,11 +1244,16 @@ class SolverSAP:
                 v_star=self.contact_jacobian.v_star, v0=self.contact_jacobian.v_star,
                 dt=self.contact_jacobian.dt_world,
                 has_history=self.has_history if self.learned_candidates == "new_contacts" else None)
-            gamma0 = self._gamma_cand[0:1] if self.learned_candidates == "new_contacts" else self._gamma_cand
+            gamma0 = self._gamma_cand[0:1]
+            if new_only:
+                gamma0_base = self._v_start
+            else:
+                v_cands = self._v_start
         mark("contact_solve")
         sr = self.contact_solve.solve(
             cr, solve_state, solve_control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
             v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, gamma0=gamma0,
+            v_candidates=v_cands, gamma0_base=gamma0_base,
             max_iterations=iters,
             optimality_abs_tol=self.optimality_abs_tol, optimality_rel_tol=self.optimality_rel_tol,
             cost_abs_tol=self.cost_abs_tol, cost_rel_tol=self.cost_rel_tol, line_search_max_iterations=ls_iters,
@@ -1242,28 +1297,6 @@ class SolverSAP:
             self.sim_time += float(dt)
         self.frame_id += 1
         return state_out
-
-    def _carry_impulses(self, cr: SapContactJacobianResult) -> None:
-        """The last solves' impulses carried to this step's contact slots by
-        contact identity (shape pair + shape1 witness point) and extrapolated
-        over impulse_history steps, into _gamma_prev (the start impulses);
-        has_history counts the past impulses known for each slot's contact
-        (0: new)."""
-        cj = self.contact_jacobian
-        inp = cj._inputs
-        H = _abi.ContactHistory()
-        H.num_envs, H.max_contacts = self.view.W, self.max_rigid_contact
-        H.num_flat = int(inp.contact_capacity)
-        H.contact_count, H.contact_source = _ptr(cr.contact_env_count), _ptr(cj.contact_env_source)
-        H.flat_shape0, H.flat_shape1, H.flat_point1 = inp.contact_shape0, inp.contact_shape1, inp.contact_point1
-        H.key_shape, H.key_point = _ptr(self._hist_key_shape), _ptr(self._hist_key_point)
-        H.key_count = _ptr(self._hist_key_count)
-        H.gamma_prev, H.gamma_hist, H.has_history = _ptr(self._gamma_last), _ptr(self._gamma_carried), _ptr(
-            self.has_history)
-        H.order, H.gamma_older, H.gamma_start = self.impulse_history, _ptr(self._gamma_older), _ptr(self._gamma_prev)
-        check(load().sapb_contact_history_update(
-            ctypes.byref(H), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)),
-            "sapb_contact_history_update")
 
     def _boundary_in(self, state_in: SapState, state_out: SapState, control: SapControl | None):
         """Public-order inputs -> SAP order (sim/solver_sap.py:1198-1261):

@@ -169,3 +169,72 @@ def test_regenerated_contacts_rollout(cuda_device):
     assert len(counts_seen) > 1, "the contact set never changed"
     assert new_seen > 0, "no contact appeared"
     assert iters["previous_impulses"] < iters["previous_velocity"]
+
+
+def test_free_motion_forms_the_start_velocity(cuda_device):
+    """With the history inside the free-motion launch, the start velocity it
+    writes is v* + A^-1 J^T gamma_start of this step's slots (numpy on the
+    launch's own A, J and start impulses), and the start impulses are the
+    history's extrapolation of the last solves' impulses."""
+    W, steps, n = 64, 5, 35
+    model, state, control, contacts, _ = models.rollout_scene("humanoid", W, 63, cuda_device)
+    solver = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32",
+                       warm_start="previous_impulses")
+    other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone())
+    past = []
+    for k in range(steps):
+        solver.step(state, other, control, contacts, 2.0e-3)
+        torch.cuda.synchronize()
+        cj = solver.contact_jacobian
+        A = cj.dynamics_matrix_env.cpu().numpy()
+        J = cj.contact_env_jacobian.cpu().numpy()
+        cnt = cj.contact_env_count.clamp(max=32).cpu().numpy()
+        vs = cj.v_star.cpu().numpy().reshape(W, n)
+        g = solver._gamma_prev.cpu().numpy()
+        got = solver._v_start.cpu().numpy().reshape(W, n)
+        for e in range(W):
+            c = int(cnt[e])
+            want = vs[e] + np.linalg.solve(A[e], J[e, :c].reshape(3 * c, n).T @ g[e, :c].reshape(-1))
+            np.testing.assert_allclose(got[e], want, rtol=1e-9, atol=1e-9 * np.abs(want).max())
+        # fixed contact set: every slot keeps its contact; start = extrapolation
+        depth = min(k, 3)
+        has = solver.has_history.cpu().numpy()
+        live = np.arange(32)[None, :] < cnt[:, None]
+        assert np.all(has[live] == depth)
+        if depth:
+            g1 = past[-1]
+            want = g1 if depth == 1 else 2 * g1 - past[-2] if depth == 2 else 3 * g1 - 3 * past[-2] + past[-3]
+            np.testing.assert_allclose(g[live], want[live], rtol=0, atol=1e-12 * np.abs(want).max())
+        past.append(solver.contact_solve.contact_gamma.cpu().numpy().copy())
+        state, other = other, state
+        assert bool(solver.contact_solve.converged_env.all())
+
+
+def test_factor_written_only_where_a_contact_is_new(cuda_device):
+    """Learned start serving new contacts: the free motion writes the LDL^T
+    factor only for worlds with a new contact in a live slot; the others keep
+    whatever the buffer held (here NaN), and the step still converges."""
+    W = 256
+    model, state, control, shapes, _ = models.site_scene("humanoid", W, 43, cuda_device)
+    solver = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32",
+                       warm_start="learned")
+    gen = ContactGenerator(shapes, solver.view, capacity=W * 32, gap=1.0e-3)
+    other = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                     body_f=state.body_f.clone())
+    seen_new = seen_old = 0
+    for k in range(12):
+        solver.contact_jacobian.dynamics_factor_env.fill_(float("nan"))
+        solver.step(state, other, control, gen.generate(state.joint_q), 2.0e-3)
+        torch.cuda.synchronize()
+        cnt = solver.contact_jacobian.contact_env_count.clamp(max=32)
+        live = torch.arange(32, device=cuda_device)[None, :] < cnt[:, None]
+        new = (live & (solver.has_history == 0)).any(1)
+        diag = torch.diagonal(solver.contact_jacobian.dynamics_factor_env, dim1=1, dim2=2)
+        written = torch.isfinite(diag).all(1)
+        assert torch.equal(written, new), k
+        seen_new += int(new.sum())
+        seen_old += int((~new).sum())
+        assert bool(solver.contact_solve.converged_env.all())
+        state, other = other, state
+    assert seen_new > 0 and seen_old > 0

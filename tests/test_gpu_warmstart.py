@@ -153,6 +153,51 @@ def test_gamma0_start_matches_oracle(cuda_device, oracle, variant, sets):
     assert got["converged"].all()
 
 
+def _start_velocity(prob, gamma):
+    """v* + A^-1 J^T gamma per world (numpy, FP64), (E*n,)."""
+    E, n = prob.num_envs, prob.dof_per_env
+    vs = prob.v_star.reshape(E, n)
+    out = np.empty((E, n))
+    for e in range(E):
+        c = int(min(prob.contact_count[e], prob.max_contacts))
+        jt = prob.jacobian[e, :c].reshape(3 * c, n).T @ gamma[e, :c].reshape(-1) if c else np.zeros(n)
+        out[e] = vs[e] + np.linalg.solve(prob.dynamics_matrix[e], jt)
+    return out.reshape(-1)
+
+
+@pytest.mark.parametrize("variant", ["armijo_decay", "monotone_decay"])
+def test_velocity_candidates_match_the_impulse_candidates(cuda_device, oracle, variant):
+    """A start velocity v* + A^-1 J^T gamma given as v_candidates, and the
+    impulses split into a base velocity (gamma0_base) plus the rest (gamma0),
+    choose the same starts as the oracle given gamma and reach the same
+    answer; worlds whose remaining impulses are all zero start at the base
+    without the factor (every third world here)."""
+    prob = scenes.humanoid_contact_problem(64, seed=33)
+    plain = oracle.solve(prob, variant)
+    rng = np.random.default_rng(5)
+    e = np.arange(64)[:, None, None]
+    noise = np.where(e % 3 == 0, 5.0, np.where(e % 2 == 0, 0.02, 0.2))
+    gamma = plain["contact_gamma"][:, :prob.max_contacts] * (1.0 + noise * rng.normal(size=(64, prob.max_contacts, 3)))
+    ref = oracle.solve(prob, variant, gamma0=gamma)
+    acc = ref["warm_start_accepted"]
+    assert 0 < (acc > 0).sum() < 64
+    dev = cuda_device
+    vc = torch.as_tensor(_start_velocity(prob, gamma), device=dev).contiguous()
+    split = np.where((e % 3 == 1), 0.0, 0.5) * gamma  # world e % 3 == 1: all in the base
+    base = torch.as_tensor(_start_velocity(prob, gamma - split), device=dev).contiguous()
+    for kw in ({"v_candidates": vc},
+               {"gamma0": torch.as_tensor(split, device=dev).contiguous(), "gamma0_base": base}):
+        t = problem_to_device(prob, dev)
+        buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, dev)
+        contact_solve(**t, buffers=buf, options=make_options(variant), **kw)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(buf.warm_start_accepted.cpu().numpy(), acc, err_msg=str(list(kw)))
+        v, vr = buf.v.cpu().numpy().reshape(64, -1), ref["v"].reshape(64, -1)
+        err = np.abs(v - vr).max(1) / np.abs(vr).max(1)
+        assert np.quantile(err, 0.95) <= 1e-6 and err.max() <= 1e-4, err.max()
+        assert bool(buf.converged.all())
+
+
 def test_exact_impulses_start_at_the_solution(cuda_device, oracle):
     """gamma0 = gamma* gives v_L = v* + A^-1 J^T gamma* = the solution, so
     Newton stops at once."""
