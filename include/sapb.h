@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 11
+#define SAPB_ABI_VERSION 12
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -357,6 +357,30 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* model, const sapb_step_
 int32_t sapb_integrate_positions(const sapb_model_desc* model, const double* joint_q_in, const double* v_prev,
                                  const double* v_new, const double* dt, int32_t mode, double* joint_q_out,
                                  void* stream);
+
+/* The step's tail in one launch (the integrators above, the public output
+ * of sim/solver_sap.py:1467-1469 with sim/sap_helpers.py:1711-1760 and the
+ * forward kinematics of sim/sap_kinematics.py:85-229): one CTA per world
+ * writes every joint's new coordinates (fixed joints copy theirs), the new
+ * velocities in SAP or public order, and optionally the body poses and
+ * public body velocities of the new public coordinates.  Replaces
+ * sapb_integrate_positions + copies + sapb_sap_to_public_velocity +
+ * sapb_eval_fk, with the same arithmetic. */
+typedef struct sapb_step_tail {
+  const double* joint_q_in;         /* [coords] start-of-step coordinates */
+  const double* v_prev;             /* [dofs] start-of-step velocity (midpoint only; SAP order) */
+  const double* v_new;              /* [dofs] the solve's velocity (SAP order) */
+  const double* dt;                 /* [W] */
+  int32_t mode;                     /* SAPB_INTEGRATE_SAP_EULER / _MIDPOINT */
+  int32_t qd_public;                /* nonzero: joint_qd_out in public order (at the new coordinates) */
+  double* joint_q_out;              /* [coords], must not alias joint_q_in */
+  double* joint_qd_out;             /* [dofs] or NULL */
+  double* body_q_out;               /* [B][7] or NULL: forward kinematics of the new coordinates */
+  double* body_qd_out;              /* [B][6] or NULL: public body velocities [v; w] (needs qd_public
+                                     * and joint_qd_out) */
+} sapb_step_tail;
+
+int32_t sapb_step_tail_launch(const sapb_model_desc* model, const sapb_step_tail* tail, void* stream);
 
 /* ---- contact history ------------------------------------------------------
  * Impulses carried from one step's contact slots to the next step's by

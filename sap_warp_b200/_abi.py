@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 11
+SAPB_ABI_VERSION = 12
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -342,6 +342,12 @@ class StepIO(C.Structure):
     _fields_ = [("inp", StepInputs), ("dof", C.POINTER(DofTerms)), ("joint_q_out", _p), ("joint_qd_out", _p)]
 
 
+class StepTail(C.Structure):
+    _fields_ = [("joint_q_in", _p), ("v_prev", _p), ("v_new", _p), ("dt", _p), ("mode", C.c_int32),
+                ("qd_public", C.c_int32), ("joint_q_out", _p), ("joint_qd_out", _p), ("body_q_out", _p),
+                ("body_qd_out", _p)]
+
+
 class ContactHistory(C.Structure):
     _fields_ = [("num_envs", C.c_int32), ("max_contacts", C.c_int32), ("num_flat", C.c_int32),
                 ("contact_count", _p), ("contact_source", _p), ("flat_shape0", _p), ("flat_shape1", _p),
@@ -363,6 +369,7 @@ EXPORTS = {
     "sapb_destroy": (None, [_p]),
     "sapb_world_order": (C.c_int32, [_p, C.c_int32, _p, _p]),
     "sapb_contact_history_update": (C.c_int32, [C.POINTER(ContactHistory), _p]),
+    "sapb_step_tail_launch": (C.c_int32, [C.POINTER(ModelDesc), C.POINTER(StepTail), _p]),
     "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_occupancy": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_ldlt_blocks": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.c_int32]),

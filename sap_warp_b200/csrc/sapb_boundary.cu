@@ -23,6 +23,7 @@
 #include <cstdint>
 
 #include "sapb_internal.h"
+#include "sapb_joint.cuh"
 #include "sapb_spatial.cuh"
 
 namespace sapb {
@@ -33,14 +34,6 @@ struct BoundaryParams {
   sapb_model_desc m;
   int32_t num_joints, num_bodies, num_articulations;
 };
-
-// Quaternion product and transform composition as the reference's transform
-// algebra (no renormalisation).
-__device__ __forceinline__ Xf xf_mul(Xf a, Xf b) { return Xf{a.p + qrot(a.q, b.p), qmul(a.q, b.q)}; }
-__device__ __forceinline__ Xf xf_inv(Xf x) {
-  const Q4 qi = qconj(x.q);
-  return Xf{-qrot(qi, x.p), qi};
-}
 
 __global__ void public_to_sap_kernel(const BoundaryParams P, const double* joint_q, const double* body_q,
                                      const double* qd_pub, const double* f_pub, const double* bf_pub,
@@ -88,86 +81,14 @@ __global__ void sap_to_public_velocity_kernel(const BoundaryParams P, const doub
                                               double* qd_pub) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= P.num_joints) return;
-  const int jt = P.m.joint_type[j];
-  const int ds = P.m.joint_qd_start[j];
-  const int dim = P.m.joint_dof_dim[2 * j] + P.m.joint_dof_dim[2 * j + 1];
-  if (jt == SAPB_JOINT_FREE || jt == SAPB_JOINT_DISTANCE) {
-    const int qs = P.m.joint_q_start[j];
-    const int child = P.m.joint_child[j];
-    const Q4 q{joint_q[qs + 3], joint_q[qs + 4], joint_q[qs + 5], joint_q[qs + 6]};
-    const V3 r = qrot(q, load3(P.m.body_com + 3 * (size_t)child));
-    const V3 w = load3(qd_sap + ds), v_o = load3(qd_sap + ds + 3);
-    store3(qd_pub + ds, v_o + cross(w, r));
-    store3(qd_pub + ds + 3, w);
-  } else {
-    for (int a = 0; a < dim; ++a) qd_pub[ds + a] = qd_sap[ds + a];
-  }
+  public_velocity_joint(P.m, j, joint_q, qd_sap, qd_pub);
 }
 
 __global__ void eval_fk_kernel(const BoundaryParams P, const double* joint_q, const double* qd_pub, double* body_q,
                                double* body_qd) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= P.num_articulations) return;
-  const int j0 = P.m.articulation_start[a], j1 = P.m.articulation_start[a + 1];
-  for (int i = j0; i < j1; ++i) {
-    const int parent = P.m.joint_parent[i], child = P.m.joint_child[i];
-    if (child < 0 || child >= P.num_bodies) continue;
-    const int jt = P.m.joint_type[i];
-    const Xf X_pj = xf_load(P.m.joint_X_p + 7 * (size_t)i);
-    const Xf X_cj = xf_load(P.m.joint_X_c + 7 * (size_t)i);
-    Xf X_wpj = X_pj;
-    V3 v_wpj = v3(0, 0, 0), w_wpj = v3(0, 0, 0);
-    if (parent >= 0 && parent < P.num_bodies) {
-      const Xf X_wp = xf_load(body_q + 7 * (size_t)parent);
-      X_wpj = xf_mul(X_wp, X_pj);
-      const V3 com_w = X_wp.p + qrot(X_wp.q, load3(P.m.body_com + 3 * (size_t)parent));
-      const V3 r_p = X_wpj.p - com_w;
-      if (body_qd) {
-        const V3 w_p = load3(body_qd + 6 * (size_t)parent + 3);
-        v_wpj = load3(body_qd + 6 * (size_t)parent) + cross(w_p, r_p);
-        w_wpj = w_p;
-      }
-    }
-    const int qs = P.m.joint_q_start[i], ds = P.m.joint_qd_start[i];
-    Xf X_j{v3(0, 0, 0), qident()};
-    V3 vj = v3(0, 0, 0), wj = v3(0, 0, 0);
-    auto qd = [&](int k) { return qd_pub ? qd_pub[k] : 0.0; };
-    if (jt == SAPB_JOINT_PRISMATIC) {
-      const V3 ax = load3(P.m.joint_axis + 3 * (size_t)ds);
-      X_j.p = joint_q[qs] * ax;
-      vj = qd(ds) * ax;
-    } else if (jt == SAPB_JOINT_REVOLUTE) {
-      const V3 ax = load3(P.m.joint_axis + 3 * (size_t)ds);
-      X_j.q = qaxis_angle(ax, joint_q[qs]);
-      wj = qd(ds) * ax;
-    } else if (jt == SAPB_JOINT_BALL) {
-      X_j.q = Q4{joint_q[qs], joint_q[qs + 1], joint_q[qs + 2], joint_q[qs + 3]};
-      wj = v3(qd(ds), qd(ds + 1), qd(ds + 2));
-    } else if (jt == SAPB_JOINT_FREE || jt == SAPB_JOINT_DISTANCE) {
-      X_j = Xf{v3(joint_q[qs], joint_q[qs + 1], joint_q[qs + 2]),
-               Q4{joint_q[qs + 3], joint_q[qs + 4], joint_q[qs + 5], joint_q[qs + 6]}};
-      vj = v3(qd(ds), qd(ds + 1), qd(ds + 2));
-      wj = v3(qd(ds + 3), qd(ds + 4), qd(ds + 5));
-    } else if (jt == SAPB_JOINT_D6) {  // sim/sap_kinematics.py:170-215
-      const int lin = P.m.joint_dof_dim[2 * i], ang = P.m.joint_dof_dim[2 * i + 1];
-      V3 ax[3];
-      d6_mobilizer(P.m.joint_axis + 3 * (size_t)ds, joint_q + qs, lin, ang, &X_j, ax);
-      for (int k = 0; k < lin && k < 3; ++k) vj = vj + qd(ds + k) * load3(P.m.joint_axis + 3 * (size_t)(ds + k));
-      for (int k = 0; k < ang && k < 3; ++k) wj = wj + qd(ds + lin + k) * ax[k];
-    }
-    const Xf X_wc = xf_mul(xf_mul(X_wpj, X_j), xf_inv(X_cj));
-    const V3 lin = v_wpj + qrot(X_wpj.q, vj), ang = w_wpj + qrot(X_wpj.q, wj);
-    double* bq = body_q + 7 * (size_t)child;
-    store3(bq, X_wc.p);
-    bq[3] = X_wc.q.x;
-    bq[4] = X_wc.q.y;
-    bq[5] = X_wc.q.z;
-    bq[6] = X_wc.q.w;
-    if (body_qd) {
-      store3(body_qd + 6 * (size_t)child, lin);
-      store3(body_qd + 6 * (size_t)child + 3, ang);
-    }
-  }
+  fk_articulation(P.m, a, P.num_bodies, joint_q, qd_pub, body_q, body_qd);
 }
 
 BoundaryParams make_params(const sapb_model_desc* m) {

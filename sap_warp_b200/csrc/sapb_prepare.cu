@@ -18,6 +18,7 @@
 
 #include "sapb_device.cuh"
 #include "sapb_internal.h"
+#include "sapb_joint.cuh"
 #include "sapb_ldlt.cuh"
 #include "sapb_spatial.cuh"
 
@@ -978,52 +979,7 @@ __global__ void integrate_kernel(const sapb_model_desc m, const double* q_in, co
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int J = m.joints_per_world * m.num_worlds;
   if (j >= J) return;
-  const int jt = m.joint_type[j];
-  const int qs = m.joint_q_start[j], ds = m.joint_qd_start[j];
-  const int world = j / m.joints_per_world;
-  const double h = dt[world];
-  const bool mid = mode == SAPB_INTEGRATE_MIDPOINT;
-  auto vel = [&](int k) { return mid ? 0.5 * (v_prev[k] + v_new[k]) : v_new[k]; };
-  if (jt == SAPB_JOINT_PRISMATIC || jt == SAPB_JOINT_REVOLUTE) {
-    q_out[qs] = q_in[qs] + h * vel(ds);
-    return;
-  }
-  if (jt == SAPB_JOINT_FIXED) return;
-  if (jt == SAPB_JOINT_BALL || jt == SAPB_JOINT_FREE || jt == SAPB_JOINT_DISTANCE) {
-    const int o = jt == SAPB_JOINT_BALL ? 0 : 3;
-    if (o == 3)
-      for (int k = 0; k < 3; ++k) q_out[qs + k] = q_in[qs + k] + h * vel(ds + 3 + k);
-    const Q4 q{q_in[qs + o], q_in[qs + o + 1], q_in[qs + o + 2], q_in[qs + o + 3]};
-    const V3 w = v3(vel(ds), vel(ds + 1), vel(ds + 2));
-    Q4 qn = q;
-    if (!mid) {
-      // qdot = 0.5 [0, w] q (sim/solver_sap.py:158-178)
-      const double hd = 0.5 * h;
-      qn = Q4{q.x + hd * (q.w * w.x + w.y * q.z - w.z * q.y), q.y + hd * (q.w * w.y + w.z * q.x - w.x * q.z),
-              q.z + hd * (q.w * w.z + w.x * q.y - w.y * q.x), q.w - hd * (w.x * q.x + w.y * q.y + w.z * q.z)};
-      const double nn = sqrt(qn.x * qn.x + qn.y * qn.y + qn.z * qn.z + qn.w * qn.w);
-      if (nn > 0.0) qn = Q4{qn.x / nn, qn.y / nn, qn.z / nn, qn.w / nn};
-    } else {
-      // exp map of the midpoint angular velocity (sim/solver_sap.py:243-262)
-      const double wn = sqrt(dot(w, w));
-      const double angle = wn * h;
-      if (angle > 1.0e-12) {
-        const V3 axis = (1.0 / wn) * w;
-        const Q4 r = qaxis_angle(axis, angle);
-        qn = qmul(r, q);
-        const double nn = sqrt(qn.x * qn.x + qn.y * qn.y + qn.z * qn.z + qn.w * qn.w);
-        if (nn > 0.0) qn = Q4{qn.x / nn, qn.y / nn, qn.z / nn, qn.w / nn};
-      }
-    }
-    q_out[qs + o] = qn.x;
-    q_out[qs + o + 1] = qn.y;
-    q_out[qs + o + 2] = qn.z;
-    q_out[qs + o + 3] = qn.w;
-    return;
-  }
-  // D6 and other multi-axis scalar joints: q += h * qd per axis
-  const int dim = m.joint_dof_dim[2 * j] + m.joint_dof_dim[2 * j + 1];
-  for (int k = 0; k < dim; ++k) q_out[qs + k] = q_in[qs + k] + h * vel(ds + k);
+  integrate_joint(m, j, q_in, v_prev, v_new, dt[j / m.joints_per_world], mode, q_out);
 }
 
 int32_t integrate_launch(const sapb_model_desc* m, const double* q_in, const double* v_prev, const double* v_new,

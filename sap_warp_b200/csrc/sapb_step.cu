@@ -78,14 +78,14 @@ struct sapb_handle {
   sapb_step_options opts;
   int32_t W, n, C, B, Q;
   // free motion + contact rows
-  double *v_star, *vdot, *A, *J, *phi0, *w_eff, *mu, *stiffness, *tau_d, *factor, *vc_star;  // (factor, vc_star: unused)
+  double *v_star, *vdot, *A, *J, *phi0, *w_eff, *mu, *stiffness, *tau_d;
   int32_t *count, *body0, *body1, *truncated;
   void* prep_ws;
   size_t prep_ws_bytes;
   // contact history (previous-impulse warm start): keys, carried impulses,
   // the impulses before them, the extrapolated start impulses
-  int32_t *source, *key_shape, *key_count, *has_history;
-  double *key_point, *gamma_last, *gamma_older, *gamma_start, *v_start;
+  int32_t *key_shape, *key_count, *has_history;
+  double *key_point, *gamma_older, *gamma_start, *v_start;
   // solve
   double *v, *gamma, *gamma_prev, *cost, *grad_norm;
   int32_t *mode, *iters, *ls_iters, *converged, *status, *ws_accepted, *guess_flag, *order;
@@ -141,11 +141,11 @@ void sapb_step_options_default(sapb_step_options* o) {
 
 void sapb_destroy(sapb_handle* h) {
   if (!h) return;
-  void* ptrs[] = {h->v_star, h->vdot, h->A, h->J, h->phi0, h->w_eff, h->mu, h->stiffness, h->tau_d, h->factor,
-                  h->vc_star, h->count, h->body0, h->body1, h->truncated, h->prep_ws, h->v, h->gamma,
-                  h->gamma_prev, h->cost, h->grad_norm, h->mode, h->iters, h->ls_iters, h->converged, h->status,
+  void* ptrs[] = {h->v_star,    h->vdot,      h->A,     h->J,  h->phi0,     h->w_eff, h->mu,
+                  h->stiffness, h->tau_d,     h->count, h->body0, h->body1, h->truncated, h->prep_ws,
+                  h->v,         h->gamma,     h->gamma_prev, h->cost, h->grad_norm, h->mode, h->iters, h->ls_iters, h->converged, h->status,
                   h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws,
-                  h->source, h->key_shape, h->key_count, h->has_history, h->key_point, h->gamma_last,
+                  h->key_shape, h->key_count, h->has_history, h->key_point,
                   h->gamma_older, h->gamma_start, h->v_start};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -258,7 +258,6 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   if (cand) {
     take(dev_alloc(&h->v_start, Wn));
     take(dev_alloc(&h->gamma_prev, WC * 3));
-    take(dev_alloc(&h->gamma_last, WC * 3));
     take(dev_alloc(&h->key_shape, WC * 2));
     take(dev_alloc(&h->key_point, WC * 3));
     take(dev_alloc(&h->key_count, W));
@@ -290,7 +289,6 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     err = cudaMemcpy(h->body_dof_count, bcount.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemset(h->guess_flag, 0, sizeof(int32_t));
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_prev, 0, sizeof(double) * WC * 3);
-  if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_last, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess && cand) err = cudaMemset(h->key_count, 0, sizeof(int32_t) * W);
   if (err == cudaSuccess && cand) err = cudaMemset(h->has_history, 0, sizeof(int32_t) * WC);
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_older, 0, sizeof(double) * WC * 3);
@@ -347,7 +345,7 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     hist.key_shape = h->key_shape;
     hist.key_point = h->key_point;
     hist.key_count = h->key_count;
-    hist.gamma_prev = h->gamma_last;
+    hist.gamma_prev = h->gamma;
     hist.gamma_hist = h->gamma_prev;
     hist.has_history = h->has_history;
     hist.order = h->opts.impulse_history;
@@ -416,21 +414,22 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     st = sapb_world_order(h->iters, h->W, h->order, stream);
     if (st != SAPB_OK) return st;
   }
-  // position integration (sim/solver_sap.py:1267-1386); joints without
-  // coordinates to integrate keep theirs
-  cudaError_t err = cudaMemcpyAsync(io->joint_q_out, io->in.joint_q, sizeof(double) * h->Q, cudaMemcpyDeviceToDevice, s);
-  if (err != cudaSuccess) {
-    set_last_error("sapb_step: %s", cudaGetErrorString(err));
-    return SAPB_ERR_CUDA;
-  }
-  st = sapb_integrate_positions(&h->model, io->in.joint_q, io->in.joint_qd, h->v, io->in.dt,
-                                h->opts.position_integration, io->joint_q_out, stream);
+  // the tail in one launch: position integration (sim/solver_sap.py:1267-1386;
+  // fixed joints keep their coordinates) and the new SAP-order velocities
+  sapb_step_tail tail;
+  memset(&tail, 0, sizeof(tail));
+  tail.joint_q_in = io->in.joint_q;
+  tail.v_prev = io->in.joint_qd;
+  tail.v_new = h->v;
+  tail.dt = io->in.dt;
+  tail.mode = h->opts.position_integration;
+  tail.joint_q_out = io->joint_q_out;
+  tail.joint_qd_out = io->joint_qd_out;
+  st = sapb_step_tail_launch(&h->model, &tail, stream);
   if (st != SAPB_OK) return st;
-  err = cudaMemcpyAsync(io->joint_qd_out, h->v, sizeof(double) * (size_t)h->W * h->n, cudaMemcpyDeviceToDevice, s);
-  if (err == cudaSuccess) err = cudaMemsetAsync(h->guess_flag, 1, sizeof(int32_t), s);  // nonzero: warm start on
-  if (err == cudaSuccess && cand)
-    err = cudaMemcpyAsync(h->gamma_last, h->gamma, sizeof(double) * (size_t)h->W * h->C * 3, cudaMemcpyDeviceToDevice,
-                          s);
+  // nonzero: warm start from this solution; the next step's history reads
+  // this solve's impulses (h->gamma) before its own solve rewrites them
+  const cudaError_t err = cudaMemsetAsync(h->guess_flag, 1, sizeof(int32_t), s);
   if (err != cudaSuccess) {
     set_last_error("sapb_step: %s", cudaGetErrorString(err));
     return SAPB_ERR_CUDA;

@@ -926,6 +926,7 @@ class SolverSAP:
         dev = view.device
         self._v_guess_active = torch.zeros(1, dtype=I32, device=dev)
         self._q_out_tmp = torch.zeros(int(model.joint_coord_count), dtype=F64, device=dev)
+        self._tail = _abi.StepTail()
         # public-order boundary (sim/solver_sap.py:1198-1261): SAP-order copies of
         # public inputs, and FP64 staging of public outputs
         D, Bt = int(model.joint_dof_count), int(model.body_count)
@@ -964,11 +965,11 @@ class SolverSAP:
         self._gamma_cand = torch.zeros(2, view.W, max(C, 1), 3, dtype=F64, device=dev)
         # [1] holds the start impulses of this step's slots: the last solves'
         # impulses carried by contact identity (sapb_contact_history_update)
-        # from the last solve's impulses by its own slots (_gamma_last) and
+        # from the last solve's impulses by its own slots (the solve's
+        # contact_gamma, read before this step's solve rewrites it) and
         # extrapolated over the impulses before them (_gamma_carried: the
         # last solve's by this step's slots, _gamma_older: the one before)
         self._gamma_prev = self._gamma_cand[1]
-        self._gamma_last = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self._gamma_carried = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self._gamma_older = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self._normal_up = torch.zeros(view.W, max(C, 1), dtype=F64, device=dev)
@@ -979,12 +980,13 @@ class SolverSAP:
             self._hist_key_count = torch.zeros(view.W, dtype=I32, device=dev)
             self.has_history = torch.zeros(view.W, max(C, 1), dtype=I32, device=dev)
             # the contact history, run by the free-motion launch on its slots:
-            # the last solve's impulses (_gamma_last, by its slots) carried by
+            # the last solve's impulses (contact_gamma, by its slots) carried by
             # contact identity and extrapolated into the start impulses
             H = _abi.ContactHistory()
             H.key_shape, H.key_point = _ptr(self._hist_key_shape), _ptr(self._hist_key_point)
             H.key_count = _ptr(self._hist_key_count)
-            H.gamma_prev, H.gamma_hist, H.has_history = (_ptr(self._gamma_last), _ptr(self._gamma_carried),
+            H.gamma_prev, H.gamma_hist, H.has_history = (_ptr(self.contact_solve.contact_gamma),
+                                                         _ptr(self._gamma_carried),
                                                          _ptr(self.has_history))
             H.order, H.gamma_older, H.gamma_start = (self.impulse_history, _ptr(self._gamma_older),
                                                      _ptr(self._gamma_prev))
@@ -1176,7 +1178,6 @@ class SolverSAP:
         self._v_guess_active.zero_()
         if hasattr(self, "_gamma_cand"):
             self._gamma_cand.zero_()
-            self._gamma_last.zero_()
             self._gamma_carried.zero_()
             self._gamma_older.zero_()
         if hasattr(self, "_hist_key_count"):
@@ -1266,28 +1267,45 @@ class SolverSAP:
                                           ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)),
                   "sapb_world_order")
         mark("integrate")
-        # position integration (sim/solver_sap.py:1267-1386)
-        mode = _abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint" else _abi.SAPB_INTEGRATE_SAP_EULER
+        # the tail in one launch (sapb_step_tail_launch): position integration
+        # (sim/solver_sap.py:1267-1386), the new velocities in the output's
+        # order and, for a public-order output, the forward kinematics of the
+        # new pose (:1467-1469); outputs written in place when they are
+        # contiguous FP64, else staged and copied
+        T = self._tail
         q_in = self.contact_jacobian._q
-        q_out = state_out.joint_q if (state_out.joint_q.dtype == F64 and state_out.joint_q.is_contiguous()
+        direct = lambda t, n: (t is not None and t.dtype == F64 and t.is_contiguous() and t.numel() == n)
+        q_out = state_out.joint_q if (direct(state_out.joint_q, q_in.numel())
                                       and state_out.joint_q.data_ptr() != q_in.data_ptr()) else self._q_out_tmp
-        q_out.copy_(q_in)  # fixed joints keep their coordinates
-        status = load().sapb_integrate_positions(
-            ctypes.byref(self.view.desc), _ptr(q_in), _ptr(v0), _ptr(sr.v_flat), _ptr(self.contact_jacobian.dt_world),
-            mode, _ptr(q_out), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream))
-        check(status, "sapb_integrate_positions")
-        if q_out is not state_out.joint_q:
-            state_out.joint_q.copy_(q_out)
+        qd_out = state_out.joint_qd if direct(state_out.joint_qd, sr.v_flat.numel()) else self._qd_pub_out
+        T.joint_q_in, T.v_prev, T.v_new = _ptr(q_in), _ptr(v0), _ptr(sr.v_flat)
+        T.dt = _ptr(self.contact_jacobian.dt_world)
+        T.mode = _abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint" else _abi.SAPB_INTEGRATE_SAP_EULER
+        T.qd_public = 1 if output_public else 0
+        T.joint_q_out, T.joint_qd_out = _ptr(q_out), _ptr(qd_out)
+        bq_out = bqd_out = None
         if output_public:
-            self._boundary_out(state_out, q_out, sr.v_flat)
-        else:
-            state_out.joint_qd.copy_(sr.v_flat)
+            nb = self._body_q_out.numel()
+            bq_out = state_out.body_q if direct(state_out.body_q, nb) else self._body_q_out
+            if getattr(state_out, "body_qd", None) is not None:
+                bqd_out = state_out.body_qd if direct(state_out.body_qd, self._body_qd_out.numel()) \
+                    else self._body_qd_out
+        T.body_q_out, T.body_qd_out = _ptr(bq_out), _ptr(bqd_out)
+        check(load().sapb_step_tail_launch(ctypes.byref(self.view.desc), ctypes.byref(T),
+                                           ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)),
+              "sapb_step_tail_launch")
+        if q_out is not state_out.joint_q:
+            state_out.joint_q.copy_(q_out.reshape(state_out.joint_q.shape))
+        if qd_out is not state_out.joint_qd:
+            state_out.joint_qd.copy_(qd_out.reshape(state_out.joint_qd.shape))
+        if bq_out is not None and bq_out is not state_out.body_q and state_out.body_q is not None:
+            state_out.body_q.copy_(bq_out.reshape(state_out.body_q.shape))
+        if bqd_out is not None and bqd_out is not state_out.body_qd:
+            state_out.body_qd.copy_(bqd_out.reshape(state_out.body_qd.shape))
         if state_out.body_f is not None and state_in.body_f is not None and state_out.body_f is not state_in.body_f:
             state_out.body_f.copy_(state_in.body_f)
         mark(None)
         self._v_guess_active.fill_(1)  # warm start from this step's solution (sim/solver_sap.py:1441-1451)
-        if self.warm_start != "previous_velocity":
-            self._gamma_last.copy_(sr.contact_gamma)
         self.last_contact_jacobian_result = cr
         self.last_contact_solve_result = sr
         self.last_solve_iterations = -1
@@ -1325,23 +1343,6 @@ class SolverSAP:
                                  joint_target_vel=control.joint_target_vel, joint_act=control.joint_act,
                                  joint_f_order="sap")
         return state_in, control, getattr(state_out, "joint_qd_order", "sap") == "public"
-
-    def _boundary_out(self, state_out: SapState, q_out: torch.Tensor, v_sap: torch.Tensor) -> None:
-        """SAP-order result -> public output (sim/solver_sap.py:1467-1469): the
-        public joint velocities at the new pose, then the forward kinematics
-        of the new public coordinates into body_q / body_qd."""
-        lib, stream = load(), ctypes.c_void_p(torch.cuda.current_stream(self.view.device).cuda_stream)
-        desc = ctypes.byref(self.view.desc)
-        check(lib.sapb_sap_to_public_velocity(desc, _ptr(q_out), _ptr(v_sap), _ptr(self._qd_pub_out), stream),
-              "sapb_sap_to_public_velocity")
-        state_out.joint_qd.copy_(self._qd_pub_out)
-        want_qd = getattr(state_out, "body_qd", None) is not None
-        check(lib.sapb_eval_fk(desc, _ptr(q_out), _ptr(self._qd_pub_out), _ptr(self._body_q_out),
-                               _ptr(self._body_qd_out) if want_qd else None, stream), "sapb_eval_fk")
-        if state_out.body_q is not None:
-            state_out.body_q.copy_(self._body_q_out.reshape(state_out.body_q.shape))
-        if want_qd:
-            state_out.body_qd.copy_(self._body_qd_out.reshape(state_out.body_qd.shape))
 
     def update_contacts(self, contacts: SapContacts) -> None:
         raise NotImplementedError("SolverSAP does not expose contact-force writeback yet.")

@@ -113,3 +113,54 @@ def test_public_order_step_matches_sap_order_step(cuda_device):
     bq_ref, bqd_ref = ob.eval_fk(g, q_out, v_pub_ref)
     np.testing.assert_allclose(pub_out.body_q.cpu().numpy(), bq_ref, rtol=1e-10, atol=1e-10)
     np.testing.assert_allclose(pub_out.body_qd.cpu().numpy(), bqd_ref, rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.parametrize("kind", ["humanoid", "joints", "arm_box"])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fused_tail_equals_the_separate_launches(cuda_device, kind, mode):
+    """sapb_step_tail_launch (integration, velocities in SAP or public order,
+    forward kinematics of the new pose, one CTA per world) writes the same
+    bits as sapb_integrate_positions after a copy of the coordinates, then
+    sapb_sap_to_public_velocity and sapb_eval_fk."""
+    from sap_warp_b200 import _abi
+
+    rng, tpl, g, q = _case(kind, 17)
+    model = models.to_model(tpl, g, q.reshape(4, -1), cuda_device)
+    view = _ModelView(model)
+    D, B = g["counts"]["dofs"], g["counts"]["bodies"]
+    dev = cuda_device
+    tq, v0, v1 = _t(q, dev), _t(rng.normal(size=D), dev), _t(rng.normal(size=D), dev)
+    dt = torch.full((4,), 2.0e-3, dtype=torch.float64, device=dev)
+    lib, s = load(), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    d = ctypes.byref(view.desc)
+    # separate launches
+    q_sep = tq.clone()
+    check(lib.sapb_integrate_positions(d, tq.data_ptr(), v0.data_ptr(), v1.data_ptr(), dt.data_ptr(), mode,
+                                       q_sep.data_ptr(), s), "integrate")
+    qd_pub = torch.zeros(D, dtype=torch.float64, device=dev)
+    check(lib.sapb_sap_to_public_velocity(d, q_sep.data_ptr(), v1.data_ptr(), qd_pub.data_ptr(), s), "public")
+    bq_sep = torch.zeros(B, 7, dtype=torch.float64, device=dev)
+    bqd_sep = torch.zeros(B, 6, dtype=torch.float64, device=dev)
+    check(lib.sapb_eval_fk(d, q_sep.data_ptr(), qd_pub.data_ptr(), bq_sep.data_ptr(), bqd_sep.data_ptr(), s), "fk")
+    for public in (0, 1):
+        q_out = torch.full_like(tq, float("nan"))
+        qd_out = torch.full_like(v1, float("nan"))
+        bq = torch.full((B, 7), float("nan"), dtype=torch.float64, device=dev)
+        bqd = torch.full((B, 6), float("nan"), dtype=torch.float64, device=dev)
+        T = _abi.StepTail()
+        T.joint_q_in, T.v_prev, T.v_new, T.dt = tq.data_ptr(), v0.data_ptr(), v1.data_ptr(), dt.data_ptr()
+        T.mode, T.qd_public = mode, public
+        T.joint_q_out, T.joint_qd_out = q_out.data_ptr(), qd_out.data_ptr()
+        T.body_q_out = bq.data_ptr()
+        T.body_qd_out = bqd.data_ptr() if public else None
+        check(lib.sapb_step_tail_launch(d, ctypes.byref(T), s), "sapb_step_tail_launch")
+        torch.cuda.synchronize()
+        assert torch.equal(q_out, q_sep)
+        assert torch.equal(qd_out, qd_pub if public else v1)
+        if public:
+            assert torch.equal(bq, bq_sep) and torch.equal(bqd, bqd_sep)
+        else:
+            assert torch.equal(bq, bq_sep)  # poses do not depend on the velocities
+    # aliasing the input coordinates is refused
+    T.joint_q_out = tq.data_ptr()
+    assert lib.sapb_step_tail_launch(d, ctypes.byref(T), s) == _abi.SAPB_ERR_INVALID_ARGUMENT
