@@ -198,6 +198,8 @@ def _as_tensor(x, device=None):
         return x
     if hasattr(x, "__dlpack__"):
         return torch.from_dlpack(x)
+    if hasattr(x, "__cuda_array_interface__"):
+        return torch.as_tensor(x, device=device if device is not None else "cuda")
     return torch.as_tensor(x, device=device)
 
 
