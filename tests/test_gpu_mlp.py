@@ -114,9 +114,14 @@ def test_backward_matches_oracle_and_autograd(cuda_device, rows):
     _, gm, _ = om.backward(params, x, t, mirror=True)
     _, gx, _ = om.backward(params, x, t, mirror=False)
     gm, gx = om.unpack(gm), om.unpack(gx)
+    # measured on B200: <= 5e-4 from the mirror (the kernels' own rounding
+    # points), <= 4.3e-3 from float64 autograd -- the mirror's own distance
+    # from autograd (BF16 activations), which the kernels must not exceed by
+    # more than the mirror difference
     for k in gm:
-        assert rel_norm(g[k], gm[k]) < 2e-2, (k, rel_norm(g[k], gm[k]))
-        assert rel_norm(g[k], gx[k]) < 6e-2, (k, rel_norm(g[k], gx[k]))
+        assert rel_norm(g[k], gm[k]) < 2e-3, (k, rel_norm(g[k], gm[k]))
+        assert rel_norm(g[k], gx[k]) < 1e-2, (k, rel_norm(g[k], gx[k]))
+        assert rel_norm(g[k], gx[k]) <= rel_norm(gm[k], gx[k]) + 2e-3, k
 
 
 def test_adam_matches_oracle(cuda_device):
