@@ -55,8 +55,8 @@ sys.path.insert(0, ROOT)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one contact
 # solve launch of the headline arm on this workload (4096 humanoids, learned
 # start, FP32 Hessian; the fifth step after the 100-step settling prefix),
-# from one ncu capture: 167.60 MB read + 9.28 MB written.
-NCU_SOLVE_TRAFFIC_BYTES = 176_878_592
+# from one ncu capture: 159.64 MB read + 5.68 MB written.
+NCU_SOLVE_TRAFFIC_BYTES = 165_321_984
 
 METRIC = "world-steps/s, 4096 humanoids: learned+FP32 vs plain FP64, same B200, same tol"
 WORLDS = 4096
@@ -78,17 +78,16 @@ def parse():
     return ap.parse_args()
 
 
-def solve_bytes_per_world(n: int, counts: np.ndarray, candidate_sets: int) -> np.ndarray:
+def solve_bytes_per_world(n: int, counts: np.ndarray, velocities: int = 0, impulse_sets: int = 0,
+                          factor: bool = False) -> np.ndarray:
     """Compulsory FP64 I/O of the contact solve per world with the actual
     contact count C: reads A (n^2), J (3Cn), v*, v0, v_guess (3n), 5 contact
     parameters (5C); writes v, v_guess (2n), gamma (3C), mode (C/2 words);
-    plus for candidate starts the factor (n^2) and the impulse sets (3C
-    each)."""
+    plus for candidate starts the start or base velocities (n each), the
+    impulse sets (3C each) and the factor (n^2) where it is read."""
     C = counts.astype(np.int64)
     b = 8 * (n * n + 3 * C * n + 3 * n + 5 * C) + 8 * (2 * n + 3 * C) + 4 * C
-    if candidate_sets:
-        b = b + 8 * (n * n + candidate_sets * 3 * C)
-    return b
+    return b + 8 * (velocities * n + impulse_sets * 3 * C + (n * n if factor else 0))
 
 
 class ClockSampler:
@@ -565,19 +564,25 @@ def main():
     tm = problem_to_device(mix, dev)
     mbuf = ContactSolveBuffers(mix.num_envs, mix.dof_per_env, mix.max_contacts, dev)
     order = torch.as_tensor(scenes.work_order(mix), dtype=torch.int32).to(dev)
-    uneven = {"worlds": mix.num_envs, "dofs": "13 (arm+box, 2 trees) / 18 / 35, padded to 35",
+    uneven = {"worlds": mix.num_envs, "dofs": "13 (arm+box, 2 trees) / 18 / 35: padded to 35 (identity blocks), "
+                                              "or each world's own count (per_world_dofs: dof_count, compact storage)",
               "contacts": "2-8 gripper / min(Poisson(12), 64)"}
-    for label, opts, wo in (("fp64_sorted", make_options("armijo_decay"), order),
-                            ("fp32_sorted", make_options("armijo_decay", hessian_precision="fp32"), order),
-                            ("fp32_index_order", make_options("armijo_decay", hessian_precision="fp32"), None)):
+    tc = problem_to_device(scenes.compact_problem(mix), dev)
+    dcount = torch.as_tensor(mix.dofs_active, dtype=torch.int32).to(dev)
+    for label, opts, wo, tt, dc in (
+            ("fp64_sorted", make_options("armijo_decay"), order, tm, None),
+            ("fp32_sorted", make_options("armijo_decay", hessian_precision="fp32"), order, tm, None),
+            ("fp32_index_order", make_options("armijo_decay", hessian_precision="fp32"), None, tm, None),
+            ("fp64_per_world_dofs", make_options("armijo_decay"), order, tc, dcount),
+            ("fp32_per_world_dofs", make_options("armijo_decay", hessian_precision="fp32"), order, tc, dcount)):
         for _ in range(max(args.warmup, 1)):
-            contact_solve(**tm, buffers=mbuf, options=opts, world_order=wo)
+            contact_solve(**tt, buffers=mbuf, options=opts, world_order=wo, dof_count=dc)
         barrier()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         k_mix = max(1, min(args.steps, 20))
         a0.record(stream)
         for _ in range(k_mix):
-            contact_solve(**tm, buffers=mbuf, options=opts, world_order=wo)
+            contact_solve(**tt, buffers=mbuf, options=opts, world_order=wo, dof_count=dc)
         a1.record(stream)
         barrier()
         ms = max_over_ranks(a0.elapsed_time(a1) / k_mix)
@@ -713,7 +718,9 @@ def main():
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     n = 35
     solve_ms = fast["stages"].get("contact_solve", float("nan"))
-    alg = float(solve_bytes_per_world(n, fast["counts"], 2).sum())
+    # learned arm on a fixed contact set: the base velocity (the history's
+    # start) and the network's impulse set, all zero, so no factor is read
+    alg = float(solve_bytes_per_world(n, fast["counts"], velocities=1, impulse_sets=1).sum())
     achieved = alg / (solve_ms * 1e-3) / 1e9
     # FP64 arithmetic of the plain arm's solve (algorithmic count from its
     # measured Newton iterations and line-search trials) against the measured

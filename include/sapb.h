@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 12
+#define SAPB_ABI_VERSION 13
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -187,6 +187,15 @@ typedef struct sapb_contact_problem {
    * A^-1 J^T gamma_c (NULL: base = v*).  A world whose candidate impulses are
    * all zero then starts at the base without reading dynamics_factor. */
   const double* gamma0_base;
+  /* Optional [E] DOF count of each world (uneven batches without padding,
+   * 1..dof_per_env): world e uses the first dof_count[e] of its dof_per_env
+   * DOF slots.  Its A block is stored compact at the start of its slot
+   * (dof_count[e]^2 values, row stride dof_count[e]), its Jacobian rows
+   * likewise (stride dof_count[e]), its per-DOF arrays (v*, v0, v_guess, v,
+   * dof terms, candidates, factor) at e * dof_per_env + [0, dof_count[e]);
+   * the rest of its v slots are written as zero.  Runs the runtime-size
+   * kernel.  NULL: every world has dof_per_env DOFs. */
+  const int32_t* dof_count;
 } sapb_contact_problem;
 
 /* Outputs: the SapContactSolveResult fields a caller reads

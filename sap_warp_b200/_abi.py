@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 12
+SAPB_ABI_VERSION = 13
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -125,6 +125,7 @@ class ContactProblem(C.Structure):
         ("v_candidates", _p),
         ("v_candidate_count", C.c_int32),
         ("gamma0_base", _p),
+        ("dof_count", _p),
     ]
 
 

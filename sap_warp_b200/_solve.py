@@ -149,6 +149,7 @@ def build_problem(
     v_candidates: torch.Tensor | None = None,
     gamma0_base: torch.Tensor | None = None,
     dynamics_factor: torch.Tensor | None = None,
+    dof_count: torch.Tensor | None = None,
 ) -> _abi.ContactProblem:
     """sapb_contact_problem over device tensors (shapes and dtypes checked)."""
     E, n, C = num_envs, dof_per_env, max_contacts
@@ -181,6 +182,7 @@ def build_problem(
         P.v_candidate_count = int(v_candidates.numel() // max(E * n, 1))
     P.gamma0_base = _ptr(gamma0_base, F64, E * n, "gamma0_base")
     P.dynamics_factor = _ptr(dynamics_factor, F64, E * n * n, "dynamics_factor")
+    P.dof_count = _ptr(dof_count, I32, E, "dof_count")
     if dof_terms is not None:
         P.dof = ctypes.pointer(dof_terms.struct)
     return P

@@ -50,7 +50,9 @@ int ldlt_block_widths(int n, int32_t* out, int capacity) {
 
 static cudaError_t solve_dispatch(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
   // Kernels specialised on the DOF count of the common trees (humanoid 35,
-  // quadruped 18, arm + box 13, single free body 6); a generic one otherwise.
+  // quadruped 18, arm + box 13, single free body 6); a generic one otherwise
+  // and for per-world DOF counts.
+  if (P.p.dof_count) return launch_solve_ns<0>(P, fp32, stream, blocks_out);
   switch (P.p.dof_per_env) {
 #define SAPB_DISPATCH_N(NV) \
   case NV:                  \

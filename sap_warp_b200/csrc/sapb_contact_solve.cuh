@@ -105,7 +105,9 @@ struct World {
   __device__ __forceinline__ int dofs() const { return NS > 0 ? NS : n; }
   __device__ __forceinline__ int ldJ() const { return NS > 0 ? (NS + 3) / 4 * 4 + 1 : L.ldJ; }
   __device__ __forceinline__ int ldH() const { return NS > 0 ? ((NS % 2 == 0) ? NS + 1 : NS) : L.ldH; }
-  __device__ __forceinline__ int nb() const { return NS > 0 ? (NS + 3) / 4 : L.nb; }
+  __device__ __forceinline__ int nb() const { return NS > 0 ? (NS + 3) / 4 : (n + 3) / 4; }
+  // shift of the kernel's triangle list (built for L.n DOFs) to this world's n
+  __device__ __forceinline__ int tri_shift() const { return NS > 0 ? 0 : L.n - n; }
   __device__ double* V(int k) const { return vec + (size_t)k * ldJ(); }
   __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
   __device__ double* part(int which, int warp) const {
@@ -415,7 +417,7 @@ __device__ void assemble_hessian(const World<NT, HT, NS>& w, double diag_shift) 
 template <int NT, typename HT, int NS, int LB>
 __device__ void factor_and_solve(const World<NT, HT, NS>& w) {
   HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
-  ldlt_blocked<NT, HT, LB>(w.H, w.dofs(), w.ldH(), dinv, w.tri);
+  ldlt_blocked<NT, HT, LB>(w.H, w.dofs(), w.ldH(), dinv, w.tri, w.tri_shift());
   if ((threadIdx.x >> 5) == 0) {
     const bool ok = ldlt_pivots_ok_warp<HT>(w.H, w.dofs(), w.ldH());
     if (threadIdx.x == 0) *w.factor_ok = ok ? 1 : 0;
@@ -479,10 +481,13 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   __shared__ unsigned long long s_partmask;
   __shared__ int s_factor_ok;
   const int tid = threadIdx.x;
-  const int n = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
-  const Layout L = make_layout(n, C, (int)sizeof(HT));
+  // n_max: the DOF slots of a world in the arrays (and the shared-memory
+  // layout); a world's own DOF count may be smaller (dof_count, generic
+  // kernel only), its arrays compact at the start of its slots
+  const int n_max = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
+  const Layout L = make_layout(n_max, C, (int)sizeof(HT));
   const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
-  build_triangle_list<NT>(reinterpret_cast<uint16_t*>(smem + L.off_tri), n);
+  build_triangle_list<NT>(reinterpret_cast<uint16_t*>(smem + L.off_tri), n_max);
 
   if (tid == 0) s_next = atomicAdd(P.queue, 1);
   for (;;) {
@@ -500,28 +505,29 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       const int nt = s_next;
       const int nx = nt < P.p.num_envs ? (P.p.world_order ? P.p.world_order[nt] : nt) : P.p.num_envs;
       if (nx >= 0 && nx < P.p.num_envs) {
-        const char* a0 = reinterpret_cast<const char*>(P.p.dynamics_matrix + (size_t)nx * n * n);
-        const size_t abytes = sizeof(double) * (size_t)n * n;
+        const char* a0 = reinterpret_cast<const char*>(P.p.dynamics_matrix + (size_t)nx * n_max * n_max);
+        const size_t abytes = sizeof(double) * (size_t)n_max * n_max;
         int cnt = P.p.contact_count[nx];
         cnt = cnt < 0 ? 0 : (cnt > C ? C : cnt);
-        const char* j0 = reinterpret_cast<const char*>(P.p.jacobian + (size_t)nx * C * 3 * n);
-        const size_t jbytes = sizeof(double) * (size_t)cnt * 3 * n;
+        const char* j0 = reinterpret_cast<const char*>(P.p.jacobian + (size_t)nx * C * 3 * n_max);
+        const size_t jbytes = sizeof(double) * (size_t)cnt * 3 * n_max;
         for (size_t off = (size_t)tid * 128; off < abytes; off += (size_t)NT * 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(a0 + off));
         for (size_t off = (size_t)tid * 128; off < jbytes; off += (size_t)NT * 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(j0 + off));
         if (P.p.v_candidates) {
           const int KV = P.p.v_candidate_count > 1 ? P.p.v_candidate_count : 1;
-          const size_t vbytes = sizeof(double) * (size_t)n;
+          const size_t vbytes = sizeof(double) * (size_t)n_max;
           for (int k = 0; k < KV; ++k) {
-            const char* v0p = reinterpret_cast<const char*>(P.p.v_candidates + ((size_t)k * P.p.num_envs + nx) * n);
+            const char* v0p =
+                reinterpret_cast<const char*>(P.p.v_candidates + ((size_t)k * P.p.num_envs + nx) * n_max);
             for (size_t off = (size_t)tid * 128; off < vbytes; off += (size_t)NT * 128)
               asm volatile("prefetch.global.L2 [%0];" ::"l"(v0p + off));
           }
         }
         if (P.p.gamma0) {
           if (P.p.dynamics_factor) {
-            const char* f0 = reinterpret_cast<const char*>(P.p.dynamics_factor + (size_t)nx * n * n);
+            const char* f0 = reinterpret_cast<const char*>(P.p.dynamics_factor + (size_t)nx * n_max * n_max);
             for (size_t off = (size_t)tid * 128; off < abytes; off += (size_t)NT * 128)
               asm volatile("prefetch.global.L2 [%0];" ::"l"(f0 + off));
           }
@@ -536,8 +542,14 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       }
     }
 
+    int n_world = n_max;
+    if (NS == 0 && P.p.dof_count) {
+      n_world = P.p.dof_count[e];
+      n_world = n_world < 1 ? 1 : (n_world > n_max ? n_max : n_world);
+    }
+    const int n = n_world;
     World<NT, HT, NS> w{L,
-                    P.p.dynamics_matrix + (size_t)e * n * n,
+                    P.p.dynamics_matrix + (size_t)e * n_max * n_max,
                     reinterpret_cast<double*>(smem + L.off_J),
                     reinterpret_cast<HT*>(smem + L.off_scr),
                     reinterpret_cast<HT*>(smem + L.off_H),
@@ -555,12 +567,12 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
     if (count < 0) count = 0;
     w.count = count;
     const double dt = P.p.dt[e];
-    const size_t base = (size_t)e * n;
+    const size_t base = (size_t)e * n_max;
 
     // ---- stage J, per-contact constants and vectors -------------------------
     {
       const int rows = 3 * count;
-      const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n;
+      const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n_max;
       const int ldj = w.ldJ();
       // Flat copy of the contiguous rows*n block by asynchronous 8-byte
       // copies (all in flight at once, completed before the barrier after the
@@ -618,7 +630,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
         int coord = D.dof_coord_index[dof];
         if (coord >= D.joint_coord_count) coord = -1;
         int target = D.dof_target_index[dof];
-        if (target < 0 || target >= P.p.num_envs * n) target = (int)dof;
+        if (target < 0 || target >= P.p.num_envs * n_max) target = (int)dof;
         if (D.joint_target_mode[target] != 0) {
           const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
           if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {
@@ -780,13 +792,13 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
           }
         };
         for (int k = 0; k < KV; ++k) {
-          const double* vk = P.p.v_candidates + ((size_t)k * P.p.num_envs + e) * n;
+          const double* vk = P.p.v_candidates + ((size_t)k * P.p.num_envs + e) * n_max;
           for (int i = tid; i < n; i += NT)
             w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? __ldg(vk + i) : w.V(V_VSTAR)[i];
           try_start(k + 1);
         }
         if (KG > 0) {
-          const double* base_g = P.p.gamma0_base ? P.p.gamma0_base + (size_t)e * n : nullptr;
+          const double* base_g = P.p.gamma0_base ? P.p.gamma0_base + (size_t)e * n_max : nullptr;
           // a world whose candidate impulses are all zero starts at the base
           int nz = 0;
           for (int q = tid; q < KG * 3 * count; q += NT) {
@@ -801,7 +813,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
             const int ldj = w.ldJ();
             if (P.p.dynamics_factor) {
               // the free motion's LDL^T of A
-              const double* Lg = P.p.dynamics_factor + (size_t)e * n * n;
+              const double* Lg = P.p.dynamics_factor + (size_t)e * n_max * n_max;
               load_lower<NT, HT, NS>(w, Lg, nullptr, 0.0);
               HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
               for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
@@ -809,7 +821,8 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
             } else {
               load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
               __syncthreads();
-              ldlt_blocked<NT, HT, LB>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri);  // the factor of A
+              ldlt_blocked<NT, HT, LB>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri,
+                                       w.tri_shift());  // the factor of A
             }
             // Two sets at a time: stage their impulses in the (here unused)
             // scratch, form J^T gamma for both (threads 0-63 set k0, 64-127
@@ -924,7 +937,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       }
     }
     // ---- outputs ------------------------------------------------------------
-    for (int i = tid; i < n; i += NT) P.out.v[base + i] = w.V(V_V)[i];
+    for (int i = tid; i < n_max; i += NT) P.out.v[base + i] = i < n ? w.V(V_V)[i] : 0.0;
     for (int c = tid; c < C; c += NT) {
       const size_t ci = (size_t)e * C + c;
       const bool live = evaluated && c < count;

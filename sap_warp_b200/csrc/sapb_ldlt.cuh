@@ -21,7 +21,8 @@ __device__ __forceinline__ void build_triangle_list(uint16_t* tri, int n) {
   }
 }
 
-// In-place right-looking LDL^T of the lower triangle of H (row stride ldH):
+// In-place right-looking LDL^T of the lower triangle of H (row stride ldH;
+// tri: the triangle list of build_triangle_list for n + tri_shift DOFs):
 // afterwards H_ik = L_ik d_k below the diagonal (L unit lower), d_k on it,
 // dinv[k] = 1/d_k.  B-column blocks, two barriers per block:
 // every thread factors the block's diagonal block in
@@ -33,7 +34,7 @@ __device__ __forceinline__ void build_triangle_list(uint16_t* tri, int n) {
 //   d_k = H_kk - sum_{e<k} W_ke^2 / d_e,  W_ik = H_ik - sum_{e<k} W_ie W_ke / d_e.
 // H must be complete when called (barrier before); complete on return.
 template <int NT, typename T, int B>
-__device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri) {
+__device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri, int tri_shift = 0) {
   static_assert(B >= 1 && B <= 8, "block width");
   const int tid = threadIdx.x;
   for (int K = 0; K < n; K += B) {
@@ -103,7 +104,7 @@ __device__ void ldlt_blocked(T* H, int n, int ldH, T* dinv, const uint16_t* tri)
     const int cnt = rest * (rest + 1) / 2;
     for (int e = tid; e < cnt; e += NT) {
       const int ij = tri[e];
-      const int i = ij >> 8, j = ij & 255;
+      const int i = (ij >> 8) - tri_shift, j = (ij & 255) - tri_shift;
       T acc = H[(size_t)i * ldH + j];
 #pragma unroll
       for (int c = 0; c < B; ++c)

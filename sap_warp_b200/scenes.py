@@ -434,6 +434,26 @@ def mixed_contact_problem(num_worlds: int, seed: int = 3, max_contacts: int = 64
     return prob, parts
 
 
+def compact_problem(p: ContactProblemArrays) -> ContactProblemArrays:
+    """A padded mixed batch (dofs_active set) in the layout of per-world DOF
+    counts (sapb_contact_problem.dof_count): world e's A block and Jacobian
+    rows stored compact, row stride dofs_active[e], at the start of its
+    slots; per-DOF arrays unchanged (the world's DOFs first in its slots).
+    The padding's identity block and zero columns are dropped."""
+    assert p.dofs_active is not None
+    E, n, C = p.num_envs, p.dof_per_env, p.max_contacts
+    A = np.zeros((E, n * n))
+    J = np.zeros((E, C * 3 * n))
+    for e in range(E):
+        ne = int(p.dofs_active[e])
+        A[e, :ne * ne] = p.dynamics_matrix[e, :ne, :ne].reshape(-1)
+        J[e, :C * 3 * ne] = p.jacobian[e, :, :, :ne].reshape(-1)
+    q = ContactProblemArrays(**{f: getattr(p, f) for f in p.__dataclass_fields__})
+    q.dynamics_matrix = A.reshape(E, n, n)
+    q.jacobian = J.reshape(E, C, 3, n)
+    return q
+
+
 def work_order(prob: ContactProblemArrays) -> np.ndarray:
     """Worlds by descending estimated solve work n^3/3 + C n^2 (n the
     world's own DOF count): the order a persistent kernel should take them in

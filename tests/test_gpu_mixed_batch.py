@@ -69,3 +69,30 @@ def test_mixed_batch_fp32_hessian(cuda_device, oracle, mixed):
     vr = oracle.solve(prob, "armijo_decay")["v"].reshape(prob.num_envs, -1)
     err = np.abs(v - vr).max(1) / np.abs(vr).max(1)
     assert np.quantile(err, 0.98) <= 1e-6 and err.max() <= 1e-4, err.max()
+
+
+def test_per_world_dof_counts_without_padding(cuda_device, mixed):
+    """The same batch with each world's own DOF count (dof_count, compact
+    storage, no identity padding): every world equals its homogeneous solve
+    (the specialised kernels of its size) to rounding, with the same Newton
+    iterations up to one, and the padding of v is written as zero."""
+    prob, parts = mixed
+    cp = scenes.compact_problem(prob)
+    t = problem_to_device(cp, cuda_device)
+    buf = ContactSolveBuffers(cp.num_envs, cp.dof_per_env, cp.max_contacts, cuda_device)
+    dc = torch.as_tensor(cp.dofs_active, dtype=torch.int32).to(cuda_device)
+    buf.v.fill_(float("nan"))
+    contact_solve(**t, buffers=buf, options=make_options("armijo_decay"), dof_count=dc,
+                  world_order=torch.as_tensor(scenes.work_order(cp), dtype=torch.int32).to(cuda_device))
+    torch.cuda.synchronize()
+    v, it = buf.v.cpu().numpy().reshape(cp.num_envs, -1), buf.newton_iterations.cpu().numpy()
+    assert buf.converged.all()
+    off = 0
+    for q in parts:
+        vq, itq, _ = solve(q, cuda_device)
+        E, n = q.num_envs, q.dof_per_env
+        err = np.abs(v[off:off + E, :n] - vq).max(1) / np.maximum(np.abs(vq).max(1), 1e-300)
+        assert err.max() <= 1e-9, (n, err.max())
+        assert np.all(v[off:off + E, n:] == 0.0)
+        assert np.abs(it[off:off + E] - itq).max() <= 1
+        off += E
