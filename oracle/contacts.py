@@ -73,6 +73,57 @@ def generate(shapes, body_q, gap=1.0e-3):
             face[k] = s * ha[k]
             emit(a, b, Xa[0] + qrot(Xa[1], face), vw, qrot(Xa[1], nl), ma, mb)
 
+    def box_edge(a, b, Xa, ha, Xb, hb, g, ma, mb):
+        """The edge-edge contact of two boxes: separating axes over the 6
+        face and 9 edge-pair axes; the best edge axis, if it beats every face
+        axis by a relative 1e-6 and lies within g, gives one contact at the
+        closest points of its two supporting edges when both lie inside the
+        edges (as sap_collide_box_box's edge case,
+        sim/collision/primitive.py:692-1148)."""
+        A = [qrot(Xa[1], e) for e in np.eye(3)]
+        B = [qrot(Xb[1], e) for e in np.eye(3)]
+        d = Xb[0] - Xa[0]
+
+        def radius(E, h, L):
+            return h[0] * abs(np.dot(E[0], L)) + h[1] * abs(np.dot(E[1], L)) + h[2] * abs(np.dot(E[2], L))
+
+        best_face = -1.0e300
+        for k in range(3):
+            sa = abs(np.dot(d, A[k])) - (ha[k] + radius(B, hb, A[k]))
+            sb = abs(np.dot(d, B[k])) - (radius(A, ha, B[k]) + hb[k])
+            best_face = max(best_face, max(sa, sb))
+        best_edge, bi, bj, bL = -1.0e300, -1, -1, None
+        for i in range(3):
+            for j in range(3):
+                L = np.cross(A[i], B[j])
+                ln = np.sqrt(np.dot(L, L))
+                if ln < 1.0e-6:
+                    continue
+                L = (1.0 / ln) * L
+                if np.dot(d, L) < 0.0:
+                    L = -L
+                sep = np.dot(d, L) - radius(A, ha, L) - radius(B, hb, L)
+                if sep > best_edge:
+                    best_edge, bi, bj, bL = sep, i, j, L
+        scale = max(max(ha), max(hb))
+        if bi < 0 or not best_edge > best_face + 1.0e-6 * scale or not best_edge < g:
+            return
+        cA, cB = Xa[0].copy(), Xb[0].copy()
+        for m in range(3):
+            if m != bi:
+                cA = cA + (ha[m] if np.dot(A[m], bL) >= 0.0 else -ha[m]) * A[m]
+            if m != bj:
+                cB = cB - (hb[m] if np.dot(B[m], bL) >= 0.0 else -hb[m]) * B[m]
+        u, v, w = A[bi], B[bj], cA - cB
+        uv, uw, vw = np.dot(u, v), np.dot(u, w), np.dot(v, w)
+        den = 1.0 - uv * uv
+        if den < 1.0e-12:
+            return
+        s_, t_ = (uv * vw - uw) / den, (vw - uv * uw) / den
+        if abs(s_) > ha[bi] or abs(t_) > hb[bj]:
+            return
+        emit(a, b, cA + s_ * u, cB + t_ * v, bL, ma, mb)
+
     groups = getattr(shapes, "shape_collision_group", None)
 
     def groups_meet(ga, gb):  # sim/collision/broad_phase_common.py:133-150
@@ -94,6 +145,14 @@ def generate(shapes, body_q, gap=1.0e-3):
         s1, s2 = shapes.shape_scale[a], shapes.shape_scale[b]
         if t1 == PLANE and t2 == PLANE:
             return
+        if t1 != PLANE:
+            # the kernel's conservative bounding-sphere cut
+            ra = s1[0] if t1 == SPHERE else np.sqrt(np.dot(s1, s1))
+            rb = s2[0] if t2 == SPHERE else np.sqrt(np.dot(s2, s2))
+            dd = Xb[0] - Xa[0]
+            reach = (ra + rb + 1.7320508075688772 * (abs(m1) + abs(m2) + abs(gap))) * (1.0 + 1.0e-12) + 1.0e-12
+            if np.dot(dd, dd) > reach * reach:
+                return
         if t1 == PLANE:
             n = qrot(Xa[1], np.array([0.0, 0.0, 1.0]))
             if t2 == SPHERE:
@@ -151,6 +210,7 @@ def generate(shapes, body_q, gap=1.0e-3):
         if t1 == BOX and t2 == BOX:
             box_vs_box(a, b, Xa, s1, Xb, s2, gap + m1 + m2, m1, m2)
             box_vs_box(b, a, Xb, s2, Xa, s1, gap + m1 + m2, m2, m1)
+            box_edge(a, b, Xa, s1, Xb, s2, gap + m1 + m2, m1, m2)
 
     for w in range(E):
         base, gbase = w * Sw, E * Sw

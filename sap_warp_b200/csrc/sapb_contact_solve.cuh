@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 
 #include "sapb_device.cuh"
 #include "sapb_internal.h"
@@ -107,7 +108,7 @@ struct World {
   __device__ __forceinline__ int ldH() const { return NS > 0 ? ((NS % 2 == 0) ? NS + 1 : NS) : L.ldH; }
   __device__ __forceinline__ int nb() const { return NS > 0 ? (NS + 3) / 4 : (n + 3) / 4; }
   // shift of the kernel's triangle list (built for L.n DOFs) to this world's n
-  __device__ __forceinline__ int tri_shift() const { return NS > 0 ? 0 : L.n - n; }
+  __device__ __forceinline__ int tri_shift() const { return L.n - dofs(); }
   __device__ double* V(int k) const { return vec + (size_t)k * ldJ(); }
   __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
   __device__ double* part(int which, int warp) const {
@@ -467,6 +468,442 @@ __device__ void line_coefficients(const World<NT, HT, NS>& w, double c4[4]) {
   c4[3] = r[3];
 }
 
+template <int NS> struct LdltBlocks { static constexpr int kCount = 1; static constexpr int kW[1] = {4}; };
+template <> struct LdltBlocks<35> { static constexpr int kCount = 2; static constexpr int kW[2] = {5, 4}; };
+template <> struct LdltBlocks<18> { static constexpr int kCount = 2; static constexpr int kW[2] = {6, 4}; };
+template <> struct LdltBlocks<13> { static constexpr int kCount = 2; static constexpr int kW[2] = {4, 5}; };
+template <> struct LdltBlocks<6> { static constexpr int kCount = 1; static constexpr int kW[1] = {6}; };
+
+// One world of the persistent solve: stage its J and constants, the
+// candidate starts, the Newton loop, the outputs.  NS: the world's DOF count
+// at compile time (0: n_rt at run time); the shared-memory layout L may be
+// sized for more DOFs (n_max) than the world has.
+template <int NT, typename HT, int NS, int LSV, int LB>
+__device__ __forceinline__ void solve_world(const SolveParams& P, const Layout& L, unsigned char* smem, double* red,
+                                            unsigned long long& s_partmask, int& s_factor_ok, const int e,
+                                            const int n_max, const int n_rt, const bool use_guess) {
+  const int tid = threadIdx.x;
+  const int C = P.p.max_contacts;
+  const int n = NS > 0 ? NS : n_rt;
+  World<NT, HT, NS> w{L,
+                  P.p.dynamics_matrix + (size_t)e * n_max * n_max,
+                  reinterpret_cast<double*>(smem + L.off_J),
+                  reinterpret_cast<HT*>(smem + L.off_scr),
+                  reinterpret_cast<HT*>(smem + L.off_H),
+                  reinterpret_cast<HT*>(smem + L.off_G),
+                  reinterpret_cast<double*>(smem + L.off_vec),
+                  reinterpret_cast<double*>(smem + L.off_con),
+                  reinterpret_cast<int*>(smem + L.off_flags),
+                  reinterpret_cast<const uint16_t*>(smem + L.off_tri),
+                  red,
+                  &s_factor_ok,
+                  n,
+                  0};
+  int count = P.p.contact_count[e];
+  if (count > C) count = C;
+  if (count < 0) count = 0;
+  w.count = count;
+  const double dt = P.p.dt[e];
+  const size_t base = (size_t)e * n_max;
+
+  // ---- stage J, per-contact constants and vectors -------------------------
+  {
+    const int rows = 3 * count;
+    const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n_max;
+    const int ldj = w.ldJ();
+    // Flat copy of the contiguous rows*n block by asynchronous 8-byte
+    // copies (all in flight at once, completed before the barrier after the
+    // per-DOF setup below; the rows land at stride ldj).
+    const int total = rows * n;
+    for (int k = tid; k < total; k += NT) {
+      const int r = k / n, j = k - r * n;
+      const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(w.J + (size_t)r * ldj + j));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(Jg + k) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    // zero padding columns n..ldj-1
+    for (int k = tid; k < rows * (ldj - n); k += NT) {
+      const int r = k / (ldj - n), j = n + (k - r * (ldj - n));
+      w.J[(size_t)r * ldj + j] = 0.0;
+    }
+    for (int c = tid; c < count; c += NT) {
+      const size_t ci = (size_t)e * C + c;
+      const double tau = P.p.tau_d ? P.p.tau_d[ci] : P.o.contact_tau_d;
+      const ContactConst cc = make_contact_const(P.p.phi0[ci], P.p.w_eff[ci], P.p.mu[ci], P.p.stiffness[ci], tau,
+                                                 P.o.contact_beta, P.o.contact_sigma, dt);
+      w.Cn(C_RT)[c] = cc.rt;
+      w.Cn(C_RN)[c] = cc.rn;
+      w.Cn(C_RTINV)[c] = cc.rt_inv;
+      w.Cn(C_RNINV)[c] = cc.rn_inv;
+      w.Cn(C_VHAT)[c] = cc.vhat_n;
+      w.Cn(C_MU)[c] = cc.mu;
+      w.Cn(C_MUHAT)[c] = cc.mu_hat;
+      w.Cn(C_FACTOR)[c] = cc.factor;
+    }
+    for (int i = tid; i < w.ldJ(); i += NT) {
+      if (i < n) {
+        w.V(V_VSTAR)[i] = P.p.v_star[base + i];
+        double v = P.p.v0[base + i];
+        if (P.p.v_guess) {
+          if (use_guess) v = P.p.v_guess[base + i];
+          P.p.v_guess[base + i] = v;
+        }
+        w.V(V_V)[i] = v;
+        double d = __ldg(w.A + (size_t)i * n + i);
+        if (d < 1.0e-12 || !isfinite(d)) d = 1.0e-12;
+        w.V(V_AINV)[i] = 1.0 / d;
+        w.V(V_DSCALE)[i] = 1.0 / sqrt(d);
+      } else {
+        for (int k = 0; k < Layout::kVecs; ++k) w.V(k)[i] = 0.0;
+      }
+    }
+  }
+  // ---- PD and limit terms (sim/contact_solve.py:490-683) ------------------
+  for (int i = tid; i < n; i += NT) {
+    int fl = 0;
+    const size_t dof = base + i;
+    const sapb_dof_terms& D = P.dof;
+    if (D.has_pd) {
+      int coord = D.dof_coord_index[dof];
+      if (coord >= D.joint_coord_count) coord = -1;
+      int target = D.dof_target_index[dof];
+      if (target < 0 || target >= P.p.num_envs * n_max) target = (int)dof;
+      if (D.joint_target_mode[target] != 0) {
+        const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
+        if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {
+          double kpe, kde;
+          effective_pd_gains(kp, kd, dt, w.V(V_AINV)[i], &kpe, &kde);
+          const double gain = dt * kpe + kde;
+          if (gain > 0.0) {
+            double q0 = 0.0, qd = 0.0;
+            if (coord >= 0) {
+              q0 = D.joint_q[coord];
+              qd = D.joint_target_pos ? (double)D.joint_target_pos[target] : 0.0;
+            }
+            const double vd = D.joint_target_vel ? (double)D.joint_target_vel[target] : 0.0;
+            const double u0 = D.joint_act ? (double)D.joint_act[target] : 0.0;
+            fl |= kFlagPd;
+            w.V(V_PDA)[i] = kpe * (qd - q0) + kde * vd + u0;
+            w.V(V_PDGAIN)[i] = gain;
+            w.V(V_PDLIM)[i] = (double)D.joint_effort_limit[target];
+          }
+        }
+      }
+    }
+    w.V(V_LOR)[i] = 1.0;
+    w.V(V_UPR)[i] = 1.0;
+    if (D.has_limits) {
+      int coord = D.dof_coord_index[dof];
+      if (coord >= D.joint_coord_count) coord = -1;
+      const double ke = coord >= 0 ? D.joint_limit_ke[dof] : 0.0;
+      if (coord >= 0 && D.limit_supported[dof] != 0 && ke > 0.0) {
+        const double q0 = D.joint_q[coord];
+        const double lower = D.joint_limit_lower[dof], upper = D.joint_limit_upper[dof];
+        const double speed = fmax(fabs(P.p.v0[base + i]), fabs(w.V(V_VSTAR)[i]));
+        const double window = kLimitWindow * dt * speed;
+        const double kd = D.joint_limit_kd[dof];
+        const double tau_d = kd > 0.0 ? kd / ke : 0.0;
+        const double bf = kLimitBeta * kLimitBeta / (4.0 * kPi * kPi);
+        const double r_nr = bf * fmax(w.V(V_AINV)[i], 1.0e-12);
+        const double r_soft = 1.0 / (dt * ke * (dt + tau_d));
+        const double rr = fmax(r_nr, r_soft);
+        if (isfinite(lower) && q0 - lower <= window) {
+          fl |= kFlagLo;
+          w.V(V_LOVHAT)[i] = -(q0 - lower) / (dt + tau_d);
+          w.V(V_LOR)[i] = rr;
+          w.V(V_LORINV)[i] = 1.0 / rr;
+        }
+        if (isfinite(upper) && upper - q0 <= window) {
+          fl |= kFlagUp;
+          w.V(V_UPVHAT)[i] = -(upper - q0) / (dt + tau_d);
+          w.V(V_UPR)[i] = rr;
+          w.V(V_UPRINV)[i] = 1.0 / rr;
+        }
+      }
+    }
+    w.flags[i] = fl;
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's J copies
+  __syncthreads();
+  // ---- participating DOFs (sim/contact_solve.py:423-488) ------------------
+  // A DOF takes part if a model term acts on it or a contact's body DOF
+  // range or J column covers it.  The contacts mark their DOFs in a 64-bit
+  // mask in parallel (n <= 60 here).
+  if (tid == 0) s_partmask = 0ull;
+  __syncthreads();
+  for (int c = tid; c < count; c += NT) {
+    const size_t ci = (size_t)e * C + c;
+    unsigned long long mk = 0ull;
+    if (P.p.body_dof_start) {
+      const int bs[2] = {P.p.body0 ? P.p.body0[ci] : -1, P.p.body1 ? P.p.body1[ci] : -1};
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int b = bs[q];
+        if (b < 0 || b >= P.p.num_bodies) continue;
+        const int s = P.p.body_dof_start[b], m = P.p.body_dof_count[b];
+        if (s < 0 || m <= 0 || s >= n) continue;
+        const int hi = s + m < n ? s + m : n;
+        mk |= ((1ull << (hi - s)) - 1ull) << s;
+      }
+    }
+    const double* Jc = w.J + (size_t)(3 * c) * w.ldJ();
+    if (mk != (1ull << n) - 1ull)
+      for (int j = 0; j < n; ++j)
+        if (Jc[j] != 0.0 || Jc[w.ldJ() + j] != 0.0 || Jc[2 * w.ldJ() + j] != 0.0) mk |= 1ull << j;
+    atomicOr(&s_partmask, mk);
+  }
+  __syncthreads();
+  int any_model_term = 0;
+  for (int i = tid; i < n; i += NT) {
+    const int model = (w.flags[i] & (kFlagPd | kFlagLo | kFlagUp)) ? 1 : 0;
+    any_model_term |= model;
+    if (model || ((s_partmask >> i) & 1ull)) w.flags[i] |= kFlagPart;
+  }
+  const int model_terms = __syncthreads_or(any_model_term);
+  const bool unconstrained = (count == 0) && !model_terms;
+  // ---- input check: a NaN / Inf in A, J, the contact parameters, v* or
+  // the start velocity leaves the world unsolved (SAPB_WORLD_NOT_FINITE)
+  int bad = 0;
+  for (int k = tid; k < n * n; k += NT)
+    if (!isfinite(__ldg(w.A + k))) bad = 1;
+  {
+    const int ldj = w.ldJ(), tot = 3 * count * n;
+    for (int k = tid; k < tot; k += NT) {
+      const int r = k / n, j = k - r * n;
+      if (!isfinite(w.J[(size_t)r * ldj + j])) bad = 1;
+    }
+  }
+  for (int c = tid; c < count; c += NT) {
+    const size_t ci = (size_t)e * C + c;
+    if (!isfinite(P.p.phi0[ci]) || !isfinite(P.p.w_eff[ci]) || !isfinite(P.p.mu[ci]) ||
+        !isfinite(P.p.stiffness[ci]) || (P.p.tau_d && !isfinite(P.p.tau_d[ci])))
+      bad = 1;
+  }
+  for (int i = tid; i < n; i += NT)
+    if (!isfinite(w.V(V_VSTAR)[i]) || !isfinite(w.V(V_V)[i])) bad = 1;
+  const bool not_finite = __syncthreads_or(bad) != 0;
+
+  int newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
+  double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
+  int ws_accepted = 0;
+  bool evaluated = false;
+  if (not_finite) {
+    status = SAPB_WORLD_NOT_FINITE;  // v stays the start velocity
+  } else if (unconstrained) {
+    converged = 1;
+    for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
+    __syncthreads();
+  } else {
+    for (int i = tid; i < n; i += NT)
+      if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
+    __syncthreads();
+    // Candidate starts (no counterpart in the reference): v_candidate_count
+    // start velocities, then gamma0_count impulse sets with v_c = base +
+    // A^-1 J^T gamma_c (base v* or gamma0_base), each taken on the
+    // participating DOFs (v* on the others), A factored once in this
+    // kernel's factor precision or read from the free motion's factor;
+    // the start with the lowest cost among the plain start and the
+    // candidates is taken.  Its evaluation seeds iteration 0 when it was
+    // the last one evaluated.
+    bool have_e4 = false;
+    double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
+    const int KV = P.p.v_candidates ? (P.p.v_candidate_count > 1 ? P.p.v_candidate_count : 1) : 0;
+    const int KG = P.p.gamma0 ? (P.p.gamma0_count > 1 ? P.p.gamma0_count : 1) : 0;
+    if ((KV > 0 || KG > 0) && count > 0) {
+      double e4p[4];
+      evaluate<NT, HT, NS>(w, P, dt, e4p);
+      double best_cost = e4p[0];
+      for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
+      bool last_is_best = false;
+      auto try_start = [&](int index) {  // V(V_V) holds the candidate
+        __syncthreads();
+        double e4c[4];
+        evaluate<NT, HT, NS>(w, P, dt, e4c);
+        last_is_best = false;
+        if (e4c[0] < best_cost) {
+          best_cost = e4c[0];
+          ws_accepted = index;
+          last_is_best = true;
+          for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
+          for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
+        }
+      };
+      for (int k = 0; k < KV; ++k) {
+        const double* vk = P.p.v_candidates + ((size_t)k * P.p.num_envs + e) * n_max;
+        for (int i = tid; i < n; i += NT)
+          w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? __ldg(vk + i) : w.V(V_VSTAR)[i];
+        try_start(k + 1);
+      }
+      if (KG > 0) {
+        const double* base_g = P.p.gamma0_base ? P.p.gamma0_base + (size_t)e * n_max : nullptr;
+        // a world whose candidate impulses are all zero starts at the base
+        int nz = 0;
+        for (int q = tid; q < KG * 3 * count; q += NT) {
+          const int kk = q / (3 * count), r = q - kk * 3 * count;
+          if (__ldg(P.p.gamma0 + ((size_t)kk * P.p.num_envs + e) * C * 3 + r) != 0.0) nz = 1;
+        }
+        if (!__syncthreads_or(nz)) {
+          for (int i = tid; i < n; i += NT)
+            w.V(V_V)[i] = (w.flags[i] & kFlagPart) && base_g ? __ldg(base_g + i) : w.V(V_VSTAR)[i];
+          try_start(KV + 1);
+        } else {
+          const int ldj = w.ldJ();
+          if (P.p.dynamics_factor) {
+            // the free motion's LDL^T of A
+            const double* Lg = P.p.dynamics_factor + (size_t)e * n_max * n_max;
+            load_lower<NT, HT, NS>(w, Lg, nullptr, 0.0);
+            HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
+            for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
+            __syncthreads();
+          } else {
+            load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
+            __syncthreads();
+            ldlt_blocked<NT, HT, LB>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri,
+                                     w.tri_shift());  // the factor of A
+          }
+          // Two sets at a time: stage their impulses in the (here unused)
+          // scratch, form J^T gamma for both (threads 0-63 set k0, 64-127
+          // set k0+1), solve both with the factor on warps 0 and 1, then
+          // evaluate the candidates in order.
+          double* gs = reinterpret_cast<double*>(w.GJ);
+          for (int k0 = 0; k0 < KG; k0 += 2) {
+            const int nk = KG - k0 < 2 ? KG - k0 : 2;
+            for (int q = tid; q < nk * 3 * count; q += NT) {
+              const int kk = q / (3 * count), r = q - kk * 3 * count;
+              gs[q] = __ldg(P.p.gamma0 + ((size_t)(k0 + kk) * P.p.num_envs + e) * C * 3 + r);
+            }
+            __syncthreads();
+            {
+              const int kk = tid >> 6, i = tid & 63;
+              if (kk < nk && i < n) {
+                const double* g = gs + kk * 3 * count;
+                double acc = 0.0;
+                for (int c = 0; c < count; ++c) {
+                  const double* Jc = w.J + (size_t)(3 * c) * ldj;
+                  acc += Jc[i] * g[3 * c] + Jc[ldj + i] * g[3 * c + 1] + Jc[2 * ldj + i] * g[3 * c + 2];
+                }
+                w.V(kk == 0 ? V_GRAD : V_DP)[i] = -acc;  // the solves give -H^-1 rhs
+              }
+            }
+            __syncthreads();
+            solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
+            if (nk > 1) solve_warp<NT, HT, NS>(w, V_DP, V_DV2, 1);
+            __syncthreads();
+            for (int kk = 0; kk < nk; ++kk) {
+              const double* dvk = w.V(kk == 0 ? V_DV : V_DV2);
+              for (int i = tid; i < n; i += NT)
+                w.V(V_V)[i] = (w.flags[i] & kFlagPart)
+                                  ? (base_g ? __ldg(base_g + i) : w.V(V_VSTAR)[i]) + dvk[i]
+                                  : w.V(V_VSTAR)[i];
+              try_start(KV + k0 + kk + 1);
+            }
+          }
+        }
+      }
+      if (last_is_best) {
+        have_e4 = true;
+      } else {
+        const int src = ws_accepted > 0 ? V_BEST : V_SAVE;
+        for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(src)[i];
+      }
+      __syncthreads();
+    }
+    const double cost_min_alpha = LSV == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
+    int it = 0;
+    bool active = true;
+    for (;;) {
+      double e4[4];
+      if (have_e4) {
+        for (int k = 0; k < 4; ++k) e4[k] = e4_seed[k];
+        have_e4 = false;
+      } else {
+        evaluate<NT, HT, NS>(w, P, dt, e4);
+      }
+      evaluated = true;
+      cost = e4[0];
+      // convergence test (sim/contact_solve.py:2043-2087)
+      const double gn = sqrt(fmax(e4[1], 0.0)), pn = sqrt(fmax(e4[2], 0.0)), jn = sqrt(fmax(e4[3], 0.0));
+      grad_norm = gn;
+      const double opt_tol = P.o.optimality_abs_tol + P.o.optimality_rel_tol * fmax(pn, jn);
+      const bool opt = gn <= opt_tol;
+      bool cost_ok = false;
+      if (it > 0 && alpha > cost_min_alpha) {
+        const double sc = 0.5 * (fabs(cost) + fabs(previous_cost));
+        const double tol = P.o.cost_abs_tol + P.o.cost_rel_tol * sc;
+        if (fabs(cost - previous_cost) < tol) cost_ok = true;
+      }
+      newton_iterations = it;
+      if (opt || cost_ok) {
+        converged = 1;
+        active = false;
+      } else if (it >= P.o.max_iterations) {
+        active = false;
+      } else {
+        converged = 0;
+      }
+      if (!active) break;
+      // Newton direction
+      assemble_hessian<NT, HT, NS>(w, P.o.diag_shift);
+      factor_and_solve<NT, HT, NS, LB>(w);
+      if (!*w.factor_ok) {  // H not SPD (uniform: published by the barrier above)
+        status = SAPB_WORLD_NOT_SPD;
+        converged = 0;
+        break;
+      }
+      LsResult r;
+      double c4[4];
+      line_coefficients<NT, HT, NS>(w, c4);
+      if constexpr (LSV == SAPB_LS_ARMIJO_DECAY)
+        r = ls_armijo<NT, 1>(w, P, dt, cost, c4);
+      else if constexpr (LSV == SAPB_LS_EXACT_ROOT)
+        r = ls_exact<NT>(w, P, dt, cost, c4);
+      else
+        r = ls_monotone<NT, 1>(w, P, dt, cost, c4);
+      alpha = r.alpha;
+      status = r.status;
+      constexpr bool mono = LSV == SAPB_LS_MONOTONE_DECAY;
+      if (r.accepted || mono) ls_total += r.iterations;
+      if (r.accepted) {
+        previous_cost = cost;
+        for (int i = tid; i < n; i += NT) w.V(V_V)[i] += r.alpha * w.V(V_DV)[i];
+      } else if (mono) {
+        previous_cost = cost;
+      }
+      __syncthreads();
+      ++it;
+    }
+  }
+  // ---- outputs ------------------------------------------------------------
+  for (int i = tid; i < n_max; i += NT) P.out.v[base + i] = i < n ? w.V(V_V)[i] : 0.0;
+  for (int c = tid; c < C; c += NT) {
+    const size_t ci = (size_t)e * C + c;
+    const bool live = evaluated && c < count;
+    if (P.out.contact_gamma) {
+      P.out.contact_gamma[ci * 3 + 0] = live ? w.Cn(C_GAMMA + 0)[c] : 0.0;
+      P.out.contact_gamma[ci * 3 + 1] = live ? w.Cn(C_GAMMA + 1)[c] : 0.0;
+      P.out.contact_gamma[ci * 3 + 2] = live ? w.Cn(C_GAMMA + 2)[c] : 0.0;
+    }
+    if (P.out.contact_mode) {
+      int mode = SAPB_CONTACT_MODE_NONE;
+      if (live) {
+        double g[3], cst;
+        mode = project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cst, nullptr);
+      }
+      P.out.contact_mode[ci] = mode;
+    }
+  }
+  if (tid == 0) {
+    if (P.out.cost) P.out.cost[e] = evaluated ? cost : 0.0;
+    if (P.out.newton_iterations) P.out.newton_iterations[e] = newton_iterations;
+    if (P.out.line_search_iterations) P.out.line_search_iterations[e] = ls_total;
+    if (P.out.converged) P.out.converged[e] = converged;
+    if (P.out.status) P.out.status[e] = status;
+    if (P.out.grad_norm) P.out.grad_norm[e] = grad_norm;
+    if (P.out.warm_start_accepted) P.out.warm_start_accepted[e] = ws_accepted;
+  }
+  __syncthreads();
+}
+
 // LSV: the line search, fixed at compile time (SAPB_LS_ARMIJO_DECAY,
 // SAPB_LS_EXACT_ROOT or SAPB_LS_MONOTONE_DECAY) so that one instantiation
 // holds the code of one search only (smaller instruction footprint).  LB:
@@ -547,424 +984,32 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
       n_world = P.p.dof_count[e];
       n_world = n_world < 1 ? 1 : (n_world > n_max ? n_max : n_world);
     }
-    const int n = n_world;
-    World<NT, HT, NS> w{L,
-                    P.p.dynamics_matrix + (size_t)e * n_max * n_max,
-                    reinterpret_cast<double*>(smem + L.off_J),
-                    reinterpret_cast<HT*>(smem + L.off_scr),
-                    reinterpret_cast<HT*>(smem + L.off_H),
-                    reinterpret_cast<HT*>(smem + L.off_G),
-                    reinterpret_cast<double*>(smem + L.off_vec),
-                    reinterpret_cast<double*>(smem + L.off_con),
-                    reinterpret_cast<int*>(smem + L.off_flags),
-                    reinterpret_cast<const uint16_t*>(smem + L.off_tri),
-                    red,
-                    &s_factor_ok,
-                    n,
-                    0};
-    int count = P.p.contact_count[e];
-    if (count > C) count = C;
-    if (count < 0) count = 0;
-    w.count = count;
-    const double dt = P.p.dt[e];
-    const size_t base = (size_t)e * n_max;
-
-    // ---- stage J, per-contact constants and vectors -------------------------
-    {
-      const int rows = 3 * count;
-      const double* Jg = P.p.jacobian + (size_t)e * C * 3 * n_max;
-      const int ldj = w.ldJ();
-      // Flat copy of the contiguous rows*n block by asynchronous 8-byte
-      // copies (all in flight at once, completed before the barrier after the
-      // per-DOF setup below; the rows land at stride ldj).
-      const int total = rows * n;
-      for (int k = tid; k < total; k += NT) {
-        const int r = k / n, j = k - r * n;
-        const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(w.J + (size_t)r * ldj + j));
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(Jg + k) : "memory");
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      // zero padding columns n..ldj-1
-      for (int k = tid; k < rows * (ldj - n); k += NT) {
-        const int r = k / (ldj - n), j = n + (k - r * (ldj - n));
-        w.J[(size_t)r * ldj + j] = 0.0;
-      }
-      for (int c = tid; c < count; c += NT) {
-        const size_t ci = (size_t)e * C + c;
-        const double tau = P.p.tau_d ? P.p.tau_d[ci] : P.o.contact_tau_d;
-        const ContactConst cc = make_contact_const(P.p.phi0[ci], P.p.w_eff[ci], P.p.mu[ci], P.p.stiffness[ci], tau,
-                                                   P.o.contact_beta, P.o.contact_sigma, dt);
-        w.Cn(C_RT)[c] = cc.rt;
-        w.Cn(C_RN)[c] = cc.rn;
-        w.Cn(C_RTINV)[c] = cc.rt_inv;
-        w.Cn(C_RNINV)[c] = cc.rn_inv;
-        w.Cn(C_VHAT)[c] = cc.vhat_n;
-        w.Cn(C_MU)[c] = cc.mu;
-        w.Cn(C_MUHAT)[c] = cc.mu_hat;
-        w.Cn(C_FACTOR)[c] = cc.factor;
-      }
-      for (int i = tid; i < L.ldJ; i += NT) {
-        if (i < n) {
-          w.V(V_VSTAR)[i] = P.p.v_star[base + i];
-          double v = P.p.v0[base + i];
-          if (P.p.v_guess) {
-            if (use_guess) v = P.p.v_guess[base + i];
-            P.p.v_guess[base + i] = v;
-          }
-          w.V(V_V)[i] = v;
-          double d = __ldg(w.A + (size_t)i * n + i);
-          if (d < 1.0e-12 || !isfinite(d)) d = 1.0e-12;
-          w.V(V_AINV)[i] = 1.0 / d;
-          w.V(V_DSCALE)[i] = 1.0 / sqrt(d);
-        } else {
-          for (int k = 0; k < Layout::kVecs; ++k) w.V(k)[i] = 0.0;
+    if constexpr (NS == 0) {
+      if (P.p.dof_count) {
+        // each world's own DOF count: the specialised code of its size class
+        switch (n_world) {
+          case 35:
+            solve_world<NT, HT, 35, LSV, LdltBlocks<35>::kW[0]>(P, L, smem, red, s_partmask, s_factor_ok, e,
+                                                                 n_max, 35, use_guess);
+            continue;
+          case 18:
+            solve_world<NT, HT, 18, LSV, LdltBlocks<18>::kW[0]>(P, L, smem, red, s_partmask, s_factor_ok, e,
+                                                                 n_max, 18, use_guess);
+            continue;
+          case 13:
+            solve_world<NT, HT, 13, LSV, LdltBlocks<13>::kW[0]>(P, L, smem, red, s_partmask, s_factor_ok, e,
+                                                                 n_max, 13, use_guess);
+            continue;
+          case 6:
+            solve_world<NT, HT, 6, LSV, LdltBlocks<6>::kW[0]>(P, L, smem, red, s_partmask, s_factor_ok, e,
+                                                                 n_max, 6, use_guess);
+            continue;
+          default:
+            break;
         }
       }
     }
-    // ---- PD and limit terms (sim/contact_solve.py:490-683) ------------------
-    for (int i = tid; i < n; i += NT) {
-      int fl = 0;
-      const size_t dof = base + i;
-      const sapb_dof_terms& D = P.dof;
-      if (D.has_pd) {
-        int coord = D.dof_coord_index[dof];
-        if (coord >= D.joint_coord_count) coord = -1;
-        int target = D.dof_target_index[dof];
-        if (target < 0 || target >= P.p.num_envs * n_max) target = (int)dof;
-        if (D.joint_target_mode[target] != 0) {
-          const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
-          if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {
-            double kpe, kde;
-            effective_pd_gains(kp, kd, dt, w.V(V_AINV)[i], &kpe, &kde);
-            const double gain = dt * kpe + kde;
-            if (gain > 0.0) {
-              double q0 = 0.0, qd = 0.0;
-              if (coord >= 0) {
-                q0 = D.joint_q[coord];
-                qd = D.joint_target_pos ? (double)D.joint_target_pos[target] : 0.0;
-              }
-              const double vd = D.joint_target_vel ? (double)D.joint_target_vel[target] : 0.0;
-              const double u0 = D.joint_act ? (double)D.joint_act[target] : 0.0;
-              fl |= kFlagPd;
-              w.V(V_PDA)[i] = kpe * (qd - q0) + kde * vd + u0;
-              w.V(V_PDGAIN)[i] = gain;
-              w.V(V_PDLIM)[i] = (double)D.joint_effort_limit[target];
-            }
-          }
-        }
-      }
-      w.V(V_LOR)[i] = 1.0;
-      w.V(V_UPR)[i] = 1.0;
-      if (D.has_limits) {
-        int coord = D.dof_coord_index[dof];
-        if (coord >= D.joint_coord_count) coord = -1;
-        const double ke = coord >= 0 ? D.joint_limit_ke[dof] : 0.0;
-        if (coord >= 0 && D.limit_supported[dof] != 0 && ke > 0.0) {
-          const double q0 = D.joint_q[coord];
-          const double lower = D.joint_limit_lower[dof], upper = D.joint_limit_upper[dof];
-          const double speed = fmax(fabs(P.p.v0[base + i]), fabs(w.V(V_VSTAR)[i]));
-          const double window = kLimitWindow * dt * speed;
-          const double kd = D.joint_limit_kd[dof];
-          const double tau_d = kd > 0.0 ? kd / ke : 0.0;
-          const double bf = kLimitBeta * kLimitBeta / (4.0 * kPi * kPi);
-          const double r_nr = bf * fmax(w.V(V_AINV)[i], 1.0e-12);
-          const double r_soft = 1.0 / (dt * ke * (dt + tau_d));
-          const double rr = fmax(r_nr, r_soft);
-          if (isfinite(lower) && q0 - lower <= window) {
-            fl |= kFlagLo;
-            w.V(V_LOVHAT)[i] = -(q0 - lower) / (dt + tau_d);
-            w.V(V_LOR)[i] = rr;
-            w.V(V_LORINV)[i] = 1.0 / rr;
-          }
-          if (isfinite(upper) && upper - q0 <= window) {
-            fl |= kFlagUp;
-            w.V(V_UPVHAT)[i] = -(upper - q0) / (dt + tau_d);
-            w.V(V_UPR)[i] = rr;
-            w.V(V_UPRINV)[i] = 1.0 / rr;
-          }
-        }
-      }
-      w.flags[i] = fl;
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's J copies
-    __syncthreads();
-    // ---- participating DOFs (sim/contact_solve.py:423-488) ------------------
-    // A DOF takes part if a model term acts on it or a contact's body DOF
-    // range or J column covers it.  The contacts mark their DOFs in a 64-bit
-    // mask in parallel (n <= 60 here).
-    if (tid == 0) s_partmask = 0ull;
-    __syncthreads();
-    for (int c = tid; c < count; c += NT) {
-      const size_t ci = (size_t)e * C + c;
-      unsigned long long mk = 0ull;
-      if (P.p.body_dof_start) {
-        const int bs[2] = {P.p.body0 ? P.p.body0[ci] : -1, P.p.body1 ? P.p.body1[ci] : -1};
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int b = bs[q];
-          if (b < 0 || b >= P.p.num_bodies) continue;
-          const int s = P.p.body_dof_start[b], m = P.p.body_dof_count[b];
-          if (s < 0 || m <= 0 || s >= n) continue;
-          const int hi = s + m < n ? s + m : n;
-          mk |= ((1ull << (hi - s)) - 1ull) << s;
-        }
-      }
-      const double* Jc = w.J + (size_t)(3 * c) * L.ldJ;
-      if (mk != (1ull << n) - 1ull)
-        for (int j = 0; j < n; ++j)
-          if (Jc[j] != 0.0 || Jc[L.ldJ + j] != 0.0 || Jc[2 * L.ldJ + j] != 0.0) mk |= 1ull << j;
-      atomicOr(&s_partmask, mk);
-    }
-    __syncthreads();
-    int any_model_term = 0;
-    for (int i = tid; i < n; i += NT) {
-      const int model = (w.flags[i] & (kFlagPd | kFlagLo | kFlagUp)) ? 1 : 0;
-      any_model_term |= model;
-      if (model || ((s_partmask >> i) & 1ull)) w.flags[i] |= kFlagPart;
-    }
-    const int model_terms = __syncthreads_or(any_model_term);
-    const bool unconstrained = (count == 0) && !model_terms;
-    // ---- input check: a NaN / Inf in A, J, the contact parameters, v* or
-    // the start velocity leaves the world unsolved (SAPB_WORLD_NOT_FINITE)
-    int bad = 0;
-    for (int k = tid; k < n * n; k += NT)
-      if (!isfinite(__ldg(w.A + k))) bad = 1;
-    {
-      const int ldj = w.ldJ(), tot = 3 * count * n;
-      for (int k = tid; k < tot; k += NT) {
-        const int r = k / n, j = k - r * n;
-        if (!isfinite(w.J[(size_t)r * ldj + j])) bad = 1;
-      }
-    }
-    for (int c = tid; c < count; c += NT) {
-      const size_t ci = (size_t)e * C + c;
-      if (!isfinite(P.p.phi0[ci]) || !isfinite(P.p.w_eff[ci]) || !isfinite(P.p.mu[ci]) ||
-          !isfinite(P.p.stiffness[ci]) || (P.p.tau_d && !isfinite(P.p.tau_d[ci])))
-        bad = 1;
-    }
-    for (int i = tid; i < n; i += NT)
-      if (!isfinite(w.V(V_VSTAR)[i]) || !isfinite(w.V(V_V)[i])) bad = 1;
-    const bool not_finite = __syncthreads_or(bad) != 0;
-
-    int newton_iterations = 0, ls_total = 0, converged = 0, status = 0;
-    double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
-    int ws_accepted = 0;
-    bool evaluated = false;
-    if (not_finite) {
-      status = SAPB_WORLD_NOT_FINITE;  // v stays the start velocity
-    } else if (unconstrained) {
-      converged = 1;
-      for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
-      __syncthreads();
-    } else {
-      for (int i = tid; i < n; i += NT)
-        if (!(w.flags[i] & kFlagPart)) w.V(V_V)[i] = w.V(V_VSTAR)[i];
-      __syncthreads();
-      // Candidate starts (no counterpart in the reference): v_candidate_count
-      // start velocities, then gamma0_count impulse sets with v_c = base +
-      // A^-1 J^T gamma_c (base v* or gamma0_base), each taken on the
-      // participating DOFs (v* on the others), A factored once in this
-      // kernel's factor precision or read from the free motion's factor;
-      // the start with the lowest cost among the plain start and the
-      // candidates is taken.  Its evaluation seeds iteration 0 when it was
-      // the last one evaluated.
-      bool have_e4 = false;
-      double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
-      const int KV = P.p.v_candidates ? (P.p.v_candidate_count > 1 ? P.p.v_candidate_count : 1) : 0;
-      const int KG = P.p.gamma0 ? (P.p.gamma0_count > 1 ? P.p.gamma0_count : 1) : 0;
-      if ((KV > 0 || KG > 0) && count > 0) {
-        double e4p[4];
-        evaluate<NT, HT, NS>(w, P, dt, e4p);
-        double best_cost = e4p[0];
-        for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
-        bool last_is_best = false;
-        auto try_start = [&](int index) {  // V(V_V) holds the candidate
-          __syncthreads();
-          double e4c[4];
-          evaluate<NT, HT, NS>(w, P, dt, e4c);
-          last_is_best = false;
-          if (e4c[0] < best_cost) {
-            best_cost = e4c[0];
-            ws_accepted = index;
-            last_is_best = true;
-            for (int q = 0; q < 4; ++q) e4_seed[q] = e4c[q];
-            for (int i = tid; i < n; i += NT) w.V(V_BEST)[i] = w.V(V_V)[i];
-          }
-        };
-        for (int k = 0; k < KV; ++k) {
-          const double* vk = P.p.v_candidates + ((size_t)k * P.p.num_envs + e) * n_max;
-          for (int i = tid; i < n; i += NT)
-            w.V(V_V)[i] = (w.flags[i] & kFlagPart) ? __ldg(vk + i) : w.V(V_VSTAR)[i];
-          try_start(k + 1);
-        }
-        if (KG > 0) {
-          const double* base_g = P.p.gamma0_base ? P.p.gamma0_base + (size_t)e * n_max : nullptr;
-          // a world whose candidate impulses are all zero starts at the base
-          int nz = 0;
-          for (int q = tid; q < KG * 3 * count; q += NT) {
-            const int kk = q / (3 * count), r = q - kk * 3 * count;
-            if (__ldg(P.p.gamma0 + ((size_t)kk * P.p.num_envs + e) * C * 3 + r) != 0.0) nz = 1;
-          }
-          if (!__syncthreads_or(nz)) {
-            for (int i = tid; i < n; i += NT)
-              w.V(V_V)[i] = (w.flags[i] & kFlagPart) && base_g ? __ldg(base_g + i) : w.V(V_VSTAR)[i];
-            try_start(KV + 1);
-          } else {
-            const int ldj = w.ldJ();
-            if (P.p.dynamics_factor) {
-              // the free motion's LDL^T of A
-              const double* Lg = P.p.dynamics_factor + (size_t)e * n_max * n_max;
-              load_lower<NT, HT, NS>(w, Lg, nullptr, 0.0);
-              HT* dinv = reinterpret_cast<HT*>(w.V(V_DINV));
-              for (int i = tid; i < n; i += NT) dinv[i] = fast_recip(HT(__ldg(Lg + (size_t)i * n + i)));
-              __syncthreads();
-            } else {
-              load_lower<NT, HT, NS>(w, w.A, nullptr, 0.0);
-              __syncthreads();
-              ldlt_blocked<NT, HT, LB>(w.H, n, w.ldH(), reinterpret_cast<HT*>(w.V(V_DINV)), w.tri,
-                                       w.tri_shift());  // the factor of A
-            }
-            // Two sets at a time: stage their impulses in the (here unused)
-            // scratch, form J^T gamma for both (threads 0-63 set k0, 64-127
-            // set k0+1), solve both with the factor on warps 0 and 1, then
-            // evaluate the candidates in order.
-            double* gs = reinterpret_cast<double*>(w.GJ);
-            for (int k0 = 0; k0 < KG; k0 += 2) {
-              const int nk = KG - k0 < 2 ? KG - k0 : 2;
-              for (int q = tid; q < nk * 3 * count; q += NT) {
-                const int kk = q / (3 * count), r = q - kk * 3 * count;
-                gs[q] = __ldg(P.p.gamma0 + ((size_t)(k0 + kk) * P.p.num_envs + e) * C * 3 + r);
-              }
-              __syncthreads();
-              {
-                const int kk = tid >> 6, i = tid & 63;
-                if (kk < nk && i < n) {
-                  const double* g = gs + kk * 3 * count;
-                  double acc = 0.0;
-                  for (int c = 0; c < count; ++c) {
-                    const double* Jc = w.J + (size_t)(3 * c) * ldj;
-                    acc += Jc[i] * g[3 * c] + Jc[ldj + i] * g[3 * c + 1] + Jc[2 * ldj + i] * g[3 * c + 2];
-                  }
-                  w.V(kk == 0 ? V_GRAD : V_DP)[i] = -acc;  // the solves give -H^-1 rhs
-                }
-              }
-              __syncthreads();
-              solve_warp<NT, HT, NS>(w, V_GRAD, V_DV, 0);
-              if (nk > 1) solve_warp<NT, HT, NS>(w, V_DP, V_DV2, 1);
-              __syncthreads();
-              for (int kk = 0; kk < nk; ++kk) {
-                const double* dvk = w.V(kk == 0 ? V_DV : V_DV2);
-                for (int i = tid; i < n; i += NT)
-                  w.V(V_V)[i] = (w.flags[i] & kFlagPart)
-                                    ? (base_g ? __ldg(base_g + i) : w.V(V_VSTAR)[i]) + dvk[i]
-                                    : w.V(V_VSTAR)[i];
-                try_start(KV + k0 + kk + 1);
-              }
-            }
-          }
-        }
-        if (last_is_best) {
-          have_e4 = true;
-        } else {
-          const int src = ws_accepted > 0 ? V_BEST : V_SAVE;
-          for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(src)[i];
-        }
-        __syncthreads();
-      }
-      const double cost_min_alpha = LSV == SAPB_LS_MONOTONE_DECAY ? 0.0 : 0.5;
-      int it = 0;
-      bool active = true;
-      for (;;) {
-        double e4[4];
-        if (have_e4) {
-          for (int k = 0; k < 4; ++k) e4[k] = e4_seed[k];
-          have_e4 = false;
-        } else {
-          evaluate<NT, HT, NS>(w, P, dt, e4);
-        }
-        evaluated = true;
-        cost = e4[0];
-        // convergence test (sim/contact_solve.py:2043-2087)
-        const double gn = sqrt(fmax(e4[1], 0.0)), pn = sqrt(fmax(e4[2], 0.0)), jn = sqrt(fmax(e4[3], 0.0));
-        grad_norm = gn;
-        const double opt_tol = P.o.optimality_abs_tol + P.o.optimality_rel_tol * fmax(pn, jn);
-        const bool opt = gn <= opt_tol;
-        bool cost_ok = false;
-        if (it > 0 && alpha > cost_min_alpha) {
-          const double sc = 0.5 * (fabs(cost) + fabs(previous_cost));
-          const double tol = P.o.cost_abs_tol + P.o.cost_rel_tol * sc;
-          if (fabs(cost - previous_cost) < tol) cost_ok = true;
-        }
-        newton_iterations = it;
-        if (opt || cost_ok) {
-          converged = 1;
-          active = false;
-        } else if (it >= P.o.max_iterations) {
-          active = false;
-        } else {
-          converged = 0;
-        }
-        if (!active) break;
-        // Newton direction
-        assemble_hessian<NT, HT, NS>(w, P.o.diag_shift);
-        factor_and_solve<NT, HT, NS, LB>(w);
-        if (!*w.factor_ok) {  // H not SPD (uniform: published by the barrier above)
-          status = SAPB_WORLD_NOT_SPD;
-          converged = 0;
-          break;
-        }
-        LsResult r;
-        double c4[4];
-        line_coefficients<NT, HT, NS>(w, c4);
-        if constexpr (LSV == SAPB_LS_ARMIJO_DECAY)
-          r = ls_armijo<NT, 1>(w, P, dt, cost, c4);
-        else if constexpr (LSV == SAPB_LS_EXACT_ROOT)
-          r = ls_exact<NT>(w, P, dt, cost, c4);
-        else
-          r = ls_monotone<NT, 1>(w, P, dt, cost, c4);
-        alpha = r.alpha;
-        status = r.status;
-        constexpr bool mono = LSV == SAPB_LS_MONOTONE_DECAY;
-        if (r.accepted || mono) ls_total += r.iterations;
-        if (r.accepted) {
-          previous_cost = cost;
-          for (int i = tid; i < n; i += NT) w.V(V_V)[i] += r.alpha * w.V(V_DV)[i];
-        } else if (mono) {
-          previous_cost = cost;
-        }
-        __syncthreads();
-        ++it;
-      }
-    }
-    // ---- outputs ------------------------------------------------------------
-    for (int i = tid; i < n_max; i += NT) P.out.v[base + i] = i < n ? w.V(V_V)[i] : 0.0;
-    for (int c = tid; c < C; c += NT) {
-      const size_t ci = (size_t)e * C + c;
-      const bool live = evaluated && c < count;
-      if (P.out.contact_gamma) {
-        P.out.contact_gamma[ci * 3 + 0] = live ? w.Cn(C_GAMMA + 0)[c] : 0.0;
-        P.out.contact_gamma[ci * 3 + 1] = live ? w.Cn(C_GAMMA + 1)[c] : 0.0;
-        P.out.contact_gamma[ci * 3 + 2] = live ? w.Cn(C_GAMMA + 2)[c] : 0.0;
-      }
-      if (P.out.contact_mode) {
-        int mode = SAPB_CONTACT_MODE_NONE;
-        if (live) {
-          double g[3], cst;
-          mode = project_contact(w.cc(c), w.Cn(C_VC + 0)[c], w.Cn(C_VC + 1)[c], w.Cn(C_VC + 2)[c], g, &cst, nullptr);
-        }
-        P.out.contact_mode[ci] = mode;
-      }
-    }
-    if (tid == 0) {
-      if (P.out.cost) P.out.cost[e] = evaluated ? cost : 0.0;
-      if (P.out.newton_iterations) P.out.newton_iterations[e] = newton_iterations;
-      if (P.out.line_search_iterations) P.out.line_search_iterations[e] = ls_total;
-      if (P.out.converged) P.out.converged[e] = converged;
-      if (P.out.status) P.out.status[e] = status;
-      if (P.out.grad_norm) P.out.grad_norm[e] = grad_norm;
-      if (P.out.warm_start_accepted) P.out.warm_start_accepted[e] = ws_accepted;
-    }
-    __syncthreads();
+    solve_world<NT, HT, NS, LSV, LB>(P, L, smem, red, s_partmask, s_factor_ok, e, n_max, n_world, use_guess);
   }
 }
 
@@ -1015,36 +1060,36 @@ static cudaError_t launch_solve(const SolveParams& P, cudaStream_t stream, int* 
 // default), from measurements on B200: 35 DOFs = 7 blocks of 5 is fastest
 // in both precisions; wider blocks lengthen the serial diagonal chain and
 // the register block, narrower ones add barriers.
-template <int NS> struct LdltBlocks { static constexpr int kCount = 1; static constexpr int kW[1] = {4}; };
-template <> struct LdltBlocks<35> { static constexpr int kCount = 2; static constexpr int kW[2] = {5, 4}; };
-template <> struct LdltBlocks<18> { static constexpr int kCount = 2; static constexpr int kW[2] = {6, 4}; };
-template <> struct LdltBlocks<13> { static constexpr int kCount = 2; static constexpr int kW[2] = {4, 5}; };
-template <> struct LdltBlocks<6> { static constexpr int kCount = 1; static constexpr int kW[1] = {6}; };
 
-template <int NS, int LB>
-static cudaError_t launch_solve_lb(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
-  return fp32 ? launch_solve<128, float, 4, NS, LB>(P, stream, blocks_out)
-              : launch_solve<128, double, 3, NS, LB>(P, stream, blocks_out);
+// One Hessian precision of the kernels of one DOF specialisation NS (every
+// line search, every LDL^T block width), instantiated in a translation unit
+// of its own (sapb_solve_n*_f32.cu / _f64.cu) so they compile in parallel.
+template <int NS, bool FP32>
+cudaError_t launch_solve_np(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
+  using HT = typename std::conditional<FP32, float, double>::type;
+  constexpr int MINB = FP32 ? 4 : 3;
+  if constexpr (LdltBlocks<NS>::kCount > 1) {
+    if (P.o.ldlt_block == LdltBlocks<NS>::kW[1])
+      return launch_solve<128, HT, MINB, NS, LdltBlocks<NS>::kW[LdltBlocks<NS>::kCount > 1 ? 1 : 0]>(P, stream,
+                                                                                                      blocks_out);
+  }
+  return launch_solve<128, HT, MINB, NS, LdltBlocks<NS>::kW[0]>(P, stream, blocks_out);  // the default (0 or unknown)
 }
 
-// The kernels of one DOF specialisation NS (both Hessian precisions, every
-// line search), instantiated in a translation unit of their own
-// (sapb_solve_n*.cu) so the specialisations compile in parallel.
 template <int NS>
-cudaError_t launch_solve_ns(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
-  constexpr int n = LdltBlocks<NS>::kCount;
-  const int want = P.o.ldlt_block;
-  if (n > 1 && want == LdltBlocks<NS>::kW[n > 1 ? 1 : 0])
-    return launch_solve_lb<NS, LdltBlocks<NS>::kW[n > 1 ? 1 : 0]>(P, fp32, stream, blocks_out);
-  return launch_solve_lb<NS, LdltBlocks<NS>::kW[0]>(P, fp32, stream, blocks_out);  // the default (0 or unknown)
+inline cudaError_t launch_solve_ns(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
+  return fp32 ? launch_solve_np<NS, true>(P, stream, blocks_out) : launch_solve_np<NS, false>(P, stream, blocks_out);
 }
 
-
-extern template cudaError_t launch_solve_ns<35>(const SolveParams&, bool, cudaStream_t, int*);
-extern template cudaError_t launch_solve_ns<18>(const SolveParams&, bool, cudaStream_t, int*);
-extern template cudaError_t launch_solve_ns<13>(const SolveParams&, bool, cudaStream_t, int*);
-extern template cudaError_t launch_solve_ns<6>(const SolveParams&, bool, cudaStream_t, int*);
-extern template cudaError_t launch_solve_ns<0>(const SolveParams&, bool, cudaStream_t, int*);
+#define SAPB_EXTERN_SOLVE(NS)                                                                  \
+  extern template cudaError_t launch_solve_np<NS, true>(const SolveParams&, cudaStream_t, int*); \
+  extern template cudaError_t launch_solve_np<NS, false>(const SolveParams&, cudaStream_t, int*);
+SAPB_EXTERN_SOLVE(35)
+SAPB_EXTERN_SOLVE(18)
+SAPB_EXTERN_SOLVE(13)
+SAPB_EXTERN_SOLVE(6)
+SAPB_EXTERN_SOLVE(0)
+#undef SAPB_EXTERN_SOLVE
 
 }  // namespace sapb
 

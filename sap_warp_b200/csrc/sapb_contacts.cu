@@ -10,8 +10,10 @@
 // signed surface distance.  This file covers the primitive pairs of the
 // synthetic scenes with closed-form tests:
 //   plane-sphere, plane-box (the deepest four corners), sphere-sphere, sphere-box (closest
-//   point), box-box (corners of each box against the faces of the other:
-//   vertex-face contacts, no edge-edge).
+//   point), box-box (corners of each box against the faces of the other,
+//   and, when a separating-axis test over the 15 axes finds an edge-edge
+//   axis the least penetrating, one contact between the two crossing edges,
+//   as sap_collide_box_box does for edges, sim/collision/primitive.py:692-1148).
 // Spheres keep their centre as the witness point with the radius in the
 // margin (the reference's radius_eff); boxes and planes have zero radius.
 // A contact is emitted when its signed distance is below the gap.
@@ -139,6 +141,65 @@ __device__ void box_corners_vs_box(const GenParams& P, int sa_box, int sb_vert, 
   }
 }
 
+// Edge-edge contact of two boxes (normal from a to b): the separating-axis
+// test over the 3 + 3 face axes and the 9 edge-pair axes; when the best
+// (least penetrating) edge axis beats every face axis by a relative 1e-6 and
+// lies within the gap, the two edges supporting it (A's farthest along the
+// axis, B's farthest against it) give one contact at their closest points,
+// provided those lie inside both edges (the edges cross; otherwise a corner
+// is involved and the vertex-face tests cover it).
+__device__ void box_edge_contact(int a, int b, Xf Xa, V3 ha, Xf Xb, V3 hb, double gap, double ma, double mb,
+                                 Emit& emit) {
+  const V3 A[3] = {qrot(Xa.q, v3(1, 0, 0)), qrot(Xa.q, v3(0, 1, 0)), qrot(Xa.q, v3(0, 0, 1))};
+  const V3 B[3] = {qrot(Xb.q, v3(1, 0, 0)), qrot(Xb.q, v3(0, 1, 0)), qrot(Xb.q, v3(0, 0, 1))};
+  const double hA[3] = {ha.x, ha.y, ha.z}, hB[3] = {hb.x, hb.y, hb.z};
+  const V3 d = Xb.p - Xa.p;
+  auto radius = [&](const V3* E, const double* h, V3 L) {
+    return h[0] * fabs(dot(E[0], L)) + h[1] * fabs(dot(E[1], L)) + h[2] * fabs(dot(E[2], L));
+  };
+  double best_face = -1.0e300;
+  for (int k = 0; k < 3; ++k) {
+    const double sa = fabs(dot(d, A[k])) - (hA[k] + radius(B, hB, A[k]));
+    const double sb = fabs(dot(d, B[k])) - (radius(A, hA, B[k]) + hB[k]);
+    best_face = fmax(best_face, fmax(sa, sb));
+  }
+  // separated along a face axis by the gap or more: no edge axis can be both
+  // better and within the gap
+  if (!(best_face < gap)) return;
+  double best_edge = -1.0e300;
+  int bi = -1, bj = -1;
+  V3 bL = v3(0, 0, 0);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      V3 L = cross(A[i], B[j]);
+      const double len = sqrt(dot(L, L));
+      if (len < 1.0e-6) continue;  // parallel edges: the face axes decide
+      L = (1.0 / len) * L;
+      if (dot(d, L) < 0.0) L = -L;
+      const double sep = dot(d, L) - radius(A, hA, L) - radius(B, hB, L);
+      if (sep > best_edge) {
+        best_edge = sep;
+        bi = i;
+        bj = j;
+        bL = L;
+      }
+    }
+  const double scale = fmax(fmax(fmax(hA[0], hA[1]), fmax(hA[2], hB[0])), fmax(hB[1], hB[2]));
+  if (bi < 0 || !(best_edge > best_face + 1.0e-6 * scale) || !(best_edge < gap)) return;
+  V3 cA = Xa.p, cB = Xb.p;
+  for (int m = 0; m < 3; ++m) {
+    if (m != bi) cA = cA + (dot(A[m], bL) >= 0.0 ? hA[m] : -hA[m]) * A[m];
+    if (m != bj) cB = cB - (dot(B[m], bL) >= 0.0 ? hB[m] : -hB[m]) * B[m];
+  }
+  const V3 u = A[bi], v = B[bj], w = cA - cB;
+  const double uv = dot(u, v), uw = dot(u, w), vw = dot(v, w);
+  const double den = 1.0 - uv * uv;
+  if (den < 1.0e-12) return;
+  const double s = (uv * vw - uw) / den, t = (vw - uv * uw) / den;
+  if (fabs(s) > hA[bi] || fabs(t) > hB[bj]) return;
+  emit(a, b, cA + s * u, cB + t * v, bL, ma, mb);
+}
+
 // sap_test_group_pair (sim/collision/broad_phase_common.py:133-150)
 __device__ __forceinline__ bool groups_meet(int ga, int gb) {
   if (ga == 0 || gb == 0) return false;
@@ -261,6 +322,7 @@ __device__ void pair_contacts(const GenParams& P, int sa, int sb, Emit& emit) {
   if (t1 == SAPB_SHAPE_BOX && t2 == SAPB_SHAPE_BOX) {
     box_corners_vs_box(P, a, b, Xa, sa3, Xb, sb3, gap + m1 + m2, m1, m2, emit);
     box_corners_vs_box(P, b, a, Xb, sb3, Xa, sa3, gap + m1 + m2, m2, m1, emit);
+    box_edge_contact(a, b, Xa, sa3, Xb, sb3, gap + m1 + m2, m1, m2, emit);
   }
 }
 

@@ -1,0 +1,6 @@
+// Contact-solve kernels specialised on 18 DOFs per world; FP64 Hessian and factor.
+#include "sapb_contact_solve.cuh"
+
+namespace sapb {
+template cudaError_t launch_solve_np<18, false>(const SolveParams&, cudaStream_t, int*);
+}  // namespace sapb

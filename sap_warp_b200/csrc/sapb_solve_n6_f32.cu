@@ -1,0 +1,6 @@
+// Contact-solve kernels specialised on 6 DOFs per world; FP32 Hessian and factor.
+#include "sapb_contact_solve.cuh"
+
+namespace sapb {
+template cudaError_t launch_solve_np<6, true>(const SolveParams&, cudaStream_t, int*);
+}  // namespace sapb

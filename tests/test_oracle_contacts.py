@@ -99,3 +99,33 @@ def test_small_box_on_big_box():
     world1 = bq[1, :3] + c["point1"]
     phi = np.einsum("ij,ij->i", world1 - (bq[0, :3] + c["point0"]), c["normal"])
     np.testing.assert_allclose(phi, -5e-4, atol=1e-12)
+
+
+def test_crossed_box_edges_touch_edge_to_edge():
+    """Two unit cubes each standing on an edge, the lower one's top edge along
+    x, the upper one's bottom edge along y, crossing above the origin with
+    1 mm of overlap: no corner of either cube is inside the other, so the one
+    contact is edge-edge -- normal +z from the lower to the upper cube,
+    witness points on the two edges at the crossing, phi0 = -1 mm."""
+    r = np.sqrt(0.5)
+    qx = np.array([np.sin(np.pi / 8), 0.0, 0.0, np.cos(np.pi / 8)])  # 45 degrees about x
+    qy = np.array([0.0, np.sin(np.pi / 8), 0.0, np.cos(np.pi / 8)])  # 45 degrees about y
+    top = r  # the lower cube's top edge height
+    z1 = top + r - 1e-3
+    shapes, bq = _scene([SAPB_SHAPE_BOX, SAPB_SHAPE_BOX], [[0.5, 0.5, 0.5], [0.5, 0.5, 0.5]],
+                        [np.concatenate([[0.0, 0.0, 0.0], qx]), np.concatenate([[0.0, 0.0, z1], qy])])
+    c = oc.generate(shapes, bq, gap=1e-4)
+    edge = [k for k in range(len(c["shape0"])) if c["shape0"][k] == 0 and c["shape1"][k] == 1]
+    assert len(edge) == 1, c
+    k = edge[0]
+    np.testing.assert_allclose(c["normal"][k], [0.0, 0.0, 1.0], atol=1e-12)
+    w0 = bq[0, :3] + oc.qrot(bq[0, 3:], c["point0"][k])
+    w1 = bq[1, :3] + oc.qrot(bq[1, 3:], c["point1"][k])
+    np.testing.assert_allclose(w0, [0.0, 0.0, top], atol=1e-12)
+    np.testing.assert_allclose(w1, [0.0, 0.0, z1 - r], atol=1e-12)
+    np.testing.assert_allclose(np.dot(w1 - w0, c["normal"][k]), -1e-3, atol=1e-12)
+    # lifted 1 mm clear of each other: nothing
+    shapes, bq = _scene([SAPB_SHAPE_BOX, SAPB_SHAPE_BOX], [[0.5, 0.5, 0.5], [0.5, 0.5, 0.5]],
+                        [np.concatenate([[0.0, 0.0, 0.0], qx]), np.concatenate([[0.0, 0.0, top + r + 1e-3], qy])])
+    c = oc.generate(shapes, bq, gap=1e-4)
+    assert not any(c["shape0"][k] == 0 and c["shape1"][k] == 1 for k in range(len(c["shape0"])))
