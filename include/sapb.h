@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 13
+#define SAPB_ABI_VERSION 14
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -248,6 +248,23 @@ typedef struct sapb_model_desc {
   const double* shape_material_mu;  /* [S] or NULL -> fallback */
   const double* shape_material_ke;  /* [S] or NULL -> fallback */
   const double* shape_material_tau; /* [S] or NULL -> fallback */
+  /* Uneven batches (no counterpart in the reference, whose per-world blocks
+   * are equal, sim/contact_solve.py:3327-3335).  NULL: every world has the
+   * *_per_world counts.  Else [W+1] prefix offsets of each world's joints,
+   * bodies, DOFs and articulations in the global arrays, the world of each
+   * body [B], and the totals; the *_per_world counts are then the largest
+   * world's (coordinates follow joint_q_start).  The free motion then writes
+   * the solve's per-DOF arrays (v*, vdot, v_start, qd_slots) in slots of
+   * dofs_per_world per world, A and the Jacobian rows compact in their
+   * slots -- the layout of sapb_contact_problem.dof_count -- and the step's
+   * tail reads the solve's velocities from those slots.  The dense layout
+   * only; sapb_integrate_positions and the C handle take equal blocks. */
+  const int32_t* world_joint_start;
+  const int32_t* world_body_start;
+  const int32_t* world_dof_start;
+  const int32_t* world_articulation_start;
+  const int32_t* body_world;
+  int32_t total_joints, total_bodies, total_dofs, total_articulations;
 } sapb_model_desc;
 
 /* Start-of-step state, control and the flat contact buffer of collision
@@ -337,6 +354,9 @@ typedef struct sapb_prepare_outputs {
    * free motion's own LDL^T), or NULL.  Dense layout; needs history with
    * gamma_start. */
   double* v_start;
+  /* [W][dofs_per_world] the start-of-step velocities in the solve's slots
+   * (uneven batches: the solve's v0), or NULL */
+  double* qd_slots;
 } sapb_prepare_outputs;
 
 /* Device workspace bytes of sapb_free_motion_contacts. */

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 13
+SAPB_ABI_VERSION = 14
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -238,6 +238,15 @@ class ModelDesc(C.Structure):
         ("shape_material_mu", _p),
         ("shape_material_ke", _p),
         ("shape_material_tau", _p),
+        ("world_joint_start", _p),
+        ("world_body_start", _p),
+        ("world_dof_start", _p),
+        ("world_articulation_start", _p),
+        ("body_world", _p),
+        ("total_joints", C.c_int32),
+        ("total_bodies", C.c_int32),
+        ("total_dofs", C.c_int32),
+        ("total_articulations", C.c_int32),
     ]
 
 
@@ -298,6 +307,7 @@ class PrepareOutputs(C.Structure):
         ("contact_source", _p),
         ("history", _p),
         ("v_start", _p),
+        ("qd_slots", _p),
     ]
 
 

@@ -94,9 +94,9 @@ __global__ void eval_fk_kernel(const BoundaryParams P, const double* joint_q, co
 BoundaryParams make_params(const sapb_model_desc* m) {
   BoundaryParams P;
   P.m = *m;
-  P.num_joints = m->num_worlds * m->joints_per_world;
-  P.num_bodies = m->num_worlds * m->bodies_per_world;
-  P.num_articulations = m->num_worlds * m->articulations_per_world;
+  P.num_joints = model_joints(*m);
+  P.num_bodies = model_bodies(*m);
+  P.num_articulations = model_articulations(*m);
   return P;
 }
 

@@ -229,6 +229,14 @@ static int32_t check_model(const sapb_model_desc* m, const char* where) {
     sapb::set_last_error("%s: missing model array", where);
     return SAPB_ERR_INVALID_ARGUMENT;
   }
+  const bool uneven = m->world_joint_start || m->world_body_start || m->world_dof_start ||
+                      m->world_articulation_start || m->body_world;
+  if (uneven && (!m->world_joint_start || !m->world_body_start || !m->world_dof_start ||
+                 !m->world_articulation_start || !m->body_world || m->total_joints <= 0 || m->total_bodies <= 0 ||
+                 m->total_dofs <= 0 || m->total_articulations <= 0)) {
+    sapb::set_last_error("%s: an uneven batch needs all four world offset arrays, body_world and the totals", where);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
   return SAPB_OK;
 }
 
@@ -257,6 +265,10 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inpu
                               !out->tau_d || !out->body0 || !out->body1)) {
     sapb::set_last_error("sapb_free_motion_contacts: missing contact output array");
     return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (blk && m->world_joint_start) {
+    sapb::set_last_error("sapb_free_motion_contacts: tree-blocked outputs need equal per-world blocks");
+    return SAPB_ERR_UNSUPPORTED;
   }
   if (blk && (m->bodies_per_world > 64 || m->dofs_per_world != 6 * m->bodies_per_world ||
               m->joints_per_world != m->bodies_per_world || out->dynamics_factor)) {
@@ -357,6 +369,11 @@ int32_t sapb_integrate_positions(const sapb_model_desc* m, const double* q_in, c
                                  const double* v_new, const double* dt, int32_t mode, double* q_out, void* stream) {
   const int32_t st = check_model(m, "sapb_integrate_positions");
   if (st != SAPB_OK) return st;
+  if (m->world_joint_start) {
+    sapb::set_last_error("sapb_integrate_positions: equal per-world blocks only (sapb_step_tail_launch takes uneven "
+                         "batches)");
+    return SAPB_ERR_UNSUPPORTED;
+  }
   if (!q_in || !v_new || !dt || !q_out || (mode == SAPB_INTEGRATE_MIDPOINT && !v_prev) ||
       (mode != SAPB_INTEGRATE_MIDPOINT && mode != SAPB_INTEGRATE_SAP_EULER)) {
     sapb::set_last_error("sapb_integrate_positions: bad arguments");

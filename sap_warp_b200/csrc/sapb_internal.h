@@ -16,6 +16,49 @@ constexpr size_t kMaxSmemPerBlock = 227 * 1024 - 1024;
 
 void set_last_error(const char* fmt, ...);
 
+// A world's block of joints, bodies, DOFs and articulations in the global
+// model arrays: equal blocks, or the offsets of an uneven batch.
+struct WorldSpan {
+  int j0, nj, b0, nb, d0, nd, a0, na;
+};
+__host__ __device__ inline WorldSpan world_span(const sapb_model_desc& m, int e) {
+  WorldSpan w;
+  if (m.world_joint_start) {
+    w.j0 = m.world_joint_start[e];
+    w.nj = m.world_joint_start[e + 1] - w.j0;
+    w.b0 = m.world_body_start[e];
+    w.nb = m.world_body_start[e + 1] - w.b0;
+    w.d0 = m.world_dof_start[e];
+    w.nd = m.world_dof_start[e + 1] - w.d0;
+    w.a0 = m.world_articulation_start[e];
+    w.na = m.world_articulation_start[e + 1] - w.a0;
+  } else {
+    w.j0 = e * m.joints_per_world;
+    w.nj = m.joints_per_world;
+    w.b0 = e * m.bodies_per_world;
+    w.nb = m.bodies_per_world;
+    w.d0 = e * m.dofs_per_world;
+    w.nd = m.dofs_per_world;
+    w.a0 = e * m.articulations_per_world;
+    w.na = m.articulations_per_world;
+  }
+  return w;
+}
+__host__ __device__ inline int model_joints(const sapb_model_desc& m) {
+  return m.world_joint_start ? m.total_joints : m.num_worlds * m.joints_per_world;
+}
+__host__ __device__ inline int model_bodies(const sapb_model_desc& m) {
+  return m.world_joint_start ? m.total_bodies : m.num_worlds * m.bodies_per_world;
+}
+__host__ __device__ inline int model_articulations(const sapb_model_desc& m) {
+  return m.world_joint_start ? m.total_articulations : m.num_worlds * m.articulations_per_world;
+}
+// The world of body b (-1 outside the model).
+__host__ __device__ inline int body_world_of(const sapb_model_desc& m, int b) {
+  if (b < 0 || b >= model_bodies(m)) return -1;
+  return m.body_world ? m.body_world[b] : b / m.bodies_per_world;
+}
+
 size_t contact_solve_smem_bytes(int n, int C, int hessian_precision);
 int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant);
 int ldlt_block_widths(int n, int32_t* out, int capacity);

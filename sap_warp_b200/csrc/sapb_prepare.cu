@@ -98,15 +98,14 @@ __global__ void scatter_contacts_kernel(const PrepParams P) {
   const int S = P.m.num_shapes;
   const int b0 = (sh0 >= 0 && sh0 < S) ? P.m.shape_body[sh0] : -1;
   const int b1 = (sh1 >= 0 && sh1 < S) ? P.m.shape_body[sh1] : -1;
-  const int B = P.m.bodies_per_world;
-  const int nb = B * P.m.num_worlds;
   // _contact_env_from_shapes (sim/sap_helpers.py:439-464)
+  const int w0 = body_world_of(P.m, b0), w1 = body_world_of(P.m, b1);
   int env = -1;
-  if (b0 >= 0 && b0 < nb) env = b0 / B;
-  else if (b1 >= 0 && b1 < nb) env = b1 / B;
+  if (w0 >= 0) env = w0;
+  else if (w1 >= 0) env = w1;
   if (env < 0) return;
-  if (b0 >= 0 && (b0 >= nb || b0 / B != env)) return;
-  if (b1 >= 0 && (b1 >= nb || b1 / B != env)) return;
+  if (b0 >= 0 && w0 != env) return;
+  if (b1 >= 0 && w1 != env) return;
   const int slot = atomicAdd(&P.env_count[env], 1);
   if (slot < P.o.max_contacts)
     P.env_src[(size_t)env * P.o.max_contacts + slot] = t;
@@ -212,10 +211,16 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x;
   const int e = blockIdx.x;
-  const int B = P.m.bodies_per_world, n = P.m.dofs_per_world, C = P.o.max_contacts;
-  const int Jw = P.m.joints_per_world;
+  const int C = P.o.max_contacts;
   const bool blk = P.o.tree_blocked != 0;  // worlds of free bodies, tree-blocked outputs
-  const PrepLayout L = prep_layout(B, n, C, blk);
+  // shared memory laid out for the largest world; this world's own block
+  const PrepLayout L = prep_layout(P.m.bodies_per_world, P.m.dofs_per_world, C, blk);
+  const WorldSpan ws = world_span(P.m, e);
+  const int B = ws.nb, n = ws.nd, Jw = ws.nj;
+  // the solve's per-DOF arrays: slots of dofs_per_world per world (the world's
+  // global DOF offset when the blocks are equal)
+  const int n_slot = P.m.dofs_per_world;
+  const size_t vs0 = (size_t)e * n_slot;
   double* poseA = reinterpret_cast<double*>(smem + L.pose);
   double* poseB = reinterpret_cast<double*>(smem + L.pose2);
   double* fm = reinterpret_cast<double*>(smem + L.fm);
@@ -244,7 +249,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   uint16_t* tri = reinterpret_cast<uint16_t*>(smem + L.tri);
   double* jg = reinterpret_cast<double*>(smem + L.jg);
   const bool want_vstart = VS && !blk && P.out.v_start && P.gamma_start;
-  const int j0 = e * Jw, b0g = e * B, d0 = e * n;
+  const int j0 = ws.j0, b0g = ws.b0, d0 = ws.d0;
   const double* q = P.in.joint_q;
   const double* qd = P.in.joint_qd;
 
@@ -551,7 +556,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
       Tm[k] = v;
     }
   }
-  double* Ag = blk ? nullptr : P.out.dynamics_matrix + (size_t)e * n * n;
+  double* Ag = blk ? nullptr : P.out.dynamics_matrix + (size_t)e * n_slot * n_slot;  // compact, stride n
   for (int k = tid; k < (blk ? 0 : n * n); k += kPrepNT) {
     const int i = k / n, j = k - i * n;
     if (j > i) continue;
@@ -617,7 +622,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   } else {
   ldlt_blocked<kPrepNT, double, 5>(H, n, n, dinv, tri);  // width 5: measured fastest for 35 DOFs
   if (write_factor) {
-    double* Lg = P.out.dynamics_factor + (size_t)e * n * n;
+    double* Lg = P.out.dynamics_factor + (size_t)e * n_slot * n_slot;
     for (int k = tid; k < n * n; k += kPrepNT) {
       const int i = k / n, j = k - i * n;
       if (j <= i) Lg[k] = H[k];
@@ -721,8 +726,9 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   __syncthreads();
   for (int i = tid; i < n; i += kPrepNT) {
     const double vd = vdot[i];
-    P.out.v_star[d0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vd;
-    if (P.out.vdot) P.out.vdot[d0 + i] = vd;
+    P.out.v_star[vs0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vd;
+    if (P.out.vdot) P.out.vdot[vs0 + i] = vd;
+    if (P.out.qd_slots) P.out.qd_slots[vs0 + i] = P.in.joint_qd[d0 + i];
   }
   if (P.out.body_q) {
     for (int k = tid; k < 7 * B; k += kPrepNT) {
@@ -737,7 +743,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   // side 1's (a contact between two shapes of one tree keeps the combined
   // columns on side 0).
   const int ncols = blk ? 12 : n;
-  double* Jout = P.out.jacobian + (size_t)e * C * 3 * ncols;
+  double* Jout = P.out.jacobian + (size_t)e * C * 3 * (blk ? 12 : n_slot);  // rows compact, stride ncols
   auto tree_of = [&](int lb) {
     if (lb < 0 || bj[lb] < 0) return -1;
     const int t = (P.m.joint_qd_start[bj[lb]] - d0) / 6;
@@ -890,7 +896,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
       ldlt_solve_warp<double>(H, n, n, dinv, jg, z, false, ldlt_pivots_ok_warp<double>(H, n, n));
       __syncwarp();
       for (int i = tid; i < n; i += 32)
-        P.out.v_start[d0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vdot[i] + z[i];
+        P.out.v_start[vs0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vdot[i] + z[i];
     }
   } else if (want_vstart) {
     __syncthreads();
@@ -908,7 +914,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     }
     __syncthreads();
     for (int i = tid; i < n; i += kPrepNT)
-      P.out.v_start[d0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vdot[i] + z[i];
+      P.out.v_start[vs0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vdot[i] + z[i];
   }
 }
 

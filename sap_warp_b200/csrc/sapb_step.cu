@@ -166,6 +166,10 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     set_last_error("sapb_create: invalid model description");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
+  if (model->world_joint_start) {
+    set_last_error("sapb_create: the handle takes equal per-world blocks");
+    return SAPB_ERR_UNSUPPORTED;
+  }
   if (opts->prepare.tree_blocked) {
     set_last_error("sapb_create: the handle runs the dense layout (tree_blocked must be 0)");
     return SAPB_ERR_UNSUPPORTED;

@@ -18,30 +18,32 @@ namespace {
 
 __global__ void step_tail_kernel(const sapb_model_desc m, const sapb_step_tail T) {
   const int e = blockIdx.x;
-  const int Jw = m.joints_per_world;
+  const WorldSpan ws = world_span(m, e);
   const double h = T.dt[e];
-  for (int jl = threadIdx.x; jl < Jw; jl += blockDim.x) {
-    const int j = e * Jw + jl;
+  // the solve's velocities by global DOF index: its slots of dofs_per_world
+  // per world (an offset of zero when the blocks are equal)
+  const double* v_new = T.v_new + ((long long)e * m.dofs_per_world - ws.d0);
+  for (int jl = threadIdx.x; jl < ws.nj; jl += blockDim.x) {
+    const int j = ws.j0 + jl;
     if (m.joint_type[j] == SAPB_JOINT_FIXED) {
       for (int k = m.joint_q_start[j]; k < m.joint_q_start[j + 1]; ++k) T.joint_q_out[k] = T.joint_q_in[k];
     } else {
-      integrate_joint(m, j, T.joint_q_in, T.v_prev, T.v_new, h, T.mode, T.joint_q_out);
+      integrate_joint(m, j, T.joint_q_in, T.v_prev, v_new, h, T.mode, T.joint_q_out);
     }
     if (T.joint_qd_out) {
       if (T.qd_public) {
-        public_velocity_joint(m, j, T.joint_q_out, T.v_new, T.joint_qd_out);
+        public_velocity_joint(m, j, T.joint_q_out, v_new, T.joint_qd_out);
       } else {
         const int ds = m.joint_qd_start[j];
         const int dim = m.joint_dof_dim[2 * j] + m.joint_dof_dim[2 * j + 1];
-        for (int k = 0; k < dim; ++k) T.joint_qd_out[ds + k] = T.v_new[ds + k];
+        for (int k = 0; k < dim; ++k) T.joint_qd_out[ds + k] = v_new[ds + k];
       }
     }
   }
   if (!T.body_q_out) return;  // uniform over the block
   __syncthreads();            // this world's new coordinates and velocities
-  const int Aw = m.articulations_per_world;
-  for (int al = threadIdx.x; al < Aw; al += blockDim.x)
-    fk_articulation(m, e * Aw + al, m.num_worlds * m.bodies_per_world, T.joint_q_out,
+  for (int al = threadIdx.x; al < ws.na; al += blockDim.x)
+    fk_articulation(m, ws.a0 + al, model_bodies(m), T.joint_q_out,
                     T.qd_public ? T.joint_qd_out : nullptr, T.body_q_out, T.body_qd_out);
 }
 

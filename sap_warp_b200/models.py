@@ -603,3 +603,106 @@ def box_shapes(host: dict):
                     shape_type=np.concatenate([np.full(E * B, SAPB_SHAPE_BOX), [SAPB_SHAPE_PLANE]]).astype(np.int32),
                     shape_scale=scale, shape_X_bs=X,
                     shape_body=np.concatenate([np.arange(E * B), [-1]]).astype(np.int32))
+
+
+def concat_models(parts) -> SapModel:
+    """One uneven batch from models of equal-block worlds (each of one or
+    more worlds, of any sizes): the global arrays concatenated, their body,
+    joint, DOF, coordinate, articulation and world indices shifted, and the
+    per-world offsets (world_*_start) set."""
+    import dataclasses
+
+    dev = parts[0].device
+    cat = lambda name: torch.cat([getattr(m, name) for m in parts])
+    offs = {k: np.cumsum([0] + [int(getattr(m, k)) for m in parts]) for k in
+            ("joint_count", "body_count", "joint_dof_count", "joint_coord_count", "articulation_count",
+             "world_count", "shape_count")}
+
+    def shifted(name, key, keep_negative=True):
+        out = []
+        for i, m in enumerate(parts):
+            t = getattr(m, name)
+            o = int(offs[key][i])
+            out.append(torch.where(t >= 0, t + o, t) if keep_negative else t + o)
+        return torch.cat(out)
+
+    def starts(name, key):  # [N+1] prefix arrays
+        out = [getattr(m, name)[:-1] + int(offs[key][i]) for i, m in enumerate(parts)]
+        out.append(torch.tensor([int(offs[key][-1])], dtype=parts[0].__getattribute__(name).dtype, device=dev))
+        return torch.cat(out)
+
+    def world_starts(key):
+        w = []
+        for i, m in enumerate(parts):
+            W = int(m.world_count)
+            per = int(getattr(m, key)) // W
+            w.extend(int(offs[key][i]) + per * np.arange(W))
+        w.append(int(offs[key][-1]))
+        return torch.as_tensor(np.asarray(w), dtype=torch.int32, device=dev)
+
+    f = {fl.name: getattr(parts[0], fl.name) for fl in dataclasses.fields(SapModel)}
+    for name in ("joint_count", "body_count", "joint_dof_count", "joint_coord_count", "articulation_count",
+                 "world_count", "shape_count"):
+        f[name] = int(offs[name][-1])
+    for name in ("joint_type", "joint_dof_dim", "joint_axis", "joint_X_p", "joint_X_c", "joint_q", "joint_qd",
+                 "body_q", "body_qd", "body_mass", "body_inertia", "body_com", "body_flags", "gravity",
+                 "joint_armature", "joint_target_mode", "joint_target_ke", "joint_target_kd", "joint_target_pos",
+                 "joint_target_vel", "joint_f", "joint_act", "joint_effort_limit", "joint_limit_lower",
+                 "joint_limit_upper", "joint_limit_ke", "joint_limit_kd"):
+        f[name] = cat(name)
+    for name in ("shape_material_mu", "shape_material_ke", "shape_material_tau"):
+        f[name] = None if any(getattr(m, name) is None for m in parts) else cat(name)
+    f["joint_parent"] = shifted("joint_parent", "body_count")
+    f["joint_child"] = shifted("joint_child", "body_count")
+    f["joint_ancestor"] = shifted("joint_ancestor", "joint_count")
+    f["joint_articulation"] = shifted("joint_articulation", "articulation_count")
+    f["body_world"] = shifted("body_world", "world_count", keep_negative=False)
+    f["shape_body"] = shifted("shape_body", "body_count")
+    f["joint_q_start"] = starts("joint_q_start", "joint_coord_count")
+    f["joint_qd_start"] = starts("joint_qd_start", "joint_dof_count")
+    f["articulation_start"] = starts("articulation_start", "joint_count")
+    f["world_joint_start"] = world_starts("joint_count")
+    f["world_body_start"] = world_starts("body_count")
+    f["world_dof_start"] = world_starts("joint_dof_count")
+    f["world_articulation_start"] = world_starts("articulation_count")
+    f["body_label"], f["joint_label"] = (), ()
+    return SapModel(**f)
+
+
+def concat_contacts(parts, shape_offsets) -> "SapContacts":
+    """The live contacts of several flat buffers in one (shape indices
+    shifted by each part's shape offset); synchronous (test and bench set-up)."""
+    from .runtime import SapContacts
+
+    names = [k for k in vars(parts[0]) if isinstance(getattr(parts[0], k), torch.Tensor) and k != "rigid_contact_count"]
+    counts = [int(c.rigid_contact_count.item()) for c in parts]
+    out = {}
+    for k in names:
+        seg = []
+        for c, n, o in zip(parts, counts, shape_offsets):
+            t = getattr(c, k)[:n]
+            if k in ("rigid_contact_shape0", "rigid_contact_shape1"):
+                t = torch.where(t >= 0, t + int(o), t)
+            seg.append(t)
+        out[k] = torch.cat(seg).contiguous()
+    cnt = torch.tensor([sum(counts)], dtype=torch.int32, device=parts[0].rigid_contact_count.device)
+    return SapContacts(rigid_contact_count=cnt, **out)
+
+
+def mixed_rollout_scene(worlds_per_kind, seed: int, device, kinds=("arm_box", "quadruped", "humanoid"), **kw):
+    """An uneven batch of rollout scenes: `worlds_per_kind` worlds of each
+    kind (arm + box 13 DOF, quadruped 18, humanoid 35 by default), their
+    models, states, controls and contacts concatenated.  Returns (model,
+    state, control, contacts, parts) with parts the per-kind
+    (model, state, control, contacts)."""
+    from .runtime import SapControl, SapState
+
+    parts = [rollout_scene(k, worlds_per_kind, seed + i, device, **kw)[:4] for i, k in enumerate(kinds)]
+    models_ = [p[0] for p in parts]
+    model = concat_models(models_)
+    state = SapState(joint_q=torch.cat([p[1].joint_q for p in parts]), joint_qd=torch.cat([p[1].joint_qd for p in parts]),
+                     body_q=torch.cat([p[1].body_q for p in parts]), body_f=torch.cat([p[1].body_f for p in parts]))
+    control = SapControl(joint_f=torch.cat([p[2].joint_f for p in parts]))
+    shape_offs = np.cumsum([0] + [int(m.shape_count) for m in models_])[:-1]
+    contacts = concat_contacts([p[3] for p in parts], shape_offs)
+    return model, state, control, contacts, parts

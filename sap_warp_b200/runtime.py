@@ -88,6 +88,13 @@ class SapModel:
     up_axis: int = 2
     body_label: tuple = ()
     joint_label: tuple = ()
+    # uneven batches (an extension: worlds of different sizes in one model):
+    # int32 [W+1] offsets of each world's joints, bodies, DOFs and
+    # articulations in the arrays above; None: equal per-world blocks
+    world_joint_start: torch.Tensor | None = None
+    world_body_start: torch.Tensor | None = None
+    world_dof_start: torch.Tensor | None = None
+    world_articulation_start: torch.Tensor | None = None
 
     def state(self, requires_grad: bool | None = None) -> "SapState":
         """A SapState initialised from the model's joint and body arrays."""

@@ -94,12 +94,30 @@ class _ModelView:
             model.joint_coord_count)
         if J <= 0 or D <= 0:
             raise ValueError("SolverSAP requires a model with articulated joint DOFs.")
-        if J % W or B % W or D % W or Q % W or int(model.articulation_count) % W:
-            raise ValueError("SolverSAP requires contiguous equal-sized per-world joint/body/dof/coord blocks "
-                             f"(worlds={W}, joints={J}, bodies={B}, dofs={D}, coords={Q}).")
+        self.uneven = getattr(model, "world_joint_start", None) is not None
         self.model = model
-        self.W, self.Jw, self.Bw, self.n, self.Qw = W, J // W, B // W, D // W, Q // W
-        self.Aw = int(model.articulation_count) // W
+        if self.uneven:
+            # worlds of different sizes: per-world blocks from the offsets;
+            # the *_per_world sizes are the largest world's
+            off = {k: getattr(model, "world_" + k + "_start").cpu().numpy().astype(np.int64)
+                   for k in ("joint", "body", "dof", "articulation")}
+            for k, tot in (("joint", J), ("body", B), ("dof", D), ("articulation", int(model.articulation_count))):
+                o = off[k]
+                if len(o) != W + 1 or o[0] != 0 or o[-1] != tot or np.any(np.diff(o) < 0):
+                    raise ValueError(f"world_{k}_start must be {W + 1} nondecreasing offsets from 0 to {tot}")
+            self.world_offsets = off
+            self.dof_counts = np.diff(off["dof"]).astype(np.int32)
+            self.W, self.Jw, self.Bw = W, int(np.diff(off["joint"]).max()), int(np.diff(off["body"]).max())
+            self.n, self.Aw = int(self.dof_counts.max()), int(np.diff(off["articulation"]).max())
+            self.Qw = int(Q)  # coordinates follow joint_q_start
+        else:
+            if J % W or B % W or D % W or Q % W or int(model.articulation_count) % W:
+                raise ValueError("SolverSAP requires contiguous equal-sized per-world joint/body/dof/coord blocks "
+                                 f"(worlds={W}, joints={J}, bodies={B}, dofs={D}, coords={Q}) or the world "
+                                 "offsets of an uneven batch.")
+            self.W, self.Jw, self.Bw, self.n, self.Qw = W, J // W, B // W, D // W, Q // W
+            self.Aw = int(model.articulation_count) // W
+            self.dof_counts = None
         jt = model.joint_type.cpu().numpy()
         parent_joint = model.joint_ancestor.cpu().numpy()
         if np.any(parent_joint >= np.arange(J)):
@@ -109,7 +127,7 @@ class _ModelView:
         # tree-blocked layout; by default those beyond the dense solve's 60
         # DOFs do
         jp = model.joint_parent.cpu().numpy()
-        self.free_bodies = bool(self.Jw == self.Bw and self.n == 6 * self.Bw and self.Bw <= 64
+        self.free_bodies = bool(not self.uneven and self.Jw == self.Bw and self.n == 6 * self.Bw and self.Bw <= 64
                                 and np.all(jt == SAP_JOINT_FREE) and np.all(jp < 0))
         self.tree_blocked = self.free_bodies and self.n > 60
         d = _abi.ModelDesc()
@@ -123,6 +141,9 @@ class _ModelView:
             self._keep[name] = t
             return t.data_ptr()
 
+        def k_(name, t):
+            return k(name, t, I32)
+
         for name in ("joint_type", "joint_parent", "joint_child", "joint_ancestor", "joint_q_start",
                      "joint_qd_start", "articulation_start"):
             setattr(d, name, k(name, getattr(model, name), I32))
@@ -135,6 +156,15 @@ class _ModelView:
             for name in ("shape_material_mu", "shape_material_ke", "shape_material_tau"):
                 t = getattr(model, name)
                 setattr(d, name, k(name, t, F64) if t is not None else 0)
+        if self.uneven:
+            for kind in ("joint", "body", "dof", "articulation"):
+                setattr(d, f"world_{kind}_start", k_(f"world_{kind}_start", getattr(model, f"world_{kind}_start")))
+            d.body_world = k_("body_world", model.body_world)
+            d.total_joints, d.total_bodies, d.total_dofs = J, B, D
+            d.total_articulations = int(model.articulation_count)
+            self.dof_count_t = torch.as_tensor(self.dof_counts, dtype=I32, device=self.device)
+        else:
+            self.dof_count_t = None
         self.desc = d
         self._build_dof_maps(jt)
 
@@ -178,8 +208,12 @@ class _ModelView:
             for j in js:
                 b = int(child[j])
                 if 0 <= b < B:
-                    env = b // self.Bw
-                    bstart[b] = s0 - env * self.n
+                    if self.uneven:
+                        env = int(np.searchsorted(self.world_offsets["body"], b, side="right") - 1)
+                        bstart[b] = s0 - int(self.world_offsets["dof"][env])
+                    else:
+                        env = b // self.Bw
+                        bstart[b] = s0 - env * self.n
                     bcount[b] = tot
         dev = self.device
         self.dof_coord_index = torch.as_tensor(coord, device=dev)
@@ -334,7 +368,9 @@ class SapContactJacobian:
         self.contact_env_point = z(W, C, 3)
         self.contact_env_R_WC = z(W, C, 3, 3)
         self.truncated = z(1, dt=I32)
-        self.body_q_sap = z(v.W * v.Bw, 7)
+        self.body_q_sap = z(int(model.body_count), 7)
+        # uneven batches: the start-of-step velocities in the solve's slots
+        self.qd_slots = z(W * n) if v.uneven else None
         self.dynamics_factor_env = None  # allocated by keep_dynamics_factor()
         self.dt_world = z(W)
         ws = int(load().sapb_prepare_workspace_size(ctypes.byref(v.desc), C))
@@ -349,6 +385,7 @@ class SapContactJacobian:
         o.point, o.frame = _ptr(self.contact_env_point), _ptr(self.contact_env_R_WC)
         o.truncated_count, o.body_q = _ptr(self.truncated), _ptr(self.body_q_sap)
         o.tree_mass, o.contact_tree = _ptr(self.tree_mass_env), _ptr(self.contact_env_tree)
+        o.qd_slots = _ptr(self.qd_slots)
         self.outputs = o
 
     def keep_dynamics_factor(self) -> None:
@@ -692,6 +729,7 @@ class SapContactSolve:
         r = contact_result
         P.contact_count, P.dynamics_matrix = _ptr(r.contact_env_count), _ptr(r.dynamics_matrix_env)
         P.world_order = _ptr(_checked_order(world_order, W))
+        P.dof_count = _ptr(v.dof_count_t)  # uneven batches: each world's own DOF count
         P.jacobian, P.phi0, P.w_eff = _ptr(r.contact_env_jacobian), _ptr(r.contact_env_phi0), _ptr(r.contact_env_w_eff)
         P.mu, P.stiffness, P.tau_d = _ptr(r.contact_env_mu), _ptr(r.contact_env_stiffness), _ptr(r.contact_env_tau_d)
         P.body0, P.body1 = _ptr(r.contact_env_body0), _ptr(r.contact_env_body1)
@@ -944,6 +982,11 @@ class SolverSAP:
         if self.contact_solve.tree_blocked and self.warm_start == "learned":
             raise NotImplementedError("the tree-blocked layout takes the previous-velocity or previous-impulses "
                                       "warm start")
+        if view.uneven:
+            if self.warm_start == "learned":
+                raise NotImplementedError("uneven batches take the previous-velocity or previous-impulses warm start")
+            if view.has_pd or view.has_limits:
+                raise NotImplementedError("uneven batches take no drive or limit terms")
         self.learned_candidates = str(learned_candidates).strip().lower().replace("-", "_")
         if self.learned_candidates not in ("new_contacts", "all_contacts"):
             raise ValueError(f"learned_candidates must be 'new_contacts' or 'all_contacts', got {learned_candidates!r}.")
@@ -1217,6 +1260,9 @@ class SolverSAP:
         else:
             iters, ls_iters = self.max_iterations, self.line_search_max_iterations
         v0 = self.contact_jacobian._qd
+        # the solve's start velocity in its own layout (uneven batches: slots
+        # of the largest world's DOF count, written by the free motion)
+        v0_solve = self.contact_jacobian.qd_slots if self.view.uneven else v0
         mark("warm_start")
         # the contact history ran inside the free-motion launch: _gamma_prev
         # holds the start impulses, _v_start the start velocity
@@ -1252,7 +1298,7 @@ class SolverSAP:
                 v_cands = self._v_start
         mark("contact_solve")
         sr = self.contact_solve.solve(
-            cr, solve_state, solve_control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0,
+            cr, solve_state, solve_control, self.contact_jacobian.dt_world, self.contact_jacobian.v_star, v0=v0_solve,
             v_guess=self.contact_solve.v_flat, v_guess_active=self._v_guess_active, gamma0=gamma0,
             v_candidates=v_cands, gamma0_base=gamma0_base,
             max_iterations=iters,
@@ -1277,7 +1323,7 @@ class SolverSAP:
         direct = lambda t, n: (t is not None and t.dtype == F64 and t.is_contiguous() and t.numel() == n)
         q_out = state_out.joint_q if (direct(state_out.joint_q, q_in.numel())
                                       and state_out.joint_q.data_ptr() != q_in.data_ptr()) else self._q_out_tmp
-        qd_out = state_out.joint_qd if direct(state_out.joint_qd, sr.v_flat.numel()) else self._qd_pub_out
+        qd_out = state_out.joint_qd if direct(state_out.joint_qd, self._qd_pub_out.numel()) else self._qd_pub_out
         T.joint_q_in, T.v_prev, T.v_new = _ptr(q_in), _ptr(v0), _ptr(sr.v_flat)
         T.dt = _ptr(self.contact_jacobian.dt_world)
         T.mode = _abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint" else _abi.SAPB_INTEGRATE_SAP_EULER
