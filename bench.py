@@ -589,6 +589,37 @@ def main():
         uneven[label] = {"value": mix.num_envs * world_size / (ms * 1e-3), "ms_per_solve": ms,
                          "all_converged": bool(mbuf.converged.all())}
 
+    # ---- the uneven batch as whole steps: one model of arm + box (13 DOF),
+    # quadruped (18) and humanoid (35) worlds, a third each (models.concat_models),
+    # stepped as one batch (CUDA graph of two steps, replayed) ----
+    per_kind = max(1, (2 * args.worlds) // 3)
+    umodel, ustate, ucontrol, ucon, _ = models.mixed_rollout_scene(per_kind, 3 + 1000 * rank, dev)
+    UW = int(umodel.world_count)
+    uneven_step = {"worlds": UW, "dofs": "13 (arm+box) / 18 / 35, each world its own count (no padding)",
+                   "contacts": "8-32 ground contacts per world", "timing": "graph of two steps, replayed"}
+    for label, prec, warm in (("plain_fp64", "fp64", "previous_velocity"),
+                              ("previous_impulses_fp32", "fp32", "previous_impulses")):
+        usolver = SolverSAP(umodel, max_rigid_contact=MAX_CONTACTS, contact_preset_variant="drake",
+                            hessian_precision=prec, warm_start=warm)
+        ua = SapState(joint_q=ustate.joint_q.clone(), joint_qd=ustate.joint_qd.clone(), body_q=ustate.body_q.clone(),
+                      body_f=ustate.body_f.clone())
+        ub = SapState(joint_q=ustate.joint_q.clone(), joint_qd=ustate.joint_qd.clone(), body_q=ustate.body_q.clone(),
+                      body_f=ustate.body_f.clone())
+        ugraph = usolver.capture_steps(ua, ub, ucontrol, ucon, DT, warmup=max((args.warmup + 1) // 2, 1))
+        barrier()
+        k_u = max(1, min(args.steps, 20) // 2)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(k_u):
+            ugraph.replay()
+        a1.record(stream)
+        barrier()
+        ms = max_over_ranks(a0.elapsed_time(a1) / (2 * k_u))
+        del ugraph
+        uneven_step[label] = {"value": UW * world_size / (ms * 1e-3), "ms_per_step": ms,
+                              "mean_newton_iterations": float(usolver.contact_solve.newton_iterations_env.double().mean()),
+                              "all_converged": bool(usolver.contact_solve.converged_env.all())}
+
     # ---- the launch-shape autotuner's view: each resident-CTA count per SM
     # timed on the snapshot and on the uneven batch (SolveAutotuner's rule) ----
     from sap_warp_b200 import _abi as _abi_mod
@@ -774,6 +805,7 @@ def main():
                                   "impulse_history": 1},
         "stage2_solve_only": snap,
         "uneven_batch_solve_only": uneven,
+        "uneven_batch_step": uneven_step,
         "box_worlds_solve_only": box_line,
         "box_worlds_step": box_step,
         "regenerated_contacts_rollout": site,
