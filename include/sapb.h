@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 14
+#define SAPB_ABI_VERSION 15
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -107,6 +107,9 @@ typedef struct sapb_solve_options {
   int32_t ldlt_block;             /* column-block width of the dense solve's LDL^T: 0 the default for the DOF
                                    * count, else one of sapb_contact_solve_ldlt_blocks (others: the default);
                                    * the width changes the factorization's rounding, not the tolerance */
+  int32_t skip_plain_start;       /* nonzero, with candidate starts: start from the best candidate without
+                                   * evaluating the plain start (v_guess or v0), which is kept only as the
+                                   * fallback when no candidate's cost is finite; 0: the plain start competes */
 } sapb_solve_options;
 
 /* Per-DOF drive and limit model (the arrays SapContactSolve.prepare reads,

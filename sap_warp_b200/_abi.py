@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 14
+SAPB_ABI_VERSION = 15
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -68,6 +68,7 @@ class SolveOptions(C.Structure):
         ("cubic_init", C.c_int32),
         ("ctas_per_sm", C.c_int32),
         ("ldlt_block", C.c_int32),
+        ("skip_plain_start", C.c_int32),
     ]
 
 

@@ -702,17 +702,22 @@ __device__ __forceinline__ void solve_world(const SolveParams& P, const Layout& 
     // A^-1 J^T gamma_c (base v* or gamma0_base), each taken on the
     // participating DOFs (v* on the others), A factored once in this
     // kernel's factor precision or read from the free motion's factor;
-    // the start with the lowest cost among the plain start and the
-    // candidates is taken.  Its evaluation seeds iteration 0 when it was
-    // the last one evaluated.
+    // the start with the lowest cost among the plain start (unless skipped)
+    // and the candidates is taken.  Its evaluation seeds iteration 0 when it
+    // was the last one evaluated.
     bool have_e4 = false;
     double e4_seed[4] = {0.0, 0.0, 0.0, 0.0};
     const int KV = P.p.v_candidates ? (P.p.v_candidate_count > 1 ? P.p.v_candidate_count : 1) : 0;
     const int KG = P.p.gamma0 ? (P.p.gamma0_count > 1 ? P.p.gamma0_count : 1) : 0;
     if ((KV > 0 || KG > 0) && count > 0) {
-      double e4p[4];
-      evaluate<NT, HT, NS>(w, P, dt, e4p);
-      double best_cost = e4p[0];
+      // the plain start competes unless the caller skips it; it stays the
+      // fallback when no candidate's cost is finite
+      double best_cost = 1.0e300;
+      if (!P.o.skip_plain_start) {
+        double e4p[4];
+        evaluate<NT, HT, NS>(w, P, dt, e4p);
+        best_cost = e4p[0];
+      }
       for (int i = tid; i < n; i += NT) w.V(V_SAVE)[i] = w.V(V_V)[i];
       bool last_is_best = false;
       auto try_start = [&](int index) {  // V(V_V) holds the candidate

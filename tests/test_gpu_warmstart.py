@@ -260,3 +260,33 @@ def test_learned_start_against_previous_impulses(cuda_device):
     assert stats["learned"][1] > 0, stats  # the network served new contacts
     assert stats["previous_impulses"][0] < 0.8 * stats["previous_velocity"][0], stats
     assert stats["learned"][0] <= 1.02 * stats["previous_impulses"][0], stats
+
+
+def test_skipping_the_plain_start_keeps_it_as_the_fallback(cuda_device, oracle):
+    """skip_plain_start: the candidate start velocity is taken without
+    evaluating the plain one; where the candidate's cost is not finite (NaN
+    here, every fourth world) the plain start is the fallback and those
+    worlds solve exactly as without candidates."""
+    prob = scenes.humanoid_contact_problem(64, seed=35)
+    sol = oracle.solve(prob, "armijo_decay")
+    g = sol["contact_gamma"][:, :prob.max_contacts] * 1.01
+    vc = _start_velocity(prob, g).reshape(64, -1)
+    vc[::4] = np.nan
+    t = problem_to_device(prob, cuda_device)
+    plain = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, cuda_device)
+    contact_solve(**t, buffers=plain, options=make_options("armijo_decay"))
+    buf = ContactSolveBuffers(prob.num_envs, prob.dof_per_env, prob.max_contacts, cuda_device)
+    opts = make_options("armijo_decay")
+    opts.skip_plain_start = 1
+    contact_solve(**t, buffers=buf, options=opts,
+                  v_candidates=torch.as_tensor(vc.reshape(-1), device=cuda_device).contiguous())
+    torch.cuda.synchronize()
+    acc = buf.warm_start_accepted.cpu().numpy()
+    assert np.all(acc[::4] == 0) and np.all(np.delete(acc, np.s_[::4]) == 1)
+    v, vp = buf.v.cpu().numpy().reshape(64, -1), plain.v.cpu().numpy().reshape(64, -1)
+    np.testing.assert_array_equal(v[::4], vp[::4])
+    assert bool(buf.converged.all())
+    # the candidate worlds start elsewhere than the oracle and stop at the
+    # same tolerance: agreement to the conditioning times that tolerance
+    err = np.abs(v - sol["v"].reshape(64, -1)).max(1) / np.abs(sol["v"].reshape(64, -1)).max(1)
+    assert err.max() <= 1e-4, err.max()
