@@ -55,8 +55,8 @@ sys.path.insert(0, ROOT)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one contact
 # solve launch of the headline arm on this workload (4096 humanoids, learned
 # start, FP32 Hessian; the fifth step after the 100-step settling prefix),
-# from one ncu capture: 159.64 MB read + 5.68 MB written.
-NCU_SOLVE_TRAFFIC_BYTES = 165_321_984
+# from one ncu capture: 159.75 MB read + 6.61 MB written.
+NCU_SOLVE_TRAFFIC_BYTES = 166_363_136
 
 METRIC = "world-steps/s, 4096 humanoids: learned+FP32 vs plain FP64, same B200, same tol"
 WORLDS = 4096
