@@ -707,6 +707,61 @@ def main():
                           "mean_newton_iterations": float(torch.stack(its).double().sum()) / (512 * k_bs),
                           "candidate_taken": float(torch.stack(acc).double().sum()) / (512 * k_bs),
                           "all_converged": bool(bsolver.contact_solve.converged_env.all())}
+    # ---- worlds of a 7-revolute arm gripping one of its free boxes (trees of
+    # 7 and 6 DOFs, tree-blocked in blocks of 7): the dense and the
+    # tree-blocked step on 2048 worlds of the arm and 8 boxes (55 DOFs: both
+    # layouts apply), and the tree-blocked step on 512 worlds of the arm and
+    # 32 boxes (199 DOFs: beyond the dense kernel)
+    def time_steps(solver, st0, ctl, con, worlds, k):
+        sa = SapState(joint_q=st0.joint_q.clone(), joint_qd=st0.joint_qd.clone(), body_q=st0.body_q.clone(),
+                      body_f=st0.body_f.clone())
+        sb = SapState(joint_q=st0.joint_q.clone(), joint_qd=st0.joint_qd.clone(), body_q=st0.body_q.clone(),
+                      body_f=st0.body_f.clone())
+        for _ in range(2):
+            solver.step(sa, sb, ctl, con, DT)
+            sa, sb = sb, sa
+        barrier()
+        its = []
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(k):
+            solver.step(sa, sb, ctl, con, DT)
+            its.append(solver.contact_solve.newton_iterations_env.sum())
+            sa, sb = sb, sa
+        a1.record(stream)
+        barrier()
+        ms = max_over_ranks(a0.elapsed_time(a1) / k)
+        return {"value": worlds * world_size / (ms * 1e-3), "ms_per_step": ms,
+                "mean_newton_iterations": float(torch.stack(its).double().sum()) / (worlds * k),
+                "all_converged": bool(solver.contact_solve.converged_env.all())}
+
+    k_arm = max(1, min(args.steps, 10))
+    arm_step = {"trees": "a 7-revolute fixed-base arm (7 DOFs) and free boxes (6 DOFs each), tree-blocked in "
+                         "blocks of 7; the arm's last link grips one box (2-8 contacts coupling the two trees)"}
+    amodel, astate, acontrol, acon, _, _ = models.box_scene(2048, 77 + 1000 * rank, dev, boxes=8, sites=(3, 5),
+                                                            arm=True)
+    arm_step["arm_8_boxes"] = {"worlds": 2048, "dofs": 55,
+                               "contacts": f"{int(acon.rigid_contact_count.item())} in all"}
+    for label, blocked, prec, warm in (("dense_fp64_previous_velocity", False, "fp64", "previous_velocity"),
+                                       ("blocked_fp64_previous_velocity", True, "fp64", "previous_velocity"),
+                                       ("dense_fp32_previous_impulses", False, "fp32", "previous_impulses"),
+                                       ("blocked_fp32_previous_impulses", True, "fp32", "previous_impulses")):
+        asolver = SolverSAP(amodel, max_rigid_contact=112, contact_preset_variant="drake", hessian_precision=prec,
+                            warm_start=warm, tree_blocked=blocked)
+        arm_step["arm_8_boxes"][label] = time_steps(asolver, astate, acontrol, acon, 2048, k_arm)
+        del asolver
+    amodel, astate, acontrol, acon, _, _ = models.box_scene(512, 78 + 1000 * rank, dev, boxes=32, sites=(8, 12),
+                                                            arm=True)
+    arm_step["arm_32_boxes"] = {"worlds": 512, "dofs": 199,
+                                "contacts": f"{int(acon.rigid_contact_count.item())} in all"}
+    for label, prec, warm in (("blocked_fp64_previous_velocity", "fp64", "previous_velocity"),
+                              ("blocked_fp32_previous_impulses", "fp32", "previous_impulses")):
+        asolver = SolverSAP(amodel, max_rigid_contact=384, contact_preset_variant="drake", hessian_precision=prec,
+                            warm_start=warm)
+        arm_step["arm_32_boxes"][label] = time_steps(asolver, astate, acontrol, acon, 512, k_arm)
+        del asolver
+    del amodel, astate, acontrol, acon
+
     # ---- contact generation for the same worlds' shapes (64 boxes each + a
     # ground plane): forward kinematics, count, scan, write ----
     from sap_warp_b200.collision import ContactGenerator
@@ -808,6 +863,7 @@ def main():
         "uneven_batch_step": uneven_step,
         "box_worlds_solve_only": box_line,
         "box_worlds_step": box_step,
+        "arm_box_worlds_step": arm_step,
         "regenerated_contacts_rollout": site,
         "contact_generation": contact_gen,
         "autotune_launch_shape": tuned,

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 15
+#define SAPB_ABI_VERSION 16
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -302,19 +302,26 @@ typedef struct sapb_prepare_options {
   double fallback_mu;
   double fallback_stiffness;
   double fallback_tau_d;
-  /* Nonzero: tree-blocked outputs for worlds whose every body is a free body
-   * (a free joint to the world: one tree of 6 DOFs per body, DOF order body
-   * by body).  tree_mass and contact_tree are written, jacobian is
-   * [W][C][3][12] in the layout of sapb_blocked_problem, and
-   * dynamics_matrix / dynamics_factor are not written (may be NULL).  No
-   * counterpart in the reference, which keeps such worlds dense
-   * (sim/contact_jacobian.py:110-150, 404-562).  At most 64 bodies. */
+  /* Nonzero: tree-blocked outputs.  The trees are the world's articulations
+   * (a free body is one tree of 6 DOFs; an arm another), each holding at
+   * most tree_dofs DOFs, contiguous in the world's DOF order.  tree_mass
+   * [W][T][NB][NB] (T articulations per world, NB = tree_dofs: a tree's
+   * block of A, padded with the identity beyond its own DOFs) and
+   * contact_tree are written, jacobian is [W][C][3][2 NB] in the layout of
+   * sapb_blocked_problem (zero in padded columns), and dynamics_matrix /
+   * dynamics_factor are not written (may be NULL).  A world with a tree of
+   * more than tree_dofs DOFs gets NaN in v_star, so the solve reports it
+   * SAPB_WORLD_NOT_FINITE.  No counterpart in the reference, which keeps
+   * every world dense: A_env with the zero blocks between trees and rows
+   * over all DOFs (sim/contact_jacobian.py:110-150, 404-562).  At most 64
+   * bodies per world. */
   int32_t tree_blocked;
   /* Nonzero (with a history whose has_history marks new contacts): write
    * dynamics_factor only for worlds with a new contact in a live slot, the
    * only worlds whose network-predicted impulses need it; other worlds'
    * factors are left unwritten. */
   int32_t factor_new_contacts_only;
+  int32_t tree_dofs;                /* NB of the tree-blocked outputs (0: 6, worlds of free bodies) */
 } sapb_prepare_options;
 
 /* Outputs: SapFreeMotionResult (sim/free_motion.py:63-68) and the
@@ -343,7 +350,7 @@ typedef struct sapb_prepare_outputs {
   double* dynamics_factor;          /* [W][n][n] LDL^T of A (below the diagonal L_ik d_k, on it d_k;
                                        above it unspecified), or NULL */
   double* vc_star;                  /* [W][C][3] free-motion contact velocities J_c v*, or NULL */
-  double* tree_mass;                /* [W][B][6][6] diagonal blocks of A (tree_blocked only) */
+  double* tree_mass;                /* [W][T][NB][NB] diagonal blocks of A (tree_blocked only) */
   int32_t* contact_tree;            /* [W][C][2] tree of each contact side, -1 static (tree_blocked only) */
   int32_t* contact_source;          /* [W][C] flat contact index of each slot, -1 past the world's count, or NULL */
   /* The contact history (sapb_contact_history_update), run by this launch
@@ -666,18 +673,23 @@ int32_t sapb_contact_solve_noalloc(const sapb_contact_problem* problem, const sa
 
 /* ---- worlds of many small trees ---------------------------------------------
  * The stage-2 problem in a tree-blocked layout, for worlds made of up to 64
- * trees of tree_dofs DOFs each (for example 64 free bodies: 384 DOFs).  The
- * reference keeps such worlds dense: A_env with its zero blocks between trees
+ * trees of at most tree_dofs DOFs each (for example 64 free bodies: 384
+ * DOFs; or a 7-DOF arm among free boxes).  The reference keeps such worlds
+ * dense: A_env with its zero blocks between trees
  * (sim/contact_jacobian.py:110-150) and J rows over all n DOFs (:404-562).
  * Here A is its diagonal tree blocks and each contact row holds the columns
- * of the (at most two) trees the contact touches.  World DOF order is tree
- * by tree: DOF t * tree_dofs + a is DOF a of tree t.  A contact whose two
- * sides lie on one tree is given as one side with the summed columns.  No
- * PD or limit terms (free bodies have none). */
+ * of the (at most two) trees the contact touches.  Trees are contiguous in
+ * the world's DOF order: tree t holds DOFs tree_dof_start[t] ..
+ * tree_dof_start[t+1]-1 (NULL: DOFs t * tree_dofs .. , every tree full).
+ * A tree's block and row columns are NB = tree_dofs wide; a tree with fewer
+ * DOFs is padded with the identity in its block and zero columns, padding
+ * the solve keeps to itself (the per-DOF vectors are the world's own DOFs).
+ * A contact whose two sides lie on one tree is given as one side with the
+ * summed columns.  No PD or limit terms. */
 typedef struct sapb_blocked_problem {
   int32_t num_envs;
   int32_t trees_per_env;          /* T <= 64 */
-  int32_t tree_dofs;              /* NB: 6 (a free body) */
+  int32_t tree_dofs;              /* NB: a block size sapb_blocked_tree_block returns (6: a free body) */
   int32_t max_contacts;           /* C: per-world slot capacity */
   const int32_t* contact_count;   /* [E] contacts per world (clamped to C) */
   const double* tree_mass;        /* [E,T,NB,NB] diagonal blocks of A */
@@ -688,7 +700,7 @@ typedef struct sapb_blocked_problem {
   const double* mu;               /* [E,C] */
   const double* stiffness;        /* [E,C] */
   const double* tau_d;            /* [E,C] or NULL -> options.contact_tau_d */
-  const double* v_star;           /* [E*n] free-motion velocity */
+  const double* v_star;           /* [E*n] free-motion velocity (n = dofs_per_world) */
   const double* v0;               /* [E*n] start-of-step velocity */
   double* v_guess;                /* [E*n] warm start in / seeded velocity out, or NULL */
   const int32_t* v_guess_active;  /* [1] nonzero: start from v_guess; NULL: never */
@@ -701,10 +713,19 @@ typedef struct sapb_blocked_problem {
    * v0); warm_start_accepted reports 1 then.  gamma0_count must be <= 1. */
   const double* gamma0;
   int32_t gamma0_count;
+  /* Trees of different sizes: [T+1] first DOF of each tree in the world
+   * (device, the same for every world; increasing, each tree at most
+   * tree_dofs DOFs, tree_dof_start[T] = dofs_per_world), or NULL. */
+  const int32_t* tree_dof_start;
+  int32_t dofs_per_world;         /* n; 0: T * tree_dofs */
 } sapb_blocked_problem;
 
+/* The block size NB the blocked solve is built with for trees of up to
+ * tree_dofs DOFs: the smallest of 6, 7 and 12 that holds them (0: none). */
+int32_t sapb_blocked_tree_block(int32_t tree_dofs);
+
 /* Off-diagonal factor blocks one world of this shape can hold on chip
- * (0: the shape does not fit or tree_dofs != 6).  A world whose
+ * (0: the shape does not fit or tree_dofs is not a built block size).  A world whose
  * elimination (rounds of independent minimum-degree trees, with fill) needs
  * more gets the per-world status SAPB_WORLD_FACTOR_CAPACITY. */
 int32_t sapb_blocked_fill_capacity(int32_t trees_per_env, int32_t tree_dofs, int32_t max_contacts,
@@ -723,12 +744,15 @@ int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* problem, const sa
                                    const sapb_solve_outputs* out, void* workspace, size_t workspace_bytes,
                                    void* stream);
 
-/* Gather a dense problem whose worlds are trees_per_env trees of tree_dofs
- * DOFs (body_dof_start of a body = its tree's first DOF) into the blocked
- * layout: tree_mass [E,T,NB,NB], jacobian [E,C,3,2NB], contact_tree [E,C,2]
- * (device pointers).  The other blocked fields alias the dense ones. */
+/* Gather a dense problem whose worlds are trees_per_env trees into the
+ * blocked layout: tree_mass [E,T,NB,NB], jacobian [E,C,3,2NB], contact_tree
+ * [E,C,2] (device pointers).  tree_dof_start (device [T+1], or NULL: trees of
+ * tree_dofs DOFs each) as in sapb_blocked_problem; a body's tree is the one
+ * holding body_dof_start of the body.  The other blocked fields alias the
+ * dense ones. */
 int32_t sapb_dense_to_blocked(const sapb_contact_problem* dense, int32_t trees_per_env, int32_t tree_dofs,
-                              double* tree_mass, double* jacobian, int32_t* contact_tree, void* stream);
+                              const int32_t* tree_dof_start, double* tree_mass, double* jacobian,
+                              int32_t* contact_tree, void* stream);
 
 /* Last CUDA error string seen by the library on this thread ("" if none). */
 const char* sapb_last_error(void);

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 15
+SAPB_ABI_VERSION = 16
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -153,6 +153,8 @@ class BlockedProblem(C.Structure):
         ("world_order", _p),
         ("gamma0", _p),
         ("gamma0_count", C.c_int32),
+        ("tree_dof_start", _p),
+        ("dofs_per_world", C.c_int32),
     ]
 
 
@@ -280,6 +282,7 @@ class PrepareOptions(C.Structure):
         ("fallback_tau_d", C.c_double),
         ("tree_blocked", C.c_int32),
         ("factor_new_contacts_only", C.c_int32),
+        ("tree_dofs", C.c_int32),
     ]
 
 
@@ -399,7 +402,8 @@ EXPORTS = {
         C.c_int32,
         [C.POINTER(BlockedProblem), C.POINTER(SolveOptions), C.POINTER(SolveOutputs), _p, C.c_size_t, _p],
     ),
-    "sapb_dense_to_blocked": (C.c_int32, [C.POINTER(ContactProblem), C.c_int32, C.c_int32, _p, _p, _p, _p]),
+    "sapb_dense_to_blocked": (C.c_int32, [C.POINTER(ContactProblem), C.c_int32, C.c_int32, _p, _p, _p, _p, _p]),
+    "sapb_blocked_tree_block": (C.c_int32, [C.c_int32]),
     "sapb_prepare_workspace_size": (C.c_size_t, [C.POINTER(ModelDesc), C.c_int32]),
     "sapb_free_motion_contacts": (
         C.c_int32,

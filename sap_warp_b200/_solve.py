@@ -272,19 +272,26 @@ def blocked_contact_solve(
     v_guess_active: torch.Tensor | None = None,
     world_order: torch.Tensor | None = None,
     gamma0: torch.Tensor | None = None,
+    tree_dof_start: torch.Tensor | None = None,
 ) -> ContactSolveBuffers:
     """Launch the tree-blocked solve (sapb_blocked_contact_solve) for worlds of
-    `trees_per_env` trees of `tree_dofs` DOFs; results land in `buffers`
-    (dof_per_env = trees_per_env * tree_dofs), no host sync.  gamma0 (E, C, 3):
-    starting impulses of a candidate start v* + A^-1 J^T gamma0."""
+    `trees_per_env` trees in blocks of `tree_dofs` DOFs; results land in
+    `buffers` (dof_per_env = trees_per_env * tree_dofs, or the last entry of
+    tree_dof_start, int32 [T+1], for trees of different sizes), no host
+    sync.  gamma0 (E, C, 3): starting impulses of a candidate start
+    v* + A^-1 J^T gamma0."""
     lib = load()
     b = buffers
     E, C, T, NB = b.num_envs, b.max_contacts, trees_per_env, tree_dofs
-    if T * NB != b.dof_per_env:
+    if tree_dof_start is None and T * NB != b.dof_per_env:
         raise ValueError(f"buffers hold {b.dof_per_env} DOFs per world, not {T} trees x {NB}")
-    n = T * NB
+    if tree_dof_start is not None and b.dof_per_env > T * NB:
+        raise ValueError(f"{T} trees of at most {NB} DOFs cannot hold {b.dof_per_env} DOFs per world")
+    n = b.dof_per_env
     P = _abi.BlockedProblem()
     P.num_envs, P.trees_per_env, P.tree_dofs, P.max_contacts = E, T, NB, C
+    P.tree_dof_start = _ptr(tree_dof_start, I32, T + 1, "tree_dof_start")
+    P.dofs_per_world = n
     P.contact_count = _ptr(contact_count, I32, E, "contact_count")
     P.tree_mass = _ptr(tree_mass, F64, E * T * NB * NB, "tree_mass")
     P.jacobian = _ptr(jacobian, F64, E * C * 3 * 2 * NB, "jacobian")
@@ -329,9 +336,11 @@ def blocked_fill_capacity(trees_per_env: int, tree_dofs: int, max_contacts: int,
 
 
 def dense_to_blocked(arrays: dict, num_envs: int, dof_per_env: int, max_contacts: int, trees_per_env: int,
-                     tree_dofs: int = 6, stream: torch.cuda.Stream | None = None) -> dict:
+                     tree_dofs: int = 6, stream: torch.cuda.Stream | None = None,
+                     tree_dof_start: torch.Tensor | None = None) -> dict:
     """Blocked tensors (tree_mass, jacobian, contact_tree) gathered on the
-    device from the dense problem tensors of `build_problem`."""
+    device from the dense problem tensors of `build_problem`; tree_dof_start
+    (int32 [T+1]) for trees of different sizes, each at most tree_dofs."""
     lib = load()
     E, C, T, NB = num_envs, max_contacts, trees_per_env, tree_dofs
     dev = arrays["dynamics_matrix"].device
@@ -340,7 +349,8 @@ def dense_to_blocked(arrays: dict, num_envs: int, dof_per_env: int, max_contacts
     jac = torch.empty(E, C, 3, 2 * NB, dtype=F64, device=dev)
     ct = torch.empty(E, C, 2, dtype=I32, device=dev)
     s = stream if stream is not None else torch.cuda.current_stream(dev)
-    status = lib.sapb_dense_to_blocked(ctypes.byref(P), T, NB, tm.data_ptr(), jac.data_ptr(), ct.data_ptr(),
+    tds = _ptr(tree_dof_start, I32, T + 1, "tree_dof_start")
+    status = lib.sapb_dense_to_blocked(ctypes.byref(P), T, NB, tds, tm.data_ptr(), jac.data_ptr(), ct.data_ptr(),
                                        ctypes.c_void_p(s.cuda_stream))
     check(status, "sapb_dense_to_blocked")
     return dict(tree_mass=tm, jacobian=jac, contact_tree=ct)

@@ -24,6 +24,13 @@
 //    lists), forward / backward block solves the same way.
 // Precision as in the dense kernel: gradient, costs, line search, update and
 // convergence test in FP64; H and its factor in HT (double or float).
+//
+// Trees of different sizes (an arm among free bodies) share one block size
+// NB: a tree of fewer DOFs is padded with the identity in its block of A and
+// zero columns in the rows, so its padded velocities stay at zero through
+// the Newton loop (zero gradient, identity Hessian there); the per-DOF
+// vectors in global memory are the world's own DOFs, mapped at load and
+// store.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -48,6 +55,7 @@ struct BlockedParams {
   int32_t use_guess_flag_ptr_valid;
   int32_t* queue;
   int32_t capacity;  // off-diagonal factor blocks one world may hold
+  int32_t nd;        // DOFs of a world in the global per-DOF vectors
 };
 
 // The per-DOF vectors the blocked kernel keeps, mapped from the V_* slots the
@@ -736,11 +744,38 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[8 * (NT / 32)];
   __shared__ int s_next;
+  __shared__ int s_tstart[kBMaxTrees], s_tcount[kBMaxTrees];
+  __shared__ int s_bad_layout;
   const int tid = threadIdx.x;
   const int T = P.p.trees_per_env, C = P.p.max_contacts;
   const int n = T * NB;
   const BLayout L = make_blayout(T, NB, C, (int)sizeof(HT), P.capacity);
   const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
+
+  // tree t's DOFs in the global vectors: s_tstart[t] .. + s_tcount[t]; an
+  // invalid map (decreasing, a tree above NB, beyond the world) leaves its
+  // trees empty and every world NOT_FINITE
+  if (tid == 0) s_bad_layout = 0;
+  __syncthreads();
+  for (int t = tid; t < T; t += NT) {
+    int st = t * NB, cnt = NB;
+    if (P.p.tree_dof_start) {
+      st = P.p.tree_dof_start[t];
+      cnt = P.p.tree_dof_start[t + 1] - st;
+    }
+    if (st < 0 || cnt < 0 || cnt > NB || st + cnt > P.nd) {
+      s_bad_layout = 1;
+      st = 0;
+      cnt = 0;
+    }
+    s_tstart[t] = st;
+    s_tcount[t] = cnt;
+  }
+  __syncthreads();
+  auto gidx = [&](int i) {
+    const int t = i / NB, a = i - t * NB;
+    return a < s_tcount[t] ? s_tstart[t] + a : -1;
+  };
 
   if (tid == 0) s_next = atomicAdd(P.queue, 1);
   for (;;) {
@@ -782,7 +817,7 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
     if (count < 0) count = 0;
     w.count = count;
     const double dt = P.p.dt[e];
-    const size_t base = (size_t)e * n;
+    const size_t base = (size_t)e * P.nd;
     int8_t* tree_w = reinterpret_cast<int8_t*>(smem + L.off_tree);
     uint16_t* list_w = reinterpret_cast<uint16_t*>(smem + L.off_list);
 
@@ -810,21 +845,33 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
     if constexpr (sizeof(HT) == 4) {
       for (int k = tid; k < count * 6 * NB; k += NT) w.JA[k] = (float)__ldg(w.J + k);
     }
+    bool bad = s_bad_layout != 0;  // NaN / Inf in the world's inputs
     for (int i = tid; i < n; i += NT) {
-      w.V(V_VSTAR)[i] = P.p.v_star[base + i];
-      double v = P.p.v0[base + i];
-      if (P.p.v_guess) {
-        if (use_guess) v = P.p.v_guess[base + i];
-        P.p.v_guess[base + i] = v;
+      const int gi = gidx(i);
+      double vs = 0.0, v = 0.0;  // padded DOFs: zero
+      if (gi >= 0) {
+        vs = P.p.v_star[base + gi];
+        v = P.p.v0[base + gi];
+        if (P.p.v_guess) {
+          if (use_guess) v = P.p.v_guess[base + gi];
+          P.p.v_guess[base + gi] = v;
+        }
       }
+      w.V(V_VSTAR)[i] = vs;
       w.V(V_V)[i] = v;
+      bad = bad || !isfinite(vs) || !isfinite(v);
       const int t = i / NB, a = i - t * NB;
-      double d = __ldg(w.A + ((size_t)t * NB + a) * NB + a);
+      const double* Ar = w.A + ((size_t)t * NB + a) * NB;
+      for (int b = 0; b < NB; ++b) bad = bad || !isfinite(__ldg(Ar + b));
+      double d = __ldg(Ar + a);
       if (d < 1.0e-12 || !isfinite(d)) d = 1.0e-12;
       w.V(V_DSCALE)[i] = 1.0 / sqrt(d);
       w.flags[i] = 0;
     }
-    __syncthreads();
+    for (int k = tid; k < count * 6 * NB; k += NT) bad = bad || !isfinite(__ldg(w.J + k));
+    for (int c = tid; c < count; c += NT)  // the contact constants formed above
+      for (int q = C_RT; q < C_VC; ++q) bad = bad || !isfinite(w.Cn(q)[c]);
+    bad = __syncthreads_or(bad) != 0;
     for (int c = tid; c < count; c += NT) {
       const int t0 = tree_w[2 * c], t1 = tree_w[2 * c + 1];
       if (t0 >= 0 && t1 >= 0) {
@@ -863,7 +910,9 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
     int newton_iterations = 0, ls_total = 0, converged = 0, status = 0, accepted = 0;
     double cost = 0.0, previous_cost = 0.0, alpha = 1.0, grad_norm = 0.0;
     bool evaluated = false;
-    if (!fits) {
+    if (bad) {
+      status = SAPB_WORLD_NOT_FINITE;  // not solved: v = the start velocity
+    } else if (!fits) {
       status = SAPB_WORLD_FACTOR_CAPACITY;
       for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
@@ -1002,7 +1051,10 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
       }
     }
     // ---- outputs ------------------------------------------------------------
-    for (int i = tid; i < n; i += NT) P.out.v[base + i] = w.V(V_V)[i];
+    for (int i = tid; i < n; i += NT) {
+      const int gi = gidx(i);
+      if (gi >= 0) P.out.v[base + gi] = w.V(V_V)[i];
+    }
     for (int c = tid; c < C; c += NT) {
       const size_t ci = (size_t)e * C + c;
       const bool live = evaluated && c < count;
@@ -1082,8 +1134,16 @@ cudaError_t launch_blocked(const BlockedParams& P, cudaStream_t stream) {
 
 }  // namespace
 
+int32_t blocked_tree_block(int tree_dofs) {
+  if (tree_dofs < 0) return 0;
+  if (tree_dofs <= 6) return 6;
+  if (tree_dofs <= 7) return 7;
+  if (tree_dofs <= 12) return 12;
+  return 0;
+}
+
 int32_t blocked_fill_capacity(int T, int NB, int C, bool fp32) {
-  if (NB != 6 || T < 1 || T > kBMaxTrees || C < 0) return 0;
+  if (NB < 1 || blocked_tree_block(NB) != NB || T < 1 || T > kBMaxTrees || C < 0) return 0;
   return fp32 ? blocked_capacity<float>(T, NB, C) : blocked_capacity<double>(T, NB, C);
 }
 
@@ -1096,6 +1156,7 @@ int32_t blocked_solve_launch(const sapb_blocked_problem* p, const sapb_solve_opt
   P.out = *out;
   P.use_guess_flag_ptr_valid = (p->v_guess && p->v_guess_active) ? 1 : 0;
   P.queue = reinterpret_cast<int32_t*>(workspace);
+  P.nd = p->dofs_per_world > 0 ? p->dofs_per_world : p->trees_per_env * p->tree_dofs;
   if (p->num_envs == 0) return SAPB_OK;
   const bool fp32 = o->hessian_precision == SAPB_FP32 || o->linear_solve_precision == SAPB_FP32;
   P.capacity = blocked_fill_capacity(p->trees_per_env, p->tree_dofs, p->max_contacts, fp32);
@@ -1104,7 +1165,18 @@ int32_t blocked_solve_launch(const sapb_blocked_problem* p, const sapb_solve_opt
                    p->trees_per_env, p->max_contacts);
     return SAPB_ERR_UNSUPPORTED;
   }
-  const cudaError_t err = fp32 ? launch_blocked<float, 6>(P, stream) : launch_blocked<double, 6>(P, stream);
+  cudaError_t err;
+  switch (p->tree_dofs) {
+    case 6:
+      err = fp32 ? launch_blocked<float, 6>(P, stream) : launch_blocked<double, 6>(P, stream);
+      break;
+    case 7:
+      err = fp32 ? launch_blocked<float, 7>(P, stream) : launch_blocked<double, 7>(P, stream);
+      break;
+    default:
+      err = fp32 ? launch_blocked<float, 12>(P, stream) : launch_blocked<double, 12>(P, stream);
+      break;
+  }
   if (err != cudaSuccess) {
     set_last_error("blocked contact solve launch: %s", cudaGetErrorString(err));
     return SAPB_ERR_CUDA;
@@ -1114,44 +1186,58 @@ int32_t blocked_solve_launch(const sapb_blocked_problem* p, const sapb_solve_opt
 
 // ---- dense -> blocked gather -------------------------------------------------
 
-__global__ void dense_to_blocked_kernel(sapb_contact_problem d, int T, int NB, double* tree_mass, double* jac,
-                                        int32_t* contact_tree) {
+// The tree holding world DOF s (-1: none): tree t holds tds[t] .. tds[t+1]-1,
+// or t * NB .. with tds NULL.
+__device__ inline int tree_of_dof(const int32_t* tds, int T, int NB, int s) {
+  if (s < 0) return -1;
+  if (!tds) return s / NB < T ? s / NB : -1;
+  for (int t = 0; t < T; ++t)
+    if (s >= tds[t] && s < tds[t + 1]) return t;
+  return -1;
+}
+
+__global__ void dense_to_blocked_kernel(sapb_contact_problem d, int T, int NB, const int32_t* tds,
+                                        double* tree_mass, double* jac, int32_t* contact_tree) {
   const int n = d.dof_per_env, C = d.max_contacts;
   const size_t E = (size_t)d.num_envs;
   const size_t nA = E * T * NB * NB, nJ = E * C * 3 * 2 * NB, nT = E * C;
   const size_t total = nA + nJ + nT;
+  auto tstart = [&](int t) { return tds ? tds[t] : t * NB; };
+  auto tcount = [&](int t) {  // clamped to NB and to the world's DOFs
+    const int s0 = tstart(t);
+    int c = tds ? tds[t + 1] - s0 : NB;
+    if (c > NB) c = NB;
+    if (s0 < 0 || c < 0) return 0;
+    return s0 + c > n ? (n > s0 ? n - s0 : 0) : c;
+  };
+  auto body_tree = [&](const int* bodies, size_t ec) {
+    if (!bodies || bodies[ec] < 0 || bodies[ec] >= d.num_bodies) return -1;
+    return tree_of_dof(tds, T, NB, d.body_dof_start[bodies[ec]]);
+  };
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
     if (k < nA) {
       const size_t e = k / ((size_t)T * NB * NB);
       const int r = (int)(k - e * T * NB * NB);
       const int t = r / (NB * NB), a = (r / NB) % NB, b = r % NB;
-      tree_mass[k] = d.dynamics_matrix[(e * n + t * NB + a) * n + t * NB + b];
+      const int s0 = tstart(t), nt = tcount(t);
+      // a tree's own block, the identity in its padding
+      tree_mass[k] = (a < nt && b < nt) ? d.dynamics_matrix[(e * n + s0 + a) * n + s0 + b] : (a == b ? 1.0 : 0.0);
     } else if (k < nA + nJ) {
       const size_t q = k - nA;
       const size_t row = q / (2 * NB);  // (e, c, r)
       const int col = (int)(q - row * 2 * NB);
       const size_t ec = row / 3;
       const int side = col / NB, a = col % NB;
-      const int* bodies = side == 0 ? d.body0 : d.body1;
-      const int* other = side == 0 ? d.body1 : d.body0;
-      int tt = -1, to = -1;
-      if (bodies && bodies[ec] >= 0 && bodies[ec] < d.num_bodies && d.body_dof_start[bodies[ec]] >= 0)
-        tt = d.body_dof_start[bodies[ec]] / NB;
-      if (other && other[ec] >= 0 && other[ec] < d.num_bodies && d.body_dof_start[other[ec]] >= 0)
-        to = d.body_dof_start[other[ec]] / NB;
+      const int tt = body_tree(side == 0 ? d.body0 : d.body1, ec);
+      const int to = body_tree(side == 0 ? d.body1 : d.body0, ec);
       double v = 0.0;
       // a contact whose two sides lie on one tree keeps its (summed) columns on side 0
-      if (tt >= 0 && tt < T && !(side == 1 && tt == to)) v = d.jacobian[row * n + tt * NB + a];
+      if (tt >= 0 && a < tcount(tt) && !(side == 1 && tt == to)) v = d.jacobian[row * n + tstart(tt) + a];
       jac[q] = v;
     } else {
       const size_t ec = k - nA - nJ;
-      int t0 = -1, t1 = -1;
-      if (d.body0 && d.body0[ec] >= 0 && d.body0[ec] < d.num_bodies && d.body_dof_start[d.body0[ec]] >= 0)
-        t0 = d.body_dof_start[d.body0[ec]] / NB;
-      if (d.body1 && d.body1[ec] >= 0 && d.body1[ec] < d.num_bodies && d.body_dof_start[d.body1[ec]] >= 0)
-        t1 = d.body_dof_start[d.body1[ec]] / NB;
-      if (t0 >= T) t0 = -1;
-      if (t1 >= T) t1 = -1;
+      const int t0 = body_tree(d.body0, ec);
+      int t1 = body_tree(d.body1, ec);
       if (t1 == t0) t1 = -1;
       contact_tree[2 * ec] = t0;
       contact_tree[2 * ec + 1] = t1;
@@ -1159,12 +1245,12 @@ __global__ void dense_to_blocked_kernel(sapb_contact_problem d, int T, int NB, d
   }
 }
 
-int32_t dense_to_blocked_launch(const sapb_contact_problem* d, int T, int NB, double* tree_mass, double* jac,
-                                int32_t* contact_tree, cudaStream_t stream) {
+int32_t dense_to_blocked_launch(const sapb_contact_problem* d, int T, int NB, const int32_t* tree_dof_start,
+                                double* tree_mass, double* jac, int32_t* contact_tree, cudaStream_t stream) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  dense_to_blocked_kernel<<<sms * 4, 256, 0, stream>>>(*d, T, NB, tree_mass, jac, contact_tree);
+  dense_to_blocked_kernel<<<sms * 4, 256, 0, stream>>>(*d, T, NB, tree_dof_start, tree_mass, jac, contact_tree);
   const cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) {
     set_last_error("dense to blocked gather: %s", cudaGetErrorString(err));

@@ -132,6 +132,8 @@ int32_t sapb_contact_solve(const sapb_contact_problem* p, const sapb_solve_optio
   return sapb::contact_solve_launch(p, o, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
+int32_t sapb_blocked_tree_block(int32_t tree_dofs) { return sapb::blocked_tree_block(tree_dofs); }
+
 int32_t sapb_blocked_fill_capacity(int32_t trees_per_env, int32_t tree_dofs, int32_t max_contacts,
                                    int32_t hessian_precision) {
   return sapb::blocked_fill_capacity(trees_per_env, tree_dofs, max_contacts, hessian_precision == SAPB_FP32);
@@ -156,10 +158,16 @@ int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* p, const sapb_sol
                          p->num_envs, p->trees_per_env, p->max_contacts);
     return SAPB_ERR_INVALID_ARGUMENT;
   }
-  if (p->trees_per_env > 64 || p->tree_dofs != 6) {
-    sapb::set_last_error("sapb_blocked_contact_solve: supported are <= 64 trees of 6 DOFs (got %d of %d)",
-                         p->trees_per_env, p->tree_dofs);
+  if (p->trees_per_env > 64 || p->tree_dofs < 1 || sapb::blocked_tree_block(p->tree_dofs) != p->tree_dofs) {
+    sapb::set_last_error("sapb_blocked_contact_solve: supported are <= 64 trees in blocks of 6, 7 or 12 DOFs "
+                         "(got %d trees, tree_dofs %d)", p->trees_per_env, p->tree_dofs);
     return SAPB_ERR_UNSUPPORTED;
+  }
+  if (p->dofs_per_world < 0 || p->dofs_per_world > p->trees_per_env * p->tree_dofs ||
+      (!p->tree_dof_start && p->dofs_per_world != 0 && p->dofs_per_world != p->trees_per_env * p->tree_dofs)) {
+    sapb::set_last_error("sapb_blocked_contact_solve: dofs_per_world=%d does not fit %d trees of at most %d DOFs",
+                         p->dofs_per_world, p->trees_per_env, p->tree_dofs);
+    return SAPB_ERR_INVALID_ARGUMENT;
   }
   if (p->max_contacts > 32767) {
     sapb::set_last_error("sapb_blocked_contact_solve: max_contacts=%d > 32767", p->max_contacts);
@@ -196,20 +204,22 @@ int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* p, const sapb_sol
 }
 
 int32_t sapb_dense_to_blocked(const sapb_contact_problem* d, int32_t trees_per_env, int32_t tree_dofs,
-                              double* tree_mass, double* jacobian, int32_t* contact_tree, void* stream) {
+                              const int32_t* tree_dof_start, double* tree_mass, double* jacobian,
+                              int32_t* contact_tree, void* stream) {
   if (!d || !tree_mass || !jacobian || !contact_tree || !d->dynamics_matrix || !d->body_dof_start ||
       (d->max_contacts > 0 && !d->jacobian)) {
     sapb::set_last_error("sapb_dense_to_blocked: missing array");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
-  if (trees_per_env < 1 || tree_dofs < 1 || trees_per_env * tree_dofs != d->dof_per_env || d->num_envs < 0 ||
-      d->max_contacts < 0) {
-    sapb::set_last_error("sapb_dense_to_blocked: %d trees of %d DOFs do not make dof_per_env=%d", trees_per_env,
-                         tree_dofs, d->dof_per_env);
+  const int64_t cover = (int64_t)trees_per_env * tree_dofs;
+  if (trees_per_env < 1 || trees_per_env > 64 || tree_dofs < 1 || d->num_envs < 0 || d->max_contacts < 0 ||
+      (tree_dof_start ? cover < d->dof_per_env : cover != d->dof_per_env)) {
+    sapb::set_last_error("sapb_dense_to_blocked: %d trees of %s%d DOFs do not make dof_per_env=%d", trees_per_env,
+                         tree_dof_start ? "at most " : "", tree_dofs, d->dof_per_env);
     return SAPB_ERR_INVALID_ARGUMENT;
   }
-  return sapb::dense_to_blocked_launch(d, trees_per_env, tree_dofs, tree_mass, jacobian, contact_tree,
-                                       static_cast<cudaStream_t>(stream));
+  return sapb::dense_to_blocked_launch(d, trees_per_env, tree_dofs, tree_dof_start, tree_mass, jacobian,
+                                       contact_tree, static_cast<cudaStream_t>(stream));
 }
 
 size_t sapb_prepare_workspace_size(const sapb_model_desc* m, int32_t max_contacts) {
@@ -270,11 +280,14 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inpu
     sapb::set_last_error("sapb_free_motion_contacts: tree-blocked outputs need equal per-world blocks");
     return SAPB_ERR_UNSUPPORTED;
   }
-  if (blk && (m->bodies_per_world > 64 || m->dofs_per_world != 6 * m->bodies_per_world ||
-              m->joints_per_world != m->bodies_per_world || out->dynamics_factor)) {
-    sapb::set_last_error("sapb_free_motion_contacts: tree-blocked outputs need worlds of <= 64 free bodies "
-                         "(got %d bodies, %d joints, %d DOFs) and no dynamics_factor output",
-                         m->bodies_per_world, m->joints_per_world, m->dofs_per_world);
+  const int tree_block = blk ? (o->tree_dofs > 0 ? o->tree_dofs : 6) : 0;
+  if (blk && (m->bodies_per_world > 64 || m->articulations_per_world < 1 ||
+              sapb::blocked_tree_block(tree_block) != tree_block ||
+              (int64_t)m->articulations_per_world * tree_block < m->dofs_per_world || out->dynamics_factor)) {
+    sapb::set_last_error("sapb_free_motion_contacts: tree-blocked outputs need worlds of <= 64 bodies whose "
+                         "articulations fit blocks of tree_dofs in {6, 7, 12} (got %d bodies, %d articulations, "
+                         "%d DOFs, tree_dofs %d) and no dynamics_factor output",
+                         m->bodies_per_world, m->articulations_per_world, m->dofs_per_world, tree_block);
     return SAPB_ERR_UNSUPPORTED;
   }
   if (!blk && (m->bodies_per_world > 64 || m->dofs_per_world > 128)) {
@@ -282,7 +295,7 @@ int32_t sapb_free_motion_contacts(const sapb_model_desc* m, const sapb_step_inpu
                          m->bodies_per_world, m->dofs_per_world);
     return SAPB_ERR_UNSUPPORTED;
   }
-  const size_t smem = sapb::prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, o->max_contacts, blk);
+  const size_t smem = sapb::prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, o->max_contacts, tree_block);
   if (smem > sapb::kMaxSmemPerBlock) {
     sapb::set_last_error("sapb_free_motion_contacts: world too large for one block (%zu bytes of shared memory)",
                          smem);

@@ -65,11 +65,12 @@ int ldlt_block_widths(int n, int32_t* out, int capacity);
 int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_options* o, const sapb_solve_outputs* out,
                              void* workspace, size_t workspace_bytes, cudaStream_t stream);
 
+int32_t blocked_tree_block(int tree_dofs);
 int32_t blocked_fill_capacity(int T, int NB, int C, bool fp32);
 int32_t blocked_solve_launch(const sapb_blocked_problem* p, const sapb_solve_options* o,
                              const sapb_solve_outputs* out, void* workspace, cudaStream_t stream);
-int32_t dense_to_blocked_launch(const sapb_contact_problem* d, int T, int NB, double* tree_mass, double* jac,
-                                int32_t* contact_tree, cudaStream_t stream);
+int32_t dense_to_blocked_launch(const sapb_contact_problem* d, int T, int NB, const int32_t* tree_dof_start,
+                                double* tree_mass, double* jac, int32_t* contact_tree, cudaStream_t stream);
 
 int32_t public_to_sap_launch(const sapb_model_desc* m, const double* joint_q, const double* body_q,
                              const double* qd_pub, const double* f_pub, const double* bf_pub, double* qd_sap,
@@ -83,7 +84,8 @@ size_t contacts_workspace_bytes(const sapb_collision_shapes* s);
 int32_t contacts_launch(const sapb_collision_shapes* s, const double* body_q, const sapb_contact_outputs* out,
                         void* workspace, cudaStream_t stream);
 
-size_t prepare_smem_bytes(int B, int n, int C, bool tree_blocked);
+// tree_block: 0 for the dense layout, else the block size of the tree-blocked outputs
+size_t prepare_smem_bytes(int B, int n, int C, int tree_block);
 // The contact history; rank_src non-NULL: the free-motion launch's slot
 // list, ranked in place and used as the slots' sources (sapb_history.cu).
 int32_t history_launch(const sapb_contact_history* h, int32_t* rank_src, cudaStream_t stream);

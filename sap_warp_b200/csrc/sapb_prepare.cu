@@ -49,10 +49,12 @@ __host__ __device__ inline size_t prep_align(size_t x) { return (x + 15) / 16 * 
 // add without shifts.
 struct PrepLayout {
   size_t pose, pose2, fm, vj, cb, vb, fb, ib, fs, S, F, vec, H, con, conint, anc, jmp, bj, par, dbody, tri, jg,
-      total;
+      trees, total;
 };
 
-__host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk) {
+// tb: 0 for the dense layout, else the block size of the tree-blocked outputs
+__host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, int tb) {
+  const bool blk = tb > 0;
   PrepLayout L;
   const size_t Cc = (size_t)(C > 0 ? C : 1);
   size_t o = 0;
@@ -73,7 +75,7 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk)
   L.S = take(sizeof(double) * 6 * n);       // motion subspace columns
   L.F = take(sizeof(double) * 6 * n);       // composite inertia times S
   L.vec = take(sizeof(double) * 4 * n);     // tau, vdot, diag(A), 1/d
-  L.H = take(sizeof(double) * (blk ? (size_t)36 * B : (size_t)n * n));  // A (tree blocks when blocked)
+  L.H = take(sizeof(double) * (blk ? (size_t)tb * tb * B : (size_t)n * n));  // A (tree blocks when blocked)
   L.con = take(sizeof(double) * 21 * Cc);   // per contact: x0 3, x1 3, -, -, frame 9
   L.conint = take(sizeof(int) * 2 * Cc);    // local bodies lb0, lb1
   L.anc = take(sizeof(uint64_t) * 2 * B);   // ancestor-or-self masks (two buffers; then bodies by depth)
@@ -83,6 +85,7 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, bool blk)
   L.dbody = take(sizeof(int) * n);          // body of each DOF
   L.tri = take(sizeof(uint16_t) * (blk ? 1 : (size_t)(n * (n - 1) / 2 + 1)));  // LDL^T triangle list
   L.jg = take(sizeof(double) * (blk ? 1 : (size_t)(kPrepNT / 32) * n));  // per-warp J^T gamma_start partials
+  L.trees = take(sizeof(int) * (blk ? (size_t)2 * B + 1 : 1));  // tree of each body; first DOF of each tree
   L.total = o;
   return L;
 }
@@ -212,11 +215,13 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   const int tid = threadIdx.x;
   const int e = blockIdx.x;
   const int C = P.o.max_contacts;
-  const bool blk = P.o.tree_blocked != 0;  // worlds of free bodies, tree-blocked outputs
+  const bool blk = P.o.tree_blocked != 0;  // tree-blocked outputs: the trees are the articulations
+  const int tb = blk ? (P.o.tree_dofs > 0 ? P.o.tree_dofs : 6) : 0;  // their block size
   // shared memory laid out for the largest world; this world's own block
-  const PrepLayout L = prep_layout(P.m.bodies_per_world, P.m.dofs_per_world, C, blk);
+  const PrepLayout L = prep_layout(P.m.bodies_per_world, P.m.dofs_per_world, C, tb);
   const WorldSpan ws = world_span(P.m, e);
   const int B = ws.nb, n = ws.nd, Jw = ws.nj;
+  const int ntree = blk ? (ws.na < B ? ws.na : B) : 0;
   // the solve's per-DOF arrays: slots of dofs_per_world per world (the world's
   // global DOF offset when the blocks are equal)
   const int n_slot = P.m.dofs_per_world;
@@ -248,13 +253,18 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   int* dbody = reinterpret_cast<int*>(smem + L.dbody);
   uint16_t* tri = reinterpret_cast<uint16_t*>(smem + L.tri);
   double* jg = reinterpret_cast<double*>(smem + L.jg);
+  int* btree = reinterpret_cast<int*>(smem + L.trees);  // [B] tree of a body, -1
+  int* tds = btree + B;                                  // [ntree + 1] first DOF of each tree
   const bool want_vstart = VS && !blk && P.out.v_start && P.gamma_start;
   const int j0 = ws.j0, b0g = ws.b0, d0 = ws.d0;
   const double* q = P.in.joint_q;
   const double* qd = P.in.joint_qd;
 
   // ---- topology of this world --------------------------------------------
-  for (int b = tid; b < B; b += kPrepNT) bj[b] = -1;
+  for (int b = tid; b < B; b += kPrepNT) {
+    bj[b] = -1;
+    if (blk) btree[b] = -1;
+  }
   for (int i = tid; i < n; i += kPrepNT) dbody[i] = -1;
   if (!blk) build_triangle_list<kPrepNT>(tri, n);
   for (int k = tid; k < 6 * n; k += kPrepNT) S[k] = 0.0;
@@ -282,7 +292,31 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     for (int k = 0; k < dim; ++k)
       if (dl + k >= 0 && dl + k < n) dbody[dl + k] = cb;
   }
-  const bool write_factor = P.out.dynamics_factor && __syncthreads_or(newc) != 0;
+  // the trees of the tree-blocked outputs: the world's articulations, each a
+  // contiguous DOF range
+  for (int t = tid; t < ntree; t += kPrepNT) {
+    const int ja = P.m.articulation_start[ws.a0 + t], jb = P.m.articulation_start[ws.a0 + t + 1];
+    tds[t] = P.m.joint_qd_start[ja] - d0;
+    if (t == ntree - 1) tds[ntree] = P.m.joint_qd_start[jb] - d0;
+    for (int j = ja; j < jb; ++j) {
+      const int cb = P.m.joint_child[j] - b0g;
+      if (cb >= 0 && cb < B) btree[cb] = t;
+    }
+  }
+  // (the barrier is unconditional: the topology and the tree starts above
+  // are read across threads below)
+  const bool write_factor = __syncthreads_or(newc) != 0 && P.out.dynamics_factor != nullptr;
+  // a tree beyond the block size (or a broken articulation range): the
+  // world's v* is NaN, which the solve reports as not finite
+  bool tree_bad = false;
+  if (blk) {
+    bool bad = false;
+    for (int t = tid; t < ntree; t += kPrepNT) {
+      const int cnt = tds[t + 1] - tds[t];
+      bad = bad || cnt < 0 || cnt > tb || tds[t] < 0 || tds[t + 1] > n;
+    }
+    tree_bad = __syncthreads_or(bad) != 0;
+  }
 
   // ---- local transforms X_{parent body, body} = X_p X_FM(q) X_c^-1 ---------
   // (sim/sap_helpers.py:1164-1243)
@@ -537,20 +571,26 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   __syncthreads();
   // ---- A = composite-rigid-body pairs + armature ------------------------------
   if (blk) {
-    // free bodies: the 6 x 6 block of each tree (DOFs 6 t .. 6 t + 5)
-    double* Tm = P.out.tree_mass + (size_t)e * 36 * B;
-    for (int k = tid; k < 36 * B; k += kPrepNT) {
-      const int t = k / 36, a = (k / 6) % 6, b = k % 6;
-      const int i = 6 * t + (a > b ? a : b), j = 6 * t + (a > b ? b : a);
-      const int bi = dbody[i], bjj = dbody[j];
-      double v = 0.0;
-      if (bi >= 0 && bjj >= 0) {
-        if ((anc[bi] >> bjj) & 1ull) v = sdot(sv_load(S + 6 * j), sv_load(Fi + 6 * i));
-        else if ((anc[bjj] >> bi) & 1ull) v = sdot(sv_load(S + 6 * i), sv_load(Fi + 6 * j));
-      }
-      if (a == b) {
-        v += P.m.joint_armature[d0 + i];
-        adiag[i] = v;
+    // the tb x tb block of each tree (its DOFs tds[t] ..), the identity in
+    // the padding of a tree with fewer DOFs
+    const int bb = tb * tb;
+    double* Tm = P.out.tree_mass + (size_t)e * ntree * bb;
+    for (int k = tid; k < ntree * bb; k += kPrepNT) {
+      const int t = k / bb, a = (k - t * bb) / tb, b = k % tb;
+      const int s0 = tds[t], nt = tds[t + 1] - s0;
+      double v = a == b ? 1.0 : 0.0;
+      if (!tree_bad && a < nt && b < nt) {
+        const int i = s0 + (a > b ? a : b), j = s0 + (a > b ? b : a);
+        const int bi = dbody[i], bjj = dbody[j];
+        v = 0.0;
+        if (bi >= 0 && bjj >= 0) {
+          if ((anc[bi] >> bjj) & 1ull) v = sdot(sv_load(S + 6 * j), sv_load(Fi + 6 * i));
+          else if ((anc[bjj] >> bi) & 1ull) v = sdot(sv_load(S + 6 * i), sv_load(Fi + 6 * j));
+        }
+        if (a == b) {
+          v += P.m.joint_armature[d0 + i];
+          adiag[i] = v;
+        }
       }
       H[k] = v;
       Tm[k] = v;
@@ -578,46 +618,35 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
 
   // ---- free-motion solve A vdot = tau: LDL^T (H_ik = L_ik d_k below the diagonal)
   if (blk) {
-    // a thread per tree: LDL^T of its 6 x 6 block and the solve, in registers
-    for (int t = tid; t < B; t += kPrepNT) {
-      double Lr[6][6], Dr[6], z[6];
-#pragma unroll
-      for (int a = 0; a < 6; ++a)
-#pragma unroll
-        for (int b = 0; b <= a; ++b) Lr[a][b] = H[36 * t + 6 * a + b];
-#pragma unroll
-      for (int b = 0; b < 6; ++b) {
-        double d = Lr[b][b];
-#pragma unroll
-        for (int q = 0; q < b; ++q) d -= Lr[b][q] * Lr[b][q] * Dr[q];
-        Dr[b] = d;
+    // a thread per tree: LDL^T of its block (its own DOFs; H_ab = L_ab d_b
+    // below the diagonal, d on it) in place and the solve of its DOFs
+    for (int t = tid; t < ntree; t += kPrepNT) {
+      if (tree_bad) break;
+      const int s0 = tds[t], nt = tds[t + 1] - s0;
+      double* Ht = H + (size_t)t * tb * tb;
+      for (int b = 0; b < nt; ++b) {
+        double d = Ht[b * tb + b];
+        for (int q = 0; q < b; ++q) d -= Ht[b * tb + q] * Ht[b * tb + q] * Ht[q * tb + q];
+        Ht[b * tb + b] = d;
         const double r = 1.0 / d;
-#pragma unroll
-        for (int a = b + 1; a < 6; ++a) {
-          double v = Lr[a][b];
-#pragma unroll
-          for (int q = 0; q < b; ++q) v -= Lr[a][q] * Lr[b][q] * Dr[q];
-          Lr[a][b] = v * r;
+        for (int a = b + 1; a < nt; ++a) {
+          double v = Ht[a * tb + b];
+          for (int q = 0; q < b; ++q) v -= Ht[a * tb + q] * Ht[b * tb + q] * Ht[q * tb + q];
+          Ht[a * tb + b] = v * r;
         }
       }
-#pragma unroll
-      for (int a = 0; a < 6; ++a) {
-        double v = tau[6 * t + a];
-#pragma unroll
-        for (int q = 0; q < a; ++q) v -= Lr[a][q] * z[q];
+      double* z = vdot + s0;
+      for (int a = 0; a < nt; ++a) {
+        double v = tau[s0 + a];
+        for (int q = 0; q < a; ++q) v -= Ht[a * tb + q] * z[q];
         z[a] = v;
       }
-#pragma unroll
-      for (int a = 0; a < 6; ++a) z[a] /= Dr[a];
-#pragma unroll
-      for (int a = 5; a >= 0; --a) {
+      for (int a = 0; a < nt; ++a) z[a] /= Ht[a * tb + a];
+      for (int a = nt - 1; a >= 0; --a) {
         double v = z[a];
-#pragma unroll
-        for (int q = a + 1; q < 6; ++q) v -= Lr[q][a] * z[q];
+        for (int q = a + 1; q < nt; ++q) v -= Ht[q * tb + a] * z[q];
         z[a] = v;
       }
-#pragma unroll
-      for (int a = 0; a < 6; ++a) vdot[6 * t + a] = z[a];
     }
   } else {
   ldlt_blocked<kPrepNT, double, 5>(H, n, n, dinv, tri);  // width 5: measured fastest for 35 DOFs
@@ -726,7 +755,8 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   __syncthreads();
   for (int i = tid; i < n; i += kPrepNT) {
     const double vd = vdot[i];
-    P.out.v_star[vs0 + i] = P.in.joint_qd[d0 + i] + P.in.dt[e] * vd;
+    P.out.v_star[vs0 + i] = tree_bad ? __longlong_as_double(0x7ff8000000000000ll)
+                                     : P.in.joint_qd[d0 + i] + P.in.dt[e] * vd;
     if (P.out.vdot) P.out.vdot[vs0 + i] = vd;
     if (P.out.qd_slots) P.out.qd_slots[vs0 + i] = P.in.joint_qd[d0 + i];
   }
@@ -739,16 +769,12 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   // ---- contact rows, free-motion contact velocities and diag_delassus
   // weights, one warp per contact: lanes over the DOF columns, row / weight
   // partial sums reduced by shuffles.
-  // Tree-blocked rows hold 12 columns: the 6 DOFs of side 0's tree, then
-  // side 1's (a contact between two shapes of one tree keeps the combined
-  // columns on side 0).
-  const int ncols = blk ? 12 : n;
-  double* Jout = P.out.jacobian + (size_t)e * C * 3 * (blk ? 12 : n_slot);  // rows compact, stride ncols
-  auto tree_of = [&](int lb) {
-    if (lb < 0 || bj[lb] < 0) return -1;
-    const int t = (P.m.joint_qd_start[bj[lb]] - d0) / 6;
-    return (t >= 0 && t < B) ? t : -1;
-  };
+  // Tree-blocked rows hold 2 tb columns: the tb columns of side 0's tree
+  // (zero beyond its own DOFs), then side 1's (a contact between two shapes
+  // of one tree keeps the combined columns on side 0).
+  const int ncols = blk ? 2 * tb : n;
+  double* Jout = P.out.jacobian + (size_t)e * C * 3 * (blk ? 2 * tb : n_slot);  // rows compact, stride ncols
+  auto tree_of = [&](int lb) { return lb < 0 ? -1 : btree[lb]; };
   {
     const int lane = tid & 31, warp = tid >> 5;
     const bool dd = P.o.contact_weight_mode == SAPB_WEIGHT_DIAG_DELASSUS;
@@ -780,8 +806,8 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
         V3 rel = v3(0, 0, 0);
         int dof = col;
         if (blk) {
-          const int ts = col < 6 ? t0 : t1;
-          dof = ts >= 0 ? 6 * ts + col % 6 : -1;
+          const int ts = col < tb ? t0 : t1, a = col < tb ? col : col - tb;
+          dof = (ts >= 0 && !tree_bad && a < tds[ts + 1] - tds[ts]) ? tds[ts] + a : -1;
         }
         const int bcol = dof >= 0 ? dbody[dof] : -1;
         if (bcol >= 0) {
@@ -918,7 +944,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
   }
 }
 
-size_t prepare_smem_bytes(int B, int n, int C, bool blk) { return prep_layout(B, n, C, blk).total; }
+size_t prepare_smem_bytes(int B, int n, int C, int tree_block) { return prep_layout(B, n, C, tree_block).total; }
 
 int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, const sapb_prepare_options* o,
                        const sapb_prepare_outputs* out, void* workspace, size_t workspace_bytes,
@@ -960,7 +986,8 @@ int32_t prepare_launch(const sapb_model_desc* m, const sapb_step_inputs* in, con
     P.hist_depth = hh.has_history;
   }
   if (err == cudaSuccess) {
-    const size_t smem = prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, C, o->tree_blocked != 0);
+    const int tree_block = o->tree_blocked ? (o->tree_dofs > 0 ? o->tree_dofs : 6) : 0;
+    const size_t smem = prepare_smem_bytes(m->bodies_per_world, m->dofs_per_world, C, tree_block);
     const bool vs = out->v_start && P.gamma_start && !o->tree_blocked;
     err = cudaFuncSetAttribute(vs ? prepare_world_kernel<true> : prepare_world_kernel<false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -52,7 +52,8 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
     + 29-revolute serial chain, 35 DOF), 'quadruped' (free base + 4 legs x 3
     revolute, 18 DOF), 'box' (one free box, 6 DOF), 'boxes' (`boxes` free
     bodies, each its own tree: 6 * boxes DOF), 'arm_box' (7-revolute
-    fixed-base arm + free box, 13 DOF), 'slider' (free base + prismatic +
+    fixed-base arm + free box, 13 DOF), 'arm_boxes' (the arm and `boxes`
+    free boxes: 7 + 6 * boxes DOF in 1 + boxes trees), 'slider' (free base + prismatic +
     revolute chain), 'joints' (a chain through every mobilizer kind: free
     base, ball, D6 (1 translation + 2 rotations), distance, D6 (2 + 1), D6
     (3 rotations), revolute, D6 (3 translations), prismatic; 29 DOF)."""
@@ -73,10 +74,11 @@ def world_template(kind: str, rng: np.random.Generator, *, random_child_frames: 
     elif kind == "boxes":
         for _ in range(boxes):
             joints.append((SAP_JOINT_FREE, -1, None))
-    elif kind == "arm_box":
+    elif kind in ("arm_box", "arm_boxes"):
         for k in range(7):
             joints.append((SAP_JOINT_REVOLUTE, k - 1, None))
-        joints.append((SAP_JOINT_FREE, -1, None))
+        for _ in range(1 if kind == "arm_box" else boxes):
+            joints.append((SAP_JOINT_FREE, -1, None))
     elif kind == "slider":
         joints.append((SAP_JOINT_FREE, -1, None))
         joints.append((SAP_JOINT_PRISMATIC, 0, None))
@@ -472,7 +474,8 @@ def _quat_z(yaw: np.ndarray) -> np.ndarray:
 
 def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20), points_per_pair=(4, 8),
               side_pairs=(2, 8), size_range=(0.05, 0.2), density_range=(500.0, 2000.0), v_std: float = 0.05,
-              phi0_range=(-2.0e-3, 0.0), mu_range=(0.3, 1.0), stiffness: float = 1.0e5, tau_d: float = 0.01):
+              phi0_range=(-2.0e-3, 0.0), mu_range=(0.3, 1.0), stiffness: float = 1.0e5, tau_d: float = 0.01,
+              arm: bool = False, gripper=(2, 8)):
     """Worlds of `boxes` free boxes stacked on a grid of sites on the ground
     (the model behind scenes.box_stack_problem, as a SapModel with a flat
     contact buffer): box sizes U[size_range] m per axis, density
@@ -481,6 +484,10 @@ def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20)
     (or the ground), plus a few side contacts between boxes of neighbouring
     stacks; witness points in the body frames of their shapes, normal from
     shape0 to shape1, phi0 ~ U[phi0_range]; joint velocities ~ N(0, v_std).
+    arm: the world also holds a 7-revolute fixed-base arm (bodies 0-6, the
+    boxes after it: 7 + 6 * boxes DOFs in 1 + boxes trees) whose last link
+    grips one box through U{gripper} contacts, which couple the arm's tree
+    with the box's.
     Returns (model, state, control, contacts, host contact dict, host arrays
     dict(tpl, g, q, qd))."""
     from .runtime import SapControl, SapState
@@ -488,11 +495,14 @@ def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20)
 
     rng = np.random.default_rng(seed)
     E, B = worlds, boxes
-    tpl = world_template("boxes", rng, boxes=B)
+    a0 = 7 if arm else 0  # first box body
+    Bt = B + a0           # bodies (and shapes) per world
+    tpl = world_template("arm_boxes" if arm else "boxes", rng, boxes=B)
     g = replicate(tpl, E, rng, mu_range=mu_range, stiffness=stiffness, tau_d=0.5 * tau_d)
-    q = np.zeros((E, 7 * B))
-    ground = E * B
-    rows = []  # (world, shape0, shape1, x1 world, normal, lower body or -1, upper body)
+    Q = tpl["coords_per_world"]
+    q = np.zeros((E, Q))
+    ground = E * Bt
+    rows = []  # (world, lower box or -1, upper box, x1 world, normal)
     pos_all = np.zeros((E, B, 3))
     R_all = np.zeros((E, B, 3, 3))
     dims_all = np.zeros((E, B, 3))
@@ -516,13 +526,13 @@ def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20)
             below[k] = top_box[st]
             top_z[st] += dims[k, 2]
             top_box[st] = k
-        sl = slice(e * B, (e + 1) * B)
+        sl = slice(e * Bt + a0, (e + 1) * Bt)
         a, b, c = dims[:, 0], dims[:, 1], dims[:, 2]
         g["body_mass"][sl] = mass
         g["body_inertia"][sl] = (mass / 12.0)[:, None, None] * np.stack(
             [np.diag(v) for v in np.stack([b * b + c * c, a * a + c * c, a * a + b * b], -1)])
         g["body_com"][sl] = np.stack([np.zeros(B), np.zeros(B), 0.5 * c], -1)
-        q7 = q[e].reshape(B, 7)
+        q7 = q[e, a0:].reshape(B, 7)
         q7[:, :3] = origin
         q7[:, 3:] = _quat_z(yaw)
         pos_all[e], R_all[e] = origin, R
@@ -559,8 +569,8 @@ def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20)
                 rows.append((e, u, w, x1, nrm))
     N = len(rows)
     phi0 = rng.uniform(*phi0_range, size=N)
-    shape0 = np.array([r[0] * B + r[1] if r[1] >= 0 else ground for r in rows], np.int32)
-    shape1 = np.array([r[0] * B + r[2] for r in rows], np.int32)
+    shape0 = np.array([r[0] * Bt + a0 + r[1] if r[1] >= 0 else ground for r in rows], np.int32)
+    shape1 = np.array([r[0] * Bt + a0 + r[2] for r in rows], np.int32)
     x1 = np.stack([r[3] for r in rows])
     nrm = np.stack([r[4] for r in rows])
     x0 = x1 - phi0[:, None] * nrm
@@ -571,18 +581,62 @@ def box_scene(worlds: int, seed: int, device, *, boxes: int = 64, sites=(12, 20)
     p1 = np.einsum("nji,nj->ni", Ru, x1 - pos_all[ew, up])
     Rl = R_all[ew, np.maximum(lo, 0)]
     p0 = np.where((lo >= 0)[:, None], np.einsum("nji,nj->ni", Rl, x0 - pos_all[ew, np.maximum(lo, 0)]), x0)
+    if arm:
+        q[:, :a0] = rng.uniform(-1.0, 1.0, size=a0)[None, :] + rng.normal(scale=0.05, size=(E, a0))
+    model = to_model(tpl, g, q, device)
+    if arm:
+        # the arm's last link grips one box: x1 inside the box, x0 = x1 -
+        # phi0 n in the link's frame (its pose from one free-motion pass)
+        from .runtime import SapContacts as _SC
+        from .solver import SapContactJacobian
+
+        st0 = SapState(joint_q=torch.as_tensor(q.reshape(-1), dtype=torch.float64, device=device),
+                       joint_qd=torch.zeros(model.joint_dof_count, dtype=torch.float64, device=device),
+                       body_q=model.body_q.clone())
+        ctl0 = SapControl(joint_f=torch.zeros(model.joint_dof_count, dtype=torch.float64, device=device))
+        cj = SapContactJacobian(model, max_rigid_contact=1, fallback_tau_d=0.0)
+        cj.compute(st0, _SC(), control=ctl0, dt=2.0e-3)
+        link = cj.body_q_sap.reshape(E, Bt, 7)[:, a0 - 1].cpu().numpy()
+        gs, gp0, gp1, gn = [], [], [], []
+        for e in range(E):
+            u = int(rng.integers(0, B))
+            Rl6 = _quat_to_matrix(link[e, 3:])
+            for _ in range(int(rng.integers(gripper[0], gripper[1] + 1))):
+                r = rng.uniform(-0.4, 0.4, size=3) * dims_all[e, u] + np.array([0.0, 0.0, 0.5 * dims_all[e, u, 2]])
+                xb = pos_all[e, u] + R_all[e, u] @ r
+                nv = _random_unit(rng, 1)[0]
+                ph = rng.uniform(*phi0_range)
+                xa = xb - ph * nv
+                gs.append((e * Bt + a0 - 1, e * Bt + a0 + u))
+                gp0.append(Rl6.T @ (xa - link[e, :3]))
+                gp1.append(r)
+                gn.append(nv)
+        M = len(gs)
+        shape0 = np.concatenate([shape0, np.array([t[0] for t in gs], np.int32)])
+        shape1 = np.concatenate([shape1, np.array([t[1] for t in gs], np.int32)])
+        p0 = np.concatenate([p0, np.stack(gp0)])
+        p1 = np.concatenate([p1, np.stack(gp1)])
+        nrm = np.concatenate([nrm, np.stack(gn)])
+        N += M
     z = np.zeros(N)
     con = dict(count=np.array([N], np.int32), shape0=shape0, shape1=shape1, point0=p0.astype(np.float32),
                point1=p1.astype(np.float32), normal=nrm.astype(np.float32), margin0=z.astype(np.float32),
                margin1=z.astype(np.float32), point0d=p0, point1d=p1, normald=nrm, margin0d=z, margin1d=z.copy())
-    qd = rng.normal(scale=v_std, size=(E, 6 * B))
-    model = to_model(tpl, g, q, device)
+    qd = rng.normal(scale=v_std, size=(E, tpl["dofs_per_world"]))
     state = SapState(joint_q=torch.as_tensor(q.reshape(-1), dtype=torch.float64, device=device),
                      joint_qd=torch.as_tensor(qd.reshape(-1), dtype=torch.float64, device=device),
                      body_q=model.body_q.clone(),
                      body_f=torch.zeros(model.body_count, 6, dtype=torch.float64, device=device))
     control = SapControl(joint_f=torch.zeros(model.joint_dof_count, dtype=torch.float64, device=device))
     return model, state, control, contacts_to_torch(con, device), con, dict(tpl=tpl, g=g, q=q, qd=qd, dims=dims_all)
+
+
+def _quat_to_matrix(q: np.ndarray) -> np.ndarray:
+    """Rotation matrix of a unit quaternion (x, y, z, w)."""
+    x, y, z, w = q / np.linalg.norm(q)
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
 
 
 def box_shapes(host: dict):
@@ -592,6 +646,8 @@ def box_shapes(host: dict):
     from .collision import ShapeSet
     from ._abi import SAPB_SHAPE_BOX, SAPB_SHAPE_PLANE
 
+    if host["tpl"]["kind"] != "boxes":
+        raise ValueError("box_shapes takes the host arrays of a box_scene without an arm")
     dims = host["dims"]
     E, B = dims.shape[:2]
     X = np.zeros((E * B + 1, 7))

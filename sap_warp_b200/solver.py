@@ -123,13 +123,21 @@ class _ModelView:
         if np.any(parent_joint >= np.arange(J)):
             raise ValueError("joints must be ordered parents before children")
         self.device = model.joint_type.device
-        # worlds made only of free bodies (one 6-DOF tree per body) may use the
-        # tree-blocked layout; by default those beyond the dense solve's 60
-        # DOFs do
-        jp = model.joint_parent.cpu().numpy()
-        self.free_bodies = bool(not self.uneven and self.Jw == self.Bw and self.n == 6 * self.Bw and self.Bw <= 64
-                                and np.all(jt == SAP_JOINT_FREE) and np.all(jp < 0))
-        self.tree_blocked = self.free_bodies and self.n > 60
+        # the tree-blocked layout: the trees are the world's articulations
+        # (a free body, an arm), each in a block of tree_block DOFs (6, 7 or
+        # 12: the smallest holding the largest tree); worlds of equal blocks
+        # with <= 64 bodies may use it, and by default those beyond the dense
+        # solve's 60 DOFs do
+        self.tree_dof_start, self.tree_block = None, 0
+        if not self.uneven and self.Bw <= 64 and 1 <= self.Aw <= 64:
+            art = model.articulation_start.cpu().numpy()[:self.Aw + 1]
+            ds0 = model.joint_qd_start.cpu().numpy()
+            tds = np.array([int(ds0[int(a)]) for a in art], np.int64)
+            if tds[0] == 0 and tds[-1] == self.n and np.all(np.diff(tds) >= 0):
+                self.tree_block = tree_block_for(int(np.diff(tds).max()))
+                self.tree_dof_start = torch.as_tensor(tds.astype(np.int32), device=model.joint_type.device)
+        self.tree_eligible = self.tree_block > 0
+        self.tree_blocked = self.tree_eligible and self.n > 60
         d = _abi.ModelDesc()
         d.num_worlds, d.joints_per_world, d.bodies_per_world = W, self.Jw, self.Bw
         d.dofs_per_world, d.coords_per_world, d.articulations_per_world = self.n, self.Qw, self.Aw
@@ -237,11 +245,22 @@ def _checked_order(order: torch.Tensor | None, W: int) -> torch.Tensor | None:
     return order
 
 
+def tree_block_for(tree_dofs: int) -> int:
+    """The block size of the tree-blocked solve for trees of up to tree_dofs
+    DOFs: the smallest of 6, 7 and 12 that holds them, 0 if none does (the
+    rule of sapb_blocked_tree_block)."""
+    for nb in (6, 7, 12):
+        if 0 <= tree_dofs <= nb:
+            return nb
+    return 0
+
+
 def _pick_tree_blocked(view: _ModelView, tree_blocked: bool | None) -> bool:
     if tree_blocked is None:
         return view.tree_blocked
-    if tree_blocked and not view.free_bodies:
-        raise ValueError("the tree-blocked layout needs worlds made only of free bodies (<= 64 per world)")
+    if tree_blocked and not view.tree_eligible:
+        raise ValueError("the tree-blocked layout needs equal worlds of <= 64 bodies whose articulations hold at "
+                         "most 12 DOFs each")
     return bool(tree_blocked)
 
 
@@ -278,10 +297,11 @@ class SapContactJacobianResult:
     # LDL^T of dynamics_matrix_env from the free-motion solve (no counterpart
     # in the reference's result), or None when not requested
     dynamics_factor_env: torch.Tensor | None = None
-    # tree-blocked layout (worlds of free bodies; no counterpart in the
-    # reference): the diagonal 6 x 6 blocks of A [W, B, 6, 6] and the tree of
-    # each contact side [W, C, 2]; contact_env_jacobian is then [W, C, 3, 12]
-    # and dynamics_matrix_env is None
+    # tree-blocked layout (no counterpart in the reference): the diagonal
+    # blocks of A, one per articulation [W, T, NB, NB] (the identity beyond a
+    # tree's own DOFs), and the tree of each contact side [W, C, 2];
+    # contact_env_jacobian is then [W, C, 3, 2 NB] and dynamics_matrix_env is
+    # None
     tree_mass_env: torch.Tensor | None = None
     contact_env_tree: torch.Tensor | None = None
 
@@ -344,15 +364,17 @@ class SapContactJacobian:
         self.opts.fallback_stiffness = float(fallback_stiffness)
         self.opts.fallback_tau_d = float(fallback_tau_d)
         self.opts.tree_blocked = 1 if self.tree_blocked else 0
+        self.opts.tree_dofs = v.tree_block if self.tree_blocked else 0
         W, n, C, dev = v.W, v.n, self.max_rigid_contact, v.device
         z = lambda *s, dt=F64: torch.zeros(*s, dtype=dt, device=dev)
         self.v_star = z(W * n)
         self.vdot = z(W * n)
         if self.tree_blocked:
             self.dynamics_matrix_env = None
-            self.tree_mass_env = z(W, v.Bw, 6, 6)
+            NB = v.tree_block
+            self.tree_mass_env = z(W, v.Aw, NB, NB)
             self.contact_env_tree = torch.full((W, C, 2), -1, dtype=I32, device=dev)
-            self.contact_env_jacobian = z(W, C, 3, 12)
+            self.contact_env_jacobian = z(W, C, 3, 2 * NB)
         else:
             self.dynamics_matrix_env = z(W, n, n)
             self.tree_mass_env = self.contact_env_tree = None
@@ -566,7 +588,7 @@ class SapContactSolve:
         self.grad_norm = z(W)
         self.warm_start_accepted_env = z(W, dt=I32)
         self.dt_world = z(W)
-        ws = int(load().sapb_blocked_solve_workspace_size(W, v.Bw, C) if self.tree_blocked
+        ws = int(load().sapb_blocked_solve_workspace_size(W, v.Aw, C) if self.tree_blocked
                  else load().sapb_contact_solve_workspace_size(W, n, C))
         self.workspace = torch.zeros(max(ws, 16), dtype=torch.uint8, device=dev)
         self.zero_f32 = z(W * n, dt=F32)
@@ -788,7 +810,8 @@ class SapContactSolve:
             raise ValueError("the tree-blocked solve needs a tree-blocked SapContactJacobianResult")
         v = self.view
         P = _abi.BlockedProblem()
-        P.num_envs, P.trees_per_env, P.tree_dofs = v.W, v.Bw, 6
+        P.num_envs, P.trees_per_env, P.tree_dofs = v.W, v.Aw, v.tree_block
+        P.tree_dof_start, P.dofs_per_world = _ptr(v.tree_dof_start), v.n
         P.max_contacts = int(r.contact_env_jacobian.shape[1])
         P.contact_count, P.tree_mass = _ptr(r.contact_env_count), _ptr(r.tree_mass_env)
         P.world_order = _ptr(_checked_order(world_order, v.W))

@@ -52,6 +52,13 @@ def test_no_compute_entry_points_without_gpu(lib):
     assert lib.sapb_blocked_fill_capacity(64, 6, 448, _abi.SAPB_FP64) > 100
     assert lib.sapb_blocked_fill_capacity(64, 6, 448, _abi.SAPB_FP32) > 100
     assert lib.sapb_blocked_fill_capacity(64, 5, 448, _abi.SAPB_FP64) == 0
+    # block sizes of trees of different sizes: the smallest built block that holds them
+    from sap_warp_b200.solver import tree_block_for
+    for nt in range(-1, 15):
+        assert lib.sapb_blocked_tree_block(nt) == tree_block_for(nt)
+    assert [tree_block_for(k) for k in (1, 6, 7, 8, 12, 13)] == [6, 6, 7, 12, 12, 0]
+    assert lib.sapb_blocked_fill_capacity(24, 7, 256, _abi.SAPB_FP64) > 20
+    assert lib.sapb_blocked_fill_capacity(16, 12, 128, _abi.SAPB_FP32) > 10
     assert b"null" in lib.sapb_last_error()
     assert lib.sapb_mlp_param_count() == _abi.SAPB_MLP_PARAM_COUNT
     assert lib.sapb_mlp_packed_count() == _abi.SAPB_MLP_PACKED_COUNT
