@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 16
+#define SAPB_ABI_VERSION 17
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -136,6 +136,11 @@ typedef struct sapb_dof_terms {
   const float* joint_target_pos;  /* [E*n] or NULL (zeros) */
   const float* joint_target_vel;  /* [E*n] or NULL (zeros) */
   const float* joint_act;         /* [E*n] or NULL (zeros) */
+  /* Uneven batches (the solve's dof_count): [E+1] offsets of each world's
+   * DOFs in the model's global DOF order, in which the per-DOF arrays above
+   * and dof_target_index then are (world e's DOF i is world_dof_start[e] +
+   * i); NULL: the per-DOF arrays are in the solve's [E*n] layout. */
+  const int32_t* world_dof_start;
 } sapb_dof_terms;
 
 /* The stage-2 problem of one step: SapContactJacobianResult fields

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 16
+SAPB_ABI_VERSION = 17
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -92,6 +92,7 @@ class DofTerms(C.Structure):
         ("joint_target_pos", _p),
         ("joint_target_vel", _p),
         ("joint_act", _p),
+        ("world_dof_start", _p),
     ]
 
 

@@ -561,13 +561,15 @@ __device__ __forceinline__ void solve_world(const SolveParams& P, const Layout& 
   // ---- PD and limit terms (sim/contact_solve.py:490-683) ------------------
   for (int i = tid; i < n; i += NT) {
     int fl = 0;
-    const size_t dof = base + i;
     const sapb_dof_terms& D = P.dof;
+    // the per-DOF arrays: the solve's layout, or the model's global DOF order
+    const size_t dof = D.world_dof_start ? (size_t)D.world_dof_start[e] + i : base + i;
     if (D.has_pd) {
       int coord = D.dof_coord_index[dof];
       if (coord >= D.joint_coord_count) coord = -1;
       int target = D.dof_target_index[dof];
-      if (target < 0 || target >= P.p.num_envs * n_max) target = (int)dof;
+      const int ndof = D.world_dof_start ? D.world_dof_start[P.p.num_envs] : P.p.num_envs * n_max;
+      if (target < 0 || target >= ndof) target = (int)dof;
       if (D.joint_target_mode[target] != 0) {
         const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
         if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {

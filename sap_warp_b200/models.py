@@ -745,20 +745,68 @@ def concat_contacts(parts, shape_offsets) -> "SapContacts":
     return SapContacts(rigid_contact_count=cnt, **out)
 
 
-def mixed_rollout_scene(worlds_per_kind, seed: int, device, kinds=("arm_box", "quadruped", "humanoid"), **kw):
+def with_drives(model: SapModel, state, control, rng: np.random.Generator, *, ke=(10.0, 1.0e3), kd=(0.1, 10.0),
+                effort: float = 5.0, limit: float = 0.3, limit_ke: float = 1.0e4, limit_kd: float = 10.0):
+    """The model with a drive on every revolute and prismatic DOF (gains
+    U[ke], U[kd], effort limit `effort`) and joint limits +-`limit` around
+    the state's coordinate there (stiffness limit_ke, damping limit_kd), and
+    the control with drive targets near that coordinate (target velocities
+    ~ N(0, 1)).  Returns (model, control)."""
+    import dataclasses
+
+    from .runtime import SapControl
+
+    jt = model.joint_type.cpu().numpy()
+    ds, qs = model.joint_qd_start.cpu().numpy(), model.joint_q_start.cpu().numpy()
+    q = state.joint_q.cpu().numpy()
+    D = int(model.joint_dof_count)
+    on = np.zeros(D, bool)
+    q_at = np.zeros(D)
+    for j, t in enumerate(jt):
+        if t in (SAP_JOINT_REVOLUTE, SAP_JOINT_PRISMATIC):
+            on[ds[j]] = True
+            q_at[ds[j]] = q[qs[j]]
+    dev = model.joint_type.device
+    f32 = lambda a: torch.as_tensor(np.asarray(a, np.float32), device=dev)
+    f64 = lambda a: torch.as_tensor(np.asarray(a, np.float64), device=dev)
+    m2 = dataclasses.replace(
+        model, joint_target_mode=torch.as_tensor(on.astype(np.int32), device=dev),
+        joint_target_ke=f32(np.where(on, rng.uniform(*ke, D), 0.0)),
+        joint_target_kd=f32(np.where(on, rng.uniform(*kd, D), 0.0)),
+        joint_effort_limit=f32(np.where(on, effort, 0.0)),
+        joint_limit_lower=f64(np.where(on, q_at - limit, -np.inf)),
+        joint_limit_upper=f64(np.where(on, q_at + limit, np.inf)),
+        joint_limit_ke=f64(np.where(on, limit_ke, 0.0)), joint_limit_kd=f64(np.where(on, limit_kd, 0.0)))
+    c2 = SapControl(joint_f=control.joint_f, joint_target_pos=f32(np.where(on, q_at + rng.uniform(-0.2, 0.2, D), 0.0)),
+                    joint_target_vel=f32(np.where(on, rng.normal(size=D), 0.0)))
+    return m2, c2
+
+
+def mixed_rollout_scene(worlds_per_kind, seed: int, device, kinds=("arm_box", "quadruped", "humanoid"),
+                        drives: bool = False, **kw):
     """An uneven batch of rollout scenes: `worlds_per_kind` worlds of each
     kind (arm + box 13 DOF, quadruped 18, humanoid 35 by default), their
-    models, states, controls and contacts concatenated.  Returns (model,
-    state, control, contacts, parts) with parts the per-kind
-    (model, state, control, contacts)."""
+    models, states, controls and contacts concatenated; drives: each part
+    with_drives (seeded).  Returns (model, state, control, contacts, parts)
+    with parts the per-kind (model, state, control, contacts)."""
     from .runtime import SapControl, SapState
 
     parts = [rollout_scene(k, worlds_per_kind, seed + i, device, **kw)[:4] for i, k in enumerate(kinds)]
+    if drives:
+        rng = np.random.default_rng(seed + 100)
+        driven = []
+        for pm, ps, pc, pcon in parts:
+            dm, dc = with_drives(pm, ps, pc, rng)
+            driven.append((dm, ps, dc, pcon))
+        parts = driven
     models_ = [p[0] for p in parts]
     model = concat_models(models_)
     state = SapState(joint_q=torch.cat([p[1].joint_q for p in parts]), joint_qd=torch.cat([p[1].joint_qd for p in parts]),
                      body_q=torch.cat([p[1].body_q for p in parts]), body_f=torch.cat([p[1].body_f for p in parts]))
-    control = SapControl(joint_f=torch.cat([p[2].joint_f for p in parts]))
+    cat = lambda name: (torch.cat([getattr(p[2], name) for p in parts])
+                        if all(getattr(p[2], name) is not None for p in parts) else None)
+    control = SapControl(joint_f=cat("joint_f"), joint_target_pos=cat("joint_target_pos"),
+                         joint_target_vel=cat("joint_target_vel"))
     shape_offs = np.cumsum([0] + [int(m.shape_count) for m in models_])[:-1]
     contacts = concat_contacts([p[3] for p in parts], shape_offs)
     return model, state, control, contacts, parts

@@ -615,6 +615,10 @@ class SapContactSolve:
                 joint_limit_ke=_f64(m.joint_limit_ke), joint_limit_kd=_f64(m.joint_limit_kd))
             for k, t in self._dof_keep.items():
                 setattr(self.dof, k, t.data_ptr())
+            if v.uneven:
+                # per-DOF arrays in the model's global order, each world's
+                # from its DOF offset (the solve runs in slots)
+                self.dof.world_dof_start = v._keep["world_dof_start"].data_ptr()
 
     def options(self, line_search_variant, **kw) -> _abi.SolveOptions:
         from ._solve import make_options
@@ -1015,11 +1019,6 @@ class SolverSAP:
         if self.contact_solve.tree_blocked and self.warm_start == "learned":
             raise NotImplementedError("the tree-blocked layout takes the previous-velocity or previous-impulses "
                                       "warm start")
-        if view.uneven:
-            if self.warm_start == "learned":
-                raise NotImplementedError("uneven batches take the previous-velocity or previous-impulses warm start")
-            if view.has_pd or view.has_limits:
-                raise NotImplementedError("uneven batches take no drive or limit terms")
         self.learned_candidates = str(learned_candidates).strip().lower().replace("-", "_")
         if self.learned_candidates not in ("new_contacts", "all_contacts"):
             raise ValueError(f"learned_candidates must be 'new_contacts' or 'all_contacts', got {learned_candidates!r}.")

@@ -2,8 +2,9 @@
 + box 13 DOF, quadruped 18, humanoid 35; models.concat_models), stepped as
 one batch -- one free-motion launch, one persistent solve launch with each
 world at its own DOF count, one tail launch -- against the same worlds
-stepped as three homogeneous batches, and a graph-captured rollout against
-eager steps."""
+stepped as three homogeneous batches (previous-velocity, previous-impulse and
+learned starts; with and without drive and limit terms), and a
+graph-captured rollout against eager steps."""
 
 import numpy as np
 import pytest
@@ -21,13 +22,18 @@ def _pair(state):
                      body_f=state.body_f.clone()) for _ in range(2)]
 
 
-@pytest.mark.parametrize("warm", ["previous_velocity", "previous_impulses"])
-def test_uneven_batch_steps_like_its_homogeneous_parts(cuda_device, warm):
+@pytest.mark.parametrize("warm,drives", [("previous_velocity", False), ("previous_impulses", False),
+                                         ("learned", False), ("previous_impulses", True), ("learned", True)])
+def test_uneven_batch_steps_like_its_homogeneous_parts(cuda_device, warm, drives):
+    """Also with the learned start (the network, the start velocity and the
+    free motion's factor in the solve's slots) and with drive and limit terms
+    (their per-DOF arrays read in the model's global order)."""
     Wk, steps = 64, 6
-    model, state, control, contacts, parts = models.mixed_rollout_scene(Wk, 31, cuda_device)
+    model, state, control, contacts, parts = models.mixed_rollout_scene(Wk, 31, cuda_device, drives=drives)
     kw = dict(max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32", warm_start=warm)
     solver = SolverSAP(model, **kw)
     assert solver.view.uneven and list(np.unique(solver.view.dof_counts)) == [13, 18, 35]
+    assert solver.view.has_pd == drives and solver.view.has_limits == drives
     a, b = _pair(state)
     for _ in range(steps):
         solver.step(a, b, control, contacts, 2.0e-3)
