@@ -680,7 +680,7 @@ def main():
     bmodel, bstate, bcontrol, bcon, _, bhost = models.box_scene(512, 75 + 1000 * rank, dev)
     box_step = {"worlds": 512, "trees": "64 free boxes per world (n = 384)",
                 "contacts": f"{int(bcon.rigid_contact_count.item())} in all"}
-    for warm in ("previous_velocity", "previous_impulses"):
+    for warm in ("previous_velocity", "previous_impulses", "learned"):
         bsolver = SolverSAP(bmodel, max_rigid_contact=512, contact_preset_variant="drake", hessian_precision="fp32",
                             warm_start=warm)
         ba = SapState(joint_q=bstate.joint_q.clone(), joint_qd=bstate.joint_qd.clone(), body_q=bstate.body_q.clone(),

@@ -419,6 +419,13 @@ class SapContactJacobian:
             v = self.view
             self.dynamics_factor_env = torch.zeros(v.W, v.n, v.n, dtype=F64, device=v.device)
             self.outputs.dynamics_factor = _ptr(self.dynamics_factor_env)
+        self.keep_contact_velocities()
+
+    def keep_contact_velocities(self) -> None:
+        """Also write the free-motion contact velocities J_c v* (the
+        warm-start network's inputs); in either layout."""
+        if getattr(self, "contact_env_vc_star", None) is None:
+            v = self.view
             self.contact_env_vc_star = torch.zeros(v.W, self.max_rigid_contact, 3, dtype=F64, device=v.device)
             self.outputs.vc_star = _ptr(self.contact_env_vc_star)
 
@@ -1016,9 +1023,6 @@ class SolverSAP:
         if self.warm_start not in ("previous_velocity", "previous_impulses", "learned"):
             raise ValueError("warm_start must be 'previous_velocity', 'previous_impulses' or 'learned', "
                              f"got {warm_start!r}.")
-        if self.contact_solve.tree_blocked and self.warm_start == "learned":
-            raise NotImplementedError("the tree-blocked layout takes the previous-velocity or previous-impulses "
-                                      "warm start")
         self.learned_candidates = str(learned_candidates).strip().lower().replace("-", "_")
         if self.learned_candidates not in ("new_contacts", "all_contacts"):
             raise ValueError(f"learned_candidates must be 'new_contacts' or 'all_contacts', got {learned_candidates!r}.")
@@ -1072,12 +1076,17 @@ class SolverSAP:
                 self._v_start = torch.zeros(view.W * view.n, dtype=F64, device=dev)
             self.contact_jacobian.set_history(
                 H, v_start=self._v_start,
-                factor_new_contacts_only=self.warm_start == "learned" and self.learned_candidates == "new_contacts")
+                factor_new_contacts_only=(self.warm_start == "learned" and self.learned_candidates == "new_contacts"
+                                          and not self.contact_solve.tree_blocked))
         if self.learned_warm_start is not None:
             self.learned_warm_start.set_regularization(contact_beta, contact_sigma, 2.0 * shape_tau)
             # network inputs J_c v* and, for the network's impulses, the
-            # factor of A (new contacts only in the new_contacts mode)
-            self.contact_jacobian.keep_dynamics_factor()
+            # factor of A (new contacts only in the new_contacts mode; the
+            # tree-blocked solve factors A's tree blocks itself)
+            if self.contact_solve.tree_blocked:
+                self.contact_jacobian.keep_contact_velocities()
+            else:
+                self.contact_jacobian.keep_dynamics_factor()
             self._gamma_zero = torch.zeros(view.W, max(C, 1), 3, dtype=F64, device=dev)
         self.work_order = str(work_order).strip().lower().replace("-", "_")
         if self.work_order not in ("previous_iterations", "index"):
@@ -1306,6 +1315,20 @@ class SolverSAP:
                 v_cands = self._v_start
             else:
                 gamma0 = self._gamma_prev  # tree-blocked: the solve maps them tree by tree
+        elif self.warm_start == "learned" and self.contact_solve.tree_blocked:
+            # one impulse set for the tree-blocked candidate: the history's
+            # start impulses where a contact has them, the network's on new
+            # contacts (the solve forms v* + A^-1 J^T gamma tree by tree)
+            self._normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
+            self.learned_warm_start.predict(
+                num_envs=self.view.W, dof_per_env=int(cr.contact_env_jacobian.shape[-1]),
+                max_contacts=self.max_rigid_contact, normal_up=self._normal_up, gamma_prev=self._gamma_prev,
+                out=self._gamma_cand[0], vc_star=self.contact_jacobian.contact_env_vc_star,
+                contact_count=cr.contact_env_count, dynamics_matrix=None, jacobian=cr.contact_env_jacobian,
+                phi0=cr.contact_env_phi0, w_eff=cr.contact_env_w_eff, mu=cr.contact_env_mu,
+                stiffness=cr.contact_env_stiffness, tau_d=cr.contact_env_tau_d, v_star=self.contact_jacobian.v_star,
+                v0=self.contact_jacobian.v_star, dt=self.contact_jacobian.dt_world, has_history=self.has_history)
+            gamma0 = self._gamma_cand[0]
         elif self.warm_start == "learned":
             self._normal_up.copy_(cr.contact_env_R_WC[..., 2, 2])
             # new_contacts: the network's impulses on new contacts only (zero

@@ -91,14 +91,17 @@ def test_arm_blocked_rows_match_dense_rows(cuda_device, weight_mode, point_mode)
     assert gripped >= 2 * W  # every world's gripper contacts touch the arm's tree
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_arm_box_step_matches_oracle_pipeline(cuda_device, oracle, precision):
+@pytest.mark.parametrize("precision,warm", [("fp64", "previous_velocity"), ("fp32", "previous_velocity"),
+                                            ("fp64", "learned")])
+def test_arm_box_step_matches_oracle_pipeline(cuda_device, oracle, precision, warm):
     """SolverSAP.step (tree-blocked, trees of 7 and 6 DOFs) == C free motion
-    and rows -> C oracle dense solve -> C integration."""
+    and rows -> C oracle dense solve -> C integration; the learned start
+    (the network's impulses as the blocked solve's candidate) changes the
+    start, not the answer."""
     W, Bx, C = 16, 6, 96
     model, state, control, con, host, hv = models.box_scene(W, 72, cuda_device, boxes=Bx, sites=(2, 4), arm=True)
     solver = SolverSAP(model, max_rigid_contact=C, contact_preset_variant="drake", contact_tau_d=0.0,
-                       tree_blocked=True, hessian_precision=precision)
+                       tree_blocked=True, hessian_precision=precision, warm_start=warm)
     out = _clone(state)
     solver.step(state, out, control, con, DT)
     torch.cuda.synchronize()
@@ -153,6 +156,32 @@ def test_arm_blocked_step_matches_dense_step(cuda_device):
     scale = np.abs(runs[False][0]).max()
     np.testing.assert_allclose(runs[True][0], runs[False][0], rtol=0, atol=2e-5 * scale)
     np.testing.assert_allclose(runs[True][1], runs[False][1], rtol=0, atol=1e-8)
+
+
+def test_learned_start_rollout_in_tree_blocked_layout(cuda_device):
+    """An arm among 24 boxes (tree-blocked), 8 steps from the previous
+    velocity and with the learned start (history impulses where a contact
+    has them, the network's on new contacts): both converge, the learned
+    candidate is taken, and the trajectories agree to the solve's
+    tolerance."""
+    model, state, control, con, _, _ = models.box_scene(48, 77, cuda_device, boxes=24, sites=(6, 9), arm=True)
+    kw = dict(max_rigid_contact=256, contact_preset_variant="drake", hessian_precision="fp32")
+    runs = {}
+    for warm in ("previous_velocity", "learned"):
+        solver = SolverSAP(model, warm_start=warm, **kw)
+        assert solver.contact_solve.tree_blocked
+        a, b = _clone(state), _clone(state)
+        taken = []
+        for _ in range(8):
+            solver.step(a, b, control, con, DT)
+            assert bool(solver.contact_solve.converged_env.all())
+            taken.append(float(solver.contact_solve.warm_start_accepted_env.double().mean()))
+            a, b = b, a
+        torch.cuda.synchronize()
+        runs[warm] = (np.mean(taken[2:]), a.joint_qd.clone())
+    assert runs["learned"][0] > 0.5
+    qv, ql = runs["previous_velocity"][1], runs["learned"][1]
+    assert float((ql - qv).abs().max() / qv.abs().max()) < 1e-3
 
 
 def test_dense_to_blocked_gather_with_tree_map(cuda_device):
