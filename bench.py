@@ -635,7 +635,7 @@ def main():
                                                             opts.line_search_variant))
 
         def time_ms(shape, tt=tt, bb=bb, opts=opts, wo=wo):
-            opts.ctas_per_sm, opts.ldlt_block = shape
+            opts.ctas_per_sm, opts.ldlt_block, opts.threads_per_cta = shape
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             contact_solve(**tt, buffers=bb, options=opts, world_order=wo)
@@ -645,12 +645,19 @@ def main():
 
         wl = (__import__("ctypes").c_int32 * 8)()
         nw = max(min(int(_load_lib().sapb_contact_solve_ldlt_blocks(bb.dof_per_env, wl, 8)), 8), 1)
+        # the 256-thread runtime-size kernel at its own occupancy, its width
+        occ_w = int(_load_lib().sapb_contact_solve_occupancy_threads(bb.dof_per_env, bb.max_contacts,
+                                                                      opts.hessian_precision,
+                                                                      opts.line_search_variant, 256))
+        gw = (__import__("ctypes").c_int32 * 8)()
+        _load_lib().sapb_contact_solve_ldlt_blocks(1, gw, 8)
+        cands = [(k, int(wl[w]), 128) for w in range(nw) for k in range(1, occ + 1)]
+        cands += [(k, int(gw[0]), 256) for k in range(1, occ_w + 1)]
         tuner = SolveAutotuner(repeats=5)
-        chosen = tuner.tune(label, [(k, int(wl[w])) for w in range(nw) for k in range(1, occ + 1)], time_ms,
-                            default=(occ, int(wl[0])))
-        opts.ctas_per_sm, opts.ldlt_block = 0, 0
-        tuned[label] = {"occupancy": occ, "ldlt_blocks": [int(wl[w]) for w in range(nw)], "chosen": list(chosen),
-                        "ms": tuner.table[label]["ms"]}
+        chosen = tuner.tune(label, cands, time_ms, default=(occ, int(wl[0]), 128))
+        opts.ctas_per_sm, opts.ldlt_block, opts.threads_per_cta = 0, 0, 0
+        tuned[label] = {"occupancy": occ, "occupancy_256_threads": occ_w, "ldlt_blocks": [int(wl[w]) for w in range(nw)],
+                        "chosen": list(chosen), "ms": tuner.table[label]["ms"]}
 
     # ---- worlds of 64 free boxes (384 DOFs, ~400 contacts): tree-blocked solve ----
     boxes = scenes.box_stack_problem(512, seed=4 + 1000 * rank)
@@ -746,9 +753,15 @@ def main():
                                        ("blocked_fp64_previous_velocity", True, "fp64", "previous_velocity"),
                                        ("dense_fp32_previous_impulses", False, "fp32", "previous_impulses"),
                                        ("blocked_fp32_previous_impulses", True, "fp32", "previous_impulses")):
+        # the dense arms autotuned (CTAs per SM, LDL^T width, 128 or 256
+        # threads per world: these worlds leave one CTA per SM)
         asolver = SolverSAP(amodel, max_rigid_contact=112, contact_preset_variant="drake", hessian_precision=prec,
-                            warm_start=warm, tree_blocked=blocked)
+                            warm_start=warm, tree_blocked=blocked, autotune=not blocked)
         arm_step["arm_8_boxes"][label] = time_steps(asolver, astate, acontrol, acon, 2048, k_arm)
+        if not blocked:
+            arm_step["arm_8_boxes"][label]["autotune"] = {
+                k.split("-NVIDIA")[0]: {"chosen": v["choice"], "ms": v["ms"]}
+                for k, v in asolver.contact_solve.autotuner.table.items()}
         del asolver
     amodel, astate, acontrol, acon, _, _ = models.box_scene(512, 78 + 1000 * rank, dev, boxes=32, sites=(8, 12),
                                                             arm=True)

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 17
+#define SAPB_ABI_VERSION 18
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -110,6 +110,10 @@ typedef struct sapb_solve_options {
   int32_t skip_plain_start;       /* nonzero, with candidate starts: start from the best candidate without
                                    * evaluating the plain start (v_guess or v0), which is kept only as the
                                    * fallback when no candidate's cost is finite; 0: the plain start competes */
+  int32_t threads_per_cta;        /* threads of one world's CTA in the dense solve: 0 or 128 the default (the
+                                   * kernel specialised on the DOF count), 256 the runtime-size kernel with
+                                   * eight warps per world (for worlds whose shared memory leaves one or two
+                                   * CTAs per SM); results do not depend on it beyond rounding */
 } sapb_solve_options;
 
 /* Per-DOF drive and limit model (the arrays SapContactSolve.prepare reads,
@@ -626,6 +630,11 @@ int32_t sapb_generate_contacts(const sapb_collision_shapes* shapes, const double
  * (the upper end of sapb_solve_options.ctas_per_sm), or a negative status. */
 int32_t sapb_contact_solve_occupancy(int32_t dof_per_env, int32_t max_contacts, int32_t hessian_precision,
                                      int32_t line_search_variant);
+
+/* The same for a threads_per_cta choice of sapb_solve_options (0, 128 or
+ * 256), or a negative status. */
+int32_t sapb_contact_solve_occupancy_threads(int32_t dof_per_env, int32_t max_contacts, int32_t hessian_precision,
+                                             int32_t line_search_variant, int32_t threads_per_cta);
 
 /* The LDL^T column-block widths the dense solve is built with for worlds of
  * dof_per_env DOFs (the first is the default), written to widths (at most

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 17
+SAPB_ABI_VERSION = 18
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -69,6 +69,7 @@ class SolveOptions(C.Structure):
         ("ctas_per_sm", C.c_int32),
         ("ldlt_block", C.c_int32),
         ("skip_plain_start", C.c_int32),
+        ("threads_per_cta", C.c_int32),
     ]
 
 
@@ -388,6 +389,7 @@ EXPORTS = {
     "sapb_step_tail_launch": (C.c_int32, [C.POINTER(ModelDesc), C.POINTER(StepTail), _p]),
     "sapb_contact_solve_workspace_size": (C.c_size_t, [C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_occupancy": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "sapb_contact_solve_occupancy_threads": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "sapb_contact_solve_ldlt_blocks": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.c_int32]),
     "sapb_contact_solve": (
         C.c_int32,

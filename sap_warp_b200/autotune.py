@@ -7,10 +7,12 @@ counter, and each world is solved by one CTA, so results do not depend on k
 LDL^T factorization's column-block width b (sapb_contact_solve_ldlt_blocks):
 the best width depends on the DOF count (35 DOFs: seven blocks of 5), and
 the width changes the factorization's rounding (not the tolerance the
-solve reaches).  The tuner times every (k, b) on the caller's own first
-solve (CUDA events, best of a few runs each) and keeps the fastest in a
-table keyed by (DOFs per world, contact-slot bucket, precision, line search,
-GPU name, SM count), which it can persist as JSON.  The default shape (the
+solve reaches); and a runtime-size kernel with 256 threads per world, which
+pays where shared memory leaves one CTA per SM.  The tuner times every
+(k, b, threads) on the caller's own first solve (CUDA events, best of a few
+runs each) and keeps the fastest in a table keyed by (DOFs per world,
+contact-slot bucket, precision, line search, GPU name, SM count), which it
+can persist as JSON.  The default shape (the
 occupancy bound, the first width) is kept unless another beats it by more
 than a margin.
 """
@@ -47,7 +49,7 @@ def _shape(value):
 
 class SolveAutotuner:
     """Choice of launch shape per problem key: an int (resident CTAs per SM)
-    or a tuple (CTAs per SM, LDL^T block width).
+    or a tuple (CTAs per SM, LDL^T block width[, threads per CTA]).
 
     cache_path: a JSON file to load the table from and write it back to after
     each new choice (None: this process only).  repeats: timed runs per

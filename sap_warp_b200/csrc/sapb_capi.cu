@@ -35,6 +35,18 @@ int32_t sapb_contact_solve_occupancy(int32_t dof_per_env, int32_t max_contacts, 
   return sapb::contact_solve_occupancy(dof_per_env, max_contacts, hessian_precision, line_search_variant);
 }
 
+int32_t sapb_contact_solve_occupancy_threads(int32_t dof_per_env, int32_t max_contacts, int32_t hessian_precision,
+                                             int32_t line_search_variant, int32_t threads_per_cta) {
+  if (line_search_variant < SAPB_LS_MONOTONE_DECAY || line_search_variant > SAPB_LS_EXACT_ROOT ||
+      !(threads_per_cta == 0 || threads_per_cta == 128 || threads_per_cta == 256)) {
+    sapb::set_last_error("sapb_contact_solve_occupancy_threads: unknown line search variant %d or thread count %d",
+                         line_search_variant, threads_per_cta);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  return sapb::contact_solve_occupancy(dof_per_env, max_contacts, hessian_precision, line_search_variant,
+                                       threads_per_cta);
+}
+
 int32_t sapb_contact_solve_ldlt_blocks(int32_t dof_per_env, int32_t* widths, int32_t capacity) {
   if (dof_per_env < 1 || capacity < 0 || (capacity > 0 && !widths)) {
     sapb::set_last_error("sapb_contact_solve_ldlt_blocks: invalid argument");
@@ -119,6 +131,10 @@ int32_t sapb_contact_solve(const sapb_contact_problem* p, const sapb_solve_optio
   }
   if (o->line_search_variant < SAPB_LS_MONOTONE_DECAY || o->line_search_variant > SAPB_LS_EXACT_ROOT) {
     sapb::set_last_error("sapb_contact_solve: unknown line search variant %d", o->line_search_variant);
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (!(o->threads_per_cta == 0 || o->threads_per_cta == 128 || o->threads_per_cta == 256)) {
+    sapb::set_last_error("sapb_contact_solve: threads_per_cta must be 0, 128 or 256 (got %d)", o->threads_per_cta);
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   if (o->line_search_variant == SAPB_LS_ARMIJO_DECAY && !(o->rho > 0.0 && o->rho < 1.0)) {

@@ -5,23 +5,25 @@
 
 namespace sapb {
 
-size_t contact_solve_smem_bytes(int n, int C, int hessian_precision) {
-  return make_layout(n, C, hessian_precision == SAPB_FP32 ? 4 : 8).total;
+size_t contact_solve_smem_bytes(int n, int C, int hessian_precision, int threads) {
+  return make_layout(n, C, hessian_precision == SAPB_FP32 ? 4 : 8, (threads > 0 ? threads : 128) / 32).total;
 }
 
 // Resident CTAs per SM of the kernel a problem of this shape launches: the
 // same dispatch with num_envs = 0, which stops at the occupancy query.
 static cudaError_t solve_dispatch(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out);
 
-int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant) {
+int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant, int threads) {
   if (n < 1 || C < 0) return SAPB_ERR_INVALID_ARGUMENT;
   const bool fp32 = hessian_precision == SAPB_FP32;
-  if (contact_solve_smem_bytes(n, C, fp32 ? SAPB_FP32 : SAPB_FP64) > kMaxSmemPerBlock) return SAPB_ERR_UNSUPPORTED;
+  if (contact_solve_smem_bytes(n, C, fp32 ? SAPB_FP32 : SAPB_FP64, threads) > kMaxSmemPerBlock)
+    return SAPB_ERR_UNSUPPORTED;
   SolveParams P;
   memset(&P, 0, sizeof(P));
   P.p.dof_per_env = n;
   P.p.max_contacts = C;
   P.o.line_search_variant = variant;
+  P.o.threads_per_cta = threads;
   int per_sm = 0;
   const cudaError_t err = solve_dispatch(P, fp32, nullptr, &per_sm);
   if (err != cudaSuccess) {
@@ -51,7 +53,10 @@ int ldlt_block_widths(int n, int32_t* out, int capacity) {
 static cudaError_t solve_dispatch(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
   // Kernels specialised on the DOF count of the common trees (humanoid 35,
   // quadruped 18, arm + box 13, single free body 6); a generic one otherwise
-  // and for per-world DOF counts.
+  // and for per-world DOF counts; the generic one with eight warps per world
+  // on request.
+  if (P.o.threads_per_cta == 256)
+    return fp32 ? launch_solve_wide<true>(P, stream, blocks_out) : launch_solve_wide<false>(P, stream, blocks_out);
   if (P.p.dof_count) return launch_solve_ns<0>(P, fp32, stream, blocks_out);
   switch (P.p.dof_per_env) {
 #define SAPB_DISPATCH_N(NV) \
@@ -82,7 +87,8 @@ int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_opt
   // J^T G J assembly and the LDL^T factorization run in FP32; the gradient,
   // costs, line search and convergence test stay FP64 in every variant.
   const bool fp32 = o->hessian_precision == SAPB_FP32 || o->linear_solve_precision == SAPB_FP32;
-  const size_t smem = contact_solve_smem_bytes(p->dof_per_env, p->max_contacts, fp32 ? SAPB_FP32 : SAPB_FP64);
+  const size_t smem =
+      contact_solve_smem_bytes(p->dof_per_env, p->max_contacts, fp32 ? SAPB_FP32 : SAPB_FP64, o->threads_per_cta);
   if (smem > kMaxSmemPerBlock) {
     set_last_error("contact solve: world too large for the on-chip path (shared memory %zu > %zu bytes)", smem,
                    (size_t)kMaxSmemPerBlock);

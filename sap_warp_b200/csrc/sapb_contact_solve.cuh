@@ -45,17 +45,19 @@ __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a -
 // and odd, so thread-per-row reads of J are free of bank conflicts.  ldH odd
 // for conflict-free column reads in the factorization.
 struct Layout {
-  int n, C, ldJ, ldH, nb;
+  int n, C, ldJ, ldH, nb, nw;
   size_t off_J, off_scr, off_H, off_G, off_vec, off_con, off_flags, off_tri, total;
   static constexpr int kVecs = 23;
   static constexpr int kConPer = 17;
-  static constexpr int kMaxWarps = 4;  // partial-sum scratch (blocks of <= 128 threads)
+  static constexpr int kMinWarps = 4;  // partial-sum scratch of at least four warps
 };
 
-__host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
+// warps: of the CTA (the partial-sum scratch holds one row per warp)
+__host__ __device__ inline Layout make_layout(int n, int C, int hsize, int warps = 4) {
   Layout L;
   L.n = n;
   L.C = C;
+  L.nw = warps > Layout::kMinWarps ? warps : Layout::kMinWarps;
   L.ldJ = (n + 3) / 4 * 4 + 1;
   L.ldH = (n % 2 == 0) ? n + 1 : n;
   L.nb = (n + 3) / 4;
@@ -64,7 +66,7 @@ __host__ __device__ inline Layout make_layout(int n, int C, int hsize) {
   o = align_up(o + sizeof(double) * (size_t)3 * C * L.ldJ, 16);
   L.off_scr = o;  // the partial sums of the DOF products, or two staged impulse sets
   {
-    const size_t part = sizeof(double) * 3 * Layout::kMaxWarps * 64;
+    const size_t part = sizeof(double) * 3 * (size_t)L.nw * 64;
     const size_t gam = sizeof(double) * 6 * (size_t)(C > 0 ? C : 1);
     o = align_up(o + (part > gam ? part : gam), 16);
   }
@@ -112,7 +114,7 @@ struct World {
   __device__ double* V(int k) const { return vec + (size_t)k * ldJ(); }
   __device__ double* Cn(int k) const { return con + (size_t)k * L.C; }
   __device__ double* part(int which, int warp) const {
-    return reinterpret_cast<double*>(GJ) + ((size_t)which * Layout::kMaxWarps + warp) * 64;
+    return reinterpret_cast<double*>(GJ) + ((size_t)which * L.nw + warp) * 64;
   }
   __device__ ContactConst cc(int c) const {
     ContactConst x;
@@ -918,7 +920,6 @@ __device__ __forceinline__ void solve_world(const SolveParams& P, const Layout& 
 // autotuner chooses: the best width depends on the DOF count).
 template <int NT, typename HT, int MINB, int NS, int LSV, int LB>
 __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolveParams P) {
-  static_assert(NT / 32 <= Layout::kMaxWarps, "partial-sum scratch sized for kMaxWarps warps");
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[8 * (NT / 32)];
   __shared__ int s_next;
@@ -929,7 +930,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
   // layout); a world's own DOF count may be smaller (dof_count, generic
   // kernel only), its arrays compact at the start of its slots
   const int n_max = NS > 0 ? NS : P.p.dof_per_env, C = P.p.max_contacts;
-  const Layout L = make_layout(n_max, C, (int)sizeof(HT));
+  const Layout L = make_layout(n_max, C, (int)sizeof(HT), NT / 32);
   const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
   build_triangle_list<NT>(reinterpret_cast<uint16_t*>(smem + L.off_tri), n_max);
 
@@ -1022,7 +1023,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
 
 template <int NT, typename HT, int MINB, int NS, int LSV, int LB>
 static cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
-  const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT));
+  const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT), NT / 32);
   auto kern = contact_solve_kernel<NT, HT, MINB, NS, LSV, LB>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (err != cudaSuccess) return err;
@@ -1087,6 +1088,18 @@ template <int NS>
 inline cudaError_t launch_solve_ns(const SolveParams& P, bool fp32, cudaStream_t stream, int* blocks_out) {
   return fp32 ? launch_solve_np<NS, true>(P, stream, blocks_out) : launch_solve_np<NS, false>(P, stream, blocks_out);
 }
+
+// The runtime-size kernel with 256 threads (eight warps) per world, the
+// default LDL^T width: for worlds whose shared memory leaves one or two CTAs
+// per SM (sapb_solve_options.threads_per_cta = 256), instantiated in
+// sapb_solve_nwide_f32.cu / _f64.cu.
+template <bool FP32>
+cudaError_t launch_solve_wide(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
+  using HT = typename std::conditional<FP32, float, double>::type;
+  return launch_solve<256, HT, FP32 ? 2 : 1, 0, LdltBlocks<0>::kW[0]>(P, stream, blocks_out);
+}
+extern template cudaError_t launch_solve_wide<true>(const SolveParams&, cudaStream_t, int*);
+extern template cudaError_t launch_solve_wide<false>(const SolveParams&, cudaStream_t, int*);
 
 #define SAPB_EXTERN_SOLVE(NS)                                                                  \
   extern template cudaError_t launch_solve_np<NS, true>(const SolveParams&, cudaStream_t, int*); \

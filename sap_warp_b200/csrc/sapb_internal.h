@@ -59,8 +59,8 @@ __host__ __device__ inline int body_world_of(const sapb_model_desc& m, int b) {
   return m.body_world ? m.body_world[b] : b / m.bodies_per_world;
 }
 
-size_t contact_solve_smem_bytes(int n, int C, int hessian_precision);
-int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant);
+size_t contact_solve_smem_bytes(int n, int C, int hessian_precision, int threads = 128);
+int32_t contact_solve_occupancy(int n, int C, int hessian_precision, int variant, int threads = 128);
 int ldlt_block_widths(int n, int32_t* out, int capacity);
 int32_t contact_solve_launch(const sapb_contact_problem* p, const sapb_solve_options* o, const sapb_solve_outputs* out,
                              void* workspace, size_t workspace_bytes, cudaStream_t stream);

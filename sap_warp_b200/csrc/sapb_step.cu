@@ -193,7 +193,8 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   const size_t solve_smem = contact_solve_smem_bytes(n, C, opts->solve.hessian_precision == SAPB_FP32 ||
                                                                    opts->solve.linear_solve_precision == SAPB_FP32
                                                                ? SAPB_FP32
-                                                               : SAPB_FP64);
+                                                               : SAPB_FP64,
+                                                       opts->solve.threads_per_cta);
   if (solve_smem > kMaxSmemPerBlock) {
     set_last_error("sapb_create: worlds of %d DOFs and %d contact slots exceed the on-chip solve", n, C);
     return SAPB_ERR_UNSUPPORTED;

@@ -660,12 +660,15 @@ class SapContactSolve:
                             rho=float(rho), line_search_relative_slop=float(line_search_relative_slop))
         return variant, opts
 
-    def _launch_shape(self, P, opts, variant: str, stream, guess: torch.Tensor | None = None) -> tuple[int, int]:
-        """(resident CTAs per SM, LDL^T block width) for this problem: (0, 0)
-        -- the occupancy bound and the default width -- without an
-        autotuner; with one, its choice for the problem's key among every
-        CTA count up to the bound and every width the kernel is built with,
-        timed here on this very problem the first time the key is seen
+    def _launch_shape(self, P, opts, variant: str, stream,
+                      guess: torch.Tensor | None = None) -> tuple[int, int, int]:
+        """(resident CTAs per SM, LDL^T block width, threads per CTA) for this
+        problem: (0, 0, 0) -- the occupancy bound, the default width and
+        kernel -- without an autotuner; with one, its choice for the
+        problem's key among every CTA count up to the bound and every width
+        the kernel is built with, and every CTA count of the 256-thread
+        runtime-size kernel, timed here on this very problem the first time
+        the key is seen
         (never while a graph is being captured: then the defaults).  The solve
         writes its start back into the warm-start guess `guess` (and the
         guess may be the output velocity itself), so the guess is saved
@@ -674,7 +677,7 @@ class SapContactSolve:
         from .autotune import tuning_key
 
         if self.autotuner is None:
-            return 0, 0
+            return 0, 0, 0
         v = self.view
         fp32 = opts.hessian_precision == _abi.SAPB_FP32 or opts.linear_solve_precision == _abi.SAPB_FP32
         if self._device_props is None:
@@ -684,9 +687,10 @@ class SapContactSolve:
                          props.multi_processor_count)
         known = self.autotuner.lookup(key)
         if known is not None:
-            return known if isinstance(known, tuple) else (known, 0)
+            known = known if isinstance(known, tuple) else (known,)
+            return tuple(known) + (0,) * (3 - len(known))
         if torch.cuda.is_current_stream_capturing():
-            return 0, 0
+            return 0, 0, 0
         lib = load()
         occ = int(lib.sapb_contact_solve_occupancy(v.n, int(P.max_contacts),
                                                    _abi.SAPB_FP32 if fp32 else _abi.SAPB_FP64,
@@ -700,7 +704,7 @@ class SapContactSolve:
 
         def time_ms(shape) -> float:
             o = _abi.SolveOptions.from_buffer_copy(opts)
-            o.ctas_per_sm, o.ldlt_block = shape
+            o.ctas_per_sm, o.ldlt_block, o.threads_per_cta = shape
             if saved is not None:
                 guess.copy_(saved)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -712,8 +716,17 @@ class SapContactSolve:
             e1.synchronize()
             return e0.elapsed_time(e1)
 
-        cands = [(k, int(widths[b])) for b in range(nw) for k in range(1, occ + 1)]
-        chosen = self.autotuner.tune(key, cands, time_ms, default=(occ, int(widths[0])))
+        cands = [(k, int(widths[b]), 128) for b in range(nw) for k in range(1, occ + 1)]
+        # the runtime-size kernel with eight warps per world (its default
+        # width), where its shared memory fits
+        occ_wide = int(lib.sapb_contact_solve_occupancy_threads(v.n, int(P.max_contacts),
+                                                                _abi.SAPB_FP32 if fp32 else _abi.SAPB_FP64,
+                                                                int(opts.line_search_variant), 256))
+        if occ_wide >= 1:
+            gw = (ctypes.c_int32 * 8)()
+            lib.sapb_contact_solve_ldlt_blocks(1, gw, 8)  # the runtime-size kernel's widths
+            cands += [(k, int(gw[0]), 256) for k in range(1, occ_wide + 1)]
+        chosen = self.autotuner.tune(key, cands, time_ms, default=(occ, int(widths[0]), 128))
         if saved is not None:
             guess.copy_(saved)
         return chosen
@@ -806,7 +819,8 @@ class SapContactSolve:
             P.dof = ctypes.pointer(self.dof)
         stream = ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream)
         opts.skip_plain_start = 1 if skip_plain_start else 0
-        opts.ctas_per_sm, opts.ldlt_block = self._launch_shape(P, opts, variant, stream, v_guess)
+        opts.ctas_per_sm, opts.ldlt_block, opts.threads_per_cta = self._launch_shape(P, opts, variant, stream,
+                                                                                      v_guess)
         status = load().sapb_contact_solve(ctypes.byref(P), ctypes.byref(opts), ctypes.byref(self.outputs),
                                            self.workspace.data_ptr(), self.workspace.numel(), stream)
         check(status, "sapb_contact_solve")

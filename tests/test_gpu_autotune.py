@@ -1,7 +1,8 @@
-"""The dense solve's launch shape (resident CTAs per SM) and LDL^T block
-width on the GPU: the occupancy bound, results independent of the CTA
-count (bit for bit) and of the block width (to the solve's tolerance), and
-SolverSAP's autotuner timing the candidates on its first solve."""
+"""The dense solve's launch shape (resident CTAs per SM), LDL^T block width
+and threads per world on the GPU: the occupancy bound, results independent
+of the CTA count (bit for bit), of the block width and of the 256-thread
+kernel (to the solve's tolerance), and SolverSAP's autotuner timing the
+candidates on its first solve."""
 
 import ctypes
 import json
@@ -25,6 +26,12 @@ def test_occupancy_bound(cuda_device):
     fp64 = lib.sapb_contact_solve_occupancy(35, 32, _abi.SAPB_FP64, _abi.LINE_SEARCH_VARIANTS["armijo_decay"])
     assert 1 <= fp64 <= fp32 <= 8
     assert lib.sapb_contact_solve_occupancy(35, 32, _abi.SAPB_FP64, 99) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    armijo = _abi.LINE_SEARCH_VARIANTS["armijo_decay"]
+    assert lib.sapb_contact_solve_occupancy_threads(35, 32, _abi.SAPB_FP32, armijo, 128) == fp32
+    wide = lib.sapb_contact_solve_occupancy_threads(35, 32, _abi.SAPB_FP32, armijo, 256)
+    assert 1 <= wide <= fp32
+    assert lib.sapb_contact_solve_occupancy_threads(35, 32, _abi.SAPB_FP32, armijo, 64) == \
+        _abi.SAPB_ERR_INVALID_ARGUMENT
 
 
 def test_results_do_not_depend_on_the_launch_shape(cuda_device):
@@ -73,9 +80,15 @@ def test_solver_autotune_writes_its_choice(cuda_device, tmp_path):
     widths = (ctypes.c_int32 * 8)()
     nw = load().sapb_contact_solve_ldlt_blocks(35, widths, 8)
     assert nw >= 2 and widths[0] == 5
-    assert set(entry["ms"]) == {f"{k},{widths[b]}" for b in range(nw) for k in range(1, occ + 1)}
-    k, b = entry["choice"]
-    assert 1 <= k <= occ and b in list(widths)[:nw] and entry["ctas_per_sm"] == k
+    armijo = _abi.LINE_SEARCH_VARIANTS["armijo_decay"]
+    occ_wide = load().sapb_contact_solve_occupancy_threads(35, 32, _abi.SAPB_FP32, armijo, 256)
+    gw = (ctypes.c_int32 * 8)()
+    load().sapb_contact_solve_ldlt_blocks(1, gw, 8)
+    assert set(entry["ms"]) == ({f"{k},{widths[b]},128" for b in range(nw) for k in range(1, occ + 1)}
+                                | {f"{k},{gw[0]},256" for k in range(1, occ_wide + 1)})
+    k, b, nt = entry["choice"]
+    assert entry["ctas_per_sm"] == k and ((nt == 128 and 1 <= k <= occ and b in list(widths)[:nw])
+                                          or (nt == 256 and 1 <= k <= occ_wide and b == gw[0]))
     assert all(np.isfinite(float(v)) and float(v) > 0 for v in entry["ms"].values())
 
 
@@ -128,3 +141,36 @@ def test_every_ldlt_block_width_reaches_the_tolerance(cuda_device, oracle):
             n = prob.dof_per_env
             err = np.abs(buf.v.cpu().numpy() - ref["v"]).reshape(-1, n).max(1) / np.abs(ref["v"]).reshape(-1, n).max(1)
             assert np.quantile(err, 0.98) <= 1e-6 and err.max() <= 1e-4, (prec, b, err.max())
+
+
+@pytest.mark.parametrize("kind", ["humanoid", "mixed"])
+def test_wide_kernel_matches_the_oracle(cuda_device, oracle, kind):
+    """The 256-thread runtime-size kernel (threads_per_cta = 256) solves to
+    the same tolerance as the default kernel: against the FP64 oracle on the
+    humanoid batch and on the uneven batch with per-world DOF counts, in both
+    precisions; CTA counts do not change a bit."""
+    if kind == "humanoid":
+        prob = scenes.humanoid_contact_problem(256, seed=85)
+        gpu_prob, extra = prob, {}
+    else:
+        prob, _ = scenes.mixed_contact_problem(384, seed=86)  # padded: the oracle's input
+        gpu_prob = scenes.compact_problem(prob)
+        extra = {"dof_count": torch.as_tensor(gpu_prob.dofs_active, dtype=torch.int32, device=cuda_device)}
+    ref = oracle.solve(prob, "armijo_decay")
+    t = problem_to_device(gpu_prob, cuda_device)
+    n = prob.dof_per_env
+    for prec in ("fp64", "fp32"):
+        outs = []
+        for k in (0, 1):
+            buf = ContactSolveBuffers(prob.num_envs, n, prob.max_contacts, cuda_device)
+            contact_solve(**t, **extra, buffers=buf, options=make_options(
+                "armijo_decay", hessian_precision=prec, linear_solve_precision=prec, threads_per_cta=256,
+                ctas_per_sm=k))
+            torch.cuda.synchronize()
+            outs.append(buf.v.clone())
+            assert bool(buf.converged.all()), (kind, prec)
+        assert torch.equal(outs[0], outs[1])
+        got = outs[0].cpu().numpy().reshape(-1, n)
+        want = ref["v"].reshape(-1, n)
+        err = np.abs(got - want).max(1) / np.maximum(np.abs(want).max(1), 1e-30)
+        assert np.quantile(err, 0.98) <= 1e-6 and err.max() <= 1e-4, (kind, prec, err.max())
