@@ -34,8 +34,12 @@ def _nvcc() -> str:
     return cand
 
 
+# The units that take longest to compile start first.
+_HEAVY = ("sapb_solve_ngeneric", "sapb_solve_nwide", "sapb_blocked_solve", "sapb_mlp", "sapb_solve_n35")
+
+
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    return sorted(CSRC.glob("*.cu"), key=lambda p: (not p.stem.startswith(_HEAVY), p.name))
 
 
 def needs_build() -> bool:

@@ -1022,7 +1022,7 @@ __global__ void __launch_bounds__(NT, MINB) contact_solve_kernel(const SolvePara
 }
 
 template <int NT, typename HT, int MINB, int NS, int LSV, int LB>
-static cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
+cudaError_t launch_solve_ls(const SolveParams& P, cudaStream_t stream, int* blocks_out) {
   const Layout L = make_layout(P.p.dof_per_env, P.p.max_contacts, (int)sizeof(HT), NT / 32);
   auto kern = contact_solve_kernel<NT, HT, MINB, NS, LSV, LB>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
@@ -1100,6 +1100,21 @@ cudaError_t launch_solve_wide(const SolveParams& P, cudaStream_t stream, int* bl
 }
 extern template cudaError_t launch_solve_wide<true>(const SolveParams&, cudaStream_t, int*);
 extern template cudaError_t launch_solve_wide<false>(const SolveParams&, cudaStream_t, int*);
+
+// The runtime-size kernels (128 and 256 threads) are the largest: each line
+// search's kernel is instantiated in a translation unit of its own
+// (sapb_solve_n{generic,wide}_f{32,64}_{armijo,exact,monotone}.cu).
+#define SAPB_RUNTIME_SIZE_KERNELS(X, LSV)                                         \
+  X(128, float, 4, 0, LSV, LdltBlocks<0>::kW[0])                                \
+  X(128, double, 3, 0, LSV, LdltBlocks<0>::kW[0])                               \
+  X(256, float, 2, 0, LSV, LdltBlocks<0>::kW[0])                                \
+  X(256, double, 1, 0, LSV, LdltBlocks<0>::kW[0])
+#define SAPB_EXTERN_LS(NT, HT, MINB, NS, LSV, LB) \
+  extern template cudaError_t launch_solve_ls<NT, HT, MINB, NS, LSV, LB>(const SolveParams&, cudaStream_t, int*);
+SAPB_RUNTIME_SIZE_KERNELS(SAPB_EXTERN_LS, SAPB_LS_ARMIJO_DECAY)
+SAPB_RUNTIME_SIZE_KERNELS(SAPB_EXTERN_LS, SAPB_LS_EXACT_ROOT)
+SAPB_RUNTIME_SIZE_KERNELS(SAPB_EXTERN_LS, SAPB_LS_MONOTONE_DECAY)
+#undef SAPB_EXTERN_LS
 
 #define SAPB_EXTERN_SOLVE(NS)                                                                  \
   extern template cudaError_t launch_solve_np<NS, true>(const SolveParams&, cudaStream_t, int*); \
