@@ -113,7 +113,9 @@ typedef struct sapb_solve_options {
   int32_t threads_per_cta;        /* threads of one world's CTA in the dense solve: 0 or 128 the default (the
                                    * kernel specialised on the DOF count), 256 the runtime-size kernel with
                                    * eight warps per world (for worlds whose shared memory leaves one or two
-                                   * CTAs per SM); results do not depend on it beyond rounding */
+                                   * CTAs per SM); in the tree-blocked solve 128 or 256, 0 picking 128 for
+                                   * worlds of up to 128 padded DOFs (T * tree_dofs) and 256 beyond; results
+                                   * do not depend on it beyond rounding */
 } sapb_solve_options;
 
 /* Per-DOF drive and limit model (the arrays SapContactSolve.prepare reads,

@@ -35,7 +35,7 @@ def _nvcc() -> str:
 
 
 # The units that take longest to compile start first.
-_HEAVY = ("sapb_solve_ngeneric", "sapb_solve_nwide", "sapb_blocked_solve", "sapb_mlp", "sapb_solve_n35")
+_HEAVY = ("sapb_solve_ngeneric", "sapb_solve_nwide", "sapb_blocked_nb", "sapb_mlp", "sapb_solve_n35")
 
 
 def sources() -> list[Path]:
