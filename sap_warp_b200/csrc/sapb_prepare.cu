@@ -25,6 +25,10 @@
 namespace sapb {
 
 constexpr int kPrepNT = 128;
+// per-contact scratch of the free-motion kernel: witness points x0, x1 (3
+// each), then the contact frame (9)
+constexpr int kConStride = 15;
+constexpr int kConFrame = 6;
 
 struct PrepParams {
   sapb_model_desc m;
@@ -65,7 +69,6 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, int tb) {
   };
   L.pose = take(sizeof(double) * 8 * B);    // p 3, q 4 (pointer-jumping buffer A)
   L.pose2 = take(sizeof(double) * 8 * B);   // buffer B
-  L.fm = take(sizeof(double) * 8 * B);      // X_FM of the body's joint
   L.vj = take(sizeof(double) * 6 * B);      // joint velocity S q_dot
   L.cb = take(sizeof(double) * 6 * B);      // joint bias acceleration
   L.vb = take(sizeof(double) * 6 * B);      // body velocity
@@ -75,8 +78,15 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, int tb) {
   L.S = take(sizeof(double) * 6 * n);       // motion subspace columns
   L.F = take(sizeof(double) * 6 * n);       // composite inertia times S
   L.vec = take(sizeof(double) * 4 * n);     // tau, vdot, diag(A), 1/d
-  L.H = take(sizeof(double) * (blk ? (size_t)tb * tb * B : (size_t)n * n));  // A (tree blocks when blocked)
-  L.con = take(sizeof(double) * 21 * Cc);   // per contact: x0 3, x1 3, -, -, frame 9
+  // A (tree blocks when blocked); before A is formed, X_FM of each body's
+  // joint (8 per body) lives in the same bytes
+  {
+    const size_t hb = sizeof(double) * (blk ? (size_t)tb * tb * B : (size_t)n * n);
+    const size_t fb = sizeof(double) * 8 * B;
+    L.H = take(hb > fb ? hb : fb);
+    L.fm = L.H;
+  }
+  L.con = take(sizeof(double) * kConStride * Cc);  // per contact: x0 3, x1 3, frame 9
   L.conint = take(sizeof(int) * 2 * Cc);    // local bodies lb0, lb1
   L.anc = take(sizeof(uint64_t) * 2 * B);   // ancestor-or-self masks (two buffers; then bodies by depth)
   L.jmp = take(sizeof(int) * 2 * B);        // pointer-jumping parents (two buffers)
@@ -210,7 +220,7 @@ __device__ __forceinline__ void pose_store(double* p, Xf x) {
 // VS: the candidate start velocity is written (v_start; a separate
 // instantiation keeps its registers off the plain path).
 template <bool VS>
-__global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepParams P) {
+__global__ void __launch_bounds__(kPrepNT, 6) prepare_world_kernel(const PrepParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x;
   const int e = blockIdx.x;
@@ -743,11 +753,11 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     if (P.out.point) store3(P.out.point + 3 * ci, pC);
     if (P.out.frame)
       for (int k = 0; k < 9; ++k) P.out.frame[9 * ci + k] = F[k];
-    double* cs = con + 21 * (size_t)c;
+    double* cs = con + kConStride * (size_t)c;
     const bool mid = P.o.contact_point_mode == SAPB_POINT_MIDPOINT;
     store3(cs + 0, mid ? pC : x0);
     store3(cs + 3, mid ? pC : x1);
-    for (int k = 0; k < 9; ++k) cs[12 + k] = F[k];
+    for (int k = 0; k < 9; ++k) cs[kConFrame + k] = F[k];
     conint[2 * c] = (lb0 >= 0 && lb0 < B) ? lb0 : -1;
     conint[2 * c + 1] = (lb1 >= 0 && lb1 < B) ? lb1 : -1;
   }
@@ -783,7 +793,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     double jgr0 = 0.0, jgr1 = 0.0;
     const double h = P.in.dt[e];
     for (int c = warp; c < cc; c += kPrepNT / 32) {
-      const double* cs = con + 21 * (size_t)c;
+      const double* cs = con + kConStride * (size_t)c;
       const int lb0 = conint[2 * c], lb1 = conint[2 * c + 1];
       int t0 = -1, t1 = -1;
       if (blk) {
@@ -817,7 +827,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
         }
         double rw[3];
         for (int r = 0; r < 3; ++r) {
-          rw[r] = dot(load3(cs + 12 + 3 * r), rel);
+          rw[r] = dot(load3(cs + kConFrame + 3 * r), rel);
           Jout[((size_t)c * 3 + r) * ncols + col] = rw[r];
         }
         if (dof < 0) continue;
@@ -879,7 +889,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
     const size_t ci = (size_t)e * C + c;
     double w = 0.0;
     {
-      const double* cs = con + 21 * (size_t)c;
+      const double* cs = con + kConStride * (size_t)c;
       const int lbs[2] = {conint[2 * c], conint[2 * c + 1]};
       // body-inertia weights use the witnesses, whatever the point mode
       const int src = P.env_src[ci];
@@ -897,7 +907,7 @@ __global__ void __launch_bounds__(kPrepNT, 5) prepare_world_kernel(const PrepPar
         const double* Ic = P.m.body_inertia + 9 * (size_t)(b0g + lb);
         const double ix = fmax(Ic[0], 1.0e-12), iy = fmax(Ic[4], 1.0e-12), iz = fmax(Ic[8], 1.0e-12);
         for (int d = 0; d < 3; ++d) {
-          const V3 cb = qrot(qconj(qq), cross(r, load3(cs + 12 + 3 * d)));
+          const V3 cb = qrot(qconj(qq), cross(r, load3(cs + kConFrame + 3 * d)));
           wsum += 1.0 / mass + cb.x * cb.x / ix + cb.y * cb.y / iy + cb.z * cb.z / iz;
         }
       }
