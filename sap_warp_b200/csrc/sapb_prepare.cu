@@ -69,24 +69,30 @@ __host__ __device__ inline PrepLayout prep_layout(int B, int n, int C, int tb) {
   };
   L.pose = take(sizeof(double) * 8 * B);    // p 3, q 4 (pointer-jumping buffer A)
   L.pose2 = take(sizeof(double) * 8 * B);   // buffer B
-  L.vj = take(sizeof(double) * 6 * B);      // joint velocity S q_dot
-  L.cb = take(sizeof(double) * 6 * B);      // joint bias acceleration
-  L.vb = take(sizeof(double) * 6 * B);      // body velocity
-  L.fb = take(sizeof(double) * 6 * B);      // body force
-  L.ib = take(sizeof(double) * 10 * B);     // inertia: m, h = m c, I_O (xx yy zz xy xz yz)
-  L.fs = take(sizeof(double) * 16 * B);     // subtree force 6 + composite inertia 10
+  // The body arrays, dead once tau and the F columns are formed; A (tree
+  // blocks when blocked) is formed after that and takes their bytes
+  {
+    const size_t body = (size_t)50 * B;  // vj 6, cb 6, vb 6, fb 6, ib 10, fs 16 per body
+    const size_t h = blk ? (size_t)tb * tb * B : (size_t)n * n;
+    const size_t at = take(sizeof(double) * (body > h ? body : h));
+    L.vj = at;                                 // joint velocity S q_dot
+    L.cb = at + sizeof(double) * 6 * B;        // joint bias acceleration
+    L.vb = at + sizeof(double) * 12 * B;       // body velocity
+    L.fb = at + sizeof(double) * 18 * B;       // body force
+    L.ib = at + sizeof(double) * 24 * B;       // inertia: m, h = m c, I_O (xx yy zz xy xz yz)
+    L.fs = at + sizeof(double) * 34 * B;       // subtree force 6 + composite inertia 10
+    L.H = at;
+  }
   L.S = take(sizeof(double) * 6 * n);       // motion subspace columns
   L.F = take(sizeof(double) * 6 * n);       // composite inertia times S
   L.vec = take(sizeof(double) * 4 * n);     // tau, vdot, diag(A), 1/d
-  // A (tree blocks when blocked); before A is formed, X_FM of each body's
-  // joint (8 per body) lives in the same bytes
+  // per contact: x0 3, x1 3, frame 9; before the contacts are set up, X_FM
+  // of each body's joint (8 per body) lives in the same bytes
   {
-    const size_t hb = sizeof(double) * (blk ? (size_t)tb * tb * B : (size_t)n * n);
-    const size_t fb = sizeof(double) * 8 * B;
-    L.H = take(hb > fb ? hb : fb);
-    L.fm = L.H;
+    const size_t con = (size_t)kConStride * Cc, fm = (size_t)8 * B;
+    L.con = take(sizeof(double) * (con > fm ? con : fm));
+    L.fm = L.con;
   }
-  L.con = take(sizeof(double) * kConStride * Cc);  // per contact: x0 3, x1 3, frame 9
   L.conint = take(sizeof(int) * 2 * Cc);    // local bodies lb0, lb1
   L.anc = take(sizeof(uint64_t) * 2 * B);   // ancestor-or-self masks (two buffers; then bodies by depth)
   L.jmp = take(sizeof(int) * 2 * B);        // pointer-jumping parents (two buffers)
@@ -220,7 +226,7 @@ __device__ __forceinline__ void pose_store(double* p, Xf x) {
 // VS: the candidate start velocity is written (v_start; a separate
 // instantiation keeps its registers off the plain path).
 template <bool VS>
-__global__ void __launch_bounds__(kPrepNT, 6) prepare_world_kernel(const PrepParams P) {
+__global__ void __launch_bounds__(kPrepNT, 7) prepare_world_kernel(const PrepParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x;
   const int e = blockIdx.x;
