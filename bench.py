@@ -598,7 +598,8 @@ def main():
     uneven_step = {"worlds": UW, "dofs": "13 (arm+box) / 18 / 35, each world its own count (no padding)",
                    "contacts": "8-32 ground contacts per world", "timing": "graph of two steps, replayed"}
     for label, prec, warm in (("plain_fp64", "fp64", "previous_velocity"),
-                              ("previous_impulses_fp32", "fp32", "previous_impulses")):
+                              ("previous_impulses_fp32", "fp32", "previous_impulses"),
+                              ("learned_fp32", "fp32", "learned")):
         usolver = SolverSAP(umodel, max_rigid_contact=MAX_CONTACTS, contact_preset_variant="drake",
                             hessian_precision=prec, warm_start=warm)
         ua = SapState(joint_q=ustate.joint_q.clone(), joint_qd=ustate.joint_qd.clone(), body_q=ustate.body_q.clone(),
