@@ -271,6 +271,40 @@ def oracle_errors(dev) -> dict:
         torch.cuda.synchronize()
         row[prec] = rel(buf.v.cpu().numpy(), ref["v"], boxes.dof_per_env)
     out["boxes_384dof"] = row
+    # worlds of an arm gripping one of 8 boxes, whole-step free motion and
+    # rows on the GPU in the tree-blocked layout (trees of 7 and 6 DOFs) ->
+    # the blocked solve, against the oracle's free motion, rows and dense
+    # solve of the same step
+    from sap_warp_b200 import models
+    from sap_warp_b200.runtime import SapState
+    from sap_warp_b200.solver import SolverSAP
+
+    W, C = 64, 112
+    model, state, control, con, host, hv = models.box_scene(W, SEED + 21, dev, boxes=8, sites=(3, 5), arm=True)
+    hm = oracle.HostModel(hv["tpl"], hv["g"])
+    dt = np.full(W, DT)
+    r = oracle.free_motion_contacts(hm, hv["q"], hv["qd"], host, dt, C, point_mode="contact_midpoint",
+                                    weight_mode="diag_delassus")
+    tds = np.concatenate([[0], 7 + 6 * np.arange(9)]).astype(np.int32)
+    bstart = np.concatenate([np.zeros(7, np.int32), tds[1:-1]])
+    bcount = np.concatenate([np.full(7, 7, np.int32), np.full(8, 6, np.int32)])
+    prob = scenes.ContactProblemArrays(
+        num_envs=W, dof_per_env=55, max_contacts=C, bodies_per_env=15,
+        contact_count=np.minimum(r["count"], C).astype(np.int32), dynamics_matrix=r["A"], jacobian=r["jac"],
+        phi0=r["phi0"], w_eff=r["w"], mu=r["mu"], stiffness=r["k"], tau_d=r["tau"], body0=r["body0"],
+        body1=r["body1"], body_dof_start=np.tile(bstart, W), body_dof_count=np.tile(bcount, W),
+        v_star=r["v_star"].reshape(-1), v0=hv["qd"].reshape(-1), dt=dt)
+    ref = oracle.solve(prob, "armijo_decay")
+    row = {}
+    for prec in ("fp64", "fp32"):
+        solver = SolverSAP(model, max_rigid_contact=C, contact_preset_variant="drake", contact_tau_d=0.0,
+                           tree_blocked=True, hessian_precision=prec)
+        out_state = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(),
+                             body_q=state.body_q.clone(), body_f=state.body_f.clone())
+        solver.step(state, out_state, control, con, DT)
+        torch.cuda.synchronize()
+        row[prec] = rel(solver.last_contact_solve_result.v_flat.cpu().numpy(), ref["v"], 55)
+    out["arm_8_boxes_55dof_tree_blocked"] = row
     return out
 
 
