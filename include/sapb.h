@@ -494,7 +494,10 @@ typedef struct sapb_handle sapb_handle;
 #define SAPB_WORK_ORDER_PREVIOUS_ITERATIONS 1  /* most Newton iterations of the last step first */
 
 typedef struct sapb_step_options {
-  sapb_prepare_options prepare;     /* max_contacts, weight / point modes, fallbacks; tree_blocked = 0 */
+  sapb_prepare_options prepare;     /* max_contacts, weight / point modes, fallbacks; tree_blocked: the
+                                     * tree-blocked layout and solve (the trees are world 0's articulations,
+                                     * tree_dofs 0: the smallest block holding them; no drive or limit
+                                     * terms) */
   sapb_solve_options solve;         /* the contact solve's options (line search, precisions, tolerances) */
   int32_t position_integration;     /* SAPB_INTEGRATE_SAP_EULER / SAPB_INTEGRATE_MIDPOINT */
   int32_t warm_start;               /* SAPB_WARM_START_* */

@@ -92,6 +92,13 @@ struct sapb_handle {
   int32_t *body_dof_start, *body_dof_count;
   void* solve_ws;
   size_t solve_ws_bytes;
+  // tree-blocked layout (opts.prepare.tree_blocked): T trees (the
+  // articulations) in blocks of NB DOFs, their first DOFs, A's tree blocks
+  // and the tree of each contact side
+  bool blk;
+  int32_t T, NB;
+  int32_t *tree_dof_start, *contact_tree;
+  double* tree_mass;
 };
 
 extern "C" {
@@ -146,7 +153,8 @@ void sapb_destroy(sapb_handle* h) {
                   h->v,         h->gamma,     h->gamma_prev, h->cost, h->grad_norm, h->mode, h->iters, h->ls_iters, h->converged, h->status,
                   h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws,
                   h->key_shape, h->key_count, h->has_history, h->key_point,
-                  h->gamma_older, h->gamma_start, h->v_start};
+                  h->gamma_older, h->gamma_start, h->v_start, h->tree_dof_start, h->contact_tree,
+                  h->tree_mass};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -170,10 +178,6 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     set_last_error("sapb_create: the handle takes equal per-world blocks");
     return SAPB_ERR_UNSUPPORTED;
   }
-  if (opts->prepare.tree_blocked) {
-    set_last_error("sapb_create: the handle runs the dense layout (tree_blocked must be 0)");
-    return SAPB_ERR_UNSUPPORTED;
-  }
   if (opts->position_integration != SAPB_INTEGRATE_SAP_EULER && opts->position_integration != SAPB_INTEGRATE_MIDPOINT) {
     set_last_error("sapb_create: position_integration must be SAPB_INTEGRATE_SAP_EULER or _MIDPOINT");
     return SAPB_ERR_INVALID_ARGUMENT;
@@ -190,11 +194,10 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     set_last_error("sapb_create: work_order by previous iterations supports at most %d worlds", kOrderMaxWorlds);
     return SAPB_ERR_UNSUPPORTED;
   }
-  const size_t solve_smem = contact_solve_smem_bytes(n, C, opts->solve.hessian_precision == SAPB_FP32 ||
-                                                                   opts->solve.linear_solve_precision == SAPB_FP32
-                                                               ? SAPB_FP32
-                                                               : SAPB_FP64,
-                                                       opts->solve.threads_per_cta);
+  const bool blk = opts->prepare.tree_blocked != 0;
+  const bool fp32 = opts->solve.hessian_precision == SAPB_FP32 || opts->solve.linear_solve_precision == SAPB_FP32;
+  const size_t solve_smem =
+      blk ? 0 : contact_solve_smem_bytes(n, C, fp32 ? SAPB_FP32 : SAPB_FP64, opts->solve.threads_per_cta);
   if (solve_smem > kMaxSmemPerBlock) {
     set_last_error("sapb_create: worlds of %d DOFs and %d contact slots exceed the on-chip solve", n, C);
     return SAPB_ERR_UNSUPPORTED;
@@ -231,10 +234,40 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
       }
     }
   }
+  // tree-blocked layout: the trees are world 0's articulations (every world
+  // alike), each a contiguous DOF range within the block size
+  const int32_t Aw = model->articulations_per_world;
+  std::vector<int32_t> tds;
+  int32_t NB = 0;
+  if (blk) {
+    tds.resize(Aw + 1);
+    int largest = 0;
+    bool ok = model->bodies_per_world <= 64 && Aw >= 1 && Aw <= 64;
+    for (int t = 0; ok && t <= Aw; ++t) {
+      tds[t] = t < Aw ? qd_start[art[t]] : n;
+      if (t > 0) {
+        ok = tds[t] >= tds[t - 1];
+        largest = tds[t] - tds[t - 1] > largest ? tds[t] - tds[t - 1] : largest;
+      }
+    }
+    ok = ok && tds[0] == 0;
+    NB = opts->prepare.tree_dofs > 0 ? opts->prepare.tree_dofs : blocked_tree_block(largest);
+    if (!ok || NB < 1 || blocked_tree_block(NB) != NB || largest > NB ||
+        (Aw > 1 && blocked_fill_capacity(Aw, NB, C, fp32) < 1)) {
+      set_last_error("sapb_create: the tree-blocked layout needs <= 64 bodies and articulations per world, each "
+                     "articulation in one block of 6, 7 or 12 DOFs (largest %d, tree_dofs %d), and the worlds' "
+                     "factor on chip", largest, opts->prepare.tree_dofs);
+      return SAPB_ERR_UNSUPPORTED;
+    }
+  }
   sapb_handle* h = new sapb_handle;
   memset(h, 0, sizeof(*h));
   h->model = *model;
   h->opts = *opts;
+  h->blk = blk;
+  h->T = blk ? Aw : 0;
+  h->NB = NB;
+  if (blk) h->opts.prepare.tree_dofs = NB;
   if (h->opts.impulse_history == 0) h->opts.impulse_history = 3;
   h->W = W;
   h->n = n;
@@ -249,8 +282,15 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   };
   take(dev_alloc(&h->v_star, Wn));
   take(dev_alloc(&h->vdot, Wn));
-  take(dev_alloc(&h->A, Wn * n));
-  take(dev_alloc(&h->J, WC * 3 * n));
+  if (blk) {
+    take(dev_alloc(&h->tree_mass, (size_t)W * h->T * NB * NB));
+    take(dev_alloc(&h->contact_tree, WC * 2));
+    take(dev_alloc(&h->tree_dof_start, (size_t)h->T + 1));
+    take(dev_alloc(&h->J, WC * 3 * 2 * NB));
+  } else {
+    take(dev_alloc(&h->A, Wn * n));
+    take(dev_alloc(&h->J, WC * 3 * n));
+  }
   take(dev_alloc(&h->phi0, WC));
   take(dev_alloc(&h->w_eff, WC));
   take(dev_alloc(&h->mu, WC));
@@ -261,7 +301,7 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   take(dev_alloc(&h->body1, WC));
   take(dev_alloc(&h->truncated, 1));
   if (cand) {
-    take(dev_alloc(&h->v_start, Wn));
+    if (!blk) take(dev_alloc(&h->v_start, Wn));  // the tree-blocked solve forms its candidate itself
     take(dev_alloc(&h->gamma_prev, WC * 3));
     take(dev_alloc(&h->key_shape, WC * 2));
     take(dev_alloc(&h->key_point, WC * 3));
@@ -285,13 +325,15 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   take(dev_alloc(&h->body_dof_start, B));
   take(dev_alloc(&h->body_dof_count, B));
   h->prep_ws_bytes = sapb_prepare_workspace_size(model, C);
-  h->solve_ws_bytes = sapb_contact_solve_workspace_size(W, n, C);
+  h->solve_ws_bytes = blk ? sapb_blocked_solve_workspace_size(W, h->T, C) : sapb_contact_solve_workspace_size(W, n, C);
   if (err == cudaSuccess) err = cudaMalloc(&h->prep_ws, h->prep_ws_bytes > 0 ? h->prep_ws_bytes : 16);
   if (err == cudaSuccess) err = cudaMalloc(&h->solve_ws, h->solve_ws_bytes > 0 ? h->solve_ws_bytes : 16);
   if (err == cudaSuccess)
     err = cudaMemcpy(h->body_dof_start, bstart.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice);
   if (err == cudaSuccess)
     err = cudaMemcpy(h->body_dof_count, bcount.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess && blk)
+    err = cudaMemcpy(h->tree_dof_start, tds.data(), sizeof(int32_t) * (h->T + 1), cudaMemcpyHostToDevice);
   if (err == cudaSuccess) err = cudaMemset(h->guess_flag, 0, sizeof(int32_t));
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_prev, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess && cand) err = cudaMemset(h->key_count, 0, sizeof(int32_t) * W);
@@ -330,7 +372,9 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   memset(&po, 0, sizeof(po));
   po.v_star = h->v_star;
   po.vdot = h->vdot;
-  po.dynamics_matrix = h->A;
+  po.dynamics_matrix = h->A;  // NULL in the tree-blocked layout
+  po.tree_mass = h->tree_mass;
+  po.contact_tree = h->contact_tree;
   po.jacobian = h->J;
   po.contact_count = h->count;
   po.phi0 = h->phi0;
@@ -357,11 +401,57 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     hist.gamma_older = h->gamma_older;
     hist.gamma_start = h->gamma_start;
     po.history = &hist;
-    po.v_start = h->v_start;
+    po.v_start = h->v_start;  // NULL in the tree-blocked layout
   }
   int32_t st = sapb_free_motion_contacts(&h->model, &io->in, &h->opts.prepare, &po, h->prep_ws, h->prep_ws_bytes,
                                          stream);
   if (st != SAPB_OK) return st;
+  sapb_solve_outputs so;
+  memset(&so, 0, sizeof(so));
+  so.v = h->v;
+  so.contact_gamma = h->gamma;
+  so.contact_mode = h->mode;
+  so.cost = h->cost;
+  so.newton_iterations = h->iters;
+  so.line_search_iterations = h->ls_iters;
+  so.converged = h->converged;
+  so.status = h->status;
+  so.grad_norm = h->grad_norm;
+  so.warm_start_accepted = h->ws_accepted;
+  if (h->blk) {
+    // the tree-blocked solve: the same Newton loop on A's tree blocks, the
+    // history's start impulses as its candidate
+    if (io->dof && (io->dof->has_pd || io->dof->has_limits)) {
+      set_last_error("sapb_step: the tree-blocked layout takes no drive or limit terms");
+      return SAPB_ERR_UNSUPPORTED;
+    }
+    sapb_blocked_problem bp;
+    memset(&bp, 0, sizeof(bp));
+    bp.num_envs = h->W;
+    bp.trees_per_env = h->T;
+    bp.tree_dofs = h->NB;
+    bp.max_contacts = h->C;
+    bp.contact_count = h->count;
+    bp.tree_mass = h->tree_mass;
+    bp.jacobian = h->J;
+    bp.contact_tree = h->contact_tree;
+    bp.phi0 = h->phi0;
+    bp.w_eff = h->w_eff;
+    bp.mu = h->mu;
+    bp.stiffness = h->stiffness;
+    bp.tau_d = h->tau_d;
+    bp.v_star = h->v_star;
+    bp.v0 = io->in.joint_qd;
+    bp.v_guess = h->v;
+    bp.v_guess_active = h->guess_flag;
+    bp.dt = io->in.dt;
+    bp.world_order = order ? h->order : nullptr;
+    bp.gamma0 = cand ? h->gamma_start : nullptr;
+    bp.gamma0_count = cand ? 1 : 0;
+    bp.tree_dof_start = h->tree_dof_start;
+    bp.dofs_per_world = h->n;
+    st = sapb_blocked_contact_solve(&bp, &h->opts.solve, &so, h->solve_ws, h->solve_ws_bytes, stream);
+  } else {
   // contact solve (sim/solver_sap.py:1434-1460), warm start from the last
   // solution once a step has run
   sapb_contact_problem p;
@@ -401,19 +491,8 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     p.v_candidate_count = 1;
   }
   p.world_order = order ? h->order : nullptr;
-  sapb_solve_outputs so;
-  memset(&so, 0, sizeof(so));
-  so.v = h->v;
-  so.contact_gamma = h->gamma;
-  so.contact_mode = h->mode;
-  so.cost = h->cost;
-  so.newton_iterations = h->iters;
-  so.line_search_iterations = h->ls_iters;
-  so.converged = h->converged;
-  so.status = h->status;
-  so.grad_norm = h->grad_norm;
-  so.warm_start_accepted = h->ws_accepted;
   st = sapb_contact_solve(&p, &h->opts.solve, &so, h->solve_ws, h->solve_ws_bytes, stream);
+  }
   if (st != SAPB_OK) return st;
   if (order) {
     st = sapb_world_order(h->iters, h->W, h->order, stream);

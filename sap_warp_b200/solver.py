@@ -1133,8 +1133,6 @@ class SolverSAP:
         options, integrator, warm start (previous velocity or previous
         impulses, with the same impulse history) and work order, so a C host stepping the same model gets
         the same trajectory."""
-        if self.contact_solve.tree_blocked:
-            raise NotImplementedError("the C step handle runs the dense layout")
         if self.warm_start == "learned":
             raise NotImplementedError("the C step handle takes the previous-velocity or previous-impulses warm start")
         if self.static_substep:
