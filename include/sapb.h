@@ -272,7 +272,8 @@ typedef struct sapb_model_desc {
    * dofs_per_world per world, A and the Jacobian rows compact in their
    * slots -- the layout of sapb_contact_problem.dof_count -- and the step's
    * tail reads the solve's velocities from those slots.  The dense layout
-   * only; sapb_integrate_positions and the C handle take equal blocks. */
+   * only (the C handle included); sapb_integrate_positions takes equal
+   * blocks. */
   const int32_t* world_joint_start;
   const int32_t* world_body_start;
   const int32_t* world_dof_start;

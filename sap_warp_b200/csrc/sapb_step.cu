@@ -99,6 +99,10 @@ struct sapb_handle {
   int32_t T, NB;
   int32_t *tree_dof_start, *contact_tree;
   double* tree_mass;
+  // uneven batches (model world offsets): the start velocities in the
+  // solve's slots and each world's DOF count
+  double* qd_slots;
+  int32_t* dof_count;
 };
 
 extern "C" {
@@ -154,7 +158,7 @@ void sapb_destroy(sapb_handle* h) {
                   h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws,
                   h->key_shape, h->key_count, h->has_history, h->key_point,
                   h->gamma_older, h->gamma_start, h->v_start, h->tree_dof_start, h->contact_tree,
-                  h->tree_mass};
+                  h->tree_mass, h->qd_slots, h->dof_count};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -167,15 +171,19 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   }
   *out = nullptr;
   const int32_t W = model->num_worlds, n = model->dofs_per_world, C = opts->prepare.max_contacts;
-  const int32_t B = W * model->bodies_per_world, Q = W * model->coords_per_world;
-  const int32_t J = W * model->joints_per_world, A = W * model->articulations_per_world;
+  const bool uneven = model->world_joint_start != nullptr;
+  // totals (an uneven batch: from its offsets; dofs_per_world is the
+  // largest world's, the solve's slot size)
+  const int32_t B = model_bodies(*model), J = model_joints(*model), A = model_articulations(*model);
+  int32_t Q = W * model->coords_per_world;
   if (W < 1 || n < 1 || C < 1 || model->bodies_per_world < 1 || J < 1 || A < 1 || !model->joint_child ||
       !model->joint_qd_start || !model->joint_dof_dim || !model->articulation_start) {
     set_last_error("sapb_create: invalid model description");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
-  if (model->world_joint_start) {
-    set_last_error("sapb_create: the handle takes equal per-world blocks");
+  if (uneven && (opts->prepare.tree_blocked || !model->world_body_start || !model->world_dof_start ||
+                 !model->world_articulation_start || !model->body_world)) {
+    set_last_error("sapb_create: an uneven batch needs all its world offsets and the dense layout");
     return SAPB_ERR_UNSUPPORTED;
   }
   if (opts->position_integration != SAPB_INTEGRATE_SAP_EULER && opts->position_integration != SAPB_INTEGRATE_MIDPOINT) {
@@ -213,10 +221,27 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     err = cudaMemcpy(dim.data(), model->joint_dof_dim, sizeof(int32_t) * 2 * J, cudaMemcpyDeviceToHost);
   if (err == cudaSuccess)
     err = cudaMemcpy(art.data(), model->articulation_start, sizeof(int32_t) * (A + 1), cudaMemcpyDeviceToHost);
+  std::vector<int32_t> wbody(W + 1, 0), wdof(W + 1, 0);
+  if (uneven) {
+    if (err == cudaSuccess)
+      err = cudaMemcpy(wbody.data(), model->world_body_start, sizeof(int32_t) * (W + 1), cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess)
+      err = cudaMemcpy(wdof.data(), model->world_dof_start, sizeof(int32_t) * (W + 1), cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess && model->joint_q_start)
+      err = cudaMemcpy(&Q, model->joint_q_start + J, sizeof(int32_t), cudaMemcpyDeviceToHost);
+  }
   if (err != cudaSuccess) {
     set_last_error("sapb_create: reading the model: %s", cudaGetErrorString(err));
     return SAPB_ERR_CUDA;
   }
+  // the world of a body and its first DOF
+  auto world_of = [&](int b) {
+    if (!uneven) return b / model->bodies_per_world;
+    int e = 0;
+    while (e + 1 < W && wbody[e + 1] <= b) ++e;
+    return e;
+  };
+  auto dof0_of = [&](int e) { return uneven ? wdof[e] : e * n; };
   std::vector<int32_t> bstart(B, -1), bcount(B, 0);
   for (int a = 0; a < A; ++a) {
     int s0 = -1, tot = 0;
@@ -229,7 +254,7 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     for (int j = art[a]; j < art[a + 1] && j < J; ++j) {
       const int b = child[j];
       if (b >= 0 && b < B) {
-        bstart[b] = s0 - (b / model->bodies_per_world) * n;
+        bstart[b] = s0 - dof0_of(world_of(b));
         bcount[b] = tot;
       }
     }
@@ -324,6 +349,10 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   take(dev_alloc(&h->order, W));
   take(dev_alloc(&h->body_dof_start, B));
   take(dev_alloc(&h->body_dof_count, B));
+  if (uneven) {
+    take(dev_alloc(&h->qd_slots, Wn));
+    take(dev_alloc(&h->dof_count, W));
+  }
   h->prep_ws_bytes = sapb_prepare_workspace_size(model, C);
   h->solve_ws_bytes = blk ? sapb_blocked_solve_workspace_size(W, h->T, C) : sapb_contact_solve_workspace_size(W, n, C);
   if (err == cudaSuccess) err = cudaMalloc(&h->prep_ws, h->prep_ws_bytes > 0 ? h->prep_ws_bytes : 16);
@@ -334,6 +363,11 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     err = cudaMemcpy(h->body_dof_count, bcount.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice);
   if (err == cudaSuccess && blk)
     err = cudaMemcpy(h->tree_dof_start, tds.data(), sizeof(int32_t) * (h->T + 1), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess && uneven) {
+    std::vector<int32_t> cnt(W);
+    for (int e = 0; e < W; ++e) cnt[e] = wdof[e + 1] - wdof[e];
+    err = cudaMemcpy(h->dof_count, cnt.data(), sizeof(int32_t) * W, cudaMemcpyHostToDevice);
+  }
   if (err == cudaSuccess) err = cudaMemset(h->guess_flag, 0, sizeof(int32_t));
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_prev, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess && cand) err = cudaMemset(h->key_count, 0, sizeof(int32_t) * W);
@@ -385,6 +419,7 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   po.body0 = h->body0;
   po.body1 = h->body1;
   po.truncated_count = h->truncated;
+  po.qd_slots = h->qd_slots;  // uneven batches: the start velocities in the solve's slots
   // previous impulses: the contact history runs inside the launch (the last
   // solves' impulses carried to this step's slots by contact identity and
   // extrapolated), and the free motion forms the start v* + A^-1 J^T gamma
@@ -473,7 +508,8 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   p.body_dof_start = h->body_dof_start;
   p.body_dof_count = h->body_dof_count;
   p.v_star = h->v_star;
-  p.v0 = io->in.joint_qd;
+  p.v0 = h->qd_slots ? h->qd_slots : io->in.joint_qd;
+  p.dof_count = h->dof_count;
   p.v_guess = h->v;
   p.v_guess_active = h->guess_flag;
   p.dt = io->in.dt;
@@ -484,6 +520,7 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     dof_local = *io->dof;
     dof_local.joint_q = io->in.joint_q;
     dof_local.joint_coord_count = h->Q;
+    dof_local.world_dof_start = h->model.world_dof_start;  // uneven: the per-DOF arrays in global order
     p.dof = &dof_local;
   }
   if (cand) {

@@ -124,6 +124,8 @@ def _c_steps(solver, state, control, contacts, dt, steps, device):
         inp.contact_normal = _p(contacts.rigid_contact_normald)
         inp.contact_margin0, inp.contact_margin1 = (_p(contacts.rigid_contact_margin0d),
                                                     _p(contacts.rigid_contact_margin1d))
+        if solver.contact_solve.dof is not None:
+            io.dof = ctypes.pointer(solver.contact_solve.dof)
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         for k in range(steps):
             src, dst = k % 2, 1 - k % 2
@@ -175,3 +177,28 @@ def test_c_handle_refuses_trees_beyond_their_block(cuda_device):
     assert load().sapb_create(ctypes.byref(solver.view.desc), ctypes.byref(opts), ctypes.byref(handle)) == \
         _abi.SAPB_ERR_UNSUPPORTED
     assert not handle.value
+
+
+@pytest.mark.parametrize("drives", [False, True])
+def test_c_step_uneven_batch_equals_solver_steps(cuda_device, drives):
+    """The handle on an uneven batch (arm + box 13 DOF, quadruped 18,
+    humanoid 35, each world at its own DOF count; with and without drive
+    and limit terms) steps like SolverSAP, bit for bit."""
+    dt, steps = 2.0e-3, 4
+    model, state, control, contacts, _ = models.mixed_rollout_scene(32, 66, cuda_device, drives=drives)
+    solver = SolverSAP(model, max_rigid_contact=32, contact_preset_variant="drake", hessian_precision="fp32",
+                       warm_start="previous_impulses")
+    assert solver.view.uneven and solver.view.has_pd == drives
+    a = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                 body_f=state.body_f.clone())
+    b = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                 body_f=state.body_f.clone())
+    for _ in range(steps):
+        solver.step(a, b, control, contacts, dt)
+        a, b = b, a
+    torch.cuda.synchronize()
+    q, qd, status, conv, iters = _c_steps(solver, state, control, contacts, dt, steps, cuda_device)
+    assert torch.equal(q, a.joint_q.to(torch.float64)) and torch.equal(qd, a.joint_qd.to(torch.float64))
+    assert torch.equal(status, solver.contact_solve.ls_status)
+    assert torch.equal(iters, solver.contact_solve.newton_iterations_env)
+    assert np.all(conv == 1)
