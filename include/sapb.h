@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 18
+#define SAPB_ABI_VERSION 19
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -491,6 +491,10 @@ typedef struct sapb_handle sapb_handle;
 #define SAPB_WARM_START_PREVIOUS_VELOCITY 0  /* the reference's: start from the last solution */
 #define SAPB_WARM_START_PREVIOUS_IMPULSES 1  /* also try v* + A^-1 J^T gamma0, gamma0 the start impulses
                                                * of the contact history (candidate start) */
+#define SAPB_WARM_START_LEARNED 2  /* the history's start, plus the network's impulses on new contacts
+                                    * (sapb_step_options.network; SolverSAP(warm_start="learned")) */
+
+struct sapb_step_network;
 #define SAPB_WORK_ORDER_INDEX 0
 #define SAPB_WORK_ORDER_PREVIOUS_ITERATIONS 1  /* most Newton iterations of the last step first */
 
@@ -505,6 +509,8 @@ typedef struct sapb_step_options {
   int32_t work_order;               /* SAPB_WORK_ORDER_* */
   int32_t impulse_history;          /* previous impulses: the contact history's order (1 carried, 2 linear,
                                      * 3 quadratic extrapolation; 0 = 3) */
+  const struct sapb_step_network* network;  /* SAPB_WARM_START_LEARNED: the network (kept alive by the caller
+                                             * for the handle's life), else NULL */
 } sapb_step_options;
 
 /* One step's device arrays: the start-of-step state, control and contacts
@@ -808,6 +814,19 @@ typedef struct sapb_warmstart_norm {
   float output_scale[SAPB_MLP_OUTPUTS];
   float output_shift[SAPB_MLP_OUTPUTS];
 } sapb_warmstart_norm;
+
+/* The warm-start network of the C step handle (SAPB_WARM_START_LEARNED):
+ * its device weights, the normalisation, and the two tau_d fallbacks the
+ * Python LearnedWarmStart uses (features: its tau_fallback; the impulse
+ * map's regularization: contact_tau_d, with contact_beta / contact_sigma
+ * those of the step's solve options). */
+typedef struct sapb_step_network {
+  const uint16_t* packed;           /* SAPB_MLP_PACKED_COUNT BF16 weights, the forward's layout (device) */
+  const float* bias;                /* SAPB_MLP_BIAS_COUNT (device) */
+  sapb_warmstart_norm norm;
+  double feature_tau_d;
+  double impulse_tau_d;
+} sapb_step_network;
 
 /* Saved forward state of one training batch of `rows` rows. */
 typedef struct sapb_mlp_train_buffers {

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 18
+SAPB_ABI_VERSION = 19
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -346,13 +346,20 @@ class AdamOptions(C.Structure):
 
 SAPB_WARM_START_PREVIOUS_VELOCITY = 0
 SAPB_WARM_START_PREVIOUS_IMPULSES = 1
+SAPB_WARM_START_LEARNED = 2
 SAPB_WORK_ORDER_INDEX = 0
 SAPB_WORK_ORDER_PREVIOUS_ITERATIONS = 1
 
 
+class StepNetwork(C.Structure):
+    _fields_ = [("packed", _p), ("bias", _p), ("norm", WarmstartNorm), ("feature_tau_d", C.c_double),
+                ("impulse_tau_d", C.c_double)]
+
+
 class StepOptions(C.Structure):
     _fields_ = [("prepare", PrepareOptions), ("solve", SolveOptions), ("position_integration", C.c_int32),
-                ("warm_start", C.c_int32), ("work_order", C.c_int32), ("impulse_history", C.c_int32)]
+                ("warm_start", C.c_int32), ("work_order", C.c_int32), ("impulse_history", C.c_int32),
+                ("network", C.POINTER(StepNetwork))]
 
 
 class StepIO(C.Structure):

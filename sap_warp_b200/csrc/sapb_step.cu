@@ -61,6 +61,13 @@ __global__ void __launch_bounds__(kOrderThreads) world_order_kernel(const int32_
   for (int i = threadIdx.x; i < W; i += kOrderThreads) order[i] = (int32_t)(keys[i] & 0xffffu);
 }
 
+// The up component of each contact frame (R_WC[2][2]), the network's
+// "normal" feature.
+__global__ void frame_up_kernel(const double* frame, long long n, double* up) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    up[i] = frame[9 * i + 8];
+}
+
 template <typename T>
 cudaError_t dev_alloc(T** p, size_t count) {
   *p = nullptr;
@@ -103,6 +110,14 @@ struct sapb_handle {
   // solve's slots and each world's DOF count
   double* qd_slots;
   int32_t* dof_count;
+  // learned start: the network, the contact frames and their up component,
+  // the free-motion contact velocities, the factor of A (worlds with a new
+  // contact), the features / outputs / active tiles, the network's impulses
+  sapb_step_network net;
+  double *frame, *normal_up, *vc_star, *factor, *gamma_cand, *gamma_zero;
+  uint16_t* feat;
+  float* mlp_y;
+  int32_t* tiles;
 };
 
 extern "C" {
@@ -158,7 +173,8 @@ void sapb_destroy(sapb_handle* h) {
                   h->ws_accepted, h->guess_flag, h->order, h->body_dof_start, h->body_dof_count, h->solve_ws,
                   h->key_shape, h->key_count, h->has_history, h->key_point,
                   h->gamma_older, h->gamma_start, h->v_start, h->tree_dof_start, h->contact_tree,
-                  h->tree_mass, h->qd_slots, h->dof_count};
+                  h->tree_mass, h->qd_slots, h->dof_count, h->frame, h->normal_up, h->vc_star,
+                  h->factor, h->gamma_cand, h->gamma_zero, h->feat, h->mlp_y, h->tiles};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -190,8 +206,14 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     set_last_error("sapb_create: position_integration must be SAPB_INTEGRATE_SAP_EULER or _MIDPOINT");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
-  if (opts->warm_start != SAPB_WARM_START_PREVIOUS_VELOCITY && opts->warm_start != SAPB_WARM_START_PREVIOUS_IMPULSES) {
-    set_last_error("sapb_create: warm_start must be SAPB_WARM_START_PREVIOUS_VELOCITY or _PREVIOUS_IMPULSES");
+  if (opts->warm_start != SAPB_WARM_START_PREVIOUS_VELOCITY && opts->warm_start != SAPB_WARM_START_PREVIOUS_IMPULSES &&
+      opts->warm_start != SAPB_WARM_START_LEARNED) {
+    set_last_error("sapb_create: warm_start must be SAPB_WARM_START_PREVIOUS_VELOCITY, _PREVIOUS_IMPULSES or _LEARNED");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (opts->warm_start == SAPB_WARM_START_LEARNED &&
+      (!opts->network || !opts->network->packed || !opts->network->bias)) {
+    set_last_error("sapb_create: the learned start needs opts->network with its device weights");
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   if (opts->impulse_history < 0 || opts->impulse_history > 3) {
@@ -300,7 +322,11 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   h->B = B;
   h->Q = Q;
   const size_t Wn = (size_t)W * n, WC = (size_t)W * C;
-  const bool cand = opts->warm_start == SAPB_WARM_START_PREVIOUS_IMPULSES;
+  // the contact history runs for both candidate starts
+  const bool cand = opts->warm_start != SAPB_WARM_START_PREVIOUS_VELOCITY;
+  const bool learned = opts->warm_start == SAPB_WARM_START_LEARNED;
+  if (learned) h->net = *opts->network;
+  h->opts.network = nullptr;  // the handle keeps its own copy
   err = cudaSuccess;
   auto take = [&](cudaError_t e) {
     if (err == cudaSuccess) err = e;
@@ -334,6 +360,18 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
     take(dev_alloc(&h->has_history, WC));
     take(dev_alloc(&h->gamma_older, WC * 3));
     take(dev_alloc(&h->gamma_start, WC * 3));
+  }
+  const size_t tiles = (WC + 127) / 128;
+  if (learned) {
+    take(dev_alloc(&h->frame, WC * 9));
+    take(dev_alloc(&h->normal_up, WC));
+    take(dev_alloc(&h->vc_star, WC * 3));
+    if (!blk) take(dev_alloc(&h->factor, Wn * n));
+    take(dev_alloc(&h->gamma_cand, WC * 3));
+    take(dev_alloc(&h->gamma_zero, WC * 3));
+    take(dev_alloc(&h->feat, WC * SAPB_MLP_INPUTS_PADDED));
+    take(dev_alloc(&h->mlp_y, WC * SAPB_MLP_OUTPUTS));
+    take(dev_alloc(&h->tiles, tiles));
   }
   take(dev_alloc(&h->v, Wn));
   take(dev_alloc(&h->gamma, WC * 3));
@@ -375,6 +413,17 @@ int32_t sapb_create(const sapb_model_desc* model, const sapb_step_options* opts,
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_older, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess && cand) err = cudaMemset(h->gamma_start, 0, sizeof(double) * WC * 3);
   if (err == cudaSuccess) err = cudaMemset(h->iters, 0, sizeof(int32_t) * W);
+  if (learned) {  // every learned buffer starts at zero (dead slots keep what they hold)
+    if (err == cudaSuccess) err = cudaMemset(h->frame, 0, sizeof(double) * WC * 9);
+    if (err == cudaSuccess) err = cudaMemset(h->normal_up, 0, sizeof(double) * WC);
+    if (err == cudaSuccess) err = cudaMemset(h->vc_star, 0, sizeof(double) * WC * 3);
+    if (err == cudaSuccess && h->factor) err = cudaMemset(h->factor, 0, sizeof(double) * Wn * n);
+    if (err == cudaSuccess) err = cudaMemset(h->gamma_cand, 0, sizeof(double) * WC * 3);
+    if (err == cudaSuccess) err = cudaMemset(h->gamma_zero, 0, sizeof(double) * WC * 3);
+    if (err == cudaSuccess) err = cudaMemset(h->feat, 0, sizeof(uint16_t) * WC * SAPB_MLP_INPUTS_PADDED);
+    if (err == cudaSuccess) err = cudaMemset(h->mlp_y, 0, sizeof(float) * WC * SAPB_MLP_OUTPUTS);
+    if (err == cudaSuccess) err = cudaMemset(h->tiles, 0, sizeof(int32_t) * tiles);
+  }
   if (err == cudaSuccess) {
     std::vector<int32_t> idx(W);
     for (int i = 0; i < W; ++i) idx[i] = i;
@@ -399,7 +448,8 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     return SAPB_ERR_INVALID_ARGUMENT;
   }
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const bool cand = h->opts.warm_start == SAPB_WARM_START_PREVIOUS_IMPULSES;
+  const bool cand = h->opts.warm_start != SAPB_WARM_START_PREVIOUS_VELOCITY;  // the contact history runs
+  const bool learned = h->opts.warm_start == SAPB_WARM_START_LEARNED;
   const bool order = h->opts.work_order == SAPB_WORK_ORDER_PREVIOUS_ITERATIONS;
   // free motion and contact rows (sim/solver_sap.py:1415-1433)
   sapb_prepare_outputs po;
@@ -419,6 +469,11 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   po.body0 = h->body0;
   po.body1 = h->body1;
   po.truncated_count = h->truncated;
+  if (learned) {  // the network's inputs and, for its impulses, the factor of A where a contact is new
+    po.frame = h->frame;
+    po.vc_star = h->vc_star;
+    po.dynamics_factor = h->factor;  // NULL in the tree-blocked layout
+  }
   po.qd_slots = h->qd_slots;  // uneven batches: the start velocities in the solve's slots
   // previous impulses: the contact history runs inside the launch (the last
   // solves' impulses carried to this step's slots by contact identity and
@@ -441,6 +496,50 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   int32_t st = sapb_free_motion_contacts(&h->model, &io->in, &h->opts.prepare, &po, h->prep_ws, h->prep_ws_bytes,
                                          stream);
   if (st != SAPB_OK) return st;
+  if (learned) {
+    // the network's impulses (LearnedWarmStart.predict): features, the tiles
+    // holding a new contact, the forward over them, the impulse map; the
+    // history's impulses where a contact has them (tree-blocked: one set with
+    // the history's start impulses; dense: zero there, the start velocity
+    // already holding them)
+    const long long slots = (long long)h->W * h->C;
+    frame_up_kernel<<<(int)((slots + 255) / 256 < 4096 ? (slots + 255) / 256 : 4096), 256, 0, s>>>(h->frame, slots,
+                                                                                                 h->normal_up);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_last_error("sapb_step: %s", cudaGetErrorString(e));
+      return SAPB_ERR_CUDA;
+    }
+    sapb_contact_problem q;
+    memset(&q, 0, sizeof(q));
+    q.num_envs = h->W;
+    q.dof_per_env = h->blk ? 2 * h->NB : h->n;
+    q.max_contacts = h->C;
+    q.contact_count = h->count;
+    q.dynamics_matrix = h->A;
+    q.jacobian = h->J;
+    q.phi0 = h->phi0;
+    q.w_eff = h->w_eff;
+    q.mu = h->mu;
+    q.stiffness = h->stiffness;
+    q.tau_d = h->tau_d;
+    q.v_star = h->v_star;
+    q.v0 = h->v_star;
+    q.dt = io->in.dt;
+    const double* gprev = h->blk ? h->gamma_start : h->gamma_zero;
+    st = sapb_warmstart_features(&q, h->normal_up, gprev, h->vc_star, &h->net.norm, h->net.feature_tau_d, h->feat,
+                                 nullptr, stream);
+    if (st == SAPB_OK) st = sapb_warmstart_active_tiles(&q, h->has_history, h->tiles, stream);
+    if (st == SAPB_OK)
+      st = sapb_mlp_forward_tiles(h->net.packed, h->net.bias, h->feat, (int32_t)slots, h->mlp_y, h->tiles, stream);
+    if (st == SAPB_OK) {
+      sapb_solve_options io_opts = h->opts.solve;
+      io_opts.contact_tau_d = h->net.impulse_tau_d;
+      st = sapb_warmstart_impulses(&q, h->mlp_y, gprev, h->has_history, &h->net.norm, &io_opts, h->gamma_cand,
+                                   stream);
+    }
+    if (st != SAPB_OK) return st;
+  }
   sapb_solve_outputs so;
   memset(&so, 0, sizeof(so));
   so.v = h->v;
@@ -481,7 +580,7 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     bp.v_guess_active = h->guess_flag;
     bp.dt = io->in.dt;
     bp.world_order = order ? h->order : nullptr;
-    bp.gamma0 = cand ? h->gamma_start : nullptr;
+    bp.gamma0 = learned ? h->gamma_cand : (cand ? h->gamma_start : nullptr);
     bp.gamma0_count = cand ? 1 : 0;
     bp.tree_dof_start = h->tree_dof_start;
     bp.dofs_per_world = h->n;
@@ -523,7 +622,14 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     dof_local.world_dof_start = h->model.world_dof_start;  // uneven: the per-DOF arrays in global order
     p.dof = &dof_local;
   }
-  if (cand) {
+  if (learned) {
+    // the network's impulses on new contacts through the factor of A, over
+    // the history's start velocity
+    p.gamma0 = h->gamma_cand;
+    p.gamma0_count = 1;
+    p.gamma0_base = h->v_start;
+    p.dynamics_factor = h->factor;
+  } else if (cand) {
     p.v_candidates = h->v_start;
     p.v_candidate_count = 1;
   }

@@ -1133,8 +1133,8 @@ class SolverSAP:
         options, integrator, warm start (previous velocity or previous
         impulses, with the same impulse history) and work order, so a C host stepping the same model gets
         the same trajectory."""
-        if self.warm_start == "learned":
-            raise NotImplementedError("the C step handle takes the previous-velocity or previous-impulses warm start")
+        if self.warm_start == "learned" and self.learned_candidates != "new_contacts":
+            raise NotImplementedError("the C step handle runs the learned start on new contacts only")
         if self.static_substep:
             iters, ls_iters = self.static_substep_iterations, self.static_substep_line_search_iterations
         else:
@@ -1150,8 +1150,19 @@ class SolverSAP:
         o.solve.skip_plain_start = 0 if self.plain_start else 1
         o.position_integration = (_abi.SAPB_INTEGRATE_MIDPOINT if self.position_integration == "midpoint"
                                   else _abi.SAPB_INTEGRATE_SAP_EULER)
-        o.warm_start = (_abi.SAPB_WARM_START_PREVIOUS_IMPULSES if self.warm_start == "previous_impulses"
-                        else _abi.SAPB_WARM_START_PREVIOUS_VELOCITY)
+        o.warm_start = {"previous_impulses": _abi.SAPB_WARM_START_PREVIOUS_IMPULSES,
+                        "learned": _abi.SAPB_WARM_START_LEARNED}.get(self.warm_start,
+                                                                     _abi.SAPB_WARM_START_PREVIOUS_VELOCITY)
+        if self.warm_start == "learned":
+            # the network by reference: its device weights stay with this solver
+            lw = self.learned_warm_start
+            net = _abi.StepNetwork()
+            net.packed, net.bias = lw.mlp.packed.data_ptr(), lw.mlp.bias.data_ptr()
+            net.norm = lw.norm_struct
+            net.feature_tau_d = float(lw.tau_fallback)
+            net.impulse_tau_d = float(lw.solve_options.contact_tau_d)
+            self._c_network = net
+            o.network = ctypes.pointer(net)
         o.work_order = (_abi.SAPB_WORK_ORDER_PREVIOUS_ITERATIONS if self.work_order == "previous_iterations"
                         else _abi.SAPB_WORK_ORDER_INDEX)
         o.impulse_history = self.impulse_history

@@ -202,3 +202,35 @@ def test_c_step_uneven_batch_equals_solver_steps(cuda_device, drives):
     assert torch.equal(status, solver.contact_solve.ls_status)
     assert torch.equal(iters, solver.contact_solve.newton_iterations_env)
     assert np.all(conv == 1)
+
+
+@pytest.mark.parametrize("kind", ["humanoid", "arm_boxes"])
+def test_c_step_learned_equals_solver_steps(cuda_device, kind):
+    """The handle's learned start (SAPB_WARM_START_LEARNED: the history's
+    start plus the network's impulses on new contacts) steps like
+    SolverSAP(warm_start="learned"), bit for bit, in the dense layout
+    (humanoids) and the tree-blocked one (an arm among boxes)."""
+    dt, steps = 2.0e-3, 4
+    if kind == "humanoid":
+        model, state, control, contacts, _ = models.rollout_scene("humanoid", 256, 67, cuda_device)
+        kw = dict(max_rigid_contact=32)
+    else:
+        model, state, control, contacts, _, _ = models.box_scene(128, 68, cuda_device, boxes=8, sites=(3, 5),
+                                                                 arm=True)
+        kw = dict(max_rigid_contact=112, tree_blocked=True)
+    solver = SolverSAP(model, contact_preset_variant="drake", hessian_precision="fp32", warm_start="learned", **kw)
+    a = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                 body_f=state.body_f.clone())
+    b = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),
+                 body_f=state.body_f.clone())
+    for _ in range(steps):
+        solver.step(a, b, control, contacts, dt)
+        a, b = b, a
+    torch.cuda.synchronize()
+    if kind == "humanoid":  # the start the network feeds is taken (the box stacks often keep the plain one)
+        assert int(solver.contact_solve.warm_start_accepted_env.sum()) > 0
+    q, qd, status, conv, iters = _c_steps(solver, state, control, contacts, dt, steps, cuda_device)
+    assert torch.equal(q, a.joint_q.to(torch.float64)) and torch.equal(qd, a.joint_qd.to(torch.float64))
+    assert torch.equal(status, solver.contact_solve.ls_status)
+    assert torch.equal(iters, solver.contact_solve.newton_iterations_env)
+    assert np.all(conv == 1)
