@@ -2,10 +2,11 @@
 // the step from C (SolverSAP.__init__ / .step, sim/solver_sap.py:749-968 and
 // :1388-1494, as a C API): sapb_create allocates every work buffer once,
 // sapb_step runs free motion + contact rows, the contact solve (with the
-// previous-velocity or previous-impulse warm start) and the position
-// integration on the caller's stream without host synchronisation (so a
-// caller may capture it in a CUDA graph), sapb_get_status copies the
-// per-world solve statuses, sapb_destroy frees the buffers.
+// previous-velocity, previous-impulse or learned warm start; dense or
+// tree-blocked; equal or uneven worlds) and the position integration on the
+// caller's stream without host synchronisation (so a caller may capture it
+// in a CUDA graph), sapb_get_status copies the per-world solve statuses,
+// sapb_destroy frees the buffers.
 //
 // Also the stable work-order sort (sapb_world_order): the persistent solve
 // takes the worlds in the order of the previous step's Newton iterations,
