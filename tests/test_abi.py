@@ -99,6 +99,9 @@ def test_struct_layout_matches_header(tmp_path):
         " sizeof(sapb_step_io), offsetof(sapb_step_io, joint_qd_out));"
         " printf(\"%zu %zu %zu %zu\\n\", sizeof(sapb_contact_history), offsetof(sapb_contact_history, order),"
         " offsetof(sapb_contact_history, gamma_start), offsetof(sapb_step_options, impulse_history));"
+        " printf(\"%zu %zu %zu %zu %zu\\n\", sizeof(sapb_step_network), offsetof(sapb_step_network, impulse_tau_d),"
+        " offsetof(sapb_step_options, network), offsetof(sapb_blocked_problem, tree_dof_start),"
+        " offsetof(sapb_dof_terms, world_dof_start));"
         " return 0;}\n"
     )
     exe = tmp_path / "sizes"
@@ -113,5 +116,7 @@ def test_struct_layout_matches_header(tmp_path):
             ctypes.sizeof(_abi.BlockedProblem), _abi.BlockedProblem.world_order.offset,
             ctypes.sizeof(_abi.StepOptions), _abi.StepOptions.work_order.offset, ctypes.sizeof(_abi.StepIO),
             _abi.StepIO.joint_qd_out.offset, ctypes.sizeof(_abi.ContactHistory), _abi.ContactHistory.order.offset,
-            _abi.ContactHistory.gamma_start.offset, _abi.StepOptions.impulse_history.offset]
+            _abi.ContactHistory.gamma_start.offset, _abi.StepOptions.impulse_history.offset,
+            ctypes.sizeof(_abi.StepNetwork), _abi.StepNetwork.impulse_tau_d.offset, _abi.StepOptions.network.offset,
+            _abi.BlockedProblem.tree_dof_start.offset, _abi.DofTerms.world_dof_start.offset]
     assert got == want
