@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define SAPB_ABI_VERSION 19
+#define SAPB_ABI_VERSION 20
 
 /* ---- return / status codes ------------------------------------------------ */
 #define SAPB_OK 0
@@ -501,8 +501,7 @@ struct sapb_step_network;
 typedef struct sapb_step_options {
   sapb_prepare_options prepare;     /* max_contacts, weight / point modes, fallbacks; tree_blocked: the
                                      * tree-blocked layout and solve (the trees are world 0's articulations,
-                                     * tree_dofs 0: the smallest block holding them; no drive or limit
-                                     * terms) */
+                                     * tree_dofs 0: the smallest block holding them) */
   sapb_solve_options solve;         /* the contact solve's options (line search, precisions, tolerances) */
   int32_t position_integration;     /* SAPB_INTEGRATE_SAP_EULER / SAPB_INTEGRATE_MIDPOINT */
   int32_t warm_start;               /* SAPB_WARM_START_* */
@@ -711,7 +710,7 @@ int32_t sapb_contact_solve_noalloc(const sapb_contact_problem* problem, const sa
  * DOFs is padded with the identity in its block and zero columns, padding
  * the solve keeps to itself (the per-DOF vectors are the world's own DOFs).
  * A contact whose two sides lie on one tree is given as one side with the
- * summed columns.  No PD or limit terms. */
+ * summed columns.  Drive and limit terms through `dof` (optional). */
 typedef struct sapb_blocked_problem {
   int32_t num_envs;
   int32_t trees_per_env;          /* T <= 64 */
@@ -744,6 +743,9 @@ typedef struct sapb_blocked_problem {
    * tree_dofs DOFs, tree_dof_start[T] = dofs_per_world), or NULL. */
   const int32_t* tree_dof_start;
   int32_t dofs_per_world;         /* n; 0: T * tree_dofs */
+  /* Drive and limit terms (sim/contact_solve.py:490-683), the per-DOF arrays
+   * in the [E*n] layout of the world's own DOFs, or NULL: none. */
+  const sapb_dof_terms* dof;
 } sapb_blocked_problem;
 
 /* The block size NB the blocked solve is built with for trees of up to

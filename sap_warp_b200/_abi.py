@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-SAPB_ABI_VERSION = 19
+SAPB_ABI_VERSION = 20
 
 SAPB_OK = 0
 SAPB_ERR_INVALID_ARGUMENT = -100
@@ -157,6 +157,7 @@ class BlockedProblem(C.Structure):
         ("gamma0_count", C.c_int32),
         ("tree_dof_start", _p),
         ("dofs_per_world", C.c_int32),
+        ("dof", C.POINTER(DofTerms)),
     ]
 
 

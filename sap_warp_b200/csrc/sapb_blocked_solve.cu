@@ -28,9 +28,15 @@ int32_t blocked_solve_launch(const sapb_blocked_problem* p, const sapb_solve_opt
   P.use_guess_flag_ptr_valid = (p->v_guess && p->v_guess_active) ? 1 : 0;
   P.queue = reinterpret_cast<int32_t*>(workspace);
   P.nd = p->dofs_per_world > 0 ? p->dofs_per_world : p->trees_per_env * p->tree_dofs;
+  if (p->dof) P.dof = *p->dof;
   if (p->num_envs == 0) return SAPB_OK;
   const bool fp32 = o->hessian_precision == SAPB_FP32 || o->linear_solve_precision == SAPB_FP32;
+  const bool terms = P.dof.has_pd || P.dof.has_limits;
+  // the on-chip factor capacity, less the drive / limit vectors' room
   P.capacity = blocked_fill_capacity(p->trees_per_env, p->tree_dofs, p->max_contacts, fp32);
+  if (terms && P.capacity > 0)
+    P.capacity = fp32 ? blocked_capacity<float>(p->trees_per_env, p->tree_dofs, p->max_contacts, true)
+                      : blocked_capacity<double>(p->trees_per_env, p->tree_dofs, p->max_contacts, true);
   if (P.capacity < 1 && p->trees_per_env > 1) {
     set_last_error("blocked contact solve: a world of %d trees and %d contact slots does not fit on chip",
                    p->trees_per_env, p->max_contacts);

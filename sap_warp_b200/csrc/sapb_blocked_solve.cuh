@@ -50,7 +50,7 @@ constexpr int kBMaxTrees = 64;
 
 struct BlockedParams {
   sapb_blocked_problem p;
-  sapb_dof_terms dof;  // all zero: blocked worlds carry no PD or limit terms
+  sapb_dof_terms dof;  // the drive / limit terms (all zero without)
   sapb_solve_options o;
   sapb_solve_outputs out;
   int32_t use_guess_flag_ptr_valid;
@@ -61,15 +61,21 @@ struct BlockedParams {
 
 // The per-DOF vectors the blocked kernel keeps, mapped from the V_* slots the
 // line searches name.  Slot kBVecs-1 holds the saved plain start while a
-// candidate start is evaluated (V_SAVE) and absorbs the PD / limit slots,
-// which the line searches only touch when PD or limit terms exist (never
-// here).
+// candidate start is evaluated (V_SAVE) and, without drive / limit terms,
+// absorbs their slots (which nothing then reads); with them, kBTermVecs
+// more slots follow (bterm).
 __host__ __device__ constexpr int bslot(int k) {
   return k == V_V ? 0 : k == V_VSTAR ? 1 : k == V_DV ? 2 : k == V_GRAD ? 3 : k == V_ARES ? 4 : k == V_DP ? 5
        : k == V_DSCALE ? 6 : k == V_TMP0 ? 7 : 8;
 }
 static_assert(bslot(V_SAVE) == 8, "the saved start has the spare slot");
 constexpr int kBVecs = 9;
+__host__ __device__ constexpr int bterm(int k) {
+  return k == V_AINV ? 0 : k == V_PDA ? 1 : k == V_PDGAIN ? 2 : k == V_PDLIM ? 3 : k == V_LOVHAT ? 4
+       : k == V_UPVHAT ? 5 : k == V_LOR ? 6 : k == V_UPR ? 7 : k == V_LORINV ? 8 : k == V_UPRINV ? 9
+       : k == V_HDIAG ? 10 : -1;
+}
+constexpr int kBTermVecs = 11;
 
 // Integer scratch inside off_int.
 enum BInt {
@@ -94,7 +100,8 @@ struct BLayout {
 
 __host__ __device__ inline size_t balign(size_t x) { return (x + 15) / 16 * 16; }
 
-__host__ __device__ inline BLayout make_blayout(int T, int NB, int C, int hsize, int cap) {
+// terms: the worlds carry drive / limit terms (their vector slots)
+__host__ __device__ inline BLayout make_blayout(int T, int NB, int C, int hsize, int cap, bool terms = false) {
   BLayout L;
   L.T = T;
   L.NB = NB;
@@ -104,7 +111,7 @@ __host__ __device__ inline BLayout make_blayout(int T, int NB, int C, int hsize,
   const size_t bb = (size_t)NB * NB * hsize;
   size_t o = 0;
   L.off_vec = o;
-  o = balign(o + sizeof(double) * (size_t)kBVecs * L.n);
+  o = balign(o + sizeof(double) * (size_t)(kBVecs + (terms ? kBTermVecs : 0)) * L.n);
   L.off_con = o;
   o = balign(o + sizeof(double) * (size_t)C_END * L.C);
   L.off_G = o;
@@ -148,7 +155,13 @@ struct BWorld {
   int* flags;
   double* red;
   __device__ __forceinline__ int dofs() const { return n; }
-  __device__ __forceinline__ double* V(int k) const { return vec + (size_t)bslot(k) * n; }
+  bool terms;  // drive / limit terms: their slots after the kBVecs
+  int has_pd, has_limits;
+  double dt;
+  __device__ __forceinline__ double* V(int k) const {
+    const int t = terms ? bterm(k) : -1;
+    return vec + (size_t)(t >= 0 ? kBVecs + t : bslot(k)) * n;
+  }
   __device__ __forceinline__ double* Cn(int k) const { return con + (size_t)k * C; }
   __device__ ContactConst cc(int c) const {
     ContactConst x;
@@ -265,10 +278,45 @@ __device__ void bevaluate(const BWorld<NT, HT, NB>& w, double out4[4]) {
                __ldg(j0 + 4 * NB) * w.Cn(C_GAMMA + 2)[c];
       }
     }
+    double mc = 0.5 * w.V(V_TMP0)[i] * a_res;
+    if (w.terms) {  // drive and limit terms (as the dense solve's evaluate)
+      const double vi = vt[a], dt = w.dt;
+      const int fl = w.flags[i];
+      double pdg = 0.0, lg = 0.0, hd = 0.0;
+      if (w.has_pd && (fl & kFlagPd)) {
+        const double gain = w.V(V_PDGAIN)[i], lim = w.V(V_PDLIM)[i];
+        const double y = w.V(V_PDA)[i] - gain * vi;
+        pdg = dt * clamp_limit(y, lim);
+        hd += dt * gain * clamp_limit_derivative(y, lim);
+        if (gain > 0.0) mc += (dt / gain) * clamp_limit_antiderivative(y, lim);
+      }
+      if (w.has_limits) {
+        double lc = 0.0;
+        if (fl & kFlagLo) {
+          const double g = w.V(V_LORINV)[i] * (w.V(V_LOVHAT)[i] - vi);
+          if (g > 0.0) {
+            lg += g;
+            hd += w.V(V_LORINV)[i];
+            lc += 0.5 * w.V(V_LOR)[i] * g * g;
+          }
+        }
+        if (fl & kFlagUp) {
+          const double g = w.V(V_UPRINV)[i] * (w.V(V_UPVHAT)[i] + vi);
+          if (g > 0.0) {
+            lg -= g;
+            hd += w.V(V_UPRINV)[i];
+            lc += 0.5 * w.V(V_UPR)[i] * g * g;
+          }
+        }
+        mc += lc;
+      }
+      imp += pdg + lg;
+      w.V(V_HDIAG)[i] = hd;
+    }
     const double grad = a_res - imp;
     w.V(V_ARES)[i] = a_res;
     w.V(V_GRAD)[i] = grad;
-    model_cost += 0.5 * w.V(V_TMP0)[i] * a_res;
+    model_cost += mc;
     if (w.flags[i] & kFlagPart) {
       const double s = w.V(V_DSCALE)[i];
       const double gs = s * grad, ps = s * a_v, js = s * imp;
@@ -386,7 +434,9 @@ __device__ void bassemble(const BWorld<NT, HT, NB>& w, double diag_shift) {
       HT* Fr = w.F + (t * NB + a) * NB;
 #pragma unroll
       for (int b = 0; b < NB; ++b)
-        if (b <= a) Fr[b] = HT(__ldg(Ar + b) + (a == b ? diag_shift : 0.0)) + acc[b];
+        if (b <= a)
+          Fr[b] = HT(__ldg(Ar + b) + (a == b ? diag_shift + (w.terms ? w.V(V_HDIAG)[t * NB + a] : 0.0) : 0.0)) +
+                  acc[b];
     } else {
       const int q = item - ndiag;
       const int sl = q / NB, a = q - sl * NB;
@@ -752,7 +802,8 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
   const int tid = threadIdx.x;
   const int T = P.p.trees_per_env, C = P.p.max_contacts;
   const int n = T * NB;
-  const BLayout L = make_blayout(T, NB, C, (int)sizeof(HT), P.capacity);
+  const bool terms = P.dof.has_pd || P.dof.has_limits;
+  const BLayout L = make_blayout(T, NB, C, (int)sizeof(HT), P.capacity, terms);
   const bool use_guess = P.use_guess_flag_ptr_valid && P.p.v_guess_active[0] != 0;
 
   // tree t's DOFs in the global vectors: s_tstart[t] .. + s_tcount[t]; an
@@ -792,6 +843,9 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
     if (e < 0 || e >= P.p.num_envs) continue;
 
     BWorld<NT, HT, NB> w;
+    w.terms = terms;
+    w.has_pd = P.dof.has_pd;
+    w.has_limits = P.dof.has_limits;
     w.n = n;
     w.C = L.C;
     w.T = T;
@@ -875,6 +929,88 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
     for (int c = tid; c < count; c += NT)  // the contact constants formed above
       for (int q = C_RT; q < C_VC; ++q) bad = bad || !isfinite(w.Cn(q)[c]);
     bad = __syncthreads_or(bad) != 0;
+    w.dt = dt;
+    // drive and limit terms of the world's own DOFs (sim/contact_solve.py:
+    // 490-683, as in the dense solve); a DOF they act on takes part
+    bool wterms = false;
+    if (terms) {
+      const sapb_dof_terms& D = P.dof;
+      const int ndof = P.p.num_envs * P.nd;
+      for (int i = tid; i < n; i += NT) {
+        const int gi = gidx(i);
+        const int t = i / NB, a = i - t * NB;
+        double d = __ldg(w.A + ((size_t)t * NB + a) * NB + a);
+        if (d < 1.0e-12 || !isfinite(d)) d = 1.0e-12;
+        w.V(V_AINV)[i] = 1.0 / d;
+        w.V(V_LOR)[i] = 1.0;
+        w.V(V_UPR)[i] = 1.0;
+        w.V(V_HDIAG)[i] = 0.0;
+        int fl = 0;
+        if (gi >= 0) {
+          const size_t dof = base + gi;
+          if (D.has_pd) {
+            int coord = D.dof_coord_index[dof];
+            if (coord >= D.joint_coord_count) coord = -1;
+            int target = D.dof_target_index[dof];
+            if (target < 0 || target >= ndof) target = (int)dof;
+            if (D.joint_target_mode[target] != 0) {
+              const double kp = (double)D.joint_target_ke[target], kd = (double)D.joint_target_kd[target];
+              if (!(kp <= 0.0 && kd <= 0.0) && !(coord < 0 && kp > 0.0)) {
+                double kpe, kde;
+                effective_pd_gains(kp, kd, dt, w.V(V_AINV)[i], &kpe, &kde);
+                const double gain = dt * kpe + kde;
+                if (gain > 0.0) {
+                  double q0 = 0.0, qd = 0.0;
+                  if (coord >= 0) {
+                    q0 = D.joint_q[coord];
+                    qd = D.joint_target_pos ? (double)D.joint_target_pos[target] : 0.0;
+                  }
+                  const double vd = D.joint_target_vel ? (double)D.joint_target_vel[target] : 0.0;
+                  const double u0 = D.joint_act ? (double)D.joint_act[target] : 0.0;
+                  fl |= kFlagPd;
+                  w.V(V_PDA)[i] = kpe * (qd - q0) + kde * vd + u0;
+                  w.V(V_PDGAIN)[i] = gain;
+                  w.V(V_PDLIM)[i] = (double)D.joint_effort_limit[target];
+                }
+              }
+            }
+          }
+          if (D.has_limits) {
+            int coord = D.dof_coord_index[dof];
+            if (coord >= D.joint_coord_count) coord = -1;
+            const double ke = coord >= 0 ? D.joint_limit_ke[dof] : 0.0;
+            if (coord >= 0 && D.limit_supported[dof] != 0 && ke > 0.0) {
+              const double q0 = D.joint_q[coord];
+              const double lower = D.joint_limit_lower[dof], upper = D.joint_limit_upper[dof];
+              const double speed = fmax(fabs(P.p.v0[base + gi]), fabs(w.V(V_VSTAR)[i]));
+              const double window = kLimitWindow * dt * speed;
+              const double kdl = D.joint_limit_kd[dof];
+              const double tau_d = kdl > 0.0 ? kdl / ke : 0.0;
+              const double bf = kLimitBeta * kLimitBeta / (4.0 * kPi * kPi);
+              const double r_nr = bf * fmax(w.V(V_AINV)[i], 1.0e-12);
+              const double r_soft = 1.0 / (dt * ke * (dt + tau_d));
+              const double rr = fmax(r_nr, r_soft);
+              if (isfinite(lower) && q0 - lower <= window) {
+                fl |= kFlagLo;
+                w.V(V_LOVHAT)[i] = -(q0 - lower) / (dt + tau_d);
+                w.V(V_LOR)[i] = rr;
+                w.V(V_LORINV)[i] = 1.0 / rr;
+              }
+              if (isfinite(upper) && upper - q0 <= window) {
+                fl |= kFlagUp;
+                w.V(V_UPVHAT)[i] = -(upper - q0) / (dt + tau_d);
+                w.V(V_UPR)[i] = rr;
+                w.V(V_UPRINV)[i] = 1.0 / rr;
+              }
+            }
+          }
+        }
+        if (fl) fl |= kFlagPart;
+        w.flags[i] = fl;
+        wterms = wterms || fl != 0;
+      }
+    }
+    wterms = __syncthreads_or(wterms) != 0;
     for (int c = tid; c < count; c += NT) {
       const int t0 = tree_w[2 * c], t1 = tree_w[2 * c + 1];
       if (t0 >= 0 && t1 >= 0) {
@@ -905,7 +1041,7 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
         if (tree_w[2 * c + 1] == t) list_w[q++] = (uint16_t)((c << 1) | 1);
       }
       if (w.iw[BI_CNT + t] > 0)
-        for (int a = 0; a < NB; ++a) w.flags[t * NB + a] = kFlagPart;
+        for (int a = 0; a < NB; ++a) w.flags[t * NB + a] |= kFlagPart;
     }
     __syncthreads();
     const bool fits = bsymbolic<NT, HT, NB>(w, L.cap);
@@ -919,7 +1055,7 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
       status = SAPB_WORLD_FACTOR_CAPACITY;
       for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
-    } else if (count == 0) {
+    } else if (count == 0 && !wterms) {
       converged = 1;
       for (int i = tid; i < n; i += NT) w.V(V_V)[i] = w.V(V_VSTAR)[i];
       __syncthreads();
@@ -1091,8 +1227,8 @@ __global__ void __launch_bounds__(NT, 1) blocked_solve_kernel(const BlockedParam
 namespace blk {
 
 template <typename HT>
-int blocked_capacity(int T, int NB, int C) {
-  const BLayout L0 = make_blayout(T, NB, C, (int)sizeof(HT), 0);
+int blocked_capacity(int T, int NB, int C, bool terms = false) {
+  const BLayout L0 = make_blayout(T, NB, C, (int)sizeof(HT), 0, terms);
   const size_t per = (size_t)NB * NB * sizeof(HT) + 2;
   if (L0.total + 64 > kMaxSmemPerBlock) return 0;
   size_t cap = (kMaxSmemPerBlock - L0.total - 64) / per;
@@ -1103,7 +1239,8 @@ int blocked_capacity(int T, int NB, int C) {
 
 template <int NT, typename HT, int NB, int LSV>
 cudaError_t launch_blocked_ls(const BlockedParams& P, cudaStream_t stream) {
-  const BLayout L = make_blayout(P.p.trees_per_env, NB, P.p.max_contacts, (int)sizeof(HT), P.capacity);
+  const BLayout L = make_blayout(P.p.trees_per_env, NB, P.p.max_contacts, (int)sizeof(HT), P.capacity,
+                                 P.dof.has_pd || P.dof.has_limits);
   auto kern = blocked_solve_kernel<NT, HT, NB, LSV>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
   if (err != cudaSuccess) return err;

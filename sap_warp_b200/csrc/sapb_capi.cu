@@ -203,6 +203,22 @@ int32_t sapb_blocked_contact_solve(const sapb_blocked_problem* p, const sapb_sol
                          p->gamma0_count);
     return SAPB_ERR_UNSUPPORTED;
   }
+  if (p->dof && (p->dof->has_pd || p->dof->has_limits) && (!p->dof->dof_coord_index || !p->dof->joint_q)) {
+    sapb::set_last_error("sapb_blocked_contact_solve: drive / limit terms need dof_coord_index and joint_q");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->dof && p->dof->has_pd &&
+      (!p->dof->dof_target_index || !p->dof->joint_target_mode || !p->dof->joint_target_ke ||
+       !p->dof->joint_target_kd || !p->dof->joint_effort_limit)) {
+    sapb::set_last_error("sapb_blocked_contact_solve: drive terms need their target and gain arrays");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
+  if (p->dof && p->dof->has_limits &&
+      (!p->dof->limit_supported || !p->dof->joint_limit_lower || !p->dof->joint_limit_upper ||
+       !p->dof->joint_limit_ke || !p->dof->joint_limit_kd)) {
+    sapb::set_last_error("sapb_blocked_contact_solve: limit terms need their limit arrays");
+    return SAPB_ERR_INVALID_ARGUMENT;
+  }
   if (o->line_search_variant < SAPB_LS_MONOTONE_DECAY || o->line_search_variant > SAPB_LS_EXACT_ROOT) {
     sapb::set_last_error("sapb_blocked_contact_solve: unknown line search variant %d", o->line_search_variant);
     return SAPB_ERR_INVALID_ARGUMENT;

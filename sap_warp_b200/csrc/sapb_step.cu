@@ -556,10 +556,6 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
   if (h->blk) {
     // the tree-blocked solve: the same Newton loop on A's tree blocks, the
     // history's start impulses as its candidate
-    if (io->dof && (io->dof->has_pd || io->dof->has_limits)) {
-      set_last_error("sapb_step: the tree-blocked layout takes no drive or limit terms");
-      return SAPB_ERR_UNSUPPORTED;
-    }
     sapb_blocked_problem bp;
     memset(&bp, 0, sizeof(bp));
     bp.num_envs = h->W;
@@ -585,6 +581,15 @@ int32_t sapb_step(sapb_handle* h, const sapb_step_io* io, void* stream) {
     bp.gamma0_count = cand ? 1 : 0;
     bp.tree_dof_start = h->tree_dof_start;
     bp.dofs_per_world = h->n;
+    // the drive / limit terms at this step's coordinates
+    sapb_dof_terms bdof;
+    if (io->dof) {
+      bdof = *io->dof;
+      bdof.joint_q = io->in.joint_q;
+      bdof.joint_coord_count = h->Q;
+      bdof.world_dof_start = nullptr;
+      bp.dof = &bdof;
+    }
     st = sapb_blocked_contact_solve(&bp, &h->opts.solve, &so, h->solve_ws, h->solve_ws_bytes, stream);
   } else {
   // contact solve (sim/solver_sap.py:1434-1460), warm start from the last

@@ -568,8 +568,6 @@ class SapContactSolve:
         if v.n > 60 and not self.tree_blocked:
             raise NotImplementedError(f"the dense on-chip solve supports up to 60 DOFs per world, got {v.n} "
                                       "(worlds of free bodies use the tree-blocked solve)")
-        if self.tree_blocked and (v.has_pd or v.has_limits):
-            raise NotImplementedError("the tree-blocked solve has no joint drive or limit terms")
         self.model = model
         self.max_rigid_contact = max(int(max_rigid_contact), 1)
         self.contact_beta, self.contact_sigma = float(contact_beta), float(contact_sigma)
@@ -770,7 +768,7 @@ class SapContactSolve:
         W, n, C = v.W, v.n, self.max_rigid_contact
         if self.tree_blocked:
             return self._solve_blocked(contact_result, opts, v_star, v0, v_guess, v_guess_active, world_order,
-                                       gamma0)
+                                       gamma0, state=state, control=control)
         P = _abi.ContactProblem()
         P.num_envs, P.dof_per_env, P.max_contacts = W, n, int(contact_result.contact_env_jacobian.shape[1])
         P.num_bodies = int(v.body_dof_start.numel())
@@ -808,14 +806,7 @@ class SapContactSolve:
             P.v_candidates = _ptr(v_candidates)
             P.v_candidate_count = int(v_candidates.numel() // (W * n))
         if self.dof is not None:
-            self._jq = _f64(state.joint_q)
-            self.dof.joint_q = _ptr(self._jq)
-            for name, t in (("joint_target_pos", getattr(control, "joint_target_pos", None)),
-                            ("joint_target_vel", getattr(control, "joint_target_vel", None)),
-                            ("joint_act", getattr(control, "joint_act", None))):
-                tt = t.to(F32).contiguous() if t is not None else None
-                self._dof_keep["_" + name] = tt
-                setattr(self.dof, name, _ptr(tt))
+            self._set_dof_inputs(state, control)
             P.dof = ctypes.pointer(self.dof)
         stream = ctypes.c_void_p(torch.cuda.current_stream(v.device).cuda_stream)
         opts.skip_plain_start = 1 if skip_plain_start else 0
@@ -826,8 +817,20 @@ class SapContactSolve:
         check(status, "sapb_contact_solve")
         return self.result()
 
+    def _set_dof_inputs(self, state, control) -> None:
+        """This step's coordinates and drive targets into the drive / limit
+        terms (sapb_dof_terms reads them by address)."""
+        self._jq = _f64(state.joint_q)
+        self.dof.joint_q = _ptr(self._jq)
+        for name, t in (("joint_target_pos", getattr(control, "joint_target_pos", None)),
+                        ("joint_target_vel", getattr(control, "joint_target_vel", None)),
+                        ("joint_act", getattr(control, "joint_act", None))):
+            tt = t.to(F32).contiguous() if t is not None else None
+            self._dof_keep["_" + name] = tt
+            setattr(self.dof, name, _ptr(tt))
+
     def _solve_blocked(self, r: SapContactJacobianResult, opts, v_star, v0, v_guess, v_guess_active,
-                       world_order=None, gamma0=None):
+                       world_order=None, gamma0=None, state=None, control=None):
         """The tree-blocked solve (sapb_blocked_contact_solve) on the
         tree-blocked result of SapContactJacobian; gamma0 (W, C, 3): one set
         of candidate starting impulses."""
@@ -837,6 +840,9 @@ class SapContactSolve:
         P = _abi.BlockedProblem()
         P.num_envs, P.trees_per_env, P.tree_dofs = v.W, v.Aw, v.tree_block
         P.tree_dof_start, P.dofs_per_world = _ptr(v.tree_dof_start), v.n
+        if self.dof is not None:
+            self._set_dof_inputs(state, control)
+            P.dof = ctypes.pointer(self.dof)
         P.max_contacts = int(r.contact_env_jacobian.shape[1])
         P.contact_count, P.tree_mass = _ptr(r.contact_env_count), _ptr(r.tree_mass_env)
         P.world_order = _ptr(_checked_order(world_order, v.W))

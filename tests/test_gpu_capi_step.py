@@ -144,13 +144,16 @@ def _c_steps(solver, state, control, contacts, dt, steps, device):
     return q[last], qd[last], status, conv, iters
 
 
-@pytest.mark.parametrize("warm", ["previous_velocity", "previous_impulses"])
-def test_c_step_tree_blocked_equals_solver_steps(cuda_device, warm):
+@pytest.mark.parametrize("warm,drives", [("previous_velocity", False), ("previous_impulses", False),
+                                         ("previous_impulses", True)])
+def test_c_step_tree_blocked_equals_solver_steps(cuda_device, warm, drives):
     """The handle in the tree-blocked layout (an arm among 8 boxes: trees of
-    7 and 6 DOFs in blocks of 7) steps like SolverSAP(tree_blocked=True),
-    bit for bit."""
+    7 and 6 DOFs in blocks of 7; with drives and limits on the arm) steps
+    like SolverSAP(tree_blocked=True), bit for bit."""
     W, dt, steps = 128, 2.0e-3, 4
     model, state, control, contacts, _, _ = models.box_scene(W, 64, cuda_device, boxes=8, sites=(3, 5), arm=True)
+    if drives:
+        model, control = models.with_drives(model, state, control, np.random.default_rng(6))
     solver = SolverSAP(model, max_rigid_contact=112, contact_preset_variant="drake", hessian_precision="fp32",
                        warm_start=warm, tree_blocked=True)
     a = SapState(joint_q=state.joint_q.clone(), joint_qd=state.joint_qd.clone(), body_q=state.body_q.clone(),

@@ -307,3 +307,38 @@ def test_tree_beyond_block_rejected_and_nonfinite_world_reported(cuda_device):
     assert bool(conv[[0, 2, 3]].all())
     torch.testing.assert_close(v[n:2 * n], v0[n:2 * n], rtol=0, atol=0)  # v = the start velocity
     assert torch.isfinite(v).all()
+
+
+def test_driven_arm_blocked_step_matches_dense_step(cuda_device):
+    """A position-controlled arm among boxes (drives and limits on its
+    joints, models.with_drives): three steps of the tree-blocked solve, its
+    drive / limit terms read through the tree map, agree with the dense
+    solve's to the solve's tolerance."""
+    W, Bx = 24, 6
+    model, state, control, con, _, _ = models.box_scene(W, 79, cuda_device, boxes=Bx, sites=(2, 4), arm=True)
+    model, control = models.with_drives(model, state, control, np.random.default_rng(5))
+    kw = dict(max_rigid_contact=96, contact_preset_variant="drake", warm_start="previous_impulses")
+    runs = {}
+    for blocked in (False, True):
+        solver = SolverSAP(model, tree_blocked=blocked, **kw)
+        assert solver.view.has_pd and solver.view.has_limits
+        a, b = _clone(state), _clone(state)
+        for _ in range(3):
+            solver.step(a, b, control, con, DT)
+            a, b = b, a
+        torch.cuda.synchronize()
+        assert bool(solver.contact_solve.converged_env.all())
+        runs[blocked] = (a.joint_qd.cpu().numpy(), a.joint_q.cpu().numpy())
+    scale = np.abs(runs[False][0]).max()
+    np.testing.assert_allclose(runs[True][0], runs[False][0], rtol=0, atol=2e-5 * scale)
+    np.testing.assert_allclose(runs[True][1], runs[False][1], rtol=0, atol=1e-8)
+    # the drives act: the arm's velocities differ from an undriven run
+    free = SolverSAP(models.box_scene(W, 79, cuda_device, boxes=Bx, sites=(2, 4), arm=True)[0], tree_blocked=True,
+                     **kw)
+    a, b = _clone(state), _clone(state)
+    for _ in range(3):
+        free.step(a, b, control, con, DT)
+        a, b = b, a
+    torch.cuda.synchronize()
+    arm = np.arange(W)[:, None] * (7 + 6 * Bx) + np.arange(7)[None, :]
+    assert np.abs(a.joint_qd.cpu().numpy()[arm] - runs[True][0][arm]).max() > 1e-3 * scale
