@@ -753,7 +753,9 @@ typedef struct sapb_blocked_problem {
 int32_t sapb_blocked_tree_block(int32_t tree_dofs);
 
 /* Off-diagonal factor blocks one world of this shape can hold on chip
- * (0: the shape does not fit or tree_dofs is not a built block size).  A world whose
+ * without drive / limit terms (with them, their 11 vectors per DOF take
+ * room first; 0: the shape does not fit or tree_dofs is not a built block
+ * size).  A world whose
  * elimination (rounds of independent minimum-degree trees, with fill) needs
  * more gets the per-world status SAPB_WORLD_FACTOR_CAPACITY. */
 int32_t sapb_blocked_fill_capacity(int32_t trees_per_env, int32_t tree_dofs, int32_t max_contacts,
