@@ -75,6 +75,21 @@ def test_no_compute_entry_points_without_gpu(lib):
     assert so.prepare.max_contacts == 128 and so.solve.line_search_variant == _abi.SAPB_LS_ARMIJO_DECAY
     assert so.work_order == _abi.SAPB_WORK_ORDER_PREVIOUS_ITERATIONS and so.impulse_history == 3
     assert lib.sapb_create(None, ctypes.byref(so), None) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    # option checks that come before any device access (the model's arrays are never read here)
+    md = _abi.ModelDesc()
+    md.num_worlds, md.joints_per_world, md.bodies_per_world, md.dofs_per_world = 2, 1, 1, 6
+    md.coords_per_world, md.articulations_per_world = 7, 1
+    md.joint_child = md.joint_qd_start = md.joint_dof_dim = md.articulation_start = 16  # never dereferenced
+    h = ctypes.c_void_p()
+    so.warm_start = _abi.SAPB_WARM_START_LEARNED  # without a network
+    assert lib.sapb_create(ctypes.byref(md), ctypes.byref(so), ctypes.byref(h)) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    assert b"network" in lib.sapb_last_error() and not h.value
+    so.warm_start = 7
+    assert lib.sapb_create(ctypes.byref(md), ctypes.byref(so), ctypes.byref(h)) == _abi.SAPB_ERR_INVALID_ARGUMENT
+    so.warm_start = _abi.SAPB_WARM_START_PREVIOUS_VELOCITY
+    so.solve.threads_per_cta = 64  # checked by the solve entry point
+    assert lib.sapb_contact_solve_occupancy_threads(35, 32, _abi.SAPB_FP32, _abi.SAPB_LS_ARMIJO_DECAY, 64) == \
+        _abi.SAPB_ERR_INVALID_ARGUMENT
     assert lib.sapb_step(None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
     assert lib.sapb_get_status(None, None, None, None, None) == _abi.SAPB_ERR_INVALID_ARGUMENT
     lib.sapb_destroy(None)
